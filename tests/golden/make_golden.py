@@ -1,0 +1,494 @@
+"""Generate the golden fixtures of the GPU eikonal path from the reference itself.
+
+Runs only where the reference source tree is available (``--ref``, default
+/root/reference): it imports the reference's numpy modules (``agd.Metrics``,
+``agd.FiniteDifferences``, ``agd.Selling``) for the host-side preparation, and
+drives the reference's own CUDA kernels compiled for the host by
+``oracle/ref_emul/Makefile`` (libraries in ``oracle/_ref/``).
+
+The host loops around the kernels restate, in numpy, the reference's driver code:
+  SetGeometry / SetRHS / SetArgs      agd/Eikonal/HFM_CUDA/_SetGeometry.py:16-282, _SetArgs.py:8-177
+  fast_iterative_method, InitStop     _solvers.py:94-120, _StopCriterion.py:62-84
+  PostProcess (flow), values_expand   _PostProcess.py:19-95
+  SolveAD (reverse), graph_reverse    _PostProcess.py:155-219, graph_reverse.py:10-77
+  GetGeodesics, inf_convolution       _GetGeodesics.py:9-147, inf_convolution.py:24-93
+
+Output: one ``<case>.npz`` per case in this directory, holding the dictIn inputs
+and the reference outputs.  Usage::
+
+    make -C oracle/ref_emul REF=/root/reference
+    python tests/golden/make_golden.py [--ref /root/reference]
+"""
+import argparse
+import ctypes
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REPO = os.path.dirname(os.path.dirname(HERE))
+REFLIB = os.path.join(REPO, "oracle", "_ref")
+P = ctypes.c_void_p
+
+
+def ptr(a):
+    return a.ctypes.data_as(P) if a is not None else None
+
+
+def lib(name):
+    return ctypes.CDLL(os.path.join(REFLIB, name))
+
+
+# ----------------------------------------------------------------------------
+# Seeded synthetic fields
+# ----------------------------------------------------------------------------
+def smooth_noise(rng, shape, sigma):
+    from scipy.ndimage import gaussian_filter
+    g = gaussian_filter(rng.standard_normal(shape), sigma, mode="wrap")
+    return (g - g.mean()) / g.std()
+
+
+def riemann2_metric(rng, shape, sigma, lam_max):
+    th = np.arctan2(smooth_noise(rng, shape, sigma), smooth_noise(rng, shape, sigma))
+    lam = rng.uniform(1.0, lam_max, shape)
+    c, s = np.cos(th), np.sin(th)
+    # M = R diag(1, lam) R^T
+    m00 = c * c + lam * s * s
+    m01 = c * s * (1 - lam)
+    m11 = s * s + lam * c * c
+    return np.stack([np.stack([m00, m01]), np.stack([m01, m11])]).astype(np.float32)
+
+
+def riemann3_metric(rng, shape, sigma, ev_max):
+    from scipy.ndimage import gaussian_filter
+    a = rng.standard_normal((3, 3) + shape)
+    a = gaussian_filter(a, (0, 0) + (sigma,) * 3, mode="wrap")
+    am = np.moveaxis(a, (0, 1), (-2, -1))
+    u, _, vt = np.linalg.svd(am)
+    rot = u @ vt  # polar factor
+    ev = np.exp(rng.uniform(0, np.log(ev_max), shape + (3,)))
+    m = rot @ (ev[..., :, None] * np.swapaxes(rot, -1, -2))
+    return np.moveaxis(m, (-2, -1), (0, 1)).astype(np.float32)
+
+
+# ----------------------------------------------------------------------------
+# Reference pipeline (numpy restatement of the host code + emulated kernels)
+# ----------------------------------------------------------------------------
+MODELS = {
+    "Isotropic2": dict(tag="iso2", shape_i=(16, 16), niter_i=16, front=4),
+    "Isotropic3": dict(tag="iso3", shape_i=(4, 4, 4), niter_i=8, front=4),
+    "Riemann2": dict(tag="riem2", shape_i=(8, 8), niter_i=8, front=4),
+    "Riemann3": dict(tag="riem3", shape_i=(4, 4, 4), niter_i=4, front=6),
+}
+
+
+class RefPipeline:
+    def __init__(self, case):
+        from agd import FiniteDifferences as fd
+        from agd import Metrics
+        self.fd, self.Metrics = fd, Metrics
+        self.c = case
+        self.model = case["model"]
+        self.md = MODELS[self.model]
+        self.ndim = int(self.model[-1])
+        self.shape = tuple(int(s) for s in case["dims"])
+        self.h = np.asarray(case["gridScales"], np.float32)
+        self.origin = np.asarray(case["origin"], np.float32)
+        self.shape_i = self.md["shape_i"]
+        self.size_i = int(np.prod(self.shape_i))
+        self.shape_o = tuple(int(x) for x in fd.round_up_ratio(np.array(self.shape), np.array(self.shape_i)))
+        self.size_o = int(np.prod(self.shape_o))
+        self.multip = bool(case.get("multiprecision", False))
+
+    def bexp(self, a, cval):
+        return np.ascontiguousarray(self.fd.block_expand(a, self.shape_i, mode="constant", constant_values=cval))
+
+    def bsq(self, a):
+        return self.fd.block_squeeze(a, self.shape)
+
+    def point_from_index(self, idx, to=False):
+        start = self.origin + 0.5 * self.h
+        idx = np.asarray(idx, np.float32)
+        return (idx - start) / self.h if to else start + self.h * idx
+
+    def setup(self):
+        c, nd = self.c, self.ndim
+        cost = np.asarray(c.get("cost", np.ones(self.shape, np.float32)), np.float32)
+        cost = np.broadcast_to(cost, self.shape).astype(np.float32)
+        if self.model.startswith("Riemann"):
+            metric = self.Metrics.Riemann.from_HFM(np.asarray(c["metric"], np.float32))
+            dual = metric.with_costs(self.h).dual()
+            self.geom = self.bexp(dual.flatten().astype(np.float32), np.inf)
+        else:
+            self.geom = np.zeros(1, np.float32)
+        float_res = np.finfo(np.float32).resolution
+        self.atol = np.float32(np.nanmean(cost) * float_res * 5.0)
+        self.rtol = np.float32(0.0 if self.multip else float_res * 5.0)
+        seeds = np.asarray(c["seeds"], np.float32)
+        seedValues = np.asarray(c.get("seedValues", np.zeros(len(seeds))), np.float32)
+        seedIdx = np.round(self.point_from_index(seeds, to=True)).astype(int)
+        self.seedIndices = seedIdx
+        rhs = cost.copy()
+        seedTags = np.zeros(self.shape, bool)
+        pos = tuple(seedIdx.T)
+        rhs[pos] = seedValues
+        seedTags[pos] = True
+        self.trigger = seedTags.copy()
+        self.seedTags = seedTags
+        self.rhs_b = self.bexp(rhs, np.inf).astype(np.float32)
+        sp = self.bexp(seedTags, True)
+        self.seeds_b = np.packbits(sp.reshape(-1), bitorder="little")
+        self.values_b = np.full(self.shape_o + self.shape_i, np.inf, np.float32)
+        self.valuesq_b = np.zeros(self.values_b.shape, np.int32) if self.multip else None
+        if self.multip:
+            hmin = float(np.min(self.h))
+            self.multip_step = np.float32(2.0 ** np.floor(np.log2(hmin / 10)))
+            self.multip_max = np.float32(np.iinfo(np.int32).max * float(self.multip_step) / 2)
+        else:
+            self.multip_step = self.multip_max = np.float32(0)
+        self.iso_w = (self.h.astype(np.float32) ** -2).astype(np.float32)
+
+    def solve(self):
+        md = self.md
+        name = f"libagdref_eik_{md['tag']}{'mp' if self.multip else ''}.so"
+        L = lib(name)
+        trig_o = self.bexp(self.trigger, False).reshape(self.shape_o + (-1,)).any(-1).astype(np.uint8)
+        nup = ctypes.c_longlong(0)
+        L.agdref_fim_solve.restype = ctypes.c_int
+        shp = (ctypes.c_int * self.ndim)(*self.shape)
+        self.niter_o = L.agdref_fim_solve(
+            shp, ctypes.c_float(self.atol), ctypes.c_float(self.rtol), md["front"], ptr(self.iso_w),
+            ctypes.c_float(self.multip_step), ctypes.c_float(self.multip_max), ptr(self.values_b),
+            ptr(self.valuesq_b), ptr(self.geom), ptr(self.seeds_b), ptr(self.rhs_b), ptr(trig_o), 2000,
+            ctypes.byref(nup))
+        self.tile_visits = nup.value
+
+    def values(self):
+        v = self.values_b
+        if self.multip:
+            v = v + self.valuesq_b.astype(np.float32) * self.multip_step
+        return self.bsq(v)
+
+    def flow(self):
+        assert not self.multip
+        L = lib(f"libagdref_flow_{self.md['tag']}.so")
+        nd, st = self.ndim, self.size_o * self.size_i
+        nact = self.ndim if self.model.startswith("Iso") else self.ndim * (self.ndim + 1) // 2
+        self.nact = nact
+        oi = self.shape_o + self.shape_i
+        self.fw = np.empty((nact,) + oi, np.float32)
+        self.fws = np.empty(oi, np.float32)
+        self.fi = np.empty((nact,) + oi, np.int32)
+        self.fv = np.empty((nd,) + oi, np.float32)
+        L.agdref_flow((ctypes.c_int * nd)(*self.shape), ptr(self.iso_w), ctypes.c_float(0), ctypes.c_float(0),
+                      ptr(self.values_b), None, ptr(self.geom), ptr(self.seeds_b), ptr(self.rhs_b),
+                      ptr(self.fw), ptr(self.fws), ptr(self.fi), ptr(self.fv))
+
+    def infconv_eucl(self):
+        nd = self.ndim
+        L = lib(f"libagdref_infconv{nd}.so")
+        L.agdref_infconv.restype = P
+        rg = np.arange(-1, 2)
+        X = np.meshgrid(*(rg,) * nd)
+        kern = np.round(5 * np.sqrt(sum(x.astype(float) ** 2 for x in X))).astype(np.uint8)
+        kern = np.ascontiguousarray(kern)
+        eucl = np.full(self.shape, 255, np.uint8)
+        eucl[self.trigger] = 0
+        out = np.empty_like(eucl)
+        res = L.agdref_infconv((ctypes.c_int * nd)(*self.shape), ptr(kern), 6, ptr(eucl), ptr(out))
+        arr = eucl if res == eucl.ctypes.data else out
+        arr = arr.copy()
+        arr[arr > 5 * 6] = 255
+        return arr
+
+    def geodesics(self, tips):
+        nd = self.ndim
+        L = lib(f"libagdref_geo{nd}_{self.shape_i[0]}.so")
+        eucl = self.infconv_eucl()
+        eucl_b = self.bexp(eucl, 255).astype(np.uint8)
+        step = 0.25
+        max_len = int(max(40, 20 * np.max(self.shape) / step))
+        typical_len = min(max_len, int(max(40, 0.5 * np.max(self.shape) / step)))
+        tips_c = self.point_from_index(tips, to=True).astype(np.float32)
+        geos = [[t.reshape(1, -1)] for t in tips_c]
+        stops = ["Stopping criterion"] * len(tips_c)
+        corresp = list(range(len(tips_c)))
+        codes = ["Continue", "AtSeed", "InWall", "Stationnary", "PastSeed", "VanishingFlow"]
+        geoIt, geoMaxIt = 0, int(np.ceil(max_len / typical_len))
+        pastseed = 0
+        while corresp:
+            if geoIt >= geoMaxIt:
+                break
+            geoIt += 1
+            nG = len(corresp)
+            x_s = np.full((nG, typical_len, nd), np.nan, np.float32)
+            x_s[:, 0, :] = np.stack([geos[i][-1][-1, :] for i in corresp])
+            len_s = np.full(nG, -1, np.int32)
+            stop_s = np.full(nG, -1, np.int8)
+            L.agdref_geodesic_chunk((ctypes.c_int * nd)(*self.shape), nG, typical_len, pastseed,
+                                    ctypes.c_float(4.0), ctypes.c_float(step), ptr(self.values_b),
+                                    ptr(self.fv), ptr(self.fws), ptr(eucl_b), ptr(x_s), ptr(len_s),
+                                    ptr(stop_s))
+            nxt = []
+            for i, x, l, s in zip(corresp, x_s, len_s, stop_s):
+                geos[i].append(x[1:int(l)])
+                if s != 0:
+                    stops[i] = codes[int(s)]
+                else:
+                    nxt.append(i)
+            corresp = nxt
+            pastseed = 0
+        cat = [np.concatenate(g, axis=0) for g in geos]
+        phys = [self.point_from_index(g).T for g in cat]
+        return phys, stops, eucl
+
+    def reverse_ad(self, sens):
+        """sens: (*shape, 1).  Returns (costSensitivity, seedValueSensitivity)."""
+        nd = self.ndim
+        diag = self.fws.copy()
+        boundary = diag == 0.0
+        diag[boundary] = 1.0
+        invalid = np.iinfo(np.int32).max
+        indices = self.fi.copy()
+        weights = self.fw
+        indices[weights == 0] = invalid
+        idxT, wT = self.graph_reverse(indices, weights, invalid)
+        rhs = self.bexp(np.moveaxis(sens, -1, 0).astype(np.float32), np.nan)
+        rhs = np.ascontiguousarray(rhs.astype(np.float32))
+        tag = self.md["tag"]
+        L = lib(f"libagdref_lin_{tag}_r.so")
+        L.agdref_nindex.restype = ctypes.c_int
+        nidx = L.agdref_nindex()
+        assert len(idxT) <= nidx, (len(idxT), nidx)
+        st = self.size_o * self.size_i
+        idx_pad = np.full((nidx, st), invalid, np.int32)
+        w_pad = np.zeros((nidx, st), np.float32)
+        idx_pad[: len(idxT)] = idxT.reshape(len(idxT), -1)
+        w_pad[: len(wT)] = wT.reshape(len(wT), -1)
+        float_res = np.finfo(np.float32).resolution
+        rtol = np.float32(float_res * 5)
+        fin = rhs[np.isfinite(rhs)]
+        atol = np.float32(rtol * np.mean(np.abs(fin)))
+        sol = np.full(rhs.shape, np.inf, np.float32)
+        domain = np.isfinite(self.values_b)
+        trigger = np.logical_and(np.all(w_pad.reshape((nidx,) + domain.shape) == 0.0, axis=0), domain)
+        trig_o = trigger.reshape(self.shape_o + (-1,)).any(-1).astype(np.uint8)
+        self.rev_niter = L.agdref_linear_solve((ctypes.c_int * nd)(*self.shape_o), ctypes.c_float(atol),
+                                               ctypes.c_float(rtol), ptr(sol), ptr(rhs), ptr(diag),
+                                               ptr(idx_pad), ptr(w_pad), ptr(trig_o), 2000)
+        allS = np.moveaxis(self.bsq(sol), 0, -1)
+        pos = tuple(self.seedIndices.T)
+        seedS = allS[pos].copy()
+        allS[pos] = 0
+        return allS, seedS
+
+    def graph_reverse(self, fwd, fwd_weight, invalid, nrev=None):
+        L = lib("libagdref_graphrev.so")
+        nfwd = len(fwd)
+        shape = fwd.shape[1:]
+        size = int(np.prod(shape))
+        if nrev is None:
+            nrev = 2 * nfwd
+        assert nrev <= 127
+        rev = np.full((nrev,) + shape, invalid, np.int32)
+        rev_w = np.zeros((nrev,) + shape, np.float32)
+        irev = np.zeros((nfwd,) + shape, np.int8)
+        fwd = np.ascontiguousarray(fwd)
+        fwd_weight = np.ascontiguousarray(fwd_weight)
+        irev_mmax = 0
+        for _ in range(nrev):
+            irev_max = int(np.max(irev))
+            irev_mmax = max(irev_max, irev_mmax)
+            if irev_max == -1:
+                return rev[: irev_mmax + 1], rev_w[: irev_mmax + 1]
+            if irev_max == nrev:
+                return self.graph_reverse(fwd, fwd_weight, invalid, 2 * nrev)
+            L.agdref_graph_reverse_launch(size, nfwd, nrev, ptr(fwd), ptr(rev), ptr(irev), ptr(fwd_weight),
+                                          ptr(rev_w))
+        raise RuntimeError("graph_reverse did not terminate")
+
+
+# ----------------------------------------------------------------------------
+# Cases
+# ----------------------------------------------------------------------------
+def rect(dims, h, origin=None):
+    dims = np.asarray(dims, np.float32)
+    return dict(dims=dims, gridScales=np.full(len(dims), h, np.float32),
+                origin=np.zeros(len(dims), np.float32) if origin is None else np.asarray(origin, np.float32))
+
+
+def make_cases():
+    cases = {}
+    rng = np.random.default_rng(1234)
+    # Isotropic2, non-multiple-of-tile shape, variable cost, two seeds, tips, receivers
+    sh = (70, 53)
+    c = dict(model="Isotropic2", **rect(sh, 1.0 / 70))
+    c["cost"] = np.exp(0.5 * smooth_noise(rng, sh, 3.0)).astype(np.float32)
+    c["seeds"] = np.array([[0.31, 0.22], [0.72, 0.55]], np.float32)
+    c["seedValues"] = np.array([0.0, 0.05], np.float32)
+    c["tips"] = c["seeds"][:1] * 0 + rng.uniform(0.05, 0.7, (6, 2)).astype(np.float32)
+    cases["iso2"] = c
+    # Riemann2 anisotropic, three seeds with seed values
+    sh = (61, 77)
+    c = dict(model="Riemann2", **rect(sh, 1.0 / 61))
+    m = riemann2_metric(rng, sh, 6.0, 20.0)
+    c["metric"] = np.moveaxis(np.stack([m[0, 0], m[1, 0], m[1, 1]]), 0, -1)
+    c["seeds"] = np.array([[0.2, 0.3], [0.7, 0.9], [0.5, 0.6]], np.float32)
+    c["seedValues"] = np.array([0.0, 0.1, 0.05], np.float32)
+    c["tips"] = rng.uniform(0.05, 0.95, (6, 2)).astype(np.float32) * np.array([1.0, 77 / 61], np.float32)
+    cases["riem2"] = c
+    # Same Riemann2 problem with the multiprecision option
+    c2 = dict(c)
+    c2["multiprecision"] = True
+    c2.pop("tips")
+    cases["riem2_mp"] = c2
+    # Riemann2 with the anisotropy range of the 1024^2 workload (lambda in [1,100])
+    sh = (64, 64)
+    c = dict(model="Riemann2", **rect(sh, 1.0 / 64))
+    m = riemann2_metric(rng, sh, 4.0, 100.0)
+    c["metric"] = np.moveaxis(np.stack([m[0, 0], m[1, 0], m[1, 1]]), 0, -1)
+    c["seeds"] = rng.uniform(0.1, 0.9, (4, 2)).astype(np.float32)
+    c["tips"] = rng.uniform(0.05, 0.95, (8, 2)).astype(np.float32)
+    cases["riem2_aniso"] = c
+    # Isotropic3
+    sh = (21, 18, 23)
+    c = dict(model="Isotropic3", **rect(sh, 1.0 / 21))
+    c["cost"] = np.exp(0.5 * smooth_noise(rng, sh, 2.0)).astype(np.float32)
+    c["seeds"] = np.array([[0.5, 0.4, 0.5]], np.float32)
+    c["tips"] = rng.uniform(0.05, 0.8, (4, 3)).astype(np.float32)
+    cases["iso3"] = c
+    # Riemann3
+    sh = (20, 22, 19)
+    c = dict(model="Riemann3", **rect(sh, 1.0 / 20))
+    m = riemann3_metric(rng, sh, 2.0, 9.0)
+    c["metric"] = np.moveaxis(np.stack([m[i, j] for i in range(3) for j in range(i + 1)]), 0, -1)
+    c["seeds"] = np.array([[0.45, 0.5, 0.48]], np.float32)
+    c["tips"] = rng.uniform(0.05, 0.9, (4, 3)).astype(np.float32)
+    cases["riem3"] = c
+    # EikonalAD_GPU.ipynb cells 35-42: seedValueSensitivity == [[0],[1]]
+    n = 50
+    c = dict(model="Isotropic2", dims=np.array([n + 1, n + 1], np.float32),
+             gridScales=np.full(2, 1.0 / n, np.float32), origin=np.full(2, -0.5 / n, np.float32))
+    c["seeds"] = np.array([[0.0, 0.0], [0.0, 0.5]], np.float32)
+    c["cost"] = np.ones((n + 1, n + 1), np.float32)
+    c["traits"] = dict(shape_i=(8, 8), niter_i=16)
+    sens = np.zeros((n + 1, n + 1, 1), np.float32)
+    sens[-1, -1] = 1.0
+    c["sensitivity"] = sens
+    cases["ad_notebook"] = c
+    # receivers sensitivity for the other AD cases
+    for key in ("iso2", "riem2", "riem3", "iso3"):
+        cc = cases[key]
+        shp = tuple(int(s) for s in cc["dims"])
+        sens = np.zeros(shp + (1,), np.float32)
+        flat = rng.choice(int(np.prod(shp)), 5, replace=False)
+        sens.reshape(-1)[flat] = 1.0
+        cc["sensitivity"] = sens
+    return cases
+
+
+def run_case(name, case):
+    pipe = RefPipeline(case)
+    if "traits" in case:
+        tr = case["traits"]
+        assert pipe.model == "Isotropic2" and tuple(tr["shape_i"]) == (8, 8) and tr["niter_i"] == 16
+        pipe.md = dict(pipe.md, shape_i=(8, 8), niter_i=16, tag="iso2s8")
+        pipe.shape_i = pipe.md["shape_i"]
+        pipe.size_i = int(np.prod(pipe.shape_i))
+        pipe.shape_o = tuple(int(x) for x in pipe.fd.round_up_ratio(np.array(pipe.shape), np.array(pipe.shape_i)))
+        pipe.size_o = int(np.prod(pipe.shape_o))
+    pipe.setup()
+    pipe.solve()
+    out = dict(values=pipe.values().astype(np.float32), niter_o=pipe.niter_o, tile_visits=pipe.tile_visits,
+               atol=pipe.atol, rtol=pipe.rtol)
+    if not pipe.multip:
+        pipe.flow()
+        out["values_after_flow"] = pipe.values().astype(np.float32)
+        out["flow_vector"] = np.stack([pipe.bsq(v) for v in pipe.fv]).astype(np.float32)
+        out["flow_weightsum"] = pipe.bsq(pipe.fws).astype(np.float32)
+        if "tips" in case:
+            geos, stops, eucl = pipe.geodesics(case["tips"])
+            out["geodesic_lengths"] = np.array([g.shape[1] for g in geos], np.int32)
+            out["geodesics_concat"] = np.concatenate(geos, axis=1).astype(np.float32)
+            out["geodesic_stopping_criteria"] = np.array(stops)
+            out["eucl"] = eucl
+        if "sensitivity" in case:
+            cs, ss = pipe.reverse_ad(case["sensitivity"])
+            out["costSensitivity"] = cs.astype(np.float32)
+            out["seedValueSensitivity"] = ss.astype(np.float32)
+    return out
+
+
+def selling_fixture(rng, nd, n):
+    """Reference kernel decomposition (fp32) and agd.Selling (fp64) of random SPD tensors."""
+    from agd import Selling
+    if nd == 2:
+        th = rng.uniform(0, np.pi, n)
+        lam = np.exp(rng.uniform(0, np.log(100), n))
+        c, s = np.cos(th), np.sin(th)
+        M = np.stack([np.stack([c * c + lam * s * s, c * s * (1 - lam)]),
+                      np.stack([c * s * (1 - lam), s * s + lam * c * c])])
+        flat = np.stack([M[0, 0], M[1, 0], M[1, 1]], -1).astype(np.float32)
+    else:
+        a = rng.standard_normal((n, 3, 3))
+        q, _ = np.linalg.qr(a)
+        ev = np.exp(rng.uniform(0, np.log(50), (n, 3)))
+        Mm = q @ (ev[:, :, None] * np.swapaxes(q, 1, 2))
+        M = np.moveaxis(Mm, 0, -1)
+        flat = np.stack([Mm[:, i, j] for i in range(3) for j in range(i + 1)], -1).astype(np.float32)
+    sd = nd * (nd + 1) // 2
+    L = lib(f"libagdref_eik_riem{nd}.so")
+    w = np.zeros((n, sd), np.float32)
+    e = np.zeros((n, sd, nd), np.int32)
+    L.agdref_selling(ptr(np.ascontiguousarray(flat)), n, ptr(w), ptr(e))
+    M64 = np.zeros((nd, nd, n))
+    k = 0
+    for i in range(nd):
+        for j in range(i + 1):
+            M64[i, j] = flat[:, k]
+            M64[j, i] = flat[:, k]
+            k += 1
+    cw, ce = Selling.Decomposition(M64)
+    return dict(m=flat, ref_w=w, ref_e=e, agd_w=np.moveaxis(cw, -1, 0), agd_e=np.moveaxis(ce, -1, 0).astype(np.int32))
+
+
+def save(name, case, out):
+    d = {}
+    for k, v in case.items():
+        if k == "traits":
+            d["in_traits_shape_i"] = np.array(v["shape_i"], np.int32)
+            d["in_traits_niter_i"] = np.int32(v["niter_i"])
+        elif k == "model":
+            d["in_model"] = np.array(v)
+        else:
+            d["in_" + k] = np.asarray(v)
+    for k, v in out.items():
+        d["out_" + k] = np.asarray(v)
+    np.savez_compressed(os.path.join(HERE, name + ".npz"), **d)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--ref", default="/root/reference")
+    ap.add_argument("--only", default=None)
+    args = ap.parse_args()
+    sys.path.insert(0, args.ref)
+    cases = make_cases()
+    for name, case in cases.items():
+        if args.only and name != args.only:
+            continue
+        out = run_case(name, case)
+        save(name, case, out)
+        print(name, "niter_o", out["niter_o"], "visits", out["tile_visits"],
+              "stops", list(out.get("geodesic_stopping_criteria", [])))
+    if not args.only or args.only.startswith("selling"):
+        rng = np.random.default_rng(99)
+        for nd in (2, 3):
+            f = selling_fixture(rng, nd, 3000)
+            np.savez_compressed(os.path.join(HERE, f"selling{nd}.npz"), **f)
+            print("selling", nd)
+
+
+if __name__ == "__main__":
+    main()
