@@ -1,0 +1,226 @@
+"""Python face of the CPU oracle (liboracle.so, built from hfm_oracle.cpp).
+
+TEST INFRASTRUCTURE: imported only by tests/, __graft_entry__.smoke() and the
+CPU-baseline leg of bench.py, as the checker or the timed CPU baseline.  The
+product path never imports it.
+
+`run(case, dtype)` restates the reference's GPU pipeline for one dictIn-like
+case dictionary (keys as in agd.Eikonal.dictIn): host preparation
+(agd/Eikonal/HFM_CUDA/_SetGeometry.py:127-137,238-253; _SetArgs.py:8-133),
+solve (FIM over tiles), flow, geodesics (_GetGeodesics.py:9-147) and reverse
+sensitivity (_PostProcess.py:155-219), on the CPU, in float32 or float64.
+"""
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB = os.path.join(HERE, "liboracle.so")
+_P = ctypes.c_void_p
+_lib = None
+
+DEFAULT_TRAITS = {  # agd/Eikonal/HFM_CUDA/kernel_traits.py:61-88
+    "Riemann2": ((8, 8), 8, 4),
+    "Riemann3": ((4, 4, 4), 4, 6),
+    "Isotropic2": ((16, 16), 16, 4),
+    "Isotropic3": ((4, 4, 4), 8, 4),
+}
+STOP_CODES = ["Continue", "AtSeed", "InWall", "Stationnary", "PastSeed", "VanishingFlow"]
+
+
+def build():
+    """Compile liboracle.so (g++, OpenMP)."""
+    src = os.path.join(HERE, "hfm_oracle.cpp")
+    subprocess.check_call(["g++", "-O2", "-fPIC", "-shared", "-std=c++17", "-fopenmp", "-ffp-contract=off",
+                           "-Wno-unknown-pragmas", src, "-o", LIB])
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB):
+            build()
+        _lib = ctypes.CDLL(LIB)
+        _lib.agdo_eikonal.restype = ctypes.c_int
+        _lib.agdo_reverse.restype = ctypes.c_int
+    return _lib
+
+
+def _p(a):
+    return None if a is None else a.ctypes.data_as(_P)
+
+
+def selling(m):
+    """Selling decomposition of packed symmetric matrices m (n, symdim) float32.
+    Returns weights (n, symdim) and integer offsets (n, symdim, ndim)."""
+    m = np.ascontiguousarray(m, np.float32)
+    n, sd = m.shape
+    nd = 2 if sd == 3 else 3
+    w = np.zeros((n, sd), np.float32)
+    e = np.zeros((n, sd, nd), np.int32)
+    lib().agdo_selling_f32(nd, _p(m), n, _p(w), _p(e))
+    return w, e
+
+
+def dual_metric_flat(metric_hfm, h):
+    """Dual of metric.with_costs(h), lower-triangular planes (symdim, *shape), float32.
+    metric_hfm: (*shape, symdim) HFM layout (Metrics.Riemann.from_HFM)."""
+    mh = np.asarray(metric_hfm, np.float32)
+    nd = 2 if mh.shape[-1] == 3 else 3
+    M = np.zeros(mh.shape[:-1] + (nd, nd), np.float32)
+    k = 0
+    for i in range(nd):
+        for j in range(i + 1):
+            M[..., i, j] = mh[..., k]
+            M[..., j, i] = mh[..., k]
+            k += 1
+    h = np.asarray(h, np.float32)
+    M = M * h[:, None] * h[None, :]
+    Dm = np.linalg.inv(M).astype(np.float32)
+    return np.stack([Dm[..., i, j] for i in range(nd) for j in range(i + 1)]).astype(np.float32)
+
+
+class Prepared:
+    pass
+
+
+def prepare(case):
+    """Host preparation of a case (model, dims, gridScales, origin, cost, metric,
+    seeds, seedValues, traits, multiprecision)."""
+    pr = Prepared()
+    pr.model = str(case["model"])
+    pr.ndim = int(pr.model[-1])
+    pr.riemann = pr.model.startswith("Riemann")
+    pr.shape = tuple(int(s) for s in np.asarray(case["dims"]))
+    pr.h = np.broadcast_to(np.asarray(case.get("gridScales", case.get("gridScale")), np.float32), (pr.ndim,)).copy()
+    pr.origin = np.asarray(case.get("origin", np.zeros(pr.ndim)), np.float32)
+    si, niter, front = DEFAULT_TRAITS[pr.model]
+    tr = case.get("traits")
+    if tr is not None:
+        si = tuple(int(s) for s in tr.get("shape_i", si))
+        niter = int(tr.get("niter_i", niter))
+    pr.shape_i, pr.niter_i, pr.front = tuple(si), niter, int(case.get("fim_front_width", front))
+    cost = np.broadcast_to(np.asarray(case.get("cost", 1.0), np.float32), pr.shape).astype(np.float32)
+    pr.geom = dual_metric_flat(case["metric"], pr.h) if pr.riemann else None
+    res = np.finfo(np.float32).resolution
+    pr.atol = float(np.float32(np.nanmean(cost) * res * 5.0)) if "atol" not in case else float(case["atol"])
+    pr.rtol = float(np.float32(res * 5.0)) if "rtol" not in case else float(case["rtol"])
+    seeds = np.asarray(case["seeds"], np.float32).reshape(-1, pr.ndim)
+    sv = np.asarray(case.get("seedValues", np.zeros(len(seeds))), np.float32)
+    start = pr.origin + 0.5 * pr.h
+    pr.seed_idx = np.round((seeds - start) / pr.h).astype(int)
+    rhs = cost.copy()
+    mask = np.zeros(pr.shape, np.uint8)
+    pos = tuple(pr.seed_idx.T)
+    rhs[pos] = sv
+    mask[pos] = 1
+    pr.rhs, pr.seed_mask = rhs, mask
+    pr.iso_w = (pr.h.astype(np.float64) ** -2) if not pr.riemann else None
+    if pr.iso_w is not None:
+        pr.iso_w = np.asarray(pr.h.astype(np.float32) ** -2, np.float64)
+    return pr
+
+
+def eikonal(pr, dtype=np.float32, values=None, nthreads=1, flow=False, nitermax=2000):
+    """Solve; returns dict(values, niter_o, tile_visits[, flow_vector, flow_weightsum, flow_weights, flow_indices])."""
+    L = lib()
+    N = int(np.prod(pr.shape))
+    u = np.full(pr.shape, np.inf, np.float64) if values is None else np.array(values, np.float64)
+    visits = ctypes.c_longlong(0)
+    nact = pr.ndim * (pr.ndim + 1) // 2 if pr.riemann else pr.ndim
+    fv = fws = fw = fi = None
+    if flow:
+        fv = np.zeros((pr.ndim,) + pr.shape)
+        fws = np.zeros(pr.shape)
+        fw = np.zeros((nact,) + pr.shape)
+        fi = np.zeros((nact,) + pr.shape, np.int32)
+    geom = None if pr.geom is None else np.ascontiguousarray(pr.geom, np.float32)
+    iso = None if pr.iso_w is None else np.ascontiguousarray(pr.iso_w, np.float64)
+    niter = L.agdo_eikonal(int(dtype == np.float64), pr.ndim, 1 if pr.riemann else 0,
+                           (ctypes.c_int * pr.ndim)(*pr.shape), (ctypes.c_int * pr.ndim)(*pr.shape_i),
+                           pr.niter_i, pr.front, _p(iso), _p(geom), _p(np.ascontiguousarray(pr.rhs)),
+                           _p(np.ascontiguousarray(pr.seed_mask)), _p(u), ctypes.c_double(pr.atol),
+                           ctypes.c_double(pr.rtol), nitermax, nthreads, ctypes.byref(visits), _p(fv), _p(fws),
+                           _p(fw), _p(fi))
+    out = dict(values=u, niter_o=niter, tile_visits=visits.value)
+    if flow:
+        out.update(flow_vector=fv, flow_weightsum=fws, flow_weights=fw, flow_indices=fi)
+    return out
+
+
+def geodesics(pr, values, flow_vector, flow_weightsum, tips, step=0.25, causality=4.0):
+    """Backtrack from physical tips; returns (list of (ndim, len) physical paths, stop codes)."""
+    L = lib()
+    nd = pr.ndim
+    shp = (ctypes.c_int * nd)(*pr.shape)
+    eucl = np.zeros(pr.shape, np.uint8)
+    L.agdo_eucl_map(nd, shp, _p(np.ascontiguousarray(pr.seed_mask)), _p(eucl))
+    u = np.ascontiguousarray(values, np.float32)
+    fv = np.ascontiguousarray(flow_vector, np.float32)
+    fws = np.ascontiguousarray(flow_weightsum, np.float32)
+    max_len = int(max(40, 20 * max(pr.shape) / step))
+    typical = min(max_len, int(max(40, 0.5 * max(pr.shape) / step)))
+    eucl_delay = int(np.sqrt(nd) / step)
+    nymin_delay = int(8.0 * np.sqrt(nd) / step)
+    start = pr.origin + 0.5 * pr.h
+    tips_c = ((np.asarray(tips, np.float32) - start) / pr.h).astype(np.float32)
+    geos = [[t.reshape(1, -1)] for t in tips_c]
+    stops = ["Stopping criterion"] * len(tips_c)
+    corresp = list(range(len(tips_c)))
+    it, maxit = 0, int(np.ceil(max_len / typical))
+    while corresp and it < maxit:
+        it += 1
+        n = len(corresp)
+        x_s = np.full((n, typical, nd), np.nan, np.float32)
+        x_s[:, 0] = np.stack([geos[i][-1][-1] for i in corresp])
+        len_s = np.zeros(n, np.int32)
+        stop_s = np.zeros(n, np.int8)
+        L.agdo_geodesic_chunk(nd, shp, n, typical, 0, ctypes.c_float(causality), ctypes.c_float(step), eucl_delay,
+                              nymin_delay, _p(u), _p(fv), _p(fws), _p(eucl), _p(x_s), _p(len_s), _p(stop_s))
+        nxt = []
+        for i, x, l, s in zip(corresp, x_s, len_s, stop_s):
+            geos[i].append(x[1:int(l)])
+            if s != 0:
+                stops[i] = STOP_CODES[int(s)]
+            else:
+                nxt.append(i)
+        corresp = nxt
+    paths = [(start + pr.h * np.concatenate(g, 0)).T for g in geos]
+    return paths, stops
+
+
+def reverse(pr, values, flow_weights, flow_indices, flow_weightsum, sens):
+    """Reverse sensitivity lam (grid) for rhs `sens` (grid, float)."""
+    nact = flow_weights.shape[0]
+    N = int(np.prod(pr.shape))
+    lam = np.zeros(N)
+    lib().agdo_reverse(nact, ctypes.c_long(N), _p(np.ascontiguousarray(values, np.float64).reshape(-1)),
+                       _p(np.ascontiguousarray(flow_weights, np.float64).reshape(nact, -1)),
+                       _p(np.ascontiguousarray(flow_indices, np.int32).reshape(nact, -1)),
+                       _p(np.ascontiguousarray(flow_weightsum, np.float64).reshape(-1)),
+                       _p(np.ascontiguousarray(sens, np.float64).reshape(-1)), _p(lam))
+    return lam.reshape(pr.shape)
+
+
+def run(case, dtype=np.float32, nthreads=1):
+    """Whole pipeline for a case; returns a dict like the reference's hfmOut."""
+    pr = prepare(case)
+    need_flow = "tips" in case or "sensitivity" in case
+    r = eikonal(pr, dtype, nthreads=nthreads, flow=need_flow)
+    out = dict(values=r["values"], niter_o=r["niter_o"], tile_visits=r["tile_visits"], prepared=pr)
+    if need_flow:
+        out["flow_vector"], out["flow_weightsum"] = r["flow_vector"], r["flow_weightsum"]
+    if "tips" in case:
+        out["geodesics"], out["geodesic_stopping_criteria"] = geodesics(
+            pr, r["values"], r["flow_vector"], r["flow_weightsum"], case["tips"])
+    if "sensitivity" in case:
+        sens = np.asarray(case["sensitivity"])[..., 0]
+        lam = reverse(pr, r["values"], r["flow_weights"], r["flow_indices"], r["flow_weightsum"], sens)
+        pos = tuple(pr.seed_idx.T)
+        out["seedValueSensitivity"] = lam[pos][:, None]
+        cs = lam.copy()
+        cs[pos] = 0
+        out["costSensitivity"] = cs[..., None]
+    return out

@@ -1,0 +1,36 @@
+import os
+import sys
+
+import numpy as np
+import pytest
+
+REPO = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+if REPO not in sys.path:
+    sys.path.insert(0, REPO)
+GOLDEN = os.path.join(REPO, "tests", "golden")
+
+
+def pytest_configure(config):
+    config.addinivalue_line("markers", "gpu: needs a CUDA GPU (B200) and the built CUDA library")
+
+
+def load_case(name):
+    """Golden fixture -> (dictIn-like case dict, reference outputs dict)."""
+    d = np.load(os.path.join(GOLDEN, name + ".npz"))
+    case = {k[3:]: d[k] for k in d.files if k.startswith("in_")}
+    case["model"] = str(case["model"])
+    if "traits_shape_i" in case:
+        case["traits"] = dict(shape_i=tuple(int(s) for s in case.pop("traits_shape_i")),
+                              niter_i=int(case.pop("traits_niter_i")))
+    if "multiprecision" in case:
+        case["multiprecision"] = bool(case["multiprecision"])
+    out = {k[4:]: d[k] for k in d.files if k.startswith("out_")}
+    return case, out
+
+
+CASES = ["iso2", "riem2", "riem2_aniso", "iso3", "riem3", "ad_notebook"]
+
+
+@pytest.fixture(params=CASES)
+def golden_case(request):
+    return (request.param,) + load_case(request.param)

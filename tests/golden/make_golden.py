@@ -450,7 +450,7 @@ def selling_fixture(rng, nd, n):
             M64[j, i] = flat[:, k]
             k += 1
     cw, ce = Selling.Decomposition(M64)
-    return dict(m=flat, ref_w=w, ref_e=e, agd_w=np.moveaxis(cw, -1, 0), agd_e=np.moveaxis(ce, -1, 0).astype(np.int32))
+    return dict(m=flat, ref_w=w, ref_e=e, agd_w=np.moveaxis(cw, -1, 0), agd_e=np.moveaxis(ce, -1, 0).transpose(0, 2, 1).astype(np.int32))
 
 
 def save(name, case, out):

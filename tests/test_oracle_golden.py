@@ -1,0 +1,100 @@
+"""The CPU oracle against golden outputs of the reference's own kernels.
+
+The fixtures in tests/golden were produced by tests/golden/make_golden.py, which
+runs the reference's CUDA sources compiled for the host.  These tests pin the
+oracle that the GPU parity tests then use at sizes beyond the fixtures.
+"""
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from conftest import load_case, CASES
+
+REL = 1e-5  # parity bar for float32 values
+
+
+def _geodesic_split(out):
+    L, G = out["geodesic_lengths"], out["geodesics_concat"]
+    o, res = 0, []
+    for l in L:
+        res.append(G[:, o:o + l])
+        o += l
+    return res
+
+
+@pytest.mark.parametrize("name", CASES)
+@pytest.mark.parametrize("dtype", [np.float32, np.float64])
+def test_values(name, dtype):
+    case, ref = load_case(name)
+    r = O.run(case, dtype)
+    want = ref.get("values_after_flow", ref["values"])
+    fin = np.isfinite(want)
+    assert np.array_equal(fin, np.isfinite(r["values"]))
+    rel = np.abs(r["values"][fin] - want[fin]) / np.maximum(np.abs(want[fin]), 1e-30)
+    assert rel.max() < REL
+    if dtype == np.float32:  # same schedule: same number of outer iterations and tile visits
+        assert r["niter_o"] == int(ref["niter_o"])
+        assert r["tile_visits"] == int(ref["tile_visits"])
+
+
+@pytest.mark.parametrize("name", [c for c in CASES if c != "ad_notebook"])
+def test_geodesics(name):
+    case, ref = load_case(name)
+    r = O.run(case, np.float32)
+    assert list(r["geodesic_stopping_criteria"]) == [str(s) for s in ref["geodesic_stopping_criteria"]]
+    for p, g in zip(r["geodesics"], _geodesic_split(ref)):
+        assert p.shape == g.shape
+        assert np.abs(p - g).max() < 1e-4 * np.abs(g).max()
+
+
+@pytest.mark.parametrize("name", ["iso2", "riem2", "iso3", "riem3", "ad_notebook"])
+def test_reverse_sensitivity(name):
+    case, ref = load_case(name)
+    r = O.run(case, np.float64)
+    cs, want = r["costSensitivity"], ref["costSensitivity"]
+    assert np.abs(cs - want).max() <= 1e-5 * np.abs(want).max()
+    np.testing.assert_allclose(r["seedValueSensitivity"], ref["seedValueSensitivity"], rtol=1e-5, atol=1e-6)
+
+
+def test_ad_notebook_known_answer():
+    """EikonalAD_GPU.ipynb cell 42: seedValueSensitivity == [[0],[1]] within 1e-6."""
+    case, _ = load_case("ad_notebook")
+    r = O.run(case, np.float64)
+    assert np.abs(r["seedValueSensitivity"] - np.array([[0.0], [1.0]])).max() < 1e-6
+
+
+@pytest.mark.parametrize("nd", [2, 3])
+def test_selling_bitexact(nd):
+    """Offsets bit-exact against the reference kernel's decomposition; weights to an ulp."""
+    import os
+    from conftest import GOLDEN
+    f = np.load(os.path.join(GOLDEN, f"selling{nd}.npz"))
+    w, e = O.selling(f["m"])
+    assert np.array_equal(e, f["ref_e"])
+    np.testing.assert_allclose(w, f["ref_w"], rtol=2e-6, atol=0)
+
+
+def _canonical(w, e, thresh):
+    out = set()
+    for wk, ek in zip(w, e):
+        if wk <= thresh:
+            continue
+        ek = tuple(int(x) for x in ek)
+        neg = tuple(-x for x in ek)
+        out.add(max(ek, neg))
+    return out
+
+
+@pytest.mark.parametrize("nd", [2, 3])
+def test_selling_vs_agd_selling(nd):
+    """Same positive-weight offset sets (up to sign and order) as agd.Selling.Decomposition."""
+    import os
+    from conftest import GOLDEN
+    f = np.load(os.path.join(GOLDEN, f"selling{nd}.npz"))
+    w, e = O.selling(f["m"])
+    bad = 0
+    for i in range(len(w)):
+        tw = 1e-5 * f["agd_w"][i].max()
+        if _canonical(w[i], e[i], tw) != _canonical(f["agd_w"][i], f["agd_e"][i], tw):
+            bad += 1
+    assert bad == 0
