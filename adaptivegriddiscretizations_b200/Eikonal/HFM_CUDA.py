@@ -1,0 +1,629 @@
+"""GPU eikonal solver behind dictIn.Run() (the reference's HFM_CUDA package).
+
+`RunGPU(hfmIn)` mirrors agd/Eikonal/HFM_CUDA/__init__.py:10-25 and the
+Interface class of _Interface.py:23-174: every key is read through GetValue,
+which records help texts, defaults, used and unused keys in
+hfmOut['keys']; the same keys, defaults and errors as the reference are used
+for the Isotropic2/3 and Riemann2/3 models.  The work is done by
+libagd_b200.so through the C ABI of include/agd_b200.h:
+  SetGeometry/SetArgs  -> agd_prep_geom, agd_block_expand, agd_prep_seeds
+  Solve (FIM)          -> agd_plan_create / agd_plan_upload / agd_plan_run
+  PostProcess (flow)   -> agd_flow
+  GetGeodesics         -> agd_eucl_map, agd_geodesics
+  SolveAD (reverse)    -> agd_reverse
+"""
+import ctypes
+import math
+import numbers
+import warnings
+from collections import OrderedDict
+
+import numpy as np
+import torch
+
+from .. import _lib
+from .. import Metrics
+
+# Default traits (agd/Eikonal/HFM_CUDA/kernel_traits.py:61-88): shape_i, niter_i, fim_front_width.
+DEFAULT_TRAITS = {
+    "Riemann2": ((8, 8), 8, 4),
+    "Riemann3": ((4, 4, 4), 4, 6),
+    "Isotropic2": ((16, 16), 16, 4),
+    "Isotropic3": ((4, 4, 4), 8, 4),
+}
+SUPPORTED_TILES = {2: {(8, 8), (16, 16)}, 3: {(4, 4, 4)}}
+GEODESIC_CODES = ["Continue", "AtSeed", "InWall", "Stationnary", "PastSeed", "VanishingFlow"]
+_FLOAT_RES = float(np.finfo(np.float32).resolution)
+
+
+def RunGPU(hfmIn, *args, cache=None, **kwargs):
+    """Runs the GPU eikonal solver.
+
+    Main input: hfmIn, a dictIn.  Set hfmIn['verbosity'] to 1 or 2 to display
+    information on the run (0 to silence it); hfmOut['keys']['help'] holds a
+    short help for every key that was looked up."""
+    if cache is not None:
+        print("Warning : gpu eikonal solver does not support caching")
+    return Interface(hfmIn).Run(*args, **kwargs)
+
+
+def RunBatch(hfmIns, launch=None):
+    """Solves several dictIn in one persistent launch (all of the same dimension).
+
+    Each instance keeps its own model, tile shape, tolerances and options; the
+    per-instance post-processing (flow, geodesics, sensitivities, outputs) is the
+    same as RunGPU's.  Returns the list of outputs."""
+    itfs = [Interface(h) for h in hfmIns]
+    for it in itfs:
+        it.SetKernelTraits()
+        it.SetGeometry()
+        it.SetArgs()
+    plan = BatchPlan(itfs, launch=launch)
+    plan.run()
+    plan.finish()
+    outs = []
+    for it in itfs:
+        it.PostProcess()
+        it.SolveAD()
+        it.GetGeodesics()
+        it.FinalCheck()
+        if it.extractValues or it.retself:
+            r = [it.hfmOut]
+            if it.extractValues:
+                r.insert(0, it.values)
+            if it.retself:
+                r.append(it)
+            outs.append(r)
+        else:
+            outs.append(it.hfmOut)
+    return outs
+
+
+class BatchPlan:
+    """A plan over prepared Interfaces: device workspace, descriptors uploaded
+    once, and `run()` that only enqueues device work (graph capturable)."""
+
+    def __init__(self, itfs, launch=None):
+        L = _lib.lib()
+        self.itfs = itfs
+        self.n = len(itfs)
+        arr = (_lib.AgdInstance * self.n)(*[it.instance() for it in itfs])
+        self._arr = arr
+        self.plan = ctypes.c_void_p()
+        _lib.check(L.agd_plan_create(arr, self.n, ctypes.byref(self.plan)), "plan")
+        self.nbytes = int(L.agd_plan_workspace_bytes(self.plan))
+        self.ws = torch.empty(self.nbytes, dtype=torch.uint8, device="cuda")
+        self.stats = torch.zeros((self.n, 2), dtype=torch.int64, device="cuda")
+        self.launch = launch
+        _lib.check(L.agd_plan_upload(self.plan, _lib.ptr(self.ws), self.nbytes, _lib.stream_ptr()), "upload")
+        self.grid_updates_per_visit = [it.size_i for it in itfs]
+
+    def run(self, stream=None):
+        L = _lib.lib()
+        lp = ctypes.byref(self.launch) if self.launch is not None else None
+        _lib.check(L.agd_plan_run(self.plan, _lib.ptr(self.ws), self.nbytes, _lib.ptr(self.stats), lp,
+                                  _lib.stream_ptr(stream)), "solve")
+
+    def read_stats(self):
+        s = self.stats.cpu().numpy()
+        return (s[:, 0] & 0xffffffff).astype(np.int64), ((s[:, 0] >> 32) & 0xffffffff).astype(np.int64), s[:, 1]
+
+    def finish(self):
+        niter, status, visits = self.read_stats()
+        for i, it in enumerate(self.itfs):
+            it.tile_visits = int(visits[i])
+            it.stats["eikonal"].update({"niter_o": int(niter[i]), "time": None, "nupdate_o_total": int(visits[i]),
+                                        "grid_updates": int(visits[i]) * it.size_i})
+            st = int(status[i])
+            if st & ~_lib.AGD_STATUS_NOT_CONVERGED:
+                raise _lib.AgdError(st, f"eikonal solve failed on the device (instance {i})")
+            if st & _lib.AGD_STATUS_NOT_CONVERGED:
+                msg = f"Instance {i} did not reach convergence after {it.nitermax_o} iterations"
+                if it.raiseOnNonConvergence:
+                    raise ValueError(msg)
+                it.Warn(msg)
+            it._values = None
+
+    def __del__(self):
+        try:
+            _lib.lib().agd_plan_destroy(self.plan)
+        except Exception:  # noqa: BLE001
+            pass
+
+
+def _to_tensor(x, dtype=torch.float32):
+    if isinstance(x, torch.Tensor):
+        return x.to(device="cuda", dtype=dtype)
+    return torch.as_tensor(np.asarray(x, dtype=np.float32 if dtype == torch.float32 else None), device="cuda",
+                           dtype=dtype)
+
+
+class Interface:
+    """Carries out the work of RunGPU (agd/Eikonal/HFM_CUDA/_Interface.py:23-174)."""
+
+    def __init__(self, hfmIn):
+        self.hfmIn = hfmIn
+        if hfmIn["arrayOrdering"] != "RowMajor":
+            raise ValueError("Only RowMajor indexing supported")
+        self.hfmOut = {"keys": {
+            "used": ["origin", "arrayOrdering", "dims", "mode", "projective"],
+            "default": OrderedDict(),
+            "visited": [],
+            "help": OrderedDict(),
+            "kernelStats": OrderedDict(),
+        }}
+        self.verbosity = 1
+        self.verbosity = self.GetValue("verbosity", default=1,
+                                       help="Choose the amount of detail displayed on the run")
+        self.clear_hfmIn = self.GetValue("clear_hfmIn", default=False,
+                                         help="Delete hfmIn member fields. (May save memory.)")
+        self.model = self.GetValue("model", help="Minimal path model to be solved.")
+        if self.model not in DEFAULT_TRAITS:
+            raise ValueError(f"Unsupported model {self.model!r}; supported: {sorted(DEFAULT_TRAITS)}")
+        self.ndim = len(np.asarray(_host(hfmIn["dims"])).reshape(-1))
+        if self.ndim != int(self.model[-1]):
+            raise ValueError(f"Model {self.model} expects {self.model[-1]} dimensions, got dims of length {self.ndim}")
+        self.stats = {"eikonal": {}, "flow": {}, "geodesic": {}, "reverseAD": {}}
+
+    @property
+    def model_(self):
+        return self.model[:-1]
+
+    # ------------------------------------------------------------- keys ---
+    def HasValue(self, key):
+        self.hfmOut["keys"]["visited"].append(key)
+        return key in self.hfmIn
+
+    def GetValue(self, key, default="_None", verbosity=2, array_float=False, help="Sorry : no help for this key"):
+        """Value of a key, with the reference's bookkeeping (_Interface.py:80-122)."""
+        assert key not in self.hfmOut["keys"]["help"]
+        self.hfmOut["keys"]["help"][key] = help
+        self.hfmOut["keys"]["default"][key] = default
+        if key in self.hfmIn:
+            self.hfmOut["keys"]["used"].append(key)
+            value = self.hfmIn[key]
+            if array_float is False:
+                return value
+            value = _to_tensor(value)
+            if isinstance(array_float, tuple):
+                shapeRef, shape = array_float, tuple(value.shape)
+                if len(shapeRef) != len(shape):
+                    raise ValueError(f"Field {key} has incorrect number of dimensions. "
+                                     f"Expected shape {shapeRef}, found {shape}")
+                for sRef, s in zip(shapeRef, shape):
+                    if sRef not in (-1, s):
+                        raise ValueError(f"Field {key} has incorrect dimensions. "
+                                         f"Expected shape {shapeRef}, found {shape}")
+            return value
+        elif isinstance(default, str) and default == "_None":
+            raise ValueError(f"Missing value for key {key}")
+        else:
+            if verbosity <= self.verbosity:
+                if isinstance(default, str) and default == "_Dummy":
+                    print(f"see out['keys']['default'][{key}] for default")
+                else:
+                    print(f"key {key} defaults to {default}")
+            if isinstance(default, numbers.Number) and array_float is not False:
+                default = _to_tensor(default)
+            return default
+
+    def Warn(self, msg):
+        if self.verbosity >= -1:
+            print("---- Warning ----\n", msg, "\n-----------------\n")
+
+    # -------------------------------------------------------------- run ---
+    def Run(self):
+        self.SetKernelTraits()
+        self.SetGeometry()
+        self.SetArgs()
+        self.Solve()
+        self.PostProcess()
+        self.SolveAD()
+        self.GetGeodesics()
+        self.FinalCheck()
+        if self.extractValues or self.retself:
+            retval = [self.hfmOut]
+            if self.extractValues:
+                retval.insert(0, self.values)
+            if self.retself:
+                retval.append(self)
+            return retval
+        return self.hfmOut
+
+    def SetKernelTraits(self):
+        """Traits (agd/Eikonal/HFM_CUDA/_Kernel.py:23-92)."""
+        si, niter, front = DEFAULT_TRAITS[self.model]
+        traits = {"shape_i": si, "niter_i": niter}
+        traits.update(self.GetValue("traits", default=dict(traits),
+                                    help="Optional trait parameters for the eikonal kernel."))
+        self.shape_i = tuple(int(s) for s in traits["shape_i"])
+        self.niter_i = int(traits["niter_i"])
+        if self.shape_i not in SUPPORTED_TILES[self.ndim]:
+            raise ValueError(f"Unsupported shape_i {self.shape_i} for {self.model}; "
+                             f"built tile shapes: {sorted(SUPPORTED_TILES[self.ndim])}")
+        if self.model.startswith("Riemann") and self.ndim == 2 and self.shape_i != (8, 8):
+            raise ValueError("Riemann2 is built with shape_i (8,8)")
+        self.traits = traits
+        self.values_float64 = self.GetValue("values_float64", default=False,
+                                            help="Export values using the float64 data type")
+        self.multiprecision = self.values_float64 or self.GetValue(
+            "multiprecision", default=False, help="Use multiprecision arithmetic, to improve accuracy")
+        if self.multiprecision:
+            raise NotImplementedError("multiprecision is not available in this build")
+        self.factoringRadius = self.GetValue("factoringRadius", default=0,
+                                             help="Use source factorization, to improve accuracy")
+        if self.factoringRadius:
+            raise NotImplementedError("source factorization is not available in this build")
+        order = self.GetValue("order", default=1, help="Use second order scheme to improve accuracy")
+        if order not in {1, 2}:
+            raise ValueError(f"Unsupported scheme order {order}")
+        if order == 2:
+            raise NotImplementedError("the second order scheme is not available in this build")
+        solver = self.GetValue("solver", default="FIM",
+                               help="Choice of fixed point solver (AGSI, global_iteration)")
+        alt = {"FIM": "fast_iterative_method", "AGSI": "adaptive_gauss_siedel_iteration"}
+        self.solver = alt.get(solver, solver)
+        if self.solver != "fast_iterative_method":
+            raise NotImplementedError(f"solver {solver!r}: this build schedules tiles by the fast iterative method")
+        self.fim_front_width = int(self.GetValue(
+            "fim_front_width", default=front,
+            help="Dictates the max front width in the FIM variant.\n(original FIM : 2. Must be >=2.)"))
+        if not 2 <= self.fim_front_width <= 255:
+            raise ValueError("fim_front_width must be an integer in [2, 255]")
+        self.nitermax_o = int(self.GetValue("nitermax_o", default=2000,
+                                            help="Maximum number of iterations of the solver"))
+        self.raiseOnNonConvergence = self.GetValue("raiseOnNonConvergence", default=True,
+                                                   help="Raise an exception if a solver fails to converge")
+        self.size_i = int(np.prod(self.shape_i))
+
+    def SetGeometry(self):
+        """Domain, metric and cost (agd/Eikonal/HFM_CUDA/_SetGeometry.py:16-282)."""
+        L = _lib.lib()
+        self.shape = self.hfmIn.shape
+        if any(s <= 0 for s in self.shape):
+            raise ValueError(f"Invalid domain shape {self.shape}")
+        self.shape_o = tuple((s + i - 1) // i for s, i in zip(self.shape, self.shape_i))
+        self.size_o = int(np.prod(self.shape_o))
+        self.size_tot = self.size_o * self.size_i
+        if "gridScale" in self.hfmIn:
+            self.GetValue("gridScale", help="Scale of the computational grid")
+        else:
+            self.GetValue("gridScales", array_float=(self.ndim,), help="Axis independent scales of the computational grid")
+        self.h = np.asarray(self.hfmIn.gridScales, np.float32).reshape(-1)
+        self.c_shape = (ctypes.c_int * 3)(*self.shape, *([1] * (3 - self.ndim)))
+        self.c_shape_i = (ctypes.c_int * 3)(*self.shape_i, *([1] * (3 - self.ndim)))
+        self.stream = _lib.stream_ptr()
+
+        if self.model_ == "Riemann":
+            metric = self.GetValue("metric", default=None, verbosity=3, help="Metric of the minimal path model")
+            dual = self.GetValue("dualMetric", default=None, verbosity=3,
+                                 help="Dual metric of the minimal path model")
+            if metric is None and dual is None:
+                raise ValueError("Missing value for key metric")
+            src, is_dual = (metric, 0) if metric is not None else (dual, 1)
+            flat = _metric_hfm(src, self.ndim)
+            symdim = self.ndim * (self.ndim + 1) // 2
+            bcast = 1 if flat.dim() == 1 else 0
+            if not bcast and tuple(flat.shape[:-1]) != self.shape:
+                raise ValueError("Inconsistent dimensions for geometry data. "
+                                 "It should match (the last coordinates of) domain shape.")
+            self._metric_flat = flat.contiguous()
+            self.geom = torch.empty(symdim * self.size_tot, dtype=torch.float32, device="cuda")
+            hs = (ctypes.c_double * 3)(*[float(x) for x in self.h], *([1.0] * (3 - self.ndim)))
+            _lib.check(L.agd_prep_geom(self.ndim, self.c_shape, self.c_shape_i, _lib.ptr(self._metric_flat), bcast,
+                                       is_dual, hs, _lib.ptr(self.geom), self.stream), "prep_geom")
+        else:
+            self.geom = None
+
+        self.exportGeodesicFlow = self.GetValue("exportGeodesicFlow", default=False,
+                                                help="Export the upwind geodesic flow (direction of the geodesics)")
+        self.tips = self.GetValue("tips", default=None, array_float=(-1, self.ndim),
+                                  help="Tips from which to compute the minimal geodesics")
+        self.hasTips = self.tips is not None
+
+        if self.HasValue("speed"):
+            cost = 1.0 / self.GetValue("speed", array_float=True, help="speed = 1/cost (scales the metric, accepts AD)")
+        else:
+            cost = self.GetValue("cost", array_float=True, default=None,
+                                 help="cost = 1/speed (scales the metric, accepts AD)")
+            if cost is None:
+                cost = torch.ones((), dtype=torch.float32, device="cuda")
+        cost = cost.to(torch.float32)
+        if cost.dim() != 0 and tuple(cost.shape) != self.shape:
+            raise ValueError(f"Field cost has incorrect dimensions. Found {tuple(cost.shape)}, "
+                             f"whereas domain has shape {self.shape}")
+        self.cost = cost
+        if self.HasValue("atol") and self.HasValue("rtol"):
+            tol = None
+        else:
+            tol = self.GetValue("tol", default="_Dummy", array_float=tuple(),
+                                help="Convergence tolerance for the fixed point solver (determines atol, rtol)")
+            if isinstance(tol, str) and tol == "_Dummy":
+                mean_cost = float(torch.nanmean(cost.float())) if cost.dim() else float(cost)
+                tol = np.float32(mean_cost * _FLOAT_RES * 5.0)
+                self.hfmOut["keys"]["default"]["tol"] = np.float32(tol)
+            else:
+                tol = float(tol)
+        self.atol = float(self.GetValue("atol", default=tol, array_float=tuple(),
+                                        help="Absolute convergence tolerance for the fixed point solver"))
+        self.rtol = float(self.GetValue("rtol", default=_FLOAT_RES * 5.0, array_float=tuple(),
+                                        help="Relative convergence tolerance for the fixed point solver"))
+        if self.GetValue("walls", default=None, help="Obstacles in the domain") is not None:
+            raise NotImplementedError("walls are not available in this build")
+
+    def SetArgs(self):
+        """Initial values, rhs, seeds (agd/Eikonal/HFM_CUDA/_SetArgs.py:8-177)."""
+        L = _lib.lib()
+        values = self.GetValue("values", default=None, array_float=self.shape,
+                               help="Initial values for the eikonal solver")
+        self.values_t = torch.empty(self.size_tot, dtype=torch.float32, device="cuda")
+        if values is None:
+            self.values_t.fill_(math.inf)
+        else:
+            v = values.contiguous().float()
+            _lib.check(L.agd_block_expand(self.ndim, self.c_shape, self.c_shape_i, 1, _lib.ptr(v), 0,
+                                          ctypes.c_float(math.inf), _lib.ptr(self.values_t), self.stream),
+                       "values")
+        self.rhs_t = torch.empty(self.size_tot, dtype=torch.float32, device="cuda")
+        c = self.cost.contiguous()
+        _lib.check(L.agd_block_expand(self.ndim, self.c_shape, self.c_shape_i, 1, _lib.ptr(c.reshape(-1)),
+                                      1 if c.dim() == 0 else 0, ctypes.c_float(math.inf), _lib.ptr(self.rhs_t),
+                                      self.stream), "rhs")
+        seeds = self.GetValue("seeds", default=None, array_float=(-1, self.ndim),
+                              help="Points from where the front propagation starts")
+        self.reverseAD = self.HasValue("sensitivity")
+        if seeds is None:
+            raise ValueError("Missing value for key seeds (trigger-only fronts are not available in this build)")
+        seedValues = self.GetValue("seedValues", default=torch.zeros(len(seeds), device="cuda"),
+                                   array_float=(len(seeds),), help="Initial value for the front propagation")
+        seedRadius = self.GetValue("seedRadius", default=0.0,
+                                   help="Spread the seeds over a radius given in pixels, so as to improve accuracy.")
+        if seedRadius:
+            raise NotImplementedError("seedRadius spreading is not available in this build")
+        ci = self.hfmIn.PointFromIndex(_host(seeds), to=True)
+        idx = np.round(ci).astype(np.int64)
+        inside = np.all((idx >= 0) & (idx < np.array(self.shape)), axis=1)
+        if not np.all(inside):
+            raise ValueError(f"Seeds outside the domain: {np.asarray(_host(seeds))[~inside].tolist()}")
+        self.seedIndices = idx
+        self.seed_values = seedValues.contiguous().float()
+        self.seed_idx_t = torch.as_tensor(idx.astype(np.int32), device="cuda").contiguous()
+        self.seedbits = torch.empty(self.size_tot // 8, dtype=torch.uint8, device="cuda")
+        _lib.check(L.agd_prep_seeds(self.ndim, self.c_shape, self.c_shape_i, _lib.ptr(self.seed_idx_t),
+                                    _lib.ptr(self.seed_values), len(idx), _lib.ptr(self.rhs_t),
+                                    _lib.ptr(self.seedbits), None, self.stream), "seeds")
+
+    def instance(self):
+        inst = _lib.AgdInstance()
+        inst.model = _lib.AGD_MODEL_RIEMANN if self.model_ == "Riemann" else _lib.AGD_MODEL_ISOTROPIC
+        inst.ndim = self.ndim
+        for k in range(3):
+            inst.shape[k] = self.shape[k] if k < self.ndim else 1
+            inst.shape_i[k] = self.shape_i[k] if k < self.ndim else 1
+            inst.iso_weights[k] = float(self.h[k]) ** -2 if k < self.ndim else 0.0
+        inst.niter_i = self.niter_i
+        inst.fim_front_width = self.fim_front_width
+        inst.nitermax_o = self.nitermax_o
+        inst.flags = 0
+        inst.atol, inst.rtol = self.atol, self.rtol
+        inst.values = self.values_t.data_ptr()
+        inst.geom = self.geom.data_ptr() if self.geom is not None else None
+        inst.rhs = self.rhs_t.data_ptr()
+        inst.seedbits = self.seedbits.data_ptr()
+        return inst
+
+    def Solve(self):
+        """The eikonal solve (agd/Eikonal/HFM_CUDA/_solvers.py:15-57)."""
+        L = _lib.lib()
+        inst = self.instance()
+        plan = ctypes.c_void_p()
+        _lib.check(L.agd_plan_create(ctypes.byref(inst), 1, ctypes.byref(plan)), "plan")
+        try:
+            nbytes = L.agd_plan_workspace_bytes(plan)
+            ws = torch.empty(nbytes, dtype=torch.uint8, device="cuda")
+            stats = torch.zeros(2, dtype=torch.int64, device="cuda")
+            _lib.check(L.agd_plan_upload(plan, _lib.ptr(ws), nbytes, self.stream), "upload")
+            start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            start.record()
+            _lib.check(L.agd_plan_run(plan, _lib.ptr(ws), nbytes, _lib.ptr(stats), None, self.stream), "solve")
+            stop.record()
+            stop.synchronize()
+        finally:
+            L.agd_plan_destroy(plan)
+        s = stats.cpu().numpy()
+        niter_o = int(s[0] & 0xffffffff)
+        status = int((s[0] >> 32) & 0xffffffff)
+        self.tile_visits = int(s[1])
+        t = start.elapsed_time(stop) / 1000.0
+        self.stats["eikonal"].update({"niter_o": niter_o, "time": t, "nupdate_o_total": self.tile_visits,
+                                      "grid_updates": self.tile_visits * self.size_i})
+        if status & ~_lib.AGD_STATUS_NOT_CONVERGED:
+            raise _lib.AgdError(status, "eikonal solve failed on the device")
+        if status & _lib.AGD_STATUS_NOT_CONVERGED:
+            msg = (f"Solver fast_iterative_method for kernel eikonal did not reach convergence after "
+                   f"maximum allowed number {self.nitermax_o} of iterations")
+            if self.raiseOnNonConvergence:
+                raise ValueError(msg)
+            self.Warn(msg)
+        self._values = None
+
+    def squeeze(self, t, nplanes=1):
+        L = _lib.lib()
+        out = torch.empty((nplanes,) + self.shape, dtype=torch.float32, device="cuda")
+        _lib.check(L.agd_block_squeeze(self.ndim, self.c_shape, self.c_shape_i, nplanes, _lib.ptr(t),
+                                       _lib.ptr(out), self.stream), "block_squeeze")
+        return out if nplanes > 1 else out[0]
+
+    @property
+    def values(self):
+        if self._values is None:
+            self._values = self.squeeze(self.values_t)
+        return self._values
+
+    def PostProcess(self):
+        """Upwind flow, if needed (agd/Eikonal/HFM_CUDA/_PostProcess.py:46-95)."""
+        self.flow_needed = self.reverseAD or self.hasTips or self.exportGeodesicFlow
+        if not self.flow_needed:
+            return
+        L = _lib.lib()
+        nact = self.ndim if self.model_ == "Isotropic" else self.ndim * (self.ndim + 1) // 2
+        self.nact = nact
+        self.flow_vector = torch.empty(self.ndim * self.size_tot, dtype=torch.float32, device="cuda")
+        self.flow_weightsum = torch.empty(self.size_tot, dtype=torch.float32, device="cuda")
+        self.flow_weights = self.flow_indices = None
+        if self.reverseAD:
+            self.flow_weights = torch.empty(nact * self.size_tot, dtype=torch.float32, device="cuda")
+            self.flow_indices = torch.empty(nact * self.size_tot, dtype=torch.int32, device="cuda")
+        inst = self.instance()
+        _lib.check(L.agd_flow(ctypes.byref(inst), _lib.ptr(self.flow_vector), _lib.ptr(self.flow_weightsum),
+                              _lib.ptr(self.flow_weights), _lib.ptr(self.flow_indices), self.stream), "flow")
+        if self.exportGeodesicFlow:
+            fv = self.squeeze(self.flow_vector, self.ndim)
+            h = torch.as_tensor(self.h, device="cuda").reshape((self.ndim,) + (1,) * self.ndim)
+            self.hfmOut["flow"] = fv * (-h)
+
+    def SolveAD(self):
+        """Reverse-mode sensitivity (agd/Eikonal/HFM_CUDA/_PostProcess.py:155-219)."""
+        if not self.reverseAD:
+            return
+        L = _lib.lib()
+        sens = self.GetValue("sensitivity", help="Reverse automatic differentiation")
+        sens = _to_tensor(sens)
+        if tuple(sens.shape[:-1]) != self.shape:
+            raise ValueError(f"Reverse AD rhs shape {tuple(sens.shape)} does not start with {self.shape}")
+        nrhs = sens.shape[-1]
+        inst = self.instance()
+        nbytes = L.agd_reverse_workspace_bytes(ctypes.byref(inst))
+        ws = torch.empty(max(int(nbytes), 1), dtype=torch.uint8, device="cuda")
+        stats = torch.zeros(2, dtype=torch.int64, device="cuda")
+        res = rtol = _FLOAT_RES * 5.0
+        lam_all = []
+        for r in range(nrhs):
+            col = sens[..., r].contiguous()
+            s_t = torch.empty(self.size_tot, dtype=torch.float32, device="cuda")
+            _lib.check(L.agd_block_expand(self.ndim, self.c_shape, self.c_shape_i, 1, _lib.ptr(col), 0,
+                                          ctypes.c_float(0.0), _lib.ptr(s_t), self.stream), "sensitivity")
+            fin = col[torch.isfinite(col)]
+            atol = float(rtol * fin.abs().mean()) if fin.numel() else 0.0
+            lam = torch.empty(self.size_tot, dtype=torch.float32, device="cuda")
+            _lib.check(L.agd_reverse(ctypes.byref(inst), _lib.ptr(self.flow_weights), _lib.ptr(self.flow_indices),
+                                     _lib.ptr(self.flow_weightsum), _lib.ptr(s_t), _lib.ptr(lam),
+                                     ctypes.c_float(atol), ctypes.c_float(res), _lib.ptr(ws), int(nbytes),
+                                     _lib.ptr(stats), None, self.stream), "reverse")
+            st = stats.cpu().numpy()
+            status = int((st[0] >> 32) & 0xffffffff)
+            if status:
+                raise _lib.AgdError(status, "reverse sensitivity solve failed on the device")
+            self.stats["reverseAD"] = {"niter_o": int(st[0] & 0xffffffff), "nupdate_o_total": int(st[1])}
+            lam_all.append(self.squeeze(lam))
+        allS = torch.stack(lam_all, dim=-1)
+        pos = tuple(torch.as_tensor(self.seedIndices.T, device="cuda").long())
+        seedS = allS[pos].clone()
+        allS[pos] = 0
+        self.hfmOut["costSensitivity"] = allS
+        self.hfmOut["seedValueSensitivity"] = seedS
+
+    def GetGeodesics(self):
+        """Geodesic backtracking (agd/Eikonal/HFM_CUDA/_GetGeodesics.py:9-147)."""
+        if not self.hasTips:
+            return
+        L = _lib.lib()
+        step = float(self.GetValue("geodesic_step", default=0.25,
+                                   help="Step size, in pixels, for the geodesic ODE solver"))
+        eucl_delay = int(self.GetValue("geodesic_PastSeed_delay", default=np.sqrt(self.ndim) / step,
+                                       help="Delay, in iterations, for the 'PastSeed' stopping criterion of the "
+                                            "geodesic ODE solver"))
+        nymin_delay = int(self.GetValue("geodesic_Stationnary_delay", default=8.0 * np.sqrt(self.ndim) / step,
+                                        help="Delay, in iterations, for the 'Stationnary' stopping criterion of "
+                                             "the geodesic ODE solver"))
+        max_len = int(max(40, 20 * np.max(self.shape) / step))
+        max_len = self.GetValue("geodesic_max_length", default=max_len, help="Maximum allowed length of geodesics.")
+        typical_len = int(max(40, 0.5 * np.max(self.shape) / step))
+        typical_len = int(self.GetValue("geodesic_typical_length", default=min(max_len, typical_len),
+                                        help="Typical expected length of geodesics (number of points)."))
+        causality = float(self.GetValue("geodesic_causalityTolerance", default=4.0,
+                                        help="Used in criterion for rejecting points in flow interpolation"))
+        eucl_bound = float(self.GetValue("geodesic_targetTolerance", default=6,
+                                         help="Tolerance, in pixels, for declaring a seed as reached."))
+        if max_len == np.inf or max_len is None:
+            max_chunks = 1 << 20
+        else:
+            max_chunks = int(np.ceil(float(max_len) / typical_len))
+        tips = self.tips
+        ntips = int(tips.shape[0])
+        seed_mask = torch.zeros(self.shape, dtype=torch.uint8, device="cuda")
+        seed_mask[tuple(torch.as_tensor(self.seedIndices.T, device="cuda").long())] = 1
+        eucl = torch.empty(self.shape, dtype=torch.uint8, device="cuda")
+        tmp = torch.empty_like(eucl)
+        _lib.check(L.agd_eucl_map(self.ndim, self.c_shape, _lib.ptr(seed_mask), int(np.ceil(eucl_bound)),
+                                  int(5 * eucl_bound), _lib.ptr(eucl), _lib.ptr(tmp), self.stream), "eucl")
+        start = torch.as_tensor(self.hfmIn.corners[0] + 0.5 * self.hfmIn.gridScales, device="cuda")
+        hh = torch.as_tensor(self.h, device="cuda")
+        tips_c = ((tips.float() - start) / hh).contiguous()
+        cap = max_chunks * (typical_len - 1) + 1
+        paths = torch.empty((ntips, cap, self.ndim), dtype=torch.float32, device="cuda")
+        lengths = torch.empty(ntips, dtype=torch.int32, device="cuda")
+        stops = torch.empty(ntips, dtype=torch.int8, device="cuda")
+        inst = self.instance()
+        _lib.check(L.agd_geodesics(ctypes.byref(inst), _lib.ptr(self.flow_vector), _lib.ptr(self.flow_weightsum),
+                                   _lib.ptr(eucl), _lib.ptr(tips_c), ntips, ctypes.c_float(step),
+                                   ctypes.c_float(causality), typical_len, max_chunks, eucl_delay, nymin_delay,
+                                   _lib.ptr(paths), cap, _lib.ptr(lengths), _lib.ptr(stops), self.stream),
+                   "geodesics")
+        lens = lengths.cpu().numpy()
+        codes = stops.cpu().numpy()
+        geos = []
+        for i in range(ntips):
+            g = paths[i, : int(lens[i])] * hh + start
+            geos.append(g.T.contiguous())
+        crit = []
+        for i in range(ntips):
+            if codes[i] == 0:
+                crit.append("Stopping criterion")
+            else:
+                crit.append(GEODESIC_CODES[int(codes[i])])
+        if any(c == "Stopping criterion" for c in crit):
+            self.Warn("Geodesic solver failed to converge, or geodesic has too many points"
+                      " (in latter case, try setting 'geodesic_max_length':np.inf)")
+        self.hfmOut["geodesics"] = geos
+        self.hfmOut["geodesic_stopping_criteria"] = crit
+
+    def FinalCheck(self):
+        if self.GetValue("exportValues", False, help="Return the solution numerical values"):
+            self.hfmOut["values"] = self.values
+        self.extractValues = self.GetValue("extractValues", False,
+                                           help="Return the solution numerical values separately from other data")
+        self.retself = self.GetValue("retself", False, help="Return the class instance that did the work")
+        self.hfmOut["stats"] = self.stats
+        self.hfmOut["solverGPUTime"] = self.stats["eikonal"].get("time")
+        self.hfmOut["keys"]["unused"] = list(set(self.hfmIn.keys()) - set(self.hfmOut["keys"]["used"]))
+        if self.verbosity >= 1 and self.hfmOut["keys"]["unused"]:
+            print(f"!! Warning !! Unused keys from user : {self.hfmOut['keys']['unused']}")
+
+
+def _host(x):
+    if isinstance(x, torch.Tensor):
+        return x.detach().cpu().numpy()
+    return x
+
+
+def _metric_hfm(src, ndim):
+    """A metric given as a Metrics.Riemann-like object (attribute m, shape
+    (d,d,*shape) or (d,d)) or as an HFM array (*shape, symdim) -> float32 CUDA
+    tensor in HFM layout (*shape, symdim), or (symdim,) for a constant metric."""
+    symdim = ndim * (ndim + 1) // 2
+    if hasattr(src, "m"):
+        m = _to_tensor(src.m)
+        if m.shape[0] != ndim or m.shape[1] != ndim:
+            raise ValueError("Metric dimension does not match the model")
+        rows = [m[i, j] for i in range(ndim) for j in range(i + 1)]
+        return torch.movedim(torch.stack(rows), 0, -1).contiguous()
+    if isinstance(src, Metrics.Isotropic) or hasattr(src, "cost"):
+        c = _to_tensor(src.cost)
+        eye = [(1.0 if i == j else 0.0) for i in range(ndim) for j in range(i + 1)]
+        e = torch.as_tensor(eye, device="cuda", dtype=torch.float32)
+        return (c[..., None] ** 2 * e).contiguous() if c.dim() else (c ** 2 * e).contiguous()
+    arr = _to_tensor(src)
+    if arr.shape[-1] != symdim:
+        raise ValueError(f"Metric array must have {symdim} components in its last axis (HFM layout)")
+    return arr.contiguous()

@@ -1,0 +1,10 @@
+"""B200-native GPU eikonal solver with the surface of agd.Eikonal.dictIn(...).Run().
+
+Models Isotropic2/3 and Riemann2/3; outputs values, geodesics and reverse-mode
+sensitivities.  The work is done by libagd_b200.so (CUDA for sm_100a) through
+the C ABI declared in include/agd_b200.h; torch provides device memory and
+streams.
+"""
+from . import Eikonal, Metrics
+
+__all__ = ["Eikonal", "Metrics"]

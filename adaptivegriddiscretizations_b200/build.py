@@ -1,0 +1,39 @@
+"""Builds libagd_b200.so (the CUDA kernels and the C ABI of include/agd_b200.h)
+in-tree for sm_100a with nvcc."""
+import os
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REPO = os.path.dirname(HERE)
+CSRC = os.path.join(HERE, "csrc")
+LIB = os.path.join(HERE, "libagd_b200.so")
+SOURCES = ["capi.cu", "eikonal.cu", "geodesic.cu", "adjoint.cu"]
+NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", "-std=c++17",
+              "--shared", "-Xcompiler", "-fPIC", "-Xcompiler", "-fvisibility=hidden",
+              "-I" + os.path.join(REPO, "include")]
+
+
+def nvcc():
+    for cand in (os.environ.get("NVCC"), "/usr/local/cuda/bin/nvcc", "nvcc"):
+        if cand and (os.path.isabs(cand) and os.path.exists(cand) or not os.path.isabs(cand)):
+            return cand
+    return "nvcc"
+
+
+def build(verbose=False, extra=()):
+    srcs = [os.path.join(CSRC, s) for s in SOURCES]
+    newest = max(os.path.getmtime(p) for p in srcs + [os.path.join(REPO, "include", "agd_b200.h")] +
+                 [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".cuh", ".h"))])
+    if os.path.exists(LIB) and os.path.getmtime(LIB) >= newest and not extra:
+        return LIB
+    cmd = [nvcc()] + NVCC_FLAGS + list(extra) + srcs + ["-o", LIB + ".tmp"]
+    if verbose:
+        print(" ".join(cmd))
+    subprocess.check_call(cmd)
+    os.replace(LIB + ".tmp", LIB)
+    return LIB
+
+
+if __name__ == "__main__":
+    build(verbose=True, extra=tuple(sys.argv[1:]))

@@ -1,0 +1,245 @@
+// Shared device code of the B200 eikonal path: tile geometry, Selling's
+// decomposition, the eikonal update operator, and the bounded grid barrier used
+// by the persistent kernels.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "../../include/agd_b200.h"
+
+namespace agd {
+
+constexpr unsigned kFull = 0xffffffffu;
+constexpr int kIntMax = 2147483647;
+
+__device__ __forceinline__ float finf() { return __int_as_float(0x7f800000); }
+
+// ------------------------------------------------------------------ tiles ---
+// A tile ("block" in the reference) of S0 x S1 (x S2) points; the bilevel index
+// of a point is n_t = n_o * SIZE + n_i (agd/FiniteDifferences.py:164-222,
+// cuda/Grid.h:15-35), with row-major n_o over tiles and n_i inside the tile.
+template <int D_, int S0_, int S1_, int S2_>
+struct Tile {
+    static constexpr int D = D_, S0 = S0_, S1 = S1_, S2 = (D_ == 3 ? S2_ : 1);
+    static constexpr int SIZE = S0 * S1 * S2;
+    static constexpr int P = SIZE / 32;  // points per lane (one warp per tile)
+    static_assert(SIZE % 32 == 0, "tile size must be a multiple of the warp size");
+    __device__ __forceinline__ static void pos(int n_i, int *x) {
+        if (D == 2) {
+            x[0] = n_i / S1;
+            x[1] = n_i % S1;
+        } else {
+            x[0] = n_i / (S1 * S2);
+            x[1] = (n_i / S2) % S1;
+            x[2] = n_i % S2;
+        }
+    }
+    __device__ __forceinline__ static int extent(int k) { return k == 0 ? S0 : (k == 1 ? S1 : S2); }
+    __device__ __forceinline__ static int local(const int *y) {
+        return D == 2 ? y[0] * S1 + y[1] : (y[0] * S1 + y[1]) * S2 + y[2];
+    }
+};
+
+// Per-instance geometry helpers (shape: true grid shape, shape_o: tiles per axis).
+template <int D, class TL>
+__device__ __forceinline__ int bilevel_index(const int *y, const int *shape_o) {
+    int n_o = 0, n_i = 0;
+#pragma unroll
+    for (int k = 0; k < D; ++k) {
+        const int s = TL::extent(k);
+        const int yo = y[k] / s, yi = y[k] - yo * s;
+        n_o = n_o * shape_o[k] + yo;
+        n_i = n_i * s + yi;
+    }
+    return n_o * TL::SIZE + n_i;
+}
+
+// ---------------------------------------------------------------- Selling ---
+// <x, m y> for integer vectors x, y and m packed lower-triangular.  Follows the
+// accumulation order of the reference's scal_vmv (cuda/Geometry_.h).
+template <int D>
+__device__ __forceinline__ float scal_vmv(const int *x, const float *m, const int *y) {
+    float r = 0.f;
+    int k = 0;
+#pragma unroll
+    for (int i = 0; i < D; ++i)
+#pragma unroll
+        for (int j = 0; j <= i; ++j, ++k)
+            r += float(i == j ? x[i] * y[i] : x[i] * y[j] + x[j] * y[i]) * m[k];
+    return r;
+}
+
+// Selling's algorithm: obtuse superbase by cyclic reduction from the canonical
+// superbase, then weights -<b_i, m b_j> and offsets perp(b_k)
+// (agd/Eikonal/HFM_CUDA/cuda/Geometry2.h:21-48).  The cyclic loop is unrolled by
+// its period so that every superbase index is a compile-time constant.
+__device__ __forceinline__ void selling2(const float *m, float *w, int (*e)[3]) {
+    int b0[2] = {1, 0}, b1[2] = {0, 1}, b2[2] = {-1, -1};
+    int iter = 0, red = 0;
+#define AGD_SELL2_STEP(BI, BJ, BK)                                   \
+    if (iter >= 100 || red >= 3) goto done;                          \
+    if (scal_vmv<2>(BI, m, BJ) > 0.f) {                              \
+        BK[0] = BI[0] - BJ[0]; BK[1] = BI[1] - BJ[1];                 \
+        BI[0] = -BI[0]; BI[1] = -BI[1];                              \
+        red = 0;                                                     \
+    }                                                                \
+    ++iter; ++red;
+    while (true) {
+        AGD_SELL2_STEP(b0, b1, b2)
+        AGD_SELL2_STEP(b1, b2, b0)
+        AGD_SELL2_STEP(b2, b0, b1)
+    }
+#undef AGD_SELL2_STEP
+done:
+    w[0] = fmaxf(0.f, -scal_vmv<2>(b0, m, b1)); e[0][0] = -b2[1]; e[0][1] = b2[0];
+    w[1] = fmaxf(0.f, -scal_vmv<2>(b1, m, b2)); e[1][0] = -b0[1]; e[1][1] = b0[0];
+    w[2] = fmaxf(0.f, -scal_vmv<2>(b2, m, b0)); e[2][0] = -b1[1]; e[2][1] = b1[0];
+}
+
+__device__ __forceinline__ void cross3(const int *a, const int *b, int *o) {
+    o[0] = a[1] * b[2] - a[2] * b[1];
+    o[1] = a[2] * b[0] - a[0] * b[2];
+    o[2] = a[0] * b[1] - a[1] * b[0];
+}
+
+// 3D: the reduction visits the six pairs {i,j} of the superbase cyclically, in
+// the order (01)(02)(03)(12)(13)(23); a positive <b_i, m b_j> is fixed by
+// b_k += b_i, b_l += b_i, b_i = -b_i.  Offsets are b_k x b_l
+// (agd/Eikonal/HFM_CUDA/cuda/Geometry3.h:22-58).
+__device__ __forceinline__ void selling3(const float *m, float *w, int (*e)[3]) {
+    int b0[3] = {1, 0, 0}, b1[3] = {0, 1, 0}, b2[3] = {0, 0, 1}, b3[3] = {-1, -1, -1};
+    int iter = 0, red = 0;
+#define AGD_SELL3_STEP(BI, BJ, BK, BL)                               \
+    if (iter >= 100 || red >= 6) goto done;                          \
+    if (scal_vmv<3>(BI, m, BJ) > 0.f) {                              \
+        _Pragma("unroll") for (int c = 0; c < 3; ++c) {              \
+            BK[c] += BI[c]; BL[c] += BI[c]; BI[c] = -BI[c];          \
+        }                                                            \
+        red = 0;                                                     \
+    }                                                                \
+    ++iter; ++red;
+    while (true) {
+        AGD_SELL3_STEP(b0, b1, b2, b3)
+        AGD_SELL3_STEP(b0, b2, b1, b3)
+        AGD_SELL3_STEP(b0, b3, b1, b2)
+        AGD_SELL3_STEP(b1, b2, b0, b3)
+        AGD_SELL3_STEP(b1, b3, b0, b2)
+        AGD_SELL3_STEP(b2, b3, b0, b1)
+    }
+#undef AGD_SELL3_STEP
+done:
+    w[0] = fmaxf(0.f, -scal_vmv<3>(b0, m, b1)); cross3(b2, b3, e[0]);
+    w[1] = fmaxf(0.f, -scal_vmv<3>(b0, m, b2)); cross3(b1, b3, e[1]);
+    w[2] = fmaxf(0.f, -scal_vmv<3>(b0, m, b3)); cross3(b1, b2, e[2]);
+    w[3] = fmaxf(0.f, -scal_vmv<3>(b1, m, b2)); cross3(b0, b3, e[3]);
+    w[4] = fmaxf(0.f, -scal_vmv<3>(b1, m, b3)); cross3(b0, b2, e[4]);
+    w[5] = fmaxf(0.f, -scal_vmv<3>(b2, m, b3)); cross3(b0, b1, e[5]);
+}
+
+// ------------------------------------------------------ eikonal operator ---
+// Sorting network on (value, weight) pairs, ascending values.  A comparator
+// keeps its pair only when strictly ordered, which is the tie rule of the
+// reference's index networks (cuda/NetworkSort.h:17-60), so equal values end
+// in the same relative order.
+__device__ __forceinline__ void cswap(float *v, float *w, int i, int j) {
+    const bool keep = v[i] < v[j];
+    const float vi = v[i], vj = v[j], wi = w[i], wj = w[j];
+    v[i] = keep ? vi : vj; v[j] = keep ? vj : vi;
+    w[i] = keep ? wi : wj; w[j] = keep ? wj : wi;
+}
+template <int N>
+__device__ __forceinline__ void sort_pairs(float *v, float *w) {
+    if (N == 2) {
+        cswap(v, w, 0, 1);
+    } else if (N == 3) {
+        cswap(v, w, 1, 2); cswap(v, w, 0, 2); cswap(v, w, 0, 1);
+    } else if (N == 6) {
+        cswap(v, w, 1, 2); cswap(v, w, 4, 5);
+        cswap(v, w, 0, 2); cswap(v, w, 3, 5);
+        cswap(v, w, 0, 1); cswap(v, w, 3, 4); cswap(v, w, 2, 5);
+        cswap(v, w, 0, 3); cswap(v, w, 1, 4);
+        cswap(v, w, 2, 4); cswap(v, w, 1, 3);
+        cswap(v, w, 2, 3);
+    }
+}
+
+// Solves sum_k w_k (u - v_k)_+^2 = rhs^2 for u by accumulating the sorted
+// neighbour values until the root lies in the current interval
+// (agd/Eikonal/HFM_CUDA/cuda/HFM.h:142-190).  v and w are clobbered (sorted).
+template <int NACT>
+__device__ __forceinline__ float hfm_update(float rhs, float *v, float *w) {
+    sort_pairs<NACT>(v, w);
+    const float vmin = v[0];
+    if (vmin == finf()) return vmin;
+    float a = w[0], b = 0.f, c = -rhs * rhs;
+    bool stop = false;
+#pragma unroll
+    for (int q = 1; q < NACT; ++q) {
+        const float t = v[q] - vmin;
+        stop = stop || ((a * t - 2.f * b) * t + c > 0.f);
+        if (!stop) {
+            a += w[q];
+            b += w[q] * t;
+            c += w[q] * t * t;
+        }
+    }
+    const float delta = b * b - a * c;
+    const float sd = sqrtf(fmaxf(0.f, delta));
+    const float value = a == 0.f ? finf() : (b + sd) / a;
+    return vmin + value;
+}
+
+// ----------------------------------------------------------- grid barrier ---
+// Software grid barrier for cooperatively launched kernels.  Waits are bounded
+// in time (globaltimer); a timeout raises AGD_STATUS_WATCHDOG in *err and the
+// caller must leave.  Returns false if an error is pending.
+struct GridBarrier {
+    unsigned int count;
+    unsigned int gen;
+};
+
+__device__ __forceinline__ unsigned long long globaltimer() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+__device__ __forceinline__ unsigned int ld_acquire(const unsigned int *p) {
+    unsigned int v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+__device__ inline bool grid_barrier(GridBarrier *bar, unsigned int nblocks, unsigned int *err,
+                                    unsigned long long timeout_ns) {
+    __shared__ int s_ok;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int ok = 1;
+        const unsigned int g = ld_acquire(&bar->gen);
+        __threadfence();
+        if (atomicAdd(&bar->count, 1u) == nblocks - 1) {
+            atomicExch(&bar->count, 0u);
+            __threadfence();
+            atomicAdd(&bar->gen, 1u);
+        } else {
+            const unsigned long long t0 = globaltimer();
+            while (ld_acquire(&bar->gen) == g) {
+                if (ld_acquire(err) != 0u) { ok = 0; break; }
+                if (globaltimer() - t0 > timeout_ns) {
+                    atomicOr(err, (unsigned)AGD_STATUS_WATCHDOG);
+                    ok = 0;
+                    break;
+                }
+                __nanosleep(100);
+            }
+        }
+        __threadfence();
+        if (ld_acquire(err) != 0u) ok = 0;
+        s_ok = ok;
+    }
+    __syncthreads();
+    return s_ok != 0;
+}
+
+}  // namespace agd

@@ -1,0 +1,923 @@
+// Persistent, device-scheduled block-iterative eikonal solver for B200
+// (Isotropic2/3, Riemann2/3), plus the flow pass and the layout kernels.
+//
+// Scheduling.  The reference iterates on the host: every outer iteration it
+// compacts the flags of the tiles to update (cp.flatnonzero), tests for
+// termination (np.any, a device->host sync) and launches `Update` on the
+// active tiles (agd/Eikonal/HFM_CUDA/_solvers.py:94-120).  Here one
+// cooperative launch runs all outer iterations ("epochs"): the active tiles of
+// epoch e sit in a device list; warps take tiles from it, and a tile that must
+// be visited at epoch e+1 is appended to the next list the first time it is
+// tagged (dedupe by an epoch-stamped flag).  A bounded software grid barrier
+// separates epochs.  Fast-iterative-method scores (cuda/Propagation.h:103-167)
+// are epoch-stamped too, so no per-epoch clearing pass is needed.
+//
+// Tile visit.  One warp per tile (points n_i = lane + 32 p), tile values in
+// shared memory, niter_i local sweeps with __syncwarp between phases, and an
+// early exit when a full sweep changes nothing (the state is then a fixed point
+// of the visit, so the result equals that of the remaining sweeps).  Values of
+// neighbours outside the tile are read once per visit through L2 (ld.cg), as
+// other SMs update them concurrently.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <vector>
+
+#include "agd_common.cuh"
+#include "agd_internal.h"
+
+namespace agd {
+
+// ------------------------------------------------------------- variants ---
+enum Variant { V_ISO2_8 = 0, V_ISO2_16, V_RIEM2_8, V_ISO3_4, V_RIEM3_4, V_COUNT };
+
+int variant_of(const agd_instance &a) {
+    if (a.ndim == 2) {
+        if (a.model == AGD_MODEL_RIEMANN && a.shape_i[0] == 8 && a.shape_i[1] == 8) return V_RIEM2_8;
+        if (a.model == AGD_MODEL_ISOTROPIC && a.shape_i[0] == 8 && a.shape_i[1] == 8) return V_ISO2_8;
+        if (a.model == AGD_MODEL_ISOTROPIC && a.shape_i[0] == 16 && a.shape_i[1] == 16) return V_ISO2_16;
+    } else if (a.ndim == 3 && a.shape_i[0] == 4 && a.shape_i[1] == 4 && a.shape_i[2] == 4) {
+        return a.model == AGD_MODEL_RIEMANN ? V_RIEM3_4 : V_ISO3_4;
+    }
+    return -1;
+}
+
+struct Ctrl {
+    unsigned int cnt[3];  // list lengths, rotating: epoch e reads cnt[e%3], fills cnt[(e+1)%3]
+    unsigned int err;
+    GridBarrier bar;
+    unsigned int epochs;  // last epoch run
+};
+
+// Workspace: [Inst x n][tile_inst][list0][list1][flags][score0][score1][Ctrl][stats x n]
+struct WsLayout {
+    size_t inst, tile_inst, list0, list1, flags, score0, score1, ctrl, stats, total;
+    int total_tiles;
+};
+
+static size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
+
+static bool layout(const agd_instance *a, int n, WsLayout &L, std::vector<Inst> *out) {
+    long long tiles = 0;
+    if (out) out->resize(n);
+    for (int i = 0; i < n; ++i) {
+        Inst I;
+        std::memset(&I, 0, sizeof(I));
+        I.a = a[i];
+        I.size_o = 1;
+        for (int k = 0; k < a[i].ndim; ++k) {
+            if (a[i].shape[k] <= 0 || a[i].shape_i[k] <= 0) return false;
+            I.shape_o[k] = (a[i].shape[k] + a[i].shape_i[k] - 1) / a[i].shape_i[k];
+            I.size_o *= I.shape_o[k];
+        }
+        I.size_i = 1;
+        for (int k = 0; k < a[i].ndim; ++k) I.size_i *= a[i].shape_i[k];
+        I.size_tot = (long long)I.size_o * I.size_i;
+        I.tile_base = (int)tiles;
+        I.variant = variant_of(a[i]);
+        tiles += I.size_o;
+        if (tiles > 0x3fffffff) return false;
+        if (out) (*out)[i] = I;
+    }
+    size_t off = 0;
+    L.inst = off; off = align256(off + sizeof(Inst) * n);
+    L.tile_inst = off; off = align256(off + sizeof(int) * tiles);
+    L.list0 = off; off = align256(off + sizeof(int) * tiles);
+    L.list1 = off; off = align256(off + sizeof(int) * tiles);
+    L.flags = off; off = align256(off + sizeof(unsigned) * tiles);
+    L.score0 = off; off = align256(off + sizeof(unsigned) * tiles);
+    L.score1 = off; off = align256(off + sizeof(unsigned) * tiles);
+    L.ctrl = off; off = align256(off + sizeof(Ctrl));
+    L.stats = off; off = align256(off + sizeof(agd_stats) * n);
+    L.total = off;
+    L.total_tiles = (int)tiles;
+    return true;
+}
+
+// --------------------------------------------------------- kernel context ---
+struct Sched {
+    const Inst *inst;
+    const int *tile_inst;
+    int *list0, *list1;
+    unsigned *flags, *score0, *score1;
+    Ctrl *ctrl;
+    agd_stats *stats;
+    int max_epochs;
+    unsigned long long timeout_ns;
+};
+
+__device__ __forceinline__ void push_tile(const Sched &S, int t, int e) {
+    const unsigned tag = (unsigned)(e + 1);
+    if (atomicMax(&S.flags[t], tag) < tag) {
+        int *nxt = (e & 1) ? S.list0 : S.list1;  // epoch e+1 reads list[(e+1)&1]
+        const unsigned idx = atomicAdd(&S.ctrl->cnt[(e + 1) % 3], 1u);
+        nxt[idx] = t;
+    }
+}
+
+__device__ __forceinline__ unsigned score_at(const Sched &S, int t, int e) {
+    // Score written at epoch e (0 if the tile was not visited at epoch e).
+    const unsigned *arr = (e & 1) ? S.score1 : S.score0;
+    const unsigned w = __ldcg(arr + t);
+    return (int)(w >> 8) == e ? (w & 0xffu) : 0u;
+}
+
+// ------------------------------------------------------------- tile visit ---
+template <class TL, int MODEL>
+struct Visit {
+    static constexpr int D = TL::D, P = TL::P;
+    static constexpr int NACT = MODEL == AGD_MODEL_ISOTROPIC ? D : D * (D + 1) / 2;
+    static constexpr int NTOT = 2 * NACT;
+    static constexpr int SD = D * (D + 1) / 2;
+
+    // Stencil of the point with bilevel index n_t: weights and offsets.
+    __device__ __forceinline__ static void stencil(const Inst &I, size_t n_t, float *w, int (*e)[3]) {
+        if (MODEL == AGD_MODEL_ISOTROPIC) {
+#pragma unroll
+            for (int k = 0; k < D; ++k) {
+                w[k] = I.a.iso_weights[k];
+#pragma unroll
+                for (int c = 0; c < 3; ++c) e[k][c] = (c == k);
+            }
+        } else {
+            float m[SD];
+#pragma unroll
+            for (int c = 0; c < SD; ++c) m[c] = __ldg(I.a.geom + (size_t)c * I.size_tot + n_t);
+            if (D == 2) selling2(m, w, e);
+            else selling3(m, w, e);
+        }
+    }
+
+    __device__ static void run(const Sched &S, const Inst &I, int ii, int n_o, int e, int lane, float *us) {
+        const agd_instance &A = I.a;
+        int xo[3] = {0, 0, 0};
+        {
+            int r = n_o;
+#pragma unroll
+            for (int k = D - 1; k >= 0; --k) {
+                xo[k] = r % I.shape_o[k];
+                r /= I.shape_o[k];
+            }
+        }
+        const size_t base = (size_t)n_o * TL::SIZE;
+        float uold[P], rhs[P];
+        float wts[P][NACT];
+        float nbv[P][NTOT];
+        int nbl[P][NTOT];
+        bool seed[P];
+#pragma unroll
+        for (int p = 0; p < P; ++p) {
+            const int n_i = lane + 32 * p;
+            const size_t n_t = base + n_i;
+            int xi[3] = {0, 0, 0}, xt[3] = {0, 0, 0};
+            TL::pos(n_i, xi);
+#pragma unroll
+            for (int k = 0; k < D; ++k) xt[k] = xo[k] * TL::extent(k) + xi[k];
+            uold[p] = __ldcg(A.values + n_t);
+            seed[p] = (__ldg(A.seedbits + (n_t >> 3)) >> (n_t & 7)) & 1;
+            rhs[p] = __ldg(A.rhs + n_t);
+            us[n_i] = seed[p] ? rhs[p] : uold[p];
+            int ev[NACT][3];
+            if (seed[p]) continue;  // seeds (and padding) keep their value: no stencil needed
+            stencil(I, n_t, wts[p], ev);
+#pragma unroll
+            for (int k = 0; k < NACT; ++k) {
+#pragma unroll
+                for (int s = 0; s < 2; ++s) {
+                    const int eps = 2 * s - 1;
+                    int yi[3] = {0, 0, 0}, yt[3] = {0, 0, 0};
+                    bool intile = true, indom = true;
+#pragma unroll
+                    for (int c = 0; c < D; ++c) {
+                        const int off = eps * ev[k][c];
+                        yi[c] = xi[c] + off;
+                        yt[c] = xt[c] + off;
+                        intile = intile && yi[c] >= 0 && yi[c] < TL::extent(c);
+                        indom = indom && yt[c] >= 0 && yt[c] < A.shape[c];
+                    }
+                    if (intile) {
+                        nbl[p][2 * k + s] = TL::local(yi);
+                        nbv[p][2 * k + s] = 0.f;
+                    } else {
+                        nbl[p][2 * k + s] = -1;
+                        nbv[p][2 * k + s] =
+                            indom ? __ldcg(A.values + bilevel_index<D, TL>(yt, I.shape_o)) : finf();
+                    }
+                }
+            }
+        }
+        __syncwarp();
+        for (int it = 0; it < A.niter_i; ++it) {
+            bool moved = false;
+#pragma unroll
+            for (int p = 0; p < P; ++p) {
+                const int n_i = lane + 32 * p;
+                float cand = finf();
+                if (!seed[p]) {
+                    float v[NACT], w[NACT];
+#pragma unroll
+                    for (int k = 0; k < NACT; ++k) {
+                        const int l0 = nbl[p][2 * k], l1 = nbl[p][2 * k + 1];
+                        const float a = l0 >= 0 ? us[l0] : nbv[p][2 * k];
+                        const float b = l1 >= 0 ? us[l1] : nbv[p][2 * k + 1];
+                        v[k] = a > b ? b : a;
+                        w[k] = wts[p][k];
+                    }
+                    cand = hfm_update<NACT>(rhs[p], v, w);
+                }
+                __syncwarp();
+                if (!seed[p] && us[n_i] > cand) {
+                    us[n_i] = cand;
+                    moved = true;
+                }
+                __syncwarp();
+            }
+            if (!__any_sync(kFull, moved)) break;
+        }
+        bool notconv = false;
+#pragma unroll
+        for (int p = 0; p < P; ++p) {
+            const int n_i = lane + 32 * p;
+            const float u = us[n_i];
+            __stcg(A.values + base + n_i, u);
+            const float diff = fabsf(uold[p] - u);
+            const float tol = A.atol + A.rtol * fabsf(u);
+            if (!(isnan(diff) || diff <= tol)) notconv = true;
+        }
+        const bool changed = __any_sync(kFull, notconv);
+        __syncwarp();
+
+        // Fast iterative method (cuda/Propagation.h:103-167).
+        const int t = I.tile_base + n_o;
+        const int front = A.fim_front_width;
+        int nb = -1;  // neighbour tile handled by this lane (lanes 0..2D-1)
+        if (lane < 2 * D) {
+            int y[3] = {xo[0], xo[1], xo[2]};
+            y[lane >> 1] += 2 * (lane & 1) - 1;
+            bool ok = true;
+#pragma unroll
+            for (int k = 0; k < D; ++k) ok = ok && y[k] >= 0 && y[k] < I.shape_o[k];
+            if (ok) {
+                int m = 0;
+#pragma unroll
+                for (int k = 0; k < D; ++k) m = m * I.shape_o[k] + y[k];
+                nb = I.tile_base + m;
+            }
+        }
+        int sn;
+        bool prop;
+        if (!changed) {
+            const int sp = (int)score_at(S, t, e - 1);
+            if (sp == 0 || sp == front) { sn = 0; prop = false; }
+            else { sn = front; prop = true; }
+        } else {
+            sn = 1;
+            if (lane == 0) push_tile(S, t, e);
+            if (front > 2) {
+                const int sq = nb >= 0 ? (int)score_at(S, nb, e - 1) - 1 : -1;
+                int mx = sq;
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) mx = max(mx, __shfl_xor_sync(kFull, mx, o));
+                sn = max(sn, mx);
+            }
+            prop = sn > 1;
+        }
+        if (lane == 0) {
+            unsigned *arr = (e & 1) ? S.score1 : S.score0;
+            __stcg(arr + t, ((unsigned)e << 8) | (unsigned)sn);
+            atomicAdd((unsigned long long *)&S.stats[ii].tile_visits, 1ull);
+            atomicMax(&S.stats[ii].niter_o, e);
+        }
+        if (prop && nb >= 0) push_tile(S, nb, e);
+    }
+};
+
+template <unsigned VMASK>
+__device__ __forceinline__ void dispatch(const Sched &S, int t, int e, int lane, float *us) {
+    const int ii = __ldg(S.tile_inst + t);
+    const Inst &I = S.inst[ii];
+    if (e > I.a.nitermax_o) {
+        if (lane == 0) atomicOr(&S.stats[ii].status, (int)AGD_STATUS_NOT_CONVERGED);
+        return;
+    }
+    const int n_o = t - I.tile_base;
+    switch (I.variant) {
+        case V_ISO2_8:
+            if constexpr ((VMASK >> V_ISO2_8) & 1) Visit<Tile<2, 8, 8, 1>, AGD_MODEL_ISOTROPIC>::run(S, I, ii, n_o, e, lane, us);
+            break;
+        case V_ISO2_16:
+            if constexpr ((VMASK >> V_ISO2_16) & 1) Visit<Tile<2, 16, 16, 1>, AGD_MODEL_ISOTROPIC>::run(S, I, ii, n_o, e, lane, us);
+            break;
+        case V_RIEM2_8:
+            if constexpr ((VMASK >> V_RIEM2_8) & 1) Visit<Tile<2, 8, 8, 1>, AGD_MODEL_RIEMANN>::run(S, I, ii, n_o, e, lane, us);
+            break;
+        case V_ISO3_4:
+            if constexpr ((VMASK >> V_ISO3_4) & 1) Visit<Tile<3, 4, 4, 4>, AGD_MODEL_ISOTROPIC>::run(S, I, ii, n_o, e, lane, us);
+            break;
+        case V_RIEM3_4:
+            if constexpr ((VMASK >> V_RIEM3_4) & 1) Visit<Tile<3, 4, 4, 4>, AGD_MODEL_RIEMANN>::run(S, I, ii, n_o, e, lane, us);
+            break;
+        default:
+            break;
+    }
+}
+
+constexpr int kMaxTileSize = 256;
+
+template <unsigned VMASK, int WPB>
+__global__ void __launch_bounds__(WPB * 32) eikonal_persistent(Sched S) {
+    __shared__ float s_u[WPB][kMaxTileSize];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int nw = gridDim.x * WPB;
+    const int gw = blockIdx.x * WPB + warp;
+    int e = 1;
+    for (; e <= S.max_epochs; ++e) {
+        const unsigned ncur = ld_acquire(&S.ctrl->cnt[e % 3]);
+        if (ncur == 0) break;
+        if (blockIdx.x == 0 && threadIdx.x == 0) S.ctrl->cnt[(e + 2) % 3] = 0;
+        const int *cur = (e & 1) ? S.list1 : S.list0;
+        for (unsigned i = gw; i < ncur; i += nw) {
+            const int t = __ldcg(cur + i);
+            dispatch<VMASK>(S, t, e, lane, s_u[warp]);
+        }
+        if (!grid_barrier(&S.ctrl->bar, gridDim.x, &S.ctrl->err, S.timeout_ns)) return;
+    }
+    if (blockIdx.x == 0) {
+        // Tiles still listed when the epoch budget ran out belong to unconverged instances.
+        const unsigned nleft = (e > S.max_epochs) ? ld_acquire(&S.ctrl->cnt[e % 3]) : 0u;
+        const int *cur = (e & 1) ? S.list1 : S.list0;
+        for (unsigned i = threadIdx.x; i < nleft; i += blockDim.x) {
+            const int ii = __ldg(S.tile_inst + __ldcg(cur + i));
+            atomicOr(&S.stats[ii].status, (int)AGD_STATUS_NOT_CONVERGED);
+        }
+        if (threadIdx.x == 0) S.ctrl->epochs = (unsigned)(e - 1);
+    }
+}
+
+// ---------------------------------------------------------------- setup ---
+// tile -> instance map, and the first list: tiles flagged by `trigger`, by
+// ACTIVATE_ALL, or holding a seed point inside the domain.
+__global__ void setup_tiles(Sched S, int ninst) {
+    const int t = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    const int lane = threadIdx.x & 31;
+    // locate the instance by bisection over the tile bases
+    int lo = 0, hi = ninst - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (S.inst[mid].tile_base <= t) lo = mid; else hi = mid - 1;
+    }
+    const Inst &I = S.inst[lo];
+    if (t >= I.tile_base + I.size_o) return;  // past the last tile
+    const int n_o = t - I.tile_base;
+    if (lane == 0) const_cast<int *>(S.tile_inst)[t] = lo;
+    bool active = (I.a.flags & AGD_FLAG_ACTIVATE_ALL) != 0;
+    if (I.a.trigger) {
+        active = active || I.a.trigger[n_o] != 0;
+    } else if (!active) {
+        int xo[3], r = n_o;
+        for (int k = I.a.ndim - 1; k >= 0; --k) { xo[k] = r % I.shape_o[k]; r /= I.shape_o[k]; }
+        bool any = false;
+        for (int n_i = lane; n_i < I.size_i; n_i += 32) {
+            int xi[3], q = n_i;
+            for (int k = I.a.ndim - 1; k >= 0; --k) { xi[k] = q % I.a.shape_i[k]; q /= I.a.shape_i[k]; }
+            bool in = true;
+            for (int k = 0; k < I.a.ndim; ++k) in = in && (xo[k] * I.a.shape_i[k] + xi[k] < I.a.shape[k]);
+            const size_t n_t = (size_t)n_o * I.size_i + n_i;
+            if (in && ((I.a.seedbits[n_t >> 3] >> (n_t & 7)) & 1)) any = true;
+        }
+        active = __any_sync(kFull, any);
+    }
+    if (active && lane == 0) {
+        S.flags[t] = 1u;
+        const unsigned idx = atomicAdd(&S.ctrl->cnt[1], 1u);
+        S.list1[idx] = t;
+    }
+}
+
+__global__ void finish_stats(Sched S, int ninst, agd_stats *out) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= ninst) return;
+    agd_stats st = S.stats[i];
+    st.status |= (int)S.ctrl->err;
+    if (out) out[i] = st;
+}
+
+// --------------------------------------------------------------- launch ---
+template <unsigned VMASK, int WPB>
+static int launch_persistent(const Sched &S, int total_tiles, const agd_launch *cfg, cudaStream_t st) {
+    auto kern = eikonal_persistent<VMASK, WPB>;
+    int dev = 0, nsm = 0, per_sm = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return set_cuda_error("cudaGetDevice");
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, WPB * 32, 0) != cudaSuccess)
+        return set_cuda_error("occupancy query");
+    if (per_sm < 1) return set_error(AGD_STATUS_UNSUPPORTED, "persistent kernel does not fit on an SM");
+    const int max_ctas = per_sm * nsm;
+    int ctas = cfg && cfg->ctas > 0 ? cfg->ctas : (total_tiles + 4 * WPB - 1) / (4 * WPB);
+    ctas = std::max(1, std::min(ctas, max_ctas));
+    Sched s = S;
+    void *args[] = {&s};
+    const cudaError_t err = cudaLaunchCooperativeKernel((const void *)kern, dim3(ctas), dim3(WPB * 32), args, 0, st);
+    if (err != cudaSuccess) return set_cuda_error("cooperative launch", err);
+    return AGD_STATUS_OK;
+}
+
+}  // namespace agd
+
+struct agd_plan {
+    std::vector<agd::Inst> insts;
+    agd::WsLayout L;
+    unsigned vmask;
+    int ndim;
+    int max_epochs;
+};
+
+namespace agd {
+
+static int plan_create(const agd_instance *host, int n, agd_plan **out) {
+    if (!out) return set_error(AGD_STATUS_INVALID, "null plan pointer");
+    *out = nullptr;
+    if (n <= 0 || !host) return set_error(AGD_STATUS_INVALID, "no instance");
+    agd_plan *P = new agd_plan();
+    if (!layout(host, n, P->L, &P->insts)) {
+        delete P;
+        return set_error(AGD_STATUS_INVALID, "bad instance shape");
+    }
+    P->ndim = host[0].ndim;
+    P->vmask = 0;
+    P->max_epochs = 0;
+    for (int i = 0; i < n; ++i) {
+        const agd_instance &a = host[i];
+        const char *bad = nullptr;
+        int code = AGD_STATUS_INVALID;
+        if (a.ndim != P->ndim) bad = "all instances of a plan must share ndim";
+        else if (P->insts[i].variant < 0) { bad = "model/tile shape not built"; code = AGD_STATUS_UNSUPPORTED; }
+        else if (a.multip_step != 0.f) { bad = "multiprecision not built"; code = AGD_STATUS_UNSUPPORTED; }
+        else if (!a.values || !a.rhs || !a.seedbits || (a.model == AGD_MODEL_RIEMANN && !a.geom)) bad = "missing array";
+        else if (a.niter_i < 1 || a.fim_front_width < 2 || a.fim_front_width > 255 || a.nitermax_o < 0)
+            bad = "bad niter_i / fim_front_width / nitermax_o";
+        if (bad) {
+            delete P;
+            return set_error(code, bad);
+        }
+        P->vmask |= 1u << P->insts[i].variant;
+        P->max_epochs = std::max(P->max_epochs, a.nitermax_o);
+    }
+    *out = P;
+    return AGD_STATUS_OK;
+}
+
+static Sched sched_of(const agd_plan *P, void *ws) {
+    const WsLayout &L = P->L;
+    char *w = static_cast<char *>(ws);
+    Sched S;
+    S.inst = reinterpret_cast<const Inst *>(w + L.inst);
+    S.tile_inst = reinterpret_cast<const int *>(w + L.tile_inst);
+    S.list0 = reinterpret_cast<int *>(w + L.list0);
+    S.list1 = reinterpret_cast<int *>(w + L.list1);
+    S.flags = reinterpret_cast<unsigned *>(w + L.flags);
+    S.score0 = reinterpret_cast<unsigned *>(w + L.score0);
+    S.score1 = reinterpret_cast<unsigned *>(w + L.score1);
+    S.ctrl = reinterpret_cast<Ctrl *>(w + L.ctrl);
+    S.stats = reinterpret_cast<agd_stats *>(w + L.stats);
+    S.max_epochs = P->max_epochs + 1;  // one extra epoch detects an instance exceeding its budget
+    S.timeout_ns = 2000000000ull;
+    return S;
+}
+
+static int plan_run(const agd_plan *P, void *ws, size_t ws_bytes, agd_stats *stats, const agd_launch *cfg,
+                    cudaStream_t st) {
+    if (!P || !ws) return set_error(AGD_STATUS_INVALID, "null plan or workspace");
+    const WsLayout &L = P->L;
+    if (ws_bytes < L.total) return set_error(AGD_STATUS_WORKSPACE, "workspace too small");
+    const int n = (int)P->insts.size();
+    Sched S = sched_of(P, ws);
+    if (cfg && cfg->timeout_ns > 0) S.timeout_ns = (unsigned long long)cfg->timeout_ns;
+    char *w = static_cast<char *>(ws);
+    cudaError_t err = cudaMemsetAsync(w + L.flags, 0, L.ctrl - L.flags + sizeof(Ctrl), st);
+    if (err != cudaSuccess) return set_cuda_error("workspace clear", err);
+    err = cudaMemsetAsync(w + L.stats, 0, sizeof(agd_stats) * n, st);
+    if (err != cudaSuccess) return set_cuda_error("stats clear", err);
+    {
+        const int wpb = 8;
+        setup_tiles<<<(L.total_tiles + wpb - 1) / wpb, wpb * 32, 0, st>>>(S, n);
+        if ((err = cudaGetLastError()) != cudaSuccess) return set_cuda_error("setup_tiles", err);
+    }
+    int rc;
+    const unsigned vmask = P->vmask;
+    const int wpb = (cfg && cfg->warps_per_cta == 8) ? 8 : 4;
+#define AGD_LAUNCH(M) (wpb == 8 ? launch_persistent<(M), 8>(S, L.total_tiles, cfg, st) \
+                                : launch_persistent<(M), 4>(S, L.total_tiles, cfg, st))
+    if (P->ndim == 2) {
+        if (vmask == (1u << V_RIEM2_8)) rc = AGD_LAUNCH(1u << V_RIEM2_8);
+        else if (vmask == (1u << V_ISO2_16)) rc = AGD_LAUNCH(1u << V_ISO2_16);
+        else if (vmask == (1u << V_ISO2_8)) rc = AGD_LAUNCH(1u << V_ISO2_8);
+        else rc = AGD_LAUNCH((1u << V_ISO2_8) | (1u << V_ISO2_16) | (1u << V_RIEM2_8));
+    } else {
+        if (vmask == (1u << V_RIEM3_4)) rc = AGD_LAUNCH(1u << V_RIEM3_4);
+        else if (vmask == (1u << V_ISO3_4)) rc = AGD_LAUNCH(1u << V_ISO3_4);
+        else rc = AGD_LAUNCH((1u << V_ISO3_4) | (1u << V_RIEM3_4));
+    }
+#undef AGD_LAUNCH
+    if (rc != AGD_STATUS_OK) return rc;
+    finish_stats<<<(n + 127) / 128, 128, 0, st>>>(S, n, stats);
+    if ((err = cudaGetLastError()) != cudaSuccess) return set_cuda_error("finish_stats", err);
+    return AGD_STATUS_OK;
+}
+
+static int plan_upload(const agd_plan *P, void *ws, size_t ws_bytes, cudaStream_t st) {
+    if (!P || !ws) return set_error(AGD_STATUS_INVALID, "null plan or workspace");
+    if (ws_bytes < P->L.total) return set_error(AGD_STATUS_WORKSPACE, "workspace too small");
+    const cudaError_t err = cudaMemcpyAsync(static_cast<char *>(ws) + P->L.inst, P->insts.data(),
+                                            sizeof(Inst) * P->insts.size(), cudaMemcpyHostToDevice, st);
+    return err == cudaSuccess ? AGD_STATUS_OK : set_cuda_error("descriptor upload", err);
+}
+
+// ------------------------------------------------------------------ flow ---
+// Upwind flow at every point of a solved instance (FLOW_* exports of
+// cuda/Update.h:171-209 with one local iteration).  Values are not modified.
+template <class TL, int MODEL>
+__global__ void flow_kernel(Inst I, float *fvec, float *fwsum, float *fw, int *fidx) {
+    using V = Visit<TL, MODEL>;
+    constexpr int D = TL::D, P = TL::P, NACT = V::NACT;
+    const int lane = threadIdx.x & 31;
+    const int n_o = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    if (n_o >= I.size_o) return;
+    const agd_instance &A = I.a;
+    int xo[3] = {0, 0, 0};
+    {
+        int r = n_o;
+#pragma unroll
+        for (int k = D - 1; k >= 0; --k) { xo[k] = r % I.shape_o[k]; r /= I.shape_o[k]; }
+    }
+#pragma unroll
+    for (int p = 0; p < P; ++p) {
+        const int n_i = lane + 32 * p;
+        const size_t n_t = (size_t)n_o * TL::SIZE + n_i;
+        int xi[3] = {0, 0, 0}, xt[3] = {0, 0, 0};
+        TL::pos(n_i, xi);
+        bool in = true;
+#pragma unroll
+        for (int k = 0; k < D; ++k) {
+            xt[k] = xo[k] * TL::extent(k) + xi[k];
+            in = in && xt[k] < A.shape[k];
+        }
+        const bool seed = (__ldg(A.seedbits + (n_t >> 3)) >> (n_t & 7)) & 1;
+        float w[NACT], fwk[NACT];
+        int ev[NACT][3], side[NACT];
+        V::stencil(I, n_t, w, ev);
+        float v[NACT];
+#pragma unroll
+        for (int k = 0; k < NACT; ++k) {
+            side[k] = 0;
+            fwk[k] = 0.f;
+#pragma unroll
+            for (int s = 0; s < 2; ++s) {
+                int y[3] = {0, 0, 0};
+                bool ok = true;
+#pragma unroll
+                for (int c = 0; c < D; ++c) {
+                    y[c] = xt[c] + (2 * s - 1) * ev[k][c];
+                    ok = ok && y[c] >= 0 && y[c] < A.shape[c];
+                }
+                const float val = ok ? __ldg(A.values + bilevel_index<D, TL>(y, I.shape_o)) : finf();
+                if (s == 0) v[k] = val;
+                else if (v[k] > val) { v[k] = val; side[k] = 1; }
+            }
+        }
+        if (!seed && in) {
+            float vs[NACT], ws[NACT];
+#pragma unroll
+            for (int k = 0; k < NACT; ++k) { vs[k] = v[k]; ws[k] = w[k]; }
+            const float val = hfm_update<NACT>(__ldg(A.rhs + n_t), vs, ws);
+            if (val != finf()) {
+#pragma unroll
+                for (int k = 0; k < NACT; ++k) fwk[k] = w[k] * fmaxf(0.f, val - v[k]);
+            }
+        }
+        float vec[3] = {0.f, 0.f, 0.f}, sum = 0.f;
+#pragma unroll
+        for (int k = 0; k < NACT; ++k) {
+            sum += fwk[k];
+            const int eps = 2 * side[k] - 1;
+            int y[3] = {0, 0, 0};
+#pragma unroll
+            for (int c = 0; c < D; ++c) {
+                const int off = eps * ev[k][c];
+                vec[c] += fwk[k] * float(off);
+                y[c] = xt[c] + off;
+            }
+            if (fw) fw[(size_t)k * I.size_tot + n_t] = fwk[k];
+            if (fidx) fidx[(size_t)k * I.size_tot + n_t] = fwk[k] != 0.f ? bilevel_index<D, TL>(y, I.shape_o) : kIntMax;
+        }
+        if (fvec)
+#pragma unroll
+            for (int c = 0; c < D; ++c) fvec[(size_t)c * I.size_tot + n_t] = vec[c];
+        if (fwsum) fwsum[n_t] = sum;
+    }
+}
+
+static int flow_impl(const agd_instance *a, float *fvec, float *fwsum, float *fw, int *fidx, cudaStream_t st) {
+    WsLayout L;
+    std::vector<Inst> v;
+    if (!a || !layout(a, 1, L, &v)) return set_error(AGD_STATUS_INVALID, "bad instance");
+    const Inst &I = v[0];
+    const int wpb = 4, grid = (I.size_o + wpb - 1) / wpb;
+    switch (I.variant) {
+        case V_ISO2_8: flow_kernel<Tile<2, 8, 8, 1>, AGD_MODEL_ISOTROPIC><<<grid, wpb * 32, 0, st>>>(I, fvec, fwsum, fw, fidx); break;
+        case V_ISO2_16: flow_kernel<Tile<2, 16, 16, 1>, AGD_MODEL_ISOTROPIC><<<grid, wpb * 32, 0, st>>>(I, fvec, fwsum, fw, fidx); break;
+        case V_RIEM2_8: flow_kernel<Tile<2, 8, 8, 1>, AGD_MODEL_RIEMANN><<<grid, wpb * 32, 0, st>>>(I, fvec, fwsum, fw, fidx); break;
+        case V_ISO3_4: flow_kernel<Tile<3, 4, 4, 4>, AGD_MODEL_ISOTROPIC><<<grid, wpb * 32, 0, st>>>(I, fvec, fwsum, fw, fidx); break;
+        case V_RIEM3_4: flow_kernel<Tile<3, 4, 4, 4>, AGD_MODEL_RIEMANN><<<grid, wpb * 32, 0, st>>>(I, fvec, fwsum, fw, fidx); break;
+        default: return set_error(AGD_STATUS_UNSUPPORTED, "model/tile shape not built");
+    }
+    const cudaError_t err = cudaGetLastError();
+    return err == cudaSuccess ? AGD_STATUS_OK : set_cuda_error("flow_kernel", err);
+}
+
+// ---------------------------------------------------------- layout prep ---
+struct Geo {
+    int nd, shape[3], si[3], so[3], size_i;
+    long long size_tot, n;
+};
+static bool geo_of(int nd, const int *shape, const int *si, Geo &g) {
+    if (nd < 1 || nd > 3) return false;
+    g.nd = nd;
+    g.size_i = 1;
+    g.n = 1;
+    long long so = 1;
+    for (int k = 0; k < 3; ++k) { g.shape[k] = 1; g.si[k] = 1; g.so[k] = 1; }
+    for (int k = 0; k < nd; ++k) {
+        if (shape[k] <= 0 || si[k] <= 0) return false;
+        g.shape[k] = shape[k];
+        g.si[k] = si[k];
+        g.so[k] = (shape[k] + si[k] - 1) / si[k];
+        g.size_i *= si[k];
+        so *= g.so[k];
+        g.n *= shape[k];
+    }
+    g.size_tot = so * g.size_i;
+    return true;
+}
+
+// bilevel index -> grid coordinates (returns false for padding)
+__device__ __forceinline__ bool grid_coords(const Geo &g, long long n_t, int *x, long long &flat) {
+    long long n_o = n_t / g.size_i;
+    int n_i = (int)(n_t - n_o * g.size_i);
+    int xo[3], xi[3];
+    for (int k = g.nd - 1; k >= 0; --k) {
+        xo[k] = (int)(n_o % g.so[k]); n_o /= g.so[k];
+        xi[k] = n_i % g.si[k]; n_i /= g.si[k];
+    }
+    bool in = true;
+    flat = 0;
+    for (int k = 0; k < g.nd; ++k) {
+        x[k] = xo[k] * g.si[k] + xi[k];
+        in = in && x[k] < g.shape[k];
+        flat = flat * g.shape[k] + x[k];
+    }
+    return in;
+}
+
+__global__ void block_expand_kernel(Geo g, int nplanes, const float *src, int bcast, float pad, float *dst) {
+    const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (i >= g.size_tot * nplanes) return;
+    const int plane = (int)(i / g.size_tot);
+    const long long n_t = i - plane * g.size_tot;
+    int x[3];
+    long long flat;
+    const bool in = grid_coords(g, n_t, x, flat);
+    dst[i] = in ? (bcast ? src[plane] : src[plane * g.n + flat]) : pad;
+}
+
+__global__ void block_squeeze_kernel(Geo g, int nplanes, const float *src, float *dst) {
+    const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (i >= g.n * nplanes) return;
+    const int plane = (int)(i / g.n);
+    long long r = i - plane * g.n;
+    int x[3];
+    for (int k = g.nd - 1; k >= 0; --k) { x[k] = (int)(r % g.shape[k]); r /= g.shape[k]; }
+    long long n_o = 0, n_i = 0;
+    for (int k = 0; k < g.nd; ++k) {
+        n_o = n_o * g.so[k] + x[k] / g.si[k];
+        n_i = n_i * g.si[k] + x[k] % g.si[k];
+    }
+    dst[i] = src[plane * g.size_tot + n_o * g.size_i + n_i];
+}
+
+// Dual metric of M' = diag(h) M diag(h) (Riemann.with_costs, then dual), by the
+// adjugate formula; packed [d00, d10, d11(, d20, d21, d22)] planes in tile layout.
+__global__ void prep_geom_kernel(Geo g, const float *metric, int bcast, int is_dual, double h0, double h1,
+                                 double h2, float *geom) {
+    const long long n_t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (n_t >= g.size_tot) return;
+    const int sd = g.nd * (g.nd + 1) / 2;
+    int x[3];
+    long long flat;
+    const bool in = grid_coords(g, n_t, x, flat);
+    if (!in) {
+        for (int c = 0; c < sd; ++c) geom[c * g.size_tot + n_t] = finf();
+        return;
+    }
+    const float *m = bcast ? metric : metric + flat * sd;
+    const float h[3] = {(float)h0, (float)h1, (float)h2};
+    if (g.nd == 2) {
+        float a = m[0], b = m[1], c = m[2];
+        if (is_dual) {  // dualMetric.with_speeds(h): entries / (h_i h_j)
+            a = a / (h[0] * h[0]); b = b / (h[1] * h[0]); c = c / (h[1] * h[1]);
+            geom[n_t] = a; geom[g.size_tot + n_t] = b; geom[2 * g.size_tot + n_t] = c;
+            return;
+        }
+        a = a * (h[0] * h[0]); b = b * (h[1] * h[0]); c = c * (h[1] * h[1]);
+        const float det = a * c - b * b;
+        geom[n_t] = c / det;
+        geom[g.size_tot + n_t] = -b / det;
+        geom[2 * g.size_tot + n_t] = a / det;
+    } else {
+        float s[6];
+        int k = 0;
+        for (int i = 0; i < 3; ++i)
+            for (int j = 0; j <= i; ++j, ++k) s[k] = is_dual ? m[k] / (h[i] * h[j]) : m[k] * (h[i] * h[j]);
+        if (is_dual) {
+            for (int c = 0; c < 6; ++c) geom[c * g.size_tot + n_t] = s[c];
+            return;
+        }
+        // symmetric [[a,b,d],[b,c,e],[d,e,f]] with s = [a, b, c, d, e, f]
+        const float a = s[0], b = s[1], c = s[2], d = s[3], e = s[4], f = s[5];
+        const float A00 = c * f - e * e, A10 = d * e - b * f, A11 = a * f - d * d;
+        const float A20 = b * e - c * d, A21 = b * d - a * e, A22 = a * c - b * b;
+        const float det = a * A00 + b * A10 + d * A20;
+        const float out[6] = {A00 / det, A10 / det, A11 / det, A20 / det, A21 / det, A22 / det};
+        for (int q = 0; q < 6; ++q) geom[q * g.size_tot + n_t] = out[q];
+    }
+}
+
+// Seed bits: one 32-bit word (32 points) per thread, padding bits set.
+__global__ void seedbits_init_kernel(Geo g, unsigned *bits) {
+    const long long wi = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (wi * 32 >= g.size_tot) return;
+    unsigned word = 0;
+    for (int b = 0; b < 32; ++b) {
+        int x[3];
+        long long flat;
+        if (!grid_coords(g, wi * 32 + b, x, flat)) word |= 1u << b;
+    }
+    bits[wi] = word;
+}
+
+// Seeds in order (a later duplicate overrides an earlier one, as numpy assignment does).
+__global__ void seeds_kernel(Geo g, const int *idx, const float *vals, int n, float *rhs, unsigned *bits,
+                             unsigned char *trigger, int *bad) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    for (int s = 0; s < n; ++s) {
+        long long n_o = 0, n_i = 0;
+        bool ok = true;
+        for (int k = 0; k < g.nd; ++k) {
+            const int xk = idx[s * g.nd + k];
+            ok = ok && xk >= 0 && xk < g.shape[k];
+            n_o = n_o * g.so[k] + (ok ? xk / g.si[k] : 0);
+            n_i = n_i * g.si[k] + (ok ? xk % g.si[k] : 0);
+        }
+        if (!ok) { *bad = 1; continue; }
+        const long long n_t = n_o * g.size_i + n_i;
+        if (rhs) rhs[n_t] = vals ? vals[s] : 0.f;
+        if (bits) bits[n_t >> 5] |= 1u << (n_t & 31);
+        if (trigger) trigger[n_o] = 1;
+    }
+}
+
+__global__ void selling_kernel(int nd, const float *m, int n, float *w, int *e) {
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= n) return;
+    float ww[6];
+    int ee[6][3];
+    if (nd == 2) {
+        float mm[3] = {m[3 * p], m[3 * p + 1], m[3 * p + 2]};
+        selling2(mm, ww, ee);
+        for (int r = 0; r < 3; ++r) { w[3 * p + r] = ww[r]; e[(3 * p + r) * 2] = ee[r][0]; e[(3 * p + r) * 2 + 1] = ee[r][1]; }
+    } else {
+        float mm[6];
+        for (int c = 0; c < 6; ++c) mm[c] = m[6 * p + c];
+        selling3(mm, ww, ee);
+        for (int r = 0; r < 6; ++r) { w[6 * p + r] = ww[r]; for (int c = 0; c < 3; ++c) e[(6 * p + r) * 3 + c] = ee[r][c]; }
+    }
+}
+
+static inline unsigned blocks_for(long long n, int bs) { return (unsigned)((n + bs - 1) / bs); }
+
+}  // namespace agd
+
+using namespace agd;
+
+extern "C" {
+
+int agd_plan_create(const agd_instance *inst, int n, agd_plan **plan) {
+    clear_error();
+    return plan_create(inst, n, plan);
+}
+
+void agd_plan_destroy(agd_plan *plan) { delete plan; }
+
+size_t agd_plan_workspace_bytes(const agd_plan *plan) { return plan ? plan->L.total : 0; }
+
+int agd_plan_upload(const agd_plan *plan, void *workspace, size_t workspace_bytes, agd_stream_t stream) {
+    clear_error();
+    return plan_upload(plan, workspace, workspace_bytes, (cudaStream_t)stream);
+}
+
+int agd_plan_run(const agd_plan *plan, void *workspace, size_t workspace_bytes, agd_stats *stats,
+                 const agd_launch *launch, agd_stream_t stream) {
+    clear_error();
+    return plan_run(plan, workspace, workspace_bytes, stats, launch, (cudaStream_t)stream);
+}
+
+size_t agd_eikonal_workspace_bytes(const agd_instance *inst, int n) {
+    WsLayout L;
+    if (!inst || n <= 0 || !layout(inst, n, L, nullptr)) return 0;
+    return L.total;
+}
+
+int agd_eikonal_solve(const agd_instance *inst, int n, void *workspace, size_t workspace_bytes, agd_stats *stats,
+                      const agd_launch *launch, agd_stream_t stream) {
+    clear_error();
+    agd_plan *P = nullptr;
+    int rc = plan_create(inst, n, &P);
+    if (rc != AGD_STATUS_OK) return rc;
+    rc = plan_upload(P, workspace, workspace_bytes, (cudaStream_t)stream);
+    if (rc == AGD_STATUS_OK) rc = plan_run(P, workspace, workspace_bytes, stats, launch, (cudaStream_t)stream);
+    delete P;
+    return rc;
+}
+
+int agd_flow(const agd_instance *inst, float *flow_vector, float *flow_weightsum, float *flow_weights,
+             int32_t *flow_indices, agd_stream_t stream) {
+    clear_error();
+    return flow_impl(inst, flow_vector, flow_weightsum, flow_weights, flow_indices, (cudaStream_t)stream);
+}
+
+int agd_prep_geom(int ndim, const int *shape, const int *shape_i, const float *metric, int broadcast, int is_dual,
+                  const double *grid_scales, float *geom, agd_stream_t stream) {
+    clear_error();
+    Geo g;
+    if (ndim < 2 || !geo_of(ndim, shape, shape_i, g) || !metric || !geom || !grid_scales)
+        return set_error(AGD_STATUS_INVALID, "agd_prep_geom: bad arguments");
+    prep_geom_kernel<<<blocks_for(g.size_tot, 256), 256, 0, (cudaStream_t)stream>>>(
+        g, metric, broadcast, is_dual, grid_scales[0], grid_scales[1], ndim == 3 ? grid_scales[2] : 1.0, geom);
+    const cudaError_t err = cudaGetLastError();
+    return err == cudaSuccess ? AGD_STATUS_OK : set_cuda_error("prep_geom", err);
+}
+
+int agd_block_expand(int ndim, const int *shape, const int *shape_i, int nplanes, const float *src, int src_broadcast,
+                     float pad, float *dst, agd_stream_t stream) {
+    clear_error();
+    Geo g;
+    if (!geo_of(ndim, shape, shape_i, g) || nplanes < 1 || !src || !dst)
+        return set_error(AGD_STATUS_INVALID, "agd_block_expand: bad arguments");
+    block_expand_kernel<<<blocks_for(g.size_tot * nplanes, 256), 256, 0, (cudaStream_t)stream>>>(
+        g, nplanes, src, src_broadcast, pad, dst);
+    const cudaError_t err = cudaGetLastError();
+    return err == cudaSuccess ? AGD_STATUS_OK : set_cuda_error("block_expand", err);
+}
+
+int agd_block_squeeze(int ndim, const int *shape, const int *shape_i, int nplanes, const float *src, float *dst,
+                      agd_stream_t stream) {
+    clear_error();
+    Geo g;
+    if (!geo_of(ndim, shape, shape_i, g) || nplanes < 1 || !src || !dst)
+        return set_error(AGD_STATUS_INVALID, "agd_block_squeeze: bad arguments");
+    block_squeeze_kernel<<<blocks_for(g.n * nplanes, 256), 256, 0, (cudaStream_t)stream>>>(g, nplanes, src, dst);
+    const cudaError_t err = cudaGetLastError();
+    return err == cudaSuccess ? AGD_STATUS_OK : set_cuda_error("block_squeeze", err);
+}
+
+int agd_prep_seeds(int ndim, const int *shape, const int *shape_i, const int32_t *seed_index, const float *seed_values,
+                   int n, float *rhs, uint8_t *seedbits, uint8_t *trigger, agd_stream_t stream) {
+    clear_error();
+    Geo g;
+    if (!geo_of(ndim, shape, shape_i, g) || n < 0 || (n > 0 && !seed_index) || (g.size_tot % 32) != 0)
+        return set_error(AGD_STATUS_INVALID, "agd_prep_seeds: bad arguments");
+    cudaStream_t st = (cudaStream_t)stream;
+    if (seedbits)
+        seedbits_init_kernel<<<blocks_for(g.size_tot / 32, 256), 256, 0, st>>>(g, reinterpret_cast<unsigned *>(seedbits));
+    if (trigger) cudaMemsetAsync(trigger, 0, (size_t)(g.size_tot / g.size_i), st);
+    if (n > 0) {
+        seeds_kernel<<<1, 32, 0, st>>>(g, seed_index, seed_values, n, rhs, reinterpret_cast<unsigned *>(seedbits),
+                                       trigger, nullptr);
+    }
+    const cudaError_t err = cudaGetLastError();
+    return err == cudaSuccess ? AGD_STATUS_OK : set_cuda_error("prep_seeds", err);
+}
+
+int agd_selling(int ndim, const float *m, int n, float *weights, int32_t *offsets, agd_stream_t stream) {
+    clear_error();
+    if ((ndim != 2 && ndim != 3) || n < 0 || (n > 0 && (!m || !weights || !offsets)))
+        return set_error(AGD_STATUS_INVALID, "agd_selling: bad arguments");
+    if (n == 0) return AGD_STATUS_OK;
+    selling_kernel<<<blocks_for(n, 128), 128, 0, (cudaStream_t)stream>>>(ndim, m, n, weights, offsets);
+    const cudaError_t err = cudaGetLastError();
+    return err == cudaSuccess ? AGD_STATUS_OK : set_cuda_error("selling", err);
+}
+
+}  // extern "C"

@@ -1,0 +1,314 @@
+"""Benchmark: batched Riemann2 512x512 eikonal solves on B200.
+
+Workload (a "step"): one persistent launch solving a batch of independent
+Riemann2 512^2 problems from a cold start (+inf values), with metrics
+M = R(theta) diag(1, lambda) R(theta)^T, theta a smoothed random angle field
+(sigma = 8 px at 512^2, i.e. the sigma = 16 px of the 1024^2 configuration in
+the same physical units), lambda ~ U[1, 100] per pixel, 4 random seeds, cost 1,
+gridScale 1/512, default tolerances.  Seeded synthetic data.
+
+Reports solves/s (whole job), grid-updates/s, the HBM roofline of the
+persistent solver kernel from its CUDA-event time and algorithmic bytes
+(24.125 B per grid update), the end-to-end rate through the public API from
+pinned host buffers, and a CPU baseline (the oracle, all host cores).
+
+Usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, REPO)
+
+BYTES_PER_UPDATE = {"Riemann2": 24.125, "Riemann3": 36.125, "Isotropic2": 12.125, "Isotropic3": 12.125}
+METRIC = "solves/s, Riemann2 512x512 batched cold-start solves (grid-updates/s in config)"
+
+
+def peaks():
+    try:
+        with open(os.path.join(REPO, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:  # noqa: BLE001
+        return 6650.0, "fallback"
+
+
+def make_fields(n, batch, seed, sigma=8.0):
+    from scipy.ndimage import gaussian_filter
+    rng = np.random.default_rng(seed)
+    metrics, seeds = [], []
+    for _ in range(batch):
+        g1 = gaussian_filter(rng.standard_normal((n, n)), sigma, mode="wrap")
+        g2 = gaussian_filter(rng.standard_normal((n, n)), sigma, mode="wrap")
+        th = np.arctan2(g1, g2)
+        lam = rng.uniform(1.0, 100.0, (n, n))
+        c, s = np.cos(th), np.sin(th)
+        metrics.append(np.stack([c * c + lam * s * s, c * s * (1 - lam), s * s + lam * c * c], -1).astype(np.float32))
+        seeds.append(rng.uniform(0.05, 0.95, (4, 2)).astype(np.float32))
+    return metrics, seeds
+
+
+def dictins(metrics, seeds, n, to_device=True, pinned=False):
+    import torch
+    from adaptivegriddiscretizations_b200 import Eikonal
+    out = []
+    for m, s in zip(metrics, seeds):
+        mt = torch.from_numpy(m)
+        st = torch.from_numpy(s)
+        if pinned:
+            mt, st = mt.pin_memory(), st.pin_memory()
+        if to_device:
+            mt, st = mt.cuda(), st.cuda()
+        out.append(Eikonal.dictIn({"model": "Riemann2", "mode": "gpu", "verbosity": 0,
+                                   "dims": [n, n], "gridScale": 1.0 / n, "origin": [0.0, 0.0],
+                                   "metric": mt, "seeds": st, "exportValues": True}))
+    return out
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    def __init__(self, index):
+        self.index, self.proc, self.lines = index, None, []
+
+    def __enter__(self):
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:  # noqa: BLE001
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc:
+            time.sleep(0.25)
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:  # noqa: BLE001
+                self.proc.kill()
+
+    def summary(self):
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            p = [x.strip() for x in ln.split(",")]
+            if len(p) < 9:
+                continue
+            try:
+                sm.append(float(p[1]))
+                smax = float(p[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, p[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        if not sm:
+            return None
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": smax, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def cpu_baseline(n, seconds_budget=25.0):
+    """The oracle (C++ restatement of the scheme), OpenMP over all host cores, on
+    instances of the same workload; returns (solves/s, grid-updates/s, cores, sample)."""
+    from oracle import oracle as O
+    cores = os.cpu_count() or 1
+    metrics, seeds = make_fields(n, 4, 1234)
+    t0 = time.perf_counter()
+    solves, updates = 0, 0
+    for m, s in zip(metrics, seeds):
+        case = dict(model="Riemann2", dims=np.array([n, n], np.float32), gridScales=np.full(2, 1.0 / n, np.float32),
+                    origin=np.zeros(2, np.float32), metric=m, seeds=s)
+        r = O.run(case, np.float32, nthreads=cores)
+        solves += 1
+        updates += r["tile_visits"] * 64
+        if time.perf_counter() - t0 > seconds_budget:
+            break
+    dt = time.perf_counter() - t0
+    return solves / dt, updates / dt, cores, f"{solves} Riemann2 {n}^2 solve(s) of the same field distribution, float32"
+
+
+def run_reference(args, rank):
+    if rank != 0:
+        return
+    n = args.n
+    vals = []
+    for _ in range(args.warmup):
+        cpu_baseline(n, seconds_budget=1e-9)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        v, gu, cores, sample = cpu_baseline(n, seconds_budget=1e-9)
+        vals.append(v)
+    dt = time.perf_counter() - t0
+    value = args.steps / dt
+    print(json.dumps({
+        "metric": METRIC, "value": value, "unit": "solves/s", "impl": "reference", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000 * dt / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": f"Riemann2 {n}x{n}, 1 instance per step on the host cores (oracle port)",
+                   "grid": n, "seeds": 4},
+        "cpu_baseline": {"value": value, "unit": "solves/s", "cores": cores, "kind": "port",
+                         "sample": "one Riemann2 solve per step; the reference's own CPU path (the external HFM "
+                                   "library) is not available, the oracle is the C++ restatement of its scheme"},
+        "e2e": {"value": value, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--batch", type=int, default=64)
+    ap.add_argument("--n", type=int, default=512)
+    ap.add_argument("--ctas", type=int, default=0)
+    ap.add_argument("--wpc", type=int, default=4)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--e2e-steps", type=int, default=2)
+    args = ap.parse_args()
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    if args.impl == "reference":
+        run_reference(args, rank)
+        return
+
+    import torch
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+
+    from adaptivegriddiscretizations_b200 import Eikonal, _lib
+    from adaptivegriddiscretizations_b200.Eikonal.HFM_CUDA import Interface, BatchPlan
+
+    n, B = args.n, args.batch
+    metrics, seeds = make_fields(n, B, 1000 + rank)
+    ins = dictins(metrics, seeds, n, to_device=True)
+    itfs = [Interface(h) for h in ins]
+    for it in itfs:
+        it.SetKernelTraits()
+        it.SetGeometry()
+        it.SetArgs()
+    size_tot = itfs[0].size_tot
+    values = torch.full((B, size_tot), float("inf"), dtype=torch.float32, device="cuda")
+    for i, it in enumerate(itfs):
+        it.values_t = values[i]
+    launch = _lib.AgdLaunch(ctas=args.ctas, warps_per_cta=args.wpc, timeout_ns=0)
+    plan = BatchPlan(itfs, launch=launch)
+
+    def step():
+        values.fill_(float("inf"))
+        plan.run()
+
+    for _ in range(max(3, args.warmup)):
+        step()
+    torch.cuda.synchronize()
+    niter, status, visits = plan.read_stats()
+    assert not status.any(), f"solver status {status}"
+    updates_per_step = int(visits.sum()) * 64
+
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clk:
+        t0 = torch.cuda.Event(enable_timing=True)
+        t1 = torch.cuda.Event(enable_timing=True)
+        t0.record()
+        for k in range(args.steps):
+            values.fill_(float("inf"))
+            evs[k][0].record()
+            plan.run()
+            evs[k][1].record()
+        t1.record()
+        torch.cuda.synchronize()
+    elapsed = t0.elapsed_time(t1) / 1000.0
+    kern = np.array([a.elapsed_time(b) / 1000.0 for a, b in evs])
+    if dist:
+        tt = torch.tensor([elapsed], device="cuda")
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        elapsed = float(tt)
+    niter, status, visits = plan.read_stats()
+    assert not status.any()
+    updates_per_step = int(visits.sum()) * 64
+    total_solves = B * args.steps * world
+    value = total_solves / elapsed
+    hbm, peak_kind = peaks()
+    achieved = updates_per_step * BYTES_PER_UPDATE["Riemann2"] / kern.mean() / 1e9
+
+    # end to end: public API from pinned host buffers, values back to the host
+    e2e = None
+    if args.e2e_steps > 0:
+        host_ins = dictins(metrics, seeds, n, to_device=False, pinned=True)
+        h2d = sum(m.nbytes + s.nbytes for m, s in zip(metrics, seeds))
+        outs = Eikonal.RunBatch(host_ins[:2])  # warm up the path
+        torch.cuda.synchronize()
+        t_e = time.perf_counter()
+        d2h = 0
+        for _ in range(args.e2e_steps):
+            host_ins = dictins(metrics, seeds, n, to_device=False, pinned=True)
+            outs = Eikonal.RunBatch(host_ins)
+            vals = [o["values"].cpu() for o in outs]
+            d2h = sum(v.numel() * 4 for v in vals)
+        torch.cuda.synchronize()
+        te = time.perf_counter() - t_e
+        e2e = {"value": B * args.e2e_steps * world / te, "unit": "solves/s", "h2d_bytes_per_step": int(h2d),
+               "d2h_bytes_per_step": int(d2h)}
+
+    cpu = None
+    if rank == 0 and not args.no_cpu_baseline:
+        v, gu, cores, sample = cpu_baseline(n)
+        cpu = {"value": v, "unit": "solves/s", "cores": cores, "kind": "port", "sample": sample,
+               "grid_updates_per_s": gu}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1000 * elapsed / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": f"Riemann2 {n}x{n} cold-start solves, batch {B} per GPU per step, one "
+                                   f"persistent launch", "batch_per_gpu": B, "grid": n, "seeds": 4,
+                       "lambda": "U[1,100]", "theta_sigma_px": 8, "tile": "8x8", "niter_i": 8,
+                       "grid_updates_per_step": updates_per_step,
+                       "grid_updates_per_s": updates_per_step * args.steps * world / elapsed,
+                       "mean_niter_o": float(niter.mean()), "max_niter_o": int(niter.max()),
+                       "l2": "inputs larger than L2 (batch working set %.0f MB)" % (B * size_tot * 24 / 1e6),
+                       "parallelism": f"replicas x{world}"},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                         "frac": achieved / hbm, "traffic": None, "peak_kind": peak_kind,
+                         "kernel": "eikonal_persistent", "kernel_ms": float(kern.mean() * 1000),
+                         "bytes_per_update": BYTES_PER_UPDATE["Riemann2"]},
+            "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": 3 * args.steps,
+            "clocks": clk.summary(),
+        }
+        print(json.dumps(line), flush=True)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

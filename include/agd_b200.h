@@ -1,0 +1,210 @@
+/*
+ * agd_b200.h - C ABI of the B200 eikonal path (Isotropic2/3, Riemann2/3).
+ *
+ * Plain pointers and sizes only.  Every array argument is DEVICE memory owned
+ * by the caller unless stated otherwise; nothing here allocates device memory.
+ * "tile layout" is the bilevel layout of the reference's kernels: a grid of
+ * shape s padded to a multiple of the tile shape s_i, stored tile after tile
+ * (index n_o * size_i + n_i), one plane after the other for multi-component
+ * fields (agd/FiniteDifferences.py:164-222, block_expand/block_squeeze).
+ * "grid layout" is plain row-major order over the true shape.
+ *
+ * All entry points enqueue work on `stream` and return an agd_status code
+ * (0 on success); agd_last_error() describes the last failure of this thread.
+ */
+#ifndef AGD_B200_H
+#define AGD_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+#if defined(__GNUC__)
+#pragma GCC visibility push(default) /* the library is built with hidden visibility */
+#endif
+
+typedef struct CUstream_st *agd_stream_t; /* a cudaStream_t */
+
+enum agd_status {
+    AGD_STATUS_OK = 0,
+    AGD_STATUS_INVALID = 1,       /* bad argument (shape, tile, pointer, size) */
+    AGD_STATUS_NOT_CONVERGED = 2, /* nitermax_o outer iterations reached */
+    AGD_STATUS_CUDA = 4,          /* CUDA runtime error */
+    AGD_STATUS_WATCHDOG = 8,      /* a bounded device-side wait timed out */
+    AGD_STATUS_WORKSPACE = 16,    /* workspace too small */
+    AGD_STATUS_UNSUPPORTED = 32   /* tile shape / model combination not built */
+};
+
+enum agd_model { AGD_MODEL_ISOTROPIC = 0, AGD_MODEL_RIEMANN = 1 };
+
+/* One eikonal problem.  Mirrors what the reference's Interface prepares for its
+ * `Update` kernel: traits (shape_i, niter_i, fim_front_width), module constants
+ * (shape_o/shape_tot, atol, rtol, isotropic weights, multip_step/multip_max) and
+ * kernel arguments (values, valuesq, geom, seedTags, rhs), see
+ * agd/Eikonal/HFM_CUDA/_Kernel.py:94-381 and cuda/Update.h:20-50. */
+typedef struct agd_instance {
+    int model;          /* enum agd_model */
+    int ndim;           /* 2 or 3 */
+    int shape[3];       /* grid shape */
+    int shape_i[3];     /* tile shape: (8,8), (16,16) in 2D; (4,4,4) in 3D */
+    int niter_i;        /* local iterations per tile visit */
+    int fim_front_width;/* FIM front width (>= 2) */
+    int nitermax_o;     /* maximum number of outer iterations */
+    int flags;          /* AGD_FLAG_* */
+    float atol, rtol;   /* per-point convergence: |du| <= atol + rtol |u| */
+    float iso_weights[3]; /* isotropic model: gridScale^-2 per axis */
+    float multip_step;  /* multiprecision: u + uq * multip_step (0: off) */
+    float multip_max;
+    float *values;      /* tile layout, in: initial values (+inf cold), out: solution */
+    int32_t *valuesq;   /* tile layout, multiprecision integer part (or NULL) */
+    const float *geom;  /* Riemann: dual metric, symdim planes, tile layout (else NULL) */
+    const float *rhs;   /* tile layout: cost, seed values at seeds, +inf padding */
+    const uint8_t *seedbits; /* tile layout bits, little endian, padding bits set */
+    const uint8_t *trigger;  /* per tile, nonzero = active at the first iteration
+                                (NULL: tiles holding a seed) */
+} agd_instance;
+
+#define AGD_FLAG_ACTIVATE_ALL 1 /* every tile is active at the first iteration */
+
+/* Per-instance results, written by the solver into device memory. */
+typedef struct agd_stats {
+    int32_t niter_o;      /* outer iterations (epochs) used by this instance */
+    int32_t status;       /* agd_status of this instance */
+    int64_t tile_visits;  /* tile visits; grid updates = tile_visits * size_i */
+} agd_stats;
+
+/* Solver tuning (0 = automatic). */
+typedef struct agd_launch {
+    int ctas;             /* persistent CTAs (<= co-resident maximum) */
+    int warps_per_cta;    /* 4 or 8 */
+    int64_t timeout_ns;   /* bound on any device-side wait (default 2 s) */
+} agd_launch;
+
+/* ---------------------------------------------------------------- eikonal -- */
+
+/* A plan holds, in host memory, the descriptors of n instances solved together
+ * and the layout of their workspace.  It replaces the reference's per-call
+ * setup of traits, module constants and kernel arguments
+ * (agd/Eikonal/HFM_CUDA/_Kernel.py:23-381).  inst: host array of n. */
+typedef struct agd_plan agd_plan;
+int agd_plan_create(const agd_instance *inst, int n, agd_plan **plan);
+void agd_plan_destroy(agd_plan *plan);
+
+/* Bytes of device workspace needed by the plan. */
+size_t agd_plan_workspace_bytes(const agd_plan *plan);
+
+/* Copies the plan's descriptors into the workspace (once per workspace). */
+int agd_plan_upload(const agd_plan *plan, void *workspace, size_t workspace_bytes, agd_stream_t stream);
+
+/* Solves the plan's instances in one persistent launch, from the values they
+ * hold (the fixed point of the reference's `Update` kernel, iterated as by
+ * `_solvers.fast_iterative_method`).  Only memsets and kernel launches are
+ * enqueued, so a run can be captured in a CUDA graph.
+ * Replaces: _solvers.Solve / fast_iterative_method / InitStop
+ * (agd/Eikonal/HFM_CUDA/_solvers.py:15-120, _StopCriterion.py:21-84) and the
+ * eikonal `Update` kernel (cuda/Update.h:20-227) they launch.
+ * stats: DEVICE array of n agd_stats (may be NULL).  Returns AGD_STATUS_OK
+ * once enqueued; per-instance convergence is in stats[i].status. */
+int agd_plan_run(const agd_plan *plan, void *workspace, size_t workspace_bytes, agd_stats *stats,
+                 const agd_launch *launch, agd_stream_t stream);
+
+/* One-shot form: plan, upload, run, destroy. */
+size_t agd_eikonal_workspace_bytes(const agd_instance *inst, int n);
+int agd_eikonal_solve(const agd_instance *inst, int n, void *workspace, size_t workspace_bytes,
+                      agd_stats *stats, const agd_launch *launch, agd_stream_t stream);
+
+/* ------------------------------------------------------------ preparation -- */
+
+/* Dual metric of metric.with_costs(gridScales) (or of dualMetric.with_speeds)
+ * in tile layout, padded with +inf.  Replaces the host code of
+ * _SetGeometry.SetGeometry (agd/Eikonal/HFM_CUDA/_SetGeometry.py:127-137,189-194).
+ * metric: grid layout, (*shape, symdim) HFM order [m00, m10, m11, (m20, m21, m22)];
+ * with broadcast != 0 a single (symdim,) tensor for the whole grid. */
+int agd_prep_geom(int ndim, const int *shape, const int *shape_i, const float *metric, int broadcast,
+                  int is_dual, const double *grid_scales, float *geom, agd_stream_t stream);
+
+/* Grid layout -> tile layout for `nplanes` planes, padding with `pad`
+ * (fd.block_expand).  src_broadcast != 0: src holds one value per plane. */
+int agd_block_expand(int ndim, const int *shape, const int *shape_i, int nplanes, const float *src,
+                     int src_broadcast, float pad, float *dst, agd_stream_t stream);
+
+/* Tile layout -> grid layout (fd.block_squeeze). */
+int agd_block_squeeze(int ndim, const int *shape, const int *shape_i, int nplanes, const float *src,
+                      float *dst, agd_stream_t stream);
+
+/* Seeds: sets rhs at the seed points to the seed values, writes the packed
+ * seed bits (padding bits set) and, if trigger != NULL, the per-tile trigger.
+ * seed_index: (n, ndim) int32 grid indices.  Replaces _SetArgs.SetRHS/SetArgs
+ * (agd/Eikonal/HFM_CUDA/_SetArgs.py:8-177) for rounded seeds. */
+int agd_prep_seeds(int ndim, const int *shape, const int *shape_i, const int32_t *seed_index,
+                   const float *seed_values, int n, float *rhs, uint8_t *seedbits, uint8_t *trigger,
+                   agd_stream_t stream);
+
+/* Selling decomposition of n packed symmetric matrices (symdim floats each):
+ * weights (n, symdim), integer offsets (n, symdim, ndim).  Same decomposition
+ * as the kernel's decomp_m (cuda/Geometry2.h:21-48, Geometry3.h:22-58). */
+int agd_selling(int ndim, const float *m, int n, float *weights, int32_t *offsets, agd_stream_t stream);
+
+/* ------------------------------------------------------------------- flow -- */
+
+/* Upwind geodesic flow of a solved instance, one pass over all tiles (the
+ * FLOW_* variant of the reference's `Update`, cuda/Update.h:171-209, run by
+ * _PostProcess.PostProcess, agd/Eikonal/HFM_CUDA/_PostProcess.py:46-95).
+ * Outputs, tile layout, any may be NULL: flow_vector (ndim planes),
+ * flow_weightsum, flow_weights (nact planes), flow_indices (nact planes, tile
+ * layout index of the upwind neighbour, INT32_MAX when the weight is zero). */
+int agd_flow(const agd_instance *inst, float *flow_vector, float *flow_weightsum, float *flow_weights,
+             int32_t *flow_indices, agd_stream_t stream);
+
+/* -------------------------------------------------------------- geodesics -- */
+
+/* Distance-to-seed map in 1/5 pixel units, saturated at 255, grid layout
+ * (inf_convolution with a 3^ndim kernel, ceil(target_tolerance) passes, cut
+ * beyond 5*target_tolerance: agd/Eikonal/HFM_CUDA/_GetGeodesics.py:51-75).
+ * seed_mask: grid layout uint8.  tmp: scratch of the same size. */
+int agd_eucl_map(int ndim, const int *shape, const uint8_t *seed_mask, int npasses, int cut,
+                 uint8_t *eucl, uint8_t *tmp, agd_stream_t stream);
+
+/* Geodesic backtracking, one thread per tip, with the reference's chunking
+ * (chunks of `typical_len` points restarting the stopping-criteria history,
+ * at most `max_chunks` chunks), midpoint rule, causality filtered multilinear
+ * flow and stop codes (0 Continue, 1 AtSeed, 2 InWall, 3 Stationnary,
+ * 4 PastSeed, 5 VanishingFlow).  Replaces GetGeodesics + GeodesicODE
+ * (_GetGeodesics.py:9-147, cuda/Kernel_GeodesicODE.h:265-412).
+ * tips: (ntips, ndim) continuous grid indices.  paths: (ntips, cap, ndim),
+ * with cap >= max_chunks*(typical_len-1)+1; lengths, stops: ntips entries. */
+int agd_geodesics(const agd_instance *inst, const float *flow_vector, const float *flow_weightsum,
+                  const uint8_t *eucl, const float *tips, int ntips, float step, float causality,
+                  int typical_len, int max_chunks, int eucl_delay, int nymin_delay, float *paths,
+                  int cap, int32_t *lengths, int8_t *stops, agd_stream_t stream);
+
+/* ---------------------------------------------------------------- adjoint -- */
+
+/* Workspace for agd_reverse. */
+size_t agd_reverse_workspace_bytes(const agd_instance *inst);
+
+/* Reverse-mode sensitivity: solves diag*lam - W^T lam = sens on the tiles, where
+ * W holds the upwind flow weights (flow_weights/flow_indices of agd_flow) and
+ * diag = flow_weightsum (1 where it vanishes).  sens, lam: tile layout.
+ * Replaces SolveAD's reverse branch, graph_reverse and the linear Update kernel
+ * (_PostProcess.py:97-219, graph_reverse.py:10-77, cuda/GraphReverse.h:35-82,
+ * cuda/Kernel_LinearUpdate.h:99-218). */
+int agd_reverse(const agd_instance *inst, const float *flow_weights, const int32_t *flow_indices,
+                const float *flow_weightsum, const float *sens, float *lam, float atol, float rtol,
+                void *workspace, size_t workspace_bytes, agd_stats *stats, const agd_launch *launch,
+                agd_stream_t stream);
+
+/* ------------------------------------------------------------------- misc -- */
+
+const char *agd_last_error(void);
+int agd_version(void);
+
+#if defined(__GNUC__)
+#pragma GCC visibility pop
+#endif
+#ifdef __cplusplus
+}
+#endif
+#endif /* AGD_B200_H */

@@ -34,3 +34,25 @@ CASES = ["iso2", "riem2", "riem2_aniso", "iso3", "riem3", "ad_notebook"]
 @pytest.fixture(params=CASES)
 def golden_case(request):
     return (request.param,) + load_case(request.param)
+
+
+def make_dictin(case, mode="gpu", extra=None):
+    """dictIn for the package under test from a golden-case dict."""
+    from adaptivegriddiscretizations_b200 import Eikonal
+    d = {"model": case["model"], "mode": mode, "arrayOrdering": "RowMajor", "verbosity": 0}
+    for k in ("dims", "gridScales", "origin", "seeds", "seedValues", "cost", "tips", "traits", "sensitivity"):
+        if k in case:
+            d[k] = case[k]
+    if "metric" in case:
+        d["metric"] = np.asarray(case["metric"], np.float32)
+    if extra:
+        d.update(extra)
+    return Eikonal.dictIn(d)
+
+
+def gpu_available():
+    try:
+        import torch
+        return torch.cuda.is_available()
+    except Exception:  # noqa: BLE001
+        return False

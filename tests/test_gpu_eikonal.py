@@ -1,0 +1,113 @@
+"""GPU parity of the eikonal solve through the public dictIn(...).Run() surface.
+
+Against: the golden outputs of the reference's own kernels (small cases), and
+the CPU oracle (float32 and float64) on larger seeded cases.  Float32 values
+must match within 1e-5 relative; offsets of Selling's decomposition bit-exact.
+"""
+import numpy as np
+import pytest
+import torch
+
+from conftest import CASES, GOLDEN, load_case, make_dictin
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+REL = 1e-5
+
+
+def _rel(a, b):
+    a, b = np.asarray(a, np.float64), np.asarray(b, np.float64)
+    fin = np.isfinite(b)
+    assert np.array_equal(fin, np.isfinite(a)), "finite masks differ"
+    return (np.abs(a[fin] - b[fin]) / np.maximum(np.abs(b[fin]), 1e-30)).max()
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_values_vs_reference(name):
+    case, ref = load_case(name)
+    case = {k: v for k, v in case.items() if k not in ("tips", "sensitivity")}
+    out = make_dictin(case, extra={"exportValues": True}).Run()
+    v = out["values"].cpu().numpy()
+    assert v.dtype == np.float32 and v.shape == ref["values"].shape
+    assert _rel(v, ref["values"]) < REL
+    st = out["stats"]["eikonal"]
+    assert st["niter_o"] > 0 and st["grid_updates"] > 0
+
+
+def _riemann2_case(n, seed, lam_max=50.0, nseeds=4):
+    from scipy.ndimage import gaussian_filter
+    rng = np.random.default_rng(seed)
+    g1 = gaussian_filter(rng.standard_normal((n, n)), n / 64, mode="wrap")
+    g2 = gaussian_filter(rng.standard_normal((n, n)), n / 64, mode="wrap")
+    th = np.arctan2(g1, g2)
+    lam = rng.uniform(1, lam_max, (n, n))
+    c, s = np.cos(th), np.sin(th)
+    m = np.stack([c * c + lam * s * s, c * s * (1 - lam), s * s + lam * c * c], -1).astype(np.float32)
+    return dict(model="Riemann2", dims=np.array([n, n], np.float32), gridScales=np.full(2, 1.0 / n, np.float32),
+                origin=np.zeros(2, np.float32), metric=m,
+                seeds=rng.uniform(0.1, 0.9, (nseeds, 2)).astype(np.float32))
+
+
+def _iso_case(shape, seed, nseeds=2):
+    from scipy.ndimage import gaussian_filter
+    rng = np.random.default_rng(seed)
+    g = gaussian_filter(rng.standard_normal(shape), 4.0, mode="wrap")
+    g = (g - g.mean()) / g.std()
+    nd = len(shape)
+    return dict(model=f"Isotropic{nd}", dims=np.array(shape, np.float32),
+                gridScales=np.full(nd, 1.0 / shape[0], np.float32), origin=np.zeros(nd, np.float32),
+                cost=np.exp(0.5 * g).astype(np.float32),
+                seeds=rng.uniform(0.1, 0.9, (nseeds, nd)).astype(np.float32) * np.array(shape) / shape[0])
+
+
+@pytest.mark.parametrize("make", [lambda: _riemann2_case(192, 5), lambda: _iso_case((200, 150), 6),
+                                  lambda: _iso_case((40, 36, 44), 7)], ids=["riem2_192", "iso2_200x150", "iso3_40"])
+def test_values_vs_oracle(make):
+    case = make()
+    out = make_dictin(case, extra={"exportValues": True}).Run()
+    v = out["values"].cpu().numpy()
+    r32 = O.run(case, np.float32, nthreads=8)
+    assert _rel(v, r32["values"]) < REL
+    r64 = O.run(case, np.float64, nthreads=8)
+    assert _rel(v, r64["values"]) < 2e-5  # float32 solution vs the float64 solution of the same scheme
+
+
+def test_gpu_transfer_mode():
+    case, ref = load_case("riem2")
+    case = {k: v for k, v in case.items() if k not in ("tips", "sensitivity")}
+    out = make_dictin(case, mode="gpu_transfer", extra={"exportValues": True}).Run()
+    assert isinstance(out["values"], np.ndarray)
+    assert _rel(out["values"], ref["values"]) < REL
+
+
+def test_keys_bookkeeping():
+    case, _ = load_case("iso2")
+    case = {k: v for k, v in case.items() if k not in ("tips", "sensitivity")}
+    out = make_dictin(case, extra={"exportValues": True, "someUnknownKey": 3}).Run()
+    keys = out["keys"]
+    assert "someUnknownKey" in keys["unused"]
+    assert "seeds" in keys["used"] and "nitermax_o" in keys["default"]
+    assert keys["default"]["nitermax_o"] == 2000
+
+
+def test_nonconvergence_raises():
+    case, _ = load_case("riem2")
+    case = {k: v for k, v in case.items() if k not in ("tips", "sensitivity")}
+    with pytest.raises(ValueError, match="did not reach convergence"):
+        make_dictin(case, extra={"nitermax_o": 2}).Run()
+    out = make_dictin(case, extra={"nitermax_o": 2, "raiseOnNonConvergence": False, "exportValues": True}).Run()
+    assert out["stats"]["eikonal"]["niter_o"] <= 3
+
+
+@pytest.mark.parametrize("nd", [2, 3])
+def test_selling_gpu_bitexact(nd):
+    import os
+    from adaptivegriddiscretizations_b200 import _lib
+    f = np.load(os.path.join(GOLDEN, f"selling{nd}.npz"))
+    m = torch.as_tensor(f["m"], device="cuda").contiguous()
+    n, sd = m.shape
+    w = torch.empty((n, sd), dtype=torch.float32, device="cuda")
+    e = torch.empty((n, sd, nd), dtype=torch.int32, device="cuda")
+    _lib.check(_lib.lib().agd_selling(nd, _lib.ptr(m), n, _lib.ptr(w), _lib.ptr(e), _lib.stream_ptr()))
+    assert np.array_equal(e.cpu().numpy(), f["ref_e"])
+    np.testing.assert_allclose(w.cpu().numpy(), f["ref_w"], rtol=2e-6, atol=0)
