@@ -1,9 +1,317 @@
-#include "agd_internal.h"
+// Reverse-mode sensitivity of the eikonal solution on B200.
+//
+// Linearising sum_k w_k (u - v_k)_+^2 = c^2 at the solution gives, at every
+// non-seed point x, diag(x) du(x) - sum_k fw_k(x) du(y_k(x)) = r(x), where
+// fw_k are the upwind flow weights, y_k(x) the upwind neighbours and diag the
+// weight sum (1 at seeds and outside the domain).  The reverse mode solves the
+// transposed system  diag(x) lam(x) - sum_{z: y_k(z) = x} fw_k(z) lam(z) = s(x)
+// (agd/Eikonal/HFM_CUDA/_PostProcess.py:155-219).
+//
+// The reference transposes the graph with an iterative claim loop relaunched
+// from the host (graph_reverse.py:10-77, cuda/GraphReverse.h:35-82) and solves
+// with the block Gauss-Seidel kernel of cuda/Kernel_LinearUpdate.h under the
+// adaptive Gauss-Seidel tile schedule.  Here: a counting-sort CSR transpose
+// (rows sorted, so sums are deterministic), then the tile scheduler of the
+// eikonal solver with a linear tile visit.  Every tile is visited at the first
+// epoch; afterwards a point whose value moved activates exactly the tiles of
+// the points that depend on it (its forward upwind neighbours), so
+// dependencies that skip over tiles are never missed.
+#include <cuda_runtime.h>
+
+#include "sched.cuh"
+
+namespace agd {
+
+// ------------------------------------------------------------ transpose ---
+struct RevGeom {
+    long long size_tot;
+    int nact;
+};
+
+__global__ void rev_count_kernel(RevGeom g, const float *fw, const int *fidx, int *count) {
+    const long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (n >= g.size_tot) return;
+    for (int k = 0; k < g.nact; ++k) {
+        const float w = fw[k * g.size_tot + n];
+        const int y = fidx[k * g.size_tot + n];
+        if (w != 0.f && y >= 0 && y < g.size_tot) atomicAdd(count + y, 1);
+    }
+}
+
+__global__ void rev_fill_kernel(RevGeom g, const float *fw, const int *fidx, const int *rowptr, int *cursor, int *src,
+                                float *wt) {
+    const long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (n >= g.size_tot) return;
+    for (int k = 0; k < g.nact; ++k) {
+        const float w = fw[k * g.size_tot + n];
+        const int y = fidx[k * g.size_tot + n];
+        if (w != 0.f && y >= 0 && y < g.size_tot) {
+            const int pos = rowptr[y] + atomicAdd(cursor + y, 1);
+            src[pos] = (int)n;
+            wt[pos] = w;
+        }
+    }
+}
+
+// Rows in increasing source order: the fill order depends on the schedule.
+__global__ void rev_sort_kernel(RevGeom g, const int *rowptr, int *src, float *wt) {
+    const long long y = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (y >= g.size_tot) return;
+    const int a = rowptr[y], b = rowptr[y + 1];
+    for (int i = a + 1; i < b; ++i) {
+        const int s = src[i];
+        const float w = wt[i];
+        int j = i - 1;
+        while (j >= a && src[j] > s) {
+            src[j + 1] = src[j];
+            wt[j + 1] = wt[j];
+            --j;
+        }
+        src[j + 1] = s;
+        wt[j + 1] = w;
+    }
+}
+
+// Exclusive scan of n ints in three passes (blocks of 1024, block totals, offsets).
+__device__ __forceinline__ int warp_incl_scan(int v, int lane) {
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int t = __shfl_up_sync(kFull, v, o);
+        if (lane >= o) v += t;
+    }
+    return v;
+}
+
+__device__ int block_excl_scan(int v, int *tot) {
+    __shared__ int ws[32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int inc = warp_incl_scan(v, lane);
+    if (lane == 31) ws[warp] = inc;
+    __syncthreads();
+    if (warp == 0) {
+        const int nw = blockDim.x >> 5;
+        int x = lane < nw ? ws[lane] : 0;
+        x = warp_incl_scan(x, lane);
+        if (lane < nw) ws[lane] = x;
+    }
+    __syncthreads();
+    const int off = warp > 0 ? ws[warp - 1] : 0;
+    if (tot) *tot = ws[(blockDim.x >> 5) - 1];
+    __syncthreads();
+    return off + inc - v;
+}
+
+__global__ void scan_blocks_kernel(const int *in, int *out, long long n, int *block_tot) {
+    const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    const int v = i < n ? in[i] : 0;
+    int tot;
+    const int ex = block_excl_scan(v, &tot);
+    if (i < n) out[i] = ex;
+    if (threadIdx.x == 0) block_tot[blockIdx.x] = tot;
+}
+
+__global__ void scan_totals_kernel(int *block_tot, int nb, int *grand) {
+    __shared__ int carry;
+    if (threadIdx.x == 0) carry = 0;
+    __syncthreads();
+    for (int base = 0; base < nb; base += blockDim.x) {
+        const int i = base + threadIdx.x;
+        const int v = i < nb ? block_tot[i] : 0;
+        int tot;
+        const int ex = block_excl_scan(v, &tot);
+        if (i < nb) block_tot[i] = ex + carry;
+        __syncthreads();
+        if (threadIdx.x == 0) carry += tot;
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) *grand = carry;
+}
+
+__global__ void scan_add_kernel(int *out, long long n, const int *block_off) {
+    const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (i < n) out[i] += block_off[blockIdx.x];
+}
+
+// ----------------------------------------------------------- linear visit ---
+struct LinArgs {
+    const int *rowptr, *src;
+    const float *wt;
+    const float *wsum, *sens;
+    float *lam;
+    const float *fw;
+    const int *fidx;
+    int nact;
+    float atol, rtol;
+};
+
+template <int SIZE>
+struct LinearVisitor {
+    static constexpr int P = SIZE / 32;
+    static constexpr int kMaxSweeps = 4 * SIZE;  // in-tile chains are shorter than the tile
+    using Args = LinArgs;
+    struct Smem {
+        float l[SIZE];
+    };
+
+    __device__ static void visit(const Sched &S, const Args &A, int t, int ii, int e, int lane, Smem &sm) {
+        const Inst &I = S.inst[ii];
+        const int n_o = t - I.tile_base;
+        const long long base = (long long)n_o * SIZE;
+        float old[P], diag[P], acc[P];
+        int r0[P], r1[P];
+#pragma unroll
+        for (int p = 0; p < P; ++p) {
+            const int n_i = lane + 32 * p;
+            const long long n_t = base + n_i;
+            old[p] = __ldcg(A.lam + n_t);
+            sm.l[n_i] = old[p];
+            const float d = __ldg(A.wsum + n_t);
+            diag[p] = d == 0.f ? 1.f : d;
+            float a = __ldg(A.sens + n_t);
+            r0[p] = __ldg(A.rowptr + n_t);
+            r1[p] = __ldg(A.rowptr + n_t + 1);
+            for (int j = r0[p]; j < r1[p]; ++j) {  // sources outside the tile: read once per visit
+                const int z = __ldg(A.src + j);
+                if ((long long)z / SIZE != n_o) a += __ldg(A.wt + j) * __ldcg(A.lam + z);
+            }
+            acc[p] = a;
+        }
+        __syncwarp();
+        bool settled = false;
+        for (int it = 0; it < kMaxSweeps; ++it) {
+            bool moved = false;
+#pragma unroll
+            for (int p = 0; p < P; ++p) {
+                const int n_i = lane + 32 * p;
+                float v = acc[p];
+                for (int j = r0[p]; j < r1[p]; ++j) {
+                    const int z = __ldg(A.src + j);
+                    if ((long long)z / SIZE == n_o) v += __ldg(A.wt + j) * sm.l[z - (int)base];
+                }
+                v = v / diag[p];
+                __syncwarp();
+                if (v != sm.l[n_i]) {
+                    sm.l[n_i] = v;
+                    moved = true;
+                }
+                __syncwarp();
+            }
+            if (!__any_sync(kFull, moved)) {
+                settled = true;
+                break;
+            }
+        }
+        bool self = !settled;
+#pragma unroll
+        for (int p = 0; p < P; ++p) {
+            const int n_i = lane + 32 * p;
+            const long long n_t = base + n_i;
+            const float v = sm.l[n_i];
+            __stcg(A.lam + n_t, v);
+            const bool changed = fabsf(v - old[p]) > A.atol + A.rtol * fabsf(v);
+            if (!changed) continue;
+            for (int k = 0; k < A.nact; ++k) {  // the points that depend on this one
+                const float w = __ldg(A.fw + k * I.size_tot + n_t);
+                const int y = __ldg(A.fidx + k * I.size_tot + n_t);
+                if (w == 0.f || y < 0 || (long long)y >= I.size_tot) continue;
+                const int ty = y / SIZE;
+                if (ty == n_o) self = true;
+                else push_tile(S, I, ii, I.tile_base + ty, e);
+            }
+        }
+        __syncwarp();
+        if (!settled && lane == 0) push_tile(S, I, ii, t, e);
+        (void)self;
+        if (lane == 0) atomicAdd((unsigned long long *)&S.stats[ii].tile_visits, 1ull);
+    }
+};
+
+static inline unsigned nb(long long n, int bs) { return (unsigned)((n + bs - 1) / bs); }
+
+struct RevLayout {
+    WsLayout L;
+    size_t rowptr, cursor, src, wt, btot, grand, total;
+    long long size_tot;
+    int nact, size_i;
+};
+
+static bool rev_layout(const agd_instance *a, RevLayout &R, std::vector<Inst> *insts) {
+    agd_instance b = *a;
+    b.flags |= AGD_FLAG_ACTIVATE_ALL;
+    b.trigger = nullptr;
+    if (!layout(&b, 1, R.L, insts)) return false;
+    const Inst &I = (*insts)[0];
+    R.size_tot = I.size_tot;
+    R.size_i = I.size_i;
+    R.nact = a->model == AGD_MODEL_RIEMANN ? a->ndim * (a->ndim + 1) / 2 : a->ndim;
+    size_t off = R.L.total;
+    const long long nblk = (R.size_tot + 1 + 1023) / 1024;
+    R.rowptr = off; off = align256(off + sizeof(int) * (R.size_tot + 1));
+    R.cursor = off; off = align256(off + sizeof(int) * R.size_tot);
+    R.src = off; off = align256(off + sizeof(int) * R.nact * R.size_tot);
+    R.wt = off; off = align256(off + sizeof(float) * R.nact * R.size_tot);
+    R.btot = off; off = align256(off + sizeof(int) * nblk);
+    R.grand = off; off = align256(off + sizeof(int));
+    R.total = off;
+    return true;
+}
+
+}  // namespace agd
+
 using namespace agd;
+
 extern "C" {
-size_t agd_reverse_workspace_bytes(const agd_instance *) { return 0; }
-int agd_reverse(const agd_instance *, const float *, const int32_t *, const float *, const float *, float *, float,
-                float, void *, size_t, agd_stats *, const agd_launch *, agd_stream_t) {
-    return set_error(AGD_STATUS_UNSUPPORTED, "not built");
+
+size_t agd_reverse_workspace_bytes(const agd_instance *inst) {
+    if (!inst) return 0;
+    RevLayout R;
+    std::vector<Inst> v;
+    if (!rev_layout(inst, R, &v)) return 0;
+    return R.total;
 }
+
+int agd_reverse(const agd_instance *inst, const float *flow_weights, const int32_t *flow_indices,
+                const float *flow_weightsum, const float *sens, float *lam, float atol, float rtol, void *workspace,
+                size_t workspace_bytes, agd_stats *stats, const agd_launch *launch, agd_stream_t stream) {
+    clear_error();
+    if (!inst || !flow_weights || !flow_indices || !flow_weightsum || !sens || !lam || !workspace)
+        return set_error(AGD_STATUS_INVALID, "agd_reverse: missing array");
+    RevLayout R;
+    std::vector<Inst> insts;
+    if (!rev_layout(inst, R, &insts)) return set_error(AGD_STATUS_INVALID, "agd_reverse: bad instance");
+    if (insts[0].variant < 0) return set_error(AGD_STATUS_UNSUPPORTED, "agd_reverse: tile shape not built");
+    if (workspace_bytes < R.total) return set_error(AGD_STATUS_WORKSPACE, "agd_reverse: workspace too small");
+    cudaStream_t st = (cudaStream_t)stream;
+    char *w = static_cast<char *>(workspace);
+    int *rowptr = reinterpret_cast<int *>(w + R.rowptr);
+    int *cursor = reinterpret_cast<int *>(w + R.cursor);
+    int *src = reinterpret_cast<int *>(w + R.src);
+    float *wt = reinterpret_cast<float *>(w + R.wt);
+    int *btot = reinterpret_cast<int *>(w + R.btot);
+    int *grand = reinterpret_cast<int *>(w + R.grand);
+    RevGeom g{R.size_tot, R.nact};
+    cudaError_t err = cudaMemsetAsync(cursor, 0, sizeof(int) * R.size_tot, st);
+    if (err == cudaSuccess) err = cudaMemsetAsync(lam, 0, sizeof(float) * R.size_tot, st);
+    if (err != cudaSuccess) return set_cuda_error("reverse clear", err);
+    // counts (into cursor), exclusive scan into rowptr, then fill
+    rev_count_kernel<<<nb(R.size_tot, 256), 256, 0, st>>>(g, flow_weights, flow_indices, cursor);
+    const long long n1 = R.size_tot + 1;
+    cudaMemsetAsync(rowptr + R.size_tot, 0, sizeof(int), st);
+    scan_blocks_kernel<<<nb(n1, 1024), 1024, 0, st>>>(cursor, rowptr, R.size_tot, btot);
+    scan_totals_kernel<<<1, 1024, 0, st>>>(btot, (int)nb(n1, 1024), grand);
+    scan_add_kernel<<<nb(n1, 1024), 1024, 0, st>>>(rowptr, R.size_tot, btot);
+    cudaMemcpyAsync(rowptr + R.size_tot, grand, sizeof(int), cudaMemcpyDeviceToDevice, st);
+    cudaMemsetAsync(cursor, 0, sizeof(int) * R.size_tot, st);
+    rev_fill_kernel<<<nb(R.size_tot, 256), 256, 0, st>>>(g, flow_weights, flow_indices, rowptr, cursor, src, wt);
+    rev_sort_kernel<<<nb(R.size_tot, 256), 256, 0, st>>>(g, rowptr, src, wt);
+    if ((err = cudaGetLastError()) != cudaSuccess) return set_cuda_error("reverse transpose", err);
+    // solve on the tiles
+    err = cudaMemcpyAsync(w + R.L.inst, insts.data(), sizeof(Inst), cudaMemcpyHostToDevice, st);
+    if (err != cudaSuccess) return set_cuda_error("reverse descriptor upload", err);
+    LinArgs A{rowptr, src, wt, flow_weightsum, sens, lam, flow_weights, flow_indices, R.nact, atol, rtol};
+    if (R.size_i == 256) return run_sched<LinearVisitor<256>>(R.L, workspace, 1, A, stats, launch, st);
+    if (R.size_i == 64) return run_sched<LinearVisitor<64>>(R.L, workspace, 1, A, stats, launch, st);
+    return set_error(AGD_STATUS_UNSUPPORTED, "agd_reverse: tile size not built");
 }
+
+}  // extern "C"

@@ -4,13 +4,16 @@
 // Scheduling.  The reference iterates on the host: every outer iteration it
 // compacts the flags of the tiles to update (cp.flatnonzero), tests for
 // termination (np.any, a device->host sync) and launches `Update` on the
-// active tiles (agd/Eikonal/HFM_CUDA/_solvers.py:94-120).  Here one
-// cooperative launch runs all outer iterations ("epochs"): the active tiles of
-// epoch e sit in a device list; warps take tiles from it, and a tile that must
-// be visited at epoch e+1 is appended to the next list the first time it is
-// tagged (dedupe by an epoch-stamped flag).  A bounded software grid barrier
-// separates epochs.  Fast-iterative-method scores (cuda/Propagation.h:103-167)
-// are epoch-stamped too, so no per-epoch clearing pass is needed.
+// active tiles (agd/Eikonal/HFM_CUDA/_solvers.py:94-120).  Here one launch of
+// resident worker warps runs all outer iterations ("epochs") of all the
+// instances of a plan, with no grid-wide barrier: tiles wait in one global
+// device queue as (tile, epoch) entries; a visit appends the tiles to revisit
+// at the next epoch to its instance's next list (deduplicated by an
+// epoch-stamped flag), and the warp that finishes the last tile of an
+// instance's epoch publishes that instance's next list to the queue.  Each
+// instance therefore follows the reference's epoch semantics exactly (the
+// fast-iterative-method scores of cuda/Propagation.h:103-167 are
+// epoch-stamped, per instance), while instances never wait for one another.
 //
 // Tile visit.  One warp per tile (points n_i = lane + 32 p), tile values in
 // shared memory, niter_i local sweeps with __syncwarp between phases, and an
@@ -25,104 +28,9 @@
 #include <cstring>
 #include <vector>
 
-#include "agd_common.cuh"
-#include "agd_internal.h"
+#include "sched.cuh"
 
 namespace agd {
-
-// ------------------------------------------------------------- variants ---
-enum Variant { V_ISO2_8 = 0, V_ISO2_16, V_RIEM2_8, V_ISO3_4, V_RIEM3_4, V_COUNT };
-
-int variant_of(const agd_instance &a) {
-    if (a.ndim == 2) {
-        if (a.model == AGD_MODEL_RIEMANN && a.shape_i[0] == 8 && a.shape_i[1] == 8) return V_RIEM2_8;
-        if (a.model == AGD_MODEL_ISOTROPIC && a.shape_i[0] == 8 && a.shape_i[1] == 8) return V_ISO2_8;
-        if (a.model == AGD_MODEL_ISOTROPIC && a.shape_i[0] == 16 && a.shape_i[1] == 16) return V_ISO2_16;
-    } else if (a.ndim == 3 && a.shape_i[0] == 4 && a.shape_i[1] == 4 && a.shape_i[2] == 4) {
-        return a.model == AGD_MODEL_RIEMANN ? V_RIEM3_4 : V_ISO3_4;
-    }
-    return -1;
-}
-
-struct Ctrl {
-    unsigned int cnt[3];  // list lengths, rotating: epoch e reads cnt[e%3], fills cnt[(e+1)%3]
-    unsigned int err;
-    GridBarrier bar;
-    unsigned int epochs;  // last epoch run
-};
-
-// Workspace: [Inst x n][tile_inst][list0][list1][flags][score0][score1][Ctrl][stats x n]
-struct WsLayout {
-    size_t inst, tile_inst, list0, list1, flags, score0, score1, ctrl, stats, total;
-    int total_tiles;
-};
-
-static size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
-
-static bool layout(const agd_instance *a, int n, WsLayout &L, std::vector<Inst> *out) {
-    long long tiles = 0;
-    if (out) out->resize(n);
-    for (int i = 0; i < n; ++i) {
-        Inst I;
-        std::memset(&I, 0, sizeof(I));
-        I.a = a[i];
-        I.size_o = 1;
-        for (int k = 0; k < a[i].ndim; ++k) {
-            if (a[i].shape[k] <= 0 || a[i].shape_i[k] <= 0) return false;
-            I.shape_o[k] = (a[i].shape[k] + a[i].shape_i[k] - 1) / a[i].shape_i[k];
-            I.size_o *= I.shape_o[k];
-        }
-        I.size_i = 1;
-        for (int k = 0; k < a[i].ndim; ++k) I.size_i *= a[i].shape_i[k];
-        I.size_tot = (long long)I.size_o * I.size_i;
-        I.tile_base = (int)tiles;
-        I.variant = variant_of(a[i]);
-        tiles += I.size_o;
-        if (tiles > 0x3fffffff) return false;
-        if (out) (*out)[i] = I;
-    }
-    size_t off = 0;
-    L.inst = off; off = align256(off + sizeof(Inst) * n);
-    L.tile_inst = off; off = align256(off + sizeof(int) * tiles);
-    L.list0 = off; off = align256(off + sizeof(int) * tiles);
-    L.list1 = off; off = align256(off + sizeof(int) * tiles);
-    L.flags = off; off = align256(off + sizeof(unsigned) * tiles);
-    L.score0 = off; off = align256(off + sizeof(unsigned) * tiles);
-    L.score1 = off; off = align256(off + sizeof(unsigned) * tiles);
-    L.ctrl = off; off = align256(off + sizeof(Ctrl));
-    L.stats = off; off = align256(off + sizeof(agd_stats) * n);
-    L.total = off;
-    L.total_tiles = (int)tiles;
-    return true;
-}
-
-// --------------------------------------------------------- kernel context ---
-struct Sched {
-    const Inst *inst;
-    const int *tile_inst;
-    int *list0, *list1;
-    unsigned *flags, *score0, *score1;
-    Ctrl *ctrl;
-    agd_stats *stats;
-    int max_epochs;
-    unsigned long long timeout_ns;
-};
-
-__device__ __forceinline__ void push_tile(const Sched &S, int t, int e) {
-    const unsigned tag = (unsigned)(e + 1);
-    if (atomicMax(&S.flags[t], tag) < tag) {
-        int *nxt = (e & 1) ? S.list0 : S.list1;  // epoch e+1 reads list[(e+1)&1]
-        const unsigned idx = atomicAdd(&S.ctrl->cnt[(e + 1) % 3], 1u);
-        nxt[idx] = t;
-    }
-}
-
-__device__ __forceinline__ unsigned score_at(const Sched &S, int t, int e) {
-    // Score written at epoch e (0 if the tile was not visited at epoch e).
-    const unsigned *arr = (e & 1) ? S.score1 : S.score0;
-    const unsigned w = __ldcg(arr + t);
-    return (int)(w >> 8) == e ? (w & 0xffu) : 0u;
-}
 
 // ------------------------------------------------------------- tile visit ---
 template <class TL, int MODEL>
@@ -274,7 +182,7 @@ struct Visit {
             else { sn = front; prop = true; }
         } else {
             sn = 1;
-            if (lane == 0) push_tile(S, t, e);
+            if (lane == 0) push_tile(S, I, ii, t, e);
             if (front > 2) {
                 const int sq = nb >= 0 ? (int)score_at(S, nb, e - 1) - 1 : -1;
                 int mx = sq;
@@ -288,9 +196,8 @@ struct Visit {
             unsigned *arr = (e & 1) ? S.score1 : S.score0;
             __stcg(arr + t, ((unsigned)e << 8) | (unsigned)sn);
             atomicAdd((unsigned long long *)&S.stats[ii].tile_visits, 1ull);
-            atomicMax(&S.stats[ii].niter_o, e);
         }
-        if (prop && nb >= 0) push_tile(S, nb, e);
+        if (prop && nb >= 0) push_tile(S, I, ii, nb, e);
     }
 };
 
@@ -298,10 +205,6 @@ template <unsigned VMASK>
 __device__ __forceinline__ void dispatch(const Sched &S, int t, int e, int lane, float *us) {
     const int ii = __ldg(S.tile_inst + t);
     const Inst &I = S.inst[ii];
-    if (e > I.a.nitermax_o) {
-        if (lane == 0) atomicOr(&S.stats[ii].status, (int)AGD_STATUS_NOT_CONVERGED);
-        return;
-    }
     const int n_o = t - I.tile_base;
     switch (I.variant) {
         case V_ISO2_8:
@@ -326,103 +229,16 @@ __device__ __forceinline__ void dispatch(const Sched &S, int t, int e, int lane,
 
 constexpr int kMaxTileSize = 256;
 
-template <unsigned VMASK, int WPB>
-__global__ void __launch_bounds__(WPB * 32) eikonal_persistent(Sched S) {
-    __shared__ float s_u[WPB][kMaxTileSize];
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int nw = gridDim.x * WPB;
-    const int gw = blockIdx.x * WPB + warp;
-    int e = 1;
-    for (; e <= S.max_epochs; ++e) {
-        const unsigned ncur = ld_acquire(&S.ctrl->cnt[e % 3]);
-        if (ncur == 0) break;
-        if (blockIdx.x == 0 && threadIdx.x == 0) S.ctrl->cnt[(e + 2) % 3] = 0;
-        const int *cur = (e & 1) ? S.list1 : S.list0;
-        for (unsigned i = gw; i < ncur; i += nw) {
-            const int t = __ldcg(cur + i);
-            dispatch<VMASK>(S, t, e, lane, s_u[warp]);
-        }
-        if (!grid_barrier(&S.ctrl->bar, gridDim.x, &S.ctrl->err, S.timeout_ns)) return;
+template <unsigned VMASK>
+struct EikonalVisitor {
+    struct Args {};
+    struct Smem {
+        float u[kMaxTileSize];
+    };
+    __device__ __forceinline__ static void visit(const Sched &S, const Args &, int t, int, int e, int lane, Smem &sm) {
+        dispatch<VMASK>(S, t, e, lane, sm.u);
     }
-    if (blockIdx.x == 0) {
-        // Tiles still listed when the epoch budget ran out belong to unconverged instances.
-        const unsigned nleft = (e > S.max_epochs) ? ld_acquire(&S.ctrl->cnt[e % 3]) : 0u;
-        const int *cur = (e & 1) ? S.list1 : S.list0;
-        for (unsigned i = threadIdx.x; i < nleft; i += blockDim.x) {
-            const int ii = __ldg(S.tile_inst + __ldcg(cur + i));
-            atomicOr(&S.stats[ii].status, (int)AGD_STATUS_NOT_CONVERGED);
-        }
-        if (threadIdx.x == 0) S.ctrl->epochs = (unsigned)(e - 1);
-    }
-}
-
-// ---------------------------------------------------------------- setup ---
-// tile -> instance map, and the first list: tiles flagged by `trigger`, by
-// ACTIVATE_ALL, or holding a seed point inside the domain.
-__global__ void setup_tiles(Sched S, int ninst) {
-    const int t = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
-    const int lane = threadIdx.x & 31;
-    // locate the instance by bisection over the tile bases
-    int lo = 0, hi = ninst - 1;
-    while (lo < hi) {
-        const int mid = (lo + hi + 1) >> 1;
-        if (S.inst[mid].tile_base <= t) lo = mid; else hi = mid - 1;
-    }
-    const Inst &I = S.inst[lo];
-    if (t >= I.tile_base + I.size_o) return;  // past the last tile
-    const int n_o = t - I.tile_base;
-    if (lane == 0) const_cast<int *>(S.tile_inst)[t] = lo;
-    bool active = (I.a.flags & AGD_FLAG_ACTIVATE_ALL) != 0;
-    if (I.a.trigger) {
-        active = active || I.a.trigger[n_o] != 0;
-    } else if (!active) {
-        int xo[3], r = n_o;
-        for (int k = I.a.ndim - 1; k >= 0; --k) { xo[k] = r % I.shape_o[k]; r /= I.shape_o[k]; }
-        bool any = false;
-        for (int n_i = lane; n_i < I.size_i; n_i += 32) {
-            int xi[3], q = n_i;
-            for (int k = I.a.ndim - 1; k >= 0; --k) { xi[k] = q % I.a.shape_i[k]; q /= I.a.shape_i[k]; }
-            bool in = true;
-            for (int k = 0; k < I.a.ndim; ++k) in = in && (xo[k] * I.a.shape_i[k] + xi[k] < I.a.shape[k]);
-            const size_t n_t = (size_t)n_o * I.size_i + n_i;
-            if (in && ((I.a.seedbits[n_t >> 3] >> (n_t & 7)) & 1)) any = true;
-        }
-        active = __any_sync(kFull, any);
-    }
-    if (active && lane == 0) {
-        S.flags[t] = 1u;
-        const unsigned idx = atomicAdd(&S.ctrl->cnt[1], 1u);
-        S.list1[idx] = t;
-    }
-}
-
-__global__ void finish_stats(Sched S, int ninst, agd_stats *out) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= ninst) return;
-    agd_stats st = S.stats[i];
-    st.status |= (int)S.ctrl->err;
-    if (out) out[i] = st;
-}
-
-// --------------------------------------------------------------- launch ---
-template <unsigned VMASK, int WPB>
-static int launch_persistent(const Sched &S, int total_tiles, const agd_launch *cfg, cudaStream_t st) {
-    auto kern = eikonal_persistent<VMASK, WPB>;
-    int dev = 0, nsm = 0, per_sm = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess) return set_cuda_error("cudaGetDevice");
-    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, WPB * 32, 0) != cudaSuccess)
-        return set_cuda_error("occupancy query");
-    if (per_sm < 1) return set_error(AGD_STATUS_UNSUPPORTED, "persistent kernel does not fit on an SM");
-    const int max_ctas = per_sm * nsm;
-    int ctas = cfg && cfg->ctas > 0 ? cfg->ctas : (total_tiles + 4 * WPB - 1) / (4 * WPB);
-    ctas = std::max(1, std::min(ctas, max_ctas));
-    Sched s = S;
-    void *args[] = {&s};
-    const cudaError_t err = cudaLaunchCooperativeKernel((const void *)kern, dim3(ctas), dim3(WPB * 32), args, 0, st);
-    if (err != cudaSuccess) return set_cuda_error("cooperative launch", err);
-    return AGD_STATUS_OK;
-}
+};
 
 }  // namespace agd
 
@@ -431,7 +247,6 @@ struct agd_plan {
     agd::WsLayout L;
     unsigned vmask;
     int ndim;
-    int max_epochs;
 };
 
 namespace agd {
@@ -447,7 +262,6 @@ static int plan_create(const agd_instance *host, int n, agd_plan **out) {
     }
     P->ndim = host[0].ndim;
     P->vmask = 0;
-    P->max_epochs = 0;
     for (int i = 0; i < n; ++i) {
         const agd_instance &a = host[i];
         const char *bad = nullptr;
@@ -463,28 +277,9 @@ static int plan_create(const agd_instance *host, int n, agd_plan **out) {
             return set_error(code, bad);
         }
         P->vmask |= 1u << P->insts[i].variant;
-        P->max_epochs = std::max(P->max_epochs, a.nitermax_o);
     }
     *out = P;
     return AGD_STATUS_OK;
-}
-
-static Sched sched_of(const agd_plan *P, void *ws) {
-    const WsLayout &L = P->L;
-    char *w = static_cast<char *>(ws);
-    Sched S;
-    S.inst = reinterpret_cast<const Inst *>(w + L.inst);
-    S.tile_inst = reinterpret_cast<const int *>(w + L.tile_inst);
-    S.list0 = reinterpret_cast<int *>(w + L.list0);
-    S.list1 = reinterpret_cast<int *>(w + L.list1);
-    S.flags = reinterpret_cast<unsigned *>(w + L.flags);
-    S.score0 = reinterpret_cast<unsigned *>(w + L.score0);
-    S.score1 = reinterpret_cast<unsigned *>(w + L.score1);
-    S.ctrl = reinterpret_cast<Ctrl *>(w + L.ctrl);
-    S.stats = reinterpret_cast<agd_stats *>(w + L.stats);
-    S.max_epochs = P->max_epochs + 1;  // one extra epoch detects an instance exceeding its budget
-    S.timeout_ns = 2000000000ull;
-    return S;
 }
 
 static int plan_run(const agd_plan *P, void *ws, size_t ws_bytes, agd_stats *stats, const agd_launch *cfg,
@@ -493,38 +288,18 @@ static int plan_run(const agd_plan *P, void *ws, size_t ws_bytes, agd_stats *sta
     const WsLayout &L = P->L;
     if (ws_bytes < L.total) return set_error(AGD_STATUS_WORKSPACE, "workspace too small");
     const int n = (int)P->insts.size();
-    Sched S = sched_of(P, ws);
-    if (cfg && cfg->timeout_ns > 0) S.timeout_ns = (unsigned long long)cfg->timeout_ns;
-    char *w = static_cast<char *>(ws);
-    cudaError_t err = cudaMemsetAsync(w + L.flags, 0, L.ctrl - L.flags + sizeof(Ctrl), st);
-    if (err != cudaSuccess) return set_cuda_error("workspace clear", err);
-    err = cudaMemsetAsync(w + L.stats, 0, sizeof(agd_stats) * n, st);
-    if (err != cudaSuccess) return set_cuda_error("stats clear", err);
-    {
-        const int wpb = 8;
-        setup_tiles<<<(L.total_tiles + wpb - 1) / wpb, wpb * 32, 0, st>>>(S, n);
-        if ((err = cudaGetLastError()) != cudaSuccess) return set_cuda_error("setup_tiles", err);
-    }
-    int rc;
     const unsigned vmask = P->vmask;
-    const int wpb = (cfg && cfg->warps_per_cta == 8) ? 8 : 4;
-#define AGD_LAUNCH(M) (wpb == 8 ? launch_persistent<(M), 8>(S, L.total_tiles, cfg, st) \
-                                : launch_persistent<(M), 4>(S, L.total_tiles, cfg, st))
+    constexpr unsigned R2 = 1u << V_RIEM2_8, I16 = 1u << V_ISO2_16, I8 = 1u << V_ISO2_8;
+    constexpr unsigned R3 = 1u << V_RIEM3_4, I3 = 1u << V_ISO3_4;
     if (P->ndim == 2) {
-        if (vmask == (1u << V_RIEM2_8)) rc = AGD_LAUNCH(1u << V_RIEM2_8);
-        else if (vmask == (1u << V_ISO2_16)) rc = AGD_LAUNCH(1u << V_ISO2_16);
-        else if (vmask == (1u << V_ISO2_8)) rc = AGD_LAUNCH(1u << V_ISO2_8);
-        else rc = AGD_LAUNCH((1u << V_ISO2_8) | (1u << V_ISO2_16) | (1u << V_RIEM2_8));
-    } else {
-        if (vmask == (1u << V_RIEM3_4)) rc = AGD_LAUNCH(1u << V_RIEM3_4);
-        else if (vmask == (1u << V_ISO3_4)) rc = AGD_LAUNCH(1u << V_ISO3_4);
-        else rc = AGD_LAUNCH((1u << V_ISO3_4) | (1u << V_RIEM3_4));
+        if (vmask == R2) return run_sched<EikonalVisitor<R2>>(L, ws, n, {}, stats, cfg, st);
+        if (vmask == I16) return run_sched<EikonalVisitor<I16>>(L, ws, n, {}, stats, cfg, st);
+        if (vmask == I8) return run_sched<EikonalVisitor<I8>>(L, ws, n, {}, stats, cfg, st);
+        return run_sched<EikonalVisitor<R2 | I16 | I8>>(L, ws, n, {}, stats, cfg, st);
     }
-#undef AGD_LAUNCH
-    if (rc != AGD_STATUS_OK) return rc;
-    finish_stats<<<(n + 127) / 128, 128, 0, st>>>(S, n, stats);
-    if ((err = cudaGetLastError()) != cudaSuccess) return set_cuda_error("finish_stats", err);
-    return AGD_STATUS_OK;
+    if (vmask == R3) return run_sched<EikonalVisitor<R3>>(L, ws, n, {}, stats, cfg, st);
+    if (vmask == I3) return run_sched<EikonalVisitor<I3>>(L, ws, n, {}, stats, cfg, st);
+    return run_sched<EikonalVisitor<R3 | I3>>(L, ws, n, {}, stats, cfg, st);
 }
 
 static int plan_upload(const agd_plan *P, void *ws, size_t ws_bytes, cudaStream_t st) {

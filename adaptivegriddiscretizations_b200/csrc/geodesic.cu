@@ -1,11 +1,317 @@
+// Geodesic backtracking on B200: the distance-to-seed map used by the stopping
+// criteria, and the midpoint ODE on the upwind flow, one thread per tip.
+//
+// The reference runs its GeodesicODE kernel in chunks of `typical_len` steps
+// and restarts each unfinished geodesic from its last point on the host
+// (agd/Eikonal/HFM_CUDA/_GetGeodesics.py:111-134).  Here a thread runs all of
+// its chunks in one launch; a chunk boundary resets the same state the
+// reference's restart resets (stopping-criteria history, cell cache), so the
+// paths are the reference's.  The stepping follows
+// cuda/Kernel_GeodesicODE.h:164-412 with the precomputed flow of
+// GeodesicODE_Opt.h:236-245, in float.
+#include <cuda_runtime.h>
+
+#include <vector>
+
+#include "agd_common.cuh"
 #include "agd_internal.h"
+
+namespace agd {
+
+// ------------------------------------------------------ distance to seeds ---
+struct EGeo {
+    int nd, shape[3];
+    long long n;
+};
+
+// One min-plus pass: out(x) = min over the 3^d neighbours y of min(255, in(y) + k(y - x)),
+// k = round(5 |y - x|) (inf_convolution with distance_kernel(1, ndim, uint8, mult=5)).
+__global__ void infconv_kernel(EGeo g, const uint8_t *in, uint8_t *out) {
+    const long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (p >= g.n) return;
+    int x[3] = {0, 0, 0};
+    long long r = p;
+    for (int k = g.nd - 1; k >= 0; --k) { x[k] = (int)(r % g.shape[k]); r /= g.shape[k]; }
+    const int nk = g.nd == 2 ? 9 : 27;
+    int best = 255;
+    for (int ic = 0; ic < nk; ++ic) {
+        int y[3] = {0, 0, 0}, q = ic, n2 = 0;
+        bool ok = true;
+        for (int k = g.nd - 1; k >= 0; --k) {
+            const int o = q % 3 - 1;
+            q /= 3;
+            y[k] = x[k] + o;
+            n2 += o * o;
+            ok = ok && y[k] >= 0 && y[k] < g.shape[k];
+        }
+        if (!ok) continue;
+        long long m = 0;
+        for (int k = 0; k < g.nd; ++k) m = m * g.shape[k] + y[k];
+        const int kv = n2 == 0 ? 0 : (n2 == 1 ? 5 : (n2 == 2 ? 7 : 9));  // round(5 sqrt(n2))
+        const int a = in[m];
+        best = min(best, (a >= 255 - kv) ? 255 : a + kv);
+    }
+    out[p] = (uint8_t)best;
+}
+
+__global__ void eucl_init_kernel(EGeo g, const uint8_t *mask, uint8_t *out) {
+    const long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (p < g.n) out[p] = mask[p] ? 0 : 255;
+}
+
+__global__ void eucl_cut_kernel(EGeo g, const uint8_t *in, int cut, uint8_t *out) {
+    const long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (p < g.n) out[p] = in[p] > cut ? 255 : in[p];
+}
+
+// ------------------------------------------------------------ geodesics ---
+enum { kContinue = 0, kAtSeed, kInWall, kStationnary, kPastSeed, kVanishingFlow };
+
+struct GeoArgs {
+    int nd;
+    int shape[3], shape_i[3], shape_o[3];
+    int size_i;
+    long long size_tot;
+    const float *u, *fvec, *fwsum;
+    const uint8_t *eucl;
+    const float *tips;
+    int ntips;
+    float step, causality;
+    int typical_len, max_chunks, eucl_delay, nymin_delay;
+    float *paths;
+    int cap;
+    int *lengths;
+    int8_t *stops;
+};
+
+constexpr int kMaxHist = 256;  // bound on 1 + max(eucl_delay, nymin_delay)
+
+template <int D>
+struct Walker {
+    static constexpr int NC = 1 << D;
+    const GeoArgs &A;
+    int xq[D];
+    long long nymin;     // bilevel index of the retained corner
+    long long nymin_grid;
+    float thr;
+    float flow_c[NC][D], dist_c[NC], wsum_c[NC];
+
+    __device__ Walker(const GeoArgs &a) : A(a) { reset(); }
+    __device__ void reset() {
+        for (int k = 0; k < D; ++k) xq[k] = kIntMax;
+        nymin = kIntMax;
+        nymin_grid = kIntMax;
+        thr = 0.f;
+    }
+    __device__ bool inside(const int *y) const {
+        for (int k = 0; k < D; ++k)
+            if (y[k] < 0 || y[k] >= A.shape[k]) return false;
+        return true;
+    }
+    __device__ long long bilevel(const int *y) const {
+        long long n_o = 0, n_i = 0;
+        for (int k = 0; k < D; ++k) {
+            n_o = n_o * A.shape_o[k] + y[k] / A.shape_i[k];
+            n_i = n_i * A.shape_i[k] + y[k] % A.shape_i[k];
+        }
+        return n_o * A.size_i + n_i;
+    }
+    __device__ long long gridindex(const int *y) const {
+        long long n = 0;
+        for (int k = 0; k < D; ++k) n = n * A.shape[k] + y[k];
+        return n;
+    }
+    // Kernel_GeodesicODE.h:164-260 (NormalizedFlow)
+    __device__ int normalized_flow(const float *x, float *flow) {
+        bool newcell = false;
+        for (int k = 0; k < D; ++k) {
+            const int q = (int)floorf(x[k]);
+            if (q != xq[k]) newcell = true;
+            xq[k] = q;
+        }
+        float dx[D], wts[NC];
+        for (int k = 0; k < D; ++k) dx[k] = x[k] - (float)xq[k];
+        for (int i = 0; i < NC; ++i) {
+            float w = 1.f;
+            for (int k = 0; k < D; ++k) w *= ((i >> k) & 1) ? dx[k] : 1.f - dx[k];
+            wts[i] = w;
+        }
+        if (newcell) {
+            for (int i = 0; i < NC; ++i) {
+                int y[D];
+                for (int k = 0; k < D; ++k) y[k] = xq[k] + ((i >> k) & 1);
+                if (!inside(y)) {
+                    dist_c[i] = finf();
+                    continue;
+                }
+                const long long n = bilevel(y);
+                dist_c[i] = __ldg(A.u + n);
+                wsum_c[i] = __ldg(A.fwsum + n);
+                for (int k = 0; k < D; ++k) flow_c[i][k] = __ldg(A.fvec + k * A.size_tot + n);
+            }
+            float dmin = finf();
+            int imin = 0;
+            const float wthr = 0.5f / NC;
+            for (int i = 0; i < NC; ++i) {
+                if (wts[i] < wthr) continue;
+                if (dist_c[i] < dmin) { imin = i; dmin = dist_c[i]; }
+            }
+            if (dmin == finf()) return kInWall;
+            int y[D];
+            for (int k = 0; k < D; ++k) y[k] = xq[k] + ((imin >> k) & 1);
+            nymin = bilevel(y);
+            nymin_grid = gridindex(y);
+            const float ws = wsum_c[imin];
+            if (ws == 0.f) return kAtSeed;
+            thr = dmin + A.causality / ws;
+        }
+        for (int k = 0; k < D; ++k) flow[k] = 0.f;
+        for (int i = 0; i < NC; ++i) {
+            if (dist_c[i] >= thr) continue;
+            for (int k = 0; k < D; ++k) flow[k] += wts[i] * flow_c[i][k];
+        }
+        float n2 = 0.f;
+        for (int k = 0; k < D; ++k) n2 += flow[k] * flow[k];
+        const float nrm = sqrtf(n2);
+        if (!(nrm > 0.f)) return kVanishingFlow;
+        const float l = (float)(1.0 / (double)nrm);
+        for (int k = 0; k < D; ++k) flow[k] *= l;
+        return kContinue;
+    }
+};
+
+template <int D>
+__global__ void geodesic_kernel(GeoArgs A) {
+    const int tid = blockIdx.x * blockDim.x + threadIdx.x;
+    if (tid >= A.ntips) return;
+    float *out = A.paths + (long long)tid * A.cap * D;
+    float x[D];
+    for (int k = 0; k < D; ++k) {
+        x[k] = A.tips[tid * D + k];
+        out[k] = x[k];
+    }
+    int pos = 1, stop = kContinue;
+    const int hlen = 1 + max(A.eucl_delay, A.nymin_delay);
+    uint8_t eucl_p[kMaxHist];
+    long long nymin_p[kMaxHist];
+    Walker<D> W(A);
+    for (int chunk = 0; chunk < A.max_chunks; ++chunk) {
+        // a chunk starts afresh from the last point, as the reference's restart does
+        for (int l = 0; l < hlen; ++l) {
+            eucl_p[l] = 255;
+            nymin_p[l] = kIntMax;
+        }
+        W.reset();
+        int len;
+        for (len = 1; len < A.typical_len; ++len) {
+            const int l = len % hlen;
+            float xp[D], xm[D], flow[D];
+            for (int k = 0; k < D; ++k) xp[k] = x[k];
+            stop = W.normalized_flow(x, flow);
+            if (stop != kContinue) break;
+            nymin_p[l] = W.nymin;
+            eucl_p[l] = __ldg(A.eucl + W.nymin_grid);
+            if (W.nymin == nymin_p[(l - A.nymin_delay + hlen) % hlen]) { stop = kStationnary; break; }
+            // The reference's subscript is a boolean expression (cuda/Kernel_GeodesicODE.h:331).
+            const int cmp = (((l - A.eucl_delay + hlen) % hlen) != 0) && (len >= 0);
+            if (eucl_p[l] > eucl_p[cmp]) { stop = kPastSeed; break; }
+            for (int k = 0; k < D; ++k) xm[k] = (0.5f * A.step) * flow[k] + xp[k];
+            stop = W.normalized_flow(xm, flow);
+            if (stop != kContinue) break;
+            for (int k = 0; k < D; ++k) x[k] = A.step * flow[k] + xp[k];
+            if (pos < A.cap) {
+                for (int k = 0; k < D; ++k) out[pos * D + k] = x[k];
+                ++pos;
+            }
+        }
+        if (stop != kContinue) break;
+    }
+    A.lengths[tid] = pos;
+    A.stops[tid] = (int8_t)stop;
+}
+
+static inline unsigned nblocks(long long n, int bs) { return (unsigned)((n + bs - 1) / bs); }
+
+}  // namespace agd
+
 using namespace agd;
+
 extern "C" {
-int agd_eucl_map(int, const int *, const uint8_t *, int, int, uint8_t *, uint8_t *, agd_stream_t) {
-    return set_error(AGD_STATUS_UNSUPPORTED, "not built");
+
+int agd_eucl_map(int ndim, const int *shape, const uint8_t *seed_mask, int npasses, int cut, uint8_t *eucl,
+                 uint8_t *tmp, agd_stream_t stream) {
+    clear_error();
+    if ((ndim != 2 && ndim != 3) || !shape || !seed_mask || !eucl || !tmp || npasses < 0)
+        return set_error(AGD_STATUS_INVALID, "agd_eucl_map: bad arguments");
+    EGeo g;
+    g.nd = ndim;
+    g.n = 1;
+    for (int k = 0; k < 3; ++k) g.shape[k] = 1;
+    for (int k = 0; k < ndim; ++k) {
+        if (shape[k] <= 0) return set_error(AGD_STATUS_INVALID, "agd_eucl_map: bad shape");
+        g.shape[k] = shape[k];
+        g.n *= shape[k];
+    }
+    cudaStream_t st = (cudaStream_t)stream;
+    const int bs = 256;
+    uint8_t *a = eucl, *b = tmp;
+    eucl_init_kernel<<<nblocks(g.n, bs), bs, 0, st>>>(g, seed_mask, a);
+    for (int it = 0; it < npasses; ++it) {
+        infconv_kernel<<<nblocks(g.n, bs), bs, 0, st>>>(g, a, b);
+        uint8_t *t = a; a = b; b = t;
+    }
+    eucl_cut_kernel<<<nblocks(g.n, bs), bs, 0, st>>>(g, a, cut, b);
+    if (b != eucl) cudaMemcpyAsync(eucl, b, (size_t)g.n, cudaMemcpyDeviceToDevice, st);
+    const cudaError_t err = cudaGetLastError();
+    return err == cudaSuccess ? AGD_STATUS_OK : set_cuda_error("eucl_map", err);
 }
-int agd_geodesics(const agd_instance *, const float *, const float *, const uint8_t *, const float *, int, float,
-                  float, int, int, int, int, float *, int, int32_t *, int8_t *, agd_stream_t) {
-    return set_error(AGD_STATUS_UNSUPPORTED, "not built");
+
+int agd_geodesics(const agd_instance *inst, const float *flow_vector, const float *flow_weightsum, const uint8_t *eucl,
+                  const float *tips, int ntips, float step, float causality, int typical_len, int max_chunks,
+                  int eucl_delay, int nymin_delay, float *paths, int cap, int32_t *lengths, int8_t *stops,
+                  agd_stream_t stream) {
+    clear_error();
+    if (!inst || (inst->ndim != 2 && inst->ndim != 3) || ntips < 0 || !flow_vector || !flow_weightsum || !eucl ||
+        !inst->values || typical_len < 2 || max_chunks < 1 || eucl_delay < 0 || nymin_delay < 0 ||
+        1 + (eucl_delay > nymin_delay ? eucl_delay : nymin_delay) > kMaxHist || cap < 1 ||
+        (ntips > 0 && (!tips || !paths || !lengths || !stops)))
+        return set_error(AGD_STATUS_INVALID, "agd_geodesics: bad arguments");
+    if (ntips == 0) return AGD_STATUS_OK;
+    GeoArgs A;
+    A.nd = inst->ndim;
+    A.size_i = 1;
+    long long so = 1;
+    for (int k = 0; k < 3; ++k) { A.shape[k] = A.shape_i[k] = A.shape_o[k] = 1; }
+    for (int k = 0; k < A.nd; ++k) {
+        if (inst->shape[k] <= 0 || inst->shape_i[k] <= 0) return set_error(AGD_STATUS_INVALID, "bad shape");
+        A.shape[k] = inst->shape[k];
+        A.shape_i[k] = inst->shape_i[k];
+        A.shape_o[k] = (inst->shape[k] + inst->shape_i[k] - 1) / inst->shape_i[k];
+        A.size_i *= inst->shape_i[k];
+        so *= A.shape_o[k];
+    }
+    A.size_tot = so * A.size_i;
+    A.u = inst->values;
+    A.fvec = flow_vector;
+    A.fwsum = flow_weightsum;
+    A.eucl = eucl;
+    A.tips = tips;
+    A.ntips = ntips;
+    A.step = step;
+    A.causality = causality;
+    A.typical_len = typical_len;
+    A.max_chunks = max_chunks;
+    A.eucl_delay = eucl_delay;
+    A.nymin_delay = nymin_delay;
+    A.paths = paths;
+    A.cap = cap;
+    A.lengths = lengths;
+    A.stops = stops;
+    const int bs = 32;  // geodesics are few and sequential: small blocks spread them over SMs
+    if (A.nd == 2) geodesic_kernel<2><<<nblocks(ntips, bs), bs, 0, (cudaStream_t)stream>>>(A);
+    else geodesic_kernel<3><<<nblocks(ntips, bs), bs, 0, (cudaStream_t)stream>>>(A);
+    const cudaError_t err = cudaGetLastError();
+    return err == cudaSuccess ? AGD_STATUS_OK : set_cuda_error("geodesics", err);
 }
-}
+
+}  // extern "C"

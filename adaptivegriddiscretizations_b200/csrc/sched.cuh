@@ -1,0 +1,422 @@
+// Device scheduler shared by the eikonal and the adjoint solvers: per-instance
+// epochs over tiles, one global queue of tiles, no grid-wide barrier.  See
+// eikonal.cu for the scheduling scheme.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstring>
+#include <vector>
+
+#include "agd_common.cuh"
+#include "agd_internal.h"
+
+namespace agd {
+
+// ------------------------------------------------------------- variants ---
+enum Variant { V_ISO2_8 = 0, V_ISO2_16, V_RIEM2_8, V_ISO3_4, V_RIEM3_4, V_COUNT };
+
+static int variant_of(const agd_instance &a) {
+    if (a.ndim == 2) {
+        if (a.model == AGD_MODEL_RIEMANN && a.shape_i[0] == 8 && a.shape_i[1] == 8) return V_RIEM2_8;
+        if (a.model == AGD_MODEL_ISOTROPIC && a.shape_i[0] == 8 && a.shape_i[1] == 8) return V_ISO2_8;
+        if (a.model == AGD_MODEL_ISOTROPIC && a.shape_i[0] == 16 && a.shape_i[1] == 16) return V_ISO2_16;
+    } else if (a.ndim == 3 && a.shape_i[0] == 4 && a.shape_i[1] == 4 && a.shape_i[2] == 4) {
+        return a.model == AGD_MODEL_RIEMANN ? V_RIEM3_4 : V_ISO3_4;
+    }
+    return -1;
+}
+
+// Per-instance epoch state.
+struct InstState {
+    int epoch;         // current epoch (1-based)
+    int pending;       // tiles of the current epoch not yet finished
+    unsigned cnt[2];   // lengths of the instance's lists, by epoch parity
+    int done;
+};
+
+struct Ctrl {
+    unsigned head, tail;       // global queue tickets (monotonic)
+    int active;                // instances not finished
+    unsigned err;
+};
+
+// Workspace: [Inst][InstState][tile_inst][list0][list1][flags][score0][score1][queue][Ctrl][stats]
+struct WsLayout {
+    size_t inst, istate, tile_inst, list0, list1, flags, score0, score1, queue, ctrl, stats, total;
+    int total_tiles;
+    unsigned qcap;
+};
+
+static size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
+constexpr long long kMaxWarps = 148 * 64;  // resident warps of a launch, upper bound
+
+static bool layout(const agd_instance *a, int n, WsLayout &L, std::vector<Inst> *out) {
+    long long tiles = 0;
+    if (out) out->resize(n);
+    for (int i = 0; i < n; ++i) {
+        Inst I;
+        std::memset(&I, 0, sizeof(I));
+        I.a = a[i];
+        if (a[i].ndim < 2 || a[i].ndim > 3) return false;
+        I.size_o = 1;
+        for (int k = 0; k < a[i].ndim; ++k) {
+            if (a[i].shape[k] <= 0 || a[i].shape_i[k] <= 0) return false;
+            I.shape_o[k] = (a[i].shape[k] + a[i].shape_i[k] - 1) / a[i].shape_i[k];
+            I.size_o *= I.shape_o[k];
+        }
+        I.size_i = 1;
+        for (int k = 0; k < a[i].ndim; ++k) I.size_i *= a[i].shape_i[k];
+        I.size_tot = (long long)I.size_o * I.size_i;
+        I.tile_base = (int)tiles;
+        I.variant = variant_of(a[i]);
+        tiles += I.size_o;
+        if (tiles > 0x3fffffff) return false;
+        if (out) (*out)[i] = I;
+    }
+    // Queue slots: at most `tiles` entries are outstanding (an instance's current
+    // epoch list), plus the tickets held by waiting warps and the exit sentinels.
+    const unsigned qcap = (unsigned)(2 * tiles + 2 * kMaxWarps);
+    size_t off = 0;
+    L.inst = off; off = align256(off + sizeof(Inst) * n);
+    L.istate = off; off = align256(off + sizeof(InstState) * n);
+    L.tile_inst = off; off = align256(off + sizeof(int) * tiles);
+    L.list0 = off; off = align256(off + sizeof(int) * tiles);
+    L.list1 = off; off = align256(off + sizeof(int) * tiles);
+    L.flags = off; off = align256(off + sizeof(unsigned) * tiles);
+    L.score0 = off; off = align256(off + sizeof(unsigned) * tiles);
+    L.score1 = off; off = align256(off + sizeof(unsigned) * tiles);
+    L.queue = off; off = align256(off + sizeof(unsigned long long) * qcap);
+    L.ctrl = off; off = align256(off + sizeof(Ctrl));
+    L.stats = off; off = align256(off + sizeof(agd_stats) * n);
+    L.total = off;
+    L.total_tiles = (int)tiles;
+    L.qcap = qcap;
+    return true;
+}
+
+// --------------------------------------------------------- kernel context ---
+struct Sched {
+    const Inst *inst;
+    InstState *ist;
+    const int *tile_inst;
+    int *list0, *list1;
+    unsigned *flags, *score0, *score1;
+    unsigned long long *queue;
+    unsigned qcap;
+    Ctrl *ctrl;
+    agd_stats *stats;
+    int ninst;
+    int nwarps;  // worker warps of the launch
+    unsigned long long timeout_ns;
+};
+
+// Queue slot encoding: (ticket << 32) | payload, empty = all ones.  A waiting
+// consumer holding ticket h takes slot h % qcap only when it carries ticket h,
+// so slots of different laps never alias.  Payload = tile id, or kExitTile.
+constexpr unsigned long long kSlotEmpty = ~0ull;
+constexpr unsigned kExitTile = 0xffffffffu;
+
+__device__ __forceinline__ int ld_acquire_s32(const int *p) {
+    int v;
+    asm volatile("ld.acquire.gpu.global.s32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ unsigned long long ld_acquire_u64(const unsigned long long *p) {
+    unsigned long long v;
+    asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void st_release_u64(unsigned long long *p, unsigned long long v) {
+    asm volatile("st.release.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+
+// Tile t is to be visited at epoch e+1 of its instance (pushed during epoch e).
+__device__ __forceinline__ void push_tile(const Sched &S, const Inst &I, int ii, int t, int e) {
+    const unsigned tag = (unsigned)(e + 1);
+    if (atomicMax(&S.flags[t], tag) < tag) {
+        int *nxt = ((e + 1) & 1) ? S.list1 : S.list0;
+        const unsigned idx = atomicAdd(&S.ist[ii].cnt[(e + 1) & 1], 1u);
+        nxt[I.tile_base + idx] = t;
+    }
+}
+
+__device__ __forceinline__ unsigned score_at(const Sched &S, int t, int e) {
+    // Score written at epoch e (0 if the tile was not visited at epoch e).
+    const unsigned *arr = (e & 1) ? S.score1 : S.score0;
+    const unsigned w = __ldcg(arr + t);
+    return (int)(w >> 8) == e ? (w & 0xffu) : 0u;
+}
+
+__device__ __forceinline__ bool put_slot(const Sched &S, unsigned ticket, unsigned payload) {
+    unsigned long long *slot = S.queue + ticket % S.qcap;
+    const unsigned long long t0 = globaltimer();
+    while (ld_acquire_u64(slot) != kSlotEmpty) {  // the previous lap's entry is not yet taken
+        if (globaltimer() - t0 > S.timeout_ns) {
+            atomicOr(&S.ctrl->err, (unsigned)AGD_STATUS_WATCHDOG);
+            return false;
+        }
+        __nanosleep(64);
+    }
+    st_release_u64(slot, ((unsigned long long)ticket << 32) | payload);
+    return true;
+}
+
+// Appends the n tile ids src[0..n) to the global queue; warp-cooperative.
+static __device__ void enqueue_warp(const Sched &S, const int *src, int n, int lane) {
+    unsigned start = 0;
+    if (lane == 0) start = atomicAdd(&S.ctrl->tail, (unsigned)n);
+    start = __shfl_sync(kFull, start, 0);
+    for (int k = lane; k < n; k += 32)
+        if (!put_slot(S, start + (unsigned)k, (unsigned)__ldcg(src + k))) break;
+    __syncwarp();
+}
+
+// End of epoch e of instance ii (called by the warp that finished its last
+// tile): publish the next list, or retire the instance.  The stop test is the
+// reference's: no tile left to update, or nitermax_o epochs run
+// (_solvers.py:94-120 with _StopCriterion.py:62-84, _solvers.py:53-57).
+static __device__ void close_epoch(const Sched &S, int ii, int e, int lane) {
+    const Inst &I = S.inst[ii];
+    InstState &st = S.ist[ii];
+    int n = 0;
+    if (lane == 0) n = (int)atomicAdd(&st.cnt[(e + 1) & 1], 0u);
+    n = __shfl_sync(kFull, n, 0);
+    if (n == 0 || e >= I.a.nitermax_o) {
+        int last = 0;
+        if (lane == 0) {
+            S.stats[ii].niter_o = e;
+            if (e >= I.a.nitermax_o) atomicOr(&S.stats[ii].status, (int)AGD_STATUS_NOT_CONVERGED);
+            st.done = 1;
+            __threadfence();
+            last = atomicSub(&S.ctrl->active, 1) == 1;
+        }
+        last = __shfl_sync(kFull, last, 0);
+        if (last) {  // every instance is done: one exit sentinel per worker warp
+            unsigned start = 0;
+            if (lane == 0) start = atomicAdd(&S.ctrl->tail, (unsigned)S.nwarps);
+            start = __shfl_sync(kFull, start, 0);
+            for (int k = lane; k < S.nwarps; k += 32)
+                if (!put_slot(S, start + (unsigned)k, kExitTile)) break;
+        }
+        return;
+    }
+    if (lane == 0) {
+        st.cnt[e & 1] = 0u;  // the list of epoch e is consumed; epoch e+1 fills it for epoch e+2
+        st.pending = n;
+        st.epoch = e + 1;
+        __threadfence();
+    }
+    __syncwarp();
+    const int *src = (((e + 1) & 1) ? S.list1 : S.list0) + I.tile_base;
+    enqueue_warp(S, src, n, lane);
+}
+
+
+// Waits (lane 0) for the entry of ticket h.  Gives up with a watchdog error if
+// the queue receives no entry anywhere (no epoch of any instance ends) for
+// timeout_ns, or if an error is raised.
+__device__ __forceinline__ unsigned take_slot(const Sched &S, unsigned h) {
+    unsigned long long *slot = S.queue + h % S.qcap;
+    unsigned seen = ld_acquire(&S.ctrl->tail);
+    unsigned long long t0 = globaltimer();
+    unsigned backoff = 32;
+    for (unsigned it = 0;; ++it) {
+        const unsigned long long v = ld_acquire_u64(slot);
+        if (v != kSlotEmpty && (unsigned)(v >> 32) == h) {
+            st_release_u64(slot, kSlotEmpty);
+            return (unsigned)v;
+        }
+        if ((it & 15u) == 15u) {
+            if (ld_acquire(&S.ctrl->err)) return kExitTile;
+            const unsigned p = ld_acquire(&S.ctrl->tail);
+            const unsigned long long now = globaltimer();
+            if (p != seen) {
+                seen = p;
+                t0 = now;
+            } else if (now - t0 > S.timeout_ns) {
+                atomicOr(&S.ctrl->err, (unsigned)AGD_STATUS_WATCHDOG);
+                return kExitTile;
+            }
+        }
+        __nanosleep(backoff);
+        backoff = min(backoff * 2u, 1024u);
+    }
+}
+
+// Worker warps: take a tile from the queue, visit it at its instance's
+// current epoch, and close the epoch when it was the last tile of it.
+// Visitor provides: Args (by value), Smem (per warp), and
+//   static void visit(const Sched&, const Args&, int t, int ii, int e, int lane, Smem&).
+template <class Visitor, int WPB>
+__global__ void __launch_bounds__(WPB * 32) sched_worker(Sched S, typename Visitor::Args VA) {
+    __shared__ typename Visitor::Smem smem[WPB];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (ld_acquire_s32(&S.ctrl->active) == 0) return;  // nothing to solve
+    while (true) {
+        unsigned t = 0;
+        if (lane == 0) {
+            const unsigned h = atomicAdd(&S.ctrl->head, 1u);
+            t = take_slot(S, h);
+        }
+        t = __shfl_sync(kFull, t, 0);
+        if (t == kExitTile) break;
+        const int ii = __ldg(S.tile_inst + t);
+        int e = 0;
+        if (lane == 0) e = ld_acquire_s32(&S.ist[ii].epoch);  // tiles are queued at their instance's epoch
+        e = __shfl_sync(kFull, e, 0);
+        Visitor::visit(S, VA, (int)t, ii, e, lane, smem[warp]);
+        int lastone = 0;
+        if (lane == 0) {
+            __threadfence();  // this visit's pushes and stores before the count
+            lastone = atomicSub(&S.ist[ii].pending, 1) == 1;
+            if (lastone) __threadfence();
+        }
+        lastone = __shfl_sync(kFull, lastone, 0);
+        if (lastone) close_epoch(S, ii, e, lane);
+    }
+}
+
+// ---------------------------------------------------------------- setup ---
+// tile -> instance map and epoch-1 lists: tiles flagged by `trigger`, by
+// ACTIVATE_ALL, or holding a seed point inside the domain (the reference's
+// trigger = seedTags, _SetArgs.py:122 and _solvers.py:98-100).
+static __global__ void setup_tiles(Sched S) {
+    const int t = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    const int lane = threadIdx.x & 31;
+    int lo = 0, hi = S.ninst - 1;  // bisection over the tile bases
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (S.inst[mid].tile_base <= t) lo = mid; else hi = mid - 1;
+    }
+    const Inst &I = S.inst[lo];
+    if (t >= I.tile_base + I.size_o) return;  // past the last tile
+    const int n_o = t - I.tile_base;
+    if (lane == 0) const_cast<int *>(S.tile_inst)[t] = lo;
+    bool active = (I.a.flags & AGD_FLAG_ACTIVATE_ALL) != 0;
+    if (I.a.trigger) {
+        active = active || I.a.trigger[n_o] != 0;
+    } else if (!active) {
+        int xo[3], r = n_o;
+        for (int k = I.a.ndim - 1; k >= 0; --k) { xo[k] = r % I.shape_o[k]; r /= I.shape_o[k]; }
+        bool any = false;
+        for (int n_i = lane; n_i < I.size_i; n_i += 32) {
+            int xi[3], q = n_i;
+            for (int k = I.a.ndim - 1; k >= 0; --k) { xi[k] = q % I.a.shape_i[k]; q /= I.a.shape_i[k]; }
+            bool in = true;
+            for (int k = 0; k < I.a.ndim; ++k) in = in && (xo[k] * I.a.shape_i[k] + xi[k] < I.a.shape[k]);
+            const size_t n_t = (size_t)n_o * I.size_i + n_i;
+            if (in && ((I.a.seedbits[n_t >> 3] >> (n_t & 7)) & 1)) any = true;
+        }
+        active = __any_sync(kFull, any);
+    }
+    if (active && lane == 0) {
+        S.flags[t] = 1u;
+        const unsigned idx = atomicAdd(&S.ist[lo].cnt[1], 1u);
+        S.list1[I.tile_base + idx] = t;
+    }
+}
+
+// Epoch 1 of every instance: one warp per instance publishes its first list.
+static __global__ void publish_first(Sched S) {
+    const int ii = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    const int lane = threadIdx.x & 31;
+    if (ii >= S.ninst) return;
+    const Inst &I = S.inst[ii];
+    InstState &st = S.ist[ii];
+    const int n = (int)st.cnt[1];
+    if (n == 0) {
+        if (lane == 0) { st.done = 1; S.stats[ii].niter_o = 0; }
+        return;
+    }
+    if (lane == 0) {
+        st.cnt[0] = 0u;
+        st.pending = n;
+        st.epoch = 1;
+        atomicAdd(&S.ctrl->active, 1);
+        __threadfence();
+    }
+    __syncwarp();
+    enqueue_warp(S, S.list1 + I.tile_base, n, lane);
+}
+
+static __global__ void finish_stats(Sched S, agd_stats *out) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= S.ninst) return;
+    agd_stats st = S.stats[i];
+    st.status |= (int)S.ctrl->err;
+    if (!S.ist[i].done) st.status |= (int)AGD_STATUS_WATCHDOG;
+    if (out) out[i] = st;
+}
+
+// --------------------------------------------------------------- launch ---
+template <class Visitor, int WPB>
+static int launch_workers(const Sched &S, const typename Visitor::Args &VA, int total_tiles, const agd_launch *cfg,
+                          cudaStream_t st) {
+    auto kern = sched_worker<Visitor, WPB>;
+    int dev = 0, nsm = 0, per_sm = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return set_cuda_error("cudaGetDevice");
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, WPB * 32, 0) != cudaSuccess)
+        return set_cuda_error("occupancy query");
+    if (per_sm < 1) return set_error(AGD_STATUS_UNSUPPORTED, "worker kernel does not fit on an SM");
+    const int max_ctas = per_sm * nsm;  // all resident: idle warps wait on their queue ticket
+    int ctas = cfg && cfg->ctas > 0 ? cfg->ctas : (total_tiles + WPB - 1) / WPB;
+    ctas = std::max(1, std::min(ctas, max_ctas));
+    Sched s = S;
+    s.nwarps = ctas * WPB;
+    if (s.nwarps > kMaxWarps) return set_error(AGD_STATUS_INVALID, "too many worker warps");
+    kern<<<ctas, WPB * 32, 0, st>>>(s, VA);
+    const cudaError_t err = cudaGetLastError();
+    if (err != cudaSuccess) return set_cuda_error("worker launch", err);
+    return AGD_STATUS_OK;
+}
+
+// Scheduler pointers inside a workspace laid out by layout().
+static Sched sched_at(const WsLayout &L, void *ws, int ninst) {
+    char *w = static_cast<char *>(ws);
+    Sched S;
+    S.inst = reinterpret_cast<const Inst *>(w + L.inst);
+    S.ist = reinterpret_cast<InstState *>(w + L.istate);
+    S.tile_inst = reinterpret_cast<const int *>(w + L.tile_inst);
+    S.list0 = reinterpret_cast<int *>(w + L.list0);
+    S.list1 = reinterpret_cast<int *>(w + L.list1);
+    S.flags = reinterpret_cast<unsigned *>(w + L.flags);
+    S.score0 = reinterpret_cast<unsigned *>(w + L.score0);
+    S.score1 = reinterpret_cast<unsigned *>(w + L.score1);
+    S.queue = reinterpret_cast<unsigned long long *>(w + L.queue);
+    S.qcap = L.qcap;
+    S.ctrl = reinterpret_cast<Ctrl *>(w + L.ctrl);
+    S.stats = reinterpret_cast<agd_stats *>(w + L.stats);
+    S.ninst = ninst;
+    S.nwarps = 0;
+    S.timeout_ns = 2000000000ull;
+    return S;
+}
+
+// One scheduled solve over the instances already uploaded at L.inst: clears the
+// scheduler state, builds the first lists, runs the workers, writes the stats.
+template <class Visitor>
+static int run_sched(const WsLayout &L, void *ws, int n, const typename Visitor::Args &VA, agd_stats *stats,
+                     const agd_launch *cfg, cudaStream_t st) {
+    Sched S = sched_at(L, ws, n);
+    if (cfg && cfg->timeout_ns > 0) S.timeout_ns = (unsigned long long)cfg->timeout_ns;
+    char *w = static_cast<char *>(ws);
+    cudaError_t err = cudaMemsetAsync(w + L.istate, 0, sizeof(InstState) * n, st);
+    if (err == cudaSuccess) err = cudaMemsetAsync(w + L.flags, 0, L.queue - L.flags, st);
+    if (err == cudaSuccess) err = cudaMemsetAsync(w + L.queue, 0xff, L.ctrl - L.queue, st);
+    if (err == cudaSuccess) err = cudaMemsetAsync(w + L.ctrl, 0, L.total - L.ctrl, st);
+    if (err != cudaSuccess) return set_cuda_error("workspace clear", err);
+    setup_tiles<<<(L.total_tiles + 7) / 8, 256, 0, st>>>(S);
+    if ((err = cudaGetLastError()) != cudaSuccess) return set_cuda_error("setup_tiles", err);
+    publish_first<<<(n + 7) / 8, 256, 0, st>>>(S);
+    if ((err = cudaGetLastError()) != cudaSuccess) return set_cuda_error("publish_first", err);
+    const int rc = (cfg && cfg->warps_per_cta == 8) ? launch_workers<Visitor, 8>(S, VA, L.total_tiles, cfg, st)
+                                                    : launch_workers<Visitor, 4>(S, VA, L.total_tiles, cfg, st);
+    if (rc != AGD_STATUS_OK) return rc;
+    finish_stats<<<(n + 127) / 128, 128, 0, st>>>(S, stats);
+    if ((err = cudaGetLastError()) != cudaSuccess) return set_cuda_error("finish_stats", err);
+    return AGD_STATUS_OK;
+}
+
+}  // namespace agd

@@ -110,4 +110,11 @@ def test_selling_gpu_bitexact(nd):
     e = torch.empty((n, sd, nd), dtype=torch.int32, device="cuda")
     _lib.check(_lib.lib().agd_selling(nd, _lib.ptr(m), n, _lib.ptr(w), _lib.ptr(e), _lib.stream_ptr()))
     assert np.array_equal(e.cpu().numpy(), f["ref_e"])
-    np.testing.assert_allclose(w.cpu().numpy(), f["ref_w"], rtol=2e-6, atol=0)
+    # A weight is -<b_i, m b_j>, a cancelling sum: the GPU contracts its terms into
+    # fused multiply-adds, the host build of the reference does not.  The rounding
+    # difference is bounded relative to the size of the tensor, not of the weight.
+    # Its terms are bounded by |b|^2 |m|, with |b|^2 <= max |offset|^2.
+    wg, wr = w.cpu().numpy(), f["ref_w"]
+    mnorm = np.abs(f["m"]).sum(axis=1, keepdims=True) * 2
+    b2 = np.maximum((f["ref_e"].astype(np.float64) ** 2).sum(axis=2).max(axis=1, keepdims=True), 1)
+    assert (np.abs(wg - wr) <= 4 * np.finfo(np.float32).eps * b2 * mnorm).all()
