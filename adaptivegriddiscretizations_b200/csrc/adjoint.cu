@@ -222,7 +222,6 @@ struct LinearVisitor {
         __syncwarp();
         if (!settled && lane == 0) push_tile(S, I, ii, t, e);
         (void)self;
-        if (lane == 0) atomicAdd((unsigned long long *)&S.stats[ii].tile_visits, 1ull);
     }
 };
 

@@ -69,6 +69,26 @@ struct Visit {
                 r /= I.shape_o[k];
             }
         }
+        // Scores of this tile and of its neighbours at epoch e-1 (complete): loaded
+        // now, so that their latency overlaps the visit (cuda/Propagation.h:103-167).
+        const int t = I.tile_base + n_o;
+        int nb = -1;  // neighbour tile handled by this lane (lanes 0..2D-1)
+        if (lane < 2 * D) {
+            int y[3] = {xo[0], xo[1], xo[2]};
+            y[lane >> 1] += 2 * (lane & 1) - 1;
+            bool ok = true;
+#pragma unroll
+            for (int k = 0; k < D; ++k) ok = ok && y[k] >= 0 && y[k] < I.shape_o[k];
+            if (ok) {
+                int m = 0;
+#pragma unroll
+                for (int k = 0; k < D; ++k) m = m * I.shape_o[k] + y[k];
+                nb = I.tile_base + m;
+            }
+        }
+        const int sp_self = (int)score_at(S, t, e - 1);
+        const int sp_nb = nb >= 0 ? (int)score_at(S, nb, e - 1) : 0;
+
         const size_t base = (size_t)n_o * TL::SIZE;
         float uold[P], rhs[P];
         float wts[P][NACT];
@@ -158,33 +178,18 @@ struct Visit {
         __syncwarp();
 
         // Fast iterative method (cuda/Propagation.h:103-167).
-        const int t = I.tile_base + n_o;
         const int front = A.fim_front_width;
-        int nb = -1;  // neighbour tile handled by this lane (lanes 0..2D-1)
-        if (lane < 2 * D) {
-            int y[3] = {xo[0], xo[1], xo[2]};
-            y[lane >> 1] += 2 * (lane & 1) - 1;
-            bool ok = true;
-#pragma unroll
-            for (int k = 0; k < D; ++k) ok = ok && y[k] >= 0 && y[k] < I.shape_o[k];
-            if (ok) {
-                int m = 0;
-#pragma unroll
-                for (int k = 0; k < D; ++k) m = m * I.shape_o[k] + y[k];
-                nb = I.tile_base + m;
-            }
-        }
         int sn;
         bool prop;
         if (!changed) {
-            const int sp = (int)score_at(S, t, e - 1);
+            const int sp = sp_self;
             if (sp == 0 || sp == front) { sn = 0; prop = false; }
             else { sn = front; prop = true; }
         } else {
             sn = 1;
             if (lane == 0) push_tile(S, I, ii, t, e);
             if (front > 2) {
-                const int sq = nb >= 0 ? (int)score_at(S, nb, e - 1) - 1 : -1;
+                const int sq = nb >= 0 ? sp_nb - 1 : -1;
                 int mx = sq;
 #pragma unroll
                 for (int o = 16; o > 0; o >>= 1) mx = max(mx, __shfl_xor_sync(kFull, mx, o));
@@ -195,7 +200,6 @@ struct Visit {
         if (lane == 0) {
             unsigned *arr = (e & 1) ? S.score1 : S.score0;
             __stcg(arr + t, ((unsigned)e << 8) | (unsigned)sn);
-            atomicAdd((unsigned long long *)&S.stats[ii].tile_visits, 1ull);
         }
         if (prop && nb >= 0) push_tile(S, I, ii, nb, e);
     }
@@ -270,8 +274,9 @@ static int plan_create(const agd_instance *host, int n, agd_plan **out) {
         else if (P->insts[i].variant < 0) { bad = "model/tile shape not built"; code = AGD_STATUS_UNSUPPORTED; }
         else if (a.multip_step != 0.f) { bad = "multiprecision not built"; code = AGD_STATUS_UNSUPPORTED; }
         else if (!a.values || !a.rhs || !a.seedbits || (a.model == AGD_MODEL_RIEMANN && !a.geom)) bad = "missing array";
-        else if (a.niter_i < 1 || a.fim_front_width < 2 || a.fim_front_width > 255 || a.nitermax_o < 0)
-            bad = "bad niter_i / fim_front_width / nitermax_o";
+        else if (a.niter_i < 1 || a.fim_front_width < 2 || a.fim_front_width > 255 || a.nitermax_o < 0 ||
+                 a.nitermax_o > kMaxEpochs)
+            bad = "bad niter_i / fim_front_width / nitermax_o (at most 16000)";
         if (bad) {
             delete P;
             return set_error(code, bad);

@@ -76,7 +76,7 @@ static bool layout(const agd_instance *a, int n, WsLayout &L, std::vector<Inst> 
     }
     // Queue slots: at most `tiles` entries are outstanding (an instance's current
     // epoch list), plus the tickets held by waiting warps and the exit sentinels.
-    const unsigned qcap = (unsigned)(2 * tiles + 2 * kMaxWarps);
+    const unsigned qcap = (unsigned)(2 * tiles + 2 * kMaxWarps) | 1u;  // odd: see kSlotEmpty
     size_t off = 0;
     L.inst = off; off = align256(off + sizeof(Inst) * n);
     L.istate = off; off = align256(off + sizeof(InstState) * n);
@@ -111,11 +111,17 @@ struct Sched {
     unsigned long long timeout_ns;
 };
 
-// Queue slot encoding: (ticket << 32) | payload, empty = all ones.  A waiting
-// consumer holding ticket h takes slot h % qcap only when it carries ticket h,
-// so slots of different laps never alias.  Payload = tile id, or kExitTile.
+// Queue slot encoding: ticket (low 20 bits) << 44 | epoch << 30 | tile, empty =
+// all ones.  A consumer holding ticket h takes slot h % qcap only when it carries
+// the low bits of h.  The only other entry a slot can hold is the previous lap's
+// (ticket h - qcap): qcap is odd, so its low ticket bits differ.
 constexpr unsigned long long kSlotEmpty = ~0ull;
-constexpr unsigned kExitTile = 0xffffffffu;
+constexpr unsigned kExitTile = 0x3fffffffu;
+constexpr int kMaxEpochs = 16000;
+__device__ __forceinline__ unsigned long long slot_word(unsigned ticket, int epoch, unsigned tile) {
+    return ((unsigned long long)(ticket & 0xfffffu) << 44) | ((unsigned long long)(epoch & 0x3fff) << 30) |
+           (tile & 0x3fffffffu);
+}
 
 __device__ __forceinline__ int ld_acquire_s32(const int *p) {
     int v;
@@ -148,7 +154,7 @@ __device__ __forceinline__ unsigned score_at(const Sched &S, int t, int e) {
     return (int)(w >> 8) == e ? (w & 0xffu) : 0u;
 }
 
-__device__ __forceinline__ bool put_slot(const Sched &S, unsigned ticket, unsigned payload) {
+__device__ __forceinline__ bool put_slot(const Sched &S, unsigned ticket, int epoch, unsigned tile) {
     unsigned long long *slot = S.queue + ticket % S.qcap;
     const unsigned long long t0 = globaltimer();
     while (ld_acquire_u64(slot) != kSlotEmpty) {  // the previous lap's entry is not yet taken
@@ -158,17 +164,18 @@ __device__ __forceinline__ bool put_slot(const Sched &S, unsigned ticket, unsign
         }
         __nanosleep(64);
     }
-    st_release_u64(slot, ((unsigned long long)ticket << 32) | payload);
+    st_release_u64(slot, slot_word(ticket, epoch, tile));
     return true;
 }
 
-// Appends the n tile ids src[0..n) to the global queue; warp-cooperative.
-static __device__ void enqueue_warp(const Sched &S, const int *src, int n, int lane) {
+// Appends the n tile ids src[0..n), to be visited at epoch e, to the global queue;
+// warp-cooperative.
+static __device__ void enqueue_warp(const Sched &S, const int *src, int n, int e, int lane) {
     unsigned start = 0;
     if (lane == 0) start = atomicAdd(&S.ctrl->tail, (unsigned)n);
     start = __shfl_sync(kFull, start, 0);
     for (int k = lane; k < n; k += 32)
-        if (!put_slot(S, start + (unsigned)k, (unsigned)__ldcg(src + k))) break;
+        if (!put_slot(S, start + (unsigned)k, e, (unsigned)__ldcg(src + k))) break;
     __syncwarp();
 }
 
@@ -197,7 +204,7 @@ static __device__ void close_epoch(const Sched &S, int ii, int e, int lane) {
             if (lane == 0) start = atomicAdd(&S.ctrl->tail, (unsigned)S.nwarps);
             start = __shfl_sync(kFull, start, 0);
             for (int k = lane; k < S.nwarps; k += 32)
-                if (!put_slot(S, start + (unsigned)k, kExitTile)) break;
+                if (!put_slot(S, start + (unsigned)k, 0, kExitTile)) break;
         }
         return;
     }
@@ -205,27 +212,28 @@ static __device__ void close_epoch(const Sched &S, int ii, int e, int lane) {
         st.cnt[e & 1] = 0u;  // the list of epoch e is consumed; epoch e+1 fills it for epoch e+2
         st.pending = n;
         st.epoch = e + 1;
+        S.stats[ii].tile_visits += n;  // tile visits = the lengths of the published lists
         __threadfence();
     }
     __syncwarp();
     const int *src = (((e + 1) & 1) ? S.list1 : S.list0) + I.tile_base;
-    enqueue_warp(S, src, n, lane);
+    enqueue_warp(S, src, n, e + 1, lane);
 }
 
 
 // Waits (lane 0) for the entry of ticket h.  Gives up with a watchdog error if
 // the queue receives no entry anywhere (no epoch of any instance ends) for
 // timeout_ns, or if an error is raised.
-__device__ __forceinline__ unsigned take_slot(const Sched &S, unsigned h) {
+__device__ __forceinline__ unsigned long long take_slot(const Sched &S, unsigned h) {
     unsigned long long *slot = S.queue + h % S.qcap;
     unsigned seen = ld_acquire(&S.ctrl->tail);
     unsigned long long t0 = globaltimer();
     unsigned backoff = 32;
     for (unsigned it = 0;; ++it) {
         const unsigned long long v = ld_acquire_u64(slot);
-        if (v != kSlotEmpty && (unsigned)(v >> 32) == h) {
+        if (v != kSlotEmpty && (unsigned)(v >> 44) == (h & 0xfffffu)) {
             st_release_u64(slot, kSlotEmpty);
-            return (unsigned)v;
+            return v;
         }
         if ((it & 15u) == 15u) {
             if (ld_acquire(&S.ctrl->err)) return kExitTile;
@@ -248,30 +256,56 @@ __device__ __forceinline__ unsigned take_slot(const Sched &S, unsigned h) {
 // current epoch, and close the epoch when it was the last tile of it.
 // Visitor provides: Args (by value), Smem (per warp), and
 //   static void visit(const Sched&, const Args&, int t, int ii, int e, int lane, Smem&).
+#ifndef AGD_WORKER_MIN_CTAS
+#define AGD_WORKER_MIN_CTAS 6  // resident 4-warp CTAs per SM the register budget must allow
+#endif
+constexpr int kSmemInst = 1024;  // instances whose tile bases a CTA keeps in shared memory
+
+// Decrement with acquire-release semantics: publishes this warp's writes and,
+// for the warp that brings the count to zero, makes everyone else's visible.
+__device__ __forceinline__ int atomic_dec_acq_rel(int *p) {
+    int old;
+    asm volatile("atom.acq_rel.gpu.global.add.s32 %0, [%1], -1;" : "=r"(old) : "l"(p) : "memory");
+    return old;
+}
+
 template <class Visitor, int WPB>
-__global__ void __launch_bounds__(WPB * 32) sched_worker(Sched S, typename Visitor::Args VA) {
+__global__ void __launch_bounds__(WPB * 32, AGD_WORKER_MIN_CTAS * 4 / WPB) sched_worker(Sched S, typename Visitor::Args VA) {
     __shared__ typename Visitor::Smem smem[WPB];
+    __shared__ int s_base[kSmemInst];  // tile bases, to find a tile's instance without a global load
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const bool inst_in_smem = S.ninst <= kSmemInst;
+    if (inst_in_smem)
+        for (int i = threadIdx.x; i < S.ninst; i += blockDim.x) s_base[i] = S.inst[i].tile_base;
+    __syncthreads();
     if (ld_acquire_s32(&S.ctrl->active) == 0) return;  // nothing to solve
+    // Each warp holds one queue ticket ahead: the ticket for its next tile is
+    // taken when a visit starts, so the atomic's latency overlaps the visit.
+    unsigned ticket = 0;
+    if (lane == 0) ticket = atomicAdd(&S.ctrl->head, 1u);
     while (true) {
-        unsigned t = 0;
-        if (lane == 0) {
-            const unsigned h = atomicAdd(&S.ctrl->head, 1u);
-            t = take_slot(S, h);
-        }
-        t = __shfl_sync(kFull, t, 0);
+        unsigned long long v = 0;
+        if (lane == 0) v = take_slot(S, ticket);
+        v = __shfl_sync(kFull, v, 0);
+        const unsigned t = (unsigned)(v & 0x3fffffffull);
+        const int e = (int)((v >> 30) & 0x3fff);
         if (t == kExitTile) break;
-        const int ii = __ldg(S.tile_inst + t);
-        int e = 0;
-        if (lane == 0) e = ld_acquire_s32(&S.ist[ii].epoch);  // tiles are queued at their instance's epoch
-        e = __shfl_sync(kFull, e, 0);
+        if (lane == 0) ticket = atomicAdd(&S.ctrl->head, 1u);
+        int ii;
+        if (inst_in_smem) {
+            int lo = 0, hi = S.ninst - 1;
+            while (lo < hi) {
+                const int mid = (lo + hi + 1) >> 1;
+                if (s_base[mid] <= (int)t) lo = mid; else hi = mid - 1;
+            }
+            ii = lo;
+        } else {
+            ii = __ldg(S.tile_inst + t);
+        }
         Visitor::visit(S, VA, (int)t, ii, e, lane, smem[warp]);
         int lastone = 0;
-        if (lane == 0) {
-            __threadfence();  // this visit's pushes and stores before the count
-            lastone = atomicSub(&S.ist[ii].pending, 1) == 1;
-            if (lastone) __threadfence();
-        }
+        __syncwarp();
+        if (lane == 0) lastone = atomic_dec_acq_rel(&S.ist[ii].pending) == 1;
         lastone = __shfl_sync(kFull, lastone, 0);
         if (lastone) close_epoch(S, ii, e, lane);
     }
@@ -333,11 +367,12 @@ static __global__ void publish_first(Sched S) {
         st.cnt[0] = 0u;
         st.pending = n;
         st.epoch = 1;
+        S.stats[ii].tile_visits = n;
         atomicAdd(&S.ctrl->active, 1);
         __threadfence();
     }
     __syncwarp();
-    enqueue_warp(S, S.list1 + I.tile_base, n, lane);
+    enqueue_warp(S, S.list1 + I.tile_base, n, 1, lane);
 }
 
 static __global__ void finish_stats(Sched S, agd_stats *out) {

@@ -55,7 +55,7 @@ def make_fields(n, batch, seed, sigma=8.0):
     return metrics, seeds
 
 
-def dictins(metrics, seeds, n, to_device=True, pinned=False):
+def dictins(metrics, seeds, n, to_device=True, pinned=False, traits=None):
     import torch
     from adaptivegriddiscretizations_b200 import Eikonal
     out = []
@@ -66,9 +66,10 @@ def dictins(metrics, seeds, n, to_device=True, pinned=False):
             mt, st = mt.pin_memory(), st.pin_memory()
         if to_device:
             mt, st = mt.cuda(), st.cuda()
-        out.append(Eikonal.dictIn({"model": "Riemann2", "mode": "gpu", "verbosity": 0,
-                                   "dims": [n, n], "gridScale": 1.0 / n, "origin": [0.0, 0.0],
-                                   "metric": mt, "seeds": st, "exportValues": True}))
+        d = {"model": "Riemann2", "mode": "gpu", "verbosity": 0, "dims": [n, n], "gridScale": 1.0 / n,
+             "origin": [0.0, 0.0], "metric": mt, "seeds": st, "exportValues": True}
+        d.update(traits or {})
+        out.append(Eikonal.dictIn(d))
     return out
 
 
@@ -184,6 +185,8 @@ def main():
     ap.add_argument("--wpc", type=int, default=4)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=2)
+    ap.add_argument("--niter-i", type=int, default=0, help="local iterations per tile visit (0: the default, 8)")
+    ap.add_argument("--front", type=int, default=0, help="FIM front width (0: the default, 4)")
     args = ap.parse_args()
 
     rank = int(os.environ.get("RANK", "0"))
@@ -206,7 +209,12 @@ def main():
 
     n, B = args.n, args.batch
     metrics, seeds = make_fields(n, B, 1000 + rank)
-    ins = dictins(metrics, seeds, n, to_device=True)
+    traits = {}
+    if args.niter_i:
+        traits["traits"] = {"shape_i": (8, 8), "niter_i": args.niter_i}
+    if args.front:
+        traits["fim_front_width"] = args.front
+    ins = dictins(metrics, seeds, n, to_device=True, traits=traits)
     itfs = [Interface(h) for h in ins]
     for it in itfs:
         it.SetKernelTraits()
@@ -262,14 +270,14 @@ def main():
     # end to end: public API from pinned host buffers, values back to the host
     e2e = None
     if args.e2e_steps > 0:
-        host_ins = dictins(metrics, seeds, n, to_device=False, pinned=True)
+        host_ins = dictins(metrics, seeds, n, to_device=False, pinned=True, traits=traits)
         h2d = sum(m.nbytes + s.nbytes for m, s in zip(metrics, seeds))
         outs = Eikonal.RunBatch(host_ins[:2])  # warm up the path
         torch.cuda.synchronize()
         t_e = time.perf_counter()
         d2h = 0
         for _ in range(args.e2e_steps):
-            host_ins = dictins(metrics, seeds, n, to_device=False, pinned=True)
+            host_ins = dictins(metrics, seeds, n, to_device=False, pinned=True, traits=traits)
             outs = Eikonal.RunBatch(host_ins)
             vals = [o["values"].cpu() for o in outs]
             d2h = sum(v.numel() * 4 for v in vals)
@@ -291,7 +299,8 @@ def main():
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": {"workload": f"Riemann2 {n}x{n} cold-start solves, batch {B} per GPU per step, one "
                                    f"persistent launch", "batch_per_gpu": B, "grid": n, "seeds": 4,
-                       "lambda": "U[1,100]", "theta_sigma_px": 8, "tile": "8x8", "niter_i": 8,
+                       "lambda": "U[1,100]", "theta_sigma_px": 8, "tile": "8x8",
+                       "niter_i": args.niter_i or 8, "fim_front_width": args.front or 4,
                        "grid_updates_per_step": updates_per_step,
                        "grid_updates_per_s": updates_per_step * args.steps * world / elapsed,
                        "mean_niter_o": float(niter.mean()), "max_niter_o": int(niter.max()),
