@@ -255,6 +255,26 @@ struct agd_plan {
 
 namespace agd {
 
+// Checks the instances of one launch; returns the mask of tile-visit variants.
+static int validate(const agd_instance *host, const Inst *insts, int n, unsigned *vmask) {
+    *vmask = 0;
+    for (int i = 0; i < n; ++i) {
+        const agd_instance &a = host[i];
+        const char *bad = nullptr;
+        int code = AGD_STATUS_INVALID;
+        if (a.ndim != host[0].ndim) bad = "all instances of a plan must share ndim";
+        else if (insts[i].variant < 0) { bad = "model/tile shape not built"; code = AGD_STATUS_UNSUPPORTED; }
+        else if (a.multip_step != 0.f) { bad = "multiprecision not built"; code = AGD_STATUS_UNSUPPORTED; }
+        else if (!a.values || !a.rhs || !a.seedbits || (a.model == AGD_MODEL_RIEMANN && !a.geom)) bad = "missing array";
+        else if (a.niter_i < 1 || a.fim_front_width < 2 || a.fim_front_width > 255 || a.nitermax_o < 0 ||
+                 a.nitermax_o > kMaxEpochs)
+            bad = "bad niter_i / fim_front_width / nitermax_o (at most 16000)";
+        if (bad) return set_error(code, bad);
+        *vmask |= 1u << insts[i].variant;
+    }
+    return AGD_STATUS_OK;
+}
+
 static int plan_create(const agd_instance *host, int n, agd_plan **out) {
     if (!out) return set_error(AGD_STATUS_INVALID, "null plan pointer");
     *out = nullptr;
@@ -265,38 +285,22 @@ static int plan_create(const agd_instance *host, int n, agd_plan **out) {
         return set_error(AGD_STATUS_INVALID, "bad instance shape");
     }
     P->ndim = host[0].ndim;
-    P->vmask = 0;
-    for (int i = 0; i < n; ++i) {
-        const agd_instance &a = host[i];
-        const char *bad = nullptr;
-        int code = AGD_STATUS_INVALID;
-        if (a.ndim != P->ndim) bad = "all instances of a plan must share ndim";
-        else if (P->insts[i].variant < 0) { bad = "model/tile shape not built"; code = AGD_STATUS_UNSUPPORTED; }
-        else if (a.multip_step != 0.f) { bad = "multiprecision not built"; code = AGD_STATUS_UNSUPPORTED; }
-        else if (!a.values || !a.rhs || !a.seedbits || (a.model == AGD_MODEL_RIEMANN && !a.geom)) bad = "missing array";
-        else if (a.niter_i < 1 || a.fim_front_width < 2 || a.fim_front_width > 255 || a.nitermax_o < 0 ||
-                 a.nitermax_o > kMaxEpochs)
-            bad = "bad niter_i / fim_front_width / nitermax_o (at most 16000)";
-        if (bad) {
-            delete P;
-            return set_error(code, bad);
-        }
-        P->vmask |= 1u << P->insts[i].variant;
+    const int rc = validate(host, P->insts.data(), n, &P->vmask);
+    if (rc != AGD_STATUS_OK) {
+        delete P;
+        return rc;
     }
     *out = P;
     return AGD_STATUS_OK;
 }
 
-static int plan_run(const agd_plan *P, void *ws, size_t ws_bytes, agd_stats *stats, const agd_launch *cfg,
-                    cudaStream_t st) {
-    if (!P || !ws) return set_error(AGD_STATUS_INVALID, "null plan or workspace");
-    const WsLayout &L = P->L;
-    if (ws_bytes < L.total) return set_error(AGD_STATUS_WORKSPACE, "workspace too small");
-    const int n = (int)P->insts.size();
-    const unsigned vmask = P->vmask;
+// The persistent solve for the variants in vmask, on a workspace laid out by L
+// whose descriptors are already uploaded.
+static int run_variants(int ndim, unsigned vmask, const WsLayout &L, void *ws, int n, agd_stats *stats,
+                        const agd_launch *cfg, cudaStream_t st) {
     constexpr unsigned R2 = 1u << V_RIEM2_8, I16 = 1u << V_ISO2_16, I8 = 1u << V_ISO2_8;
     constexpr unsigned R3 = 1u << V_RIEM3_4, I3 = 1u << V_ISO3_4;
-    if (P->ndim == 2) {
+    if (ndim == 2) {
         if (vmask == R2) return run_sched<EikonalVisitor<R2>>(L, ws, n, {}, stats, cfg, st);
         if (vmask == I16) return run_sched<EikonalVisitor<I16>>(L, ws, n, {}, stats, cfg, st);
         if (vmask == I8) return run_sched<EikonalVisitor<I8>>(L, ws, n, {}, stats, cfg, st);
@@ -305,6 +309,14 @@ static int plan_run(const agd_plan *P, void *ws, size_t ws_bytes, agd_stats *sta
     if (vmask == R3) return run_sched<EikonalVisitor<R3>>(L, ws, n, {}, stats, cfg, st);
     if (vmask == I3) return run_sched<EikonalVisitor<I3>>(L, ws, n, {}, stats, cfg, st);
     return run_sched<EikonalVisitor<R3 | I3>>(L, ws, n, {}, stats, cfg, st);
+}
+
+static int plan_run(const agd_plan *P, void *ws, size_t ws_bytes, agd_stats *stats, const agd_launch *cfg,
+                    cudaStream_t st) {
+    if (!P || !ws) return set_error(AGD_STATUS_INVALID, "null plan or workspace");
+    const WsLayout &L = P->L;
+    if (ws_bytes < L.total) return set_error(AGD_STATUS_WORKSPACE, "workspace too small");
+    return run_variants(P->ndim, P->vmask, L, ws, (int)P->insts.size(), stats, cfg, st);
 }
 
 static int plan_upload(const agd_plan *P, void *ws, size_t ws_bytes, cudaStream_t st) {
@@ -615,7 +627,7 @@ int agd_plan_run(const agd_plan *plan, void *workspace, size_t workspace_bytes, 
 
 size_t agd_eikonal_workspace_bytes(const agd_instance *inst, int n) {
     WsLayout L;
-    if (!inst || n <= 0 || !layout(inst, n, L, nullptr)) return 0;
+    if (!inst || n <= 0 || !layout(inst, n, L, static_cast<Inst *>(nullptr))) return 0;
     return L.total;
 }
 

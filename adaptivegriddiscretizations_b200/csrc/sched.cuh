@@ -51,9 +51,8 @@ struct WsLayout {
 static size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
 constexpr long long kMaxWarps = 148 * 64;  // resident warps of a launch, upper bound
 
-static bool layout(const agd_instance *a, int n, WsLayout &L, std::vector<Inst> *out) {
+static bool layout(const agd_instance *a, int n, WsLayout &L, Inst *out) {
     long long tiles = 0;
-    if (out) out->resize(n);
     for (int i = 0; i < n; ++i) {
         Inst I;
         std::memset(&I, 0, sizeof(I));
@@ -72,7 +71,7 @@ static bool layout(const agd_instance *a, int n, WsLayout &L, std::vector<Inst> 
         I.variant = variant_of(a[i]);
         tiles += I.size_o;
         if (tiles > 0x3fffffff) return false;
-        if (out) (*out)[i] = I;
+        if (out) out[i] = I;
     }
     // Queue slots: at most `tiles` entries are outstanding (an instance's current
     // epoch list), plus the tickets held by waiting warps and the exit sentinels.
@@ -93,6 +92,11 @@ static bool layout(const agd_instance *a, int n, WsLayout &L, std::vector<Inst> 
     L.total_tiles = (int)tiles;
     L.qcap = qcap;
     return true;
+}
+
+static bool layout(const agd_instance *a, int n, WsLayout &L, std::vector<Inst> *out) {
+    if (out) out->resize(n);
+    return layout(a, n, L, out ? out->data() : static_cast<Inst *>(nullptr));
 }
 
 // --------------------------------------------------------- kernel context ---
