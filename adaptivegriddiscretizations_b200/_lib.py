@@ -57,6 +57,7 @@ SIGNATURES = {
     "agd_plan_run": (_I, [_P, _P, ctypes.c_size_t, _P, _P, _P]),
     "agd_eikonal_workspace_bytes": (ctypes.c_size_t, [_P, _I]),
     "agd_eikonal_solve": (_I, [_P, _I, _P, ctypes.c_size_t, _P, _P, _P]),
+    "agd_eikonal_solve_fixed_scratch": (_I, [_P, _I, _P, _P, _P]),
     "agd_prep_geom": (_I, [_I, _P, _P, _P, _I, _I, _P, _P, _P]),
     "agd_block_expand": (_I, [_I, _P, _P, _I, _P, _I, ctypes.c_float, _P, _P]),
     "agd_block_squeeze": (_I, [_I, _P, _P, _I, _P, _P, _P]),

@@ -26,6 +26,7 @@
 #include <algorithm>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <vector>
 
 #include "sched.cuh"
@@ -317,6 +318,55 @@ static int plan_run(const agd_plan *P, void *ws, size_t ws_bytes, agd_stats *sta
     const WsLayout &L = P->L;
     if (ws_bytes < L.total) return set_error(AGD_STATUS_WORKSPACE, "workspace too small");
     return run_variants(P->ndim, P->vmask, L, ws, (int)P->insts.size(), stats, cfg, st);
+}
+
+// ------------------------------------------------------- fixed scratch ---
+// Scratch of agd_eikonal_solve_fixed_scratch: a file-scope device array, so that
+// callers which cannot allocate device memory still get a solver.  In host code
+// the name g_fixed_scratch is only a host-side stand-in for the symbol; the
+// device address is obtained once per device with cudaGetSymbolAddress.
+constexpr size_t kFixedScratchBytes = (size_t)AGD_FIXED_SCRATCH_BYTES;
+constexpr int kFixedScratchMaxInstances = AGD_FIXED_SCRATCH_MAX_INSTANCES;
+static __device__ __align__(256) unsigned char g_fixed_scratch[kFixedScratchBytes];
+constexpr int kMaxDevices = 64;
+static void *g_fixed_scratch_addr[kMaxDevices];
+static std::mutex g_fixed_scratch_lock;
+
+static int fixed_scratch_solve(const agd_instance *host, int n, agd_stats *stats, const agd_launch *cfg,
+                               cudaStream_t st) {
+    if (!host || n <= 0) return set_error(AGD_STATUS_INVALID, "no instance");
+    if (n > kFixedScratchMaxInstances)
+        return set_error(AGD_STATUS_INVALID, "agd_eikonal_solve_fixed_scratch: more than "
+                                             "AGD_FIXED_SCRATCH_MAX_INSTANCES instances");
+    int dev = 0;
+    cudaError_t err = cudaGetDevice(&dev);
+    if (err != cudaSuccess) return set_cuda_error("cudaGetDevice", err);
+    if (dev < 0 || dev >= kMaxDevices) return set_error(AGD_STATUS_UNSUPPORTED, "device ordinal too large");
+    void *scratch = nullptr;
+    {
+        std::lock_guard<std::mutex> guard(g_fixed_scratch_lock);
+        if (!g_fixed_scratch_addr[dev]) {  // first call on this device: resolve the array's device address
+            err = cudaGetSymbolAddress(&g_fixed_scratch_addr[dev], g_fixed_scratch);
+            if (err != cudaSuccess) {
+                g_fixed_scratch_addr[dev] = nullptr;
+                return set_cuda_error("cudaGetSymbolAddress(fixed scratch)", err);
+            }
+        }
+        scratch = g_fixed_scratch_addr[dev];
+    }
+    Inst insts[kFixedScratchMaxInstances];
+    WsLayout L;
+    if (!layout(host, n, L, insts)) return set_error(AGD_STATUS_INVALID, "bad instance shape");
+    unsigned vmask = 0;
+    const int rc = validate(host, insts, n, &vmask);
+    if (rc != AGD_STATUS_OK) return rc;
+    if (L.total > kFixedScratchBytes)
+        return set_error(AGD_STATUS_WORKSPACE, "agd_eikonal_solve_fixed_scratch: these instances need more "
+                                               "scratch than AGD_FIXED_SCRATCH_BYTES; use agd_eikonal_solve");
+    // Pageable host source: the call returns once the descriptors are staged.
+    err = cudaMemcpyAsync(static_cast<char *>(scratch) + L.inst, insts, sizeof(Inst) * n, cudaMemcpyHostToDevice, st);
+    if (err != cudaSuccess) return set_cuda_error("descriptor upload", err);
+    return run_variants(host[0].ndim, vmask, L, scratch, n, stats, cfg, st);
 }
 
 static int plan_upload(const agd_plan *P, void *ws, size_t ws_bytes, cudaStream_t st) {
@@ -641,6 +691,12 @@ int agd_eikonal_solve(const agd_instance *inst, int n, void *workspace, size_t w
     if (rc == AGD_STATUS_OK) rc = plan_run(P, workspace, workspace_bytes, stats, launch, (cudaStream_t)stream);
     delete P;
     return rc;
+}
+
+int agd_eikonal_solve_fixed_scratch(const agd_instance *inst, int n, agd_stats *stats, const agd_launch *launch,
+                                    agd_stream_t stream) {
+    clear_error();
+    return fixed_scratch_solve(inst, n, stats, launch, (cudaStream_t)stream);
 }
 
 int agd_flow(const agd_instance *inst, float *flow_vector, float *flow_weightsum, float *flow_weights,

@@ -115,6 +115,28 @@ size_t agd_eikonal_workspace_bytes(const agd_instance *inst, int n);
 int agd_eikonal_solve(const agd_instance *inst, int n, void *workspace, size_t workspace_bytes,
                       agd_stats *stats, const agd_launch *launch, agd_stream_t stream);
 
+/* Same solve as agd_eikonal_solve, for callers that cannot allocate device
+ * memory: code running inside a host application that owns the device
+ * allocator (plugins, sandboxed or budgeted hosts), or that must not call
+ * cudaMalloc at that point.  It takes no workspace: its scratch is a
+ * file-scope device array of AGD_FIXED_SCRATCH_BYTES that every device which
+ * loads the library holds until the process exits.  No counterpart in the
+ * reference, which allocates its work arrays per call.
+ * - Instances needing more scratch than that (the scratch grows with the
+ *   number of tiles: about 200 Riemann2 512^2 or Isotropic2 1024^2 problems
+ *   fit), or more than AGD_FIXED_SCRATCH_MAX_INSTANCES of them, are rejected
+ *   with AGD_STATUS_WORKSPACE / AGD_STATUS_INVALID before any device work.
+ * - The first call on a device looks the array's device address up
+ *   (cudaGetSymbolAddress); make that first call before any stream capture.
+ * - Every call shares the one array, which keeps the last call's contents (the
+ *   solver clears what it needs at zero itself): calls that overlap on the GPU
+ *   race, so issue them on a single stream or otherwise serialise them.
+ * It calls no cudaMalloc, cudaFree or allocating library routine. */
+#define AGD_FIXED_SCRATCH_BYTES (32u << 20)
+#define AGD_FIXED_SCRATCH_MAX_INSTANCES 256
+int agd_eikonal_solve_fixed_scratch(const agd_instance *inst, int n, agd_stats *stats, const agd_launch *launch,
+                                    agd_stream_t stream);
+
 /* ------------------------------------------------------------ preparation -- */
 
 /* Dual metric of metric.with_costs(gridScales) (or of dualMetric.with_speeds)
