@@ -241,8 +241,6 @@ class Interface:
         if self.shape_i not in SUPPORTED_TILES[self.ndim]:
             raise ValueError(f"Unsupported shape_i {self.shape_i} for {self.model}; "
                              f"built tile shapes: {sorted(SUPPORTED_TILES[self.ndim])}")
-        if self.model.startswith("Riemann") and self.ndim == 2 and self.shape_i != (8, 8):
-            raise ValueError("Riemann2 is built with shape_i (8,8)")
         self.traits = traits
         self.values_float64 = self.GetValue("values_float64", default=False,
                                             help="Export values using the float64 data type")

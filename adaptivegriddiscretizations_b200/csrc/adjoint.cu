@@ -152,6 +152,8 @@ struct LinearVisitor {
     struct Smem {
         float l[SIZE];
     };
+    static cudaError_t prepare(const Sched &, const WsLayout &, cudaStream_t) { return cudaSuccess; }
+    static constexpr int kMinCtas = SIZE == 256 ? 4 : 6;
 
     __device__ static void visit(const Sched &S, const Args &A, int t, int ii, int e, int lane, Smem &sm) {
         const Inst &I = S.inst[ii];
@@ -238,7 +240,7 @@ static bool rev_layout(const agd_instance *a, RevLayout &R, std::vector<Inst> *i
     agd_instance b = *a;
     b.flags |= AGD_FLAG_ACTIVATE_ALL;
     b.trigger = nullptr;
-    if (!layout(&b, 1, R.L, insts)) return false;
+    if (!layout(&b, 1, R.L, insts, /*stencil_cache=*/false)) return false;
     const Inst &I = (*insts)[0];
     R.size_tot = I.size_tot;
     R.size_i = I.size_i;

@@ -15,6 +15,10 @@ struct Inst {
     long long size_tot;
     int tile_base;  // first global tile id of this instance in a batched launch
     int variant;    // compiled tile-visit variant, -1 if none
+    // Riemann models: per-point Selling stencil computed once per solve (weights,
+    // then packed offsets, symdim planes each, tile layout), or null to compute
+    // it at every visit.
+    float *stencil;
 };
 
 // Thread-local error message for agd_last_error().

@@ -33,6 +33,68 @@
 
 namespace agd {
 
+// ------------------------------------------------------- stencil cache ---
+// Offsets of the Selling stencil packed in one 32-bit word: two int16 in 2D,
+// three 10-bit signed fields in 3D.
+template <int D>
+__device__ __forceinline__ bool pack_offset(const int *e, int &word) {
+    if (D == 2) {
+        if (e[0] < -32768 || e[0] > 32767 || e[1] < -32768 || e[1] > 32767) return false;
+        word = (e[0] & 0xffff) | (e[1] << 16);
+        return true;
+    }
+    for (int c = 0; c < 3; ++c)
+        if (e[c] < -512 || e[c] > 511) return false;
+    word = (e[0] & 0x3ff) | ((e[1] & 0x3ff) << 10) | ((e[2] & 0x3ff) << 20);
+    return true;
+}
+template <int D>
+__device__ __forceinline__ void unpack_offset(int word, int *e) {
+    if (D == 2) {
+        e[0] = (int)(short)(word & 0xffff);
+        e[1] = word >> 16;
+    } else {
+        e[0] = (word << 22) >> 22;
+        e[1] = (word << 12) >> 22;
+        e[2] = (word << 2) >> 22;
+    }
+}
+
+// Selling stencil of every point of the Riemann instances of a launch, once per
+// solve (the reference recomputes it at each visit, cuda/Riemann_.h:23-29).
+// One warp per tile.
+template <int D>
+__global__ void stencil_kernel(const Inst *insts, int ninst, int total_tiles, Ctrl *ctrl) {
+    constexpr int SD = D * (D + 1) / 2;
+    const int t = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    const int lane = threadIdx.x & 31;
+    if (t >= total_tiles) return;
+    int lo = 0, hi = ninst - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (insts[mid].tile_base <= t) lo = mid; else hi = mid - 1;
+    }
+    const Inst &I = insts[lo];
+    if (!I.stencil) return;
+    const long long base = (long long)(t - I.tile_base) * I.size_i;
+    for (int n_i = lane; n_i < I.size_i; n_i += 32) {
+        const long long n_t = base + n_i;
+        float m[SD], w[SD];
+        int e[SD][3];
+#pragma unroll
+        for (int c = 0; c < SD; ++c) m[c] = __ldg(I.a.geom + (size_t)c * I.size_tot + n_t);
+        if (D == 2) selling2(m, w, e);
+        else selling3(m, w, e);
+#pragma unroll
+        for (int r = 0; r < SD; ++r) {
+            int word = 0;
+            if (!pack_offset<D>(e[r], word)) atomicOr(&ctrl->err, (unsigned)AGD_STATUS_UNSUPPORTED);
+            I.stencil[(size_t)r * I.size_tot + n_t] = w[r];
+            I.stencil[(size_t)(SD + r) * I.size_tot + n_t] = __int_as_float(word);
+        }
+    }
+}
+
 // ------------------------------------------------------------- tile visit ---
 template <class TL, int MODEL>
 struct Visit {
@@ -41,7 +103,15 @@ struct Visit {
     static constexpr int NTOT = 2 * NACT;
     static constexpr int SD = D * (D + 1) / 2;
 
-    // Stencil of the point with bilevel index n_t: weights and offsets.
+    static constexpr int kBoxed = (int)0xffc00000;  // negative quiet NaN: an in-tile index follows
+    __device__ __forceinline__ static float neighbour(float x, const float *us) {
+        const int b = __float_as_int(x);
+        const float inside = us[b & (TL::SIZE - 1)];  // index masked into this warp's tile
+        return (b >> 22) == -1 ? inside : x;
+    }
+
+    // Stencil of the point with bilevel index n_t: weights and offsets, from the
+    // per-solve cache when there is one, else by Selling's decomposition.
     __device__ __forceinline__ static void stencil(const Inst &I, size_t n_t, float *w, int (*e)[3]) {
         if (MODEL == AGD_MODEL_ISOTROPIC) {
 #pragma unroll
@@ -49,6 +119,12 @@ struct Visit {
                 w[k] = I.a.iso_weights[k];
 #pragma unroll
                 for (int c = 0; c < 3; ++c) e[k][c] = (c == k);
+            }
+        } else if (I.stencil) {
+#pragma unroll
+            for (int r = 0; r < SD; ++r) {
+                w[r] = __ldg(I.stencil + (size_t)r * I.size_tot + n_t);
+                unpack_offset<D>(__float_as_int(__ldg(I.stencil + (size_t)(SD + r) * I.size_tot + n_t)), e[r]);
             }
         } else {
             float m[SD];
@@ -93,8 +169,10 @@ struct Visit {
         const size_t base = (size_t)n_o * TL::SIZE;
         float uold[P], rhs[P];
         float wts[P][NACT];
+        // Neighbour of each stencil offset: its value when outside the tile (read
+        // once per visit), or its in-tile index boxed as a negative-NaN payload
+        // (no solution value is a NaN), so one register holds either.
         float nbv[P][NTOT];
-        int nbl[P][NTOT];
         bool seed[P];
 #pragma unroll
         for (int p = 0; p < P; ++p) {
@@ -127,10 +205,8 @@ struct Visit {
                         indom = indom && yt[c] >= 0 && yt[c] < A.shape[c];
                     }
                     if (intile) {
-                        nbl[p][2 * k + s] = TL::local(yi);
-                        nbv[p][2 * k + s] = 0.f;
+                        nbv[p][2 * k + s] = __int_as_float(kBoxed | TL::local(yi));
                     } else {
-                        nbl[p][2 * k + s] = -1;
                         nbv[p][2 * k + s] =
                             indom ? __ldcg(A.values + bilevel_index<D, TL>(yt, I.shape_o)) : finf();
                     }
@@ -148,9 +224,7 @@ struct Visit {
                     float v[NACT], w[NACT];
 #pragma unroll
                     for (int k = 0; k < NACT; ++k) {
-                        const int l0 = nbl[p][2 * k], l1 = nbl[p][2 * k + 1];
-                        const float a = l0 >= 0 ? us[l0] : nbv[p][2 * k];
-                        const float b = l1 >= 0 ? us[l1] : nbv[p][2 * k + 1];
+                        const float a = neighbour(nbv[p][2 * k], us), b = neighbour(nbv[p][2 * k + 1], us);
                         v[k] = a > b ? b : a;
                         w[k] = wts[p][k];
                     }
@@ -227,6 +301,9 @@ __device__ __forceinline__ void dispatch(const Sched &S, int t, int e, int lane,
         case V_RIEM3_4:
             if constexpr ((VMASK >> V_RIEM3_4) & 1) Visit<Tile<3, 4, 4, 4>, AGD_MODEL_RIEMANN>::run(S, I, ii, n_o, e, lane, us);
             break;
+        case V_RIEM2_16:
+            if constexpr ((VMASK >> V_RIEM2_16) & 1) Visit<Tile<2, 16, 16, 1>, AGD_MODEL_RIEMANN>::run(S, I, ii, n_o, e, lane, us);
+            break;
         default:
             break;
     }
@@ -236,12 +313,24 @@ constexpr int kMaxTileSize = 256;
 
 template <unsigned VMASK>
 struct EikonalVisitor {
+    // 256-point tiles keep 8 points per lane in registers: fewer resident warps.
+    static constexpr int kMinCtas = (VMASK & ((1u << V_RIEM2_16) | (1u << V_ISO2_16))) ? 4 : 6;
     struct Args {};
     struct Smem {
         float u[kMaxTileSize];
     };
     __device__ __forceinline__ static void visit(const Sched &S, const Args &, int t, int, int e, int lane, Smem &sm) {
         dispatch<VMASK>(S, t, e, lane, sm.u);
+    }
+    // Before the workers: the Selling stencils of the Riemann instances.
+    static cudaError_t prepare(const Sched &S, const WsLayout &L, cudaStream_t st) {
+        constexpr unsigned kRiemann = (1u << V_RIEM2_8) | (1u << V_RIEM3_4) | (1u << V_RIEM2_16);
+        if (!(VMASK & kRiemann) || L.stencil == L.total) return cudaSuccess;
+        if (VMASK & (1u << V_RIEM3_4))
+            stencil_kernel<3><<<(L.total_tiles + 7) / 8, 256, 0, st>>>(S.inst, S.ninst, L.total_tiles, S.ctrl);
+        else
+            stencil_kernel<2><<<(L.total_tiles + 7) / 8, 256, 0, st>>>(S.inst, S.ninst, L.total_tiles, S.ctrl);
+        return cudaGetLastError();
     }
 };
 
@@ -300,12 +389,13 @@ static int plan_create(const agd_instance *host, int n, agd_plan **out) {
 static int run_variants(int ndim, unsigned vmask, const WsLayout &L, void *ws, int n, agd_stats *stats,
                         const agd_launch *cfg, cudaStream_t st) {
     constexpr unsigned R2 = 1u << V_RIEM2_8, I16 = 1u << V_ISO2_16, I8 = 1u << V_ISO2_8;
-    constexpr unsigned R3 = 1u << V_RIEM3_4, I3 = 1u << V_ISO3_4;
+    constexpr unsigned R3 = 1u << V_RIEM3_4, I3 = 1u << V_ISO3_4, R2L = 1u << V_RIEM2_16;
     if (ndim == 2) {
         if (vmask == R2) return run_sched<EikonalVisitor<R2>>(L, ws, n, {}, stats, cfg, st);
+        if (vmask == R2L) return run_sched<EikonalVisitor<R2L>>(L, ws, n, {}, stats, cfg, st);
         if (vmask == I16) return run_sched<EikonalVisitor<I16>>(L, ws, n, {}, stats, cfg, st);
         if (vmask == I8) return run_sched<EikonalVisitor<I8>>(L, ws, n, {}, stats, cfg, st);
-        return run_sched<EikonalVisitor<R2 | I16 | I8>>(L, ws, n, {}, stats, cfg, st);
+        return run_sched<EikonalVisitor<R2 | I16 | I8 | R2L>>(L, ws, n, {}, stats, cfg, st);
     }
     if (vmask == R3) return run_sched<EikonalVisitor<R3>>(L, ws, n, {}, stats, cfg, st);
     if (vmask == I3) return run_sched<EikonalVisitor<I3>>(L, ws, n, {}, stats, cfg, st);
@@ -356,7 +446,7 @@ static int fixed_scratch_solve(const agd_instance *host, int n, agd_stats *stats
     }
     Inst insts[kFixedScratchMaxInstances];
     WsLayout L;
-    if (!layout(host, n, L, insts)) return set_error(AGD_STATUS_INVALID, "bad instance shape");
+    if (!layout(host, n, L, insts, /*stencil_cache=*/false)) return set_error(AGD_STATUS_INVALID, "bad instance shape");
     unsigned vmask = 0;
     const int rc = validate(host, insts, n, &vmask);
     if (rc != AGD_STATUS_OK) return rc;
@@ -372,8 +462,11 @@ static int fixed_scratch_solve(const agd_instance *host, int n, agd_stats *stats
 static int plan_upload(const agd_plan *P, void *ws, size_t ws_bytes, cudaStream_t st) {
     if (!P || !ws) return set_error(AGD_STATUS_INVALID, "null plan or workspace");
     if (ws_bytes < P->L.total) return set_error(AGD_STATUS_WORKSPACE, "workspace too small");
-    const cudaError_t err = cudaMemcpyAsync(static_cast<char *>(ws) + P->L.inst, P->insts.data(),
-                                            sizeof(Inst) * P->insts.size(), cudaMemcpyHostToDevice, st);
+    std::vector<Inst> insts(P->insts);
+    rebase_stencils(insts.data(), (int)insts.size(), P->L, ws);
+    // pageable source: the call returns once the descriptors are staged
+    const cudaError_t err = cudaMemcpyAsync(static_cast<char *>(ws) + P->L.inst, insts.data(),
+                                            sizeof(Inst) * insts.size(), cudaMemcpyHostToDevice, st);
     return err == cudaSuccess ? AGD_STATUS_OK : set_cuda_error("descriptor upload", err);
 }
 
@@ -464,7 +557,7 @@ __global__ void flow_kernel(Inst I, float *fvec, float *fwsum, float *fw, int *f
 static int flow_impl(const agd_instance *a, float *fvec, float *fwsum, float *fw, int *fidx, cudaStream_t st) {
     WsLayout L;
     std::vector<Inst> v;
-    if (!a || !layout(a, 1, L, &v)) return set_error(AGD_STATUS_INVALID, "bad instance");
+    if (!a || !layout(a, 1, L, &v, /*stencil_cache=*/false)) return set_error(AGD_STATUS_INVALID, "bad instance");
     const Inst &I = v[0];
     const int wpb = 4, grid = (I.size_o + wpb - 1) / wpb;
     switch (I.variant) {
@@ -473,6 +566,7 @@ static int flow_impl(const agd_instance *a, float *fvec, float *fwsum, float *fw
         case V_RIEM2_8: flow_kernel<Tile<2, 8, 8, 1>, AGD_MODEL_RIEMANN><<<grid, wpb * 32, 0, st>>>(I, fvec, fwsum, fw, fidx); break;
         case V_ISO3_4: flow_kernel<Tile<3, 4, 4, 4>, AGD_MODEL_ISOTROPIC><<<grid, wpb * 32, 0, st>>>(I, fvec, fwsum, fw, fidx); break;
         case V_RIEM3_4: flow_kernel<Tile<3, 4, 4, 4>, AGD_MODEL_RIEMANN><<<grid, wpb * 32, 0, st>>>(I, fvec, fwsum, fw, fidx); break;
+        case V_RIEM2_16: flow_kernel<Tile<2, 16, 16, 1>, AGD_MODEL_RIEMANN><<<grid, wpb * 32, 0, st>>>(I, fvec, fwsum, fw, fidx); break;
         default: return set_error(AGD_STATUS_UNSUPPORTED, "model/tile shape not built");
     }
     const cudaError_t err = cudaGetLastError();

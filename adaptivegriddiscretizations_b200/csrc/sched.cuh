@@ -14,11 +14,12 @@
 namespace agd {
 
 // ------------------------------------------------------------- variants ---
-enum Variant { V_ISO2_8 = 0, V_ISO2_16, V_RIEM2_8, V_ISO3_4, V_RIEM3_4, V_COUNT };
+enum Variant { V_ISO2_8 = 0, V_ISO2_16, V_RIEM2_8, V_ISO3_4, V_RIEM3_4, V_RIEM2_16, V_COUNT };
 
 static int variant_of(const agd_instance &a) {
     if (a.ndim == 2) {
         if (a.model == AGD_MODEL_RIEMANN && a.shape_i[0] == 8 && a.shape_i[1] == 8) return V_RIEM2_8;
+        if (a.model == AGD_MODEL_RIEMANN && a.shape_i[0] == 16 && a.shape_i[1] == 16) return V_RIEM2_16;
         if (a.model == AGD_MODEL_ISOTROPIC && a.shape_i[0] == 8 && a.shape_i[1] == 8) return V_ISO2_8;
         if (a.model == AGD_MODEL_ISOTROPIC && a.shape_i[0] == 16 && a.shape_i[1] == 16) return V_ISO2_16;
     } else if (a.ndim == 3 && a.shape_i[0] == 4 && a.shape_i[1] == 4 && a.shape_i[2] == 4) {
@@ -43,7 +44,7 @@ struct Ctrl {
 
 // Workspace: [Inst][InstState][tile_inst][list0][list1][flags][score0][score1][queue][Ctrl][stats]
 struct WsLayout {
-    size_t inst, istate, tile_inst, list0, list1, flags, score0, score1, queue, ctrl, stats, total;
+    size_t inst, istate, tile_inst, list0, list1, flags, score0, score1, queue, ctrl, stats, stencil, total;
     int total_tiles;
     unsigned qcap;
 };
@@ -51,8 +52,8 @@ struct WsLayout {
 static size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
 constexpr long long kMaxWarps = 148 * 64;  // resident warps of a launch, upper bound
 
-static bool layout(const agd_instance *a, int n, WsLayout &L, Inst *out) {
-    long long tiles = 0;
+static bool layout(const agd_instance *a, int n, WsLayout &L, Inst *out, bool stencil_cache = true) {
+    long long tiles = 0, stencil_floats = 0;
     for (int i = 0; i < n; ++i) {
         Inst I;
         std::memset(&I, 0, sizeof(I));
@@ -69,6 +70,11 @@ static bool layout(const agd_instance *a, int n, WsLayout &L, Inst *out) {
         I.size_tot = (long long)I.size_o * I.size_i;
         I.tile_base = (int)tiles;
         I.variant = variant_of(a[i]);
+        I.stencil = nullptr;
+        if (stencil_cache && a[i].model == AGD_MODEL_RIEMANN) {
+            I.stencil = reinterpret_cast<float *>(stencil_floats);  // offset, rebased once the workspace is known
+            stencil_floats += 2ll * (a[i].ndim * (a[i].ndim + 1) / 2) * I.size_tot;
+        }
         tiles += I.size_o;
         if (tiles > 0x3fffffff) return false;
         if (out) out[i] = I;
@@ -88,15 +94,24 @@ static bool layout(const agd_instance *a, int n, WsLayout &L, Inst *out) {
     L.queue = off; off = align256(off + sizeof(unsigned long long) * qcap);
     L.ctrl = off; off = align256(off + sizeof(Ctrl));
     L.stats = off; off = align256(off + sizeof(agd_stats) * n);
+    L.stencil = off; off = align256(off + sizeof(float) * stencil_floats);
     L.total = off;
     L.total_tiles = (int)tiles;
     L.qcap = qcap;
     return true;
 }
 
-static bool layout(const agd_instance *a, int n, WsLayout &L, std::vector<Inst> *out) {
+static bool layout(const agd_instance *a, int n, WsLayout &L, std::vector<Inst> *out, bool stencil_cache = true) {
     if (out) out->resize(n);
-    return layout(a, n, L, out ? out->data() : static_cast<Inst *>(nullptr));
+    return layout(a, n, L, out ? out->data() : static_cast<Inst *>(nullptr), stencil_cache);
+}
+
+// Rebases the stencil offsets recorded by layout() onto the workspace address.
+static void rebase_stencils(Inst *insts, int n, const WsLayout &L, void *ws) {
+    for (int i = 0; i < n; ++i)
+        if (insts[i].stencil)
+            insts[i].stencil = reinterpret_cast<float *>(static_cast<char *>(ws) + L.stencil +
+                                                          reinterpret_cast<size_t>(insts[i].stencil) * sizeof(float));
 }
 
 // --------------------------------------------------------- kernel context ---
@@ -260,9 +275,7 @@ __device__ __forceinline__ unsigned long long take_slot(const Sched &S, unsigned
 // current epoch, and close the epoch when it was the last tile of it.
 // Visitor provides: Args (by value), Smem (per warp), and
 //   static void visit(const Sched&, const Args&, int t, int ii, int e, int lane, Smem&).
-#ifndef AGD_WORKER_MIN_CTAS
-#define AGD_WORKER_MIN_CTAS 6  // resident 4-warp CTAs per SM the register budget must allow
-#endif
+// Visitor::kMinCtas: resident 4-warp CTAs per SM that its register budget must allow.
 constexpr int kSmemInst = 1024;  // instances whose tile bases a CTA keeps in shared memory
 
 // Decrement with acquire-release semantics: publishes this warp's writes and,
@@ -274,7 +287,7 @@ __device__ __forceinline__ int atomic_dec_acq_rel(int *p) {
 }
 
 template <class Visitor, int WPB>
-__global__ void __launch_bounds__(WPB * 32, AGD_WORKER_MIN_CTAS * 4 / WPB) sched_worker(Sched S, typename Visitor::Args VA) {
+__global__ void __launch_bounds__(WPB * 32, Visitor::kMinCtas * 4 / WPB) sched_worker(Sched S, typename Visitor::Args VA) {
     __shared__ typename Visitor::Smem smem[WPB];
     __shared__ int s_base[kSmemInst];  // tile bases, to find a tile's instance without a global load
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -446,6 +459,7 @@ static int run_sched(const WsLayout &L, void *ws, int n, const typename Visitor:
     if (err == cudaSuccess) err = cudaMemsetAsync(w + L.queue, 0xff, L.ctrl - L.queue, st);
     if (err == cudaSuccess) err = cudaMemsetAsync(w + L.ctrl, 0, L.total - L.ctrl, st);
     if (err != cudaSuccess) return set_cuda_error("workspace clear", err);
+    if ((err = Visitor::prepare(S, L, st)) != cudaSuccess) return set_cuda_error("prepare", err);
     setup_tiles<<<(L.total_tiles + 7) / 8, 256, 0, st>>>(S);
     if ((err = cudaGetLastError()) != cudaSuccess) return set_cuda_error("setup_tiles", err);
     publish_first<<<(n + 7) / 8, 256, 0, st>>>(S);

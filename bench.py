@@ -187,6 +187,7 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--niter-i", type=int, default=0, help="local iterations per tile visit (0: the default, 8)")
     ap.add_argument("--front", type=int, default=0, help="FIM front width (0: the default, 4)")
+    ap.add_argument("--tile", type=int, default=8, help="tile side (8: the default, or 16)")
     args = ap.parse_args()
 
     rank = int(os.environ.get("RANK", "0"))
@@ -210,8 +211,8 @@ def main():
     n, B = args.n, args.batch
     metrics, seeds = make_fields(n, B, 1000 + rank)
     traits = {}
-    if args.niter_i:
-        traits["traits"] = {"shape_i": (8, 8), "niter_i": args.niter_i}
+    if args.niter_i or args.tile != 8:
+        traits["traits"] = {"shape_i": (args.tile, args.tile), "niter_i": args.niter_i or 8}
     if args.front:
         traits["fim_front_width"] = args.front
     ins = dictins(metrics, seeds, n, to_device=True, traits=traits)
@@ -236,7 +237,7 @@ def main():
     torch.cuda.synchronize()
     niter, status, visits = plan.read_stats()
     assert not status.any(), f"solver status {status}"
-    updates_per_step = int(visits.sum()) * 64
+    updates_per_step = int(visits.sum()) * args.tile ** 2
 
     evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
     if dist:
@@ -261,7 +262,7 @@ def main():
         elapsed = float(tt)
     niter, status, visits = plan.read_stats()
     assert not status.any()
-    updates_per_step = int(visits.sum()) * 64
+    updates_per_step = int(visits.sum()) * args.tile ** 2
     total_solves = B * args.steps * world
     value = total_solves / elapsed
     hbm, peak_kind = peaks()
@@ -299,7 +300,7 @@ def main():
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": {"workload": f"Riemann2 {n}x{n} cold-start solves, batch {B} per GPU per step, one "
                                    f"persistent launch", "batch_per_gpu": B, "grid": n, "seeds": 4,
-                       "lambda": "U[1,100]", "theta_sigma_px": 8, "tile": "8x8",
+                       "lambda": "U[1,100]", "theta_sigma_px": 8, "tile": f"{args.tile}x{args.tile}",
                        "niter_i": args.niter_i or 8, "fim_front_width": args.front or 4,
                        "grid_updates_per_step": updates_per_step,
                        "grid_updates_per_s": updates_per_step * args.steps * world / elapsed,
