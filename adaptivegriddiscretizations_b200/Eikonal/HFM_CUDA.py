@@ -246,8 +246,6 @@ class Interface:
                                             help="Export values using the float64 data type")
         self.multiprecision = self.values_float64 or self.GetValue(
             "multiprecision", default=False, help="Use multiprecision arithmetic, to improve accuracy")
-        if self.multiprecision:
-            raise NotImplementedError("multiprecision is not available in this build")
         self.factoringRadius = self.GetValue("factoringRadius", default=0,
                                              help="Use source factorization, to improve accuracy")
         if self.factoringRadius:
@@ -344,8 +342,14 @@ class Interface:
                 tol = float(tol)
         self.atol = float(self.GetValue("atol", default=tol, array_float=tuple(),
                                         help="Absolute convergence tolerance for the fixed point solver"))
-        self.rtol = float(self.GetValue("rtol", default=_FLOAT_RES * 5.0, array_float=tuple(),
+        self.rtol = float(self.GetValue("rtol", default=0.0 if self.multiprecision else _FLOAT_RES * 5.0,
+                                        array_float=tuple(),
                                         help="Relative convergence tolerance for the fixed point solver"))
+        if self.multiprecision:
+            # a power of two well below the grid scale (_SetGeometry.py:52-56)
+            hmin = float(np.min(self.h))
+            self.multip_step = float(2.0 ** np.floor(np.log2(hmin / 10)))
+            self.multip_max = float(np.iinfo(np.int32).max * self.multip_step / 2)
         if self.GetValue("walls", default=None, help="Obstacles in the domain") is not None:
             raise NotImplementedError("walls are not available in this build")
 
@@ -354,6 +358,10 @@ class Interface:
         L = _lib.lib()
         values = self.GetValue("values", default=None, array_float=self.shape,
                                help="Initial values for the eikonal solver")
+        self.activateAll = bool(self.GetValue(
+            "activateAll", default=False,
+            help="Visit every tile at the first iteration (for warm starts from an upper bound of the "
+                 "solution; by default only the tiles holding seeds are active at first)"))
         self.values_t = torch.empty(self.size_tot, dtype=torch.float32, device="cuda")
         if values is None:
             self.values_t.fill_(math.inf)
@@ -362,6 +370,11 @@ class Interface:
             _lib.check(L.agd_block_expand(self.ndim, self.c_shape, self.c_shape_i, 1, _lib.ptr(v), 0,
                                           ctypes.c_float(math.inf), _lib.ptr(self.values_t), self.stream),
                        "values")
+        self.valuesq_t = self.values_next_t = self.valuesq_next_t = None
+        if self.multiprecision:  # _SetArgs.py:168-177
+            self.valuesq_t = torch.zeros(self.size_tot, dtype=torch.int32, device="cuda")
+            self.values_next_t = torch.empty_like(self.values_t)
+            self.valuesq_next_t = torch.empty_like(self.valuesq_t)
         self.rhs_t = torch.empty(self.size_tot, dtype=torch.float32, device="cuda")
         c = self.cost.contiguous()
         _lib.check(L.agd_block_expand(self.ndim, self.c_shape, self.c_shape_i, 1, _lib.ptr(c.reshape(-1)),
@@ -402,9 +415,14 @@ class Interface:
         inst.niter_i = self.niter_i
         inst.fim_front_width = self.fim_front_width
         inst.nitermax_o = self.nitermax_o
-        inst.flags = 0
+        inst.flags = _lib.AGD_FLAG_ACTIVATE_ALL if self.activateAll else 0
         inst.atol, inst.rtol = self.atol, self.rtol
         inst.values = self.values_t.data_ptr()
+        if self.multiprecision:
+            inst.multip_step, inst.multip_max = self.multip_step, self.multip_max
+            inst.valuesq = self.valuesq_t.data_ptr()
+            inst.values_next = self.values_next_t.data_ptr()
+            inst.valuesq_next = self.valuesq_next_t.data_ptr()
         inst.geom = self.geom.data_ptr() if self.geom is not None else None
         inst.rhs = self.rhs_t.data_ptr()
         inst.seedbits = self.seedbits.data_ptr()
@@ -445,6 +463,19 @@ class Interface:
             self.Warn(msg)
         self._values = None
 
+    def combine_multiprecision(self):
+        """values + valuesq * multip_step (_PostProcess.py:19-36): float64 output if
+        values_float64, and float32 values for the flow, geodesics and adjoint."""
+        if not self.multiprecision or getattr(self, "_combined", False):
+            return
+        if self.values_float64:
+            u = self.squeeze(self.values_t)
+            q = self.squeeze(self.valuesq_t.float())  # |uq| < 2^24 is exact in float32
+            self._values64 = u.double() + q.double() * self.multip_step
+        self.values_t = self.values_t + self.valuesq_t.float() * np.float32(self.multip_step)
+        self._combined = True
+        self._values = None
+
     def squeeze(self, t, nplanes=1):
         L = _lib.lib()
         out = torch.empty((nplanes,) + self.shape, dtype=torch.float32, device="cuda")
@@ -454,12 +485,16 @@ class Interface:
 
     @property
     def values(self):
+        self.combine_multiprecision()
+        if self.multiprecision and self.values_float64:
+            return self._values64
         if self._values is None:
             self._values = self.squeeze(self.values_t)
         return self._values
 
     def PostProcess(self):
         """Upwind flow, if needed (agd/Eikonal/HFM_CUDA/_PostProcess.py:46-95)."""
+        self.combine_multiprecision()
         self.flow_needed = self.reverseAD or self.hasTips or self.exportGeodesicFlow
         if not self.flow_needed:
             return

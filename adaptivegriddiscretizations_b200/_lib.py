@@ -33,7 +33,8 @@ class AgdInstance(ctypes.Structure):
         ("niter_i", ctypes.c_int), ("fim_front_width", ctypes.c_int), ("nitermax_o", ctypes.c_int),
         ("flags", ctypes.c_int), ("atol", ctypes.c_float), ("rtol", ctypes.c_float),
         ("iso_weights", _c_float3), ("multip_step", ctypes.c_float), ("multip_max", ctypes.c_float),
-        ("values", ctypes.c_void_p), ("valuesq", ctypes.c_void_p), ("geom", ctypes.c_void_p),
+        ("values", ctypes.c_void_p), ("valuesq", ctypes.c_void_p), ("values_next", ctypes.c_void_p),
+        ("valuesq_next", ctypes.c_void_p), ("geom", ctypes.c_void_p),
         ("rhs", ctypes.c_void_p), ("seedbits", ctypes.c_void_p), ("trigger", ctypes.c_void_p),
     ]
 

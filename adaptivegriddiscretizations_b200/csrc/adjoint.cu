@@ -153,6 +153,7 @@ struct LinearVisitor {
         float l[SIZE];
     };
     static cudaError_t prepare(const Sched &, const WsLayout &, cudaStream_t) { return cudaSuccess; }
+    static cudaError_t finalize(const Sched &, const WsLayout &, cudaStream_t) { return cudaSuccess; }
     static constexpr int kMinCtas = SIZE == 256 ? 4 : 6;
 
     __device__ static void visit(const Sched &S, const Args &A, int t, int ii, int e, int lane, Smem &sm) {

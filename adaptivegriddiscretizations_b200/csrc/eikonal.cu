@@ -95,8 +95,36 @@ __global__ void stencil_kernel(const Inst *insts, int ninst, int total_tiles, Ct
     }
 }
 
+// Multiprecision buffers, one warp per tile.  dir 0: first -> second buffers
+// (before the solve); dir 1: second -> first buffers for the instances whose
+// last epoch was odd (after the solve).
+__global__ void mp_copy_kernel(Sched S, int dir) {
+    const int t = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    const int lane = threadIdx.x & 31;
+    if (t >= 0 && S.ninst > 0) {
+        int lo = 0, hi = S.ninst - 1;
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (S.inst[mid].tile_base <= t) lo = mid; else hi = mid - 1;
+        }
+        const Inst &I = S.inst[lo];
+        if (t >= I.tile_base + I.size_o || I.a.multip_step == 0.f) return;
+        if (dir == 1 && (S.stats[lo].niter_o & 1) == 0) return;
+        const long long base = (long long)(t - I.tile_base) * I.size_i;
+        float *uf = dir == 0 ? I.a.values : I.a.values_next, *ut = dir == 0 ? I.a.values_next : I.a.values;
+        int *qf = dir == 0 ? I.a.valuesq : I.a.valuesq_next, *qt = dir == 0 ? I.a.valuesq_next : I.a.valuesq;
+        for (int n_i = lane; n_i < I.size_i; n_i += 32) {
+            ut[base + n_i] = uf[base + n_i];
+            qt[base + n_i] = qf[base + n_i];
+        }
+    }
+}
+
 // ------------------------------------------------------------- tile visit ---
-template <class TL, int MODEL>
+// MP: multiprecision, u + uq * multip_step with uq an int32 (cuda/HFM.h:12-25):
+// Jacobi sweeps inside the tile and double-buffered epochs, as the reference
+// forces strict_iter_i and strict_iter_o with it (_Kernel.py:39-45).
+template <class TL, int MODEL, bool MP = false>
 struct Visit {
     static constexpr int D = TL::D, P = TL::P;
     static constexpr int NACT = MODEL == AGD_MODEL_ISOTROPIC ? D : D * (D + 1) / 2;
@@ -104,6 +132,25 @@ struct Visit {
     static constexpr int SD = D * (D + 1) / 2;
 
     static constexpr int kBoxed = (int)0xffc00000;  // negative quiet NaN: an in-tile index follows
+    // Multiprecision comparison and normalisation (cuda/HFM.h:12-25).
+    __device__ __forceinline__ static bool greater(float u, int uq, float v, int vq, float step) {
+        return u - v > (float)(vq - uq) * step;
+    }
+    __device__ __forceinline__ static void normalize(float &u, int &uq, float umax, float step) {
+        if (u < umax) {
+            const int n = (int)(u / step);
+            u -= (float)n * step;
+            uq += n;
+        }
+    }
+    __device__ __forceinline__ static void neighbour_mp(float x, int xq, const float *us, const int *uqs, float &v,
+                                                        int &vq) {
+        const int b = __float_as_int(x);
+        const bool in = (b >> 22) == -1;
+        const int li = b & (TL::SIZE - 1);
+        v = in ? us[li] : x;
+        vq = in ? uqs[li] : xq;
+    }
     __device__ __forceinline__ static float neighbour(float x, const float *us) {
         const int b = __float_as_int(x);
         const float inside = us[b & (TL::SIZE - 1)];  // index masked into this warp's tile
@@ -167,12 +214,28 @@ struct Visit {
         const int sp_nb = nb >= 0 ? (int)score_at(S, nb, e - 1) : 0;
 
         const size_t base = (size_t)n_o * TL::SIZE;
+        // Epoch e reads buffer (e-1)&1 and writes buffer e&1 with multiprecision.
+        const float *u_in = A.values;
+        float *u_out = A.values;
+        const int *q_in = nullptr;
+        int *q_out = nullptr;
+        const float step = A.multip_step;
+        if constexpr (MP) {
+            const bool odd = (e & 1) != 0;
+            u_in = odd ? A.values : A.values_next;
+            u_out = odd ? A.values_next : A.values;
+            q_in = odd ? A.valuesq : A.valuesq_next;
+            q_out = odd ? A.valuesq_next : A.valuesq;
+        }
+        int *uqs = reinterpret_cast<int *>(us + TL::SIZE);  // integer parts, after the float parts
         float uold[P], rhs[P];
+        int qold[P];
         float wts[P][NACT];
         // Neighbour of each stencil offset: its value when outside the tile (read
         // once per visit), or its in-tile index boxed as a negative-NaN payload
         // (no solution value is a NaN), so one register holds either.
         float nbv[P][NTOT];
+        int nbq[MP ? P : 1][MP ? NTOT : 1];
         bool seed[P];
 #pragma unroll
         for (int p = 0; p < P; ++p) {
@@ -182,10 +245,23 @@ struct Visit {
             TL::pos(n_i, xi);
 #pragma unroll
             for (int k = 0; k < D; ++k) xt[k] = xo[k] * TL::extent(k) + xi[k];
-            uold[p] = __ldcg(A.values + n_t);
+            uold[p] = __ldcg(u_in + n_t);
             seed[p] = (__ldg(A.seedbits + (n_t >> 3)) >> (n_t & 7)) & 1;
             rhs[p] = __ldg(A.rhs + n_t);
-            us[n_i] = seed[p] ? rhs[p] : uold[p];
+            if constexpr (MP) {
+                qold[p] = __ldcg(q_in + n_t);
+                float u0 = uold[p];
+                int q0 = qold[p];
+                if (seed[p]) {
+                    u0 = rhs[p];
+                    q0 = 0;
+                    normalize(u0, q0, A.multip_max, step);
+                }
+                us[n_i] = u0;
+                uqs[n_i] = q0;
+            } else {
+                us[n_i] = seed[p] ? rhs[p] : uold[p];
+            }
             int ev[NACT][3];
             if (seed[p]) continue;  // seeds (and padding) keep their value: no stencil needed
             stencil(I, n_t, wts[p], ev);
@@ -207,8 +283,9 @@ struct Visit {
                     if (intile) {
                         nbv[p][2 * k + s] = __int_as_float(kBoxed | TL::local(yi));
                     } else {
-                        nbv[p][2 * k + s] =
-                            indom ? __ldcg(A.values + bilevel_index<D, TL>(yt, I.shape_o)) : finf();
+                        const int ny = indom ? bilevel_index<D, TL>(yt, I.shape_o) : 0;
+                        nbv[p][2 * k + s] = indom ? __ldcg(u_in + ny) : finf();
+                        if constexpr (MP) nbq[p][2 * k + s] = indom ? __ldcg(q_in + ny) : 0;
                     }
                 }
             }
@@ -216,26 +293,74 @@ struct Visit {
         __syncwarp();
         for (int it = 0; it < A.niter_i; ++it) {
             bool moved = false;
+            if constexpr (MP) {
+                // strict sweeps: every point from the state at the start of the sweep
+                float cand[P];
+                int candq[P];
 #pragma unroll
-            for (int p = 0; p < P; ++p) {
-                const int n_i = lane + 32 * p;
-                float cand = finf();
-                if (!seed[p]) {
+                for (int p = 0; p < P; ++p) {
+                    cand[p] = finf();
+                    candq[p] = 0;
+                    if (seed[p]) continue;
                     float v[NACT], w[NACT];
+                    int vq[NACT];
 #pragma unroll
                     for (int k = 0; k < NACT; ++k) {
-                        const float a = neighbour(nbv[p][2 * k], us), b = neighbour(nbv[p][2 * k + 1], us);
-                        v[k] = a > b ? b : a;
+                        float a, b;
+                        int aq, bq;
+                        neighbour_mp(nbv[p][2 * k], nbq[p][2 * k], us, uqs, a, aq);
+                        neighbour_mp(nbv[p][2 * k + 1], nbq[p][2 * k + 1], us, uqs, b, bq);
+                        const bool take_b = greater(a, aq, b, bq, step);  // HFM.h:52-57
+                        v[k] = take_b ? b : a;
+                        vq[k] = take_b ? bq : aq;
                         w[k] = wts[p][k];
                     }
-                    cand = hfm_update<NACT>(rhs[p], v, w);
+                    int vqmin = kIntMax;  // HFM.h:79-87
+#pragma unroll
+                    for (int k = 0; k < NACT; ++k)
+                        if (v[k] < finf()) vqmin = min(vqmin, vq[k]);
+#pragma unroll
+                    for (int k = 0; k < NACT; ++k) v[k] += (float)(vq[k] - vqmin) * step;
+                    float c = hfm_update<NACT>(rhs[p], v, w);
+                    int cq = vqmin;
+                    if (c == finf()) cq = 0;
+                    else normalize(c, cq, A.multip_max, step);
+                    cand[p] = c;
+                    candq[p] = cq;
                 }
                 __syncwarp();
-                if (!seed[p] && us[n_i] > cand) {
-                    us[n_i] = cand;
-                    moved = true;
+#pragma unroll
+                for (int p = 0; p < P; ++p) {
+                    const int n_i = lane + 32 * p;
+                    if (!seed[p] && greater(us[n_i], uqs[n_i], cand[p], candq[p], step)) {
+                        us[n_i] = cand[p];
+                        uqs[n_i] = candq[p];
+                        moved = true;
+                    }
                 }
                 __syncwarp();
+            } else {
+#pragma unroll
+                for (int p = 0; p < P; ++p) {
+                    const int n_i = lane + 32 * p;
+                    float cand = finf();
+                    if (!seed[p]) {
+                        float v[NACT], w[NACT];
+#pragma unroll
+                        for (int k = 0; k < NACT; ++k) {
+                            const float a = neighbour(nbv[p][2 * k], us), b = neighbour(nbv[p][2 * k + 1], us);
+                            v[k] = a > b ? b : a;
+                            w[k] = wts[p][k];
+                        }
+                        cand = hfm_update<NACT>(rhs[p], v, w);
+                    }
+                    __syncwarp();
+                    if (!seed[p] && us[n_i] > cand) {
+                        us[n_i] = cand;
+                        moved = true;
+                    }
+                    __syncwarp();
+                }
             }
             if (!__any_sync(kFull, moved)) break;
         }
@@ -244,9 +369,18 @@ struct Visit {
         for (int p = 0; p < P; ++p) {
             const int n_i = lane + 32 * p;
             const float u = us[n_i];
-            __stcg(A.values + base + n_i, u);
-            const float diff = fabsf(uold[p] - u);
-            const float tol = A.atol + A.rtol * fabsf(u);
+            __stcg(u_out + base + n_i, u);
+            float diff, uabs;
+            if constexpr (MP) {
+                const int q = uqs[n_i];
+                __stcg(q_out + base + n_i, q);
+                diff = fabsf(uold[p] - u + (float)(qold[p] - q) * step);  // Update.h:212-216
+                uabs = fabsf(u + (float)q * step);
+            } else {
+                diff = fabsf(uold[p] - u);
+                uabs = fabsf(u);
+            }
+            const float tol = A.atol + A.rtol * uabs;
             if (!(isnan(diff) || diff <= tol)) notconv = true;
         }
         const bool changed = __any_sync(kFull, notconv);
@@ -304,6 +438,21 @@ __device__ __forceinline__ void dispatch(const Sched &S, int t, int e, int lane,
         case V_RIEM2_16:
             if constexpr ((VMASK >> V_RIEM2_16) & 1) Visit<Tile<2, 16, 16, 1>, AGD_MODEL_RIEMANN>::run(S, I, ii, n_o, e, lane, us);
             break;
+        case V_ISO2_8_MP:
+            if constexpr ((VMASK >> V_ISO2_8_MP) & 1) Visit<Tile<2, 8, 8, 1>, AGD_MODEL_ISOTROPIC, true>::run(S, I, ii, n_o, e, lane, us);
+            break;
+        case V_ISO2_16_MP:
+            if constexpr ((VMASK >> V_ISO2_16_MP) & 1) Visit<Tile<2, 16, 16, 1>, AGD_MODEL_ISOTROPIC, true>::run(S, I, ii, n_o, e, lane, us);
+            break;
+        case V_RIEM2_8_MP:
+            if constexpr ((VMASK >> V_RIEM2_8_MP) & 1) Visit<Tile<2, 8, 8, 1>, AGD_MODEL_RIEMANN, true>::run(S, I, ii, n_o, e, lane, us);
+            break;
+        case V_ISO3_4_MP:
+            if constexpr ((VMASK >> V_ISO3_4_MP) & 1) Visit<Tile<3, 4, 4, 4>, AGD_MODEL_ISOTROPIC, true>::run(S, I, ii, n_o, e, lane, us);
+            break;
+        case V_RIEM3_4_MP:
+            if constexpr ((VMASK >> V_RIEM3_4_MP) & 1) Visit<Tile<3, 4, 4, 4>, AGD_MODEL_RIEMANN, true>::run(S, I, ii, n_o, e, lane, us);
+            break;
         default:
             break;
     }
@@ -314,22 +463,33 @@ constexpr int kMaxTileSize = 256;
 template <unsigned VMASK>
 struct EikonalVisitor {
     // 256-point tiles keep 8 points per lane in registers: fewer resident warps.
-    static constexpr int kMinCtas = (VMASK & ((1u << V_RIEM2_16) | (1u << V_ISO2_16))) ? 4 : 6;
+    static constexpr int kMinCtas =
+        (VMASK & ((1u << V_RIEM2_16) | (1u << V_ISO2_16) | (1u << V_ISO2_16_MP))) ? 4 : 6;
     struct Args {};
     struct Smem {
-        float u[kMaxTileSize];
+        float u[2 * kMaxTileSize];  // values, then the integer parts with multiprecision
     };
     __device__ __forceinline__ static void visit(const Sched &S, const Args &, int t, int, int e, int lane, Smem &sm) {
         dispatch<VMASK>(S, t, e, lane, sm.u);
     }
-    // Before the workers: the Selling stencils of the Riemann instances.
+    // Before the workers: the second buffers of multiprecision instances start
+    // as copies of the first (_SetArgs.py:171-177), and the Selling stencils of
+    // the Riemann instances are computed.
     static cudaError_t prepare(const Sched &S, const WsLayout &L, cudaStream_t st) {
-        constexpr unsigned kRiemann = (1u << V_RIEM2_8) | (1u << V_RIEM3_4) | (1u << V_RIEM2_16);
-        if (!(VMASK & kRiemann) || L.stencil == L.total) return cudaSuccess;
-        if (VMASK & (1u << V_RIEM3_4))
+        constexpr unsigned kRiemann = (1u << V_RIEM2_8) | (1u << V_RIEM3_4) | (1u << V_RIEM2_16) |
+                                      (1u << V_RIEM2_8_MP) | (1u << V_RIEM3_4_MP);
+        if (VMASK & kMpVariants) mp_copy_kernel<<<(L.total_tiles + 7) / 8, 256, 0, st>>>(S, 0);
+        if (!(VMASK & kRiemann) || L.stencil == L.total) return cudaGetLastError();
+        if (VMASK & ((1u << V_RIEM3_4) | (1u << V_RIEM3_4_MP)))
             stencil_kernel<3><<<(L.total_tiles + 7) / 8, 256, 0, st>>>(S.inst, S.ninst, L.total_tiles, S.ctrl);
         else
             stencil_kernel<2><<<(L.total_tiles + 7) / 8, 256, 0, st>>>(S.inst, S.ninst, L.total_tiles, S.ctrl);
+        return cudaGetLastError();
+    }
+    // After the workers: an instance that ran an odd number of epochs has its
+    // result in the second buffers (the reference swaps its argument names).
+    static cudaError_t finalize(const Sched &S, const WsLayout &L, cudaStream_t st) {
+        if (VMASK & kMpVariants) mp_copy_kernel<<<(L.total_tiles + 7) / 8, 256, 0, st>>>(S, 1);
         return cudaGetLastError();
     }
 };
@@ -354,7 +514,8 @@ static int validate(const agd_instance *host, const Inst *insts, int n, unsigned
         int code = AGD_STATUS_INVALID;
         if (a.ndim != host[0].ndim) bad = "all instances of a plan must share ndim";
         else if (insts[i].variant < 0) { bad = "model/tile shape not built"; code = AGD_STATUS_UNSUPPORTED; }
-        else if (a.multip_step != 0.f) { bad = "multiprecision not built"; code = AGD_STATUS_UNSUPPORTED; }
+        else if (a.multip_step != 0.f && (!a.valuesq || !a.values_next || !a.valuesq_next || !(a.multip_step > 0.f)))
+            bad = "multiprecision needs valuesq, values_next, valuesq_next and multip_step > 0";
         else if (!a.values || !a.rhs || !a.seedbits || (a.model == AGD_MODEL_RIEMANN && !a.geom)) bad = "missing array";
         else if (a.niter_i < 1 || a.fim_front_width < 2 || a.fim_front_width > 255 || a.nitermax_o < 0 ||
                  a.nitermax_o > kMaxEpochs)
@@ -390,6 +551,15 @@ static int run_variants(int ndim, unsigned vmask, const WsLayout &L, void *ws, i
                         const agd_launch *cfg, cudaStream_t st) {
     constexpr unsigned R2 = 1u << V_RIEM2_8, I16 = 1u << V_ISO2_16, I8 = 1u << V_ISO2_8;
     constexpr unsigned R3 = 1u << V_RIEM3_4, I3 = 1u << V_ISO3_4, R2L = 1u << V_RIEM2_16;
+    constexpr unsigned MP2 = (1u << V_ISO2_8_MP) | (1u << V_ISO2_16_MP) | (1u << V_RIEM2_8_MP);
+    constexpr unsigned MP3 = (1u << V_ISO3_4_MP) | (1u << V_RIEM3_4_MP);
+    if (vmask & kMpVariants) {
+        if (ndim == 2) {
+            if (vmask == (1u << V_RIEM2_8_MP)) return run_sched<EikonalVisitor<(1u << V_RIEM2_8_MP)>>(L, ws, n, {}, stats, cfg, st);
+            return run_sched<EikonalVisitor<R2 | I16 | I8 | R2L | MP2>>(L, ws, n, {}, stats, cfg, st);
+        }
+        return run_sched<EikonalVisitor<R3 | I3 | MP3>>(L, ws, n, {}, stats, cfg, st);
+    }
     if (ndim == 2) {
         if (vmask == R2) return run_sched<EikonalVisitor<R2>>(L, ws, n, {}, stats, cfg, st);
         if (vmask == R2L) return run_sched<EikonalVisitor<R2L>>(L, ws, n, {}, stats, cfg, st);
@@ -560,7 +730,7 @@ static int flow_impl(const agd_instance *a, float *fvec, float *fwsum, float *fw
     if (!a || !layout(a, 1, L, &v, /*stencil_cache=*/false)) return set_error(AGD_STATUS_INVALID, "bad instance");
     const Inst &I = v[0];
     const int wpb = 4, grid = (I.size_o + wpb - 1) / wpb;
-    switch (I.variant) {
+    switch (base_variant_of(I.a)) {
         case V_ISO2_8: flow_kernel<Tile<2, 8, 8, 1>, AGD_MODEL_ISOTROPIC><<<grid, wpb * 32, 0, st>>>(I, fvec, fwsum, fw, fidx); break;
         case V_ISO2_16: flow_kernel<Tile<2, 16, 16, 1>, AGD_MODEL_ISOTROPIC><<<grid, wpb * 32, 0, st>>>(I, fvec, fwsum, fw, fidx); break;
         case V_RIEM2_8: flow_kernel<Tile<2, 8, 8, 1>, AGD_MODEL_RIEMANN><<<grid, wpb * 32, 0, st>>>(I, fvec, fwsum, fw, fidx); break;

@@ -14,9 +14,31 @@
 namespace agd {
 
 // ------------------------------------------------------------- variants ---
-enum Variant { V_ISO2_8 = 0, V_ISO2_16, V_RIEM2_8, V_ISO3_4, V_RIEM3_4, V_RIEM2_16, V_COUNT };
+enum Variant {
+    V_ISO2_8 = 0, V_ISO2_16, V_RIEM2_8, V_ISO3_4, V_RIEM3_4, V_RIEM2_16,
+    // multiprecision
+    V_ISO2_8_MP, V_ISO2_16_MP, V_RIEM2_8_MP, V_ISO3_4_MP, V_RIEM3_4_MP, V_COUNT
+};
+constexpr unsigned kMpVariants = (1u << V_ISO2_8_MP) | (1u << V_ISO2_16_MP) | (1u << V_RIEM2_8_MP) |
+                                 (1u << V_ISO3_4_MP) | (1u << V_RIEM3_4_MP);
+
+static int base_variant_of(const agd_instance &a);
 
 static int variant_of(const agd_instance &a) {
+    const int v = base_variant_of(a);
+    if (v < 0 || a.multip_step == 0.f) return v;
+    switch (v) {
+        case V_ISO2_8: return V_ISO2_8_MP;
+        case V_ISO2_16: return V_ISO2_16_MP;
+        case V_RIEM2_8: return V_RIEM2_8_MP;
+        case V_ISO3_4: return V_ISO3_4_MP;
+        case V_RIEM3_4: return V_RIEM3_4_MP;
+        default: return -1;  // no multiprecision build of this tile shape
+    }
+}
+
+// The variant without multiprecision.
+static int base_variant_of(const agd_instance &a) {
     if (a.ndim == 2) {
         if (a.model == AGD_MODEL_RIEMANN && a.shape_i[0] == 8 && a.shape_i[1] == 8) return V_RIEM2_8;
         if (a.model == AGD_MODEL_RIEMANN && a.shape_i[0] == 16 && a.shape_i[1] == 16) return V_RIEM2_16;
@@ -467,6 +489,7 @@ static int run_sched(const WsLayout &L, void *ws, int n, const typename Visitor:
     const int rc = (cfg && cfg->warps_per_cta == 8) ? launch_workers<Visitor, 8>(S, VA, L.total_tiles, cfg, st)
                                                     : launch_workers<Visitor, 4>(S, VA, L.total_tiles, cfg, st);
     if (rc != AGD_STATUS_OK) return rc;
+    if ((err = Visitor::finalize(S, L, st)) != cudaSuccess) return set_cuda_error("finalize", err);
     finish_stats<<<(n + 127) / 128, 128, 0, st>>>(S, stats);
     if ((err = cudaGetLastError()) != cudaSuccess) return set_cuda_error("finish_stats", err);
     return AGD_STATUS_OK;

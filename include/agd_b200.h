@@ -55,10 +55,13 @@ typedef struct agd_instance {
     int flags;          /* AGD_FLAG_* */
     float atol, rtol;   /* per-point convergence: |du| <= atol + rtol |u| */
     float iso_weights[3]; /* isotropic model: gridScale^-2 per axis */
-    float multip_step;  /* multiprecision: u + uq * multip_step (0: off) */
+    float multip_step;  /* multiprecision: u + uq * multip_step (0: off); on output the
+                           solution is values + valuesq * multip_step */
     float multip_max;
     float *values;      /* tile layout, in: initial values (+inf cold), out: solution */
     int32_t *valuesq;   /* tile layout, multiprecision integer part (or NULL) */
+    float *values_next; /* multiprecision: second buffers of the double-buffered */
+    int32_t *valuesq_next; /*  iterations (valuesNext, valuesqNext of _SetArgs.py:171-177) */
     const float *geom;  /* Riemann: dual metric, symdim planes, tile layout (else NULL) */
     const float *rhs;   /* tile layout: cost, seed values at seeds, +inf padding */
     const uint8_t *seedbits; /* tile layout bits, little endian, padding bits set */

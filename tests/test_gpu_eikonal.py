@@ -118,3 +118,39 @@ def test_selling_gpu_bitexact(nd):
     mnorm = np.abs(f["m"]).sum(axis=1, keepdims=True) * 2
     b2 = np.maximum((f["ref_e"].astype(np.float64) ** 2).sum(axis=2).max(axis=1, keepdims=True), 1)
     assert (np.abs(wg - wr) <= 4 * np.finfo(np.float32).eps * b2 * mnorm).all()
+
+
+def test_multiprecision_vs_reference():
+    """Multiprecision (u + uq * multip_step): against the reference's own
+    multiprecision solution.  Its stopping test is absolute (rtol = 0, atol =
+    5e-6 * mean cost), so the bound is absolute: two tolerances."""
+    case, ref = load_case("riem2_mp")
+    out = make_dictin(case, extra={"exportValues": True, "multiprecision": True}).Run()
+    v = out["values"].cpu().numpy()
+    want = ref["values"]
+    fin = np.isfinite(want)
+    assert np.array_equal(fin, np.isfinite(v))
+    assert np.abs(v[fin] - want[fin]).max() <= 2 * float(ref["atol"])
+    assert out["keys"]["default"]["rtol"] == 0.0
+
+
+@pytest.mark.parametrize("name", ["iso2", "riem3", "iso3"])
+def test_multiprecision_vs_float64_oracle(name):
+    case, _ = load_case(name)
+    case = {k: v for k, v in case.items() if k not in ("tips", "sensitivity")}
+    out = make_dictin(case, extra={"exportValues": True, "multiprecision": True}).Run()
+    v = out["values"].cpu().numpy().astype(np.float64)
+    r64 = O.run(case, np.float64)["values"]
+    fin = np.isfinite(r64)
+    atol = 5e-6 * float(np.mean(case.get("cost", 1.0)))
+    assert np.abs(v[fin] - r64[fin]).max() <= 4 * atol
+
+
+def test_values_float64():
+    case, ref = load_case("riem2_mp")
+    out = make_dictin(case, extra={"exportValues": True, "values_float64": True}).Run()
+    v = out["values"]
+    assert v.dtype == torch.float64
+    want = ref["values"]
+    fin = np.isfinite(want)
+    assert np.abs(v.cpu().numpy()[fin] - want[fin]).max() <= 2 * float(ref["atol"])
