@@ -179,7 +179,7 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--batch", type=int, default=64)
+    ap.add_argument("--batch", type=int, default=128)
     ap.add_argument("--n", type=int, default=512)
     ap.add_argument("--ctas", type=int, default=0)
     ap.add_argument("--wpc", type=int, default=4)
@@ -335,7 +335,7 @@ def main():
                          "frac": achieved / hbm, "traffic": None, "peak_kind": peak_kind,
                          "kernel": "eikonal_persistent", "kernel_ms": float(kern.mean() * 1000),
                          "bytes_per_update": BYTES_PER_UPDATE["Riemann2"]},
-            "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": 3 * args.steps,
+            "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": 5 * args.steps,
             "clocks": clk.summary(),
         }
         print(json.dumps(line), flush=True)
