@@ -22,8 +22,28 @@ _singleOut = {"geodesic": "geodesics"}
 _modes = ("gpu", "gpu_transfer")
 
 
+# Fields of at most this many entries keep a host copy taken when they are
+# assigned, so that reading them back (domain shape, grid scales, seeds) needs
+# no device-to-host copy and no wait for the device.
+_SHADOW_MAX = 4096
+
+
 def _is_array(x):
     return isinstance(x, (np.ndarray, torch.Tensor))
+
+
+def _host_copy(x):
+    """float32 numpy copy of a small host-side value; None for device tensors
+    (reading them would wait for the device) and for large arrays."""
+    if isinstance(x, torch.Tensor):
+        if x.device.type != "cpu" or x.numel() > _SHADOW_MAX:
+            return None
+        return x.detach().numpy().astype(np.float32, copy=True)
+    try:
+        a = np.asarray(x, dtype=np.float32)
+    except (TypeError, ValueError):
+        return None
+    return a.copy() if a.size <= _SHADOW_MAX else None
 
 
 class dictOut(MutableMapping):
@@ -88,6 +108,7 @@ class dictIn(MutableMapping):
         if store is None:
             store = {}
         self.store = {"arrayOrdering": "RowMajor"}
+        self._shadow = {}
         mode = store.get("mode", dictIn.default_mode)
         if mode not in _modes:
             raise ValueError(f"Unsupported mode {mode!r}: this solver runs on the GPU (modes {_modes})")
@@ -111,14 +132,16 @@ class dictIn(MutableMapping):
     def array_float_caster(self, x):
         if self.mode == "gpu":
             if isinstance(x, torch.Tensor):
-                return x.to(device="cuda", dtype=torch.float32)
+                return x.to(device="cuda", dtype=torch.float32, non_blocking=x.is_pinned())
             return torch.as_tensor(np.asarray(x, dtype=np.float32), device="cuda")
         if isinstance(x, torch.Tensor):
             x = x.detach().cpu().numpy()
         return np.asarray(x, dtype=np.float32)
 
     def __copy__(self):
-        return dictIn(self.store.copy())
+        other = dictIn(self.store.copy())
+        other._shadow = {k: v for k, v in self._shadow.items() if other.store.get(k) is v[0]}
+        return other
 
     def copy(self):
         return self.__copy__()
@@ -136,10 +159,15 @@ class dictIn(MutableMapping):
             raise ValueError(f"Key {key} is readonly (set at init)")
         if key in _singleIn:
             key, value = _singleIn[key], [value]
-        if key in _array_float_fields and not _is_array(value):
+        if key in _array_float_fields:
+            host = _host_copy(value)
             value = self.array_float_caster(value)
-        elif key in _array_float_fields:
-            value = self.array_float_caster(value)
+            if host is not None:
+                self._shadow[key] = (value, host)
+            else:
+                self._shadow.pop(key, None)
+        else:
+            self._shadow.pop(key, None)
         self.store[key] = value
 
     def __getitem__(self, key):
@@ -151,7 +179,9 @@ class dictIn(MutableMapping):
         return self.store[key]
 
     def __delitem__(self, key):
-        del self.store[_singleIn.get(key, key)]
+        key = _singleIn.get(key, key)
+        del self.store[key]
+        self._shadow.pop(key, None)
 
     def __iter__(self):
         return iter(self.store)
@@ -161,6 +191,16 @@ class dictIn(MutableMapping):
 
     def keys(self):
         return self.store.keys()
+
+    def host(self, key):
+        """numpy copy of a stored field.  Small fields answer from the copy
+        taken when they were assigned (an in-place change of the stored device
+        tensor after that is not seen); others are read back from the device."""
+        value = self.store[key]
+        shadow = self._shadow.get(key)
+        if shadow is not None and shadow[0] is value:
+            return shadow[1]
+        return self._np(value)
 
     def RunHelp(self, mode=None):
         from . import HFM_CUDA
@@ -191,7 +231,7 @@ class dictIn(MutableMapping):
 
     @property
     def shape(self):
-        dims = self._np(self["dims"])
+        dims = self.host("dims")
         return tuple(int(round(float(d))) for d in dims)
 
     @property
@@ -209,20 +249,20 @@ class dictIn(MutableMapping):
     @property
     def gridScales(self):
         if "gridScales" in self:
-            return self._np(self["gridScales"]).astype(np.float32)
-        return np.full(self.vdim, float(self._np(self["gridScale"])), np.float32)
+            return self.host("gridScales").astype(np.float32)
+        return np.full(self.vdim, float(self.host("gridScale")), np.float32)
 
     @property
     def corners(self):
         h = self.gridScales
-        dims = self._np(self["dims"]).astype(np.float32)
-        origin = self._np(self.get("origin", np.zeros_like(dims))).astype(np.float32)
+        dims = self.host("dims").astype(np.float32)
+        origin = self.host("origin").astype(np.float32) if "origin" in self else np.zeros_like(dims)
         return origin, origin + h * dims
 
     def Axes(self, dims=None):
         bottom, top = self.corners
         if dims is None:
-            dims = self._np(self["dims"])
+            dims = self.host("dims")
         return [np.asarray(CenteredLinspace(b, t, d), np.float32) for b, t, d in zip(bottom, top, dims)]
 
     def Grid(self, dims=None):

@@ -133,7 +133,8 @@ class BatchPlan:
 
 def _to_tensor(x, dtype=torch.float32):
     if isinstance(x, torch.Tensor):
-        return x.to(device="cuda", dtype=dtype)
+        # a copy from page-locked host memory is queued without waiting for it
+        return x.to(device="cuda", dtype=dtype, non_blocking=x.is_pinned())
     return torch.as_tensor(np.asarray(x, dtype=np.float32 if dtype == torch.float32 else None), device="cuda",
                            dtype=dtype)
 
@@ -160,7 +161,7 @@ class Interface:
         self.model = self.GetValue("model", help="Minimal path model to be solved.")
         if self.model not in DEFAULT_TRAITS:
             raise ValueError(f"Unsupported model {self.model!r}; supported: {sorted(DEFAULT_TRAITS)}")
-        self.ndim = len(np.asarray(_host(hfmIn["dims"])).reshape(-1))
+        self.ndim = len(np.asarray(hfmIn.host("dims")).reshape(-1))
         if self.ndim != int(self.model[-1]):
             raise ValueError(f"Model {self.model} expects {self.model[-1]} dimensions, got dims of length {self.ndim}")
         self.stats = {"eikonal": {}, "flow": {}, "geodesic": {}, "reverseAD": {}}
@@ -317,6 +318,7 @@ class Interface:
                                   help="Tips from which to compute the minimal geodesics")
         self.hasTips = self.tips is not None
 
+        mean_cost = None
         if self.HasValue("speed"):
             cost = 1.0 / self.GetValue("speed", array_float=True, help="speed = 1/cost (scales the metric, accepts AD)")
         else:
@@ -324,6 +326,7 @@ class Interface:
                                  help="cost = 1/speed (scales the metric, accepts AD)")
             if cost is None:
                 cost = torch.ones((), dtype=torch.float32, device="cuda")
+                mean_cost = 1.0
         cost = cost.to(torch.float32)
         if cost.dim() != 0 and tuple(cost.shape) != self.shape:
             raise ValueError(f"Field cost has incorrect dimensions. Found {tuple(cost.shape)}, "
@@ -335,7 +338,8 @@ class Interface:
             tol = self.GetValue("tol", default="_Dummy", array_float=tuple(),
                                 help="Convergence tolerance for the fixed point solver (determines atol, rtol)")
             if isinstance(tol, str) and tol == "_Dummy":
-                mean_cost = float(torch.nanmean(cost.float())) if cost.dim() else float(cost)
+                if mean_cost is None:
+                    mean_cost = float(torch.nanmean(cost.float())) if cost.dim() else float(cost)
                 tol = np.float32(mean_cost * _FLOAT_RES * 5.0)
                 self.hfmOut["keys"]["default"]["tol"] = np.float32(tol)
             else:
@@ -391,14 +395,15 @@ class Interface:
                                    help="Spread the seeds over a radius given in pixels, so as to improve accuracy.")
         if seedRadius:
             raise NotImplementedError("seedRadius spreading is not available in this build")
-        ci = self.hfmIn.PointFromIndex(_host(seeds), to=True)
+        seeds_h = self.hfmIn.host("seeds").reshape(-1, self.ndim)
+        ci = self.hfmIn.PointFromIndex(seeds_h, to=True)
         idx = np.round(ci).astype(np.int64)
         inside = np.all((idx >= 0) & (idx < np.array(self.shape)), axis=1)
         if not np.all(inside):
-            raise ValueError(f"Seeds outside the domain: {np.asarray(_host(seeds))[~inside].tolist()}")
+            raise ValueError(f"Seeds outside the domain: {np.asarray(seeds_h)[~inside].tolist()}")
         self.seedIndices = idx
         self.seed_values = seedValues.contiguous().float()
-        self.seed_idx_t = torch.as_tensor(idx.astype(np.int32), device="cuda").contiguous()
+        self.seed_idx_t = torch.from_numpy(idx.astype(np.int32)).pin_memory().to("cuda", non_blocking=True)
         self.seedbits = torch.empty(self.size_tot // 8, dtype=torch.uint8, device="cuda")
         _lib.check(L.agd_prep_seeds(self.ndim, self.c_shape, self.c_shape_i, _lib.ptr(self.seed_idx_t),
                                     _lib.ptr(self.seed_values), len(idx), _lib.ptr(self.rhs_t),
@@ -632,12 +637,6 @@ class Interface:
         self.hfmOut["keys"]["unused"] = list(set(self.hfmIn.keys()) - set(self.hfmOut["keys"]["used"]))
         if self.verbosity >= 1 and self.hfmOut["keys"]["unused"]:
             print(f"!! Warning !! Unused keys from user : {self.hfmOut['keys']['unused']}")
-
-
-def _host(x):
-    if isinstance(x, torch.Tensor):
-        return x.detach().cpu().numpy()
-    return x
 
 
 def _metric_hfm(src, ndim):
