@@ -1,0 +1,311 @@
+"""Repeated batched solves of one problem configuration (the serving path).
+
+A template dictIn fixes the model, the grid, the tile traits, the tolerances and
+the solver options; every submission brings the per-instance data of a batch
+(metrics or costs, seeds, seed values) as arrays with a leading batch axis.
+Device buffers and the solver plan are made once.  A submission queues on its
+own CUDA stream: the upload of the host inputs (without blocking the host when
+they are page-locked), two batched preparation kernels (agd_prep_batch), the
+persistent solve (agd_plan_run), the reordering of the values into grid order
+(agd_block_squeeze) and, when a host buffer is given, their copy back.  Buffer
+sets alternate, so the host submits batch k+1 while the device solves batch k.
+
+The reference solves one dictIn per Run() call (agd/Eikonal/HFM_CUDA/__init__.py:10-25)
+and has no counterpart of this class; the values are the ones RunGPU returns for
+the same inputs (same keys, defaults and tolerances, read from the template by
+the Interface of HFM_CUDA).  Only the values are produced: flow, geodesics and
+sensitivities go through RunGPU / RunBatch.
+"""
+import ctypes
+import warnings
+
+import numpy as np
+import torch
+
+from .. import _lib
+from .HFM_CUDA import Interface, _FLOAT_RES
+
+
+class _Buffers:
+    """Device buffers, plan workspace and stream of one in-flight batch."""
+
+    def __init__(self, solver):
+        s = solver
+        self.stream = torch.cuda.Stream()
+        with torch.cuda.stream(self.stream):  # owned by this stream for the allocator
+            dev = dict(dtype=torch.float32, device="cuda")
+            self.geom = torch.empty((s.batch, s.symdim * s.size_tot), **dev) if s.riemann else None
+            self.rhs = torch.empty((s.batch, s.size_tot), **dev)
+            self.values = torch.empty((s.batch, s.size_tot), **dev)
+            self.seedbits = torch.empty((s.batch, s.size_tot // 8), dtype=torch.uint8, device="cuda")
+            self.out = torch.empty((s.batch,) + s.shape, **dev)
+            self.stats = torch.zeros((s.batch, 2), dtype=torch.int64, device="cuda")
+            self.bad = torch.zeros(1, dtype=torch.int32, device="cuda")
+        self.stats_host = torch.empty((s.batch, 2), dtype=torch.int64).pin_memory()
+        self.bad_host = torch.empty(1, dtype=torch.int32).pin_memory()
+        self.metric = self.cost = self.seed_index = self.seed_values = None  # staging, made on first use
+        self.plan = None
+        self.plan_atol = None
+        self.ws = None
+        self.job = None
+
+    def staging(self, name, shape, dtype=torch.float32):
+        """Device staging tensor for an input, reused while its shape holds."""
+        t = getattr(self, name)
+        if t is None or tuple(t.shape) != tuple(shape) or t.dtype != dtype:
+            with torch.cuda.stream(self.stream):
+                t = torch.empty(shape, dtype=dtype, device="cuda")
+            setattr(self, name, t)
+        return t
+
+
+class SolverJob:
+    """A batch submitted to a BatchSolver; `result()` waits for it."""
+
+    def __init__(self, solver, buf, out):
+        self.solver, self.buf, self.out = solver, buf, out
+        self.event = torch.cuda.Event()
+        self.event.record(buf.stream)
+        self.stream = buf.stream
+        self._done = False
+        self.niter_o = self.tile_visits = None
+
+    def done(self):
+        return self.event.query()
+
+    def result(self):
+        """Values of the batch, shape (batch, *grid shape): the host buffer given to
+        submit(), else a device tensor that stays valid until this buffer set is
+        reused (after the solver's `nbuffers` next submissions)."""
+        self.event.synchronize()
+        if not self._done:
+            self._done = True
+            s = self.buf.stats_host.numpy()
+            self.niter_o = (s[:, 0] & 0xffffffff).astype(np.int64)
+            status = ((s[:, 0] >> 32) & 0xffffffff).astype(np.int64)
+            self.tile_visits = s[:, 1].copy()
+            if int(self.buf.bad_host[0]):
+                raise ValueError("Seeds outside the domain")
+            bad = np.nonzero(status & ~_lib.AGD_STATUS_NOT_CONVERGED)[0]
+            if len(bad):
+                raise _lib.AgdError(int(status[bad[0]]), f"eikonal solve failed on the device (instance {bad[0]})")
+            nc = np.nonzero(status & _lib.AGD_STATUS_NOT_CONVERGED)[0]
+            if len(nc):
+                msg = f"{len(nc)} instance(s) did not reach convergence after {self.solver.nitermax_o} iterations"
+                if self.solver.raiseOnNonConvergence:
+                    raise ValueError(msg)
+                warnings.warn(msg)
+        return self.out if self.out is not None else self.buf.out
+
+
+class BatchSolver:
+    """Solves batches of `batch` instances of the configuration of `template`.
+
+    template: a dictIn whose keys (model, dims/gridScale(s)/origin, traits,
+    tol/atol/rtol, nitermax_o, fim_front_width, ...) apply to every instance; it
+    may hold data of one instance (metric, cost, seeds), which is read only to
+    check the keys.  submit(metric=, cost=, seeds=, seedValues=, out=) takes
+    arrays with a leading batch axis: metric (batch, *shape, symdim) HFM packing
+    (Riemann models), cost (batch, *shape) (required by Isotropic models,
+    optional for Riemann), seeds (batch, nseeds, ndim) points, seedValues
+    (batch, nseeds).  Host tensors are copied in (page-locked ones without
+    blocking), device tensors are read in place."""
+
+    def __init__(self, template, batch, nbuffers=2, launch=None):
+        if batch < 1 or nbuffers < 1:
+            raise ValueError("batch and nbuffers must be positive")
+        if "metric" not in template and "dualMetric" not in template and str(template["model"]).startswith("Riemann"):
+            # the configuration needs no data: a constant metric stands in for the check of the keys
+            template = template.copy()
+            nd = int(str(template["model"])[-1])
+            template["metric"] = np.eye(nd, dtype=np.float32)[np.tril_indices(nd)]
+        itf = Interface(template)
+        itf.SetKernelTraits()
+        itf.SetGeometry()
+        if itf.multiprecision:
+            raise NotImplementedError("BatchSolver: multiprecision instances go through RunBatch")
+        for key in ("tips", "sensitivity", "exportGeodesicFlow", "walls", "seedRadius", "speed", "dualMetric"):
+            if key in template and template[key] is not None and template[key] is not False:
+                raise NotImplementedError(f"BatchSolver: key {key!r} is not available on the batched path")
+        self.template = template
+        self.batch, self.nbuffers = int(batch), int(nbuffers)
+        self.model = itf.model
+        self.riemann = itf.model_ == "Riemann"
+        self.ndim = itf.ndim
+        self.shape, self.shape_i = tuple(itf.shape), tuple(itf.shape_i)
+        self.size_tot = itf.size_tot
+        self.symdim = self.ndim * (self.ndim + 1) // 2
+        self.h = np.asarray(itf.h, np.float32)
+        bottom, _ = template.corners
+        self.start = (bottom + 0.5 * self.h).astype(np.float32)
+        self.niter_i, self.fim_front_width, self.nitermax_o = itf.niter_i, itf.fim_front_width, itf.nitermax_o
+        self.raiseOnNonConvergence = itf.raiseOnNonConvergence
+        self.rtol = itf.rtol
+        # a tolerance given by the user holds for every instance; otherwise the
+        # default follows each instance's mean cost, as for RunGPU
+        self.fixed_atol = itf.atol if ("atol" in template or "tol" in template) else None
+        self.launch = launch
+        self.c_shape = (ctypes.c_int * 3)(*self.shape, *([1] * (3 - self.ndim)))
+        self.c_shape_i = (ctypes.c_int * 3)(*self.shape_i, *([1] * (3 - self.ndim)))
+        self._bufs = [_Buffers(self) for _ in range(self.nbuffers)]
+        self._next = 0
+        self.submitted = 0
+
+    # ------------------------------------------------------------------ input --
+    def _stage(self, buf, name, x, shape, dtype=torch.float32):
+        """Device tensor holding x (batch-leading array), in place when already on the device."""
+        if not isinstance(x, torch.Tensor):
+            x = torch.from_numpy(np.ascontiguousarray(np.asarray(x), dtype=np.float32 if dtype == torch.float32
+                                                      else np.int32))
+        if tuple(x.shape) != tuple(shape):
+            raise ValueError(f"{name} has shape {tuple(x.shape)}, expected {tuple(shape)}")
+        if x.is_cuda:
+            return x.to(dtype).contiguous()
+        d = buf.staging(name, shape, dtype)
+        d.copy_(x.to(dtype), non_blocking=x.is_pinned())
+        return d
+
+    def _atol(self, cost):
+        if self.fixed_atol is not None:
+            return np.full(self.batch, self.fixed_atol, np.float32)
+        if cost is None:
+            return np.full(self.batch, np.float32(1.0 * _FLOAT_RES * 5.0), np.float32)
+        c = cost if isinstance(cost, torch.Tensor) else torch.from_numpy(np.asarray(cost, np.float32))
+        mean = torch.nanmean(c.reshape(self.batch, -1).float(), dim=1).cpu().numpy().astype(np.float64)
+        return (mean * _FLOAT_RES * 5.0).astype(np.float32)
+
+    def _plan(self, buf, atol):
+        if buf.plan is not None and np.array_equal(buf.plan_atol, atol):
+            return
+        L = _lib.lib()
+        arr = (_lib.AgdInstance * self.batch)()
+        for i in range(self.batch):
+            inst = arr[i]
+            inst.model = _lib.AGD_MODEL_RIEMANN if self.riemann else _lib.AGD_MODEL_ISOTROPIC
+            inst.ndim = self.ndim
+            for k in range(3):
+                inst.shape[k] = self.c_shape[k]
+                inst.shape_i[k] = self.c_shape_i[k]
+                inst.iso_weights[k] = float(self.h[k]) ** -2 if k < self.ndim else 0.0
+            inst.niter_i, inst.fim_front_width, inst.nitermax_o = self.niter_i, self.fim_front_width, self.nitermax_o
+            inst.atol, inst.rtol = float(atol[i]), float(self.rtol)
+            inst.values = buf.values[i].data_ptr()
+            inst.geom = buf.geom[i].data_ptr() if self.riemann else None
+            inst.rhs = buf.rhs[i].data_ptr()
+            inst.seedbits = buf.seedbits[i].data_ptr()
+        plan = ctypes.c_void_p()
+        _lib.check(L.agd_plan_create(arr, self.batch, ctypes.byref(plan)), "plan")
+        if buf.plan is not None:
+            L.agd_plan_destroy(buf.plan)
+        buf.plan = plan
+        buf.plan_atol = atol
+        nbytes = int(L.agd_plan_workspace_bytes(plan))
+        if buf.ws is None or buf.ws.numel() < nbytes:
+            with torch.cuda.stream(buf.stream):
+                buf.ws = torch.empty(nbytes, dtype=torch.uint8, device="cuda")
+        _lib.check(L.agd_plan_upload(plan, _lib.ptr(buf.ws), nbytes, _lib.stream_ptr(buf.stream)), "upload")
+
+    def _seed_index(self, buf, seeds):
+        """(batch, nseeds, ndim) grid indices of the seed points, rounded as the
+        reference does (PointFromIndex(., to=True), then np.round)."""
+        if isinstance(seeds, torch.Tensor) and seeds.is_cuda:
+            if seeds.dim() != 3 or seeds.shape[0] != self.batch or seeds.shape[2] != self.ndim:
+                raise ValueError(f"seeds must have shape (batch, nseeds, {self.ndim})")
+            start = torch.as_tensor(self.start, device="cuda")
+            h = torch.as_tensor(self.h, device="cuda")
+            return torch.round((seeds.float() - start) / h).to(torch.int32).contiguous()  # checked on the device
+        s = seeds.numpy() if isinstance(seeds, torch.Tensor) else np.asarray(seeds, np.float32)
+        s = s.astype(np.float32, copy=False)
+        if s.ndim != 3 or s.shape[0] != self.batch or s.shape[2] != self.ndim:
+            raise ValueError(f"seeds must have shape (batch, nseeds, {self.ndim})")
+        idx = np.round((s - self.start) / self.h).astype(np.int32)
+        inside = np.all((idx >= 0) & (idx < np.array(self.shape)), axis=2)
+        if not np.all(inside):
+            raise ValueError(f"Seeds outside the domain: {s[~inside].tolist()}")
+        host = torch.from_numpy(idx).pin_memory()
+        d = buf.staging("seed_index", idx.shape, torch.int32)
+        d.copy_(host, non_blocking=True)
+        return d
+
+    # ----------------------------------------------------------------- submit --
+    def submit(self, metric=None, cost=None, seeds=None, seedValues=None, out=None):
+        """Queues one batch; returns a SolverJob.  out: optional host tensor
+        (batch, *shape) float32 (page-locked for an asynchronous copy)."""
+        if seeds is None:
+            raise ValueError("Missing value for key seeds")
+        if self.riemann and metric is None:
+            raise ValueError("Missing value for key metric")
+        if not self.riemann and cost is None:
+            raise ValueError("Missing value for key cost")
+        if not self.riemann and metric is not None:
+            raise ValueError("Isotropic models take a cost, not a metric")
+        if out is not None and (tuple(out.shape) != (self.batch,) + self.shape or out.dtype != torch.float32):
+            raise ValueError(f"out must be a float32 tensor of shape {(self.batch,) + self.shape}")
+        buf = self._bufs[self._next]
+        self._next = (self._next + 1) % self.nbuffers
+        if buf.job is not None:
+            buf.job.event.synchronize()  # the previous batch of this buffer set is complete
+        atol = self._atol(cost)
+        user_stream = torch.cuda.current_stream()
+        L = _lib.lib()
+        with torch.cuda.stream(buf.stream):
+            buf.stream.wait_stream(user_stream)  # device inputs made on the caller's stream
+            self._plan(buf, atol)
+            prep = _lib.AgdBatchPrep()
+            prep.model = _lib.AGD_MODEL_RIEMANN if self.riemann else _lib.AGD_MODEL_ISOTROPIC
+            prep.ndim, prep.n = self.ndim, self.batch
+            for k in range(3):
+                prep.shape[k], prep.shape_i[k] = self.c_shape[k], self.c_shape_i[k]
+                prep.grid_scales[k] = float(self.h[k]) if k < self.ndim else 1.0
+            keep = []
+            if self.riemann:
+                m = self._stage(buf, "metric", metric, (self.batch,) + self.shape + (self.symdim,))
+                keep.append(m)
+                prep.metric, prep.geom = m.data_ptr(), buf.geom.data_ptr()
+            if cost is not None:
+                c = self._stage(buf, "cost", cost, (self.batch,) + self.shape)
+                keep.append(c)
+                prep.cost = c.data_ptr()
+            idx = self._seed_index(buf, seeds)
+            keep.append(idx)
+            prep.seed_index, prep.nseeds = idx.data_ptr(), int(idx.shape[1])
+            if seedValues is not None:
+                v = self._stage(buf, "seed_values", seedValues, (self.batch, int(idx.shape[1])))
+                keep.append(v)
+                prep.seed_values = v.data_ptr()
+            buf.bad.zero_()
+            prep.rhs, prep.values = buf.rhs.data_ptr(), buf.values.data_ptr()
+            prep.seedbits, prep.bad_seed = buf.seedbits.data_ptr(), buf.bad.data_ptr()
+            st = _lib.stream_ptr(buf.stream)
+            _lib.check(L.agd_prep_batch(ctypes.byref(prep), st), "prep_batch")
+            lp = ctypes.byref(self.launch) if self.launch is not None else None
+            _lib.check(L.agd_plan_run(buf.plan, _lib.ptr(buf.ws), buf.ws.numel(), _lib.ptr(buf.stats), lp, st),
+                       "solve")
+            _lib.check(L.agd_block_squeeze(self.ndim, self.c_shape, self.c_shape_i, self.batch, _lib.ptr(buf.values),
+                                           _lib.ptr(buf.out), st), "block_squeeze")
+            buf.stats_host.copy_(buf.stats, non_blocking=True)
+            buf.bad_host.copy_(buf.bad, non_blocking=True)
+            if out is not None:
+                out.copy_(buf.out, non_blocking=True)
+            for t in keep:  # inputs read in place on this stream stay alive until it gets past them
+                if t.is_cuda:
+                    t.record_stream(buf.stream)
+            job = SolverJob(self, buf, out)
+        buf.job = job
+        self.submitted += 1
+        return job
+
+    def solve(self, **kwargs):
+        """submit(**kwargs).result()."""
+        return self.submit(**kwargs).result()
+
+    def __del__(self):
+        try:
+            L = _lib.lib()
+            for b in self._bufs:
+                if b.plan is not None:
+                    b.stream.synchronize()
+                    L.agd_plan_destroy(b.plan)
+                    b.plan = None
+        except Exception:  # noqa: BLE001
+            pass

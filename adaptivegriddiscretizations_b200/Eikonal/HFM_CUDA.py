@@ -53,6 +53,16 @@ def RunBatch(hfmIns, launch=None):
     Each instance keeps its own model, tile shape, tolerances and options; the
     per-instance post-processing (flow, geodesics, sensitivities, outputs) is the
     same as RunGPU's.  Returns the list of outputs."""
+    return SubmitBatch(hfmIns, launch=launch).result()
+
+
+def SubmitBatch(hfmIns, launch=None):
+    """Queues the preparation and the solve of several dictIn on the current
+    CUDA stream and returns a BatchJob without waiting for the device.
+
+    The host can meanwhile prepare the next batch: submitted on a second
+    stream, its uploads and preparation kernels queue while this solve runs.
+    `BatchJob.result()` gives what RunBatch returns."""
     itfs = [Interface(h) for h in hfmIns]
     for it in itfs:
         it.SetKernelTraits()
@@ -60,23 +70,56 @@ def RunBatch(hfmIns, launch=None):
         it.SetArgs()
     plan = BatchPlan(itfs, launch=launch)
     plan.run()
-    plan.finish()
-    outs = []
-    for it in itfs:
-        it.PostProcess()
-        it.SolveAD()
-        it.GetGeodesics()
-        it.FinalCheck()
-        if it.extractValues or it.retself:
-            r = [it.hfmOut]
-            if it.extractValues:
-                r.insert(0, it.values)
-            if it.retself:
-                r.append(it)
-            outs.append(r)
-        else:
-            outs.append(it.hfmOut)
-    return outs
+    return BatchJob(plan)
+
+
+class BatchJob:
+    """A submitted batch.  The solver statistics come back to page-locked host
+    memory and the solution values are rearranged into grid order on the
+    submission stream right behind the solve, so that `result()` only waits
+    for this batch even when later work is queued on other streams."""
+
+    def __init__(self, plan):
+        self.plan = plan
+        self.stream = torch.cuda.current_stream()
+        for it in plan.itfs:
+            if it.hfmIn.get("exportValues", False) or it.hfmIn.get("extractValues", False):
+                it.values  # noqa: B018  (queues the squeeze; the tensor is cached)
+        self.stats_host = torch.empty(tuple(plan.stats.shape), dtype=plan.stats.dtype).pin_memory()
+        self.stats_host.copy_(plan.stats, non_blocking=True)
+        self.event = torch.cuda.Event()
+        self.event.record(self.stream)
+        self._outs = None
+
+    def done(self):
+        """True once the device has finished the solve (does not block)."""
+        return self.event.query()
+
+    def result(self):
+        """Waits for the solve, checks its status and returns the outputs (a list,
+        in submission order); post-processing runs on the submission stream."""
+        if self._outs is not None:
+            return self._outs
+        self.event.synchronize()
+        with torch.cuda.stream(self.stream):
+            self.plan.finish(self.stats_host.numpy())
+            outs = []
+            for it in self.plan.itfs:
+                it.PostProcess()
+                it.SolveAD()
+                it.GetGeodesics()
+                it.FinalCheck()
+                if it.extractValues or it.retself:
+                    r = [it.hfmOut]
+                    if it.extractValues:
+                        r.insert(0, it.values)
+                    if it.retself:
+                        r.append(it)
+                    outs.append(r)
+                else:
+                    outs.append(it.hfmOut)
+        self._outs = outs
+        return outs
 
 
 class BatchPlan:
@@ -104,12 +147,15 @@ class BatchPlan:
         _lib.check(L.agd_plan_run(self.plan, _lib.ptr(self.ws), self.nbytes, _lib.ptr(self.stats), lp,
                                   _lib.stream_ptr(stream)), "solve")
 
-    def read_stats(self):
-        s = self.stats.cpu().numpy()
+    def read_stats(self, s=None):
+        """(niter_o, status, tile_visits) per instance, from the device statistics
+        or from a host copy of them."""
+        if s is None:
+            s = self.stats.cpu().numpy()
         return (s[:, 0] & 0xffffffff).astype(np.int64), ((s[:, 0] >> 32) & 0xffffffff).astype(np.int64), s[:, 1]
 
-    def finish(self):
-        niter, status, visits = self.read_stats()
+    def finish(self, stats_host=None):
+        niter, status, visits = self.read_stats(stats_host)
         for i, it in enumerate(self.itfs):
             it.tile_visits = int(visits[i])
             it.stats["eikonal"].update({"niter_o": int(niter[i]), "time": None, "nupdate_o_total": int(visits[i]),
@@ -122,7 +168,6 @@ class BatchPlan:
                 if it.raiseOnNonConvergence:
                     raise ValueError(msg)
                 it.Warn(msg)
-            it._values = None
 
     def __del__(self):
         try:
@@ -374,6 +419,7 @@ class Interface:
             _lib.check(L.agd_block_expand(self.ndim, self.c_shape, self.c_shape_i, 1, _lib.ptr(v), 0,
                                           ctypes.c_float(math.inf), _lib.ptr(self.values_t), self.stream),
                        "values")
+        self._values = None
         self.valuesq_t = self.values_next_t = self.valuesq_next_t = None
         if self.multiprecision:  # _SetArgs.py:168-177
             self.valuesq_t = torch.zeros(self.size_tot, dtype=torch.int32, device="cuda")

@@ -1,5 +1,7 @@
 """Eikonal solver interface: agd.Eikonal's dictIn/dictOut surface, GPU modes."""
 from .DictIn import dictIn, dictOut, CenteredLinspace
-from .HFM_CUDA import RunGPU, RunBatch, BatchPlan
+from .HFM_CUDA import RunGPU, RunBatch, SubmitBatch, BatchJob, BatchPlan
+from .BatchSolver import BatchSolver, SolverJob
 
-__all__ = ["dictIn", "dictOut", "CenteredLinspace", "RunGPU", "RunBatch", "BatchPlan"]
+__all__ = ["dictIn", "dictOut", "CenteredLinspace", "RunGPU", "RunBatch", "SubmitBatch", "BatchJob", "BatchPlan",
+           "BatchSolver", "SolverJob"]

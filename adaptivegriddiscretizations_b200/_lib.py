@@ -47,6 +47,17 @@ class AgdLaunch(ctypes.Structure):
     _fields_ = [("ctas", ctypes.c_int), ("warps_per_cta", ctypes.c_int), ("timeout_ns", ctypes.c_int64)]
 
 
+class AgdBatchPrep(ctypes.Structure):
+    _fields_ = [
+        ("model", ctypes.c_int), ("ndim", ctypes.c_int), ("shape", _c_int3), ("shape_i", _c_int3),
+        ("n", ctypes.c_int), ("is_dual", ctypes.c_int), ("grid_scales", ctypes.c_double * 3),
+        ("metric", ctypes.c_void_p), ("cost", ctypes.c_void_p), ("seed_index", ctypes.c_void_p),
+        ("seed_values", ctypes.c_void_p), ("nseeds", ctypes.c_int), ("geom", ctypes.c_void_p),
+        ("rhs", ctypes.c_void_p), ("values", ctypes.c_void_p), ("seedbits", ctypes.c_void_p),
+        ("bad_seed", ctypes.c_void_p),
+    ]
+
+
 # Every exported symbol, with its ctypes signature.
 _P = ctypes.c_void_p
 _I = ctypes.c_int
@@ -63,6 +74,7 @@ SIGNATURES = {
     "agd_block_expand": (_I, [_I, _P, _P, _I, _P, _I, ctypes.c_float, _P, _P]),
     "agd_block_squeeze": (_I, [_I, _P, _P, _I, _P, _P, _P]),
     "agd_prep_seeds": (_I, [_I, _P, _P, _P, _P, _I, _P, _P, _P, _P]),
+    "agd_prep_batch": (_I, [_P, _P]),
     "agd_selling": (_I, [_I, _P, _I, _P, _P, _P]),
     "agd_flow": (_I, [_P, _P, _P, _P, _P, _P]),
     "agd_eucl_map": (_I, [_I, _P, _P, _I, _I, _P, _P, _P]),

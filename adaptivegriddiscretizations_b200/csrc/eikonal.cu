@@ -38,15 +38,16 @@ namespace agd {
 // three 10-bit signed fields in 3D.
 template <int D>
 __device__ __forceinline__ bool pack_offset(const int *e, int &word) {
-    if (D == 2) {
+    if constexpr (D == 2) {
         if (e[0] < -32768 || e[0] > 32767 || e[1] < -32768 || e[1] > 32767) return false;
         word = (e[0] & 0xffff) | (e[1] << 16);
         return true;
+    } else {
+        for (int c = 0; c < 3; ++c)
+            if (e[c] < -512 || e[c] > 511) return false;
+        word = (e[0] & 0x3ff) | ((e[1] & 0x3ff) << 10) | ((e[2] & 0x3ff) << 20);
+        return true;
     }
-    for (int c = 0; c < 3; ++c)
-        if (e[c] < -512 || e[c] > 511) return false;
-    word = (e[0] & 0x3ff) | ((e[1] & 0x3ff) << 10) | ((e[2] & 0x3ff) << 20);
-    return true;
 }
 template <int D>
 __device__ __forceinline__ void unpack_offset(int word, int *e) {
@@ -814,7 +815,40 @@ __global__ void block_squeeze_kernel(Geo g, int nplanes, const float *src, float
 }
 
 // Dual metric of M' = diag(h) M diag(h) (Riemann.with_costs, then dual), by the
-// adjugate formula; packed [d00, d10, d11(, d20, d21, d22)] planes in tile layout.
+// adjugate formula, packed [d00, d10, d11(, d20, d21, d22)]; with is_dual, m
+// already holds the dual metric and is only rescaled (dualMetric.with_speeds(h)).
+__device__ __forceinline__ void geom_at(int nd, const float *m, int is_dual, const float h[3], float *out) {
+    if (nd == 2) {
+        float a = m[0], b = m[1], c = m[2];
+        if (is_dual) {  // entries / (h_i h_j)
+            out[0] = a / (h[0] * h[0]); out[1] = b / (h[1] * h[0]); out[2] = c / (h[1] * h[1]);
+            return;
+        }
+        a = a * (h[0] * h[0]); b = b * (h[1] * h[0]); c = c * (h[1] * h[1]);
+        const float det = a * c - b * b;
+        out[0] = c / det;
+        out[1] = -b / det;
+        out[2] = a / det;
+        return;
+    }
+    float s[6];
+    int k = 0;
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j <= i; ++j, ++k) s[k] = is_dual ? m[k] / (h[i] * h[j]) : m[k] * (h[i] * h[j]);
+    if (is_dual) {
+        for (int c = 0; c < 6; ++c) out[c] = s[c];
+        return;
+    }
+    // symmetric [[a,b,d],[b,c,e],[d,e,f]] with s = [a, b, c, d, e, f]
+    const float a = s[0], b = s[1], c = s[2], d = s[3], e = s[4], f = s[5];
+    const float A00 = c * f - e * e, A10 = d * e - b * f, A11 = a * f - d * d;
+    const float A20 = b * e - c * d, A21 = b * d - a * e, A22 = a * c - b * b;
+    const float det = a * A00 + b * A10 + d * A20;
+    out[0] = A00 / det; out[1] = A10 / det; out[2] = A11 / det;
+    out[3] = A20 / det; out[4] = A21 / det; out[5] = A22 / det;
+}
+
+// Geometry planes in tile layout; +inf at padding points.
 __global__ void prep_geom_kernel(Geo g, const float *metric, int bcast, int is_dual, double h0, double h1,
                                  double h2, float *geom) {
     const long long n_t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
@@ -827,37 +861,10 @@ __global__ void prep_geom_kernel(Geo g, const float *metric, int bcast, int is_d
         for (int c = 0; c < sd; ++c) geom[c * g.size_tot + n_t] = finf();
         return;
     }
-    const float *m = bcast ? metric : metric + flat * sd;
     const float h[3] = {(float)h0, (float)h1, (float)h2};
-    if (g.nd == 2) {
-        float a = m[0], b = m[1], c = m[2];
-        if (is_dual) {  // dualMetric.with_speeds(h): entries / (h_i h_j)
-            a = a / (h[0] * h[0]); b = b / (h[1] * h[0]); c = c / (h[1] * h[1]);
-            geom[n_t] = a; geom[g.size_tot + n_t] = b; geom[2 * g.size_tot + n_t] = c;
-            return;
-        }
-        a = a * (h[0] * h[0]); b = b * (h[1] * h[0]); c = c * (h[1] * h[1]);
-        const float det = a * c - b * b;
-        geom[n_t] = c / det;
-        geom[g.size_tot + n_t] = -b / det;
-        geom[2 * g.size_tot + n_t] = a / det;
-    } else {
-        float s[6];
-        int k = 0;
-        for (int i = 0; i < 3; ++i)
-            for (int j = 0; j <= i; ++j, ++k) s[k] = is_dual ? m[k] / (h[i] * h[j]) : m[k] * (h[i] * h[j]);
-        if (is_dual) {
-            for (int c = 0; c < 6; ++c) geom[c * g.size_tot + n_t] = s[c];
-            return;
-        }
-        // symmetric [[a,b,d],[b,c,e],[d,e,f]] with s = [a, b, c, d, e, f]
-        const float a = s[0], b = s[1], c = s[2], d = s[3], e = s[4], f = s[5];
-        const float A00 = c * f - e * e, A10 = d * e - b * f, A11 = a * f - d * d;
-        const float A20 = b * e - c * d, A21 = b * d - a * e, A22 = a * c - b * b;
-        const float det = a * A00 + b * A10 + d * A20;
-        const float out[6] = {A00 / det, A10 / det, A11 / det, A20 / det, A21 / det, A22 / det};
-        for (int q = 0; q < 6; ++q) geom[q * g.size_tot + n_t] = out[q];
-    }
+    float out[6];
+    geom_at(g.nd, bcast ? metric : metric + flat * sd, is_dual, h, out);
+    for (int c = 0; c < sd; ++c) geom[c * g.size_tot + n_t] = out[c];
 }
 
 // Seed bits: one 32-bit word (32 points) per thread, padding bits set.
@@ -874,9 +881,8 @@ __global__ void seedbits_init_kernel(Geo g, unsigned *bits) {
 }
 
 // Seeds in order (a later duplicate overrides an earlier one, as numpy assignment does).
-__global__ void seeds_kernel(Geo g, const int *idx, const float *vals, int n, float *rhs, unsigned *bits,
-                             unsigned char *trigger, int *bad) {
-    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+__device__ void place_seeds(const Geo &g, const int *idx, const float *vals, int n, float *rhs, unsigned *bits,
+                            unsigned char *trigger, int *bad) {
     for (int s = 0; s < n; ++s) {
         long long n_o = 0, n_i = 0;
         bool ok = true;
@@ -886,12 +892,64 @@ __global__ void seeds_kernel(Geo g, const int *idx, const float *vals, int n, fl
             n_o = n_o * g.so[k] + (ok ? xk / g.si[k] : 0);
             n_i = n_i * g.si[k] + (ok ? xk % g.si[k] : 0);
         }
-        if (!ok) { *bad = 1; continue; }
+        if (!ok) {
+            if (bad) *bad = 1;
+            continue;
+        }
         const long long n_t = n_o * g.size_i + n_i;
         if (rhs) rhs[n_t] = vals ? vals[s] : 0.f;
         if (bits) bits[n_t >> 5] |= 1u << (n_t & 31);
         if (trigger) trigger[n_o] = 1;
     }
+}
+
+__global__ void seeds_kernel(Geo g, const int *idx, const float *vals, int n, float *rhs, unsigned *bits,
+                             unsigned char *trigger, int *bad) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    place_seeds(g, idx, vals, n, rhs, bits, trigger, bad);
+}
+
+struct BatchPrep {
+    Geo g;
+    int n, sd, riemann, is_dual, nseeds;
+    float h[3];
+    const float *metric, *cost, *seed_values;
+    const int *seed_index;
+    float *geom, *rhs, *values;
+    unsigned *bits;
+    int *bad;
+};
+
+// One thread per point of every instance (grid-stride; warps stay 32-aligned
+// because size_tot is a multiple of 32, so each warp's ballot is one bit word).
+__global__ void prep_batch_kernel(BatchPrep A) {
+    const long long total = A.g.size_tot * A.n;
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total; i += stride) {
+        const int inst = (int)(i / A.g.size_tot);
+        const long long n_t = i - inst * A.g.size_tot;
+        int x[3];
+        long long flat;
+        const bool in = grid_coords(A.g, n_t, x, flat);
+        A.values[i] = finf();
+        A.rhs[i] = in ? (A.cost ? A.cost[inst * A.g.n + flat] : 1.f) : finf();
+        if (A.riemann) {
+            float out[6];
+            if (in) geom_at(A.g.nd, A.metric + (inst * A.g.n + flat) * A.sd, A.is_dual, A.h, out);
+            float *geo = A.geom + (long long)inst * A.sd * A.g.size_tot + n_t;
+            for (int c = 0; c < A.sd; ++c) geo[c * A.g.size_tot] = in ? out[c] : finf();
+        }
+        const unsigned pad = __ballot_sync(0xffffffffu, !in);
+        if ((threadIdx.x & 31) == 0) A.bits[i >> 5] = pad;
+    }
+}
+
+__global__ void seeds_batch_kernel(BatchPrep A) {
+    const int inst = blockIdx.x * blockDim.x + threadIdx.x;
+    if (inst >= A.n) return;
+    place_seeds(A.g, A.seed_index + (long long)inst * A.nseeds * A.g.nd,
+                A.seed_values ? A.seed_values + (long long)inst * A.nseeds : nullptr, A.nseeds,
+                A.rhs + inst * A.g.size_tot, A.bits + inst * (A.g.size_tot / 32), nullptr, A.bad);
 }
 
 __global__ void selling_kernel(int nd, const float *m, int n, float *w, int *e) {
@@ -1020,6 +1078,44 @@ int agd_prep_seeds(int ndim, const int *shape, const int *shape_i, const int32_t
     }
     const cudaError_t err = cudaGetLastError();
     return err == cudaSuccess ? AGD_STATUS_OK : set_cuda_error("prep_seeds", err);
+}
+
+int agd_prep_batch(const agd_batch_prep *p, agd_stream_t stream) {
+    clear_error();
+    Geo g;
+    if (!p || (p->ndim != 2 && p->ndim != 3) || !geo_of(p->ndim, p->shape, p->shape_i, g) || p->n < 1 ||
+        (g.size_tot % 32) != 0 || p->nseeds < 0 || (p->nseeds > 0 && !p->seed_index) || !p->rhs ||
+        !p->values || !p->seedbits)
+        return set_error(AGD_STATUS_INVALID, "agd_prep_batch: bad arguments");
+    const bool riemann = p->model == AGD_MODEL_RIEMANN;
+    if (!riemann && p->model != AGD_MODEL_ISOTROPIC)
+        return set_error(AGD_STATUS_INVALID, "agd_prep_batch: unknown model");
+    if (riemann && (!p->metric || !p->geom))
+        return set_error(AGD_STATUS_INVALID, "agd_prep_batch: Riemann instances need metric and geom");
+    BatchPrep A;
+    A.g = g;
+    A.n = p->n;
+    A.sd = p->ndim * (p->ndim + 1) / 2;
+    A.riemann = riemann;
+    A.is_dual = p->is_dual;
+    A.nseeds = p->nseeds;
+    for (int k = 0; k < 3; ++k) A.h[k] = k < p->ndim ? (float)p->grid_scales[k] : 1.f;
+    A.metric = p->metric;
+    A.cost = p->cost;
+    A.seed_values = p->seed_values;
+    A.seed_index = p->seed_index;
+    A.geom = p->geom;
+    A.rhs = p->rhs;
+    A.values = p->values;
+    A.bits = reinterpret_cast<unsigned *>(p->seedbits);
+    A.bad = p->bad_seed;
+    cudaStream_t st = (cudaStream_t)stream;
+    const long long total = g.size_tot * p->n;
+    const unsigned blocks = (unsigned)std::min<long long>((total + 255) / 256, 148LL * 16);
+    prep_batch_kernel<<<blocks, 256, 0, st>>>(A);
+    if (p->nseeds > 0) seeds_batch_kernel<<<blocks_for(p->n, 128), 128, 0, st>>>(A);
+    const cudaError_t err = cudaGetLastError();
+    return err == cudaSuccess ? AGD_STATUS_OK : set_cuda_error("prep_batch", err);
 }
 
 int agd_selling(int ndim, const float *m, int n, float *weights, int32_t *offsets, agd_stream_t stream) {

@@ -31,6 +31,10 @@ BYTES_PER_UPDATE = {"Riemann2": 24.125, "Riemann3": 36.125, "Isotropic2": 12.125
 METRIC = "solves/s, Riemann2 512x512 batched cold-start solves (grid-updates/s in config)"
 
 
+# (grid, batch, tile, niter_i, fim_front_width) -> DRAM bytes per solver launch, measured
+MEASURED_TRAFFIC = {(512, 128, 8, 8, 4): 10.90e9 + 1.40e9}
+
+
 def peaks():
     try:
         with open(os.path.join(REPO, "MEASURED_PEAKS.json")) as f:
@@ -291,32 +295,74 @@ def main():
     total_solves = B * args.steps * world
     value = total_solves / elapsed
     hbm, peak_kind = peaks()
+    # DRAM bytes (read + write) of one sched_worker launch of this workload,
+    # from an ncu capture (dram__bytes_read.sum + dram__bytes_write.sum, one pass)
+    traffic = MEASURED_TRAFFIC.get((n, B, args.tile, args.niter_i or 8, args.front or 4))
     achieved = updates_per_step * BYTES_PER_UPDATE["Riemann2"] / kern.mean() / 1e9
 
-    # end to end: public API from pinned host buffers, values back to the host
-    e2e = None
+    # End to end, inputs in page-locked host memory, values read back to host
+    # memory every step.  Primary: Eikonal.BatchSolver (repeated batched solves of
+    # one configuration; batch k+1 is uploaded and prepared while batch k
+    # solves).  Also reported: the dictIn path (one dictIn per instance,
+    # Eikonal.SubmitBatch on two alternating streams).
+    e2e = e2e_dictin = None
     if args.e2e_steps > 0:
-        # the caller's inputs sit in page-locked host memory; every step builds
-        # the dictIn inputs from them (the seeds and the metrics cross to the
-        # device inside RunBatch's step) and reads all values back to the host
-        pin_m = [torch.from_numpy(m).pin_memory() for m in metrics]
-        pin_s = [torch.from_numpy(s).pin_memory() for s in seeds]
         h2d = sum(m.nbytes + s.nbytes for m, s in zip(metrics, seeds))
-        host_vals = torch.empty((B, n, n), dtype=torch.float32).pin_memory()
-        d2h = host_vals.numel() * 4
+        host_out = [torch.empty((B, n, n), dtype=torch.float32).pin_memory() for _ in range(2)]
+        d2h = host_out[0].numel() * 4
+        pin_metric = torch.from_numpy(np.stack(metrics)).pin_memory()
+        pin_seeds = torch.from_numpy(np.stack(seeds)).pin_memory()
+        template = dictins(metrics[:1], seeds[:1], n, to_device=False, traits=traits)[0]
+        solver = Eikonal.BatchSolver(template, B, launch=launch)
 
-        def e2e_step():
-            outs = Eikonal.RunBatch(dictins(pin_m, pin_s, n, to_device=False, traits=traits))
-            host_vals.copy_(torch.stack([o["values"] for o in outs]), non_blocking=True)
-            torch.cuda.synchronize()
+        def run_solver(nsteps):
+            pending = []
+            for k in range(nsteps):
+                pending.append(solver.submit(metric=pin_metric, seeds=pin_seeds, out=host_out[k % 2]))
+                if len(pending) == 2:
+                    pending.pop(0).result()
+            for job in pending:
+                job.result()
 
-        e2e_step()  # warm up the path at full size
+        run_solver(3)  # warm up both buffer sets
+        torch.cuda.synchronize()
         t_e = time.perf_counter()
-        for _ in range(args.e2e_steps):
-            e2e_step()
+        run_solver(args.e2e_steps)
         te = time.perf_counter() - t_e
         e2e = {"value": B * args.e2e_steps * world / te, "unit": "solves/s", "h2d_bytes_per_step": int(h2d),
-               "d2h_bytes_per_step": int(d2h)}
+               "d2h_bytes_per_step": int(d2h), "api": "Eikonal.BatchSolver.submit (two buffer sets)"}
+        del solver
+
+        pin_m = [torch.from_numpy(m).pin_memory() for m in metrics]
+        pin_s = [torch.from_numpy(s).pin_memory() for s in seeds]
+        streams = [torch.cuda.Stream(), torch.cuda.Stream()]
+
+        def submit(k):
+            with torch.cuda.stream(streams[k % 2]):
+                return Eikonal.SubmitBatch(dictins(pin_m, pin_s, n, to_device=False, traits=traits))
+
+        def collect(job):
+            outs = job.result()
+            with torch.cuda.stream(job.stream):  # copy engine only: no kernel behind the next solve
+                for i, o in enumerate(outs):
+                    host_out[0][i].copy_(o["values"], non_blocking=True)
+            job.stream.synchronize()
+
+        def run_dictin(nsteps):
+            job = submit(0)
+            for k in range(nsteps):
+                nxt = submit(k + 1) if k + 1 < nsteps else None
+                collect(job)
+                job = nxt
+
+        run_dictin(2)
+        torch.cuda.synchronize()
+        t_e = time.perf_counter()
+        run_dictin(args.e2e_steps)
+        te = time.perf_counter() - t_e
+        e2e_dictin = {"value": B * args.e2e_steps * world / te, "unit": "solves/s",
+                      "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
+                      "api": "Eikonal.SubmitBatch of dictIn inputs (two streams)"}
 
     cpu = None
     if rank == 0 and not args.no_cpu_baseline:
@@ -340,10 +386,10 @@ def main():
                        "l2": "inputs larger than L2 (batch working set %.0f MB)" % (B * size_tot * 24 / 1e6),
                        "parallelism": f"replicas x{world}"},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
-                         "frac": achieved / hbm, "traffic": None, "peak_kind": peak_kind,
+                         "frac": achieved / hbm, "traffic": traffic, "peak_kind": peak_kind,
                          "kernel": "sched_worker<EikonalVisitor>", "kernel_ms": float(kern.mean() * 1000),
                          "bytes_per_update": BYTES_PER_UPDATE["Riemann2"]},
-            "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": 5 * args.steps,
+            "cpu_baseline": cpu, "e2e": e2e, "e2e_dictin": e2e_dictin, "gpu_launches": 5 * args.steps,
             "clocks": clk.summary(),
         }
         print(json.dumps(line), flush=True)

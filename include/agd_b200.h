@@ -167,6 +167,37 @@ int agd_prep_seeds(int ndim, const int *shape, const int *shape_i, const int32_t
                    const float *seed_values, int n, float *rhs, uint8_t *seedbits, uint8_t *trigger,
                    agd_stream_t stream);
 
+/* Preparation of n instances that share one grid and tile shape, for repeated
+ * batched solves: one launch writes, for every instance, the geometry (Riemann:
+ * dual metric planes as agd_prep_geom), the right-hand side (cost, or 1, with
+ * +inf padding as agd_block_expand), values = +inf and the padding seed bits;
+ * a second launch places the seeds as agd_prep_seeds does, one thread per
+ * instance, in seed order.  The reference prepares one instance per call
+ * (_SetGeometry.py:16-282, _SetArgs.py:8-177); this batched form has no
+ * counterpart there.  Arrays are instance-major, with the per-instance sizes
+ * given beside each field. */
+typedef struct agd_batch_prep {
+    int model;                  /* AGD_MODEL_ISOTROPIC or AGD_MODEL_RIEMANN */
+    int ndim;                   /* 2 or 3 */
+    int shape[3];               /* grid shape (unused trailing entries 1) */
+    int shape_i[3];             /* tile shape */
+    int n;                      /* number of instances */
+    int is_dual;                /* Riemann: `metric` holds the dual metric */
+    double grid_scales[3];
+    const float *metric;        /* Riemann: prod(shape) x symdim, HFM packing; NULL otherwise */
+    const float *cost;          /* prod(shape), or NULL for cost 1 */
+    const int32_t *seed_index;  /* nseeds x ndim grid indices */
+    const float *seed_values;   /* nseeds, or NULL for 0 */
+    int nseeds;                 /* seeds per instance (>= 0) */
+    float *geom;                /* Riemann: symdim x size_tot (tile layout); NULL otherwise */
+    float *rhs;                 /* size_tot */
+    float *values;              /* size_tot */
+    uint8_t *seedbits;          /* size_tot / 8 */
+    int32_t *bad_seed;          /* device flag set to 1 for a seed outside the grid; may be NULL */
+} agd_batch_prep;
+
+int agd_prep_batch(const agd_batch_prep *prep, agd_stream_t stream);
+
 /* Selling decomposition of n packed symmetric matrices (symdim floats each):
  * weights (n, symdim), integer offsets (n, symdim, ndim).  Same decomposition
  * as the kernel's decomp_m (cuda/Geometry2.h:21-48, Geometry3.h:22-58). */
