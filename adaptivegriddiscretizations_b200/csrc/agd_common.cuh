@@ -184,8 +184,12 @@ __device__ __forceinline__ float hfm_update(float rhs, float *v, float *w) {
         }
     }
     const float delta = b * b - a * c;
-    const float sd = sqrtf(fmaxf(0.f, delta));
-    const float value = a == 0.f ? finf() : (b + sd) / a;
+    // Approximate square root and quotient (a few ulp): the result is compared
+    // with tolerances of ~5e-6 relative, and the hardware forms save ~15
+    // instructions per update over the correctly rounded ones.
+    float sd;
+    asm("sqrt.approx.f32 %0, %1;" : "=f"(sd) : "f"(fmaxf(0.f, delta)));
+    const float value = a == 0.f ? finf() : __fdividef(b + sd, a);
     return vmin + value;
 }
 

@@ -152,15 +152,39 @@ struct Visit {
         v = in ? us[li] : x;
         vq = in ? uqs[li] : xq;
     }
+    // Shared memory of a warp: the tile's values, then (64-point tiles without
+    // multiprecision) one slot per lane and stencil neighbour for the values
+    // read from outside the tile, so that every neighbour of a sweep is one
+    // shared load; otherwise (kSlots false) the integer parts with multiprecision.
+    static constexpr bool kSlots = !MP && TL::SIZE <= 64;
+    static constexpr int kSmemFloats = kSlots ? TL::SIZE + P * NTOT * 32 : 2 * TL::SIZE;
     __device__ __forceinline__ static float neighbour(float x, const float *us) {
         const int b = __float_as_int(x);
         const float inside = us[b & (TL::SIZE - 1)];  // index masked into this warp's tile
         return (b >> 22) == -1 ? inside : x;
     }
+    __device__ __forceinline__ static float lds(unsigned addr) {
+        float v;
+        asm volatile("ld.shared.f32 %0, [%1];" : "=f"(v) : "r"(addr) : "memory");
+        return v;
+    }
 
-    // Stencil of the point with bilevel index n_t: weights and offsets, from the
-    // per-solve cache when there is one, else by Selling's decomposition.
-    __device__ __forceinline__ static void stencil(const Inst &I, size_t n_t, float *w, int (*e)[3]) {
+    // Stencil of the point with bilevel index n_t, in two steps so that the
+    // loads of all the points of a lane are in flight together: the raw words
+    // (cached weights and packed offsets, or the dual metric), then the weights
+    // and offsets (unpacked, or by Selling's decomposition).
+    static constexpr int kRaw = MODEL == AGD_MODEL_ISOTROPIC ? 1 : 2 * SD;
+    __device__ __forceinline__ static void stencil_load(const Inst &I, size_t n_t, float *raw) {
+        if (MODEL == AGD_MODEL_ISOTROPIC) return;
+        if (I.stencil) {
+#pragma unroll
+            for (int r = 0; r < 2 * SD; ++r) raw[r] = __ldg(I.stencil + (size_t)r * I.size_tot + n_t);
+        } else {
+#pragma unroll
+            for (int c = 0; c < SD; ++c) raw[c] = __ldg(I.a.geom + (size_t)c * I.size_tot + n_t);
+        }
+    }
+    __device__ __forceinline__ static void stencil_decode(const Inst &I, const float *raw, float *w, int (*e)[3]) {
         if (MODEL == AGD_MODEL_ISOTROPIC) {
 #pragma unroll
             for (int k = 0; k < D; ++k) {
@@ -171,16 +195,22 @@ struct Visit {
         } else if (I.stencil) {
 #pragma unroll
             for (int r = 0; r < SD; ++r) {
-                w[r] = __ldg(I.stencil + (size_t)r * I.size_tot + n_t);
-                unpack_offset<D>(__float_as_int(__ldg(I.stencil + (size_t)(SD + r) * I.size_tot + n_t)), e[r]);
+                w[r] = raw[r];
+                unpack_offset<D>(__float_as_int(raw[SD + r]), e[r]);
             }
         } else {
             float m[SD];
 #pragma unroll
-            for (int c = 0; c < SD; ++c) m[c] = __ldg(I.a.geom + (size_t)c * I.size_tot + n_t);
+            for (int c = 0; c < SD; ++c) m[c] = raw[c];
             if (D == 2) selling2(m, w, e);
             else selling3(m, w, e);
         }
+    }
+
+    __device__ __forceinline__ static void stencil(const Inst &I, size_t n_t, float *w, int (*e)[3]) {
+        float raw[kRaw];
+        stencil_load(I, n_t, raw);
+        stencil_decode(I, raw, w, e);
     }
 
     __device__ static void run(const Sched &S, const Inst &I, int ii, int n_o, int e, int lane, float *us) {
@@ -232,25 +262,35 @@ struct Visit {
         float uold[P], rhs[P];
         int qold[P];
         float wts[P][NACT];
-        // Neighbour of each stencil offset: its value when outside the tile (read
-        // once per visit), or its in-tile index boxed as a negative-NaN payload
-        // (no solution value is a NaN), so one register holds either.
-        float nbv[P][NTOT];
+        // Neighbour of each stencil offset.  With kSlots: the shared-memory address
+        // of its value (the tile slot, or this lane's slot holding the value read
+        // from outside).  Otherwise: its value when outside the tile (read once
+        // per visit), or its in-tile index boxed as a negative-NaN payload (no
+        // solution value is a NaN), so one register holds either.
+        float nbv[kSlots ? 1 : P][kSlots ? 1 : NTOT];
         int nbq[MP ? P : 1][MP ? NTOT : 1];
+        unsigned nba[kSlots ? P : 1][kSlots ? NTOT : 1];
+        const unsigned us_addr = (unsigned)__cvta_generic_to_shared(us);
         bool seed[P];
+        float raw[P][kRaw];
+        // every load of the prologue that does not depend on another one is issued first
+#pragma unroll
+        for (int p = 0; p < P; ++p) {
+            const size_t n_t = base + lane + 32 * p;
+            uold[p] = __ldcg(u_in + n_t);
+            seed[p] = (__ldg(A.seedbits + (n_t >> 3)) >> (n_t & 7)) & 1;
+            rhs[p] = __ldg(A.rhs + n_t);
+            if constexpr (MP) qold[p] = __ldcg(q_in + n_t);
+            stencil_load(I, n_t, raw[p]);
+        }
 #pragma unroll
         for (int p = 0; p < P; ++p) {
             const int n_i = lane + 32 * p;
-            const size_t n_t = base + n_i;
             int xi[3] = {0, 0, 0}, xt[3] = {0, 0, 0};
             TL::pos(n_i, xi);
 #pragma unroll
             for (int k = 0; k < D; ++k) xt[k] = xo[k] * TL::extent(k) + xi[k];
-            uold[p] = __ldcg(u_in + n_t);
-            seed[p] = (__ldg(A.seedbits + (n_t >> 3)) >> (n_t & 7)) & 1;
-            rhs[p] = __ldg(A.rhs + n_t);
             if constexpr (MP) {
-                qold[p] = __ldcg(q_in + n_t);
                 float u0 = uold[p];
                 int q0 = qold[p];
                 if (seed[p]) {
@@ -265,7 +305,7 @@ struct Visit {
             }
             int ev[NACT][3];
             if (seed[p]) continue;  // seeds (and padding) keep their value: no stencil needed
-            stencil(I, n_t, wts[p], ev);
+            stencil_decode(I, raw[p], wts[p], ev);
 #pragma unroll
             for (int k = 0; k < NACT; ++k) {
 #pragma unroll
@@ -281,12 +321,22 @@ struct Visit {
                         intile = intile && yi[c] >= 0 && yi[c] < TL::extent(c);
                         indom = indom && yt[c] >= 0 && yt[c] < A.shape[c];
                     }
-                    if (intile) {
-                        nbv[p][2 * k + s] = __int_as_float(kBoxed | TL::local(yi));
+                    if constexpr (!kSlots) {
+                        if (intile) {
+                            nbv[p][2 * k + s] = __int_as_float(kBoxed | TL::local(yi));
+                        } else {
+                            const int ny = indom ? bilevel_index<D, TL>(yt, I.shape_o) : 0;
+                            nbv[p][2 * k + s] = indom ? __ldcg(u_in + ny) : finf();
+                            if constexpr (MP) nbq[p][2 * k + s] = indom ? __ldcg(q_in + ny) : 0;
+                        }
                     } else {
-                        const int ny = indom ? bilevel_index<D, TL>(yt, I.shape_o) : 0;
-                        nbv[p][2 * k + s] = indom ? __ldcg(u_in + ny) : finf();
-                        if constexpr (MP) nbq[p][2 * k + s] = indom ? __ldcg(q_in + ny) : 0;
+                        int slot = TL::local(yi);
+                        if (!intile) {
+                            slot = TL::SIZE + (p * NTOT + 2 * k + s) * 32 + lane;
+                            const int ny = indom ? bilevel_index<D, TL>(yt, I.shape_o) : 0;
+                            us[slot] = indom ? __ldcg(u_in + ny) : finf();
+                        }
+                        nba[p][2 * k + s] = us_addr + 4u * (unsigned)slot;
                     }
                 }
             }
@@ -349,7 +399,14 @@ struct Visit {
                         float v[NACT], w[NACT];
 #pragma unroll
                         for (int k = 0; k < NACT; ++k) {
-                            const float a = neighbour(nbv[p][2 * k], us), b = neighbour(nbv[p][2 * k + 1], us);
+                            float a, b;
+                            if constexpr (kSlots) {
+                                a = lds(nba[p][2 * k]);
+                                b = lds(nba[p][2 * k + 1]);
+                            } else {
+                                a = neighbour(nbv[p][2 * k], us);
+                                b = neighbour(nbv[p][2 * k + 1], us);
+                            }
                             v[k] = a > b ? b : a;
                             w[k] = wts[p][k];
                         }
@@ -461,14 +518,33 @@ __device__ __forceinline__ void dispatch(const Sched &S, int t, int e, int lane,
 
 constexpr int kMaxTileSize = 256;
 
+// Shared floats per warp for the variants of VMASK.
+template <unsigned VMASK>
+constexpr int smem_floats() {
+    int m = 0;
+    if ((VMASK >> V_ISO2_8) & 1) m = std::max(m, Visit<Tile<2, 8, 8, 1>, AGD_MODEL_ISOTROPIC>::kSmemFloats);
+    if ((VMASK >> V_ISO2_16) & 1) m = std::max(m, Visit<Tile<2, 16, 16, 1>, AGD_MODEL_ISOTROPIC>::kSmemFloats);
+    if ((VMASK >> V_RIEM2_8) & 1) m = std::max(m, Visit<Tile<2, 8, 8, 1>, AGD_MODEL_RIEMANN>::kSmemFloats);
+    if ((VMASK >> V_ISO3_4) & 1) m = std::max(m, Visit<Tile<3, 4, 4, 4>, AGD_MODEL_ISOTROPIC>::kSmemFloats);
+    if ((VMASK >> V_RIEM3_4) & 1) m = std::max(m, Visit<Tile<3, 4, 4, 4>, AGD_MODEL_RIEMANN>::kSmemFloats);
+    if ((VMASK >> V_RIEM2_16) & 1) m = std::max(m, Visit<Tile<2, 16, 16, 1>, AGD_MODEL_RIEMANN>::kSmemFloats);
+    if (VMASK & kMpVariants) m = std::max(m, 2 * kMaxTileSize);
+    return m;
+}
+
 template <unsigned VMASK>
 struct EikonalVisitor {
-    // 256-point tiles keep 8 points per lane in registers: fewer resident warps.
+    // Resident 4-warp CTAs per SM the register budget must allow: 256-point tiles
+    // keep 8 points per lane in registers, Riemann3 twelve neighbours per point,
+    // multiprecision an integer part beside every value.
     static constexpr int kMinCtas =
-        (VMASK & ((1u << V_RIEM2_16) | (1u << V_ISO2_16) | (1u << V_ISO2_16_MP))) ? 4 : 6;
+        (VMASK & ((1u << V_RIEM2_16) | (1u << V_ISO2_16) | (1u << V_ISO2_16_MP))) ? 4
+        : (VMASK & ((1u << V_RIEM3_4) | (1u << V_RIEM3_4_MP)))                    ? 6
+        : (VMASK & kMpVariants)                                                   ? 7
+                                                                                  : 9;
     struct Args {};
     struct Smem {
-        float u[2 * kMaxTileSize];  // values, then the integer parts with multiprecision
+        float u[smem_floats<VMASK>()];  // values, then out-of-tile neighbours or integer parts
     };
     __device__ __forceinline__ static void visit(const Sched &S, const Args &, int t, int, int e, int lane, Smem &sm) {
         dispatch<VMASK>(S, t, e, lane, sm.u);
