@@ -454,7 +454,6 @@ struct Visit {
             else { sn = front; prop = true; }
         } else {
             sn = 1;
-            if (lane == 0) push_tile(S, I, ii, t, e);
             if (front > 2) {
                 const int sq = nb >= 0 ? sp_nb - 1 : -1;
                 int mx = sq;
@@ -468,7 +467,10 @@ struct Visit {
             unsigned *arr = (e & 1) ? S.score1 : S.score0;
             __stcg(arr + t, ((unsigned)e << 8) | (unsigned)sn);
         }
-        if (prop && nb >= 0) push_tile(S, I, ii, nb, e);
+        // The pushes of the tile itself (lane 2D, when changed) and of its
+        // neighbours (lanes 0..2D-1) go out together.
+        const int target = lane == 2 * D ? (changed ? t : -1) : (prop ? nb : -1);
+        if (target >= 0) push_tile(S, I, ii, target, e);
     }
 };
 

@@ -1,13 +1,14 @@
 """BatchSolver (repeated batched solves of one configuration): every instance
-of a batch must give the values of the reference's own kernels (golden case) or
-of the CPU oracle (seeded cases) for that instance, 1e-5 relative, on two
-submissions in a row, from host (page-locked or not) and from device inputs."""
+of a batch must give the values of the reference's own kernels (golden case,
+1e-5 relative) or the scheme's discrete solution (seeded cases, the criteria
+of parity.py) for that instance, on two submissions in a row, from host
+(page-locked or not) and from device inputs."""
 import numpy as np
 import pytest
 import torch
 
 from conftest import load_case
-from oracle import oracle as O
+from parity import TIGHT, TIGHT_REL, assert_near_discrete, discrete_solution
 
 pytestmark = pytest.mark.gpu
 REL = 1e-5
@@ -22,8 +23,8 @@ def _rel(a, b):
 
 def _template(case):
     from adaptivegriddiscretizations_b200 import Eikonal
-    keys = ("model", "dims", "gridScales", "origin")
-    return Eikonal.dictIn({"mode": "gpu", "verbosity": 0, **{k: case[k] for k in keys}})
+    keys = ("model", "dims", "gridScales", "origin", "atol", "rtol")
+    return Eikonal.dictIn({"mode": "gpu", "verbosity": 0, **{k: case[k] for k in keys if k in case}})
 
 
 def _riemann_fields(n, batch, seed, nseeds=3, nd=2):
@@ -82,10 +83,14 @@ def test_riemann2_batch_vs_oracle_host_and_device_inputs():
     solver = Eikonal.BatchSolver(_template(_case("Riemann2", n, None, ss[0])), B)
     v_host = solver.solve(metric=ms, seeds=ss).cpu().numpy()  # pageable numpy inputs
     v_dev = solver.solve(metric=torch.from_numpy(ms).cuda(), seeds=torch.from_numpy(ss).cuda()).cpu().numpy()
+    tight = Eikonal.BatchSolver(_template(dict(_case("Riemann2", n, None, ss[0]), **TIGHT)), B)
+    v_tight = tight.solve(metric=ms, seeds=ss).cpu().numpy()
     for i in range(B):
-        r = O.run(_case("Riemann2", n, ms[i], ss[i]), np.float32, nthreads=8)["values"]
-        assert _rel(v_host[i], r) < REL
-        assert _rel(v_dev[i], r) < REL
+        case = _case("Riemann2", n, ms[i], ss[i])
+        exact = discrete_solution(case)
+        assert_near_discrete(v_host[i], case, exact)
+        assert_near_discrete(v_dev[i], case, exact)
+        assert _rel(v_tight[i], exact) < TIGHT_REL
 
 
 def test_isotropic2_per_instance_cost_tolerance():
@@ -99,8 +104,7 @@ def test_isotropic2_per_instance_cost_tolerance():
     solver = Eikonal.BatchSolver(_template(_case("Isotropic2", n, None, seeds[0])), B)
     v = solver.solve(cost=costs, seeds=seeds).cpu().numpy()
     for i in range(B):
-        r = O.run(_case("Isotropic2", n, None, seeds[i], cost=costs[i]), np.float32, nthreads=8)["values"]
-        assert _rel(v[i], r) < REL
+        assert_near_discrete(v[i], _case("Isotropic2", n, None, seeds[i], cost=costs[i]))
 
 
 def test_riemann3_batch_vs_oracle():
@@ -110,8 +114,7 @@ def test_riemann3_batch_vs_oracle():
     solver = Eikonal.BatchSolver(_template(_case("Riemann3", n, None, ss[0])), B)
     v = solver.solve(metric=ms, seeds=ss).cpu().numpy()
     for i in range(B):
-        r = O.run(_case("Riemann3", n, ms[i], ss[i]), np.float32, nthreads=8)["values"]
-        assert _rel(v[i], r) < REL
+        assert_near_discrete(v[i], _case("Riemann3", n, ms[i], ss[i]))
 
 
 def test_seeds_outside_the_domain():

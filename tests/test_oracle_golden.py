@@ -98,3 +98,27 @@ def test_selling_vs_agd_selling(nd):
         if _canonical(w[i], e[i], tw) != _canonical(f["agd_w"][i], f["agd_e"][i], tw):
             bad += 1
     assert bad == 0
+
+
+def _seeded_riemann2(n, seed, lam_max=30.0):
+    from scipy.ndimage import gaussian_filter
+    rng = np.random.default_rng(seed)
+    g1 = gaussian_filter(rng.standard_normal((n, n)), n / 32, mode="wrap")
+    g2 = gaussian_filter(rng.standard_normal((n, n)), n / 32, mode="wrap")
+    th, lam = np.arctan2(g1, g2), rng.uniform(1, lam_max, (n, n))
+    c, s = np.cos(th), np.sin(th)
+    m = np.stack([c * c + lam * s * s, c * s * (1 - lam), s * s + lam * c * c], -1).astype(np.float32)
+    return dict(model="Riemann2", dims=np.array([n, n], np.float32), gridScales=np.full(2, 1.0 / n, np.float32),
+                origin=np.zeros(2, np.float32), metric=m, seeds=rng.uniform(0.1, 0.9, (3, 2)).astype(np.float32))
+
+
+@pytest.mark.parametrize("seed", [11, 12])
+def test_reference_scheme_meets_the_parity_criteria(seed):
+    """The criteria the GPU values are held to (parity.py) are met by the
+    reference's own float32 scheme (the oracle, pinned above to the reference's
+    kernels), and with tight tolerances it reaches the discrete solution."""
+    from parity import TIGHT, TIGHT_REL, assert_near_discrete, discrete_solution, rel_err
+    case = _seeded_riemann2(80, seed)
+    exact = discrete_solution(case)
+    assert_near_discrete(O.run(case, np.float32, nthreads=4)["values"], case, exact)
+    assert rel_err(O.run(dict(case, **TIGHT), np.float32, nthreads=4)["values"], exact) < TIGHT_REL
