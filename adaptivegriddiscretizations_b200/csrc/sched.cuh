@@ -177,6 +177,20 @@ __device__ __forceinline__ unsigned long long ld_acquire_u64(const unsigned long
 __device__ __forceinline__ void st_release_u64(unsigned long long *p, unsigned long long v) {
     asm volatile("st.release.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
 }
+// Relaxed (strong, unordered) forms for the queue slots.  Everything a visit
+// reads that other warps write during the solve is read through L2 (ld.cg) at
+// addresses that depend on the slot's tile, and the producer's release store
+// of the entry makes those writes visible at L2 first; an acquire here would
+// add a fence and drop the L1 copies of the read-only data (instance
+// descriptors, stencils, right-hand sides) at every visit.
+__device__ __forceinline__ unsigned long long ld_relaxed_u64(const unsigned long long *p) {
+    unsigned long long v;
+    asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void st_relaxed_u64(unsigned long long *p, unsigned long long v) {
+    asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
 
 // Tile t is to be visited at epoch e+1 of its instance (pushed during epoch e).
 __device__ __forceinline__ void push_tile(const Sched &S, const Inst &I, int ii, int t, int e) {
@@ -198,7 +212,7 @@ __device__ __forceinline__ unsigned score_at(const Sched &S, int t, int e) {
 __device__ __forceinline__ bool put_slot(const Sched &S, unsigned ticket, int epoch, unsigned tile) {
     unsigned long long *slot = S.queue + ticket % S.qcap;
     const unsigned long long t0 = globaltimer();
-    while (ld_acquire_u64(slot) != kSlotEmpty) {  // the previous lap's entry is not yet taken
+    while (ld_relaxed_u64(slot) != kSlotEmpty) {  // the previous lap's entry is not yet taken
         if (globaltimer() - t0 > S.timeout_ns) {
             atomicOr(&S.ctrl->err, (unsigned)AGD_STATUS_WATCHDOG);
             return false;
@@ -271,9 +285,9 @@ __device__ __forceinline__ unsigned long long take_slot(const Sched &S, unsigned
     unsigned long long t0 = globaltimer();
     unsigned backoff = 32;
     for (unsigned it = 0;; ++it) {
-        const unsigned long long v = ld_acquire_u64(slot);
+        const unsigned long long v = ld_relaxed_u64(slot);
         if (v != kSlotEmpty && (unsigned)(v >> 44) == (h & 0xfffffu)) {
-            st_release_u64(slot, kSlotEmpty);
+            st_relaxed_u64(slot, kSlotEmpty);  // the slot is free for the next lap
             return v;
         }
         if ((it & 15u) == 15u) {
@@ -300,13 +314,15 @@ __device__ __forceinline__ unsigned long long take_slot(const Sched &S, unsigned
 // Visitor::kMinCtas: resident 4-warp CTAs per SM that its register budget must allow.
 constexpr int kSmemInst = 1024;  // instances whose tile bases a CTA keeps in shared memory
 
-// Decrement with acquire-release semantics: publishes this warp's writes and,
-// for the warp that brings the count to zero, makes everyone else's visible.
-__device__ __forceinline__ int atomic_dec_acq_rel(int *p) {
+// Decrement with release semantics (publishes this warp's writes); the warp
+// that brings the count to zero then fences, which makes everyone else's
+// writes visible to it (the acquire half is needed only there).
+__device__ __forceinline__ int atomic_dec_release(int *p) {
     int old;
-    asm volatile("atom.acq_rel.gpu.global.add.s32 %0, [%1], -1;" : "=r"(old) : "l"(p) : "memory");
+    asm volatile("atom.release.gpu.global.add.s32 %0, [%1], -1;" : "=r"(old) : "l"(p) : "memory");
     return old;
 }
+__device__ __forceinline__ void fence_acq_rel() { asm volatile("fence.acq_rel.gpu;" ::: "memory"); }
 
 template <class Visitor, int WPB>
 __global__ void __launch_bounds__(WPB * 32, Visitor::kMinCtas * 4 / WPB) sched_worker(Sched S, typename Visitor::Args VA) {
@@ -344,9 +360,12 @@ __global__ void __launch_bounds__(WPB * 32, Visitor::kMinCtas * 4 / WPB) sched_w
         Visitor::visit(S, VA, (int)t, ii, e, lane, smem[warp]);
         int lastone = 0;
         __syncwarp();
-        if (lane == 0) lastone = atomic_dec_acq_rel(&S.ist[ii].pending) == 1;
+        if (lane == 0) lastone = atomic_dec_release(&S.ist[ii].pending) == 1;
         lastone = __shfl_sync(kFull, lastone, 0);
-        if (lastone) close_epoch(S, ii, e, lane);
+        if (lastone) {
+            fence_acq_rel();
+            close_epoch(S, ii, e, lane);
+        }
     }
 }
 
