@@ -191,6 +191,7 @@ __device__ __forceinline__ unsigned long long ld_relaxed_u64(const unsigned long
 __device__ __forceinline__ void st_relaxed_u64(unsigned long long *p, unsigned long long v) {
     asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
 }
+__device__ __forceinline__ void fence_acq_rel() { asm volatile("fence.acq_rel.gpu;" ::: "memory"); }
 
 // Tile t is to be visited at epoch e+1 of its instance (pushed during epoch e).
 __device__ __forceinline__ void push_tile(const Sched &S, const Inst &I, int ii, int t, int e) {
@@ -209,6 +210,8 @@ __device__ __forceinline__ unsigned score_at(const Sched &S, int t, int e) {
     return (int)(w >> 8) == e ? (w & 0xffu) : 0u;
 }
 
+// Writes the entry of `ticket` once its slot is free.  The caller has made its
+// earlier writes visible (a release fence), so the entry is a relaxed store.
 __device__ __forceinline__ bool put_slot(const Sched &S, unsigned ticket, int epoch, unsigned tile) {
     unsigned long long *slot = S.queue + ticket % S.qcap;
     const unsigned long long t0 = globaltimer();
@@ -219,7 +222,7 @@ __device__ __forceinline__ bool put_slot(const Sched &S, unsigned ticket, int ep
         }
         __nanosleep(64);
     }
-    st_release_u64(slot, slot_word(ticket, epoch, tile));
+    st_relaxed_u64(slot, slot_word(ticket, epoch, tile));
     return true;
 }
 
@@ -229,6 +232,7 @@ static __device__ void enqueue_warp(const Sched &S, const int *src, int n, int e
     unsigned start = 0;
     if (lane == 0) start = atomicAdd(&S.ctrl->tail, (unsigned)n);
     start = __shfl_sync(kFull, start, 0);
+    fence_acq_rel();  // release: the instance state and the tiles' values before the entries
     for (int k = lane; k < n; k += 32)
         if (!put_slot(S, start + (unsigned)k, e, (unsigned)__ldcg(src + k))) break;
     __syncwarp();
@@ -258,6 +262,7 @@ static __device__ void close_epoch(const Sched &S, int ii, int e, int lane) {
             unsigned start = 0;
             if (lane == 0) start = atomicAdd(&S.ctrl->tail, (unsigned)S.nwarps);
             start = __shfl_sync(kFull, start, 0);
+            fence_acq_rel();
             for (int k = lane; k < S.nwarps; k += 32)
                 if (!put_slot(S, start + (unsigned)k, 0, kExitTile)) break;
         }
@@ -322,7 +327,6 @@ __device__ __forceinline__ int atomic_dec_release(int *p) {
     asm volatile("atom.release.gpu.global.add.s32 %0, [%1], -1;" : "=r"(old) : "l"(p) : "memory");
     return old;
 }
-__device__ __forceinline__ void fence_acq_rel() { asm volatile("fence.acq_rel.gpu;" ::: "memory"); }
 
 template <class Visitor, int WPB>
 __global__ void __launch_bounds__(WPB * 32, Visitor::kMinCtas * 4 / WPB) sched_worker(Sched S, typename Visitor::Args VA) {
