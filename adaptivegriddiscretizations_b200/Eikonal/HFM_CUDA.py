@@ -209,7 +209,7 @@ class Interface:
         self.ndim = len(np.asarray(hfmIn.host("dims")).reshape(-1))
         if self.ndim != int(self.model[-1]):
             raise ValueError(f"Model {self.model} expects {self.model[-1]} dimensions, got dims of length {self.ndim}")
-        self.stats = {"eikonal": {}, "flow": {}, "geodesic": {}, "reverseAD": {}}
+        self.stats = {"eikonal": {}, "flow": {}, "geodesic": {}, "forwardAD": {}, "reverseAD": {}}
 
     @property
     def model_(self):
@@ -377,6 +377,13 @@ class Interface:
             raise ValueError(f"Field cost has incorrect dimensions. Found {tuple(cost.shape)}, "
                              f"whereas domain has shape {self.shape}")
         self.cost = cost
+        # forward AD (_SetGeometry.py:231-233): the cost's first order variations, (*shape, n)
+        cv = self.GetValue("costVariation", default=None, help="First order variation of the cost function")
+        if cv is not None:
+            cv = _to_tensor(cv)
+            if cv.dim() != self.ndim + 1 or tuple(cv.shape[:-1]) != self.shape:
+                raise ValueError(f"costVariation has shape {tuple(cv.shape)}; expected {self.shape} + (n,)")
+        self.costVariation = cv
         if self.HasValue("atol") and self.HasValue("rtol"):
             tol = None
         else:
@@ -437,6 +444,16 @@ class Interface:
             raise ValueError("Missing value for key seeds (trigger-only fronts are not available in this build)")
         seedValues = self.GetValue("seedValues", default=torch.zeros(len(seeds), device="cuda"),
                                    array_float=(len(seeds),), help="Initial value for the front propagation")
+        sv = self.GetValue("seedValueVariation", default=None,
+                           help="First order variation of the seed values, (nseeds, n), for forward AD")
+        if sv is not None:
+            sv = _to_tensor(sv)
+            if sv.dim() != 2 or sv.shape[0] != len(seeds):
+                raise ValueError(f"seedValueVariation has shape {tuple(sv.shape)}; expected ({len(seeds)}, n)")
+            if self.costVariation is not None and sv.shape[1] != self.costVariation.shape[-1]:
+                raise ValueError("costVariation and seedValueVariation have different numbers of variations")
+        self.seedValueVariation = sv
+        self.forwardAD = self.costVariation is not None or sv is not None
         seedRadius = self.GetValue("seedRadius", default=0.0,
                                    help="Spread the seeds over a radius given in pixels, so as to improve accuracy.")
         if seedRadius:
@@ -546,7 +563,7 @@ class Interface:
     def PostProcess(self):
         """Upwind flow, if needed (agd/Eikonal/HFM_CUDA/_PostProcess.py:46-95)."""
         self.combine_multiprecision()
-        self.flow_needed = self.reverseAD or self.hasTips or self.exportGeodesicFlow
+        self.flow_needed = self.reverseAD or self.forwardAD or self.hasTips or self.exportGeodesicFlow
         if not self.flow_needed:
             return
         L = _lib.lib()
@@ -555,7 +572,7 @@ class Interface:
         self.flow_vector = torch.empty(self.ndim * self.size_tot, dtype=torch.float32, device="cuda")
         self.flow_weightsum = torch.empty(self.size_tot, dtype=torch.float32, device="cuda")
         self.flow_weights = self.flow_indices = None
-        if self.reverseAD:
+        if self.reverseAD or self.forwardAD:
             self.flow_weights = torch.empty(nact * self.size_tot, dtype=torch.float32, device="cuda")
             self.flow_indices = torch.empty(nact * self.size_tot, dtype=torch.int32, device="cuda")
         inst = self.instance()
@@ -567,7 +584,9 @@ class Interface:
             self.hfmOut["flow"] = fv * (-h)
 
     def SolveAD(self):
-        """Reverse-mode sensitivity (agd/Eikonal/HFM_CUDA/_PostProcess.py:155-219)."""
+        """Forward and reverse differentiation (agd/Eikonal/HFM_CUDA/_PostProcess.py:155-219)."""
+        if self.forwardAD:
+            self._forward_ad()
         if not self.reverseAD:
             return
         L = _lib.lib()
@@ -606,6 +625,47 @@ class Interface:
         allS[pos] = 0
         self.hfmOut["costSensitivity"] = allS
         self.hfmOut["seedValueSensitivity"] = seedS
+
+    def _forward_ad(self):
+        """valueVariation (*shape, n): the linearised solve with the right-hand side
+        cost * costVariation, and seedValueVariation at the seeds
+        (_PostProcess.py:181-191).  The reference returns the values as a dense AD
+        array with these coefficients; they are the hfmOut key valueVariation here."""
+        L = _lib.lib()
+        cv, sv = self.costVariation, self.seedValueVariation
+        n = cv.shape[-1] if cv is not None else sv.shape[1]
+        if cv is None:
+            cv = torch.zeros(self.shape + (n,), dtype=torch.float32, device="cuda")
+        value = (self.cost.expand(self.shape) if self.cost.dim() == 0 else self.cost).clone()
+        pos = tuple(torch.as_tensor(self.seedIndices.T, device="cuda").long())
+        value[pos] = self.seed_values.to(value.dtype)
+        rhs_all = cv * value[..., None]
+        rhs_all[pos] = sv if sv is not None else 0.0
+        inst = self.instance()
+        nbytes = L.agd_reverse_workspace_bytes(ctypes.byref(inst))
+        ws = torch.empty(max(int(nbytes), 1), dtype=torch.uint8, device="cuda")
+        stats = torch.zeros(2, dtype=torch.int64, device="cuda")
+        rtol = _FLOAT_RES * 5.0
+        out = []
+        for j in range(n):
+            col = rhs_all[..., j].contiguous()
+            r_t = torch.empty(self.size_tot, dtype=torch.float32, device="cuda")
+            _lib.check(L.agd_block_expand(self.ndim, self.c_shape, self.c_shape_i, 1, _lib.ptr(col), 0,
+                                          ctypes.c_float(0.0), _lib.ptr(r_t), self.stream), "forward rhs")
+            fin = col[torch.isfinite(col)]
+            atol = float(rtol * fin.abs().mean()) if fin.numel() else 0.0
+            du = torch.empty(self.size_tot, dtype=torch.float32, device="cuda")
+            _lib.check(L.agd_forward(ctypes.byref(inst), _lib.ptr(self.flow_weights), _lib.ptr(self.flow_indices),
+                                     _lib.ptr(self.flow_weightsum), _lib.ptr(r_t), _lib.ptr(du),
+                                     ctypes.c_float(atol), ctypes.c_float(rtol), _lib.ptr(ws), int(nbytes),
+                                     _lib.ptr(stats), None, self.stream), "forward")
+            st = stats.cpu().numpy()
+            status = int((st[0] >> 32) & 0xffffffff)
+            if status:
+                raise _lib.AgdError(status, "forward variation solve failed on the device")
+            self.stats["forwardAD"] = {"niter_o": int(st[0] & 0xffffffff), "nupdate_o_total": int(st[1])}
+            out.append(self.squeeze(du))
+        self.hfmOut["valueVariation"] = torch.stack(out, dim=-1)
 
     def GetGeodesics(self):
         """Geodesic backtracking (agd/Eikonal/HFM_CUDA/_GetGeodesics.py:9-147)."""

@@ -83,6 +83,8 @@ SIGNATURES = {
     "agd_reverse_workspace_bytes": (ctypes.c_size_t, [_P]),
     "agd_reverse": (_I, [_P, _P, _P, _P, _P, _P, ctypes.c_float, ctypes.c_float, _P, ctypes.c_size_t, _P, _P,
                          _P]),
+    "agd_forward": (_I, [_P, _P, _P, _P, _P, _P, ctypes.c_float, ctypes.c_float, _P, ctypes.c_size_t, _P, _P,
+                         _P]),
     "agd_last_error": (ctypes.c_char_p, []),
     "agd_version": (_I, []),
 }

@@ -1,10 +1,12 @@
-// Reverse-mode sensitivity of the eikonal solution on B200.
+// Forward and reverse-mode differentiation of the eikonal solution on B200.
 //
 // Linearising sum_k w_k (u - v_k)_+^2 = c^2 at the solution gives, at every
 // non-seed point x, diag(x) du(x) - sum_k fw_k(x) du(y_k(x)) = r(x), where
 // fw_k are the upwind flow weights, y_k(x) the upwind neighbours and diag the
-// weight sum (1 at seeds and outside the domain).  The reverse mode solves the
-// transposed system  diag(x) lam(x) - sum_{z: y_k(z) = x} fw_k(z) lam(z) = s(x)
+// weight sum (1 at seeds and outside the domain).  The forward mode solves it
+// for r = c dc (dc a variation of the cost; r is the seed value's variation at
+// a seed); the reverse mode solves the transposed system
+// diag(x) lam(x) - sum_{z: y_k(z) = x} fw_k(z) lam(z) = s(x)
 // (agd/Eikonal/HFM_CUDA/_PostProcess.py:155-219).
 //
 // The reference transposes the graph with an iterative claim loop relaunched
@@ -14,9 +16,12 @@
 // (rows sorted, so sums are deterministic), then the tile scheduler of the
 // eikonal solver with a linear tile visit.  Every tile is visited at the first
 // epoch; afterwards a point whose value moved activates exactly the tiles of
-// the points that depend on it (its forward upwind neighbours), so
-// dependencies that skip over tiles are never missed.
+// the points that depend on it (reverse: its upwind neighbours; forward: the
+// points it is an upwind neighbour of, from the transpose), so dependencies
+// that skip over tiles are never missed.
 #include <cuda_runtime.h>
+
+#include <cstdio>
 
 #include "sched.cuh"
 
@@ -144,7 +149,10 @@ struct LinArgs {
     float atol, rtol;
 };
 
-template <int SIZE>
+// FWD: rows from the forward flow planes (fw, fidx), activation through the
+// transpose (rowptr, src); reverse: rows from the transpose, activation
+// through the forward planes.
+template <int SIZE, bool FWD>
 struct LinearVisitor {
     static constexpr int P = SIZE / 32;
     static constexpr int kMaxSweeps = 4 * SIZE;  // in-tile chains are shorter than the tile
@@ -173,9 +181,18 @@ struct LinearVisitor {
             float a = __ldg(A.sens + n_t);
             r0[p] = __ldg(A.rowptr + n_t);
             r1[p] = __ldg(A.rowptr + n_t + 1);
-            for (int j = r0[p]; j < r1[p]; ++j) {  // sources outside the tile: read once per visit
-                const int z = __ldg(A.src + j);
-                if ((long long)z / SIZE != n_o) a += __ldg(A.wt + j) * __ldcg(A.lam + z);
+            if constexpr (FWD) {
+                for (int k = 0; k < A.nact; ++k) {  // upwind neighbours outside the tile: read once per visit
+                    const float w = __ldg(A.fw + k * I.size_tot + n_t);
+                    const int y = __ldg(A.fidx + k * I.size_tot + n_t);
+                    if (w != 0.f && y >= 0 && (long long)y < I.size_tot && (long long)y / SIZE != n_o)
+                        a += w * __ldcg(A.lam + y);
+                }
+            } else {
+                for (int j = r0[p]; j < r1[p]; ++j) {  // sources outside the tile: read once per visit
+                    const int z = __ldg(A.src + j);
+                    if ((long long)z / SIZE != n_o) a += __ldg(A.wt + j) * __ldcg(A.lam + z);
+                }
             }
             acc[p] = a;
         }
@@ -187,9 +204,18 @@ struct LinearVisitor {
             for (int p = 0; p < P; ++p) {
                 const int n_i = lane + 32 * p;
                 float v = acc[p];
-                for (int j = r0[p]; j < r1[p]; ++j) {
-                    const int z = __ldg(A.src + j);
-                    if ((long long)z / SIZE == n_o) v += __ldg(A.wt + j) * sm.l[z - (int)base];
+                if constexpr (FWD) {
+                    const long long n_t = base + n_i;
+                    for (int k = 0; k < A.nact; ++k) {
+                        const float w = __ldg(A.fw + k * I.size_tot + n_t);
+                        const int y = __ldg(A.fidx + k * I.size_tot + n_t);
+                        if (w != 0.f && y >= 0 && (long long)y / SIZE == n_o) v += w * sm.l[y - (int)base];
+                    }
+                } else {
+                    for (int j = r0[p]; j < r1[p]; ++j) {
+                        const int z = __ldg(A.src + j);
+                        if ((long long)z / SIZE == n_o) v += __ldg(A.wt + j) * sm.l[z - (int)base];
+                    }
                 }
                 v = v / diag[p];
                 __syncwarp();
@@ -213,13 +239,21 @@ struct LinearVisitor {
             __stcg(A.lam + n_t, v);
             const bool changed = fabsf(v - old[p]) > A.atol + A.rtol * fabsf(v);
             if (!changed) continue;
-            for (int k = 0; k < A.nact; ++k) {  // the points that depend on this one
-                const float w = __ldg(A.fw + k * I.size_tot + n_t);
-                const int y = __ldg(A.fidx + k * I.size_tot + n_t);
-                if (w == 0.f || y < 0 || (long long)y >= I.size_tot) continue;
-                const int ty = y / SIZE;
-                if (ty == n_o) self = true;
-                else push_tile(S, I, ii, I.tile_base + ty, e);
+            if constexpr (FWD) {
+                for (int j = r0[p]; j < r1[p]; ++j) {  // the points that depend on this one
+                    const int ty = __ldg(A.src + j) / SIZE;
+                    if (ty == n_o) self = true;
+                    else push_tile(S, I, ii, I.tile_base + ty, e);
+                }
+            } else {
+                for (int k = 0; k < A.nact; ++k) {  // the points that depend on this one
+                    const float w = __ldg(A.fw + k * I.size_tot + n_t);
+                    const int y = __ldg(A.fidx + k * I.size_tot + n_t);
+                    if (w == 0.f || y < 0 || (long long)y >= I.size_tot) continue;
+                    const int ty = y / SIZE;
+                    if (ty == n_o) self = true;
+                    else push_tile(S, I, ii, I.tile_base + ty, e);
+                }
             }
         }
         __syncwarp();
@@ -272,18 +306,35 @@ size_t agd_reverse_workspace_bytes(const agd_instance *inst) {
     return R.total;
 }
 
-int agd_reverse(const agd_instance *inst, const float *flow_weights, const int32_t *flow_indices,
-                const float *flow_weightsum, const float *sens, float *lam, float atol, float rtol, void *workspace,
-                size_t workspace_bytes, agd_stats *stats, const agd_launch *launch, agd_stream_t stream) {
-    clear_error();
-    if (!inst || !flow_weights || !flow_indices || !flow_weightsum || !sens || !lam || !workspace)
-        return set_error(AGD_STATUS_INVALID, "agd_reverse: missing array");
+}  // extern "C"
+
+namespace agd {
+
+// The transpose of the flow graph, then the linear solve on the tiles.
+template <bool FWD>
+static int linear_solve(const char *who, const agd_instance *inst, const float *flow_weights,
+                        const int32_t *flow_indices, const float *flow_weightsum, const float *rhs, float *sol,
+                        float atol, float rtol, void *workspace, size_t workspace_bytes, agd_stats *stats,
+                        const agd_launch *launch, cudaStream_t st) {
+    char msg[128];
+    if (!inst || !flow_weights || !flow_indices || !flow_weightsum || !rhs || !sol || !workspace) {
+        snprintf(msg, sizeof(msg), "%s: missing array", who);
+        return set_error(AGD_STATUS_INVALID, msg);
+    }
     RevLayout R;
     std::vector<Inst> insts;
-    if (!rev_layout(inst, R, &insts)) return set_error(AGD_STATUS_INVALID, "agd_reverse: bad instance");
-    if (insts[0].variant < 0) return set_error(AGD_STATUS_UNSUPPORTED, "agd_reverse: tile shape not built");
-    if (workspace_bytes < R.total) return set_error(AGD_STATUS_WORKSPACE, "agd_reverse: workspace too small");
-    cudaStream_t st = (cudaStream_t)stream;
+    if (!rev_layout(inst, R, &insts)) {
+        snprintf(msg, sizeof(msg), "%s: bad instance", who);
+        return set_error(AGD_STATUS_INVALID, msg);
+    }
+    if (insts[0].variant < 0) {
+        snprintf(msg, sizeof(msg), "%s: tile shape not built", who);
+        return set_error(AGD_STATUS_UNSUPPORTED, msg);
+    }
+    if (workspace_bytes < R.total) {
+        snprintf(msg, sizeof(msg), "%s: workspace too small", who);
+        return set_error(AGD_STATUS_WORKSPACE, msg);
+    }
     char *w = static_cast<char *>(workspace);
     int *rowptr = reinterpret_cast<int *>(w + R.rowptr);
     int *cursor = reinterpret_cast<int *>(w + R.cursor);
@@ -293,8 +344,8 @@ int agd_reverse(const agd_instance *inst, const float *flow_weights, const int32
     int *grand = reinterpret_cast<int *>(w + R.grand);
     RevGeom g{R.size_tot, R.nact};
     cudaError_t err = cudaMemsetAsync(cursor, 0, sizeof(int) * R.size_tot, st);
-    if (err == cudaSuccess) err = cudaMemsetAsync(lam, 0, sizeof(float) * R.size_tot, st);
-    if (err != cudaSuccess) return set_cuda_error("reverse clear", err);
+    if (err == cudaSuccess) err = cudaMemsetAsync(sol, 0, sizeof(float) * R.size_tot, st);
+    if (err != cudaSuccess) return set_cuda_error("linear solve clear", err);
     // counts (into cursor), exclusive scan into rowptr, then fill
     rev_count_kernel<<<nb(R.size_tot, 256), 256, 0, st>>>(g, flow_weights, flow_indices, cursor);
     const long long n1 = R.size_tot + 1;
@@ -306,14 +357,35 @@ int agd_reverse(const agd_instance *inst, const float *flow_weights, const int32
     cudaMemsetAsync(cursor, 0, sizeof(int) * R.size_tot, st);
     rev_fill_kernel<<<nb(R.size_tot, 256), 256, 0, st>>>(g, flow_weights, flow_indices, rowptr, cursor, src, wt);
     rev_sort_kernel<<<nb(R.size_tot, 256), 256, 0, st>>>(g, rowptr, src, wt);
-    if ((err = cudaGetLastError()) != cudaSuccess) return set_cuda_error("reverse transpose", err);
+    if ((err = cudaGetLastError()) != cudaSuccess) return set_cuda_error("linear solve transpose", err);
     // solve on the tiles
     err = cudaMemcpyAsync(w + R.L.inst, insts.data(), sizeof(Inst), cudaMemcpyHostToDevice, st);
-    if (err != cudaSuccess) return set_cuda_error("reverse descriptor upload", err);
-    LinArgs A{rowptr, src, wt, flow_weightsum, sens, lam, flow_weights, flow_indices, R.nact, atol, rtol};
-    if (R.size_i == 256) return run_sched<LinearVisitor<256>>(R.L, workspace, 1, A, stats, launch, st);
-    if (R.size_i == 64) return run_sched<LinearVisitor<64>>(R.L, workspace, 1, A, stats, launch, st);
-    return set_error(AGD_STATUS_UNSUPPORTED, "agd_reverse: tile size not built");
+    if (err != cudaSuccess) return set_cuda_error("linear solve descriptor upload", err);
+    LinArgs A{rowptr, src, wt, flow_weightsum, rhs, sol, flow_weights, flow_indices, R.nact, atol, rtol};
+    if (R.size_i == 256) return run_sched<LinearVisitor<256, FWD>>(R.L, workspace, 1, A, stats, launch, st);
+    if (R.size_i == 64) return run_sched<LinearVisitor<64, FWD>>(R.L, workspace, 1, A, stats, launch, st);
+    snprintf(msg, sizeof(msg), "%s: tile size not built", who);
+    return set_error(AGD_STATUS_UNSUPPORTED, msg);
+}
+
+}  // namespace agd
+
+extern "C" {
+
+int agd_reverse(const agd_instance *inst, const float *flow_weights, const int32_t *flow_indices,
+                const float *flow_weightsum, const float *sens, float *lam, float atol, float rtol, void *workspace,
+                size_t workspace_bytes, agd_stats *stats, const agd_launch *launch, agd_stream_t stream) {
+    clear_error();
+    return linear_solve<false>("agd_reverse", inst, flow_weights, flow_indices, flow_weightsum, sens, lam, atol, rtol,
+                               workspace, workspace_bytes, stats, launch, (cudaStream_t)stream);
+}
+
+int agd_forward(const agd_instance *inst, const float *flow_weights, const int32_t *flow_indices,
+                const float *flow_weightsum, const float *rhs, float *du, float atol, float rtol, void *workspace,
+                size_t workspace_bytes, agd_stats *stats, const agd_launch *launch, agd_stream_t stream) {
+    clear_error();
+    return linear_solve<true>("agd_forward", inst, flow_weights, flow_indices, flow_weightsum, rhs, du, atol, rtol,
+                              workspace, workspace_bytes, stats, launch, (cudaStream_t)stream);
 }
 
 }  // extern "C"

@@ -252,6 +252,17 @@ int agd_reverse(const agd_instance *inst, const float *flow_weights, const int32
                 void *workspace, size_t workspace_bytes, agd_stats *stats, const agd_launch *launch,
                 agd_stream_t stream);
 
+/* Forward-mode variation: solves diag*du - W du = rhs on the tiles, the system
+ * itself rather than its transpose (same flow arrays and diag as agd_reverse;
+ * workspace: agd_reverse_workspace_bytes).  rhs = cost * (variation of the
+ * cost), or the seed value's variation at a seed; rhs, du: tile layout.
+ * Replaces SolveAD's forward branch (_PostProcess.py:181-191) and its linear
+ * Update kernel (cuda/Kernel_LinearUpdate.h:99-218). */
+int agd_forward(const agd_instance *inst, const float *flow_weights, const int32_t *flow_indices,
+                const float *flow_weightsum, const float *rhs, float *du, float atol, float rtol,
+                void *workspace, size_t workspace_bytes, agd_stats *stats, const agd_launch *launch,
+                agd_stream_t stream);
+
 /* ------------------------------------------------------------------- misc -- */
 
 const char *agd_last_error(void);

@@ -704,6 +704,43 @@ void agdo_geodesic_chunk(int ndim, const int *shape, int ntips, int max_len, int
 // z->x are the upwind weights fw[k][z] with fidx[k][z] == x.  diag = weightsum,
 // or 1 where weightsum == 0.  Points are swept by decreasing value, repeated
 // until nothing moves, in double precision.
+// Forward linearisation (agd/Eikonal/HFM_CUDA/_PostProcess.py:181-191):
+// fwsum(x) du(x) - sum_k fw_k(x) du(y_k(x)) = rhs(x), diag 1 where fwsum = 0.
+// The upwind neighbours y_k(x) have smaller values than x, so Gauss-Seidel
+// sweeps in increasing order of the values settle in one pass (a second one
+// confirms; ties are harmless).
+int agdo_forward(int nact, long N, const double *values, const double *fw, const int *fidx,
+                 const double *fwsum, const double *rhs, double *du) {
+    std::vector<long> order(N);
+    for (long i = 0; i < N; ++i) order[i] = i;
+    std::stable_sort(order.begin(), order.end(), [&](long a, long b) {
+        const double va = std::isfinite(values[a]) ? values[a] : 1e300;
+        const double vb = std::isfinite(values[b]) ? values[b] : 1e300;
+        return va < vb;
+    });
+    for (long i = 0; i < N; ++i) du[i] = 0;
+    int sweeps = 0;
+    for (; sweeps < 1000; ++sweeps) {
+        double maxchg = 0, maxval = 0;
+        for (long q = 0; q < N; ++q) {
+            const long x = order[q];
+            double acc = rhs[x];
+            for (int k = 0; k < nact; ++k) {
+                const double w = fw[k * N + x];
+                const int y = fidx[k * N + x];
+                if (w != 0 && y != kIntMax && y >= 0 && y < N) acc += w * du[y];
+            }
+            const double d = fwsum[x] == 0 ? 1.0 : fwsum[x];
+            const double nv = acc / d;
+            maxchg = std::max(maxchg, std::fabs(nv - du[x]));
+            maxval = std::max(maxval, std::fabs(nv));
+            du[x] = nv;
+        }
+        if (maxchg <= 1e-15 * std::max(1.0, maxval)) break;
+    }
+    return sweeps;
+}
+
 int agdo_reverse(int nact, long N, const double *values, const double *fw, const int *fidx,
                  const double *fwsum, const double *sens, double *lam) {
     std::vector<long> cnt(N + 1, 0);

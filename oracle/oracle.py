@@ -40,7 +40,8 @@ def build():
 def lib():
     global _lib
     if _lib is None:
-        if not os.path.exists(LIB):
+        src = os.path.join(HERE, "hfm_oracle.cpp")
+        if not os.path.exists(LIB) or (os.path.exists(src) and os.path.getmtime(src) > os.path.getmtime(LIB)):
             build()
         _lib = ctypes.CDLL(LIB)
         _lib.agdo_eikonal.restype = ctypes.c_int
@@ -204,10 +205,39 @@ def reverse(pr, values, flow_weights, flow_indices, flow_weightsum, sens):
     return lam.reshape(pr.shape)
 
 
+def forward(pr, values, flow_weights, flow_indices, flow_weightsum, rhs):
+    """Forward variation du (grid) for the right-hand side `rhs` (grid, float)."""
+    nact = flow_weights.shape[0]
+    N = int(np.prod(pr.shape))
+    du = np.zeros(N)
+    lib().agdo_forward(nact, ctypes.c_long(N), _p(np.ascontiguousarray(values, np.float64).reshape(-1)),
+                       _p(np.ascontiguousarray(flow_weights, np.float64).reshape(nact, -1)),
+                       _p(np.ascontiguousarray(flow_indices, np.int32).reshape(nact, -1)),
+                       _p(np.ascontiguousarray(flow_weightsum, np.float64).reshape(-1)),
+                       _p(np.ascontiguousarray(rhs, np.float64).reshape(-1)), _p(du))
+    return du.reshape(pr.shape)
+
+
+def forward_rhs(pr, cost_variation, seed_value_variation):
+    """Right-hand sides of forward AD, (n, *shape): the seed values' variation at
+    the seeds, the cost's variation times the cost elsewhere (_PostProcess.py:182-183)."""
+    cv = np.moveaxis(np.asarray(cost_variation, np.float64), -1, 0).copy()
+    pos = tuple(pr.seed_idx.T)
+    if seed_value_variation is not None:
+        sv = np.asarray(seed_value_variation, np.float64)
+        for j in range(len(cv)):
+            cv[j][pos] = sv[:, j]
+    else:
+        for j in range(len(cv)):
+            cv[j][pos] = 0.0
+    mask = pr.seed_mask.astype(bool)
+    return np.where(mask, cv, cv * pr.rhs.astype(np.float64))
+
+
 def run(case, dtype=np.float32, nthreads=1):
     """Whole pipeline for a case; returns a dict like the reference's hfmOut."""
     pr = prepare(case)
-    need_flow = "tips" in case or "sensitivity" in case
+    need_flow = "tips" in case or "sensitivity" in case or "costVariation" in case
     r = eikonal(pr, dtype, nthreads=nthreads, flow=need_flow)
     out = dict(values=r["values"], niter_o=r["niter_o"], tile_visits=r["tile_visits"], prepared=pr)
     if need_flow:
@@ -215,6 +245,10 @@ def run(case, dtype=np.float32, nthreads=1):
     if "tips" in case:
         out["geodesics"], out["geodesic_stopping_criteria"] = geodesics(
             pr, r["values"], r["flow_vector"], r["flow_weightsum"], case["tips"])
+    if "costVariation" in case:
+        rhs = forward_rhs(pr, case["costVariation"], case.get("seedValueVariation"))
+        out["valueVariation"] = np.stack(
+            [forward(pr, r["values"], r["flow_weights"], r["flow_indices"], r["flow_weightsum"], x) for x in rhs], -1)
     if "sensitivity" in case:
         sens = np.asarray(case["sensitivity"])[..., 0]
         lam = reverse(pr, r["values"], r["flow_weights"], r["flow_indices"], r["flow_weightsum"], sens)

@@ -10,7 +10,7 @@ The host loops around the kernels restate, in numpy, the reference's driver code
   SetGeometry / SetRHS / SetArgs      agd/Eikonal/HFM_CUDA/_SetGeometry.py:16-282, _SetArgs.py:8-177
   fast_iterative_method, InitStop     _solvers.py:94-120, _StopCriterion.py:62-84
   PostProcess (flow), values_expand   _PostProcess.py:19-95
-  SolveAD (reverse), graph_reverse    _PostProcess.py:155-219, graph_reverse.py:10-77
+  SolveAD (forward, reverse)          _PostProcess.py:155-219, graph_reverse.py:10-77
   GetGeodesics, inf_convolution       _GetGeodesics.py:9-147, inf_convolution.py:24-93
 
 Output: one ``<case>.npz`` per case in this directory, holding the dictIn inputs
@@ -283,6 +283,44 @@ class RefPipeline:
         allS[pos] = 0
         return allS, seedS
 
+    def forward_ad(self, cost_var, seed_var):
+        """Forward AD, _PostProcess.py:181-191: cost_var (*shape, n), seed_var
+        (nseeds, n); rhs = seed variation at seeds, cost variation * cost elsewhere,
+        solved with the forward flow graph.  Returns valueVariation (*shape, n)."""
+        nd = self.ndim
+        diag = self.fws.copy()
+        diag[diag == 0.0] = 1.0
+        indices, weights = self.fi, self.fw
+        cost = np.asarray(self.c.get("cost", np.ones(self.shape, np.float32)), np.float32)
+        cost = np.broadcast_to(cost, self.shape)
+        value = cost.copy()
+        pos = tuple(self.seedIndices.T)
+        value[pos] = np.asarray(self.c.get("seedValues", np.zeros(len(self.seedIndices))), np.float32)
+        n_ad = cost_var.shape[-1]
+        grad = np.moveaxis(np.asarray(cost_var, np.float32), -1, 0).copy()
+        for j in range(n_ad):
+            grad[j][pos] = seed_var[:, j]
+        rhs_grid = np.where(self.seedTags, grad, grad * value).astype(np.float32)
+        L = lib(f"libagdref_lin_{self.md['tag']}_f.so")
+        L.agdref_nindex.restype = ctypes.c_int
+        assert L.agdref_nindex() == len(indices)
+        float_res = np.finfo(np.float32).resolution
+        rtol = np.float32(float_res * 5)
+        domain = np.isfinite(self.values_b)
+        trigger = np.logical_and(np.all(weights == 0.0, axis=0), domain)
+        trig_o = trigger.reshape(self.shape_o + (-1,)).any(-1).astype(np.uint8)
+        out = []
+        for j in range(n_ad):
+            rhs = np.ascontiguousarray(self.bexp(rhs_grid[j], np.nan).astype(np.float32))
+            fin = rhs[np.isfinite(rhs)]
+            atol = np.float32(rtol * np.mean(np.abs(fin)))
+            sol = np.full(rhs.shape, np.inf, np.float32)
+            L.agdref_linear_solve((ctypes.c_int * nd)(*self.shape_o), ctypes.c_float(atol), ctypes.c_float(rtol),
+                                  ptr(sol), ptr(rhs), ptr(diag), ptr(np.ascontiguousarray(indices)),
+                                  ptr(np.ascontiguousarray(weights)), ptr(trig_o), 2000)
+            out.append(self.bsq(sol))
+        return np.stack(out, -1)
+
     def graph_reverse(self, fwd, fwd_weight, invalid, nrev=None):
         L = lib("libagdref_graphrev.so")
         nfwd = len(fwd)
@@ -385,6 +423,15 @@ def make_cases():
         flat = rng.choice(int(np.prod(shp)), 5, replace=False)
         sens.reshape(-1)[flat] = 1.0
         cc["sensitivity"] = sens
+    # forward AD inputs (drawn last, so that the inputs above do not change):
+    # two variations of the cost, and of the seed values
+    for key in ("iso2", "riem2", "riem3"):
+        cc = cases[key]
+        shp = tuple(int(s) for s in cc["dims"])
+        cv = np.stack([smooth_noise(rng, shp, 2.0), np.zeros(shp)], -1).astype(np.float32)
+        cv[..., 1].reshape(-1)[rng.choice(int(np.prod(shp)), 3, replace=False)] = 1.0
+        cc["costVariation"] = cv
+        cc["seedValueVariation"] = rng.uniform(-1, 1, (len(cc["seeds"]), 2)).astype(np.float32)
     return cases
 
 
@@ -413,6 +460,9 @@ def run_case(name, case):
             out["geodesics_concat"] = np.concatenate(geos, axis=1).astype(np.float32)
             out["geodesic_stopping_criteria"] = np.array(stops)
             out["eucl"] = eucl
+        if "costVariation" in case:
+            out["valueVariation"] = pipe.forward_ad(case["costVariation"], case["seedValueVariation"]).astype(
+                np.float32)
         if "sensitivity" in case:
             cs, ss = pipe.reverse_ad(case["sensitivity"])
             out["costSensitivity"] = cs.astype(np.float32)

@@ -122,3 +122,31 @@ def test_reference_scheme_meets_the_parity_criteria(seed):
     exact = discrete_solution(case)
     assert_near_discrete(O.run(case, np.float32, nthreads=4)["values"], case, exact)
     assert rel_err(O.run(dict(case, **TIGHT), np.float32, nthreads=4)["values"], exact) < TIGHT_REL
+
+
+@pytest.mark.parametrize("name", ["iso2", "riem2", "riem3"])
+def test_forward_ad_vs_reference(name):
+    """valueVariation of the oracle (float64, exact solve of the forward
+    linearisation) against the reference's forward AD (its linear kernel, float32)."""
+    case, ref = load_case(name)
+    r = O.run(case, np.float64)
+    want = ref["valueVariation"]
+    got = r["valueVariation"]
+    assert got.shape == want.shape
+    scale = np.abs(want).max()
+    assert np.abs(got - want).max() <= 2e-4 * scale
+
+
+def test_forward_ad_scaling_identity():
+    """A cost variation equal to the cost, with seed values varied by themselves,
+    scales the whole solution: valueVariation == values (EikonalAD_GPU.ipynb's
+    identity, sum of the derivatives w.r.t. a piecewise cost)."""
+    case, _ = load_case("riem2")
+    case = {k: v for k, v in case.items() if k not in ("tips", "sensitivity")}
+    cost = np.ones(tuple(int(s) for s in case["dims"]), np.float32)
+    case["costVariation"] = cost[..., None]
+    case["seedValueVariation"] = np.asarray(case["seedValues"], np.float32)[:, None]
+    r = O.run(dict(case, atol=1e-14, rtol=1e-14), np.float64)  # the identity holds at the fixed point
+    u = r["values"]
+    fin = np.isfinite(u)
+    assert np.abs(r["valueVariation"][..., 0][fin] - u[fin]).max() <= 1e-9 * np.abs(u[fin]).max()
