@@ -6,7 +6,8 @@ The backward pass runs the reverse-mode adjoint of libagd_b200 (agd_reverse)
 with the incoming gradient as the 'sensitivity' right-hand side.  The adjoint
 unknown lam satisfies dJ/dcost = lam * cost (the forward linearisation of the
 scheme uses the right-hand side cost * dcost, agd/Eikonal/HFM_CUDA/_PostProcess.py:181-183),
-and the reference reports lam itself as 'costSensitivity'.
+and the reference reports lam itself as 'costSensitivity'.  Forward mode
+(torch.autograd.forward_ad) runs agd_forward with the tangent as 'costVariation'.
 """
 import torch
 
@@ -30,6 +31,13 @@ class EikonalValues(torch.autograd.Function):
         ctx.hfmIn = h
         ctx.save_for_backward(cost)
         return values
+
+    @staticmethod
+    def jvp(ctx, dcost, _):
+        h = ctx.hfmIn.copy()
+        h["costVariation"] = dcost.detach().float().contiguous()[..., None]
+        out = h.Run()
+        return out["valueVariation"][..., 0]
 
     @staticmethod
     def backward(ctx, grad):

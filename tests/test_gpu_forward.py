@@ -84,3 +84,29 @@ def test_forward_only_seed_variation():
     out2 = make_dictin(case, extra={"seedValueVariation": extra["seedValueVariation"],
                                     "costVariation": np.zeros_like(extra["costVariation"])}).Run()
     np.testing.assert_allclose(vv, out2["valueVariation"].cpu().numpy(), rtol=1e-5, atol=1e-6)
+
+
+def test_autograd_forward_mode():
+    """torch.autograd.forward_ad through EikonalValues: the tangent of the values
+    equals valueVariation, and <w, J t> = <J^T w, t> with the backward pass."""
+    import torch.autograd.forward_ad as fwAD
+    from adaptivegriddiscretizations_b200 import Eikonal
+    from adaptivegriddiscretizations_b200.autograd import eikonal_values
+    case, _, _ = _forward_case("riem2")
+    keys = ("model", "dims", "gridScales", "origin", "metric", "seeds", "seedValues")
+    h = Eikonal.dictIn({k: case[k] for k in keys} | {"verbosity": 0})
+    shape = tuple(int(s) for s in case["dims"])
+    rng = np.random.default_rng(8)
+    cost = torch.as_tensor(np.exp(0.2 * rng.standard_normal(shape)).astype(np.float32), device="cuda")
+    t = torch.as_tensor(rng.standard_normal(shape).astype(np.float32), device="cuda")
+    with fwAD.dual_level():
+        u = eikonal_values(h, fwAD.make_dual(cost, t))
+        jt = fwAD.unpack_dual(u).tangent
+    ref = make_dictin(dict(case, cost=cost.cpu().numpy()),
+                      extra={"costVariation": t.cpu().numpy()[..., None]}).Run()["valueVariation"][..., 0]
+    torch.testing.assert_close(jt, ref, rtol=1e-5, atol=1e-6)
+    w = torch.as_tensor(rng.standard_normal(shape).astype(np.float32), device="cuda")
+    c = cost.clone().requires_grad_(True)
+    (eikonal_values(h, c) * w).sum().backward()
+    lhs, rhs = float((w * jt).sum()), float((c.grad * t).sum())
+    assert abs(lhs - rhs) <= 1e-3 * max(abs(lhs), abs(rhs))
