@@ -343,6 +343,7 @@ class Interface:
             if metric is None and dual is None:
                 raise ValueError("Missing value for key metric")
             src, is_dual = (metric, 0) if metric is not None else (dual, 1)
+            self._metric_is_dual = bool(is_dual)
             flat = _metric_hfm(src, self.ndim)
             symdim = self.ndim * (self.ndim + 1) // 2
             bcast = 1 if flat.dim() == 1 else 0
@@ -444,26 +445,32 @@ class Interface:
             raise ValueError("Missing value for key seeds (trigger-only fronts are not available in this build)")
         seedValues = self.GetValue("seedValues", default=torch.zeros(len(seeds), device="cuda"),
                                    array_float=(len(seeds),), help="Initial value for the front propagation")
-        sv = self.GetValue("seedValueVariation", default=None,
-                           help="First order variation of the seed values, (nseeds, n), for forward AD")
+        # (n, nseeds), as the reference (_SetArgs.py:30-33)
+        sv = self.GetValue("seedValueVariation", default=None, array_float=(-1, len(seeds)),
+                           help="First order variation of the seed values")
         if sv is not None:
-            sv = _to_tensor(sv)
-            if sv.dim() != 2 or sv.shape[0] != len(seeds):
-                raise ValueError(f"seedValueVariation has shape {tuple(sv.shape)}; expected ({len(seeds)}, n)")
-            if self.costVariation is not None and sv.shape[1] != self.costVariation.shape[-1]:
+            if self.costVariation is not None and sv.shape[0] != self.costVariation.shape[-1]:
                 raise ValueError("costVariation and seedValueVariation have different numbers of variations")
         self.seedValueVariation = sv
         self.forwardAD = self.costVariation is not None or sv is not None
-        seedRadius = self.GetValue("seedRadius", default=0.0,
-                                   help="Spread the seeds over a radius given in pixels, so as to improve accuracy.")
-        if seedRadius:
-            raise NotImplementedError("seedRadius spreading is not available in this build")
+        seedRadius = float(self.GetValue(
+            "seedRadius", default=2.0 if self.factoringRadius else 0.0,
+            help="Spread the seeds over a radius given in pixels, so as to improve accuracy."))
         seeds_h = self.hfmIn.host("seeds").reshape(-1, self.ndim)
         ci = self.hfmIn.PointFromIndex(seeds_h, to=True)
-        idx = np.round(ci).astype(np.int64)
-        inside = np.all((idx >= 0) & (idx < np.array(self.shape)), axis=1)
-        if not np.all(inside):
-            raise ValueError(f"Seeds outside the domain: {np.asarray(seeds_h)[~inside].tolist()}")
+        if seedRadius:
+            if len(ci) != 1:
+                raise ValueError("seedRadius spreads a single seed (as the reference's SetRHS does)")
+            idx, vals = self._spread_seed(ci[0], float(_host_scalar(seedValues[0])), seedRadius)
+            seedValues = torch.as_tensor(vals, dtype=torch.float32, device="cuda")
+            self.seed_owner = np.zeros(len(idx), np.int64)  # every spread point comes from seed 0
+        else:
+            idx = np.round(ci).astype(np.int64)
+            inside = np.all((idx >= 0) & (idx < np.array(self.shape)), axis=1)
+            if not np.all(inside):
+                raise ValueError(f"Seeds outside the domain: {np.asarray(seeds_h)[~inside].tolist()}")
+            self.seed_owner = np.arange(len(idx))
+        self.nseeds_in = len(ci)
         self.seedIndices = idx
         self.seed_values = seedValues.contiguous().float()
         self.seed_idx_t = torch.from_numpy(idx.astype(np.int32)).pin_memory().to("cuda", non_blocking=True)
@@ -471,6 +478,54 @@ class Interface:
         _lib.check(L.agd_prep_seeds(self.ndim, self.c_shape, self.c_shape_i, _lib.ptr(self.seed_idx_t),
                                     _lib.ptr(self.seed_values), len(idx), _lib.ptr(self.rhs_t),
                                     _lib.ptr(self.seedbits), None, self.stream), "seeds")
+
+    def _spread_seed(self, seed, seed_value, r):
+        """SetRHS's seed spreading (agd/Eikonal/HFM_CUDA/_SetArgs.py:46-75): the grid
+        points closer than r (index units, inside the domain) to the seed become
+        seeds with value seed_value + (|d|_{M(seed)} + |d|_{M(x)}) / 2, d = x - seed,
+        M the metric with the grid scales and the cost applied (Interface.CostMetric,
+        _Interface.py:202-211), multilinearly interpolated at the seed."""
+        import itertools
+        nd = self.ndim
+        seed = np.asarray(seed, np.float64)
+        shape = np.array(self.shape)
+        aX = [np.arange(int(np.floor(c - r)), int(np.ceil(c + r) + 1)) for c in seed]
+        neigh = np.stack(np.meshgrid(*aX, indexing="ij"), axis=-1).reshape(-1, nd)
+        neigh = neigh[np.linalg.norm(neigh - seed, axis=-1) < r]
+        neigh = neigh[np.all((-0.5 <= neigh) & (neigh < shape - 0.5), axis=-1)]
+        lo = np.clip(np.floor(seed).astype(np.int64), 0, shape - 1)
+        bits = np.array(list(itertools.product((0, 1), repeat=nd)))
+        corners = np.minimum(lo + bits, shape - 1)
+        frac = np.clip(seed - lo, 0.0, 1.0)
+        wc = np.prod(np.where(bits == 1, frac, 1.0 - frac), axis=1)  # multilinear weights
+        pts = np.concatenate([neigh, corners])
+        flat = torch.as_tensor(np.ravel_multi_index(pts.T, self.shape), device="cuda")
+        cost = self.cost.reshape(-1)[flat] if self.cost.dim() else self.cost.expand(len(pts))
+        cost = cost.double().cpu().numpy()
+        h = self.h.astype(np.float64)
+        if self.model_ == "Riemann":
+            sd = nd * (nd + 1) // 2
+            fm = self._metric_flat.reshape(-1, sd)
+            fm = (fm[flat] if fm.shape[0] > 1 else fm.expand(len(pts), sd)).double().cpu().numpy()
+            M = np.zeros((len(pts), nd, nd))
+            k = 0
+            for i in range(nd):
+                for j in range(i + 1):
+                    M[:, i, j] = M[:, j, i] = fm[:, k]
+                    k += 1
+            if self._metric_is_dual:
+                M = np.linalg.inv(M)
+            m = cost[:, None, None] ** 2 * M * np.outer(h, h)  # Riemann.with_costs(h).with_cost(cost)
+            m1 = m[: len(neigh)]
+            m0 = np.tensordot(wc, m[len(neigh):], axes=1)
+        else:  # Diagonal(ones).with_costs(h).with_cost(cost): costs c*h, interpolated as such
+            m1 = (cost[: len(neigh), None] * h) ** 2
+            m1 = np.einsum("ki,ij->kij", m1, np.eye(nd))
+            m0 = np.diag((np.dot(wc, cost[len(neigh):]) * h) ** 2)
+        d = neigh - seed
+        n0 = np.sqrt(np.einsum("ki,ij,kj->k", d, m0, d))
+        n1 = np.sqrt(np.einsum("ki,kij,kj->k", d, m1, d))
+        return neigh.astype(np.int64), (seed_value + 0.5 * (n0 + n1)).astype(np.float32)
 
     def instance(self):
         inst = _lib.AgdInstance()
@@ -624,6 +679,10 @@ class Interface:
         seedS = allS[pos].clone()
         allS[pos] = 0
         self.hfmOut["costSensitivity"] = allS
+        if self.nseeds_in != len(self.seedIndices):  # spread seeds: each depends on its seed with weight 1
+            owner = torch.as_tensor(self.seed_owner, device="cuda")
+            seedS = torch.zeros((self.nseeds_in, seedS.shape[1]), dtype=seedS.dtype,
+                                device="cuda").index_add_(0, owner, seedS)
         self.hfmOut["seedValueSensitivity"] = seedS
 
     def _forward_ad(self):
@@ -633,14 +692,14 @@ class Interface:
         array with these coefficients; they are the hfmOut key valueVariation here."""
         L = _lib.lib()
         cv, sv = self.costVariation, self.seedValueVariation
-        n = cv.shape[-1] if cv is not None else sv.shape[1]
+        n = cv.shape[-1] if cv is not None else sv.shape[0]
         if cv is None:
             cv = torch.zeros(self.shape + (n,), dtype=torch.float32, device="cuda")
         value = (self.cost.expand(self.shape) if self.cost.dim() == 0 else self.cost).clone()
         pos = tuple(torch.as_tensor(self.seedIndices.T, device="cuda").long())
         value[pos] = self.seed_values.to(value.dtype)
         rhs_all = cv * value[..., None]
-        rhs_all[pos] = sv if sv is not None else 0.0
+        rhs_all[pos] = sv.T[torch.as_tensor(self.seed_owner, device="cuda")] if sv is not None else 0.0
         inst = self.instance()
         nbytes = L.agd_reverse_workspace_bytes(ctypes.byref(inst))
         ws = torch.empty(max(int(nbytes), 1), dtype=torch.uint8, device="cuda")
@@ -743,6 +802,10 @@ class Interface:
         self.hfmOut["keys"]["unused"] = list(set(self.hfmIn.keys()) - set(self.hfmOut["keys"]["used"]))
         if self.verbosity >= 1 and self.hfmOut["keys"]["unused"]:
             print(f"!! Warning !! Unused keys from user : {self.hfmOut['keys']['unused']}")
+
+
+def _host_scalar(x):
+    return float(x.item()) if isinstance(x, torch.Tensor) else float(x)
 
 
 def _metric_hfm(src, ndim):

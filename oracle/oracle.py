@@ -111,7 +111,11 @@ def prepare(case):
     seeds = np.asarray(case["seeds"], np.float32).reshape(-1, pr.ndim)
     sv = np.asarray(case.get("seedValues", np.zeros(len(seeds))), np.float32)
     start = pr.origin + 0.5 * pr.h
-    pr.seed_idx = np.round((seeds - start) / pr.h).astype(int)
+    if float(case.get("seedRadius", 0.0)):
+        pr.seed_idx, sv = _spread_seed(pr, case, cost, ((seeds - start) / pr.h)[0], float(sv[0]),
+                                       float(case["seedRadius"]))
+    else:
+        pr.seed_idx = np.round((seeds - start) / pr.h).astype(int)
     rhs = cost.copy()
     mask = np.zeros(pr.shape, np.uint8)
     pos = tuple(pr.seed_idx.T)
@@ -122,6 +126,51 @@ def prepare(case):
     if pr.iso_w is not None:
         pr.iso_w = np.asarray(pr.h.astype(np.float32) ** -2, np.float64)
     return pr
+
+
+def _spread_seed(pr, case, cost, seed, seed_value, r):
+    """Seed spreading (agd/Eikonal/HFM_CUDA/_SetArgs.py:46-75), float64: the grid
+    points within r of the seed (index units) take the value seed_value +
+    (|d|_{M(seed)} + |d|_{M(x)}) / 2 with M the cost-scaled metric in index units
+    (Interface.CostMetric, _Interface.py:202-211), interpolated multilinearly."""
+    nd = pr.ndim
+    shape = np.array(pr.shape)
+    seed = np.asarray(seed, np.float64)
+    axes = [np.arange(int(np.floor(c - r)), int(np.ceil(c + r) + 1)) for c in seed]
+    pts = np.stack(np.meshgrid(*axes, indexing="ij"), -1).reshape(-1, nd)
+    pts = pts[np.linalg.norm(pts - seed, axis=1) < r]
+    pts = pts[np.all((pts >= -0.5) & (pts < shape - 0.5), axis=1)]
+    h = pr.h.astype(np.float64)
+    c = np.asarray(cost, np.float64)
+    if pr.riemann:
+        mf = np.broadcast_to(np.asarray(case["metric"], np.float64), tuple(pr.shape) + (nd * (nd + 1) // 2,))
+        tri = [(i, j) for i in range(nd) for j in range(i + 1)]
+
+        def cm(p):  # cost-scaled metric at grid point p
+            M = np.zeros((nd, nd))
+            for q, (i, j) in enumerate(tri):
+                M[i, j] = M[j, i] = mf[tuple(p)][q]
+            return c[tuple(p)] ** 2 * M * np.outer(h, h)
+    else:
+        def cm(p):
+            return np.diag((c[tuple(p)] * h) ** 2)
+    # multilinear interpolation at the seed: of the metric entries (Riemann), of the costs c*h (Isotropic)
+    lo = np.clip(np.floor(seed).astype(int), 0, shape - 1)
+    frac = np.clip(seed - lo, 0.0, 1.0)
+    m0 = np.zeros((nd, nd))
+    c0 = 0.0
+    for bits in np.ndindex(*([2] * nd)):
+        w = np.prod([f if b else 1.0 - f for b, f in zip(bits, frac)])
+        p = np.minimum(lo + np.array(bits), shape - 1)
+        m0 += w * cm(p)
+        c0 += w * c[tuple(p)]
+    if not pr.riemann:
+        m0 = np.diag((c0 * h) ** 2)
+    vals = []
+    for p in pts:
+        d = p - seed
+        vals.append(seed_value + 0.5 * (np.sqrt(d @ m0 @ d) + np.sqrt(d @ cm(p) @ d)))
+    return pts.astype(int), np.asarray(vals, np.float32)
 
 
 def eikonal(pr, dtype=np.float32, values=None, nthreads=1, flow=False, nitermax=2000):
@@ -219,14 +268,15 @@ def forward(pr, values, flow_weights, flow_indices, flow_weightsum, rhs):
 
 
 def forward_rhs(pr, cost_variation, seed_value_variation):
-    """Right-hand sides of forward AD, (n, *shape): the seed values' variation at
-    the seeds, the cost's variation times the cost elsewhere (_PostProcess.py:182-183)."""
+    """Right-hand sides of forward AD, (n, *shape): the seed values' variation
+    (n, nseeds) at the seeds, the cost's variation times the cost elsewhere
+    (_PostProcess.py:182-183)."""
     cv = np.moveaxis(np.asarray(cost_variation, np.float64), -1, 0).copy()
     pos = tuple(pr.seed_idx.T)
     if seed_value_variation is not None:
         sv = np.asarray(seed_value_variation, np.float64)
         for j in range(len(cv)):
-            cv[j][pos] = sv[:, j]
+            cv[j][pos] = sv[j]
     else:
         for j in range(len(cv)):
             cv[j][pos] = 0.0

@@ -127,7 +127,10 @@ class RefPipeline:
         self.rtol = np.float32(0.0 if self.multip else float_res * 5.0)
         seeds = np.asarray(c["seeds"], np.float32)
         seedValues = np.asarray(c.get("seedValues", np.zeros(len(seeds))), np.float32)
-        seedIdx = np.round(self.point_from_index(seeds, to=True)).astype(int)
+        if c.get("seedRadius", 0.0):
+            seedIdx, seedValues = self.spread_seed(seeds, seedValues, float(c["seedRadius"]), cost)
+        else:
+            seedIdx = np.round(self.point_from_index(seeds, to=True)).astype(int)
         self.seedIndices = seedIdx
         rhs = cost.copy()
         seedTags = np.zeros(self.shape, bool)
@@ -148,6 +151,31 @@ class RefPipeline:
         else:
             self.multip_step = self.multip_max = np.float32(0)
         self.iso_w = (self.h.astype(np.float32) ** -2).astype(np.float32)
+
+    def spread_seed(self, seeds, seedValues, r, cost):
+        """SetRHS's seed spreading (_SetArgs.py:46-75) with the reference's own
+        metric interpolation (Interface.CostMetric, _Interface.py:202-211)."""
+        from agd import AutomaticDifferentiation as ad
+        assert len(seeds) == 1
+        seed = self.point_from_index(seeds, to=True)[0].astype(np.float64)
+        nd = self.ndim
+        if self.model.startswith("Riemann"):
+            metric = self.Metrics.Riemann.from_HFM(np.asarray(self.c["metric"], np.float64))
+        else:
+            metric = self.Metrics.Diagonal(np.ones(nd))
+        cm = metric.with_costs(self.h.astype(np.float64)).with_cost(cost.astype(np.float64))
+        grid = ad.array(np.meshgrid(*(np.arange(s, dtype=np.float64) for s in self.shape), indexing="ij"))
+        cm.set_interpolation(grid)
+        aX = [np.arange(int(np.floor(ci - r)), int(np.ceil(ci + r) + 1)) for ci in seed]
+        neigh = np.stack(np.meshgrid(*aX, indexing="ij"), axis=-1).reshape(-1, nd)
+        close = np.linalg.norm(neigh - seed, axis=-1) < r
+        neigh = neigh[close]
+        inRange = np.all(np.logical_and(-0.5 <= neigh, neigh < np.array(self.shape) - 0.5), axis=-1)
+        neigh = neigh[inRange]
+        diff = (neigh - seed).T
+        m0, m1 = cm.at(seed), cm.at(neigh.T.astype(np.float64))
+        vals = seedValues[0] + 0.5 * (m0.norm(diff) + m1.norm(diff))
+        return neigh.astype(int), vals.astype(np.float32)
 
     def solve(self):
         md = self.md
@@ -285,7 +313,7 @@ class RefPipeline:
 
     def forward_ad(self, cost_var, seed_var):
         """Forward AD, _PostProcess.py:181-191: cost_var (*shape, n), seed_var
-        (nseeds, n); rhs = seed variation at seeds, cost variation * cost elsewhere,
+        (n, nseeds) as the reference's seedValueVariation key (_SetArgs.py:30-33); rhs = seed variation at seeds, cost variation * cost elsewhere,
         solved with the forward flow graph.  Returns valueVariation (*shape, n)."""
         nd = self.ndim
         diag = self.fws.copy()
@@ -299,7 +327,7 @@ class RefPipeline:
         n_ad = cost_var.shape[-1]
         grad = np.moveaxis(np.asarray(cost_var, np.float32), -1, 0).copy()
         for j in range(n_ad):
-            grad[j][pos] = seed_var[:, j]
+            grad[j][pos] = seed_var[j]
         rhs_grid = np.where(self.seedTags, grad, grad * value).astype(np.float32)
         L = lib(f"libagdref_lin_{self.md['tag']}_f.so")
         L.agdref_nindex.restype = ctypes.c_int
@@ -423,6 +451,20 @@ def make_cases():
         flat = rng.choice(int(np.prod(shp)), 5, replace=False)
         sens.reshape(-1)[flat] = 1.0
         cc["sensitivity"] = sens
+    # seeds spread over a radius (_SetArgs.py:46-75): Riemann2 anisotropic, Isotropic2
+    c = dict(cases["riem2"])
+    for k in ("tips", "sensitivity", "seedValues"):
+        c.pop(k, None)
+    c["seeds"] = np.array([[0.43, 0.61]], np.float32)
+    c["seedValues"] = np.array([0.02], np.float32)
+    c["seedRadius"] = 2.5
+    cases["riem2_radius"] = c
+    c = dict(cases["iso2"])
+    for k in ("tips", "sensitivity", "seedValues"):
+        c.pop(k, None)
+    c["seeds"] = np.array([[0.37, 0.3]], np.float32)
+    c["seedRadius"] = 2.0
+    cases["iso2_radius"] = c
     # forward AD inputs (drawn last, so that the inputs above do not change):
     # two variations of the cost, and of the seed values
     for key in ("iso2", "riem2", "riem3"):
@@ -431,7 +473,7 @@ def make_cases():
         cv = np.stack([smooth_noise(rng, shp, 2.0), np.zeros(shp)], -1).astype(np.float32)
         cv[..., 1].reshape(-1)[rng.choice(int(np.prod(shp)), 3, replace=False)] = 1.0
         cc["costVariation"] = cv
-        cc["seedValueVariation"] = rng.uniform(-1, 1, (len(cc["seeds"]), 2)).astype(np.float32)
+        cc["seedValueVariation"] = np.ascontiguousarray(rng.uniform(-1, 1, (len(cc["seeds"]), 2)).T).astype(np.float32)
     return cases
 
 

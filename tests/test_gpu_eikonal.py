@@ -10,7 +10,7 @@ import numpy as np
 import pytest
 import torch
 
-from conftest import CASES, GOLDEN, load_case, make_dictin
+from conftest import CASES, GOLDEN, RADIUS_CASES, load_case, make_dictin
 from parity import TIGHT, TIGHT_REL, assert_near_discrete, discrete_solution
 from oracle import oracle as O
 
@@ -25,7 +25,7 @@ def _rel(a, b):
     return (np.abs(a[fin] - b[fin]) / np.maximum(np.abs(b[fin]), 1e-30)).max()
 
 
-@pytest.mark.parametrize("name", CASES)
+@pytest.mark.parametrize("name", CASES + RADIUS_CASES)
 def test_values_vs_reference(name):
     case, ref = load_case(name)
     case = {k: v for k, v in case.items() if k not in ("tips", "sensitivity")}

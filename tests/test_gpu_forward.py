@@ -41,7 +41,7 @@ def test_forward_scaling_identity(name):
     cost = np.broadcast_to(np.asarray(case.get("cost", 1.0), np.float32), shape)
     extra = {"costVariation": cost[..., None].copy(),
              "seedValueVariation": np.asarray(case.get("seedValues", np.zeros(len(case["seeds"]))),
-                                              np.float32)[:, None],
+                                              np.float32)[None, :],
              "atol": 1e-8, "rtol": 1e-8, "exportValues": True}
     out = make_dictin(case, extra=extra).Run()
     u = out["values"].cpu().numpy()
@@ -57,7 +57,7 @@ def test_forward_linearity_and_adjoint_identity():
     cv = extra["costVariation"]
     sv = extra["seedValueVariation"]
     cv3 = np.concatenate([cv, cv[..., :1] + 2 * cv[..., 1:2]], -1)
-    sv3 = np.concatenate([sv, sv[:, :1] + 2 * sv[:, 1:2]], -1)
+    sv3 = np.concatenate([sv, sv[:1] + 2 * sv[1:2]], 0)
     shape = tuple(int(s) for s in case["dims"])
     rng = np.random.default_rng(5)
     sens = np.zeros(shape + (1,), np.float32)
@@ -72,7 +72,7 @@ def test_forward_linearity_and_adjoint_identity():
     seed_s = out["seedValueSensitivity"].cpu().numpy()[:, 0]
     for j in range(2):
         lhs = float((sens[..., 0] * vv[..., j]).sum())
-        rhs = float((lam * cost * cv[..., j]).sum() + (seed_s * sv[:, j]).sum())
+        rhs = float((lam * cost * cv[..., j]).sum() + (seed_s * sv[j]).sum())
         assert abs(lhs - rhs) <= 1e-3 * max(abs(lhs), 1e-3)
 
 
@@ -110,3 +110,23 @@ def test_autograd_forward_mode():
     (eikonal_values(h, c) * w).sum().backward()
     lhs, rhs = float((w * jt).sum()), float((c.grad * t).sum())
     assert abs(lhs - rhs) <= 1e-3 * max(abs(lhs), abs(rhs))
+
+
+@pytest.mark.parametrize("name", ["riem2_radius", "iso2_radius"])
+def test_spread_seed_variations(name):
+    """Seeds spread over a radius: a unit variation of the seed value shifts every
+    reachable value by 1 (forward), and the seed-value sensitivity of a sum of
+    receivers is their number (reverse, aggregated over the spread points)."""
+    case, _ = load_case(name)
+    shape = tuple(int(s) for s in case["dims"])
+    sens = np.zeros(shape + (1,), np.float32)
+    rng = np.random.default_rng(4)
+    sens.reshape(-1)[rng.choice(int(np.prod(shape)), 9, replace=False)] = 1.0
+    out = make_dictin(case, extra={"seedValueVariation": np.ones((1, 1), np.float32), "sensitivity": sens,
+                                   "exportValues": True}).Run()
+    vv = out["valueVariation"].cpu().numpy()[..., 0]
+    fin = np.isfinite(out["values"].cpu().numpy())
+    assert np.abs(vv[fin] - 1.0).max() < 1e-4
+    ss = out["seedValueSensitivity"].cpu().numpy()
+    assert ss.shape == (1, 1)
+    assert abs(ss[0, 0] - 9.0) < 1e-3

@@ -8,7 +8,7 @@ import numpy as np
 import pytest
 
 from oracle import oracle as O
-from conftest import load_case, CASES
+from conftest import load_case, CASES, RADIUS_CASES
 
 REL = 1e-5  # parity bar for float32 values
 
@@ -22,7 +22,7 @@ def _geodesic_split(out):
     return res
 
 
-@pytest.mark.parametrize("name", CASES)
+@pytest.mark.parametrize("name", CASES + RADIUS_CASES)
 @pytest.mark.parametrize("dtype", [np.float32, np.float64])
 def test_values(name, dtype):
     case, ref = load_case(name)
@@ -145,7 +145,7 @@ def test_forward_ad_scaling_identity():
     case = {k: v for k, v in case.items() if k not in ("tips", "sensitivity")}
     cost = np.ones(tuple(int(s) for s in case["dims"]), np.float32)
     case["costVariation"] = cost[..., None]
-    case["seedValueVariation"] = np.asarray(case["seedValues"], np.float32)[:, None]
+    case["seedValueVariation"] = np.asarray(case["seedValues"], np.float32)[None, :]
     r = O.run(dict(case, atol=1e-14, rtol=1e-14), np.float64)  # the identity holds at the fixed point
     u = r["values"]
     fin = np.isfinite(u)
