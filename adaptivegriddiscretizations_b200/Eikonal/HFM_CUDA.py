@@ -292,10 +292,10 @@ class Interface:
                                             help="Export values using the float64 data type")
         self.multiprecision = self.values_float64 or self.GetValue(
             "multiprecision", default=False, help="Use multiprecision arithmetic, to improve accuracy")
-        self.factoringRadius = self.GetValue("factoringRadius", default=0,
-                                             help="Use source factorization, to improve accuracy")
-        if self.factoringRadius:
-            raise NotImplementedError("source factorization is not available in this build")
+        self.factoringRadius = float(self.GetValue("factoringRadius", default=0,
+                                                   help="Use source factorization, to improve accuracy"))
+        if self.factoringRadius and self.multiprecision:
+            raise NotImplementedError("source factorization with multiprecision is not available in this build")
         order = self.GetValue("order", default=1, help="Use second order scheme to improve accuracy")
         if order not in {1, 2}:
             raise ValueError(f"Unsupported scheme order {order}")
@@ -458,6 +458,15 @@ class Interface:
             help="Spread the seeds over a radius given in pixels, so as to improve accuracy."))
         seeds_h = self.hfmIn.host("seeds").reshape(-1, self.ndim)
         ci = self.hfmIn.PointFromIndex(seeds_h, to=True)
+        self.factor = None
+        if self.factoringRadius:  # single seed only (_Kernel.py:301-308)
+            if len(ci) != 1:
+                raise ValueError("factoringRadius needs a single seed (as the reference)")
+            m0 = self._seed_metric(np.asarray(ci[0], np.float64))
+            nd = self.ndim
+            fm = ([m0[i, j] for i in range(nd) for j in range(i + 1)] if self.model_ == "Riemann"
+                  else list(np.diag(m0)))
+            self.factor = (self.factoringRadius ** 2, np.asarray(ci[0], np.float64), np.asarray(fm, np.float64))
         if seedRadius:
             if len(ci) != 1:
                 raise ValueError("seedRadius spreads a single seed (as the reference's SetRHS does)")
@@ -479,13 +488,52 @@ class Interface:
                                     _lib.ptr(self.seed_values), len(idx), _lib.ptr(self.rhs_t),
                                     _lib.ptr(self.seedbits), None, self.stream), "seeds")
 
+    def _cost_metrics(self, pts):
+        """The metric with the grid scales and the cost applied (index units;
+        Interface.CostMetric, _Interface.py:202-211) at the grid points pts
+        (k, ndim): (k, ndim, ndim) float64, and the cost there."""
+        nd = self.ndim
+        flat = torch.as_tensor(np.ravel_multi_index(np.asarray(pts).T, self.shape), device="cuda")
+        cost = self.cost.reshape(-1)[flat] if self.cost.dim() else self.cost.expand(len(pts))
+        cost = cost.double().cpu().numpy()
+        h = self.h.astype(np.float64)
+        if self.model_ != "Riemann":  # Diagonal(ones).with_costs(h).with_cost(cost)
+            return np.einsum("ki,ij->kij", (cost[:, None] * h) ** 2, np.eye(nd)), cost
+        sd = nd * (nd + 1) // 2
+        fm = self._metric_flat.reshape(-1, sd)
+        fm = (fm[flat] if fm.shape[0] > 1 else fm.expand(len(pts), sd)).double().cpu().numpy()
+        M = np.zeros((len(pts), nd, nd))
+        k = 0
+        for i in range(nd):
+            for j in range(i + 1):
+                M[:, i, j] = M[:, j, i] = fm[:, k]
+                k += 1
+        if self._metric_is_dual:
+            M = np.linalg.inv(M)
+        return cost[:, None, None] ** 2 * M * np.outer(h, h), cost
+
+    def _seed_metric(self, seed):
+        """The cost metric at a seed (continuous index coordinates), interpolated
+        multilinearly like the reference's set_interpolation: its entries
+        (Riemann), or the costs c*h of the diagonal metric (Isotropic)."""
+        import itertools
+        nd = self.ndim
+        shape = np.array(self.shape)
+        lo = np.clip(np.floor(seed).astype(np.int64), 0, shape - 1)
+        bits = np.array(list(itertools.product((0, 1), repeat=nd)))
+        corners = np.minimum(lo + bits, shape - 1)
+        frac = np.clip(seed - lo, 0.0, 1.0)
+        wc = np.prod(np.where(bits == 1, frac, 1.0 - frac), axis=1)
+        m, cost = self._cost_metrics(corners)
+        if self.model_ == "Riemann":
+            return np.tensordot(wc, m, axes=1)
+        return np.diag((np.dot(wc, cost) * self.h.astype(np.float64)) ** 2)
+
     def _spread_seed(self, seed, seed_value, r):
         """SetRHS's seed spreading (agd/Eikonal/HFM_CUDA/_SetArgs.py:46-75): the grid
         points closer than r (index units, inside the domain) to the seed become
         seeds with value seed_value + (|d|_{M(seed)} + |d|_{M(x)}) / 2, d = x - seed,
-        M the metric with the grid scales and the cost applied (Interface.CostMetric,
-        _Interface.py:202-211), multilinearly interpolated at the seed."""
-        import itertools
+        M the cost metric (_cost_metrics), interpolated at the seed (_seed_metric)."""
         nd = self.ndim
         seed = np.asarray(seed, np.float64)
         shape = np.array(self.shape)
@@ -493,35 +541,8 @@ class Interface:
         neigh = np.stack(np.meshgrid(*aX, indexing="ij"), axis=-1).reshape(-1, nd)
         neigh = neigh[np.linalg.norm(neigh - seed, axis=-1) < r]
         neigh = neigh[np.all((-0.5 <= neigh) & (neigh < shape - 0.5), axis=-1)]
-        lo = np.clip(np.floor(seed).astype(np.int64), 0, shape - 1)
-        bits = np.array(list(itertools.product((0, 1), repeat=nd)))
-        corners = np.minimum(lo + bits, shape - 1)
-        frac = np.clip(seed - lo, 0.0, 1.0)
-        wc = np.prod(np.where(bits == 1, frac, 1.0 - frac), axis=1)  # multilinear weights
-        pts = np.concatenate([neigh, corners])
-        flat = torch.as_tensor(np.ravel_multi_index(pts.T, self.shape), device="cuda")
-        cost = self.cost.reshape(-1)[flat] if self.cost.dim() else self.cost.expand(len(pts))
-        cost = cost.double().cpu().numpy()
-        h = self.h.astype(np.float64)
-        if self.model_ == "Riemann":
-            sd = nd * (nd + 1) // 2
-            fm = self._metric_flat.reshape(-1, sd)
-            fm = (fm[flat] if fm.shape[0] > 1 else fm.expand(len(pts), sd)).double().cpu().numpy()
-            M = np.zeros((len(pts), nd, nd))
-            k = 0
-            for i in range(nd):
-                for j in range(i + 1):
-                    M[:, i, j] = M[:, j, i] = fm[:, k]
-                    k += 1
-            if self._metric_is_dual:
-                M = np.linalg.inv(M)
-            m = cost[:, None, None] ** 2 * M * np.outer(h, h)  # Riemann.with_costs(h).with_cost(cost)
-            m1 = m[: len(neigh)]
-            m0 = np.tensordot(wc, m[len(neigh):], axes=1)
-        else:  # Diagonal(ones).with_costs(h).with_cost(cost): costs c*h, interpolated as such
-            m1 = (cost[: len(neigh), None] * h) ** 2
-            m1 = np.einsum("ki,ij->kij", m1, np.eye(nd))
-            m0 = np.diag((np.dot(wc, cost[len(neigh):]) * h) ** 2)
+        m1, _ = self._cost_metrics(neigh)
+        m0 = self._seed_metric(seed)
         d = neigh - seed
         n0 = np.sqrt(np.einsum("ki,ij,kj->k", d, m0, d))
         n1 = np.sqrt(np.einsum("ki,kij,kj->k", d, m1, d))
@@ -549,6 +570,13 @@ class Interface:
         inst.geom = self.geom.data_ptr() if self.geom is not None else None
         inst.rhs = self.rhs_t.data_ptr()
         inst.seedbits = self.seedbits.data_ptr()
+        if getattr(self, "factor", None) is not None:
+            r2, origin, fm = self.factor
+            inst.factor_radius2 = float(r2)
+            for k in range(self.ndim):
+                inst.factor_origin[k] = float(origin[k])
+            for k in range(len(fm)):
+                inst.factor_metric[k] = float(fm[k])
         return inst
 
     def Solve(self):

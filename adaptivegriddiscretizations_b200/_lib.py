@@ -36,6 +36,7 @@ class AgdInstance(ctypes.Structure):
         ("values", ctypes.c_void_p), ("valuesq", ctypes.c_void_p), ("values_next", ctypes.c_void_p),
         ("valuesq_next", ctypes.c_void_p), ("geom", ctypes.c_void_p),
         ("rhs", ctypes.c_void_p), ("seedbits", ctypes.c_void_p), ("trigger", ctypes.c_void_p),
+        ("factor_radius2", ctypes.c_float), ("factor_origin", _c_float3), ("factor_metric", ctypes.c_float * 6),
     ]
 
 
@@ -115,7 +116,7 @@ def lib():
                 fn = getattr(L, name)
                 fn.restype = res
                 fn.argtypes = args
-            if L.agd_version() != 1:
+            if L.agd_version() != 2:
                 raise RuntimeError("libagd_b200.so has an unexpected ABI version")
             _lib = L
     return _lib

@@ -193,6 +193,60 @@ __device__ __forceinline__ float hfm_update(float rhs, float *v, float *w) {
     return vmin + value;
 }
 
+// ---------------------------------------------------- source factorisation ---
+// At a point x (relative to the seed) the neighbour values at x - e and x + e
+// are shifted by f0 = |x| - |x-e| - <e, m x>/|x| and f1 = |x| - |x+e| +
+// <e, m x>/|x| (norms of the seed's metric m): the scheme is then exact for the
+// distance to the seed (cuda/EuclideanFactor.h:8-26).  The differences of norms
+// are formed as quotients, without cancellation.  xx = <x,mx>, xe = <x,me>, ee = <e,me>.
+__device__ __forceinline__ void factor_pair(float xx, float xe, float ee, float &f0, float &f1) {
+    const float nx = sqrtf(xx), nm = sqrtf(xx - 2.f * xe + ee), np = sqrtf(xx + 2.f * xe + ee);
+    const float g = xe / nx;
+    f0 = (2.f * xe - ee) / (nx + nm) - g;
+    f1 = (-2.f * xe - ee) / (nx + np) + g;
+}
+
+// <x, m y> for the factorisation metric: packed lower triangle (Riemann) or diagonal.
+template <int D, bool DIAG>
+__device__ __forceinline__ float factor_dot(const float *m, const float *x, const float *y) {
+    float r = 0.f;
+    if (DIAG) {
+#pragma unroll
+        for (int i = 0; i < D; ++i) r += m[i] * x[i] * y[i];
+        return r;
+    }
+    int k = 0;
+#pragma unroll
+    for (int i = 0; i < D; ++i)
+#pragma unroll
+        for (int j = 0; j <= i; ++j, ++k) r += (i == j ? x[i] * y[i] : x[i] * y[j] + x[j] * y[i]) * m[k];
+    return r;
+}
+
+// Shifts f[2k], f[2k+1] of the neighbours x -/+ e_k of grid point xt (0 outside the radius).
+template <int D, int NACT, bool DIAG>
+__device__ __forceinline__ void factor_shifts(const agd_instance &A, const int *xt, const int (*e)[3], float *f) {
+    float xr[3] = {0.f, 0.f, 0.f}, r2 = 0.f;
+#pragma unroll
+    for (int c = 0; c < D; ++c) {
+        xr[c] = float(xt[c]) - A.factor_origin[c];
+        r2 += xr[c] * xr[c];
+    }
+    const bool in = r2 < A.factor_radius2;
+    const float xx = factor_dot<D, DIAG>(A.factor_metric, xr, xr);
+#pragma unroll
+    for (int k = 0; k < NACT; ++k) {
+        float ek[3] = {0.f, 0.f, 0.f};
+#pragma unroll
+        for (int c = 0; c < D; ++c) ek[c] = float(e[k][c]);
+        float f0 = 0.f, f1 = 0.f;
+        if (in) factor_pair(xx, factor_dot<D, DIAG>(A.factor_metric, xr, ek), factor_dot<D, DIAG>(A.factor_metric, ek, ek),
+                            f0, f1);
+        f[2 * k] = f0;
+        f[2 * k + 1] = f1;
+    }
+}
+
 // ----------------------------------------------------------- grid barrier ---
 // Software grid barrier for cooperatively launched kernels.  Waits are bounded
 // in time (globaltimer); a timeout raises AGD_STATUS_WATCHDOG in *err and the

@@ -125,7 +125,8 @@ __global__ void mp_copy_kernel(Sched S, int dir) {
 // MP: multiprecision, u + uq * multip_step with uq an int32 (cuda/HFM.h:12-25):
 // Jacobi sweeps inside the tile and double-buffered epochs, as the reference
 // forces strict_iter_i and strict_iter_o with it (_Kernel.py:39-45).
-template <class TL, int MODEL, bool MP = false>
+// FACT: source factorisation (shifted neighbour values near the seed).
+template <class TL, int MODEL, bool MP = false, bool FACT = false>
 struct Visit {
     static constexpr int D = TL::D, P = TL::P;
     static constexpr int NACT = MODEL == AGD_MODEL_ISOTROPIC ? D : D * (D + 1) / 2;
@@ -270,6 +271,7 @@ struct Visit {
         float nbv[kSlots ? 1 : P][kSlots ? 1 : NTOT];
         int nbq[MP ? P : 1][MP ? NTOT : 1];
         unsigned nba[kSlots ? P : 1][kSlots ? NTOT : 1];
+        float fsh[FACT ? P : 1][FACT ? NTOT : 1];  // factorisation shifts of the neighbour values
         const unsigned us_addr = (unsigned)__cvta_generic_to_shared(us);
         bool seed[P];
         float raw[P][kRaw];
@@ -306,6 +308,7 @@ struct Visit {
             int ev[NACT][3];
             if (seed[p]) continue;  // seeds (and padding) keep their value: no stencil needed
             stencil_decode(I, raw[p], wts[p], ev);
+            if constexpr (FACT) factor_shifts<D, NACT, MODEL == AGD_MODEL_ISOTROPIC>(A, xt, ev, fsh[p]);
 #pragma unroll
             for (int k = 0; k < NACT; ++k) {
 #pragma unroll
@@ -406,6 +409,10 @@ struct Visit {
                             } else {
                                 a = neighbour(nbv[p][2 * k], us);
                                 b = neighbour(nbv[p][2 * k + 1], us);
+                            }
+                            if constexpr (FACT) {
+                                a += fsh[p][2 * k];
+                                b += fsh[p][2 * k + 1];
                             }
                             v[k] = a > b ? b : a;
                             w[k] = wts[p][k];
@@ -513,6 +520,21 @@ __device__ __forceinline__ void dispatch(const Sched &S, int t, int e, int lane,
         case V_RIEM3_4_MP:
             if constexpr ((VMASK >> V_RIEM3_4_MP) & 1) Visit<Tile<3, 4, 4, 4>, AGD_MODEL_RIEMANN, true>::run(S, I, ii, n_o, e, lane, us);
             break;
+        case V_ISO2_8_F:
+            if constexpr ((VMASK >> V_ISO2_8_F) & 1) Visit<Tile<2, 8, 8, 1>, AGD_MODEL_ISOTROPIC, false, true>::run(S, I, ii, n_o, e, lane, us);
+            break;
+        case V_ISO2_16_F:
+            if constexpr ((VMASK >> V_ISO2_16_F) & 1) Visit<Tile<2, 16, 16, 1>, AGD_MODEL_ISOTROPIC, false, true>::run(S, I, ii, n_o, e, lane, us);
+            break;
+        case V_RIEM2_8_F:
+            if constexpr ((VMASK >> V_RIEM2_8_F) & 1) Visit<Tile<2, 8, 8, 1>, AGD_MODEL_RIEMANN, false, true>::run(S, I, ii, n_o, e, lane, us);
+            break;
+        case V_ISO3_4_F:
+            if constexpr ((VMASK >> V_ISO3_4_F) & 1) Visit<Tile<3, 4, 4, 4>, AGD_MODEL_ISOTROPIC, false, true>::run(S, I, ii, n_o, e, lane, us);
+            break;
+        case V_RIEM3_4_F:
+            if constexpr ((VMASK >> V_RIEM3_4_F) & 1) Visit<Tile<3, 4, 4, 4>, AGD_MODEL_RIEMANN, false, true>::run(S, I, ii, n_o, e, lane, us);
+            break;
         default:
             break;
     }
@@ -531,6 +553,11 @@ constexpr int smem_floats() {
     if ((VMASK >> V_RIEM3_4) & 1) m = std::max(m, Visit<Tile<3, 4, 4, 4>, AGD_MODEL_RIEMANN>::kSmemFloats);
     if ((VMASK >> V_RIEM2_16) & 1) m = std::max(m, Visit<Tile<2, 16, 16, 1>, AGD_MODEL_RIEMANN>::kSmemFloats);
     if (VMASK & kMpVariants) m = std::max(m, 2 * kMaxTileSize);
+    if ((VMASK >> V_ISO2_8_F) & 1) m = std::max(m, Visit<Tile<2, 8, 8, 1>, AGD_MODEL_ISOTROPIC, false, true>::kSmemFloats);
+    if ((VMASK >> V_ISO2_16_F) & 1) m = std::max(m, Visit<Tile<2, 16, 16, 1>, AGD_MODEL_ISOTROPIC, false, true>::kSmemFloats);
+    if ((VMASK >> V_RIEM2_8_F) & 1) m = std::max(m, Visit<Tile<2, 8, 8, 1>, AGD_MODEL_RIEMANN, false, true>::kSmemFloats);
+    if ((VMASK >> V_ISO3_4_F) & 1) m = std::max(m, Visit<Tile<3, 4, 4, 4>, AGD_MODEL_ISOTROPIC, false, true>::kSmemFloats);
+    if ((VMASK >> V_RIEM3_4_F) & 1) m = std::max(m, Visit<Tile<3, 4, 4, 4>, AGD_MODEL_RIEMANN, false, true>::kSmemFloats);
     return m;
 }
 
@@ -540,10 +567,10 @@ struct EikonalVisitor {
     // keep 8 points per lane in registers, Riemann3 twelve neighbours per point,
     // multiprecision an integer part beside every value.
     static constexpr int kMinCtas =
-        (VMASK & ((1u << V_RIEM2_16) | (1u << V_ISO2_16) | (1u << V_ISO2_16_MP))) ? 4
-        : (VMASK & ((1u << V_RIEM3_4) | (1u << V_RIEM3_4_MP)))                    ? 6
-        : (VMASK & kMpVariants)                                                   ? 7
-                                                                                  : 9;
+        (VMASK & ((1u << V_RIEM2_16) | (1u << V_ISO2_16) | (1u << V_ISO2_16_MP) | (1u << V_ISO2_16_F))) ? 4
+        : (VMASK & ((1u << V_RIEM3_4) | (1u << V_RIEM3_4_MP) | (1u << V_RIEM3_4_F)))                    ? 6
+        : (VMASK & (kMpVariants | kFactorVariants))                                                     ? 7
+                                                                                                        : 9;
     struct Args {};
     struct Smem {
         float u[smem_floats<VMASK>()];  // values, then out-of-tile neighbours or integer parts
@@ -592,6 +619,10 @@ static int validate(const agd_instance *host, const Inst *insts, int n, unsigned
         const char *bad = nullptr;
         int code = AGD_STATUS_INVALID;
         if (a.ndim != host[0].ndim) bad = "all instances of a plan must share ndim";
+        else if (a.factor_radius2 > 0.f && a.multip_step != 0.f) {
+            bad = "source factorisation with multiprecision is not built";
+            code = AGD_STATUS_UNSUPPORTED;
+        }
         else if (insts[i].variant < 0) { bad = "model/tile shape not built"; code = AGD_STATUS_UNSUPPORTED; }
         else if (a.multip_step != 0.f && (!a.valuesq || !a.values_next || !a.valuesq_next || !(a.multip_step > 0.f)))
             bad = "multiprecision needs valuesq, values_next, valuesq_next and multip_step > 0";
@@ -632,6 +663,13 @@ static int run_variants(int ndim, unsigned vmask, const WsLayout &L, void *ws, i
     constexpr unsigned R3 = 1u << V_RIEM3_4, I3 = 1u << V_ISO3_4, R2L = 1u << V_RIEM2_16;
     constexpr unsigned MP2 = (1u << V_ISO2_8_MP) | (1u << V_ISO2_16_MP) | (1u << V_RIEM2_8_MP);
     constexpr unsigned MP3 = (1u << V_ISO3_4_MP) | (1u << V_RIEM3_4_MP);
+    if (vmask & kFactorVariants) {  // factored instances, possibly beside plain ones
+        constexpr unsigned F2 = (1u << V_ISO2_8_F) | (1u << V_ISO2_16_F) | (1u << V_RIEM2_8_F);
+        constexpr unsigned F3 = (1u << V_ISO3_4_F) | (1u << V_RIEM3_4_F);
+        if (vmask & kMpVariants) return set_error(AGD_STATUS_UNSUPPORTED, "factorisation and multiprecision in one plan");
+        if (ndim == 2) return run_sched<EikonalVisitor<F2 | R2 | I16 | I8 | R2L>>(L, ws, n, {}, stats, cfg, st);
+        return run_sched<EikonalVisitor<F3 | R3 | I3>>(L, ws, n, {}, stats, cfg, st);
+    }
     if (vmask & kMpVariants) {
         if (ndim == 2) {
             if (vmask == (1u << V_RIEM2_8_MP)) return run_sched<EikonalVisitor<(1u << V_RIEM2_8_MP)>>(L, ws, n, {}, stats, cfg, st);
@@ -752,7 +790,13 @@ __global__ void flow_kernel(Inst I, float *fvec, float *fwsum, float *fw, int *f
         float w[NACT], fwk[NACT];
         int ev[NACT][3], side[NACT];
         V::stencil(I, n_t, w, ev);
-        float v[NACT];
+        float v[NACT], fsh[2 * NACT];
+        if (A.factor_radius2 > 0.f) {
+            factor_shifts<D, NACT, MODEL == AGD_MODEL_ISOTROPIC>(A, xt, ev, fsh);
+        } else {
+#pragma unroll
+            for (int k = 0; k < 2 * NACT; ++k) fsh[k] = 0.f;
+        }
 #pragma unroll
         for (int k = 0; k < NACT; ++k) {
             side[k] = 0;
@@ -766,7 +810,7 @@ __global__ void flow_kernel(Inst I, float *fvec, float *fwsum, float *fw, int *f
                     y[c] = xt[c] + (2 * s - 1) * ev[k][c];
                     ok = ok && y[c] >= 0 && y[c] < A.shape[c];
                 }
-                const float val = ok ? __ldg(A.values + bilevel_index<D, TL>(y, I.shape_o)) : finf();
+                const float val = (ok ? __ldg(A.values + bilevel_index<D, TL>(y, I.shape_o)) : finf()) + fsh[2 * k + s];
                 if (s == 0) v[k] = val;
                 else if (v[k] > val) { v[k] = val; side[k] = 1; }
             }

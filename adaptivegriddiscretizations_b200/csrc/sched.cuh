@@ -17,15 +17,30 @@ namespace agd {
 enum Variant {
     V_ISO2_8 = 0, V_ISO2_16, V_RIEM2_8, V_ISO3_4, V_RIEM3_4, V_RIEM2_16,
     // multiprecision
-    V_ISO2_8_MP, V_ISO2_16_MP, V_RIEM2_8_MP, V_ISO3_4_MP, V_RIEM3_4_MP, V_COUNT
+    V_ISO2_8_MP, V_ISO2_16_MP, V_RIEM2_8_MP, V_ISO3_4_MP, V_RIEM3_4_MP,
+    // source factorisation
+    V_ISO2_8_F, V_ISO2_16_F, V_RIEM2_8_F, V_ISO3_4_F, V_RIEM3_4_F, V_COUNT
 };
 constexpr unsigned kMpVariants = (1u << V_ISO2_8_MP) | (1u << V_ISO2_16_MP) | (1u << V_RIEM2_8_MP) |
                                  (1u << V_ISO3_4_MP) | (1u << V_RIEM3_4_MP);
+constexpr unsigned kFactorVariants = (1u << V_ISO2_8_F) | (1u << V_ISO2_16_F) | (1u << V_RIEM2_8_F) |
+                                     (1u << V_ISO3_4_F) | (1u << V_RIEM3_4_F);
 
 static int base_variant_of(const agd_instance &a);
 
 static int variant_of(const agd_instance &a) {
     const int v = base_variant_of(a);
+    if (v >= 0 && a.factor_radius2 > 0.f) {
+        if (a.multip_step != 0.f) return -1;  // no build of factorisation with multiprecision
+        switch (v) {
+            case V_ISO2_8: return V_ISO2_8_F;
+            case V_ISO2_16: return V_ISO2_16_F;
+            case V_RIEM2_8: return V_RIEM2_8_F;
+            case V_ISO3_4: return V_ISO3_4_F;
+            case V_RIEM3_4: return V_RIEM3_4_F;
+            default: return -1;
+        }
+    }
     if (v < 0 || a.multip_step == 0.f) return v;
     switch (v) {
         case V_ISO2_8: return V_ISO2_8_MP;

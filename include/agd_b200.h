@@ -67,6 +67,16 @@ typedef struct agd_instance {
     const uint8_t *seedbits; /* tile layout bits, little endian, padding bits set */
     const uint8_t *trigger;  /* per tile, nonzero = active at the first iteration
                                 (NULL: tiles holding a seed) */
+    /* Source factorisation (factoringRadius; _Kernel.py:47-49, 301-308,
+     * cuda/FiniteDifferences.h:30-75): at the points closer than
+     * sqrt(factor_radius2) (index units) to factor_origin, the neighbour values
+     * are shifted so that the scheme is exact for the distance |x - origin|_m.
+     * factor_radius2 = 0: off.  Not with multiprecision. */
+    float factor_radius2;
+    float factor_origin[3];  /* the seed, continuous index coordinates */
+    float factor_metric[6];  /* metric at the seed with cost and grid scales applied (index
+                                units): packed lower triangle (Riemann), squared costs per
+                                axis (Isotropic) */
 } agd_instance;
 
 #define AGD_FLAG_ACTIVATE_ALL 1 /* every tile is active at the first iteration */
@@ -266,7 +276,7 @@ int agd_forward(const agd_instance *inst, const float *flow_weights, const int32
 /* ------------------------------------------------------------------- misc -- */
 
 const char *agd_last_error(void);
-int agd_version(void);
+int agd_version(void); /* 2: agd_instance with the source factorisation fields */
 
 #if defined(__GNUC__)
 #pragma GCC visibility pop

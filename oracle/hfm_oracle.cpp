@@ -17,6 +17,8 @@
 //   geodesic ODE                 cuda/Kernel_GeodesicODE.h:164-412; _GetGeodesics.py:9-147
 //   distance-to-seed map         cuda/Kernel_InfConvolution.h:66-92; _GetGeodesics.py:51-75
 //   reverse AD linear system     _PostProcess.py:155-219 (solved here by ordered sweeps)
+//   forward AD linear system     _PostProcess.py:181-191 (ordered sweeps)
+//   source factorisation         cuda/EuclideanFactor.h:8-26, FiniteDifferences.h:30-75
 //
 // Arrays passed to this library are in plain row-major grid layout (not the
 // bilevel tile layout of the GPU kernels).  The tile structure is used only to
@@ -136,6 +138,44 @@ struct Problem {
     const float *geom = nullptr;  // dual metric planes, grid layout
     const float *rhs = nullptr;
     const unsigned char *seed = nullptr;
+    // Source factorisation: within fact_r2 (squared, index units) of fact_origin,
+    // neighbour values are shifted so that the scheme is exact for |x|_m, m the
+    // metric at the seed (packed lower-triangular; isotropic: D diagonal entries).
+    T fact_r2 = 0, fact_origin[3] = {0, 0, 0}, fact_m[6] = {0, 0, 0, 0, 0, 0};
+
+    T scal_fact(const T *x, const T *y) const {
+        if (model == 0) {
+            T r = 0;
+            for (int i = 0; i < D; ++i) r += fact_m[i] * x[i] * y[i];
+            return r;
+        }
+        T r = 0;
+        int k = 0;
+        for (int i = 0; i < D; ++i)
+            for (int j = 0; j <= i; ++j, ++k) r += (i == j ? x[i] * y[i] : x[i] * y[j] + x[j] * y[i]) * fact_m[k];
+        return r;
+    }
+    // Shifts of the neighbour values at x - e_k (f[2k]) and x + e_k (f[2k+1]).
+    void shifts(const int *x, int (*e)[3], T *f) const {
+        for (int k = 0; k < 2 * nact; ++k) f[k] = 0;
+        if (!(fact_r2 > 0)) return;
+        T xr[3] = {0, 0, 0}, r2 = 0;
+        for (int c = 0; c < D; ++c) {
+            xr[c] = T(x[c]) - fact_origin[c];
+            r2 += xr[c] * xr[c];
+        }
+        if (!(r2 < fact_r2)) return;
+        const T xx = scal_fact(xr, xr);
+        for (int k = 0; k < nact; ++k) {
+            T ek[3] = {0, 0, 0};
+            for (int c = 0; c < D; ++c) ek[c] = T(e[k][c]);
+            const T xe = scal_fact(xr, ek), ee = scal_fact(ek, ek);
+            const T nx = std::sqrt(xx), nm = std::sqrt(xx - 2 * xe + ee), np = std::sqrt(xx + 2 * xe + ee);
+            const T g = xe / nx;                       // <e, m x> / |x|_m
+            f[2 * k] = -g + (2 * xe - ee) / (nx + nm);     // |x| - |x-e| - <e,mx>/|x|
+            f[2 * k + 1] = g + (-2 * xe - ee) / (nx + np); // |x| - |x+e| + <e,mx>/|x|
+        }
+    }
 
     void init(int D_, int model_, const int *shape_, const int *shape_i_) {
         D = D_;
@@ -253,7 +293,7 @@ struct Solver {
         std::vector<long> pts(S);
         std::vector<int> xi(3 * S), xt(3 * S);
         tile_points(n_o, pts.data(), xi.data(), xt.data());
-        std::vector<T> ul(S), uold(S), rhs(S), w(S * 6), vo(S * 12);
+        std::vector<T> ul(S), uold(S), rhs(S), w(S * 6), vo(S * 12), sh(S * 12, T(0));
         std::vector<int> vi(S * 12);
         std::vector<char> seed(S);
         for (int n = 0; n < S; ++n) {
@@ -269,6 +309,7 @@ struct Solver {
             ul[n] = seed[n] ? rhs[n] : uold[n];
             int e[6][3];
             P.stencil(p, &w[n * 6], e);
+            if (!seed[n]) P.shifts(xt.data() + n * 3, e, &sh[n * 12]);
             for (int k = 0; k < NA; ++k)
                 for (int s = 0; s < 2; ++s) {
                     const int ks = 2 * k + s, eps = 2 * s - 1;
@@ -298,7 +339,7 @@ struct Solver {
                     T best = 0;
                     for (int s = 0; s < 2; ++s) {
                         const int ks = 2 * k + s;
-                        const T val = vi[n * 12 + ks] >= 0 ? ul[vi[n * 12 + ks]] : vo[n * 12 + ks];
+                        const T val = (vi[n * 12 + ks] >= 0 ? ul[vi[n * 12 + ks]] : vo[n * 12 + ks]) + sh[n * 12 + ks];
                         if (s == 0 || best > val) best = val;
                     }
                     v[k] = best;
@@ -399,12 +440,13 @@ struct Solver {
             const bool sd = P.seed[p] != 0;
             if (!sd) {
                 P.stencil(p, wts, e);
-                T v[6];
+                T v[6], sh[12];
+                P.shifts(x, e, sh);
                 for (int k = 0; k < NA; ++k) {
                     for (int s = 0; s < 2; ++s) {
                         int y[3];
                         for (int c = 0; c < D; ++c) y[c] = x[c] + (2 * s - 1) * e[k][c];
-                        const T val = P.inside(y) ? u[P.flat(y)] : inf<T>();
+                        const T val = (P.inside(y) ? u[P.flat(y)] : inf<T>()) + sh[2 * k + s];
                         if (s == 0) { v[k] = val; side[k] = 0; }
                         else if (v[k] > val) { v[k] = val; side[k] = 1; }
                     }
@@ -605,6 +647,9 @@ void fill_problem(Problem<T> &P, int ndim, int model, const int *shape, const in
     P.seed = seed;
 }
 
+// Source factorisation of the next solves (agdo_set_factor).
+double g_fact_r2 = 0, g_fact_origin[3] = {0, 0, 0}, g_fact_m[6] = {0, 0, 0, 0, 0, 0};
+
 template <class T>
 int eikonal_impl(int ndim, int model, const int *shape, const int *shape_i, int niter_i, int front,
                  const double *iso_w, const float *geom, const float *rhs, const unsigned char *seed,
@@ -612,6 +657,9 @@ int eikonal_impl(int ndim, int model, const int *shape, const int *shape_i, int 
                  long long *visits, double *fvec, double *fwsum, double *fw, int *fidx) {
     Solver<T> S;
     fill_problem(S.P, ndim, model, shape, shape_i, iso_w, geom, rhs, seed);
+    S.P.fact_r2 = T(g_fact_r2);
+    for (int c = 0; c < 3; ++c) S.P.fact_origin[c] = T(g_fact_origin[c]);
+    for (int c = 0; c < 6; ++c) S.P.fact_m[c] = T(g_fact_m[c]);
     S.u.assign(values, values + S.P.size);
     S.atol = T(atol);
     S.rtol = T(rtol);
@@ -674,6 +722,13 @@ int agdo_eikonal(int dbl, int ndim, int model, const int *shape, const int *shap
                                atol, rtol, nitermax, nthreads, visits, fvec, fwsum, fw, fidx);
 }
 
+// Source factorisation for the following agdo_eikonal calls (r2 = 0: off).
+void agdo_set_factor(double r2, const double *origin, const double *metric) {
+    g_fact_r2 = r2;
+    for (int c = 0; c < 3; ++c) g_fact_origin[c] = origin ? origin[c] : 0.0;
+    for (int c = 0; c < 6; ++c) g_fact_m[c] = metric ? metric[c] : 0.0;
+}
+
 void agdo_eucl_map(int ndim, const int *shape, const unsigned char *seedmask, unsigned char *out) {
     eucl_map(ndim, shape, seedmask, out);
 }
@@ -699,11 +754,6 @@ void agdo_geodesic_chunk(int ndim, const int *shape, int ntips, int max_len, int
     }
 }
 
-// Reverse-mode sensitivity: solves diag(x) lam(x) - sum_{z->x} w lam(z) = s(x)
-// (transpose of the linearised scheme, _PostProcess.py:155-219) where the entries
-// z->x are the upwind weights fw[k][z] with fidx[k][z] == x.  diag = weightsum,
-// or 1 where weightsum == 0.  Points are swept by decreasing value, repeated
-// until nothing moves, in double precision.
 // Forward linearisation (agd/Eikonal/HFM_CUDA/_PostProcess.py:181-191):
 // fwsum(x) du(x) - sum_k fw_k(x) du(y_k(x)) = rhs(x), diag 1 where fwsum = 0.
 // The upwind neighbours y_k(x) have smaller values than x, so Gauss-Seidel
@@ -741,6 +791,11 @@ int agdo_forward(int nact, long N, const double *values, const double *fw, const
     return sweeps;
 }
 
+// Reverse-mode sensitivity: solves diag(x) lam(x) - sum_{z->x} w lam(z) = s(x)
+// (transpose of the linearised scheme, _PostProcess.py:155-219) where the entries
+// z->x are the upwind weights fw[k][z] with fidx[k][z] == x.  diag = weightsum,
+// or 1 where weightsum == 0.  Points are swept by decreasing value, repeated
+// until nothing moves, in double precision.
 int agdo_reverse(int nact, long N, const double *values, const double *fw, const int *fidx,
                  const double *fwsum, const double *sens, double *lam) {
     std::vector<long> cnt(N + 1, 0);

@@ -111,9 +111,19 @@ def prepare(case):
     seeds = np.asarray(case["seeds"], np.float32).reshape(-1, pr.ndim)
     sv = np.asarray(case.get("seedValues", np.zeros(len(seeds))), np.float32)
     start = pr.origin + 0.5 * pr.h
-    if float(case.get("seedRadius", 0.0)):
-        pr.seed_idx, sv = _spread_seed(pr, case, cost, ((seeds - start) / pr.h)[0], float(sv[0]),
-                                       float(case["seedRadius"]))
+    fr = float(case.get("factoringRadius", 0.0))
+    pr.factor = None
+    if fr:  # source factorisation around the (single) seed (_Kernel.py:47-49, 301-308)
+        seed = ((seeds - start) / pr.h)[0].astype(np.float64)
+        m0 = _seed_metric(pr, case, cost, seed)
+        if pr.riemann:
+            fm = np.array([m0[i, j] for i in range(pr.ndim) for j in range(i + 1)])
+        else:
+            fm = np.diag(m0).copy()
+        pr.factor = (fr * fr, seed, fm)
+    radius = float(case.get("seedRadius", 2.0 if fr else 0.0))
+    if radius:
+        pr.seed_idx, sv = _spread_seed(pr, case, cost, ((seeds - start) / pr.h)[0], float(sv[0]), radius)
     else:
         pr.seed_idx = np.round((seeds - start) / pr.h).astype(int)
     rhs = cost.copy()
@@ -128,6 +138,46 @@ def prepare(case):
     return pr
 
 
+def _cost_metric(pr, case, cost):
+    """Grid point -> the metric with the grid scales and the cost applied, index
+    units (Interface.CostMetric, _Interface.py:202-211)."""
+    nd = pr.ndim
+    h = pr.h.astype(np.float64)
+    c = np.asarray(cost, np.float64)
+    if pr.riemann:
+        mf = np.broadcast_to(np.asarray(case["metric"], np.float64), tuple(pr.shape) + (nd * (nd + 1) // 2,))
+        tri = [(i, j) for i in range(nd) for j in range(i + 1)]
+
+        def cm(p):
+            M = np.zeros((nd, nd))
+            for q, (i, j) in enumerate(tri):
+                M[i, j] = M[j, i] = mf[tuple(p)][q]
+            return c[tuple(p)] ** 2 * M * np.outer(h, h)
+    else:
+        def cm(p):
+            return np.diag((c[tuple(p)] * h) ** 2)
+    return cm
+
+
+def _seed_metric(pr, case, cost, seed):
+    """The cost metric at a seed (continuous index coordinates), multilinearly
+    interpolated: its entries (Riemann), or the costs c*h (Isotropic)."""
+    nd = pr.ndim
+    shape = np.array(pr.shape)
+    cm = _cost_metric(pr, case, cost)
+    c = np.asarray(cost, np.float64)
+    lo = np.clip(np.floor(seed).astype(int), 0, shape - 1)
+    frac = np.clip(seed - lo, 0.0, 1.0)
+    m0 = np.zeros((nd, nd))
+    c0 = 0.0
+    for bits in np.ndindex(*([2] * nd)):
+        w = np.prod([f if b else 1.0 - f for b, f in zip(bits, frac)])
+        p = np.minimum(lo + np.array(bits), shape - 1)
+        m0 += w * cm(p)
+        c0 += w * c[tuple(p)]
+    return m0 if pr.riemann else np.diag((c0 * pr.h.astype(np.float64)) ** 2)
+
+
 def _spread_seed(pr, case, cost, seed, seed_value, r):
     """Seed spreading (agd/Eikonal/HFM_CUDA/_SetArgs.py:46-75), float64: the grid
     points within r of the seed (index units) take the value seed_value +
@@ -140,32 +190,8 @@ def _spread_seed(pr, case, cost, seed, seed_value, r):
     pts = np.stack(np.meshgrid(*axes, indexing="ij"), -1).reshape(-1, nd)
     pts = pts[np.linalg.norm(pts - seed, axis=1) < r]
     pts = pts[np.all((pts >= -0.5) & (pts < shape - 0.5), axis=1)]
-    h = pr.h.astype(np.float64)
-    c = np.asarray(cost, np.float64)
-    if pr.riemann:
-        mf = np.broadcast_to(np.asarray(case["metric"], np.float64), tuple(pr.shape) + (nd * (nd + 1) // 2,))
-        tri = [(i, j) for i in range(nd) for j in range(i + 1)]
-
-        def cm(p):  # cost-scaled metric at grid point p
-            M = np.zeros((nd, nd))
-            for q, (i, j) in enumerate(tri):
-                M[i, j] = M[j, i] = mf[tuple(p)][q]
-            return c[tuple(p)] ** 2 * M * np.outer(h, h)
-    else:
-        def cm(p):
-            return np.diag((c[tuple(p)] * h) ** 2)
-    # multilinear interpolation at the seed: of the metric entries (Riemann), of the costs c*h (Isotropic)
-    lo = np.clip(np.floor(seed).astype(int), 0, shape - 1)
-    frac = np.clip(seed - lo, 0.0, 1.0)
-    m0 = np.zeros((nd, nd))
-    c0 = 0.0
-    for bits in np.ndindex(*([2] * nd)):
-        w = np.prod([f if b else 1.0 - f for b, f in zip(bits, frac)])
-        p = np.minimum(lo + np.array(bits), shape - 1)
-        m0 += w * cm(p)
-        c0 += w * c[tuple(p)]
-    if not pr.riemann:
-        m0 = np.diag((c0 * h) ** 2)
+    cm = _cost_metric(pr, case, cost)
+    m0 = _seed_metric(pr, case, cost, seed)
     vals = []
     for p in pts:
         d = p - seed
@@ -188,6 +214,15 @@ def eikonal(pr, dtype=np.float32, values=None, nthreads=1, flow=False, nitermax=
         fi = np.zeros((nact,) + pr.shape, np.int32)
     geom = None if pr.geom is None else np.ascontiguousarray(pr.geom, np.float32)
     iso = None if pr.iso_w is None else np.ascontiguousarray(pr.iso_w, np.float64)
+    fac = getattr(pr, "factor", None)
+    if fac is None:
+        L.agdo_set_factor(ctypes.c_double(0.0), None, None)
+    else:
+        org = np.zeros(3)
+        org[: pr.ndim] = fac[1]
+        met = np.zeros(6)
+        met[: len(fac[2])] = fac[2]
+        L.agdo_set_factor(ctypes.c_double(fac[0]), _p(org), _p(met))
     niter = L.agdo_eikonal(int(dtype == np.float64), pr.ndim, 1 if pr.riemann else 0,
                            (ctypes.c_int * pr.ndim)(*pr.shape), (ctypes.c_int * pr.ndim)(*pr.shape_i),
                            pr.niter_i, pr.front, _p(iso), _p(geom), _p(np.ascontiguousarray(pr.rhs)),

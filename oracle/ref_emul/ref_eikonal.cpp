@@ -5,7 +5,8 @@
 //
 // Compile-time configuration (set by oracle/ref_emul/Makefile):
 //   AGDREF_ISO (0|1), AGDREF_NDIM, AGDREF_SHAPE_I (comma list), AGDREF_SIZE_I,
-//   AGDREF_LOG2_SIZE_I, AGDREF_NITER_I, AGDREF_MULTIP (0|1), AGDREF_FLOW (0|1).
+//   AGDREF_LOG2_SIZE_I, AGDREF_NITER_I, AGDREF_MULTIP (0|1), AGDREF_FLOW (0|1),
+//   AGDREF_FACTOR (0|1, source factorisation, factor_macro of _Kernel.py:47-49).
 //
 // The block below states the same compile-time traits that the reference's
 // `cupy_module_helper.traits_header` emits for these models
@@ -14,6 +15,12 @@
 #include <cstring>
 #include <vector>
 
+#ifndef AGDREF_FACTOR
+#define AGDREF_FACTOR 0
+#endif
+#if AGDREF_FACTOR
+#define factor_macro true
+#endif
 #define pruning_macro false
 #define geom_first_macro true
 typedef float Scalar;
@@ -138,6 +145,15 @@ void set_common(const int *shape, float atol_, float rtol_, const float *iso_w, 
 }  // namespace
 
 extern "C" {
+
+#if AGDREF_FACTOR
+// The module constants of source factorisation (_Kernel.py:301-308).
+void agdref_set_factor(const float *origin, float radius2, const float *metric) {
+    for (int k = 0; k < ndim; ++k) factor_origin[k] = origin[k];
+    factor_radius2 = radius2;
+    for (int k = 0; k < factor_size; ++k) factor_metric[k] = metric[k];
+}
+#endif
 
 #if !AGDREF_FLOW
 // Restatement of _solvers.fast_iterative_method (agd/Eikonal/HFM_CUDA/_solvers.py:94-120),

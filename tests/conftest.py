@@ -24,14 +24,16 @@ def load_case(name):
                               niter_i=int(case.pop("traits_niter_i")))
     if "multiprecision" in case:
         case["multiprecision"] = bool(case["multiprecision"])
-    if "seedRadius" in case:
-        case["seedRadius"] = float(case["seedRadius"])
+    for k in ("seedRadius", "factoringRadius"):
+        if k in case:
+            case[k] = float(case[k])
     out = {k[4:]: d[k] for k in d.files if k.startswith("out_")}
     return case, out
 
 
 CASES = ["iso2", "riem2", "riem2_aniso", "iso3", "riem3", "ad_notebook"]
 RADIUS_CASES = ["riem2_radius", "iso2_radius"]  # seeds spread over a radius (values only)
+FACTOR_CASES = ["riem2_factor", "iso2_factor"]  # source factorisation (factoringRadius)
 
 
 @pytest.fixture(params=CASES)
@@ -44,7 +46,7 @@ def make_dictin(case, mode="gpu", extra=None):
     from adaptivegriddiscretizations_b200 import Eikonal
     d = {"model": case["model"], "mode": mode, "arrayOrdering": "RowMajor", "verbosity": 0}
     for k in ("dims", "gridScales", "origin", "seeds", "seedValues", "cost", "tips", "traits", "sensitivity",
-              "seedRadius"):
+              "seedRadius", "factoringRadius"):
         if k in case:
             d[k] = case[k]
     if "metric" in case:

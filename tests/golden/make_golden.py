@@ -127,8 +127,17 @@ class RefPipeline:
         self.rtol = np.float32(0.0 if self.multip else float_res * 5.0)
         seeds = np.asarray(c["seeds"], np.float32)
         seedValues = np.asarray(c.get("seedValues", np.zeros(len(seeds))), np.float32)
-        if c.get("seedRadius", 0.0):
-            seedIdx, seedValues = self.spread_seed(seeds, seedValues, float(c["seedRadius"]), cost)
+        self.factor = None
+        fr = float(c.get("factoringRadius", 0.0))
+        if fr:  # _Kernel.py:47-49, 301-308; seedRadius defaults to 2 (_SetArgs.py:40-43)
+            seed = self.point_from_index(seeds, to=True)[0].astype(np.float64)
+            hfm = np.asarray(self.cost_metric(cost).at(seed).to_HFM(), np.float32)
+            if not self.model.startswith("Riemann"):
+                hfm = hfm ** 2
+            self.factor = (seed.astype(np.float32), np.float32(fr * fr), hfm.astype(np.float32))
+        radius = float(c.get("seedRadius", 2.0 if fr else 0.0))
+        if radius:
+            seedIdx, seedValues = self.spread_seed(seeds, seedValues, radius, cost)
         else:
             seedIdx = np.round(self.point_from_index(seeds, to=True)).astype(int)
         self.seedIndices = seedIdx
@@ -152,20 +161,27 @@ class RefPipeline:
             self.multip_step = self.multip_max = np.float32(0)
         self.iso_w = (self.h.astype(np.float32) ** -2).astype(np.float32)
 
-    def spread_seed(self, seeds, seedValues, r, cost):
-        """SetRHS's seed spreading (_SetArgs.py:46-75) with the reference's own
-        metric interpolation (Interface.CostMetric, _Interface.py:202-211)."""
+    def cost_metric(self, cost):
+        """Interface.CostMetric (_Interface.py:202-211): the metric with the grid
+        scales and the cost applied, interpolated over the grid (index units)."""
         from agd import AutomaticDifferentiation as ad
-        assert len(seeds) == 1
-        seed = self.point_from_index(seeds, to=True)[0].astype(np.float64)
         nd = self.ndim
         if self.model.startswith("Riemann"):
             metric = self.Metrics.Riemann.from_HFM(np.asarray(self.c["metric"], np.float64))
         else:
             metric = self.Metrics.Diagonal(np.ones(nd))
-        cm = metric.with_costs(self.h.astype(np.float64)).with_cost(cost.astype(np.float64))
+        cm = metric.with_costs(self.h.astype(np.float64)).with_cost(np.asarray(cost, np.float64))
         grid = ad.array(np.meshgrid(*(np.arange(s, dtype=np.float64) for s in self.shape), indexing="ij"))
         cm.set_interpolation(grid)
+        return cm
+
+    def spread_seed(self, seeds, seedValues, r, cost):
+        """SetRHS's seed spreading (_SetArgs.py:46-75) with the reference's own
+        metric interpolation."""
+        assert len(seeds) == 1
+        seed = self.point_from_index(seeds, to=True)[0].astype(np.float64)
+        nd = self.ndim
+        cm = self.cost_metric(cost)
         aX = [np.arange(int(np.floor(ci - r)), int(np.ceil(ci + r) + 1)) for ci in seed]
         neigh = np.stack(np.meshgrid(*aX, indexing="ij"), axis=-1).reshape(-1, nd)
         close = np.linalg.norm(neigh - seed, axis=-1) < r
@@ -179,8 +195,9 @@ class RefPipeline:
 
     def solve(self):
         md = self.md
-        name = f"libagdref_eik_{md['tag']}{'mp' if self.multip else ''}.so"
+        name = f"libagdref_eik_{md['tag']}{'mp' if self.multip else ''}{'f' if self.factor else ''}.so"
         L = lib(name)
+        self.set_factor(L)
         trig_o = self.bexp(self.trigger, False).reshape(self.shape_o + (-1,)).any(-1).astype(np.uint8)
         nup = ctypes.c_longlong(0)
         L.agdref_fim_solve.restype = ctypes.c_int
@@ -192,6 +209,11 @@ class RefPipeline:
             ctypes.byref(nup))
         self.tile_visits = nup.value
 
+    def set_factor(self, L):
+        if self.factor:
+            o, r2, m = self.factor
+            L.agdref_set_factor(ptr(np.ascontiguousarray(o)), ctypes.c_float(r2), ptr(np.ascontiguousarray(m)))
+
     def values(self):
         v = self.values_b
         if self.multip:
@@ -200,7 +222,8 @@ class RefPipeline:
 
     def flow(self):
         assert not self.multip
-        L = lib(f"libagdref_flow_{self.md['tag']}.so")
+        L = lib(f"libagdref_flow_{self.md['tag']}{'f' if self.factor else ''}.so")
+        self.set_factor(L)
         nd, st = self.ndim, self.size_o * self.size_i
         nact = self.ndim if self.model.startswith("Iso") else self.ndim * (self.ndim + 1) // 2
         self.nact = nact
@@ -465,6 +488,16 @@ def make_cases():
     c["seeds"] = np.array([[0.37, 0.3]], np.float32)
     c["seedRadius"] = 2.0
     cases["iso2_radius"] = c
+    # source factorisation (factoringRadius), seeds spread over the default radius 2
+    c = dict(cases["riem2_radius"])
+    c.pop("seedRadius")
+    c["factoringRadius"] = 10.0
+    c["tips"] = np.array([[0.2, 0.35], [0.8, 1.1], [0.6, 0.5]], np.float32)
+    cases["riem2_factor"] = c
+    c = dict(cases["iso2_radius"])
+    c.pop("seedRadius")
+    c["factoringRadius"] = 12.0
+    cases["iso2_factor"] = c
     # forward AD inputs (drawn last, so that the inputs above do not change):
     # two variations of the cost, and of the seed values
     for key in ("iso2", "riem2", "riem3"):

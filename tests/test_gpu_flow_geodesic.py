@@ -10,7 +10,7 @@ import torch
 from conftest import CASES, load_case, make_dictin
 
 pytestmark = pytest.mark.gpu
-GEO_CASES = [c for c in CASES if c != "ad_notebook"]
+GEO_CASES = [c for c in CASES if c != "ad_notebook"] + ["riem2_factor"]
 
 
 def _split(ref):

@@ -104,7 +104,8 @@ def test_autograd_forward_mode():
         jt = fwAD.unpack_dual(u).tangent
     ref = make_dictin(dict(case, cost=cost.cpu().numpy()),
                       extra={"costVariation": t.cpu().numpy()[..., None]}).Run()["valueVariation"][..., 0]
-    torch.testing.assert_close(jt, ref, rtol=1e-5, atol=1e-6)
+    # two solves, two schedules: agreement to the linear solver's tolerance
+    torch.testing.assert_close(jt, ref, rtol=1e-4, atol=1e-4 * float(ref.abs().max()))
     w = torch.as_tensor(rng.standard_normal(shape).astype(np.float32), device="cuda")
     c = cost.clone().requires_grad_(True)
     (eikonal_values(h, c) * w).sum().backward()
