@@ -299,8 +299,16 @@ class Interface:
         order = self.GetValue("order", default=1, help="Use second order scheme to improve accuracy")
         if order not in {1, 2}:
             raise ValueError(f"Unsupported scheme order {order}")
+        self.order = int(order)
+        self.order2_threshold = 0.0
         if order == 2:
-            raise NotImplementedError("the second order scheme is not available in this build")
+            if self.multiprecision or self.factoringRadius:
+                raise NotImplementedError("the second order scheme with multiprecision or source factorization "
+                                          "is not available in this build")
+            self.order2_threshold = float(self.GetValue(  # _Kernel.py:310-314
+                "order2_threshold", 0.3,
+                help="Relative threshold on second order differences / first order difference,"
+                     "beyond which the second order scheme deactivates"))
         solver = self.GetValue("solver", default="FIM",
                                help="Choice of fixed point solver (AGSI, global_iteration)")
         alt = {"FIM": "fast_iterative_method", "AGSI": "adaptive_gauss_siedel_iteration"}
@@ -570,6 +578,7 @@ class Interface:
         inst.geom = self.geom.data_ptr() if self.geom is not None else None
         inst.rhs = self.rhs_t.data_ptr()
         inst.seedbits = self.seedbits.data_ptr()
+        inst.order2_threshold = getattr(self, "order2_threshold", 0.0)
         if getattr(self, "factor", None) is not None:
             r2, origin, fm = self.factor
             inst.factor_radius2 = float(r2)

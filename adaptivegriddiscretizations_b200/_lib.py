@@ -37,6 +37,7 @@ class AgdInstance(ctypes.Structure):
         ("valuesq_next", ctypes.c_void_p), ("geom", ctypes.c_void_p),
         ("rhs", ctypes.c_void_p), ("seedbits", ctypes.c_void_p), ("trigger", ctypes.c_void_p),
         ("factor_radius2", ctypes.c_float), ("factor_origin", _c_float3), ("factor_metric", ctypes.c_float * 6),
+        ("order2_threshold", ctypes.c_float),
     ]
 
 

@@ -126,7 +126,8 @@ __global__ void mp_copy_kernel(Sched S, int dir) {
 // Jacobi sweeps inside the tile and double-buffered epochs, as the reference
 // forces strict_iter_i and strict_iter_o with it (_Kernel.py:39-45).
 // FACT: source factorisation (shifted neighbour values near the seed).
-template <class TL, int MODEL, bool MP = false, bool FACT = false>
+// ORD2: second order scheme (neighbours two steps away, cuda/HFM.h:91-138).
+template <class TL, int MODEL, bool MP = false, bool FACT = false, bool ORD2 = false>
 struct Visit {
     static constexpr int D = TL::D, P = TL::P;
     static constexpr int NACT = MODEL == AGD_MODEL_ISOTROPIC ? D : D * (D + 1) / 2;
@@ -158,11 +159,35 @@ struct Visit {
     // read from outside the tile, so that every neighbour of a sweep is one
     // shared load; otherwise (kSlots false) the integer parts with multiprecision.
     static constexpr bool kSlots = !MP && TL::SIZE <= 64;
-    static constexpr int kSmemFloats = kSlots ? TL::SIZE + P * NTOT * 32 : 2 * TL::SIZE;
+    static constexpr int kSmemFloats = kSlots ? TL::SIZE + (ORD2 ? 2 : 1) * P * NTOT * 32 : 2 * TL::SIZE;
     __device__ __forceinline__ static float neighbour(float x, const float *us) {
         const int b = __float_as_int(x);
         const float inside = us[b & (TL::SIZE - 1)];  // index masked into this warp's tile
         return (b >> 22) == -1 ? inside : x;
+    }
+    // Second order corrections (cuda/HFM.h:91-138): with u0 the point's value and
+    // v[k] the smaller neighbour along e_k (on side[k]), where
+    // |u0 - 2 v + v2| < thr * max_k (u0 - v_k) and u0 > v, v2 the next neighbour
+    // on that side, v becomes v + (v - v2) / 3 and its weight 9/4 of itself.
+    // Returns the mask of the corrected neighbours.
+    template <class Far>
+    __device__ __forceinline__ static unsigned order2(float u0, float *v, float *w, const int *side, Far &&far,
+                                                      float thr) {
+        float bound = 0.f;
+#pragma unroll
+        for (int k = 0; k < NACT; ++k) bound = fmaxf(bound, u0 - v[k]);
+        unsigned mask = 0;
+#pragma unroll
+        for (int k = 0; k < NACT; ++k) {
+            const float v2 = far(k, side[k]);
+            const float d2 = fabsf(u0 - 2.f * v[k] + v2);
+            if (d2 < thr * bound && u0 > v[k]) {
+                v[k] = (float)((double)v[k] + (double)(v[k] - v2) / 3.0);
+                w[k] *= 2.25f;
+                mask |= 1u << k;
+            }
+        }
+        return mask;
     }
     __device__ __forceinline__ static float lds(unsigned addr) {
         float v;
@@ -272,6 +297,9 @@ struct Visit {
         int nbq[MP ? P : 1][MP ? NTOT : 1];
         unsigned nba[kSlots ? P : 1][kSlots ? NTOT : 1];
         float fsh[FACT ? P : 1][FACT ? NTOT : 1];  // factorisation shifts of the neighbour values
+        // second order: the neighbours two steps away, as nba / nbv
+        unsigned nba2[ORD2 && kSlots ? P : 1][ORD2 && kSlots ? NTOT : 1];
+        float nbv2[ORD2 && !kSlots ? P : 1][ORD2 && !kSlots ? NTOT : 1];
         const unsigned us_addr = (unsigned)__cvta_generic_to_shared(us);
         bool seed[P];
         float raw[P][kRaw];
@@ -341,6 +369,28 @@ struct Visit {
                         }
                         nba[p][2 * k + s] = us_addr + 4u * (unsigned)slot;
                     }
+                    if constexpr (ORD2) {  // the neighbour x + 2 eps e_k
+                        bool in2 = true, dom2 = true;
+#pragma unroll
+                        for (int c = 0; c < D; ++c) {
+                            const int off = 2 * eps * ev[k][c];
+                            yi[c] = xi[c] + off;
+                            yt[c] = xt[c] + off;
+                            in2 = in2 && yi[c] >= 0 && yi[c] < TL::extent(c);
+                            dom2 = dom2 && yt[c] >= 0 && yt[c] < A.shape[c];
+                        }
+                        if constexpr (kSlots) {
+                            int slot = TL::local(yi);
+                            if (!in2) {
+                                slot = TL::SIZE + P * NTOT * 32 + (p * NTOT + 2 * k + s) * 32 + lane;
+                                us[slot] = dom2 ? __ldcg(u_in + bilevel_index<D, TL>(yt, I.shape_o)) : finf();
+                            }
+                            nba2[p][2 * k + s] = us_addr + 4u * (unsigned)slot;
+                        } else {
+                            nbv2[p][2 * k + s] = in2 ? __int_as_float(kBoxed | TL::local(yi))
+                                                     : (dom2 ? __ldcg(u_in + bilevel_index<D, TL>(yt, I.shape_o)) : finf());
+                        }
+                    }
                 }
             }
         }
@@ -400,6 +450,7 @@ struct Visit {
                     float cand = finf();
                     if (!seed[p]) {
                         float v[NACT], w[NACT];
+                        int side[ORD2 ? NACT : 1];
 #pragma unroll
                         for (int k = 0; k < NACT; ++k) {
                             float a, b;
@@ -416,7 +467,12 @@ struct Visit {
                             }
                             v[k] = a > b ? b : a;
                             w[k] = wts[p][k];
+                            if constexpr (ORD2) side[k] = a > b;
                         }
+                        if constexpr (ORD2) order2(us[n_i], v, w, side, [&](int k, int sd) {
+                            if constexpr (kSlots) return lds(nba2[p][2 * k + sd]);
+                            else return neighbour(nbv2[p][2 * k + sd], us);
+                        }, A.order2_threshold);
                         cand = hfm_update<NACT>(rhs[p], v, w);
                     }
                     __syncwarp();
@@ -535,6 +591,21 @@ __device__ __forceinline__ void dispatch(const Sched &S, int t, int e, int lane,
         case V_RIEM3_4_F:
             if constexpr ((VMASK >> V_RIEM3_4_F) & 1) Visit<Tile<3, 4, 4, 4>, AGD_MODEL_RIEMANN, false, true>::run(S, I, ii, n_o, e, lane, us);
             break;
+        case V_ISO2_8_O2:
+            if constexpr ((VMASK >> V_ISO2_8_O2) & 1) Visit<Tile<2, 8, 8, 1>, AGD_MODEL_ISOTROPIC, false, false, true>::run(S, I, ii, n_o, e, lane, us);
+            break;
+        case V_ISO2_16_O2:
+            if constexpr ((VMASK >> V_ISO2_16_O2) & 1) Visit<Tile<2, 16, 16, 1>, AGD_MODEL_ISOTROPIC, false, false, true>::run(S, I, ii, n_o, e, lane, us);
+            break;
+        case V_RIEM2_8_O2:
+            if constexpr ((VMASK >> V_RIEM2_8_O2) & 1) Visit<Tile<2, 8, 8, 1>, AGD_MODEL_RIEMANN, false, false, true>::run(S, I, ii, n_o, e, lane, us);
+            break;
+        case V_ISO3_4_O2:
+            if constexpr ((VMASK >> V_ISO3_4_O2) & 1) Visit<Tile<3, 4, 4, 4>, AGD_MODEL_ISOTROPIC, false, false, true>::run(S, I, ii, n_o, e, lane, us);
+            break;
+        case V_RIEM3_4_O2:
+            if constexpr ((VMASK >> V_RIEM3_4_O2) & 1) Visit<Tile<3, 4, 4, 4>, AGD_MODEL_RIEMANN, false, false, true>::run(S, I, ii, n_o, e, lane, us);
+            break;
         default:
             break;
     }
@@ -558,6 +629,11 @@ constexpr int smem_floats() {
     if ((VMASK >> V_RIEM2_8_F) & 1) m = std::max(m, Visit<Tile<2, 8, 8, 1>, AGD_MODEL_RIEMANN, false, true>::kSmemFloats);
     if ((VMASK >> V_ISO3_4_F) & 1) m = std::max(m, Visit<Tile<3, 4, 4, 4>, AGD_MODEL_ISOTROPIC, false, true>::kSmemFloats);
     if ((VMASK >> V_RIEM3_4_F) & 1) m = std::max(m, Visit<Tile<3, 4, 4, 4>, AGD_MODEL_RIEMANN, false, true>::kSmemFloats);
+    if ((VMASK >> V_ISO2_8_O2) & 1) m = std::max(m, Visit<Tile<2, 8, 8, 1>, AGD_MODEL_ISOTROPIC, false, false, true>::kSmemFloats);
+    if ((VMASK >> V_ISO2_16_O2) & 1) m = std::max(m, Visit<Tile<2, 16, 16, 1>, AGD_MODEL_ISOTROPIC, false, false, true>::kSmemFloats);
+    if ((VMASK >> V_RIEM2_8_O2) & 1) m = std::max(m, Visit<Tile<2, 8, 8, 1>, AGD_MODEL_RIEMANN, false, false, true>::kSmemFloats);
+    if ((VMASK >> V_ISO3_4_O2) & 1) m = std::max(m, Visit<Tile<3, 4, 4, 4>, AGD_MODEL_ISOTROPIC, false, false, true>::kSmemFloats);
+    if ((VMASK >> V_RIEM3_4_O2) & 1) m = std::max(m, Visit<Tile<3, 4, 4, 4>, AGD_MODEL_RIEMANN, false, false, true>::kSmemFloats);
     return m;
 }
 
@@ -567,10 +643,11 @@ struct EikonalVisitor {
     // keep 8 points per lane in registers, Riemann3 twelve neighbours per point,
     // multiprecision an integer part beside every value.
     static constexpr int kMinCtas =
-        (VMASK & ((1u << V_RIEM2_16) | (1u << V_ISO2_16) | (1u << V_ISO2_16_MP) | (1u << V_ISO2_16_F))) ? 4
-        : (VMASK & ((1u << V_RIEM3_4) | (1u << V_RIEM3_4_MP) | (1u << V_RIEM3_4_F)))                    ? 6
-        : (VMASK & (kMpVariants | kFactorVariants))                                                     ? 7
-                                                                                                        : 9;
+        (VMASK & ((1u << V_RIEM2_16) | (1u << V_ISO2_16) | (1u << V_ISO2_16_MP) | (1u << V_ISO2_16_F) |
+                  (1u << V_ISO2_16_O2)))                                                      ? 4
+        : (VMASK & ((1u << V_RIEM3_4) | (1u << V_RIEM3_4_MP) | (1u << V_RIEM3_4_F) | (1u << V_RIEM3_4_O2))) ? 6
+        : (VMASK & (kMpVariants | kFactorVariants | kOrder2Variants))                                ? 7
+                                                                                                     : 9;
     struct Args {};
     struct Smem {
         float u[smem_floats<VMASK>()];  // values, then out-of-tile neighbours or integer parts
@@ -663,6 +740,14 @@ static int run_variants(int ndim, unsigned vmask, const WsLayout &L, void *ws, i
     constexpr unsigned R3 = 1u << V_RIEM3_4, I3 = 1u << V_ISO3_4, R2L = 1u << V_RIEM2_16;
     constexpr unsigned MP2 = (1u << V_ISO2_8_MP) | (1u << V_ISO2_16_MP) | (1u << V_RIEM2_8_MP);
     constexpr unsigned MP3 = (1u << V_ISO3_4_MP) | (1u << V_RIEM3_4_MP);
+    if (vmask & kOrder2Variants) {  // second order instances, possibly beside plain ones
+        constexpr unsigned O2 = (1u << V_ISO2_8_O2) | (1u << V_ISO2_16_O2) | (1u << V_RIEM2_8_O2);
+        constexpr unsigned O3 = (1u << V_ISO3_4_O2) | (1u << V_RIEM3_4_O2);
+        if (vmask & (kMpVariants | kFactorVariants))
+            return set_error(AGD_STATUS_UNSUPPORTED, "second order beside multiprecision or factorisation in one plan");
+        if (ndim == 2) return run_sched<EikonalVisitor<O2 | R2 | I16 | I8 | R2L>>(L, ws, n, {}, stats, cfg, st);
+        return run_sched<EikonalVisitor<O3 | R3 | I3>>(L, ws, n, {}, stats, cfg, st);
+    }
     if (vmask & kFactorVariants) {  // factored instances, possibly beside plain ones
         constexpr unsigned F2 = (1u << V_ISO2_8_F) | (1u << V_ISO2_16_F) | (1u << V_RIEM2_8_F);
         constexpr unsigned F3 = (1u << V_ISO3_4_F) | (1u << V_RIEM3_4_F);
@@ -819,10 +904,26 @@ __global__ void flow_kernel(Inst I, float *fvec, float *fwsum, float *fw, int *f
             float vs[NACT], ws[NACT];
 #pragma unroll
             for (int k = 0; k < NACT; ++k) { vs[k] = v[k]; ws[k] = w[k]; }
+            unsigned o2 = 0;
+            if (A.order2_threshold > 0.f) {  // second order: v corrected in place, weights 9/4
+                o2 = V::order2(__ldg(A.values + n_t), vs, ws, side, [&](int k, int sd) {
+                    int y[3] = {0, 0, 0};
+                    bool ok = true;
+#pragma unroll
+                    for (int c = 0; c < D; ++c) {
+                        y[c] = xt[c] + 2 * (2 * sd - 1) * ev[k][c];
+                        ok = ok && y[c] >= 0 && y[c] < A.shape[c];
+                    }
+                    return ok ? __ldg(A.values + bilevel_index<D, TL>(y, I.shape_o)) : finf();
+                }, A.order2_threshold);
+#pragma unroll
+                for (int k = 0; k < NACT; ++k) v[k] = vs[k];
+            }
             const float val = hfm_update<NACT>(__ldg(A.rhs + n_t), vs, ws);
             if (val != finf()) {
 #pragma unroll
-                for (int k = 0; k < NACT; ++k) fwk[k] = w[k] * fmaxf(0.f, val - v[k]);
+                for (int k = 0; k < NACT; ++k)
+                    fwk[k] = w[k] * fmaxf(0.f, val - v[k]) * (((o2 >> k) & 1) ? 1.5f : 1.f);
             }
         }
         float vec[3] = {0.f, 0.f, 0.f}, sum = 0.f;

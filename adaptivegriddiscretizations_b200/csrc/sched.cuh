@@ -19,17 +19,32 @@ enum Variant {
     // multiprecision
     V_ISO2_8_MP, V_ISO2_16_MP, V_RIEM2_8_MP, V_ISO3_4_MP, V_RIEM3_4_MP,
     // source factorisation
-    V_ISO2_8_F, V_ISO2_16_F, V_RIEM2_8_F, V_ISO3_4_F, V_RIEM3_4_F, V_COUNT
+    V_ISO2_8_F, V_ISO2_16_F, V_RIEM2_8_F, V_ISO3_4_F, V_RIEM3_4_F,
+    // second order scheme
+    V_ISO2_8_O2, V_ISO2_16_O2, V_RIEM2_8_O2, V_ISO3_4_O2, V_RIEM3_4_O2, V_COUNT
 };
 constexpr unsigned kMpVariants = (1u << V_ISO2_8_MP) | (1u << V_ISO2_16_MP) | (1u << V_RIEM2_8_MP) |
                                  (1u << V_ISO3_4_MP) | (1u << V_RIEM3_4_MP);
 constexpr unsigned kFactorVariants = (1u << V_ISO2_8_F) | (1u << V_ISO2_16_F) | (1u << V_RIEM2_8_F) |
                                      (1u << V_ISO3_4_F) | (1u << V_RIEM3_4_F);
+constexpr unsigned kOrder2Variants = (1u << V_ISO2_8_O2) | (1u << V_ISO2_16_O2) | (1u << V_RIEM2_8_O2) |
+                                     (1u << V_ISO3_4_O2) | (1u << V_RIEM3_4_O2);
 
 static int base_variant_of(const agd_instance &a);
 
 static int variant_of(const agd_instance &a) {
     const int v = base_variant_of(a);
+    if (v >= 0 && a.order2_threshold > 0.f) {
+        if (a.multip_step != 0.f || a.factor_radius2 > 0.f) return -1;  // not built
+        switch (v) {
+            case V_ISO2_8: return V_ISO2_8_O2;
+            case V_ISO2_16: return V_ISO2_16_O2;
+            case V_RIEM2_8: return V_RIEM2_8_O2;
+            case V_ISO3_4: return V_ISO3_4_O2;
+            case V_RIEM3_4: return V_RIEM3_4_O2;
+            default: return -1;
+        }
+    }
     if (v >= 0 && a.factor_radius2 > 0.f) {
         if (a.multip_step != 0.f) return -1;  // no build of factorisation with multiprecision
         switch (v) {
@@ -524,8 +539,11 @@ static int run_sched(const WsLayout &L, void *ws, int n, const typename Visitor:
     if ((err = cudaGetLastError()) != cudaSuccess) return set_cuda_error("setup_tiles", err);
     publish_first<<<(n + 7) / 8, 256, 0, st>>>(S);
     if ((err = cudaGetLastError()) != cudaSuccess) return set_cuda_error("publish_first", err);
-    const int rc = (cfg && cfg->warps_per_cta == 8) ? launch_workers<Visitor, 8>(S, VA, L.total_tiles, cfg, st)
-                                                    : launch_workers<Visitor, 4>(S, VA, L.total_tiles, cfg, st);
+    // 8-warp CTAs only where their static shared memory fits in 48 KB
+    constexpr bool kWide = sizeof(typename Visitor::Smem) * 8 + sizeof(int) * kSmemInst <= 48 * 1024;
+    const int rc = (kWide && cfg && cfg->warps_per_cta == 8)
+                       ? launch_workers<Visitor, kWide ? 8 : 4>(S, VA, L.total_tiles, cfg, st)
+                       : launch_workers<Visitor, 4>(S, VA, L.total_tiles, cfg, st);
     if (rc != AGD_STATUS_OK) return rc;
     if ((err = Visitor::finalize(S, L, st)) != cudaSuccess) return set_cuda_error("finalize", err);
     finish_stats<<<(n + 127) / 128, 128, 0, st>>>(S, stats);

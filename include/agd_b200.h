@@ -77,6 +77,11 @@ typedef struct agd_instance {
     float factor_metric[6];  /* metric at the seed with cost and grid scales applied (index
                                 units): packed lower triangle (Riemann), squared costs per
                                 axis (Isotropic) */
+    /* Second order scheme (order: 2; cuda/HFM.h:91-138, 175-206): threshold on
+     * |u - 2v + v2| / max(u - v) below which a neighbour is extrapolated to
+     * second order (order2_threshold, default 0.3).  0: first order.  Not with
+     * multiprecision or source factorisation. */
+    float order2_threshold;
 } agd_instance;
 
 #define AGD_FLAG_ACTIVATE_ALL 1 /* every tile is active at the first iteration */
@@ -276,7 +281,7 @@ int agd_forward(const agd_instance *inst, const float *flow_weights, const int32
 /* ------------------------------------------------------------------- misc -- */
 
 const char *agd_last_error(void);
-int agd_version(void); /* 2: agd_instance with the source factorisation fields */
+int agd_version(void); /* 2: agd_instance with the source factorisation and second order fields */
 
 #if defined(__GNUC__)
 #pragma GCC visibility pop

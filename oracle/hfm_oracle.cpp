@@ -19,6 +19,7 @@
 //   reverse AD linear system     _PostProcess.py:155-219 (solved here by ordered sweeps)
 //   forward AD linear system     _PostProcess.py:181-191 (ordered sweeps)
 //   source factorisation         cuda/EuclideanFactor.h:8-26, FiniteDifferences.h:30-75
+//   second order scheme          cuda/HFM.h:91-138 (HFMNeighbors), 175-206 (weights)
 //
 // Arrays passed to this library are in plain row-major grid layout (not the
 // bilevel tile layout of the GPU kernels).  The tile structure is used only to
@@ -142,6 +143,8 @@ struct Problem {
     // neighbour values are shifted so that the scheme is exact for |x|_m, m the
     // metric at the seed (packed lower-triangular; isotropic: D diagonal entries).
     T fact_r2 = 0, fact_origin[3] = {0, 0, 0}, fact_m[6] = {0, 0, 0, 0, 0, 0};
+    // Second order scheme (order: 2): threshold on |u - 2v + v2| / max(u - v); 0: off.
+    T order2 = 0;
 
     T scal_fact(const T *x, const T *y) const {
         if (model == 0) {
@@ -262,6 +265,21 @@ T hfm_update(T rhs, const T *w, const T *v, int nact, T *flow_w) {
     return val;
 }
 
+// Second order corrections (HFM.h:91-138): u0 the point's value, v[k] the
+// smaller of the two neighbours along e_k (on side[k]), v2[k] the neighbour two
+// steps away on that side.  Where |u0 - 2 v + v2| < thr * max_k (u0 - v_k) and
+// u0 > v, v becomes v + (v - v2) / 3 and o2[k] = 1 (weight x 9/4, flow x 3/2).
+template <class T>
+void order2_correct(T u0, T *v, const T *v2, int nact, T thr, char *o2) {
+    T bound = 0;
+    for (int k = 0; k < nact; ++k) bound = std::max(bound, u0 - v[k]);
+    for (int k = 0; k < nact; ++k) {
+        const T d2 = std::fabs(u0 - 2 * v[k] + v2[k]);
+        o2[k] = d2 < thr * bound && u0 > v[k];
+        if (o2[k]) v[k] += (v[k] - v2[k]) / 3;
+    }
+}
+
 // ------------------------------------------------------------ tile visit ---
 template <class T>
 struct Solver {
@@ -293,8 +311,8 @@ struct Solver {
         std::vector<long> pts(S);
         std::vector<int> xi(3 * S), xt(3 * S);
         tile_points(n_o, pts.data(), xi.data(), xt.data());
-        std::vector<T> ul(S), uold(S), rhs(S), w(S * 6), vo(S * 12), sh(S * 12, T(0));
-        std::vector<int> vi(S * 12);
+        std::vector<T> ul(S), uold(S), rhs(S), w(S * 6), vo(S * 12), sh(S * 12, T(0)), vo2(S * 12);
+        std::vector<int> vi(S * 12), vi2(S * 12);
         std::vector<char> seed(S);
         for (int n = 0; n < S; ++n) {
             const long p = pts[n];
@@ -328,23 +346,53 @@ struct Solver {
                         vi[n * 12 + ks] = -1;
                         vo[n * 12 + ks] = P.inside(yt) ? u[P.flat(yt)] : inf<T>();
                     }
+                    if (P.order2 > 0) {  // the neighbour two steps away
+                        bool in2 = true;
+                        for (int c = 0; c < D; ++c) {
+                            yi[c] += eps * e[k][c];
+                            yt[c] += eps * e[k][c];
+                            if (yi[c] < 0 || yi[c] >= P.shape_i[c]) in2 = false;
+                        }
+                        if (in2) {
+                            int li = 0;
+                            for (int c = 0; c < D; ++c) li = li * P.shape_i[c] + yi[c];
+                            vi2[n * 12 + ks] = li;
+                        } else {
+                            vi2[n * 12 + ks] = -1;
+                            vo2[n * 12 + ks] = P.inside(yt) ? u[P.flat(yt)] : inf<T>();
+                        }
+                    }
                 }
         }
         for (int it = 0; it < niter_i; ++it) {
             bool moved = false;
             for (int n = 0; n < S; ++n) {
                 if (seed[n]) continue;
-                T v[6];
+                T v[6], v2[6], wk[6];
+                int side[6];
                 for (int k = 0; k < NA; ++k) {
                     T best = 0;
+                    side[k] = 0;
                     for (int s = 0; s < 2; ++s) {
                         const int ks = 2 * k + s;
                         const T val = (vi[n * 12 + ks] >= 0 ? ul[vi[n * 12 + ks]] : vo[n * 12 + ks]) + sh[n * 12 + ks];
-                        if (s == 0 || best > val) best = val;
+                        if (s == 0) best = val;
+                        else if (best > val) { best = val; side[k] = 1; }
                     }
                     v[k] = best;
+                    wk[k] = w[n * 6 + k];
                 }
-                const T cand = hfm_update<T>(rhs[n], &w[n * 6], v, NA, nullptr);
+                if (P.order2 > 0) {
+                    for (int k = 0; k < NA; ++k) {
+                        const int ks = 2 * k + side[k];
+                        v2[k] = vi2[n * 12 + ks] >= 0 ? ul[vi2[n * 12 + ks]] : vo2[n * 12 + ks];
+                    }
+                    char o2[6];
+                    order2_correct<T>(ul[n], v, v2, NA, P.order2, o2);
+                    for (int k = 0; k < NA; ++k)
+                        if (o2[k]) wk[k] *= T(9) / T(4);
+                }
+                const T cand = hfm_update<T>(rhs[n], wk, v, NA, nullptr);
                 if (ul[n] > cand) { ul[n] = cand; moved = true; }
             }
             if (!moved) break;  // a pass without change is a fixed point of the visit
@@ -451,10 +499,24 @@ struct Solver {
                         else if (v[k] > val) { v[k] = val; side[k] = 1; }
                     }
                 }
-                T f[6];
-                const T cand = hfm_update<T>(T(P.rhs[p]), wts, v, NA, f);
+                T f[6], wk[6];
+                char o2[6] = {0, 0, 0, 0, 0, 0};
+                for (int k = 0; k < NA; ++k) wk[k] = wts[k];
+                if (P.order2 > 0) {
+                    T v2[6];
+                    for (int k = 0; k < NA; ++k) {
+                        int y[3];
+                        for (int c = 0; c < D; ++c) y[c] = x[c] + 2 * (2 * side[k] - 1) * e[k][c];
+                        v2[k] = P.inside(y) ? u[P.flat(y)] : inf<T>();
+                    }
+                    order2_correct<T>(u[p], v, v2, NA, P.order2, o2);
+                    for (int k = 0; k < NA; ++k)
+                        if (o2[k]) wk[k] *= T(9) / T(4);
+                }
+                const T cand = hfm_update<T>(T(P.rhs[p]), wk, v, NA, f);
                 if (u[p] > cand) unew[p] = cand;
-                for (int k = 0; k < NA; ++k) wts[k] = f[k];
+                for (int k = 0; k < NA; ++k)  // flow weights from the plain weights, x 3/2 at second order
+                    wts[k] = cand == inf<T>() ? T(0) : wts[k] * std::fmax(T(0), cand - v[k]) * (o2[k] ? T(1.5) : T(1));
             } else {
                 P.stencil(p, wts, e);
                 for (int k = 0; k < NA; ++k) wts[k] = 0;
@@ -649,6 +711,7 @@ void fill_problem(Problem<T> &P, int ndim, int model, const int *shape, const in
 
 // Source factorisation of the next solves (agdo_set_factor).
 double g_fact_r2 = 0, g_fact_origin[3] = {0, 0, 0}, g_fact_m[6] = {0, 0, 0, 0, 0, 0};
+double g_order2 = 0;
 
 template <class T>
 int eikonal_impl(int ndim, int model, const int *shape, const int *shape_i, int niter_i, int front,
@@ -660,6 +723,7 @@ int eikonal_impl(int ndim, int model, const int *shape, const int *shape_i, int 
     S.P.fact_r2 = T(g_fact_r2);
     for (int c = 0; c < 3; ++c) S.P.fact_origin[c] = T(g_fact_origin[c]);
     for (int c = 0; c < 6; ++c) S.P.fact_m[c] = T(g_fact_m[c]);
+    S.P.order2 = T(g_order2);
     S.u.assign(values, values + S.P.size);
     S.atol = T(atol);
     S.rtol = T(rtol);
@@ -721,6 +785,9 @@ int agdo_eikonal(int dbl, int ndim, int model, const int *shape, const int *shap
     return eikonal_impl<float>(ndim, model, shape, shape_i, niter_i, front, iso_w, geom, rhs, seed, values,
                                atol, rtol, nitermax, nthreads, visits, fvec, fwsum, fw, fidx);
 }
+
+// Second order scheme for the following agdo_eikonal calls (threshold; 0: off).
+void agdo_set_order2(double threshold) { g_order2 = threshold; }
 
 // Source factorisation for the following agdo_eikonal calls (r2 = 0: off).
 void agdo_set_factor(double r2, const double *origin, const double *metric) {

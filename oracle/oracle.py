@@ -111,6 +111,7 @@ def prepare(case):
     seeds = np.asarray(case["seeds"], np.float32).reshape(-1, pr.ndim)
     sv = np.asarray(case.get("seedValues", np.zeros(len(seeds))), np.float32)
     start = pr.origin + 0.5 * pr.h
+    pr.order2 = float(case.get("order2_threshold", 0.3)) if int(case.get("order", 1)) == 2 else 0.0
     fr = float(case.get("factoringRadius", 0.0))
     pr.factor = None
     if fr:  # source factorisation around the (single) seed (_Kernel.py:47-49, 301-308)
@@ -214,6 +215,7 @@ def eikonal(pr, dtype=np.float32, values=None, nthreads=1, flow=False, nitermax=
         fi = np.zeros((nact,) + pr.shape, np.int32)
     geom = None if pr.geom is None else np.ascontiguousarray(pr.geom, np.float32)
     iso = None if pr.iso_w is None else np.ascontiguousarray(pr.iso_w, np.float64)
+    L.agdo_set_order2(ctypes.c_double(getattr(pr, "order2", 0.0)))
     fac = getattr(pr, "factor", None)
     if fac is None:
         L.agdo_set_factor(ctypes.c_double(0.0), None, None)

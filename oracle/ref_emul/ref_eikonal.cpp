@@ -6,7 +6,8 @@
 // Compile-time configuration (set by oracle/ref_emul/Makefile):
 //   AGDREF_ISO (0|1), AGDREF_NDIM, AGDREF_SHAPE_I (comma list), AGDREF_SIZE_I,
 //   AGDREF_LOG2_SIZE_I, AGDREF_NITER_I, AGDREF_MULTIP (0|1), AGDREF_FLOW (0|1),
-//   AGDREF_FACTOR (0|1, source factorisation, factor_macro of _Kernel.py:47-49).
+//   AGDREF_FACTOR (0|1, source factorisation, factor_macro of _Kernel.py:47-49),
+//   AGDREF_ORDER2 (0|1, second order scheme, order2_macro of _Kernel.py:51-54).
 //
 // The block below states the same compile-time traits that the reference's
 // `cupy_module_helper.traits_header` emits for these models
@@ -20,6 +21,12 @@
 #endif
 #if AGDREF_FACTOR
 #define factor_macro true
+#endif
+#ifndef AGDREF_ORDER2
+#define AGDREF_ORDER2 0
+#endif
+#if AGDREF_ORDER2
+#define order2_macro true
 #endif
 #define pruning_macro false
 #define geom_first_macro true
@@ -153,6 +160,11 @@ void agdref_set_factor(const float *origin, float radius2, const float *metric) 
     factor_radius2 = radius2;
     for (int k = 0; k < factor_size; ++k) factor_metric[k] = metric[k];
 }
+#endif
+
+#if AGDREF_ORDER2
+// The module constant of the second order scheme (_Kernel.py:310-314).
+void agdref_set_order2(float threshold) { order2_threshold = threshold; }
 #endif
 
 #if !AGDREF_FLOW

@@ -27,6 +27,8 @@ def load_case(name):
     for k in ("seedRadius", "factoringRadius"):
         if k in case:
             case[k] = float(case[k])
+    if "order" in case:
+        case["order"] = int(case["order"])
     out = {k[4:]: d[k] for k in d.files if k.startswith("out_")}
     return case, out
 
@@ -34,6 +36,7 @@ def load_case(name):
 CASES = ["iso2", "riem2", "riem2_aniso", "iso3", "riem3", "ad_notebook"]
 RADIUS_CASES = ["riem2_radius", "iso2_radius"]  # seeds spread over a radius (values only)
 FACTOR_CASES = ["riem2_factor", "iso2_factor"]  # source factorisation (factoringRadius)
+ORDER2_CASES = ["riem2_order2", "iso2_order2", "riem3_order2"]  # second order scheme (order: 2)
 
 
 @pytest.fixture(params=CASES)
@@ -46,7 +49,7 @@ def make_dictin(case, mode="gpu", extra=None):
     from adaptivegriddiscretizations_b200 import Eikonal
     d = {"model": case["model"], "mode": mode, "arrayOrdering": "RowMajor", "verbosity": 0}
     for k in ("dims", "gridScales", "origin", "seeds", "seedValues", "cost", "tips", "traits", "sensitivity",
-              "seedRadius", "factoringRadius"):
+              "seedRadius", "factoringRadius", "order"):
         if k in case:
             d[k] = case[k]
     if "metric" in case:

@@ -195,7 +195,7 @@ class RefPipeline:
 
     def solve(self):
         md = self.md
-        name = f"libagdref_eik_{md['tag']}{'mp' if self.multip else ''}{'f' if self.factor else ''}.so"
+        name = f"libagdref_eik_{md['tag']}{'mp' if self.multip else ''}{'f' if self.factor else ''}{self.o2tag}.so"
         L = lib(name)
         self.set_factor(L)
         trig_o = self.bexp(self.trigger, False).reshape(self.shape_o + (-1,)).any(-1).astype(np.uint8)
@@ -209,7 +209,13 @@ class RefPipeline:
             ctypes.byref(nup))
         self.tile_visits = nup.value
 
+    @property
+    def o2tag(self):
+        return "o" if int(self.c.get("order", 1)) == 2 else ""
+
     def set_factor(self, L):
+        if self.o2tag:  # order2_threshold (_Kernel.py:310-314)
+            L.agdref_set_order2(ctypes.c_float(float(self.c.get("order2_threshold", 0.3))))
         if self.factor:
             o, r2, m = self.factor
             L.agdref_set_factor(ptr(np.ascontiguousarray(o)), ctypes.c_float(r2), ptr(np.ascontiguousarray(m)))
@@ -222,7 +228,7 @@ class RefPipeline:
 
     def flow(self):
         assert not self.multip
-        L = lib(f"libagdref_flow_{self.md['tag']}{'f' if self.factor else ''}.so")
+        L = lib(f"libagdref_flow_{self.md['tag']}{'f' if self.factor else ''}{self.o2tag}.so")
         self.set_factor(L)
         nd, st = self.ndim, self.size_o * self.size_i
         nact = self.ndim if self.model.startswith("Iso") else self.ndim * (self.ndim + 1) // 2
@@ -498,6 +504,11 @@ def make_cases():
     c.pop("seedRadius")
     c["factoringRadius"] = 12.0
     cases["iso2_factor"] = c
+    # second order scheme (order: 2)
+    for key in ("riem2", "iso2", "riem3"):
+        c = {k: v for k, v in cases[key].items() if k != "sensitivity"}
+        c["order"] = 2
+        cases[key + "_order2"] = c
     # forward AD inputs (drawn last, so that the inputs above do not change):
     # two variations of the cost, and of the seed values
     for key in ("iso2", "riem2", "riem3"):

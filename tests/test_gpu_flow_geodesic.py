@@ -7,7 +7,7 @@ import numpy as np
 import pytest
 import torch
 
-from conftest import CASES, load_case, make_dictin
+from conftest import CASES, ORDER2_CASES, load_case, make_dictin
 
 pytestmark = pytest.mark.gpu
 GEO_CASES = [c for c in CASES if c != "ad_notebook"] + ["riem2_factor"]
@@ -51,3 +51,18 @@ def test_geodesics_vs_reference(name):
         m = min(g.shape[1], want.shape[1])
         assert np.abs(g[:, :m] - want[:, :m]).max() < 2e-3 * np.abs(want).max()
         assert np.linalg.norm(g[:, -1] - want[:, -1]) < 3 * float(np.max(case["gridScales"]))
+
+
+@pytest.mark.parametrize("name", ORDER2_CASES)
+def test_geodesics_order2(name):
+    """Second order: the values depend on the order of the in-tile updates (see
+    test_values_vs_reference), so the paths are compared by their stop codes and
+    their ends, which must reach the seed."""
+    case, ref = load_case(name)
+    case = {k: v for k, v in case.items() if k != "sensitivity"}
+    out = make_dictin(case).Run()
+    assert list(out["geodesic_stopping_criteria"]) == [str(s) for s in ref["geodesic_stopping_criteria"]]
+    for g, want in zip(out["geodesics"], _split(ref)):
+        g = g.cpu().numpy()
+        assert np.linalg.norm(g[:, -1] - want[:, -1]) < 3 * float(np.max(case["gridScales"]))
+        assert np.linalg.norm(g[:, 0] - want[:, 0]) < 1e-5

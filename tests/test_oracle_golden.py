@@ -8,7 +8,7 @@ import numpy as np
 import pytest
 
 from oracle import oracle as O
-from conftest import load_case, CASES, RADIUS_CASES, FACTOR_CASES
+from conftest import load_case, CASES, RADIUS_CASES, FACTOR_CASES, ORDER2_CASES
 
 REL = 1e-5  # parity bar for float32 values
 
@@ -22,7 +22,7 @@ def _geodesic_split(out):
     return res
 
 
-@pytest.mark.parametrize("name", CASES + RADIUS_CASES + FACTOR_CASES)
+@pytest.mark.parametrize("name", CASES + RADIUS_CASES + FACTOR_CASES + ORDER2_CASES)
 @pytest.mark.parametrize("dtype", [np.float32, np.float64])
 def test_values(name, dtype):
     case, ref = load_case(name)
@@ -37,7 +37,7 @@ def test_values(name, dtype):
         assert r["tile_visits"] == int(ref["tile_visits"])
 
 
-@pytest.mark.parametrize("name", [c for c in CASES if c != "ad_notebook"] + ["riem2_factor"])
+@pytest.mark.parametrize("name", [c for c in CASES if c != "ad_notebook"] + ["riem2_factor"] + ORDER2_CASES)
 def test_geodesics(name):
     case, ref = load_case(name)
     r = O.run(case, np.float32)
