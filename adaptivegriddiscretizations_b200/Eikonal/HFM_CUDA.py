@@ -415,8 +415,21 @@ class Interface:
             hmin = float(np.min(self.h))
             self.multip_step = float(2.0 ** np.floor(np.log2(hmin / 10)))
             self.multip_max = float(np.iinfo(np.int32).max * self.multip_step / 2)
-        if self.GetValue("walls", default=None, help="Obstacles in the domain") is not None:
-            raise NotImplementedError("walls are not available in this build")
+        # obstacles (_SetGeometry.py:262-280): distance map by agd_prep_walls in SetArgs
+        walls = self.GetValue("walls", default=None, help="Obstacles in the domain")
+        self.walls = self.wall_dist = None
+        if walls is not None:
+            w = _to_tensor(walls, torch.bool)
+            if tuple(w.shape) != self.shape:
+                w = w.expand(self.shape)
+            self.walls = w.to(torch.uint8).contiguous()
+            self.wallDistBound = int(self.GetValue(
+                "wallDistBound", default=10,
+                help="Bound on the computed distance to the obstacles.\n"
+                     "(Ideally a sharp upper bound on the stencil width.)"))
+            if not 0 <= self.wallDistBound <= 254:
+                raise ValueError("wallDistBound must lie in [0, 254]")
+            self.wall_dist = torch.empty(self.size_tot, dtype=torch.uint8, device="cuda")
 
     def SetArgs(self):
         """Initial values, rhs, seeds (agd/Eikonal/HFM_CUDA/_SetArgs.py:8-177)."""
@@ -492,9 +505,16 @@ class Interface:
         self.seed_values = seedValues.contiguous().float()
         self.seed_idx_t = torch.from_numpy(idx.astype(np.int32)).pin_memory().to("cuda", non_blocking=True)
         self.seedbits = torch.empty(self.size_tot // 8, dtype=torch.uint8, device="cuda")
+        # with walls, the first tiles are those of the seeds alone (_SetArgs.py:119-126)
+        self.trigger_t = None if self.walls is None else torch.zeros(self.size_o, dtype=torch.uint8, device="cuda")
         _lib.check(L.agd_prep_seeds(self.ndim, self.c_shape, self.c_shape_i, _lib.ptr(self.seed_idx_t),
                                     _lib.ptr(self.seed_values), len(idx), _lib.ptr(self.rhs_t),
-                                    _lib.ptr(self.seedbits), None, self.stream), "seeds")
+                                    _lib.ptr(self.seedbits), _lib.ptr(self.trigger_t), self.stream), "seeds")
+        if self.walls is not None:  # walls: seeds of value +inf, after the seeds
+            tmp = torch.empty(2 * int(np.prod(self.shape)), dtype=torch.uint8, device="cuda")
+            _lib.check(L.agd_prep_walls(self.ndim, self.c_shape, self.c_shape_i, _lib.ptr(self.walls),
+                                        self.wallDistBound, _lib.ptr(self.wall_dist), _lib.ptr(tmp),
+                                        _lib.ptr(self.rhs_t), _lib.ptr(self.seedbits), self.stream), "walls")
 
     def _cost_metrics(self, pts):
         """The metric with the grid scales and the cost applied (index units;
@@ -578,6 +598,10 @@ class Interface:
         inst.geom = self.geom.data_ptr() if self.geom is not None else None
         inst.rhs = self.rhs_t.data_ptr()
         inst.seedbits = self.seedbits.data_ptr()
+        if getattr(self, "trigger_t", None) is not None:
+            inst.trigger = self.trigger_t.data_ptr()
+        if getattr(self, "wall_dist", None) is not None:
+            inst.wall_dist = self.wall_dist.data_ptr()
         inst.order2_threshold = getattr(self, "order2_threshold", 0.0)
         if getattr(self, "factor", None) is not None:
             r2, origin, fm = self.factor
@@ -737,6 +761,8 @@ class Interface:
         value[pos] = self.seed_values.to(value.dtype)
         rhs_all = cv * value[..., None]
         rhs_all[pos] = sv.T[torch.as_tensor(self.seed_owner, device="cuda")] if sv is not None else 0.0
+        if self.walls is not None:  # the walls' right-hand side +inf does not vary
+            rhs_all[self.walls.bool()] = 0.0
         inst = self.instance()
         nbytes = L.agd_reverse_workspace_bytes(ctypes.byref(inst))
         ws = torch.empty(max(int(nbytes), 1), dtype=torch.uint8, device="cuda")

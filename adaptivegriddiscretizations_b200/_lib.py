@@ -37,7 +37,7 @@ class AgdInstance(ctypes.Structure):
         ("valuesq_next", ctypes.c_void_p), ("geom", ctypes.c_void_p),
         ("rhs", ctypes.c_void_p), ("seedbits", ctypes.c_void_p), ("trigger", ctypes.c_void_p),
         ("factor_radius2", ctypes.c_float), ("factor_origin", _c_float3), ("factor_metric", ctypes.c_float * 6),
-        ("order2_threshold", ctypes.c_float),
+        ("order2_threshold", ctypes.c_float), ("wall_dist", ctypes.c_void_p),
     ]
 
 
@@ -77,6 +77,7 @@ SIGNATURES = {
     "agd_block_squeeze": (_I, [_I, _P, _P, _I, _P, _P, _P]),
     "agd_prep_seeds": (_I, [_I, _P, _P, _P, _P, _I, _P, _P, _P, _P]),
     "agd_prep_batch": (_I, [_P, _P]),
+    "agd_prep_walls": (_I, [_I, _P, _P, _P, _I, _P, _P, _P, _P, _P]),
     "agd_selling": (_I, [_I, _P, _I, _P, _P, _P]),
     "agd_flow": (_I, [_P, _P, _P, _P, _P, _P]),
     "agd_eucl_map": (_I, [_I, _P, _P, _I, _I, _P, _P, _P]),
@@ -117,7 +118,7 @@ def lib():
                 fn = getattr(L, name)
                 fn.restype = res
                 fn.argtypes = args
-            if L.agd_version() != 2:
+            if L.agd_version() != 3:
                 raise RuntimeError("libagd_b200.so has an unexpected ABI version")
             _lib = L
     return _lib

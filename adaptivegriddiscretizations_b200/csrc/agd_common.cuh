@@ -247,6 +247,45 @@ __device__ __forceinline__ void factor_shifts(const agd_instance &A, const int *
     }
 }
 
+// ------------------------------------------------------------------ walls ---
+// n / d rounded to the closest integer, halves away from zero (the rounding of
+// the reference's divRoundClosest, cuda/Walls.h:12-14).
+__device__ __forceinline__ int div_round_closest(int n, int d) {
+    return ((n < 0) != (d < 0)) ? (n - d / 2) / d : (n + d / 2) / d;
+}
+
+// Whether the segment from grid point xt to xt + v meets no wall
+// (cuda/Walls.h:18-50).  wd0 is the wall distance at xt; dist(y) gives the
+// wall distance at grid point y (255 outside the grid).  Clear when xt is far
+// from every wall (255) or |v|_1 < wd0; otherwise the lattice points
+// w_k = round(k v / |v|_inf), k = 1..|v|_inf, are walked from the source: the
+// segment is clear as soon as |v - w_k|_1 is below the wall distance at
+// xt + w_k, and blocked when xt + w_k is a wall.
+template <int D, class Dist>
+__device__ __forceinline__ bool visible(int wd0, const int *xt, const int *v, Dist &&dist) {
+    if (wd0 == 255) return true;
+    int l1 = 0, linf = 0;
+#pragma unroll
+    for (int c = 0; c < D; ++c) {
+        l1 += abs(v[c]);
+        linf = max(linf, abs(v[c]));
+    }
+    if (l1 < wd0) return true;
+    for (int k = 1; k <= linf; ++k) {
+        int y[3] = {0, 0, 0}, rest = 0;
+#pragma unroll
+        for (int c = 0; c < D; ++c) {
+            const int w = div_round_closest(v[c] * k, linf);
+            rest += abs(v[c] - w);
+            y[c] = xt[c] + w;
+        }
+        const int d = dist(y);
+        if (rest < d) return true;
+        if (d == 0) return false;
+    }
+    return true;
+}
+
 // ----------------------------------------------------------- grid barrier ---
 // Software grid barrier for cooperatively launched kernels.  Waits are bounded
 // in time (globaltimer); a timeout raises AGD_STATUS_WATCHDOG in *err and the

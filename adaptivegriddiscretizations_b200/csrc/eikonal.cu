@@ -34,13 +34,15 @@
 namespace agd {
 
 // ------------------------------------------------------- stencil cache ---
-// Offsets of the Selling stencil packed in one 32-bit word: two int16 in 2D,
-// three 10-bit signed fields in 3D.
+// Offsets of the Selling stencil packed in one 32-bit word: two 15-bit signed
+// fields in 2D, three 10-bit signed fields in 3D; bits 30 and 31 flag the
+// neighbours x - e and x + e hidden by a wall (kHideShift).
+constexpr int kHideShift = 30;
 template <int D>
 __device__ __forceinline__ bool pack_offset(const int *e, int &word) {
     if constexpr (D == 2) {
-        if (e[0] < -32768 || e[0] > 32767 || e[1] < -32768 || e[1] > 32767) return false;
-        word = (e[0] & 0xffff) | (e[1] << 16);
+        if (e[0] < -16384 || e[0] > 16383 || e[1] < -16384 || e[1] > 16383) return false;
+        word = (e[0] & 0x7fff) | ((e[1] & 0x7fff) << 15);
         return true;
     } else {
         for (int c = 0; c < 3; ++c)
@@ -52,13 +54,60 @@ __device__ __forceinline__ bool pack_offset(const int *e, int &word) {
 template <int D>
 __device__ __forceinline__ void unpack_offset(int word, int *e) {
     if (D == 2) {
-        e[0] = (int)(short)(word & 0xffff);
-        e[1] = word >> 16;
+        e[0] = (word << 17) >> 17;
+        e[1] = (word << 2) >> 17;
     } else {
         e[0] = (word << 22) >> 22;
         e[1] = (word << 12) >> 22;
         e[2] = (word << 2) >> 22;
     }
+}
+
+// Bilevel index of grid point y of instance I (tile shape at run time).
+__device__ __forceinline__ long long bilevel_index_rt(const Inst &I, int D, const int *y) {
+    long long n_o = 0, n_i = 0;
+    for (int k = 0; k < D; ++k) {
+        const int s = I.a.shape_i[k], yo = y[k] / s;
+        n_o = n_o * I.shape_o[k] + yo;
+        n_i = n_i * s + (y[k] - yo * s);
+    }
+    return n_o * I.size_i + n_i;
+}
+
+// Wall distance at grid point y (255 outside the grid, as at padding).
+template <int D, class Index>
+__device__ __forceinline__ int wall_dist_at(const agd_instance &A, const int *y, Index &&index) {
+    bool in = true;
+#pragma unroll
+    for (int c = 0; c < D; ++c) in = in && y[c] >= 0 && y[c] < A.shape[c];
+    return in ? (int)__ldg(A.wall_dist + index(y)) : 255;
+}
+
+// Hidden-neighbour bits (bit s: the neighbour x + (2s - 1) e) of offset e at
+// grid point xt, wd0 the wall distance there (cuda/Walls.h:18-50 for both signs).
+template <int D, class Index>
+__device__ __forceinline__ unsigned hidden_bits(const agd_instance &A, int wd0, const int *xt, const int *e,
+                                                Index &&index) {
+    if (wd0 == 255) return 0u;
+    unsigned h = 0;
+#pragma unroll
+    for (int s = 0; s < 2; ++s) {
+        int v[3] = {0, 0, 0};
+#pragma unroll
+        for (int c = 0; c < D; ++c) v[c] = (2 * s - 1) * e[c];
+        if (!visible<D>(wd0, xt, v, [&](const int *y) { return wall_dist_at<D>(A, y, index); })) h |= 1u << s;
+    }
+    return h;
+}
+
+// Instance of global tile t (binary search over the tile bases).
+__device__ __forceinline__ const Inst &inst_of_tile(const Inst *insts, int ninst, int t) {
+    int lo = 0, hi = ninst - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (insts[mid].tile_base <= t) lo = mid; else hi = mid - 1;
+    }
+    return insts[lo];
 }
 
 // Selling stencil of every point of the Riemann instances of a launch, once per
@@ -78,20 +127,66 @@ __global__ void stencil_kernel(const Inst *insts, int ninst, int total_tiles, Ct
     const Inst &I = insts[lo];
     if (!I.stencil) return;
     const long long base = (long long)(t - I.tile_base) * I.size_i;
+    const float *__restrict__ geom = I.a.geom;
+    float *__restrict__ out = I.stencil;
+    // two points of the lane per step, their loads issued together
+    for (int n0 = lane; n0 < I.size_i; n0 += 64) {
+        float m[2][SD];
+#pragma unroll
+        for (int q = 0; q < 2; ++q)
+#pragma unroll
+            for (int c = 0; c < SD; ++c)
+                m[q][c] = n0 + 32 * q < I.size_i ? __ldg(geom + (size_t)c * I.size_tot + base + n0 + 32 * q) : 1.f;
+#pragma unroll
+        for (int q = 0; q < 2; ++q) {
+            if (n0 + 32 * q >= I.size_i) break;
+            const long long n_t = base + n0 + 32 * q;
+            float w[SD];
+            int e[SD][3];
+            if (D == 2) selling2(m[q], w, e);
+            else selling3(m[q], w, e);
+#pragma unroll
+            for (int r = 0; r < SD; ++r) {
+                int word = 0;
+                if (!pack_offset<D>(e[r], word)) atomicOr(&ctrl->err, (unsigned)AGD_STATUS_UNSUPPORTED);
+                __stcs(out + (size_t)r * I.size_tot + n_t, w[r]);
+                __stcs(out + (size_t)(SD + r) * I.size_tot + n_t, __int_as_float(word));
+            }
+        }
+    }
+}
+
+// Wall visibility of the cached stencils (cuda/FiniteDifferences.h:51-59): for
+// the Riemann instances with walls, the hidden-neighbour bits of every offset,
+// set in its packed word.  Only points within the wall distance bound walk
+// their offsets (Walls.h:18-50).  One warp per tile, after stencil_kernel.
+template <int D>
+__global__ void stencil_walls_kernel(const Inst *insts, int ninst, int total_tiles) {
+    constexpr int SD = D * (D + 1) / 2;
+    const int t = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    const int lane = threadIdx.x & 31;
+    if (t >= total_tiles) return;
+    const Inst &I = inst_of_tile(insts, ninst, t);
+    if (!I.stencil || !I.a.wall_dist) return;
+    const int n_o = t - I.tile_base;
+    const long long base = (long long)n_o * I.size_i;
     for (int n_i = lane; n_i < I.size_i; n_i += 32) {
         const long long n_t = base + n_i;
-        float m[SD], w[SD];
-        int e[SD][3];
-#pragma unroll
-        for (int c = 0; c < SD; ++c) m[c] = __ldg(I.a.geom + (size_t)c * I.size_tot + n_t);
-        if (D == 2) selling2(m, w, e);
-        else selling3(m, w, e);
-#pragma unroll
+        const int wd0 = __ldg(I.a.wall_dist + n_t);  // 255 far from the walls and at padding
+        if (wd0 == 255) continue;
+        int xt[3] = {0, 0, 0}, ro = n_o, ri = n_i;
+        for (int k = D - 1; k >= 0; --k) {
+            xt[k] = (ro % I.shape_o[k]) * I.a.shape_i[k] + ri % I.a.shape_i[k];
+            ro /= I.shape_o[k];
+            ri /= I.a.shape_i[k];
+        }
         for (int r = 0; r < SD; ++r) {
-            int word = 0;
-            if (!pack_offset<D>(e[r], word)) atomicOr(&ctrl->err, (unsigned)AGD_STATUS_UNSUPPORTED);
-            I.stencil[(size_t)r * I.size_tot + n_t] = w[r];
-            I.stencil[(size_t)(SD + r) * I.size_tot + n_t] = __int_as_float(word);
+            float *slot = I.stencil + (size_t)(SD + r) * I.size_tot + n_t;
+            const int word = __float_as_int(*slot);
+            int e[3] = {0, 0, 0};
+            unpack_offset<D>(word, e);
+            const unsigned h = hidden_bits<D>(I.a, wd0, xt, e, [&](const int *y) { return bilevel_index_rt(I, D, y); });
+            if (h) *slot = __int_as_float(word | (int)(h << kHideShift));
         }
     }
 }
@@ -127,7 +222,8 @@ __global__ void mp_copy_kernel(Sched S, int dir) {
 // forces strict_iter_i and strict_iter_o with it (_Kernel.py:39-45).
 // FACT: source factorisation (shifted neighbour values near the seed).
 // ORD2: second order scheme (neighbours two steps away, cuda/HFM.h:91-138).
-template <class TL, int MODEL, bool MP = false, bool FACT = false, bool ORD2 = false>
+// WALLS: neighbours hidden by a wall read +inf (bits of the stencil cache).
+template <class TL, int MODEL, bool MP = false, bool FACT = false, bool ORD2 = false, bool WALLS = false>
 struct Visit {
     static constexpr int D = TL::D, P = TL::P;
     static constexpr int NACT = MODEL == AGD_MODEL_ISOTROPIC ? D : D * (D + 1) / 2;
@@ -210,7 +306,13 @@ struct Visit {
             for (int c = 0; c < SD; ++c) raw[c] = __ldg(I.a.geom + (size_t)c * I.size_tot + n_t);
         }
     }
-    __device__ __forceinline__ static void stencil_decode(const Inst &I, const float *raw, float *w, int (*e)[3]) {
+    // hide[k]: the hidden-neighbour bits of offset k (WALLS: from the cache; else 0).
+    // Isotropic offsets are unit vectors, hidden exactly when the neighbour is a
+    // wall point, whose value is +inf already: no bits are needed.
+    __device__ __forceinline__ static void stencil_decode(const Inst &I, const float *raw, float *w, int (*e)[3],
+                                                          unsigned *hide) {
+#pragma unroll
+        for (int k = 0; k < NACT; ++k) hide[k] = 0u;
         if (MODEL == AGD_MODEL_ISOTROPIC) {
 #pragma unroll
             for (int k = 0; k < D; ++k) {
@@ -223,6 +325,7 @@ struct Visit {
             for (int r = 0; r < SD; ++r) {
                 w[r] = raw[r];
                 unpack_offset<D>(__float_as_int(raw[SD + r]), e[r]);
+                if constexpr (WALLS) hide[r] = (unsigned)__float_as_int(raw[SD + r]) >> kHideShift;
             }
         } else {
             float m[SD];
@@ -235,8 +338,9 @@ struct Visit {
 
     __device__ __forceinline__ static void stencil(const Inst &I, size_t n_t, float *w, int (*e)[3]) {
         float raw[kRaw];
+        unsigned hide[NACT];
         stencil_load(I, n_t, raw);
-        stencil_decode(I, raw, w, e);
+        stencil_decode(I, raw, w, e, hide);
     }
 
     __device__ static void run(const Sched &S, const Inst &I, int ii, int n_o, int e, int lane, float *us) {
@@ -334,16 +438,20 @@ struct Visit {
                 us[n_i] = seed[p] ? rhs[p] : uold[p];
             }
             int ev[NACT][3];
+            unsigned hide[NACT];
             if (seed[p]) continue;  // seeds (and padding) keep their value: no stencil needed
-            stencil_decode(I, raw[p], wts[p], ev);
+            stencil_decode(I, raw[p], wts[p], ev, hide);
             if constexpr (FACT) factor_shifts<D, NACT, MODEL == AGD_MODEL_ISOTROPIC>(A, xt, ev, fsh[p]);
 #pragma unroll
             for (int k = 0; k < NACT; ++k) {
 #pragma unroll
                 for (int s = 0; s < 2; ++s) {
                     const int eps = 2 * s - 1;
+                    // a neighbour hidden by a wall reads +inf, and so does the one after it
+                    // (cuda/FiniteDifferences.h:53-59)
+                    const bool hidden = WALLS && ((hide[k] >> s) & 1u);
                     int yi[3] = {0, 0, 0}, yt[3] = {0, 0, 0};
-                    bool intile = true, indom = true;
+                    bool intile = !hidden, indom = !hidden;
 #pragma unroll
                     for (int c = 0; c < D; ++c) {
                         const int off = eps * ev[k][c];
@@ -370,7 +478,7 @@ struct Visit {
                         nba[p][2 * k + s] = us_addr + 4u * (unsigned)slot;
                     }
                     if constexpr (ORD2) {  // the neighbour x + 2 eps e_k
-                        bool in2 = true, dom2 = true;
+                        bool in2 = !hidden, dom2 = !hidden;
 #pragma unroll
                         for (int c = 0; c < D; ++c) {
                             const int off = 2 * eps * ev[k][c];
@@ -568,13 +676,13 @@ __device__ __forceinline__ void dispatch(const Sched &S, int t, int e, int lane,
             if constexpr ((VMASK >> V_ISO2_16_MP) & 1) Visit<Tile<2, 16, 16, 1>, AGD_MODEL_ISOTROPIC, true>::run(S, I, ii, n_o, e, lane, us);
             break;
         case V_RIEM2_8_MP:
-            if constexpr ((VMASK >> V_RIEM2_8_MP) & 1) Visit<Tile<2, 8, 8, 1>, AGD_MODEL_RIEMANN, true>::run(S, I, ii, n_o, e, lane, us);
+            if constexpr ((VMASK >> V_RIEM2_8_MP) & 1) Visit<Tile<2, 8, 8, 1>, AGD_MODEL_RIEMANN, true, false, false, true>::run(S, I, ii, n_o, e, lane, us);
             break;
         case V_ISO3_4_MP:
             if constexpr ((VMASK >> V_ISO3_4_MP) & 1) Visit<Tile<3, 4, 4, 4>, AGD_MODEL_ISOTROPIC, true>::run(S, I, ii, n_o, e, lane, us);
             break;
         case V_RIEM3_4_MP:
-            if constexpr ((VMASK >> V_RIEM3_4_MP) & 1) Visit<Tile<3, 4, 4, 4>, AGD_MODEL_RIEMANN, true>::run(S, I, ii, n_o, e, lane, us);
+            if constexpr ((VMASK >> V_RIEM3_4_MP) & 1) Visit<Tile<3, 4, 4, 4>, AGD_MODEL_RIEMANN, true, false, false, true>::run(S, I, ii, n_o, e, lane, us);
             break;
         case V_ISO2_8_F:
             if constexpr ((VMASK >> V_ISO2_8_F) & 1) Visit<Tile<2, 8, 8, 1>, AGD_MODEL_ISOTROPIC, false, true>::run(S, I, ii, n_o, e, lane, us);
@@ -583,13 +691,13 @@ __device__ __forceinline__ void dispatch(const Sched &S, int t, int e, int lane,
             if constexpr ((VMASK >> V_ISO2_16_F) & 1) Visit<Tile<2, 16, 16, 1>, AGD_MODEL_ISOTROPIC, false, true>::run(S, I, ii, n_o, e, lane, us);
             break;
         case V_RIEM2_8_F:
-            if constexpr ((VMASK >> V_RIEM2_8_F) & 1) Visit<Tile<2, 8, 8, 1>, AGD_MODEL_RIEMANN, false, true>::run(S, I, ii, n_o, e, lane, us);
+            if constexpr ((VMASK >> V_RIEM2_8_F) & 1) Visit<Tile<2, 8, 8, 1>, AGD_MODEL_RIEMANN, false, true, false, true>::run(S, I, ii, n_o, e, lane, us);
             break;
         case V_ISO3_4_F:
             if constexpr ((VMASK >> V_ISO3_4_F) & 1) Visit<Tile<3, 4, 4, 4>, AGD_MODEL_ISOTROPIC, false, true>::run(S, I, ii, n_o, e, lane, us);
             break;
         case V_RIEM3_4_F:
-            if constexpr ((VMASK >> V_RIEM3_4_F) & 1) Visit<Tile<3, 4, 4, 4>, AGD_MODEL_RIEMANN, false, true>::run(S, I, ii, n_o, e, lane, us);
+            if constexpr ((VMASK >> V_RIEM3_4_F) & 1) Visit<Tile<3, 4, 4, 4>, AGD_MODEL_RIEMANN, false, true, false, true>::run(S, I, ii, n_o, e, lane, us);
             break;
         case V_ISO2_8_O2:
             if constexpr ((VMASK >> V_ISO2_8_O2) & 1) Visit<Tile<2, 8, 8, 1>, AGD_MODEL_ISOTROPIC, false, false, true>::run(S, I, ii, n_o, e, lane, us);
@@ -598,13 +706,22 @@ __device__ __forceinline__ void dispatch(const Sched &S, int t, int e, int lane,
             if constexpr ((VMASK >> V_ISO2_16_O2) & 1) Visit<Tile<2, 16, 16, 1>, AGD_MODEL_ISOTROPIC, false, false, true>::run(S, I, ii, n_o, e, lane, us);
             break;
         case V_RIEM2_8_O2:
-            if constexpr ((VMASK >> V_RIEM2_8_O2) & 1) Visit<Tile<2, 8, 8, 1>, AGD_MODEL_RIEMANN, false, false, true>::run(S, I, ii, n_o, e, lane, us);
+            if constexpr ((VMASK >> V_RIEM2_8_O2) & 1) Visit<Tile<2, 8, 8, 1>, AGD_MODEL_RIEMANN, false, false, true, true>::run(S, I, ii, n_o, e, lane, us);
             break;
         case V_ISO3_4_O2:
             if constexpr ((VMASK >> V_ISO3_4_O2) & 1) Visit<Tile<3, 4, 4, 4>, AGD_MODEL_ISOTROPIC, false, false, true>::run(S, I, ii, n_o, e, lane, us);
             break;
         case V_RIEM3_4_O2:
-            if constexpr ((VMASK >> V_RIEM3_4_O2) & 1) Visit<Tile<3, 4, 4, 4>, AGD_MODEL_RIEMANN, false, false, true>::run(S, I, ii, n_o, e, lane, us);
+            if constexpr ((VMASK >> V_RIEM3_4_O2) & 1) Visit<Tile<3, 4, 4, 4>, AGD_MODEL_RIEMANN, false, false, true, true>::run(S, I, ii, n_o, e, lane, us);
+            break;
+        case V_RIEM2_8_W:
+            if constexpr ((VMASK >> V_RIEM2_8_W) & 1) Visit<Tile<2, 8, 8, 1>, AGD_MODEL_RIEMANN, false, false, false, true>::run(S, I, ii, n_o, e, lane, us);
+            break;
+        case V_RIEM2_16_W:
+            if constexpr ((VMASK >> V_RIEM2_16_W) & 1) Visit<Tile<2, 16, 16, 1>, AGD_MODEL_RIEMANN, false, false, false, true>::run(S, I, ii, n_o, e, lane, us);
+            break;
+        case V_RIEM3_4_W:
+            if constexpr ((VMASK >> V_RIEM3_4_W) & 1) Visit<Tile<3, 4, 4, 4>, AGD_MODEL_RIEMANN, false, false, false, true>::run(S, I, ii, n_o, e, lane, us);
             break;
         default:
             break;
@@ -626,14 +743,17 @@ constexpr int smem_floats() {
     if (VMASK & kMpVariants) m = std::max(m, 2 * kMaxTileSize);
     if ((VMASK >> V_ISO2_8_F) & 1) m = std::max(m, Visit<Tile<2, 8, 8, 1>, AGD_MODEL_ISOTROPIC, false, true>::kSmemFloats);
     if ((VMASK >> V_ISO2_16_F) & 1) m = std::max(m, Visit<Tile<2, 16, 16, 1>, AGD_MODEL_ISOTROPIC, false, true>::kSmemFloats);
-    if ((VMASK >> V_RIEM2_8_F) & 1) m = std::max(m, Visit<Tile<2, 8, 8, 1>, AGD_MODEL_RIEMANN, false, true>::kSmemFloats);
+    if ((VMASK >> V_RIEM2_8_F) & 1) m = std::max(m, Visit<Tile<2, 8, 8, 1>, AGD_MODEL_RIEMANN, false, true, false, true>::kSmemFloats);
     if ((VMASK >> V_ISO3_4_F) & 1) m = std::max(m, Visit<Tile<3, 4, 4, 4>, AGD_MODEL_ISOTROPIC, false, true>::kSmemFloats);
-    if ((VMASK >> V_RIEM3_4_F) & 1) m = std::max(m, Visit<Tile<3, 4, 4, 4>, AGD_MODEL_RIEMANN, false, true>::kSmemFloats);
+    if ((VMASK >> V_RIEM3_4_F) & 1) m = std::max(m, Visit<Tile<3, 4, 4, 4>, AGD_MODEL_RIEMANN, false, true, false, true>::kSmemFloats);
     if ((VMASK >> V_ISO2_8_O2) & 1) m = std::max(m, Visit<Tile<2, 8, 8, 1>, AGD_MODEL_ISOTROPIC, false, false, true>::kSmemFloats);
     if ((VMASK >> V_ISO2_16_O2) & 1) m = std::max(m, Visit<Tile<2, 16, 16, 1>, AGD_MODEL_ISOTROPIC, false, false, true>::kSmemFloats);
-    if ((VMASK >> V_RIEM2_8_O2) & 1) m = std::max(m, Visit<Tile<2, 8, 8, 1>, AGD_MODEL_RIEMANN, false, false, true>::kSmemFloats);
+    if ((VMASK >> V_RIEM2_8_O2) & 1) m = std::max(m, Visit<Tile<2, 8, 8, 1>, AGD_MODEL_RIEMANN, false, false, true, true>::kSmemFloats);
     if ((VMASK >> V_ISO3_4_O2) & 1) m = std::max(m, Visit<Tile<3, 4, 4, 4>, AGD_MODEL_ISOTROPIC, false, false, true>::kSmemFloats);
-    if ((VMASK >> V_RIEM3_4_O2) & 1) m = std::max(m, Visit<Tile<3, 4, 4, 4>, AGD_MODEL_RIEMANN, false, false, true>::kSmemFloats);
+    if ((VMASK >> V_RIEM3_4_O2) & 1) m = std::max(m, Visit<Tile<3, 4, 4, 4>, AGD_MODEL_RIEMANN, false, false, true, true>::kSmemFloats);
+    if ((VMASK >> V_RIEM2_8_W) & 1) m = std::max(m, Visit<Tile<2, 8, 8, 1>, AGD_MODEL_RIEMANN, false, false, false, true>::kSmemFloats);
+    if ((VMASK >> V_RIEM2_16_W) & 1) m = std::max(m, Visit<Tile<2, 16, 16, 1>, AGD_MODEL_RIEMANN, false, false, false, true>::kSmemFloats);
+    if ((VMASK >> V_RIEM3_4_W) & 1) m = std::max(m, Visit<Tile<3, 4, 4, 4>, AGD_MODEL_RIEMANN, false, false, false, true>::kSmemFloats);
     return m;
 }
 
@@ -644,8 +764,9 @@ struct EikonalVisitor {
     // multiprecision an integer part beside every value.
     static constexpr int kMinCtas =
         (VMASK & ((1u << V_RIEM2_16) | (1u << V_ISO2_16) | (1u << V_ISO2_16_MP) | (1u << V_ISO2_16_F) |
-                  (1u << V_ISO2_16_O2)))                                                      ? 4
-        : (VMASK & ((1u << V_RIEM3_4) | (1u << V_RIEM3_4_MP) | (1u << V_RIEM3_4_F) | (1u << V_RIEM3_4_O2))) ? 6
+                  (1u << V_ISO2_16_O2) | (1u << V_RIEM2_16_W)))                                ? 4
+        : (VMASK & ((1u << V_RIEM3_4) | (1u << V_RIEM3_4_MP) | (1u << V_RIEM3_4_F) | (1u << V_RIEM3_4_O2) |
+                    (1u << V_RIEM3_4_W)))                                                     ? 6
         : (VMASK & (kMpVariants | kFactorVariants | kOrder2Variants))                                ? 7
                                                                                                      : 9;
     struct Args {};
@@ -660,13 +781,24 @@ struct EikonalVisitor {
     // the Riemann instances are computed.
     static cudaError_t prepare(const Sched &S, const WsLayout &L, cudaStream_t st) {
         constexpr unsigned kRiemann = (1u << V_RIEM2_8) | (1u << V_RIEM3_4) | (1u << V_RIEM2_16) |
-                                      (1u << V_RIEM2_8_MP) | (1u << V_RIEM3_4_MP);
+                                      (1u << V_RIEM2_8_MP) | (1u << V_RIEM3_4_MP) | (1u << V_RIEM2_8_F) |
+                                      (1u << V_RIEM3_4_F) | (1u << V_RIEM2_8_O2) | (1u << V_RIEM3_4_O2) |
+                                      kWallVariants;
         if (VMASK & kMpVariants) mp_copy_kernel<<<(L.total_tiles + 7) / 8, 256, 0, st>>>(S, 0);
         if (!(VMASK & kRiemann) || L.stencil == L.total) return cudaGetLastError();
-        if (VMASK & ((1u << V_RIEM3_4) | (1u << V_RIEM3_4_MP)))
-            stencil_kernel<3><<<(L.total_tiles + 7) / 8, 256, 0, st>>>(S.inst, S.ninst, L.total_tiles, S.ctrl);
-        else
-            stencil_kernel<2><<<(L.total_tiles + 7) / 8, 256, 0, st>>>(S.inst, S.ninst, L.total_tiles, S.ctrl);
+        // variants that read the hidden-neighbour bits: the walls pass follows
+        constexpr unsigned kWallCapable = kWallVariants | (1u << V_RIEM2_8_MP) | (1u << V_RIEM3_4_MP) |
+                                          (1u << V_RIEM2_8_F) | (1u << V_RIEM3_4_F) | (1u << V_RIEM2_8_O2) |
+                                          (1u << V_RIEM3_4_O2);
+        const unsigned grid = (L.total_tiles + 7) / 8;
+        if (VMASK & ((1u << V_RIEM3_4) | (1u << V_RIEM3_4_MP) | (1u << V_RIEM3_4_F) | (1u << V_RIEM3_4_O2) |
+                     (1u << V_RIEM3_4_W))) {
+            stencil_kernel<3><<<grid, 256, 0, st>>>(S.inst, S.ninst, L.total_tiles, S.ctrl);
+            if (VMASK & kWallCapable) stencil_walls_kernel<3><<<grid, 256, 0, st>>>(S.inst, S.ninst, L.total_tiles);
+        } else {
+            stencil_kernel<2><<<grid, 256, 0, st>>>(S.inst, S.ninst, L.total_tiles, S.ctrl);
+            if (VMASK & kWallCapable) stencil_walls_kernel<2><<<grid, 256, 0, st>>>(S.inst, S.ninst, L.total_tiles);
+        }
         return cudaGetLastError();
     }
     // After the workers: an instance that ran an odd number of epochs has its
@@ -689,7 +821,8 @@ struct agd_plan {
 namespace agd {
 
 // Checks the instances of one launch; returns the mask of tile-visit variants.
-static int validate(const agd_instance *host, const Inst *insts, int n, unsigned *vmask) {
+// stencil_cache: whether the launch computes the Riemann stencil cache.
+static int validate(const agd_instance *host, const Inst *insts, int n, bool stencil_cache, unsigned *vmask) {
     *vmask = 0;
     for (int i = 0; i < n; ++i) {
         const agd_instance &a = host[i];
@@ -701,9 +834,14 @@ static int validate(const agd_instance *host, const Inst *insts, int n, unsigned
             code = AGD_STATUS_UNSUPPORTED;
         }
         else if (insts[i].variant < 0) { bad = "model/tile shape not built"; code = AGD_STATUS_UNSUPPORTED; }
+        else if (a.wall_dist && a.model == AGD_MODEL_RIEMANN && !stencil_cache) {
+            bad = "walls on a Riemann instance need the stencil cache (agd_eikonal_solve)";
+            code = AGD_STATUS_UNSUPPORTED;
+        }
         else if (a.multip_step != 0.f && (!a.valuesq || !a.values_next || !a.valuesq_next || !(a.multip_step > 0.f)))
             bad = "multiprecision needs valuesq, values_next, valuesq_next and multip_step > 0";
         else if (!a.values || !a.rhs || !a.seedbits || (a.model == AGD_MODEL_RIEMANN && !a.geom)) bad = "missing array";
+        else if (reinterpret_cast<uintptr_t>(a.seedbits) % 4 != 0) bad = "seedbits must be 4-byte aligned";
         else if (a.niter_i < 1 || a.fim_front_width < 2 || a.fim_front_width > 255 || a.nitermax_o < 0 ||
                  a.nitermax_o > kMaxEpochs)
             bad = "bad niter_i / fim_front_width / nitermax_o (at most 16000)";
@@ -723,7 +861,7 @@ static int plan_create(const agd_instance *host, int n, agd_plan **out) {
         return set_error(AGD_STATUS_INVALID, "bad instance shape");
     }
     P->ndim = host[0].ndim;
-    const int rc = validate(host, P->insts.data(), n, &P->vmask);
+    const int rc = validate(host, P->insts.data(), n, /*stencil_cache=*/true, &P->vmask);
     if (rc != AGD_STATUS_OK) {
         delete P;
         return rc;
@@ -740,38 +878,41 @@ static int run_variants(int ndim, unsigned vmask, const WsLayout &L, void *ws, i
     constexpr unsigned R3 = 1u << V_RIEM3_4, I3 = 1u << V_ISO3_4, R2L = 1u << V_RIEM2_16;
     constexpr unsigned MP2 = (1u << V_ISO2_8_MP) | (1u << V_ISO2_16_MP) | (1u << V_RIEM2_8_MP);
     constexpr unsigned MP3 = (1u << V_ISO3_4_MP) | (1u << V_RIEM3_4_MP);
+    // Riemann with walls, beside plain instances of every family
+    constexpr unsigned W2 = (1u << V_RIEM2_8_W) | (1u << V_RIEM2_16_W), W3 = 1u << V_RIEM3_4_W;
     if (vmask & kOrder2Variants) {  // second order instances, possibly beside plain ones
         constexpr unsigned O2 = (1u << V_ISO2_8_O2) | (1u << V_ISO2_16_O2) | (1u << V_RIEM2_8_O2);
         constexpr unsigned O3 = (1u << V_ISO3_4_O2) | (1u << V_RIEM3_4_O2);
         if (vmask & (kMpVariants | kFactorVariants))
             return set_error(AGD_STATUS_UNSUPPORTED, "second order beside multiprecision or factorisation in one plan");
-        if (ndim == 2) return run_sched<EikonalVisitor<O2 | R2 | I16 | I8 | R2L>>(L, ws, n, {}, stats, cfg, st);
-        return run_sched<EikonalVisitor<O3 | R3 | I3>>(L, ws, n, {}, stats, cfg, st);
+        if (ndim == 2) return run_sched<EikonalVisitor<O2 | R2 | I16 | I8 | R2L | W2>>(L, ws, n, {}, stats, cfg, st);
+        return run_sched<EikonalVisitor<O3 | R3 | I3 | W3>>(L, ws, n, {}, stats, cfg, st);
     }
     if (vmask & kFactorVariants) {  // factored instances, possibly beside plain ones
         constexpr unsigned F2 = (1u << V_ISO2_8_F) | (1u << V_ISO2_16_F) | (1u << V_RIEM2_8_F);
         constexpr unsigned F3 = (1u << V_ISO3_4_F) | (1u << V_RIEM3_4_F);
         if (vmask & kMpVariants) return set_error(AGD_STATUS_UNSUPPORTED, "factorisation and multiprecision in one plan");
-        if (ndim == 2) return run_sched<EikonalVisitor<F2 | R2 | I16 | I8 | R2L>>(L, ws, n, {}, stats, cfg, st);
-        return run_sched<EikonalVisitor<F3 | R3 | I3>>(L, ws, n, {}, stats, cfg, st);
+        if (ndim == 2) return run_sched<EikonalVisitor<F2 | R2 | I16 | I8 | R2L | W2>>(L, ws, n, {}, stats, cfg, st);
+        return run_sched<EikonalVisitor<F3 | R3 | I3 | W3>>(L, ws, n, {}, stats, cfg, st);
     }
     if (vmask & kMpVariants) {
         if (ndim == 2) {
             if (vmask == (1u << V_RIEM2_8_MP)) return run_sched<EikonalVisitor<(1u << V_RIEM2_8_MP)>>(L, ws, n, {}, stats, cfg, st);
-            return run_sched<EikonalVisitor<R2 | I16 | I8 | R2L | MP2>>(L, ws, n, {}, stats, cfg, st);
+            return run_sched<EikonalVisitor<R2 | I16 | I8 | R2L | MP2 | W2>>(L, ws, n, {}, stats, cfg, st);
         }
-        return run_sched<EikonalVisitor<R3 | I3 | MP3>>(L, ws, n, {}, stats, cfg, st);
+        return run_sched<EikonalVisitor<R3 | I3 | MP3 | W3>>(L, ws, n, {}, stats, cfg, st);
     }
     if (ndim == 2) {
         if (vmask == R2) return run_sched<EikonalVisitor<R2>>(L, ws, n, {}, stats, cfg, st);
         if (vmask == R2L) return run_sched<EikonalVisitor<R2L>>(L, ws, n, {}, stats, cfg, st);
         if (vmask == I16) return run_sched<EikonalVisitor<I16>>(L, ws, n, {}, stats, cfg, st);
         if (vmask == I8) return run_sched<EikonalVisitor<I8>>(L, ws, n, {}, stats, cfg, st);
-        return run_sched<EikonalVisitor<R2 | I16 | I8 | R2L>>(L, ws, n, {}, stats, cfg, st);
+        if (vmask == (1u << V_RIEM2_8_W)) return run_sched<EikonalVisitor<(1u << V_RIEM2_8_W)>>(L, ws, n, {}, stats, cfg, st);
+        return run_sched<EikonalVisitor<R2 | I16 | I8 | R2L | W2>>(L, ws, n, {}, stats, cfg, st);
     }
     if (vmask == R3) return run_sched<EikonalVisitor<R3>>(L, ws, n, {}, stats, cfg, st);
     if (vmask == I3) return run_sched<EikonalVisitor<I3>>(L, ws, n, {}, stats, cfg, st);
-    return run_sched<EikonalVisitor<R3 | I3>>(L, ws, n, {}, stats, cfg, st);
+    return run_sched<EikonalVisitor<R3 | I3 | W3>>(L, ws, n, {}, stats, cfg, st);
 }
 
 static int plan_run(const agd_plan *P, void *ws, size_t ws_bytes, agd_stats *stats, const agd_launch *cfg,
@@ -820,7 +961,7 @@ static int fixed_scratch_solve(const agd_instance *host, int n, agd_stats *stats
     WsLayout L;
     if (!layout(host, n, L, insts, /*stencil_cache=*/false)) return set_error(AGD_STATUS_INVALID, "bad instance shape");
     unsigned vmask = 0;
-    const int rc = validate(host, insts, n, &vmask);
+    const int rc = validate(host, insts, n, /*stencil_cache=*/false, &vmask);
     if (rc != AGD_STATUS_OK) return rc;
     if (L.total > kFixedScratchBytes)
         return set_error(AGD_STATUS_WORKSPACE, "agd_eikonal_solve_fixed_scratch: these instances need more "
@@ -875,6 +1016,11 @@ __global__ void flow_kernel(Inst I, float *fvec, float *fwsum, float *fw, int *f
         float w[NACT], fwk[NACT];
         int ev[NACT][3], side[NACT];
         V::stencil(I, n_t, w, ev);
+        unsigned hide[NACT];  // neighbours hidden by a wall (Riemann offsets; see Visit::stencil_decode)
+        const int wd0 = (MODEL == AGD_MODEL_RIEMANN && A.wall_dist && in) ? (int)__ldg(A.wall_dist + n_t) : 255;
+#pragma unroll
+        for (int k = 0; k < NACT; ++k)
+            hide[k] = hidden_bits<D>(A, wd0, xt, ev[k], [&](const int *y) { return bilevel_index<D, TL>(y, I.shape_o); });
         float v[NACT], fsh[2 * NACT];
         if (A.factor_radius2 > 0.f) {
             factor_shifts<D, NACT, MODEL == AGD_MODEL_ISOTROPIC>(A, xt, ev, fsh);
@@ -889,7 +1035,7 @@ __global__ void flow_kernel(Inst I, float *fvec, float *fwsum, float *fw, int *f
 #pragma unroll
             for (int s = 0; s < 2; ++s) {
                 int y[3] = {0, 0, 0};
-                bool ok = true;
+                bool ok = !((hide[k] >> s) & 1u);
 #pragma unroll
                 for (int c = 0; c < D; ++c) {
                     y[c] = xt[c] + (2 * s - 1) * ev[k][c];
@@ -908,7 +1054,7 @@ __global__ void flow_kernel(Inst I, float *fvec, float *fwsum, float *fw, int *f
             if (A.order2_threshold > 0.f) {  // second order: v corrected in place, weights 9/4
                 o2 = V::order2(__ldg(A.values + n_t), vs, ws, side, [&](int k, int sd) {
                     int y[3] = {0, 0, 0};
-                    bool ok = true;
+                    bool ok = !((hide[k] >> sd) & 1u);
 #pragma unroll
                     for (int c = 0; c < D; ++c) {
                         y[c] = xt[c] + 2 * (2 * sd - 1) * ev[k][c];
@@ -1134,6 +1280,7 @@ __global__ void seeds_kernel(Geo g, const int *idx, const float *vals, int n, fl
 
 struct BatchPrep {
     Geo g;
+    int si_log2[3];  // log2 of the tile sides, or -1 (all) if one is not a power of two
     int n, sd, riemann, is_dual, nseeds;
     float h[3];
     const float *metric, *cost, *seed_values;
@@ -1143,17 +1290,52 @@ struct BatchPrep {
     int *bad;
 };
 
-// One thread per point of every instance (grid-stride; warps stay 32-aligned
-// because size_tot is a multiple of 32, so each warp's ballot is one bit word).
+// Bilevel index -> grid coordinates for instances of fewer than 2^31 points,
+// in 32-bit arithmetic, the in-tile part by shifts when the tile sides are
+// powers of two (si_log2 >= 0).  Returns false for padding.
+__device__ __forceinline__ bool grid_coords32(const Geo &g, const int *si_log2, int n_t, int &flat) {
+    int n_o, n_i, xo[3], xi[3];
+    if (si_log2[0] >= 0) {
+        const int lsz = si_log2[0] + si_log2[1] + si_log2[2];
+        n_o = n_t >> lsz;
+        n_i = n_t & ((1 << lsz) - 1);
+        for (int k = g.nd - 1; k >= 0; --k) {
+            xi[k] = n_i & ((1 << si_log2[k]) - 1);
+            n_i >>= si_log2[k];
+        }
+    } else {
+        n_o = n_t / g.size_i;
+        n_i = n_t - n_o * g.size_i;
+        for (int k = g.nd - 1; k >= 0; --k) {
+            xi[k] = n_i % g.si[k];
+            n_i /= g.si[k];
+        }
+    }
+    for (int k = g.nd - 1; k >= 0; --k) {
+        const int q = n_o / g.so[k];
+        xo[k] = n_o - q * g.so[k];
+        n_o = q;
+    }
+    bool in = true;
+    flat = 0;
+    for (int k = 0; k < g.nd; ++k) {
+        const int x = xo[k] * g.si[k] + xi[k];
+        in = in && x < g.shape[k];
+        flat = flat * g.shape[k] + x;
+    }
+    return in;
+}
+
+// Grid rows of blocks: blockIdx.y is the instance, the blocks of a row stride
+// over its points (warps stay 32-aligned because size_tot is a multiple of 32,
+// so each warp's ballot is one bit word).
 __global__ void prep_batch_kernel(BatchPrep A) {
-    const long long total = A.g.size_tot * A.n;
-    const long long stride = (long long)gridDim.x * blockDim.x;
-    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total; i += stride) {
-        const int inst = (int)(i / A.g.size_tot);
-        const long long n_t = i - inst * A.g.size_tot;
-        int x[3];
-        long long flat;
-        const bool in = grid_coords(A.g, n_t, x, flat);
+    const int inst = blockIdx.y;
+    const int size_tot = (int)A.g.size_tot;
+    for (int n_t = blockIdx.x * blockDim.x + threadIdx.x; n_t < size_tot; n_t += gridDim.x * blockDim.x) {
+        const long long i = (long long)inst * size_tot + n_t;
+        int flat;
+        const bool in = grid_coords32(A.g, A.si_log2, n_t, flat);
         A.values[i] = finf();
         A.rhs[i] = in ? (A.cost ? A.cost[inst * A.g.n + flat] : 1.f) : finf();
         if (A.riemann) {
@@ -1173,6 +1355,24 @@ __global__ void seeds_batch_kernel(BatchPrep A) {
     place_seeds(A.g, A.seed_index + (long long)inst * A.nseeds * A.g.nd,
                 A.seed_values ? A.seed_values + (long long)inst * A.nseeds : nullptr, A.nseeds,
                 A.rhs + inst * A.g.size_tot, A.bits + inst * (A.g.size_tot / 32), nullptr, A.bad);
+}
+
+// Wall distances in tile layout (255 at padding); with rhs / bits, the wall
+// points become seeds of value +inf (_SetArgs.py:124-126).  One thread per
+// point; whole warps leave together (size_tot is a multiple of 32), and the
+// wall bits of a warp are one seed-bit word, which only that warp writes.
+__global__ void walls_kernel(Geo g, const uint8_t *walls, const uint8_t *dist, uint8_t *wall_dist, float *rhs,
+                             unsigned *bits) {
+    const long long n_t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (n_t >= g.size_tot) return;
+    int x[3];
+    long long flat;
+    const bool in = grid_coords(g, n_t, x, flat);
+    const bool wall = in && walls[flat] != 0;
+    wall_dist[n_t] = in ? dist[flat] : (uint8_t)255;
+    if (wall && rhs) rhs[n_t] = finf();
+    const unsigned word = __ballot_sync(kFull, wall);
+    if (bits && word && (threadIdx.x & 31) == 0) bits[n_t >> 5] |= word;
 }
 
 __global__ void selling_kernel(int nd, const float *m, int n, float *w, int *e) {
@@ -1332,13 +1532,41 @@ int agd_prep_batch(const agd_batch_prep *p, agd_stream_t stream) {
     A.values = p->values;
     A.bits = reinterpret_cast<unsigned *>(p->seedbits);
     A.bad = p->bad_seed;
+    if (g.size_tot >= (1ll << 31) || p->n > 65535)
+        return set_error(AGD_STATUS_INVALID, "agd_prep_batch: at most 65535 instances of fewer than 2^31 points");
+    bool pow2 = true;
+    for (int k = 0; k < 3; ++k) {
+        int l = 0;
+        while ((1 << l) < g.si[k]) ++l;
+        A.si_log2[k] = l;
+        pow2 = pow2 && (1 << l) == g.si[k];
+    }
+    if (!pow2) A.si_log2[0] = A.si_log2[1] = A.si_log2[2] = -1;
     cudaStream_t st = (cudaStream_t)stream;
-    const long long total = g.size_tot * p->n;
-    const unsigned blocks = (unsigned)std::min<long long>((total + 255) / 256, 148LL * 16);
-    prep_batch_kernel<<<blocks, 256, 0, st>>>(A);
+    // about 16 resident 256-thread blocks per SM over all the instances
+    const long long per_inst = std::max<long long>(1, 148LL * 16 / p->n);
+    const dim3 grid((unsigned)std::min<long long>((g.size_tot + 255) / 256, per_inst), (unsigned)p->n);
+    prep_batch_kernel<<<grid, 256, 0, st>>>(A);
     if (p->nseeds > 0) seeds_batch_kernel<<<blocks_for(p->n, 128), 128, 0, st>>>(A);
     const cudaError_t err = cudaGetLastError();
     return err == cudaSuccess ? AGD_STATUS_OK : set_cuda_error("prep_batch", err);
+}
+
+int agd_prep_walls(int ndim, const int *shape, const int *shape_i, const uint8_t *walls, int bound, uint8_t *wall_dist,
+                   uint8_t *tmp, float *rhs, uint8_t *seedbits, agd_stream_t stream) {
+    clear_error();
+    Geo g;
+    if ((ndim != 2 && ndim != 3) || !shape || !shape_i || !geo_of(ndim, shape, shape_i, g) || (g.size_tot % 32) != 0 ||
+        !walls || !wall_dist || !tmp || bound < 0 || bound > 254)
+        return set_error(AGD_STATUS_INVALID, "agd_prep_walls: bad arguments (bound in [0, 254])");
+    cudaStream_t st = (cudaStream_t)stream;
+    // _SetGeometry.py:271-277: 0 at walls, `bound` passes of the L1 kernel, cut beyond `bound`
+    const int rc = distance_map(ndim, shape, walls, bound, bound, true, tmp, tmp + g.n, st);
+    if (rc != AGD_STATUS_OK) return rc;
+    walls_kernel<<<(unsigned)((g.size_tot + 255) / 256), 256, 0, st>>>(g, walls, tmp, wall_dist, rhs,
+                                                                       reinterpret_cast<unsigned *>(seedbits));
+    const cudaError_t err = cudaGetLastError();
+    return err == cudaSuccess ? AGD_STATUS_OK : set_cuda_error("prep_walls", err);
 }
 
 int agd_selling(int ndim, const float *m, int n, float *weights, int32_t *offsets, agd_stream_t stream) {

@@ -25,8 +25,9 @@ struct EGeo {
 };
 
 // One min-plus pass: out(x) = min over the 3^d neighbours y of min(255, in(y) + k(y - x)),
-// k = round(5 |y - x|) (inf_convolution with distance_kernel(1, ndim, uint8, mult=5)).
-__global__ void infconv_kernel(EGeo g, const uint8_t *in, uint8_t *out) {
+// k = round(5 |y - x|) (inf_convolution with distance_kernel(1, ndim, uint8, mult=5)),
+// or with l1, k = |y - x|_1 (distance_kernel(1, ndim, uint8, ord=1)).
+__global__ void infconv_kernel(EGeo g, const uint8_t *in, int l1, uint8_t *out) {
     const long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (p >= g.n) return;
     int x[3] = {0, 0, 0};
@@ -47,7 +48,8 @@ __global__ void infconv_kernel(EGeo g, const uint8_t *in, uint8_t *out) {
         if (!ok) continue;
         long long m = 0;
         for (int k = 0; k < g.nd; ++k) m = m * g.shape[k] + y[k];
-        const int kv = n2 == 0 ? 0 : (n2 == 1 ? 5 : (n2 == 2 ? 7 : 9));  // round(5 sqrt(n2))
+        // offsets in {-1, 0, 1}^d: |o|_1 = |o|^2; round(5 |o|) = 0, 5, 7, 9
+        const int kv = l1 ? n2 : (n2 == 0 ? 0 : (n2 == 1 ? 5 : (n2 == 2 ? 7 : 9)));
         const int a = in[m];
         best = min(best, (a >= 255 - kv) ? 255 : a + kv);
     }
@@ -232,6 +234,35 @@ __global__ void geodesic_kernel(GeoArgs A) {
 
 static inline unsigned nblocks(long long n, int bs) { return (unsigned)((n + bs - 1) / bs); }
 
+// Min-plus distance map in grid layout: 0 at the mask points, 255 elsewhere,
+// then `npasses` passes of infconv_kernel and values above `cut` set to 255.
+// tmp: scratch of prod(shape) bytes.
+int distance_map(int ndim, const int *shape, const uint8_t *mask, int npasses, int cut, bool l1, uint8_t *out,
+                 uint8_t *tmp, cudaStream_t st) {
+    if ((ndim != 2 && ndim != 3) || !shape || !mask || !out || !tmp || npasses < 0)
+        return set_error(AGD_STATUS_INVALID, "distance map: bad arguments");
+    EGeo g;
+    g.nd = ndim;
+    g.n = 1;
+    for (int k = 0; k < 3; ++k) g.shape[k] = 1;
+    for (int k = 0; k < ndim; ++k) {
+        if (shape[k] <= 0) return set_error(AGD_STATUS_INVALID, "distance map: bad shape");
+        g.shape[k] = shape[k];
+        g.n *= shape[k];
+    }
+    const int bs = 256;
+    uint8_t *a = out, *b = tmp;
+    eucl_init_kernel<<<nblocks(g.n, bs), bs, 0, st>>>(g, mask, a);
+    for (int it = 0; it < npasses; ++it) {
+        infconv_kernel<<<nblocks(g.n, bs), bs, 0, st>>>(g, a, l1 ? 1 : 0, b);
+        uint8_t *t = a; a = b; b = t;
+    }
+    eucl_cut_kernel<<<nblocks(g.n, bs), bs, 0, st>>>(g, a, cut, b);
+    if (b != out) cudaMemcpyAsync(out, b, (size_t)g.n, cudaMemcpyDeviceToDevice, st);
+    const cudaError_t err = cudaGetLastError();
+    return err == cudaSuccess ? AGD_STATUS_OK : set_cuda_error("distance map", err);
+}
+
 }  // namespace agd
 
 using namespace agd;
@@ -241,29 +272,7 @@ extern "C" {
 int agd_eucl_map(int ndim, const int *shape, const uint8_t *seed_mask, int npasses, int cut, uint8_t *eucl,
                  uint8_t *tmp, agd_stream_t stream) {
     clear_error();
-    if ((ndim != 2 && ndim != 3) || !shape || !seed_mask || !eucl || !tmp || npasses < 0)
-        return set_error(AGD_STATUS_INVALID, "agd_eucl_map: bad arguments");
-    EGeo g;
-    g.nd = ndim;
-    g.n = 1;
-    for (int k = 0; k < 3; ++k) g.shape[k] = 1;
-    for (int k = 0; k < ndim; ++k) {
-        if (shape[k] <= 0) return set_error(AGD_STATUS_INVALID, "agd_eucl_map: bad shape");
-        g.shape[k] = shape[k];
-        g.n *= shape[k];
-    }
-    cudaStream_t st = (cudaStream_t)stream;
-    const int bs = 256;
-    uint8_t *a = eucl, *b = tmp;
-    eucl_init_kernel<<<nblocks(g.n, bs), bs, 0, st>>>(g, seed_mask, a);
-    for (int it = 0; it < npasses; ++it) {
-        infconv_kernel<<<nblocks(g.n, bs), bs, 0, st>>>(g, a, b);
-        uint8_t *t = a; a = b; b = t;
-    }
-    eucl_cut_kernel<<<nblocks(g.n, bs), bs, 0, st>>>(g, a, cut, b);
-    if (b != eucl) cudaMemcpyAsync(eucl, b, (size_t)g.n, cudaMemcpyDeviceToDevice, st);
-    const cudaError_t err = cudaGetLastError();
-    return err == cudaSuccess ? AGD_STATUS_OK : set_cuda_error("eucl_map", err);
+    return distance_map(ndim, shape, seed_mask, npasses, cut, false, eucl, tmp, (cudaStream_t)stream);
 }
 
 int agd_geodesics(const agd_instance *inst, const float *flow_vector, const float *flow_weightsum, const uint8_t *eucl,

@@ -21,7 +21,10 @@ enum Variant {
     // source factorisation
     V_ISO2_8_F, V_ISO2_16_F, V_RIEM2_8_F, V_ISO3_4_F, V_RIEM3_4_F,
     // second order scheme
-    V_ISO2_8_O2, V_ISO2_16_O2, V_RIEM2_8_O2, V_ISO3_4_O2, V_RIEM3_4_O2, V_COUNT
+    V_ISO2_8_O2, V_ISO2_16_O2, V_RIEM2_8_O2, V_ISO3_4_O2, V_RIEM3_4_O2,
+    // walls (Riemann; the Riemann variants above with multiprecision, factorisation
+    // or second order read the wall bits themselves; Isotropic needs none)
+    V_RIEM2_8_W, V_RIEM2_16_W, V_RIEM3_4_W, V_COUNT
 };
 constexpr unsigned kMpVariants = (1u << V_ISO2_8_MP) | (1u << V_ISO2_16_MP) | (1u << V_RIEM2_8_MP) |
                                  (1u << V_ISO3_4_MP) | (1u << V_RIEM3_4_MP);
@@ -29,6 +32,7 @@ constexpr unsigned kFactorVariants = (1u << V_ISO2_8_F) | (1u << V_ISO2_16_F) | 
                                      (1u << V_ISO3_4_F) | (1u << V_RIEM3_4_F);
 constexpr unsigned kOrder2Variants = (1u << V_ISO2_8_O2) | (1u << V_ISO2_16_O2) | (1u << V_RIEM2_8_O2) |
                                      (1u << V_ISO3_4_O2) | (1u << V_RIEM3_4_O2);
+constexpr unsigned kWallVariants = (1u << V_RIEM2_8_W) | (1u << V_RIEM2_16_W) | (1u << V_RIEM3_4_W);
 
 static int base_variant_of(const agd_instance &a);
 
@@ -56,7 +60,18 @@ static int variant_of(const agd_instance &a) {
             default: return -1;
         }
     }
-    if (v < 0 || a.multip_step == 0.f) return v;
+    if (v < 0) return v;
+    if (a.multip_step == 0.f) {
+        if (a.wall_dist && a.model == AGD_MODEL_RIEMANN) {
+            switch (v) {
+                case V_RIEM2_8: return V_RIEM2_8_W;
+                case V_RIEM2_16: return V_RIEM2_16_W;
+                case V_RIEM3_4: return V_RIEM3_4_W;
+                default: return -1;
+            }
+        }
+        return v;
+    }
     switch (v) {
         case V_ISO2_8: return V_ISO2_8_MP;
         case V_ISO2_16: return V_ISO2_16_MP;
@@ -123,8 +138,9 @@ static bool layout(const agd_instance *a, int n, WsLayout &L, Inst *out, bool st
         I.tile_base = (int)tiles;
         I.variant = variant_of(a[i]);
         I.stencil = nullptr;
+        I.stencil_off = -1;
         if (stencil_cache && a[i].model == AGD_MODEL_RIEMANN) {
-            I.stencil = reinterpret_cast<float *>(stencil_floats);  // offset, rebased once the workspace is known
+            I.stencil_off = stencil_floats;  // the pointer is set once the workspace is known
             stencil_floats += 2ll * (a[i].ndim * (a[i].ndim + 1) / 2) * I.size_tot;
         }
         tiles += I.size_o;
@@ -158,12 +174,14 @@ static bool layout(const agd_instance *a, int n, WsLayout &L, std::vector<Inst> 
     return layout(a, n, L, out ? out->data() : static_cast<Inst *>(nullptr), stencil_cache);
 }
 
-// Rebases the stencil offsets recorded by layout() onto the workspace address.
+// Points the stencils of the instances at their offsets, recorded by layout(),
+// in the workspace's stencil region.
 static void rebase_stencils(Inst *insts, int n, const WsLayout &L, void *ws) {
     for (int i = 0; i < n; ++i)
-        if (insts[i].stencil)
-            insts[i].stencil = reinterpret_cast<float *>(static_cast<char *>(ws) + L.stencil +
-                                                          reinterpret_cast<size_t>(insts[i].stencil) * sizeof(float));
+        insts[i].stencil = insts[i].stencil_off < 0
+                               ? nullptr
+                               : reinterpret_cast<float *>(static_cast<char *>(ws) + L.stencil +
+                                                           (size_t)insts[i].stencil_off * sizeof(float));
 }
 
 // --------------------------------------------------------- kernel context ---
@@ -407,9 +425,12 @@ __global__ void __launch_bounds__(WPB * 32, Visitor::kMinCtas * 4 / WPB) sched_w
 // tile -> instance map and epoch-1 lists: tiles flagged by `trigger`, by
 // ACTIVATE_ALL, or holding a seed point inside the domain (the reference's
 // trigger = seedTags, _SetArgs.py:122 and _solvers.py:98-100).
-static __global__ void setup_tiles(Sched S) {
-    const int t = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
-    const int lane = threadIdx.x & 31;
+// One thread per tile.  The seed bits of a tile are size_i / 32 consecutive
+// words; padding bits are set, so a tile that reaches past the grid tests its
+// points one by one, the others OR their words.
+static __global__ void setup_tiles(Sched S, int total_tiles) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= total_tiles) return;
     int lo = 0, hi = S.ninst - 1;  // bisection over the tile bases
     while (lo < hi) {
         const int mid = (lo + hi + 1) >> 1;
@@ -418,25 +439,36 @@ static __global__ void setup_tiles(Sched S) {
     const Inst &I = S.inst[lo];
     if (t >= I.tile_base + I.size_o) return;  // past the last tile
     const int n_o = t - I.tile_base;
-    if (lane == 0) const_cast<int *>(S.tile_inst)[t] = lo;
+    const_cast<int *>(S.tile_inst)[t] = lo;
     bool active = (I.a.flags & AGD_FLAG_ACTIVATE_ALL) != 0;
     if (I.a.trigger) {
         active = active || I.a.trigger[n_o] != 0;
     } else if (!active) {
-        int xo[3], r = n_o;
-        for (int k = I.a.ndim - 1; k >= 0; --k) { xo[k] = r % I.shape_o[k]; r /= I.shape_o[k]; }
-        bool any = false;
-        for (int n_i = lane; n_i < I.size_i; n_i += 32) {
-            int xi[3], q = n_i;
-            for (int k = I.a.ndim - 1; k >= 0; --k) { xi[k] = q % I.a.shape_i[k]; q /= I.a.shape_i[k]; }
-            bool in = true;
-            for (int k = 0; k < I.a.ndim; ++k) in = in && (xo[k] * I.a.shape_i[k] + xi[k] < I.a.shape[k]);
-            const size_t n_t = (size_t)n_o * I.size_i + n_i;
-            if (in && ((I.a.seedbits[n_t >> 3] >> (n_t & 7)) & 1)) any = true;
+        int xo[3] = {0, 0, 0}, r = n_o;
+        bool padded = false;
+        for (int k = I.a.ndim - 1; k >= 0; --k) {
+            xo[k] = r % I.shape_o[k];
+            r /= I.shape_o[k];
+            padded = padded || (xo[k] + 1) * I.a.shape_i[k] > I.a.shape[k];
         }
-        active = __any_sync(kFull, any);
+        const unsigned *bits = reinterpret_cast<const unsigned *>(I.a.seedbits) + (size_t)n_o * (I.size_i >> 5);
+        if (!padded) {
+            unsigned any = 0;
+            for (int j = 0; j < (I.size_i >> 5); ++j) any |= __ldg(bits + j);
+            active = any != 0;
+        } else {
+            for (int n_i = 0; n_i < I.size_i && !active; ++n_i) {
+                int q = n_i;
+                bool in = true;
+                for (int k = I.a.ndim - 1; k >= 0; --k) {
+                    in = in && xo[k] * I.a.shape_i[k] + q % I.a.shape_i[k] < I.a.shape[k];
+                    q /= I.a.shape_i[k];
+                }
+                active = in && ((__ldg(bits + (n_i >> 5)) >> (n_i & 31)) & 1u);
+            }
+        }
     }
-    if (active && lane == 0) {
+    if (active) {
         S.flags[t] = 1u;
         const unsigned idx = atomicAdd(&S.ist[lo].cnt[1], 1u);
         S.list1[I.tile_base + idx] = t;
@@ -532,10 +564,11 @@ static int run_sched(const WsLayout &L, void *ws, int n, const typename Visitor:
     cudaError_t err = cudaMemsetAsync(w + L.istate, 0, sizeof(InstState) * n, st);
     if (err == cudaSuccess) err = cudaMemsetAsync(w + L.flags, 0, L.queue - L.flags, st);
     if (err == cudaSuccess) err = cudaMemsetAsync(w + L.queue, 0xff, L.ctrl - L.queue, st);
-    if (err == cudaSuccess) err = cudaMemsetAsync(w + L.ctrl, 0, L.total - L.ctrl, st);
+    // control block and stats; the stencil region after them is written in full by the stencil pass
+    if (err == cudaSuccess) err = cudaMemsetAsync(w + L.ctrl, 0, L.stencil - L.ctrl, st);
     if (err != cudaSuccess) return set_cuda_error("workspace clear", err);
     if ((err = Visitor::prepare(S, L, st)) != cudaSuccess) return set_cuda_error("prepare", err);
-    setup_tiles<<<(L.total_tiles + 7) / 8, 256, 0, st>>>(S);
+    setup_tiles<<<(L.total_tiles + 255) / 256, 256, 0, st>>>(S, L.total_tiles);
     if ((err = cudaGetLastError()) != cudaSuccess) return set_cuda_error("setup_tiles", err);
     publish_first<<<(n + 7) / 8, 256, 0, st>>>(S);
     if ((err = cudaGetLastError()) != cudaSuccess) return set_cuda_error("publish_first", err);

@@ -64,7 +64,8 @@ typedef struct agd_instance {
     int32_t *valuesq_next; /*  iterations (valuesNext, valuesqNext of _SetArgs.py:171-177) */
     const float *geom;  /* Riemann: dual metric, symdim planes, tile layout (else NULL) */
     const float *rhs;   /* tile layout: cost, seed values at seeds, +inf padding */
-    const uint8_t *seedbits; /* tile layout bits, little endian, padding bits set */
+    const uint8_t *seedbits; /* tile layout bits, little endian, padding bits set;
+                                4-byte aligned */
     const uint8_t *trigger;  /* per tile, nonzero = active at the first iteration
                                 (NULL: tiles holding a seed) */
     /* Source factorisation (factoringRadius; _Kernel.py:47-49, 301-308,
@@ -82,6 +83,14 @@ typedef struct agd_instance {
      * second order (order2_threshold, default 0.3).  0: first order.  Not with
      * multiprecision or source factorisation. */
     float order2_threshold;
+    /* Obstacles (walls; cuda/Walls.h:18-50, _SetGeometry.py:262-280): L1 distance
+     * to the nearest wall point in tile layout, uint8, 255 beyond wallDistBound
+     * and at padding (agd_prep_walls writes it).  A stencil offset whose segment
+     * meets a wall has an infinite neighbour value.  The wall points themselves
+     * are seeds of value +inf.  NULL: no walls.  Riemann instances with walls
+     * need the stencil cache of agd_eikonal_solve / agd_plan_run (the fixed
+     * scratch entry point refuses them). */
+    const uint8_t *wall_dist;
 } agd_instance;
 
 #define AGD_FLAG_ACTIVATE_ALL 1 /* every tile is active at the first iteration */
@@ -213,6 +222,17 @@ typedef struct agd_batch_prep {
 
 int agd_prep_batch(const agd_batch_prep *prep, agd_stream_t stream);
 
+/* Obstacles: from the wall mask (grid layout uint8, nonzero = wall) writes
+ * wall_dist (tile layout, size_tot bytes): the L1 distance to the nearest wall
+ * point, by `bound` min-plus passes of the 3^ndim L1 kernel (inf_convolution
+ * with distance_kernel(1, ndim, uint8, ord=1), saturated at 255), 255 beyond
+ * `bound` and at padding (_SetGeometry.py:262-280).  If rhs / seedbits are not
+ * NULL, the wall points become seeds of value +inf there (_SetArgs.py:124-126):
+ * call it after agd_prep_seeds, walls override seeds.  tmp: 2 * prod(shape)
+ * bytes of scratch. */
+int agd_prep_walls(int ndim, const int *shape, const int *shape_i, const uint8_t *walls, int bound,
+                   uint8_t *wall_dist, uint8_t *tmp, float *rhs, uint8_t *seedbits, agd_stream_t stream);
+
 /* Selling decomposition of n packed symmetric matrices (symdim floats each):
  * weights (n, symdim), integer offsets (n, symdim, ndim).  Same decomposition
  * as the kernel's decomp_m (cuda/Geometry2.h:21-48, Geometry3.h:22-58). */
@@ -281,7 +301,7 @@ int agd_forward(const agd_instance *inst, const float *flow_weights, const int32
 /* ------------------------------------------------------------------- misc -- */
 
 const char *agd_last_error(void);
-int agd_version(void); /* 2: agd_instance with the source factorisation and second order fields */
+int agd_version(void); /* 3: agd_instance with the factorisation, second order and wall fields */
 
 #if defined(__GNUC__)
 #pragma GCC visibility pop

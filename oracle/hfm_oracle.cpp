@@ -20,6 +20,7 @@
 //   forward AD linear system     _PostProcess.py:181-191 (ordered sweeps)
 //   source factorisation         cuda/EuclideanFactor.h:8-26, FiniteDifferences.h:30-75
 //   second order scheme          cuda/HFM.h:91-138 (HFMNeighbors), 175-206 (weights)
+//   wall visibility              cuda/Walls.h:12-50, FiniteDifferences.h:51-59
 //
 // Arrays passed to this library are in plain row-major grid layout (not the
 // bilevel tile layout of the GPU kernels).  The tile structure is used only to
@@ -145,6 +146,36 @@ struct Problem {
     T fact_r2 = 0, fact_origin[3] = {0, 0, 0}, fact_m[6] = {0, 0, 0, 0, 0, 0};
     // Second order scheme (order: 2): threshold on |u - 2v + v2| / max(u - v); 0: off.
     T order2 = 0;
+    // Walls: L1 distance to the nearest wall point (grid layout), 255 beyond the
+    // bound; null: no walls.  A neighbour x + v with [x, x + v] blocked by a wall
+    // has value +inf (and so has x + 2v at second order).
+    const unsigned char *wall_dist = nullptr;
+
+    int wdist(const int *y) const { return inside(y) ? int(wall_dist[flat(y)]) : 255; }
+    // Whether the segment [x, x + v] meets no wall (Walls.h:18-50): clear far from
+    // the walls or for |v|_1 below the wall distance at x; else walk the lattice
+    // points round(k v / |v|_inf), k = 1..|v|_inf, rounding halves away from 0.
+    bool visible(const int *x, const int *v) const {
+        if (!wall_dist) return true;
+        const int d0 = wdist(x);
+        if (d0 == 255) return true;
+        int l1 = 0, linf = 0;
+        for (int c = 0; c < D; ++c) { l1 += std::abs(v[c]); linf = std::max(linf, std::abs(v[c])); }
+        if (l1 < d0) return true;
+        for (int k = 1; k <= linf; ++k) {
+            int y[3], rest = 0;
+            for (int c = 0; c < D; ++c) {
+                const int num = v[c] * k;  // round(num / linf), halves away from zero
+                const int w = num >= 0 ? (num + linf / 2) / linf : -((-num + linf / 2) / linf);
+                rest += std::abs(v[c] - w);
+                y[c] = x[c] + w;
+            }
+            const int d = wdist(y);
+            if (rest < d) return true;
+            if (d == 0) return false;
+        }
+        return true;
+    }
 
     T scal_fact(const T *x, const T *y) const {
         if (model == 0) {
@@ -331,12 +362,18 @@ struct Solver {
             for (int k = 0; k < NA; ++k)
                 for (int s = 0; s < 2; ++s) {
                     const int ks = 2 * k + s, eps = 2 * s - 1;
-                    int yi[3], yt[3];
+                    int yi[3], yt[3], off[3] = {0, 0, 0};
                     bool intile = true;
                     for (int c = 0; c < D; ++c) {
-                        yi[c] = xi[n * 3 + c] + eps * e[k][c];
-                        yt[c] = xt[n * 3 + c] + eps * e[k][c];
+                        off[c] = eps * e[k][c];
+                        yi[c] = xi[n * 3 + c] + off[c];
+                        yt[c] = xt[n * 3 + c] + off[c];
                         if (yi[c] < 0 || yi[c] >= P.shape_i[c]) intile = false;
+                    }
+                    if (!seed[n] && !P.visible(xt.data() + n * 3, off)) {  // hidden by a wall
+                        vi[n * 12 + ks] = vi2[n * 12 + ks] = -1;
+                        vo[n * 12 + ks] = vo2[n * 12 + ks] = inf<T>();
+                        continue;
                     }
                     if (intile) {
                         int li = 0;
@@ -490,11 +527,14 @@ struct Solver {
                 P.stencil(p, wts, e);
                 T v[6], sh[12];
                 P.shifts(x, e, sh);
+                bool hid[12];
                 for (int k = 0; k < NA; ++k) {
                     for (int s = 0; s < 2; ++s) {
-                        int y[3];
-                        for (int c = 0; c < D; ++c) y[c] = x[c] + (2 * s - 1) * e[k][c];
-                        const T val = (P.inside(y) ? u[P.flat(y)] : inf<T>()) + sh[2 * k + s];
+                        int y[3], off[3] = {0, 0, 0};
+                        for (int c = 0; c < D; ++c) off[c] = (2 * s - 1) * e[k][c];
+                        for (int c = 0; c < D; ++c) y[c] = x[c] + off[c];
+                        hid[2 * k + s] = !P.visible(x, off);
+                        const T val = (!hid[2 * k + s] && P.inside(y) ? u[P.flat(y)] : inf<T>()) + sh[2 * k + s];
                         if (s == 0) { v[k] = val; side[k] = 0; }
                         else if (v[k] > val) { v[k] = val; side[k] = 1; }
                     }
@@ -507,7 +547,7 @@ struct Solver {
                     for (int k = 0; k < NA; ++k) {
                         int y[3];
                         for (int c = 0; c < D; ++c) y[c] = x[c] + 2 * (2 * side[k] - 1) * e[k][c];
-                        v2[k] = P.inside(y) ? u[P.flat(y)] : inf<T>();
+                        v2[k] = !hid[2 * k + side[k]] && P.inside(y) ? u[P.flat(y)] : inf<T>();
                     }
                     order2_correct<T>(u[p], v, v2, NA, P.order2, o2);
                     for (int k = 0; k < NA; ++k)
@@ -712,6 +752,7 @@ void fill_problem(Problem<T> &P, int ndim, int model, const int *shape, const in
 // Source factorisation of the next solves (agdo_set_factor).
 double g_fact_r2 = 0, g_fact_origin[3] = {0, 0, 0}, g_fact_m[6] = {0, 0, 0, 0, 0, 0};
 double g_order2 = 0;
+const unsigned char *g_wall_dist = nullptr;  // walls of the next solves (agdo_set_walls)
 
 template <class T>
 int eikonal_impl(int ndim, int model, const int *shape, const int *shape_i, int niter_i, int front,
@@ -724,14 +765,15 @@ int eikonal_impl(int ndim, int model, const int *shape, const int *shape_i, int 
     for (int c = 0; c < 3; ++c) S.P.fact_origin[c] = T(g_fact_origin[c]);
     for (int c = 0; c < 6; ++c) S.P.fact_m[c] = T(g_fact_m[c]);
     S.P.order2 = T(g_order2);
+    S.P.wall_dist = g_wall_dist;
     S.u.assign(values, values + S.P.size);
     S.atol = T(atol);
     S.rtol = T(rtol);
     S.niter_i = niter_i;
     S.front = front;
     std::vector<unsigned char> trig(S.P.size_o, 0);
-    for (long p = 0; p < S.P.size; ++p) {
-        if (!seed[p]) continue;
+    for (long p = 0; p < S.P.size; ++p) {  // the tiles of the seeds, walls excluded (_SetArgs.py:119-126)
+        if (!seed[p] || (g_wall_dist && g_wall_dist[p] == 0)) continue;
         int x[3], n_o = 0;
         long q = p;
         for (int k = ndim - 1; k >= 0; --k) { x[k] = int(q % shape[k]); q /= shape[k]; }
@@ -785,6 +827,11 @@ int agdo_eikonal(int dbl, int ndim, int model, const int *shape, const int *shap
     return eikonal_impl<float>(ndim, model, shape, shape_i, niter_i, front, iso_w, geom, rhs, seed, values,
                                atol, rtol, nitermax, nthreads, visits, fvec, fwsum, fw, fidx);
 }
+
+// Walls for the following agdo_eikonal calls: wall distances in grid layout
+// (0 at the walls, 255 far from them), kept by pointer; NULL: no walls.  The
+// walls must also be seeds of right-hand side +inf in those calls.
+void agdo_set_walls(const unsigned char *wall_dist) { g_wall_dist = wall_dist; }
 
 // Second order scheme for the following agdo_eikonal calls (threshold; 0: off).
 void agdo_set_order2(double threshold) { g_order2 = threshold; }

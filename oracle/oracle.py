@@ -87,6 +87,26 @@ class Prepared:
     pass
 
 
+def wall_distance(walls, bound):
+    """L1 distance to the nearest wall point, saturated at 255 and set to 255
+    beyond `bound` (_SetGeometry.py:262-280): `bound` min-plus passes of the
+    3^ndim kernel |o|_1 from 0 at the walls, 255 elsewhere, points outside the
+    grid ignored."""
+    walls = np.asarray(walls, bool)
+    nd = walls.ndim
+    d = np.where(walls, 0, 255).astype(np.int32)
+    offsets = np.stack(np.meshgrid(*([np.arange(-1, 2)] * nd), indexing="ij"), -1).reshape(-1, nd)
+    for _ in range(bound):
+        pad = np.pad(d, 1, constant_values=255)
+        best = d.copy()
+        for o in offsets:
+            sl = tuple(slice(1 + c, 1 + c + n) for c, n in zip(o, d.shape))
+            best = np.minimum(best, np.minimum(pad[sl] + int(np.abs(o).sum()), 255))
+        d = best
+    d[d > bound] = 255
+    return d.astype(np.uint8)
+
+
 def prepare(case):
     """Host preparation of a case (model, dims, gridScales, origin, cost, metric,
     seeds, seedValues, traits, multiprecision)."""
@@ -132,6 +152,13 @@ def prepare(case):
     pos = tuple(pr.seed_idx.T)
     rhs[pos] = sv
     mask[pos] = 1
+    pr.trigger = mask.copy()  # the seeds, walls excluded
+    pr.walls = pr.wall_dist = None
+    if case.get("walls") is not None:  # walls: seeds of value +inf (_SetArgs.py:124-126)
+        pr.walls = np.broadcast_to(np.asarray(case["walls"], bool), pr.shape).copy()
+        pr.wall_dist = wall_distance(pr.walls, int(case.get("wallDistBound", 10)))
+        mask[pr.walls] = 1
+        rhs[pr.walls] = np.inf
     pr.rhs, pr.seed_mask = rhs, mask
     pr.iso_w = (pr.h.astype(np.float64) ** -2) if not pr.riemann else None
     if pr.iso_w is not None:
@@ -216,6 +243,9 @@ def eikonal(pr, dtype=np.float32, values=None, nthreads=1, flow=False, nitermax=
     geom = None if pr.geom is None else np.ascontiguousarray(pr.geom, np.float32)
     iso = None if pr.iso_w is None else np.ascontiguousarray(pr.iso_w, np.float64)
     L.agdo_set_order2(ctypes.c_double(getattr(pr, "order2", 0.0)))
+    wd = getattr(pr, "wall_dist", None)
+    wd = None if wd is None else np.ascontiguousarray(wd, np.uint8)
+    L.agdo_set_walls(_p(wd))  # kept by pointer: wd stays alive through the solve
     fac = getattr(pr, "factor", None)
     if fac is None:
         L.agdo_set_factor(ctypes.c_double(0.0), None, None)
@@ -231,6 +261,7 @@ def eikonal(pr, dtype=np.float32, values=None, nthreads=1, flow=False, nitermax=
                            _p(np.ascontiguousarray(pr.seed_mask)), _p(u), ctypes.c_double(pr.atol),
                            ctypes.c_double(pr.rtol), nitermax, nthreads, ctypes.byref(visits), _p(fv), _p(fws),
                            _p(fw), _p(fi))
+    L.agdo_set_walls(None)
     out = dict(values=u, niter_o=niter, tile_visits=visits.value)
     if flow:
         out.update(flow_vector=fv, flow_weightsum=fws, flow_weights=fw, flow_indices=fi)
@@ -243,7 +274,7 @@ def geodesics(pr, values, flow_vector, flow_weightsum, tips, step=0.25, causalit
     nd = pr.ndim
     shp = (ctypes.c_int * nd)(*pr.shape)
     eucl = np.zeros(pr.shape, np.uint8)
-    L.agdo_eucl_map(nd, shp, _p(np.ascontiguousarray(pr.seed_mask)), _p(eucl))
+    L.agdo_eucl_map(nd, shp, _p(np.ascontiguousarray(pr.trigger)), _p(eucl))  # seeds, not walls
     u = np.ascontiguousarray(values, np.float32)
     fv = np.ascontiguousarray(flow_vector, np.float32)
     fws = np.ascontiguousarray(flow_weightsum, np.float32)
@@ -318,6 +349,8 @@ def forward_rhs(pr, cost_variation, seed_value_variation):
         for j in range(len(cv)):
             cv[j][pos] = 0.0
     mask = pr.seed_mask.astype(bool)
+    if pr.walls is not None:  # the right-hand side +inf of the walls is a constant
+        cv[:, pr.walls] = 0.0
     return np.where(mask, cv, cv * pr.rhs.astype(np.float64))
 
 

@@ -7,7 +7,8 @@
 //   AGDREF_ISO (0|1), AGDREF_NDIM, AGDREF_SHAPE_I (comma list), AGDREF_SIZE_I,
 //   AGDREF_LOG2_SIZE_I, AGDREF_NITER_I, AGDREF_MULTIP (0|1), AGDREF_FLOW (0|1),
 //   AGDREF_FACTOR (0|1, source factorisation, factor_macro of _Kernel.py:47-49),
-//   AGDREF_ORDER2 (0|1, second order scheme, order2_macro of _Kernel.py:51-54).
+//   AGDREF_ORDER2 (0|1, second order scheme, order2_macro of _Kernel.py:51-54),
+//   AGDREF_WALLS (0|1, obstacles, walls_macro of _Kernel.py:111).
 //
 // The block below states the same compile-time traits that the reference's
 // `cupy_module_helper.traits_header` emits for these models
@@ -27,6 +28,9 @@
 #endif
 #if AGDREF_ORDER2
 #define order2_macro true
+#endif
+#ifndef AGDREF_WALLS
+#define AGDREF_WALLS 0
 #endif
 #define pruning_macro false
 #define geom_first_macro true
@@ -58,7 +62,7 @@ const int niter_i = AGDREF_FLOW ? 1 : AGDREF_NITER_I;
 #define local_i_macro true
 #define periodic_macro false
 #define isotropic_macro AGDREF_ISO
-#define walls_macro false
+#define walls_macro AGDREF_WALLS
 #if AGDREF_ISO
 #define geom_indep_macro AGDREF_NDIM
 #else
@@ -96,6 +100,10 @@ struct Args {
     BoolAtom *scorePrev, *scoreNext, *updateNext;
 };
 
+#if AGDREF_WALLS
+const WallT *g_wall_dist = nullptr;  // wallDist of the next solves (tile layout)
+#endif
+
 void thunk(void *p) {
     Args &a = *static_cast<Args *>(p);
     (void)a;
@@ -106,6 +114,9 @@ void thunk(void *p) {
         a.u,
 #endif
         a.geom, a.seeds, a.rhs,
+#if AGDREF_WALLS
+        g_wall_dist,
+#endif
 #if AGDREF_FLOW
         a.fw, a.fws, a.fi, a.fv, a.list, a.updateNext
 #else
@@ -160,6 +171,11 @@ void agdref_set_factor(const float *origin, float radius2, const float *metric) 
     factor_radius2 = radius2;
     for (int k = 0; k < factor_size; ++k) factor_metric[k] = metric[k];
 }
+#endif
+
+#if AGDREF_WALLS
+// The wallDist argument of the next Update calls (_SetGeometry.py:262-280).
+void agdref_set_walls(const unsigned char *wall_dist) { g_wall_dist = wall_dist; }
 #endif
 
 #if AGDREF_ORDER2

@@ -37,6 +37,7 @@ CASES = ["iso2", "riem2", "riem2_aniso", "iso3", "riem3", "ad_notebook"]
 RADIUS_CASES = ["riem2_radius", "iso2_radius"]  # seeds spread over a radius (values only)
 FACTOR_CASES = ["riem2_factor", "iso2_factor"]  # source factorisation (factoringRadius)
 ORDER2_CASES = ["riem2_order2", "iso2_order2", "riem3_order2"]  # second order scheme (order: 2)
+WALL_CASES = ["riem2_walls", "iso2_walls", "riem3_walls"]  # obstacles (walls, wallDistBound)
 
 
 @pytest.fixture(params=CASES)
@@ -49,7 +50,7 @@ def make_dictin(case, mode="gpu", extra=None):
     from adaptivegriddiscretizations_b200 import Eikonal
     d = {"model": case["model"], "mode": mode, "arrayOrdering": "RowMajor", "verbosity": 0}
     for k in ("dims", "gridScales", "origin", "seeds", "seedValues", "cost", "tips", "traits", "sensitivity",
-              "seedRadius", "factoringRadius", "order"):
+              "seedRadius", "factoringRadius", "order", "walls", "wallDistBound"):
         if k in case:
             d[k] = case[k]
     if "metric" in case:

@@ -147,6 +147,14 @@ class RefPipeline:
         rhs[pos] = seedValues
         seedTags[pos] = True
         self.trigger = seedTags.copy()
+        self.wall_b = None
+        if c.get("walls") is not None:  # _SetGeometry.py:262-280, _SetArgs.py:124-126
+            walls = np.broadcast_to(np.asarray(c["walls"], bool), self.shape)
+            wd = self.wall_distance(walls, int(c.get("wallDistBound", 10)))
+            self.wall_grid = wd
+            self.wall_b = self.bexp(wd, 255).astype(np.uint8)
+            seedTags = np.logical_or(seedTags, walls)
+            rhs[walls] = np.inf
         self.seedTags = seedTags
         self.rhs_b = self.bexp(rhs, np.inf).astype(np.float32)
         sp = self.bexp(seedTags, True)
@@ -160,6 +168,22 @@ class RefPipeline:
         else:
             self.multip_step = self.multip_max = np.float32(0)
         self.iso_w = (self.h.astype(np.float32) ** -2).astype(np.float32)
+
+    def wall_distance(self, walls, bound):
+        """wallDist: `bound` passes of the reference's inf-convolution kernel with
+        the L1 kernel (distance_kernel(1, ndim, uint8, ord=1)), cut beyond `bound`."""
+        nd = self.ndim
+        L = lib(f"libagdref_infconv{nd}.so")
+        L.agdref_infconv.restype = P
+        X = np.meshgrid(*(np.arange(-1, 2),) * nd)
+        kern = np.ascontiguousarray(np.round(sum(np.abs(x).astype(float) for x in X)).astype(np.uint8))
+        wd = np.full(self.shape, 255, np.uint8)
+        wd[walls] = 0
+        out = np.empty_like(wd)
+        res = L.agdref_infconv((ctypes.c_int * nd)(*self.shape), ptr(kern), bound, ptr(wd), ptr(out))
+        arr = (wd if res == wd.ctypes.data else out).copy()
+        arr[arr > bound] = 255
+        return arr
 
     def cost_metric(self, cost):
         """Interface.CostMetric (_Interface.py:202-211): the metric with the grid
@@ -211,10 +235,12 @@ class RefPipeline:
 
     @property
     def o2tag(self):
-        return "o" if int(self.c.get("order", 1)) == 2 else ""
+        return ("o" if int(self.c.get("order", 1)) == 2 else "") + ("w" if self.c.get("walls") is not None else "")
 
     def set_factor(self, L):
-        if self.o2tag:  # order2_threshold (_Kernel.py:310-314)
+        if self.wall_b is not None:
+            L.agdref_set_walls(ptr(self.wall_b))
+        if "o" in self.o2tag:  # order2_threshold (_Kernel.py:310-314)
             L.agdref_set_order2(ctypes.c_float(float(self.c.get("order2_threshold", 0.3))))
         if self.factor:
             o, r2, m = self.factor
@@ -509,6 +535,31 @@ def make_cases():
         c = {k: v for k, v in cases[key].items() if k != "sensitivity"}
         c["order"] = 2
         cases[key + "_order2"] = c
+    # walls (obstacles), with a gap, a one-pixel diagonal wall (leaky for diagonal
+    # offsets, as the reference's visibility test is) and a tip inside a wall
+    c = {k: v for k, v in cases["riem2"].items() if k != "sensitivity"}
+    w = np.zeros((61, 77), bool)
+    w[25, 5:70] = True
+    w[25, 40:44] = False
+    for i in range(35, 56):
+        w[i, i + 10] = True
+    c["walls"] = w
+    c["tips"] = np.array([[0.418, 0.3], [0.1, 0.5], [0.6, 0.2], [0.3, 1.1], [0.9, 0.7]], np.float32)
+    cases["riem2_walls"] = c
+    c = {k: v for k, v in cases["iso2"].items() if k != "sensitivity"}
+    w = np.zeros((70, 53), bool)
+    w[10:65, 26] = True
+    w[40:43, 26] = False
+    c["walls"] = w
+    cases["iso2_walls"] = c
+    c = {k: v for k, v in cases["riem3"].items() if k != "sensitivity"}
+    w = np.zeros((20, 22, 19), bool)
+    w[:, 14, :] = True
+    w[8:12, 14, 6:10] = False
+    c["walls"] = w
+    c["wallDistBound"] = 3
+    c["tips"] = np.array([[0.5, 0.95, 0.5], [0.2, 0.3, 0.8]], np.float32)
+    cases["riem3_walls"] = c
     # forward AD inputs (drawn last, so that the inputs above do not change):
     # two variations of the cost, and of the seed values
     for key in ("iso2", "riem2", "riem3"):
@@ -535,6 +586,8 @@ def run_case(name, case):
     pipe.solve()
     out = dict(values=pipe.values().astype(np.float32), niter_o=pipe.niter_o, tile_visits=pipe.tile_visits,
                atol=pipe.atol, rtol=pipe.rtol)
+    if pipe.wall_b is not None:
+        out["wall_dist"] = pipe.wall_grid
     if not pipe.multip:
         pipe.flow()
         out["values_after_flow"] = pipe.values().astype(np.float32)

@@ -8,7 +8,7 @@ import numpy as np
 import pytest
 
 from oracle import oracle as O
-from conftest import load_case, CASES, RADIUS_CASES, FACTOR_CASES, ORDER2_CASES
+from conftest import load_case, CASES, RADIUS_CASES, FACTOR_CASES, ORDER2_CASES, WALL_CASES
 
 REL = 1e-5  # parity bar for float32 values
 
@@ -22,7 +22,7 @@ def _geodesic_split(out):
     return res
 
 
-@pytest.mark.parametrize("name", CASES + RADIUS_CASES + FACTOR_CASES + ORDER2_CASES)
+@pytest.mark.parametrize("name", CASES + RADIUS_CASES + FACTOR_CASES + ORDER2_CASES + WALL_CASES)
 @pytest.mark.parametrize("dtype", [np.float32, np.float64])
 def test_values(name, dtype):
     case, ref = load_case(name)
@@ -37,7 +37,8 @@ def test_values(name, dtype):
         assert r["tile_visits"] == int(ref["tile_visits"])
 
 
-@pytest.mark.parametrize("name", [c for c in CASES if c != "ad_notebook"] + ["riem2_factor"] + ORDER2_CASES)
+@pytest.mark.parametrize("name", [c for c in CASES if c != "ad_notebook"] + ["riem2_factor"] + ORDER2_CASES +
+                         ["riem2_walls", "riem3_walls", "iso2_walls"])
 def test_geodesics(name):
     case, ref = load_case(name)
     r = O.run(case, np.float32)
@@ -150,3 +151,23 @@ def test_forward_ad_scaling_identity():
     u = r["values"]
     fin = np.isfinite(u)
     assert np.abs(r["valueVariation"][..., 0][fin] - u[fin]).max() <= 1e-9 * np.abs(u[fin]).max()
+
+
+@pytest.mark.parametrize("name", WALL_CASES)
+def test_wall_distance(name):
+    """The oracle's wall distance map equals the reference's inf-convolution
+    (L1 kernel, wallDistBound passes, cut beyond the bound) bit for bit."""
+    case, ref = load_case(name)
+    wd = O.wall_distance(case["walls"], int(case.get("wallDistBound", 10)))
+    assert np.array_equal(wd, ref["wall_dist"])
+
+
+def test_wall_visibility_matters():
+    """Without the visibility test (walls only as +inf seeds) the riem2_walls
+    values move far beyond the parity bar: the golden case exercises it."""
+    case, ref = load_case("riem2_walls")
+    pr = O.prepare(case)
+    pr.wall_dist = None
+    u = O.eikonal(pr, np.float32)["values"]
+    fin = np.isfinite(ref["values"])
+    assert np.abs(u[fin] - ref["values"][fin]).max() > 1e-2
