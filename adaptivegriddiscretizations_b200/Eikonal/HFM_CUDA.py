@@ -679,7 +679,11 @@ class Interface:
     def PostProcess(self):
         """Upwind flow, if needed (agd/Eikonal/HFM_CUDA/_PostProcess.py:46-95)."""
         self.combine_multiprecision()
-        self.flow_needed = self.reverseAD or self.forwardAD or self.hasTips or self.exportGeodesicFlow
+        self.exportActiveNeighs = bool(self.GetValue(
+            "exportActiveNeighs", default=False,
+            help="Export which finite differences are active, and the min/max index."))
+        self.flow_needed = (self.reverseAD or self.forwardAD or self.hasTips or self.exportGeodesicFlow
+                            or self.exportActiveNeighs)
         if not self.flow_needed:
             return
         L = _lib.lib()
@@ -688,7 +692,7 @@ class Interface:
         self.flow_vector = torch.empty(self.ndim * self.size_tot, dtype=torch.float32, device="cuda")
         self.flow_weightsum = torch.empty(self.size_tot, dtype=torch.float32, device="cuda")
         self.flow_weights = self.flow_indices = None
-        if self.reverseAD or self.forwardAD:
+        if self.reverseAD or self.forwardAD or self.exportActiveNeighs:
             self.flow_weights = torch.empty(nact * self.size_tot, dtype=torch.float32, device="cuda")
             self.flow_indices = torch.empty(nact * self.size_tot, dtype=torch.int32, device="cuda")
         inst = self.instance()
@@ -698,6 +702,14 @@ class Interface:
             fv = self.squeeze(self.flow_vector, self.ndim)
             h = torch.as_tensor(self.h, device="cuda").reshape((self.ndim,) + (1,) * self.ndim)
             self.hfmOut["flow"] = fv * (-h)
+        if self.exportActiveNeighs:
+            # bit k: the k-th finite difference has a positive flow weight; the mix
+            # index above the nact bits is 0 for these models (cuda/Update.h:187,206)
+            fw = self.squeeze(self.flow_weights, nact).reshape((nact,) + self.shape)
+            bits = torch.zeros(self.shape, dtype=torch.int32, device="cuda")
+            for k in range(nact):
+                bits |= (fw[k] > 0).to(torch.int32) << k
+            self.hfmOut["activeNeighs"] = bits
 
     def SolveAD(self):
         """Forward and reverse differentiation (agd/Eikonal/HFM_CUDA/_PostProcess.py:155-219)."""

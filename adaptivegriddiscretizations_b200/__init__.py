@@ -5,6 +5,6 @@ sensitivities.  The work is done by libagd_b200.so (CUDA for sm_100a) through
 the C ABI declared in include/agd_b200.h; torch provides device memory and
 streams.
 """
-from . import Eikonal, Metrics
+from . import Eikonal, Metrics, Selling
 
-__all__ = ["Eikonal", "Metrics"]
+__all__ = ["Eikonal", "Metrics", "Selling"]

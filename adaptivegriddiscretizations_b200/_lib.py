@@ -79,6 +79,7 @@ SIGNATURES = {
     "agd_prep_batch": (_I, [_P, _P]),
     "agd_prep_walls": (_I, [_I, _P, _P, _P, _I, _P, _P, _P, _P, _P]),
     "agd_selling": (_I, [_I, _P, _I, _P, _P, _P]),
+    "agd_voronoi_decomposition": (_I, [_I, _P, ctypes.c_longlong, _P, _P, _I, _P]),
     "agd_flow": (_I, [_P, _P, _P, _P, _P, _P]),
     "agd_eucl_map": (_I, [_I, _P, _P, _I, _I, _P, _P, _P]),
     "agd_geodesics": (_I, [_P, _P, _P, _P, _P, _I, ctypes.c_float, ctypes.c_float, _I, _I, _I, _I, _P, _I, _P,

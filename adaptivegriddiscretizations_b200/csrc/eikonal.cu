@@ -1375,6 +1375,48 @@ __global__ void walls_kernel(Geo g, const uint8_t *walls, const uint8_t *dist, u
     if (bits && word && (threadIdx.x & 31) == 0) bits[n_t >> 5] |= word;
 }
 
+// Selling's decomposition of n packed symmetric matrices in the planar layouts
+// of the reference's VoronoiDecomposition kernel (Kernel_VoronoiDecomposition.h:45-69):
+// m[c * n + p] (lower triangle, row major), weights[r * n + p],
+// offsets[(i * SD + r) * n + p] for coordinate i of offset r.  Dimension 1: the
+// weight is the matrix, the offset 1.  One thread per matrix, grid stride.
+template <int D, class OffT>
+__global__ void voronoi_kernel(const float *__restrict__ m, long long n, float *__restrict__ w,
+                               OffT *__restrict__ e) {
+    constexpr int SD = D * (D + 1) / 2;
+    for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < n; p += (long long)gridDim.x * blockDim.x) {
+        float mm[SD], ww[SD];
+        int ee[SD][3];
+#pragma unroll
+        for (int c = 0; c < SD; ++c) mm[c] = __ldg(m + c * n + p);
+        if constexpr (D == 1) {
+            ww[0] = mm[0];
+            ee[0][0] = 1;
+        } else if constexpr (D == 2) {
+            selling2(mm, ww, ee);
+        } else {
+            selling3(mm, ww, ee);
+        }
+#pragma unroll
+        for (int r = 0; r < SD; ++r) {
+            w[r * n + p] = ww[r];
+#pragma unroll
+            for (int i = 0; i < D; ++i) e[(i * SD + r) * n + p] = (OffT)ee[r][i];
+        }
+    }
+}
+
+template <int D>
+static void launch_voronoi(const float *m, long long n, float *w, void *e, int offset_bytes, cudaStream_t st) {
+    const unsigned blocks = (unsigned)std::min<long long>((n + 255) / 256, 148LL * 32);
+    switch (offset_bytes) {
+        case 1: voronoi_kernel<D, int8_t><<<blocks, 256, 0, st>>>(m, n, w, static_cast<int8_t *>(e)); break;
+        case 2: voronoi_kernel<D, int16_t><<<blocks, 256, 0, st>>>(m, n, w, static_cast<int16_t *>(e)); break;
+        case 4: voronoi_kernel<D, int32_t><<<blocks, 256, 0, st>>>(m, n, w, static_cast<int32_t *>(e)); break;
+        default: voronoi_kernel<D, int64_t><<<blocks, 256, 0, st>>>(m, n, w, static_cast<int64_t *>(e)); break;
+    }
+}
+
 __global__ void selling_kernel(int nd, const float *m, int n, float *w, int *e) {
     const int p = blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= n) return;
@@ -1567,6 +1609,22 @@ int agd_prep_walls(int ndim, const int *shape, const int *shape_i, const uint8_t
                                                                        reinterpret_cast<unsigned *>(seedbits));
     const cudaError_t err = cudaGetLastError();
     return err == cudaSuccess ? AGD_STATUS_OK : set_cuda_error("prep_walls", err);
+}
+
+int agd_voronoi_decomposition(int ndim, const float *m, long long n, float *weights, void *offsets, int offset_bytes,
+                              agd_stream_t stream) {
+    clear_error();
+    if (ndim < 1 || ndim > 3 || n < 0 || (n > 0 && (!m || !weights || !offsets)) ||
+        (offset_bytes != 1 && offset_bytes != 2 && offset_bytes != 4 && offset_bytes != 8))
+        return set_error(AGD_STATUS_INVALID, "agd_voronoi_decomposition: bad arguments (ndim 1 to 3, "
+                                             "offset_bytes 1, 2, 4 or 8)");
+    if (n == 0) return AGD_STATUS_OK;
+    cudaStream_t st = (cudaStream_t)stream;
+    if (ndim == 1) launch_voronoi<1>(m, n, weights, offsets, offset_bytes, st);
+    else if (ndim == 2) launch_voronoi<2>(m, n, weights, offsets, offset_bytes, st);
+    else launch_voronoi<3>(m, n, weights, offsets, offset_bytes, st);
+    const cudaError_t err = cudaGetLastError();
+    return err == cudaSuccess ? AGD_STATUS_OK : set_cuda_error("voronoi_decomposition", err);
 }
 
 int agd_selling(int ndim, const float *m, int n, float *weights, int32_t *offsets, agd_stream_t stream) {

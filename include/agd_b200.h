@@ -238,6 +238,15 @@ int agd_prep_walls(int ndim, const int *shape, const int *shape_i, const uint8_t
  * as the kernel's decomp_m (cuda/Geometry2.h:21-48, Geometry3.h:22-58). */
 int agd_selling(int ndim, const float *m, int n, float *weights, int32_t *offsets, agd_stream_t stream);
 
+/* The same decomposition in the planar layouts of the reference's standalone
+ * VoronoiDecomposition kernel (Kernel_VoronoiDecomposition.h:45-69,
+ * HFM_CUDA/VoronoiDecomposition.py:15-98, dimensions 1 to 3): m (symdim, n)
+ * lower triangles row major, weights (symdim, n), offsets (ndim, symdim, n) of
+ * offset_bytes-byte signed integers (1, 2, 4 or 8).  Dimension 1: weight = m,
+ * offset = 1. */
+int agd_voronoi_decomposition(int ndim, const float *m, long long n, float *weights, void *offsets,
+                              int offset_bytes, agd_stream_t stream);
+
 /* ------------------------------------------------------------------- flow -- */
 
 /* Upwind geodesic flow of a solved instance, one pass over all tiles (the

@@ -593,6 +593,8 @@ def run_case(name, case):
         out["values_after_flow"] = pipe.values().astype(np.float32)
         out["flow_vector"] = np.stack([pipe.bsq(v) for v in pipe.fv]).astype(np.float32)
         out["flow_weightsum"] = pipe.bsq(pipe.fws).astype(np.float32)
+        # exportActiveNeighs: positive flow weights as bits (cuda/Update.h:187,206)
+        out["activeNeighs"] = sum((pipe.bsq(w) > 0).astype(np.int32) << k for k, w in enumerate(pipe.fw))
         if "tips" in case:
             geos, stops, eucl = pipe.geodesics(case["tips"])
             out["geodesic_lengths"] = np.array([g.shape[1] for g in geos], np.int32)

@@ -66,3 +66,19 @@ def test_geodesics_order2(name):
         g = g.cpu().numpy()
         assert np.linalg.norm(g[:, -1] - want[:, -1]) < 3 * float(np.max(case["gridScales"]))
         assert np.linalg.norm(g[:, 0] - want[:, 0]) < 1e-5
+
+
+@pytest.mark.parametrize("name", ["iso2", "iso3", "riem2", "riem3", "riem2_walls"])
+def test_active_neighs_vs_reference(name):
+    """exportActiveNeighs: bit k set where the k-th finite difference has a
+    positive flow weight.  A weight is a difference of two nearly equal values
+    where the upwind direction is ambiguous, so the masks may differ at such
+    points: at most 0.5 % of them, and the bits are those of the exported
+    flow weights' signs."""
+    case, ref = load_case(name)
+    case = {k: v for k, v in case.items() if k not in ("tips", "sensitivity")}
+    out = make_dictin(case, extra={"exportActiveNeighs": True}).Run()
+    bits = out["activeNeighs"].cpu().numpy()
+    assert bits.dtype == np.int32 and bits.shape == ref["activeNeighs"].shape
+    assert (bits != ref["activeNeighs"]).mean() <= 5e-3
+    assert "exportActiveNeighs" in out["keys"]["used"]

@@ -171,3 +171,13 @@ def test_wall_visibility_matters():
     u = O.eikonal(pr, np.float32)["values"]
     fin = np.isfinite(ref["values"])
     assert np.abs(u[fin] - ref["values"][fin]).max() > 1e-2
+
+
+@pytest.mark.parametrize("name", ["iso2", "iso3", "riem2", "riem3", "riem2_walls"])
+def test_active_neighs(name):
+    """exportActiveNeighs: the bits of the positive flow weights equal the
+    reference's flow_weightpos (cuda/Update.h:187,206) point for point."""
+    case, ref = load_case(name)
+    r = O.eikonal(O.prepare(case), np.float32, flow=True)
+    bits = sum((w > 0).astype(np.int32) << k for k, w in enumerate(r["flow_weights"]))
+    assert np.array_equal(bits, ref["activeNeighs"])
