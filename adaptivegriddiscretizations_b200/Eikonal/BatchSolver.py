@@ -130,6 +130,8 @@ class BatchSolver:
         self.template = template
         self.batch, self.nbuffers = int(batch), int(nbuffers)
         self.model = itf.model
+        if itf.model_ not in ("Riemann", "Isotropic"):
+            raise NotImplementedError(f"BatchSolver: model {itf.model} goes through RunGPU / RunBatch")
         self.riemann = itf.model_ == "Riemann"
         self.ndim = itf.ndim
         self.shape, self.shape_i = tuple(itf.shape), tuple(itf.shape_i)

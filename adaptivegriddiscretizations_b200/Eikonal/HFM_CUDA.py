@@ -4,9 +4,10 @@
 Interface class of _Interface.py:23-174: every key is read through GetValue,
 which records help texts, defaults, used and unused keys in
 hfmOut['keys']; the same keys, defaults and errors as the reference are used
-for the Isotropic2/3 and Riemann2/3 models.  The work is done by
+for the Isotropic2/3, Diagonal2/3 and Riemann2/3 models.  The work is done by
 libagd_b200.so through the C ABI of include/agd_b200.h:
-  SetGeometry/SetArgs  -> agd_prep_geom, agd_block_expand, agd_prep_seeds
+  SetGeometry/SetArgs  -> agd_prep_geom(_diagonal), agd_block_expand, agd_prep_seeds,
+                          agd_prep_walls
   Solve (FIM)          -> agd_plan_create / agd_plan_upload / agd_plan_run
   PostProcess (flow)   -> agd_flow
   GetGeodesics         -> agd_eucl_map, agd_geodesics
@@ -30,6 +31,8 @@ DEFAULT_TRAITS = {
     "Riemann3": ((4, 4, 4), 4, 6),
     "Isotropic2": ((16, 16), 16, 4),
     "Isotropic3": ((4, 4, 4), 8, 4),
+    "Diagonal2": ((16, 16), 16, 4),
+    "Diagonal3": ((4, 4, 4), 8, 4),
 }
 SUPPORTED_TILES = {2: {(8, 8), (16, 16)}, 3: {(4, 4, 4)}}
 GEODESIC_CODES = ["Continue", "AtSeed", "InWall", "Stationnary", "PastSeed", "VanishingFlow"]
@@ -363,6 +366,25 @@ class Interface:
             hs = (ctypes.c_double * 3)(*[float(x) for x in self.h], *([1.0] * (3 - self.ndim)))
             _lib.check(L.agd_prep_geom(self.ndim, self.c_shape, self.c_shape_i, _lib.ptr(self._metric_flat), bcast,
                                        is_dual, hs, _lib.ptr(self.geom), self.stream), "prep_geom")
+        elif self.model_ == "Diagonal":  # geom = dualMetric.costs**2 (_SetGeometry.py:134-135)
+            metric = self.GetValue("metric", default=None, verbosity=3, help="Metric of the minimal path model")
+            dual = self.GetValue("dualMetric", default=None, verbosity=3,
+                                 help="Dual metric of the minimal path model")
+            if metric is None and dual is None:
+                raise ValueError("Missing value for key metric")
+            src, is_dual = (metric, 0) if metric is not None else (dual, 1)
+            self._metric_is_dual = bool(is_dual)
+            costs = _costs_hfm(src, self.ndim)
+            bcast = 1 if costs.dim() == 1 else 0
+            if not bcast and tuple(costs.shape[:-1]) != self.shape:
+                raise ValueError("Inconsistent dimensions for geometry data. "
+                                 "It should match (the last coordinates of) domain shape.")
+            self._metric_flat = costs.contiguous()
+            self.geom = torch.empty(self.ndim * self.size_tot, dtype=torch.float32, device="cuda")
+            hs = (ctypes.c_double * 3)(*[float(x) for x in self.h], *([1.0] * (3 - self.ndim)))
+            _lib.check(L.agd_prep_geom_diagonal(self.ndim, self.c_shape, self.c_shape_i, _lib.ptr(self._metric_flat),
+                                                bcast, is_dual, hs, _lib.ptr(self.geom), self.stream),
+                       "prep_geom_diagonal")
         else:
             self.geom = None
 
@@ -525,8 +547,14 @@ class Interface:
         cost = self.cost.reshape(-1)[flat] if self.cost.dim() else self.cost.expand(len(pts))
         cost = cost.double().cpu().numpy()
         h = self.h.astype(np.float64)
-        if self.model_ != "Riemann":  # Diagonal(ones).with_costs(h).with_cost(cost)
+        if self.model_ == "Isotropic":  # Diagonal(ones).with_costs(h).with_cost(cost)
             return np.einsum("ki,ij->kij", (cost[:, None] * h) ** 2, np.eye(nd)), cost
+        if self.model_ == "Diagonal":  # Diagonal(costs).with_costs(h).with_cost(cost)
+            fc = self._metric_flat.reshape(-1, nd)
+            fc = (fc[flat] if fc.shape[0] > 1 else fc.expand(len(pts), nd)).double().cpu().numpy()
+            if self._metric_is_dual:
+                fc = 1.0 / fc
+            return np.einsum("ki,ij->kij", (fc * cost[:, None] * h) ** 2, np.eye(nd)), cost
         sd = nd * (nd + 1) // 2
         fm = self._metric_flat.reshape(-1, sd)
         fm = (fm[flat] if fm.shape[0] > 1 else fm.expand(len(pts), sd)).double().cpu().numpy()
@@ -555,7 +583,8 @@ class Interface:
         m, cost = self._cost_metrics(corners)
         if self.model_ == "Riemann":
             return np.tensordot(wc, m, axes=1)
-        return np.diag((np.dot(wc, cost) * self.h.astype(np.float64)) ** 2)
+        # diagonal metrics: the costs c*h per axis are interpolated, then squared
+        return np.diag(np.dot(wc, np.sqrt(np.diagonal(m, axis1=1, axis2=2))) ** 2)
 
     def _spread_seed(self, seed, seed_value, r):
         """SetRHS's seed spreading (agd/Eikonal/HFM_CUDA/_SetArgs.py:46-75): the grid
@@ -578,7 +607,8 @@ class Interface:
 
     def instance(self):
         inst = _lib.AgdInstance()
-        inst.model = _lib.AGD_MODEL_RIEMANN if self.model_ == "Riemann" else _lib.AGD_MODEL_ISOTROPIC
+        inst.model = {"Riemann": _lib.AGD_MODEL_RIEMANN, "Diagonal": _lib.AGD_MODEL_DIAGONAL}.get(
+            self.model_, _lib.AGD_MODEL_ISOTROPIC)
         inst.ndim = self.ndim
         for k in range(3):
             inst.shape[k] = self.shape[k] if k < self.ndim else 1
@@ -687,7 +717,7 @@ class Interface:
         if not self.flow_needed:
             return
         L = _lib.lib()
-        nact = self.ndim if self.model_ == "Isotropic" else self.ndim * (self.ndim + 1) // 2
+        nact = self.ndim * (self.ndim + 1) // 2 if self.model_ == "Riemann" else self.ndim
         self.nact = nact
         self.flow_vector = torch.empty(self.ndim * self.size_tot, dtype=torch.float32, device="cuda")
         self.flow_weightsum = torch.empty(self.size_tot, dtype=torch.float32, device="cuda")
@@ -881,6 +911,25 @@ class Interface:
 
 def _host_scalar(x):
     return float(x.item()) if isinstance(x, torch.Tensor) else float(x)
+
+
+def _costs_hfm(src, ndim):
+    """A diagonal metric given as a Metrics.Diagonal-like object (attribute costs,
+    shape (d, *shape) or (d,)), an isotropic one (attribute cost), or an HFM
+    array (*shape, d) -> float32 CUDA tensor (*shape, d), or (d,) if constant
+    (Metrics.Diagonal.from_HFM: the costs per axis, last axis)."""
+    if hasattr(src, "costs"):
+        c = _to_tensor(src.costs)
+        if c.shape[0] != ndim:
+            raise ValueError("Metric dimension does not match the model")
+        return torch.movedim(c, 0, -1).contiguous()
+    if isinstance(src, Metrics.Isotropic) or hasattr(src, "cost"):
+        c = _to_tensor(src.cost)
+        return c[..., None].expand(tuple(c.shape) + (ndim,)).contiguous()
+    arr = _to_tensor(src)
+    if arr.shape[-1] != ndim:
+        raise ValueError(f"Diagonal metric array must have {ndim} components in its last axis (HFM layout)")
+    return arr.contiguous()
 
 
 def _metric_hfm(src, ndim):

@@ -21,6 +21,7 @@ AGD_STATUS_UNSUPPORTED = 32
 
 AGD_MODEL_ISOTROPIC = 0
 AGD_MODEL_RIEMANN = 1
+AGD_MODEL_DIAGONAL = 2
 AGD_FLAG_ACTIVATE_ALL = 1
 
 _c_int3 = ctypes.c_int * 3
@@ -73,6 +74,7 @@ SIGNATURES = {
     "agd_eikonal_solve": (_I, [_P, _I, _P, ctypes.c_size_t, _P, _P, _P]),
     "agd_eikonal_solve_fixed_scratch": (_I, [_P, _I, _P, _P, _P]),
     "agd_prep_geom": (_I, [_I, _P, _P, _P, _I, _I, _P, _P, _P]),
+    "agd_prep_geom_diagonal": (_I, [_I, _P, _P, _P, _I, _I, _P, _P, _P]),
     "agd_block_expand": (_I, [_I, _P, _P, _I, _P, _I, ctypes.c_float, _P, _P]),
     "agd_block_squeeze": (_I, [_I, _P, _P, _I, _P, _P, _P]),
     "agd_prep_seeds": (_I, [_I, _P, _P, _P, _P, _I, _P, _P, _P, _P]),

@@ -226,7 +226,7 @@ __global__ void mp_copy_kernel(Sched S, int dir) {
 template <class TL, int MODEL, bool MP = false, bool FACT = false, bool ORD2 = false, bool WALLS = false>
 struct Visit {
     static constexpr int D = TL::D, P = TL::P;
-    static constexpr int NACT = MODEL == AGD_MODEL_ISOTROPIC ? D : D * (D + 1) / 2;
+    static constexpr int NACT = MODEL == AGD_MODEL_RIEMANN ? D * (D + 1) / 2 : D;
     static constexpr int NTOT = 2 * NACT;
     static constexpr int SD = D * (D + 1) / 2;
 
@@ -293,11 +293,17 @@ struct Visit {
 
     // Stencil of the point with bilevel index n_t, in two steps so that the
     // loads of all the points of a lane are in flight together: the raw words
-    // (cached weights and packed offsets, or the dual metric), then the weights
-    // and offsets (unpacked, or by Selling's decomposition).
-    static constexpr int kRaw = MODEL == AGD_MODEL_ISOTROPIC ? 1 : 2 * SD;
+    // (cached weights and packed offsets, or the dual metric; Diagonal: the
+    // weights), then the weights and offsets (unpacked, or by Selling's
+    // decomposition; unit offsets for Isotropic and Diagonal).
+    static constexpr int kRaw = MODEL == AGD_MODEL_ISOTROPIC ? 1 : (MODEL == AGD_MODEL_DIAGONAL ? D : 2 * SD);
     __device__ __forceinline__ static void stencil_load(const Inst &I, size_t n_t, float *raw) {
-        if (MODEL == AGD_MODEL_ISOTROPIC) return;
+        if constexpr (MODEL == AGD_MODEL_ISOTROPIC) return;
+        if constexpr (MODEL == AGD_MODEL_DIAGONAL) {
+#pragma unroll
+            for (int k = 0; k < D; ++k) raw[k] = __ldg(I.a.geom + (size_t)k * I.size_tot + n_t);
+            return;
+        }
         if (I.stencil) {
 #pragma unroll
             for (int r = 0; r < 2 * SD; ++r) raw[r] = __ldg(I.stencil + (size_t)r * I.size_tot + n_t);
@@ -313,10 +319,10 @@ struct Visit {
                                                           unsigned *hide) {
 #pragma unroll
         for (int k = 0; k < NACT; ++k) hide[k] = 0u;
-        if (MODEL == AGD_MODEL_ISOTROPIC) {
+        if constexpr (MODEL != AGD_MODEL_RIEMANN) {
 #pragma unroll
             for (int k = 0; k < D; ++k) {
-                w[k] = I.a.iso_weights[k];
+                w[k] = MODEL == AGD_MODEL_ISOTROPIC ? I.a.iso_weights[k] : raw[k];
 #pragma unroll
                 for (int c = 0; c < 3; ++c) e[k][c] = (c == k);
             }
@@ -441,7 +447,7 @@ struct Visit {
             unsigned hide[NACT];
             if (seed[p]) continue;  // seeds (and padding) keep their value: no stencil needed
             stencil_decode(I, raw[p], wts[p], ev, hide);
-            if constexpr (FACT) factor_shifts<D, NACT, MODEL == AGD_MODEL_ISOTROPIC>(A, xt, ev, fsh[p]);
+            if constexpr (FACT) factor_shifts<D, NACT, MODEL != AGD_MODEL_RIEMANN>(A, xt, ev, fsh[p]);
 #pragma unroll
             for (int k = 0; k < NACT; ++k) {
 #pragma unroll
@@ -645,7 +651,7 @@ struct Visit {
     }
 };
 
-template <unsigned VMASK>
+template <unsigned long long VMASK>
 __device__ __forceinline__ void dispatch(const Sched &S, int t, int e, int lane, float *us) {
     const int ii = __ldg(S.tile_inst + t);
     const Inst &I = S.inst[ii];
@@ -723,6 +729,42 @@ __device__ __forceinline__ void dispatch(const Sched &S, int t, int e, int lane,
         case V_RIEM3_4_W:
             if constexpr ((VMASK >> V_RIEM3_4_W) & 1) Visit<Tile<3, 4, 4, 4>, AGD_MODEL_RIEMANN, false, false, false, true>::run(S, I, ii, n_o, e, lane, us);
             break;
+        case V_DIAG2_8:
+            if constexpr ((VMASK >> V_DIAG2_8) & 1) Visit<Tile<2, 8, 8, 1>, AGD_MODEL_DIAGONAL>::run(S, I, ii, n_o, e, lane, us);
+            break;
+        case V_DIAG2_16:
+            if constexpr ((VMASK >> V_DIAG2_16) & 1) Visit<Tile<2, 16, 16, 1>, AGD_MODEL_DIAGONAL>::run(S, I, ii, n_o, e, lane, us);
+            break;
+        case V_DIAG3_4:
+            if constexpr ((VMASK >> V_DIAG3_4) & 1) Visit<Tile<3, 4, 4, 4>, AGD_MODEL_DIAGONAL>::run(S, I, ii, n_o, e, lane, us);
+            break;
+        case V_DIAG2_8_MP:
+            if constexpr ((VMASK >> V_DIAG2_8_MP) & 1) Visit<Tile<2, 8, 8, 1>, AGD_MODEL_DIAGONAL, true>::run(S, I, ii, n_o, e, lane, us);
+            break;
+        case V_DIAG2_16_MP:
+            if constexpr ((VMASK >> V_DIAG2_16_MP) & 1) Visit<Tile<2, 16, 16, 1>, AGD_MODEL_DIAGONAL, true>::run(S, I, ii, n_o, e, lane, us);
+            break;
+        case V_DIAG3_4_MP:
+            if constexpr ((VMASK >> V_DIAG3_4_MP) & 1) Visit<Tile<3, 4, 4, 4>, AGD_MODEL_DIAGONAL, true>::run(S, I, ii, n_o, e, lane, us);
+            break;
+        case V_DIAG2_8_F:
+            if constexpr ((VMASK >> V_DIAG2_8_F) & 1) Visit<Tile<2, 8, 8, 1>, AGD_MODEL_DIAGONAL, false, true>::run(S, I, ii, n_o, e, lane, us);
+            break;
+        case V_DIAG2_16_F:
+            if constexpr ((VMASK >> V_DIAG2_16_F) & 1) Visit<Tile<2, 16, 16, 1>, AGD_MODEL_DIAGONAL, false, true>::run(S, I, ii, n_o, e, lane, us);
+            break;
+        case V_DIAG3_4_F:
+            if constexpr ((VMASK >> V_DIAG3_4_F) & 1) Visit<Tile<3, 4, 4, 4>, AGD_MODEL_DIAGONAL, false, true>::run(S, I, ii, n_o, e, lane, us);
+            break;
+        case V_DIAG2_8_O2:
+            if constexpr ((VMASK >> V_DIAG2_8_O2) & 1) Visit<Tile<2, 8, 8, 1>, AGD_MODEL_DIAGONAL, false, false, true>::run(S, I, ii, n_o, e, lane, us);
+            break;
+        case V_DIAG2_16_O2:
+            if constexpr ((VMASK >> V_DIAG2_16_O2) & 1) Visit<Tile<2, 16, 16, 1>, AGD_MODEL_DIAGONAL, false, false, true>::run(S, I, ii, n_o, e, lane, us);
+            break;
+        case V_DIAG3_4_O2:
+            if constexpr ((VMASK >> V_DIAG3_4_O2) & 1) Visit<Tile<3, 4, 4, 4>, AGD_MODEL_DIAGONAL, false, false, true>::run(S, I, ii, n_o, e, lane, us);
+            break;
         default:
             break;
     }
@@ -731,7 +773,7 @@ __device__ __forceinline__ void dispatch(const Sched &S, int t, int e, int lane,
 constexpr int kMaxTileSize = 256;
 
 // Shared floats per warp for the variants of VMASK.
-template <unsigned VMASK>
+template <unsigned long long VMASK>
 constexpr int smem_floats() {
     int m = 0;
     if ((VMASK >> V_ISO2_8) & 1) m = std::max(m, Visit<Tile<2, 8, 8, 1>, AGD_MODEL_ISOTROPIC>::kSmemFloats);
@@ -754,19 +796,29 @@ constexpr int smem_floats() {
     if ((VMASK >> V_RIEM2_8_W) & 1) m = std::max(m, Visit<Tile<2, 8, 8, 1>, AGD_MODEL_RIEMANN, false, false, false, true>::kSmemFloats);
     if ((VMASK >> V_RIEM2_16_W) & 1) m = std::max(m, Visit<Tile<2, 16, 16, 1>, AGD_MODEL_RIEMANN, false, false, false, true>::kSmemFloats);
     if ((VMASK >> V_RIEM3_4_W) & 1) m = std::max(m, Visit<Tile<3, 4, 4, 4>, AGD_MODEL_RIEMANN, false, false, false, true>::kSmemFloats);
+    if ((VMASK >> V_DIAG2_8) & 1) m = std::max(m, Visit<Tile<2, 8, 8, 1>, AGD_MODEL_DIAGONAL>::kSmemFloats);
+    if ((VMASK >> V_DIAG2_16) & 1) m = std::max(m, Visit<Tile<2, 16, 16, 1>, AGD_MODEL_DIAGONAL>::kSmemFloats);
+    if ((VMASK >> V_DIAG3_4) & 1) m = std::max(m, Visit<Tile<3, 4, 4, 4>, AGD_MODEL_DIAGONAL>::kSmemFloats);
+    if ((VMASK >> V_DIAG2_8_F) & 1) m = std::max(m, Visit<Tile<2, 8, 8, 1>, AGD_MODEL_DIAGONAL, false, true>::kSmemFloats);
+    if ((VMASK >> V_DIAG2_16_F) & 1) m = std::max(m, Visit<Tile<2, 16, 16, 1>, AGD_MODEL_DIAGONAL, false, true>::kSmemFloats);
+    if ((VMASK >> V_DIAG3_4_F) & 1) m = std::max(m, Visit<Tile<3, 4, 4, 4>, AGD_MODEL_DIAGONAL, false, true>::kSmemFloats);
+    if ((VMASK >> V_DIAG2_8_O2) & 1) m = std::max(m, Visit<Tile<2, 8, 8, 1>, AGD_MODEL_DIAGONAL, false, false, true>::kSmemFloats);
+    if ((VMASK >> V_DIAG2_16_O2) & 1) m = std::max(m, Visit<Tile<2, 16, 16, 1>, AGD_MODEL_DIAGONAL, false, false, true>::kSmemFloats);
+    if ((VMASK >> V_DIAG3_4_O2) & 1) m = std::max(m, Visit<Tile<3, 4, 4, 4>, AGD_MODEL_DIAGONAL, false, false, true>::kSmemFloats);
     return m;
 }
 
-template <unsigned VMASK>
+template <unsigned long long VMASK>
 struct EikonalVisitor {
     // Resident 4-warp CTAs per SM the register budget must allow: 256-point tiles
     // keep 8 points per lane in registers, Riemann3 twelve neighbours per point,
     // multiprecision an integer part beside every value.
     static constexpr int kMinCtas =
-        (VMASK & ((1u << V_RIEM2_16) | (1u << V_ISO2_16) | (1u << V_ISO2_16_MP) | (1u << V_ISO2_16_F) |
-                  (1u << V_ISO2_16_O2) | (1u << V_RIEM2_16_W)))                                ? 4
-        : (VMASK & ((1u << V_RIEM3_4) | (1u << V_RIEM3_4_MP) | (1u << V_RIEM3_4_F) | (1u << V_RIEM3_4_O2) |
-                    (1u << V_RIEM3_4_W)))                                                     ? 6
+        (VMASK & ((1ull << V_RIEM2_16) | (1ull << V_ISO2_16) | (1ull << V_ISO2_16_MP) | (1ull << V_ISO2_16_F) |
+                  (1ull << V_ISO2_16_O2) | (1ull << V_RIEM2_16_W) | (1ull << V_DIAG2_16) |
+                  (1ull << V_DIAG2_16_MP) | (1ull << V_DIAG2_16_F) | (1ull << V_DIAG2_16_O2)))      ? 4
+        : (VMASK & ((1ull << V_RIEM3_4) | (1ull << V_RIEM3_4_MP) | (1ull << V_RIEM3_4_F) | (1ull << V_RIEM3_4_O2) |
+                    (1ull << V_RIEM3_4_W)))                                                     ? 6
         : (VMASK & (kMpVariants | kFactorVariants | kOrder2Variants))                                ? 7
                                                                                                      : 9;
     struct Args {};
@@ -780,19 +832,19 @@ struct EikonalVisitor {
     // as copies of the first (_SetArgs.py:171-177), and the Selling stencils of
     // the Riemann instances are computed.
     static cudaError_t prepare(const Sched &S, const WsLayout &L, cudaStream_t st) {
-        constexpr unsigned kRiemann = (1u << V_RIEM2_8) | (1u << V_RIEM3_4) | (1u << V_RIEM2_16) |
-                                      (1u << V_RIEM2_8_MP) | (1u << V_RIEM3_4_MP) | (1u << V_RIEM2_8_F) |
-                                      (1u << V_RIEM3_4_F) | (1u << V_RIEM2_8_O2) | (1u << V_RIEM3_4_O2) |
+        constexpr unsigned long long kRiemann = (1ull << V_RIEM2_8) | (1ull << V_RIEM3_4) | (1ull << V_RIEM2_16) |
+                                      (1ull << V_RIEM2_8_MP) | (1ull << V_RIEM3_4_MP) | (1ull << V_RIEM2_8_F) |
+                                      (1ull << V_RIEM3_4_F) | (1ull << V_RIEM2_8_O2) | (1ull << V_RIEM3_4_O2) |
                                       kWallVariants;
         if (VMASK & kMpVariants) mp_copy_kernel<<<(L.total_tiles + 7) / 8, 256, 0, st>>>(S, 0);
         if (!(VMASK & kRiemann) || L.stencil == L.total) return cudaGetLastError();
         // variants that read the hidden-neighbour bits: the walls pass follows
-        constexpr unsigned kWallCapable = kWallVariants | (1u << V_RIEM2_8_MP) | (1u << V_RIEM3_4_MP) |
-                                          (1u << V_RIEM2_8_F) | (1u << V_RIEM3_4_F) | (1u << V_RIEM2_8_O2) |
-                                          (1u << V_RIEM3_4_O2);
+        constexpr unsigned long long kWallCapable = kWallVariants | (1ull << V_RIEM2_8_MP) | (1ull << V_RIEM3_4_MP) |
+                                          (1ull << V_RIEM2_8_F) | (1ull << V_RIEM3_4_F) | (1ull << V_RIEM2_8_O2) |
+                                          (1ull << V_RIEM3_4_O2);
         const unsigned grid = (L.total_tiles + 7) / 8;
-        if (VMASK & ((1u << V_RIEM3_4) | (1u << V_RIEM3_4_MP) | (1u << V_RIEM3_4_F) | (1u << V_RIEM3_4_O2) |
-                     (1u << V_RIEM3_4_W))) {
+        if (VMASK & ((1ull << V_RIEM3_4) | (1ull << V_RIEM3_4_MP) | (1ull << V_RIEM3_4_F) | (1ull << V_RIEM3_4_O2) |
+                     (1ull << V_RIEM3_4_W))) {
             stencil_kernel<3><<<grid, 256, 0, st>>>(S.inst, S.ninst, L.total_tiles, S.ctrl);
             if (VMASK & kWallCapable) stencil_walls_kernel<3><<<grid, 256, 0, st>>>(S.inst, S.ninst, L.total_tiles);
         } else {
@@ -814,7 +866,7 @@ struct EikonalVisitor {
 struct agd_plan {
     std::vector<agd::Inst> insts;
     agd::WsLayout L;
-    unsigned vmask;
+    unsigned long long vmask;
     int ndim;
 };
 
@@ -822,7 +874,7 @@ namespace agd {
 
 // Checks the instances of one launch; returns the mask of tile-visit variants.
 // stencil_cache: whether the launch computes the Riemann stencil cache.
-static int validate(const agd_instance *host, const Inst *insts, int n, bool stencil_cache, unsigned *vmask) {
+static int validate(const agd_instance *host, const Inst *insts, int n, bool stencil_cache, unsigned long long *vmask) {
     *vmask = 0;
     for (int i = 0; i < n; ++i) {
         const agd_instance &a = host[i];
@@ -840,13 +892,13 @@ static int validate(const agd_instance *host, const Inst *insts, int n, bool ste
         }
         else if (a.multip_step != 0.f && (!a.valuesq || !a.values_next || !a.valuesq_next || !(a.multip_step > 0.f)))
             bad = "multiprecision needs valuesq, values_next, valuesq_next and multip_step > 0";
-        else if (!a.values || !a.rhs || !a.seedbits || (a.model == AGD_MODEL_RIEMANN && !a.geom)) bad = "missing array";
+        else if (!a.values || !a.rhs || !a.seedbits || (a.model != AGD_MODEL_ISOTROPIC && !a.geom)) bad = "missing array";
         else if (reinterpret_cast<uintptr_t>(a.seedbits) % 4 != 0) bad = "seedbits must be 4-byte aligned";
         else if (a.niter_i < 1 || a.fim_front_width < 2 || a.fim_front_width > 255 || a.nitermax_o < 0 ||
                  a.nitermax_o > kMaxEpochs)
             bad = "bad niter_i / fim_front_width / nitermax_o (at most 16000)";
         if (bad) return set_error(code, bad);
-        *vmask |= 1u << insts[i].variant;
+        *vmask |= 1ull << insts[i].variant;
     }
     return AGD_STATUS_OK;
 }
@@ -872,32 +924,52 @@ static int plan_create(const agd_instance *host, int n, agd_plan **out) {
 
 // The persistent solve for the variants in vmask, on a workspace laid out by L
 // whose descriptors are already uploaded.
-static int run_variants(int ndim, unsigned vmask, const WsLayout &L, void *ws, int n, agd_stats *stats,
+static int run_variants(int ndim, unsigned long long vmask, const WsLayout &L, void *ws, int n, agd_stats *stats,
                         const agd_launch *cfg, cudaStream_t st) {
-    constexpr unsigned R2 = 1u << V_RIEM2_8, I16 = 1u << V_ISO2_16, I8 = 1u << V_ISO2_8;
-    constexpr unsigned R3 = 1u << V_RIEM3_4, I3 = 1u << V_ISO3_4, R2L = 1u << V_RIEM2_16;
-    constexpr unsigned MP2 = (1u << V_ISO2_8_MP) | (1u << V_ISO2_16_MP) | (1u << V_RIEM2_8_MP);
-    constexpr unsigned MP3 = (1u << V_ISO3_4_MP) | (1u << V_RIEM3_4_MP);
+    constexpr unsigned long long R2 = 1ull << V_RIEM2_8, I16 = 1ull << V_ISO2_16, I8 = 1ull << V_ISO2_8;
+    constexpr unsigned long long R3 = 1ull << V_RIEM3_4, I3 = 1ull << V_ISO3_4, R2L = 1ull << V_RIEM2_16;
+    constexpr unsigned long long MP2 = (1ull << V_ISO2_8_MP) | (1ull << V_ISO2_16_MP) | (1ull << V_RIEM2_8_MP);
+    constexpr unsigned long long MP3 = (1ull << V_ISO3_4_MP) | (1ull << V_RIEM3_4_MP);
     // Riemann with walls, beside plain instances of every family
-    constexpr unsigned W2 = (1u << V_RIEM2_8_W) | (1u << V_RIEM2_16_W), W3 = 1u << V_RIEM3_4_W;
+    constexpr unsigned long long W2 = (1ull << V_RIEM2_8_W) | (1ull << V_RIEM2_16_W), W3 = 1ull << V_RIEM3_4_W;
+    if (vmask & kDiagVariants) {  // Diagonal instances run in kernels of their own
+        constexpr unsigned long long D2 = (1ull << V_DIAG2_8) | (1ull << V_DIAG2_16), D3 = 1ull << V_DIAG3_4;
+        constexpr unsigned long long DMP2 = (1ull << V_DIAG2_8_MP) | (1ull << V_DIAG2_16_MP), DMP3 = 1ull << V_DIAG3_4_MP;
+        constexpr unsigned long long DF2 = (1ull << V_DIAG2_8_F) | (1ull << V_DIAG2_16_F), DF3 = 1ull << V_DIAG3_4_F;
+        constexpr unsigned long long DO2 = (1ull << V_DIAG2_8_O2) | (1ull << V_DIAG2_16_O2), DO3 = 1ull << V_DIAG3_4_O2;
+        if (vmask & ~kDiagVariants) return set_error(AGD_STATUS_UNSUPPORTED, "Diagonal instances beside other models in one plan");
+        const bool mp = vmask & kMpVariants, f = vmask & kFactorVariants, o2 = vmask & kOrder2Variants;
+        if (int(mp) + int(f) + int(o2) > 1)
+            return set_error(AGD_STATUS_UNSUPPORTED, "Diagonal instances of several option families in one plan");
+        if (ndim == 2) {
+            if (o2) return run_sched<EikonalVisitor<DO2 | D2>>(L, ws, n, {}, stats, cfg, st);
+            if (f) return run_sched<EikonalVisitor<DF2 | D2>>(L, ws, n, {}, stats, cfg, st);
+            if (mp) return run_sched<EikonalVisitor<DMP2 | D2>>(L, ws, n, {}, stats, cfg, st);
+            return run_sched<EikonalVisitor<D2>>(L, ws, n, {}, stats, cfg, st);
+        }
+        if (o2) return run_sched<EikonalVisitor<DO3 | D3>>(L, ws, n, {}, stats, cfg, st);
+        if (f) return run_sched<EikonalVisitor<DF3 | D3>>(L, ws, n, {}, stats, cfg, st);
+        if (mp) return run_sched<EikonalVisitor<DMP3 | D3>>(L, ws, n, {}, stats, cfg, st);
+        return run_sched<EikonalVisitor<D3>>(L, ws, n, {}, stats, cfg, st);
+    }
     if (vmask & kOrder2Variants) {  // second order instances, possibly beside plain ones
-        constexpr unsigned O2 = (1u << V_ISO2_8_O2) | (1u << V_ISO2_16_O2) | (1u << V_RIEM2_8_O2);
-        constexpr unsigned O3 = (1u << V_ISO3_4_O2) | (1u << V_RIEM3_4_O2);
+        constexpr unsigned long long O2 = (1ull << V_ISO2_8_O2) | (1ull << V_ISO2_16_O2) | (1ull << V_RIEM2_8_O2);
+        constexpr unsigned long long O3 = (1ull << V_ISO3_4_O2) | (1ull << V_RIEM3_4_O2);
         if (vmask & (kMpVariants | kFactorVariants))
             return set_error(AGD_STATUS_UNSUPPORTED, "second order beside multiprecision or factorisation in one plan");
         if (ndim == 2) return run_sched<EikonalVisitor<O2 | R2 | I16 | I8 | R2L | W2>>(L, ws, n, {}, stats, cfg, st);
         return run_sched<EikonalVisitor<O3 | R3 | I3 | W3>>(L, ws, n, {}, stats, cfg, st);
     }
     if (vmask & kFactorVariants) {  // factored instances, possibly beside plain ones
-        constexpr unsigned F2 = (1u << V_ISO2_8_F) | (1u << V_ISO2_16_F) | (1u << V_RIEM2_8_F);
-        constexpr unsigned F3 = (1u << V_ISO3_4_F) | (1u << V_RIEM3_4_F);
+        constexpr unsigned long long F2 = (1ull << V_ISO2_8_F) | (1ull << V_ISO2_16_F) | (1ull << V_RIEM2_8_F);
+        constexpr unsigned long long F3 = (1ull << V_ISO3_4_F) | (1ull << V_RIEM3_4_F);
         if (vmask & kMpVariants) return set_error(AGD_STATUS_UNSUPPORTED, "factorisation and multiprecision in one plan");
         if (ndim == 2) return run_sched<EikonalVisitor<F2 | R2 | I16 | I8 | R2L | W2>>(L, ws, n, {}, stats, cfg, st);
         return run_sched<EikonalVisitor<F3 | R3 | I3 | W3>>(L, ws, n, {}, stats, cfg, st);
     }
     if (vmask & kMpVariants) {
         if (ndim == 2) {
-            if (vmask == (1u << V_RIEM2_8_MP)) return run_sched<EikonalVisitor<(1u << V_RIEM2_8_MP)>>(L, ws, n, {}, stats, cfg, st);
+            if (vmask == (1ull << V_RIEM2_8_MP)) return run_sched<EikonalVisitor<(1ull << V_RIEM2_8_MP)>>(L, ws, n, {}, stats, cfg, st);
             return run_sched<EikonalVisitor<R2 | I16 | I8 | R2L | MP2 | W2>>(L, ws, n, {}, stats, cfg, st);
         }
         return run_sched<EikonalVisitor<R3 | I3 | MP3 | W3>>(L, ws, n, {}, stats, cfg, st);
@@ -907,7 +979,7 @@ static int run_variants(int ndim, unsigned vmask, const WsLayout &L, void *ws, i
         if (vmask == R2L) return run_sched<EikonalVisitor<R2L>>(L, ws, n, {}, stats, cfg, st);
         if (vmask == I16) return run_sched<EikonalVisitor<I16>>(L, ws, n, {}, stats, cfg, st);
         if (vmask == I8) return run_sched<EikonalVisitor<I8>>(L, ws, n, {}, stats, cfg, st);
-        if (vmask == (1u << V_RIEM2_8_W)) return run_sched<EikonalVisitor<(1u << V_RIEM2_8_W)>>(L, ws, n, {}, stats, cfg, st);
+        if (vmask == (1ull << V_RIEM2_8_W)) return run_sched<EikonalVisitor<(1ull << V_RIEM2_8_W)>>(L, ws, n, {}, stats, cfg, st);
         return run_sched<EikonalVisitor<R2 | I16 | I8 | R2L | W2>>(L, ws, n, {}, stats, cfg, st);
     }
     if (vmask == R3) return run_sched<EikonalVisitor<R3>>(L, ws, n, {}, stats, cfg, st);
@@ -960,7 +1032,7 @@ static int fixed_scratch_solve(const agd_instance *host, int n, agd_stats *stats
     Inst insts[kFixedScratchMaxInstances];
     WsLayout L;
     if (!layout(host, n, L, insts, /*stencil_cache=*/false)) return set_error(AGD_STATUS_INVALID, "bad instance shape");
-    unsigned vmask = 0;
+    unsigned long long vmask = 0;
     const int rc = validate(host, insts, n, /*stencil_cache=*/false, &vmask);
     if (rc != AGD_STATUS_OK) return rc;
     if (L.total > kFixedScratchBytes)
@@ -1023,7 +1095,7 @@ __global__ void flow_kernel(Inst I, float *fvec, float *fwsum, float *fw, int *f
             hide[k] = hidden_bits<D>(A, wd0, xt, ev[k], [&](const int *y) { return bilevel_index<D, TL>(y, I.shape_o); });
         float v[NACT], fsh[2 * NACT];
         if (A.factor_radius2 > 0.f) {
-            factor_shifts<D, NACT, MODEL == AGD_MODEL_ISOTROPIC>(A, xt, ev, fsh);
+            factor_shifts<D, NACT, MODEL != AGD_MODEL_RIEMANN>(A, xt, ev, fsh);
         } else {
 #pragma unroll
             for (int k = 0; k < 2 * NACT; ++k) fsh[k] = 0.f;
@@ -1107,6 +1179,9 @@ static int flow_impl(const agd_instance *a, float *fvec, float *fwsum, float *fw
         case V_ISO3_4: flow_kernel<Tile<3, 4, 4, 4>, AGD_MODEL_ISOTROPIC><<<grid, wpb * 32, 0, st>>>(I, fvec, fwsum, fw, fidx); break;
         case V_RIEM3_4: flow_kernel<Tile<3, 4, 4, 4>, AGD_MODEL_RIEMANN><<<grid, wpb * 32, 0, st>>>(I, fvec, fwsum, fw, fidx); break;
         case V_RIEM2_16: flow_kernel<Tile<2, 16, 16, 1>, AGD_MODEL_RIEMANN><<<grid, wpb * 32, 0, st>>>(I, fvec, fwsum, fw, fidx); break;
+        case V_DIAG2_8: flow_kernel<Tile<2, 8, 8, 1>, AGD_MODEL_DIAGONAL><<<grid, wpb * 32, 0, st>>>(I, fvec, fwsum, fw, fidx); break;
+        case V_DIAG2_16: flow_kernel<Tile<2, 16, 16, 1>, AGD_MODEL_DIAGONAL><<<grid, wpb * 32, 0, st>>>(I, fvec, fwsum, fw, fidx); break;
+        case V_DIAG3_4: flow_kernel<Tile<3, 4, 4, 4>, AGD_MODEL_DIAGONAL><<<grid, wpb * 32, 0, st>>>(I, fvec, fwsum, fw, fidx); break;
         default: return set_error(AGD_STATUS_UNSUPPORTED, "model/tile shape not built");
     }
     const cudaError_t err = cudaGetLastError();
@@ -1234,6 +1309,28 @@ __global__ void prep_geom_kernel(Geo g, const float *metric, int bcast, int is_d
     float out[6];
     geom_at(g.nd, bcast ? metric : metric + flat * sd, is_dual, h, out);
     for (int c = 0; c < sd; ++c) geom[c * g.size_tot + n_t] = out[c];
+}
+
+// Diagonal model: the squared dual costs 1/(c_k h_k)^2 of metric.with_costs(h)
+// (or (d_k / h_k)^2 of dualMetric.with_speeds(h)) per axis, in float as the
+// reference forms them (_SetGeometry.py:134-135), +inf at padding.
+__global__ void prep_diag_kernel(Geo g, const float *costs, int bcast, int is_dual, double h0, double h1, double h2,
+                                 float *geom) {
+    const long long n_t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (n_t >= g.size_tot) return;
+    int x[3];
+    long long flat;
+    const bool in = grid_coords(g, n_t, x, flat);
+    const float h[3] = {(float)h0, (float)h1, (float)h2};
+    for (int k = 0; k < g.nd; ++k) {
+        float w = finf();
+        if (in) {
+            const float c = bcast ? costs[k] : costs[flat * g.nd + k];
+            const float v = is_dual ? c * (1.f / h[k]) : 1.f / (c * h[k]);
+            w = v * v;
+        }
+        geom[k * g.size_tot + n_t] = w;
+    }
 }
 
 // Seed bits: one 32-bit word (32 points) per thread, padding bits set.
@@ -1502,6 +1599,19 @@ int agd_prep_geom(int ndim, const int *shape, const int *shape_i, const float *m
         g, metric, broadcast, is_dual, grid_scales[0], grid_scales[1], ndim == 3 ? grid_scales[2] : 1.0, geom);
     const cudaError_t err = cudaGetLastError();
     return err == cudaSuccess ? AGD_STATUS_OK : set_cuda_error("prep_geom", err);
+}
+
+int agd_prep_geom_diagonal(int ndim, const int *shape, const int *shape_i, const float *costs, int broadcast,
+                           int is_dual, const double *grid_scales, float *geom, agd_stream_t stream) {
+    clear_error();
+    Geo g;
+    if (ndim < 1 || !geo_of(ndim, shape, shape_i, g) || !costs || !geom || !grid_scales)
+        return set_error(AGD_STATUS_INVALID, "agd_prep_geom_diagonal: bad arguments");
+    prep_diag_kernel<<<blocks_for(g.size_tot, 256), 256, 0, (cudaStream_t)stream>>>(
+        g, costs, broadcast, is_dual, grid_scales[0], ndim > 1 ? grid_scales[1] : 1.0, ndim > 2 ? grid_scales[2] : 1.0,
+        geom);
+    const cudaError_t err = cudaGetLastError();
+    return err == cudaSuccess ? AGD_STATUS_OK : set_cuda_error("prep_geom_diagonal", err);
 }
 
 int agd_block_expand(int ndim, const int *shape, const int *shape_i, int nplanes, const float *src, int src_broadcast,

@@ -24,15 +24,23 @@ enum Variant {
     V_ISO2_8_O2, V_ISO2_16_O2, V_RIEM2_8_O2, V_ISO3_4_O2, V_RIEM3_4_O2,
     // walls (Riemann; the Riemann variants above with multiprecision, factorisation
     // or second order read the wall bits themselves; Isotropic needs none)
-    V_RIEM2_8_W, V_RIEM2_16_W, V_RIEM3_4_W, V_COUNT
+    V_RIEM2_8_W, V_RIEM2_16_W, V_RIEM3_4_W,
+    // Diagonal: plain, multiprecision, factorisation, second order
+    V_DIAG2_8, V_DIAG2_16, V_DIAG3_4, V_DIAG2_8_MP, V_DIAG2_16_MP, V_DIAG3_4_MP,
+    V_DIAG2_8_F, V_DIAG2_16_F, V_DIAG3_4_F, V_DIAG2_8_O2, V_DIAG2_16_O2, V_DIAG3_4_O2, V_COUNT
 };
-constexpr unsigned kMpVariants = (1u << V_ISO2_8_MP) | (1u << V_ISO2_16_MP) | (1u << V_RIEM2_8_MP) |
-                                 (1u << V_ISO3_4_MP) | (1u << V_RIEM3_4_MP);
-constexpr unsigned kFactorVariants = (1u << V_ISO2_8_F) | (1u << V_ISO2_16_F) | (1u << V_RIEM2_8_F) |
-                                     (1u << V_ISO3_4_F) | (1u << V_RIEM3_4_F);
-constexpr unsigned kOrder2Variants = (1u << V_ISO2_8_O2) | (1u << V_ISO2_16_O2) | (1u << V_RIEM2_8_O2) |
-                                     (1u << V_ISO3_4_O2) | (1u << V_RIEM3_4_O2);
-constexpr unsigned kWallVariants = (1u << V_RIEM2_8_W) | (1u << V_RIEM2_16_W) | (1u << V_RIEM3_4_W);
+static_assert(V_COUNT <= 64, "variant masks are 64-bit");
+constexpr unsigned long long kMpVariants = (1ull << V_ISO2_8_MP) | (1ull << V_ISO2_16_MP) | (1ull << V_RIEM2_8_MP) |
+                                 (1ull << V_ISO3_4_MP) | (1ull << V_RIEM3_4_MP) | (1ull << V_DIAG2_8_MP) |
+                                 (1ull << V_DIAG2_16_MP) | (1ull << V_DIAG3_4_MP);
+constexpr unsigned long long kFactorVariants = (1ull << V_ISO2_8_F) | (1ull << V_ISO2_16_F) | (1ull << V_RIEM2_8_F) |
+                                     (1ull << V_ISO3_4_F) | (1ull << V_RIEM3_4_F) | (1ull << V_DIAG2_8_F) |
+                                     (1ull << V_DIAG2_16_F) | (1ull << V_DIAG3_4_F);
+constexpr unsigned long long kOrder2Variants = (1ull << V_ISO2_8_O2) | (1ull << V_ISO2_16_O2) | (1ull << V_RIEM2_8_O2) |
+                                     (1ull << V_ISO3_4_O2) | (1ull << V_RIEM3_4_O2) | (1ull << V_DIAG2_8_O2) |
+                                     (1ull << V_DIAG2_16_O2) | (1ull << V_DIAG3_4_O2);
+constexpr unsigned long long kWallVariants = (1ull << V_RIEM2_8_W) | (1ull << V_RIEM2_16_W) | (1ull << V_RIEM3_4_W);
+constexpr unsigned long long kDiagVariants = ((1ull << (V_DIAG3_4_O2 + 1)) - 1) & ~((1ull << V_DIAG2_8) - 1);
 
 static int base_variant_of(const agd_instance &a);
 
@@ -46,6 +54,9 @@ static int variant_of(const agd_instance &a) {
             case V_RIEM2_8: return V_RIEM2_8_O2;
             case V_ISO3_4: return V_ISO3_4_O2;
             case V_RIEM3_4: return V_RIEM3_4_O2;
+            case V_DIAG2_8: return V_DIAG2_8_O2;
+            case V_DIAG2_16: return V_DIAG2_16_O2;
+            case V_DIAG3_4: return V_DIAG3_4_O2;
             default: return -1;
         }
     }
@@ -57,6 +68,9 @@ static int variant_of(const agd_instance &a) {
             case V_RIEM2_8: return V_RIEM2_8_F;
             case V_ISO3_4: return V_ISO3_4_F;
             case V_RIEM3_4: return V_RIEM3_4_F;
+            case V_DIAG2_8: return V_DIAG2_8_F;
+            case V_DIAG2_16: return V_DIAG2_16_F;
+            case V_DIAG3_4: return V_DIAG3_4_F;
             default: return -1;
         }
     }
@@ -78,6 +92,9 @@ static int variant_of(const agd_instance &a) {
         case V_RIEM2_8: return V_RIEM2_8_MP;
         case V_ISO3_4: return V_ISO3_4_MP;
         case V_RIEM3_4: return V_RIEM3_4_MP;
+        case V_DIAG2_8: return V_DIAG2_8_MP;
+        case V_DIAG2_16: return V_DIAG2_16_MP;
+        case V_DIAG3_4: return V_DIAG3_4_MP;
         default: return -1;  // no multiprecision build of this tile shape
     }
 }
@@ -89,8 +106,12 @@ static int base_variant_of(const agd_instance &a) {
         if (a.model == AGD_MODEL_RIEMANN && a.shape_i[0] == 16 && a.shape_i[1] == 16) return V_RIEM2_16;
         if (a.model == AGD_MODEL_ISOTROPIC && a.shape_i[0] == 8 && a.shape_i[1] == 8) return V_ISO2_8;
         if (a.model == AGD_MODEL_ISOTROPIC && a.shape_i[0] == 16 && a.shape_i[1] == 16) return V_ISO2_16;
+        if (a.model == AGD_MODEL_DIAGONAL && a.shape_i[0] == 8 && a.shape_i[1] == 8) return V_DIAG2_8;
+        if (a.model == AGD_MODEL_DIAGONAL && a.shape_i[0] == 16 && a.shape_i[1] == 16) return V_DIAG2_16;
     } else if (a.ndim == 3 && a.shape_i[0] == 4 && a.shape_i[1] == 4 && a.shape_i[2] == 4) {
-        return a.model == AGD_MODEL_RIEMANN ? V_RIEM3_4 : V_ISO3_4;
+        if (a.model == AGD_MODEL_RIEMANN) return V_RIEM3_4;
+        if (a.model == AGD_MODEL_ISOTROPIC) return V_ISO3_4;
+        if (a.model == AGD_MODEL_DIAGONAL) return V_DIAG3_4;
     }
     return -1;
 }

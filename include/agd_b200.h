@@ -37,7 +37,9 @@ enum agd_status {
     AGD_STATUS_UNSUPPORTED = 32   /* tile shape / model combination not built */
 };
 
-enum agd_model { AGD_MODEL_ISOTROPIC = 0, AGD_MODEL_RIEMANN = 1 };
+/* Diagonal: the Isotropic scheme (unit offsets) with weights per point and
+ * axis, the squared dual costs (Isotropic_.h:32-36, _SetGeometry.py:134-135). */
+enum agd_model { AGD_MODEL_ISOTROPIC = 0, AGD_MODEL_RIEMANN = 1, AGD_MODEL_DIAGONAL = 2 };
 
 /* One eikonal problem.  Mirrors what the reference's Interface prepares for its
  * `Update` kernel: traits (shape_i, niter_i, fim_front_width), module constants
@@ -62,7 +64,8 @@ typedef struct agd_instance {
     int32_t *valuesq;   /* tile layout, multiprecision integer part (or NULL) */
     float *values_next; /* multiprecision: second buffers of the double-buffered */
     int32_t *valuesq_next; /*  iterations (valuesNext, valuesqNext of _SetArgs.py:171-177) */
-    const float *geom;  /* Riemann: dual metric, symdim planes, tile layout (else NULL) */
+    const float *geom;  /* Riemann: dual metric, symdim planes; Diagonal: squared dual
+                           costs 1/(c_k h_k)^2, ndim planes; tile layout (Isotropic: NULL) */
     const float *rhs;   /* tile layout: cost, seed values at seeds, +inf padding */
     const uint8_t *seedbits; /* tile layout bits, little endian, padding bits set;
                                 4-byte aligned */
@@ -173,6 +176,14 @@ int agd_eikonal_solve_fixed_scratch(const agd_instance *inst, int n, agd_stats *
  * with broadcast != 0 a single (symdim,) tensor for the whole grid. */
 int agd_prep_geom(int ndim, const int *shape, const int *shape_i, const float *metric, int broadcast,
                   int is_dual, const double *grid_scales, float *geom, agd_stream_t stream);
+
+/* Diagonal model: the squared dual costs, ndim planes in tile layout padded
+ * with +inf: 1/(c_k h_k)^2 of metric.with_costs(gridScales), or with is_dual
+ * (d_k / h_k)^2 of dualMetric.with_speeds(gridScales) (_SetGeometry.py:134-135).
+ * costs: grid layout (*shape, ndim) HFM order; with broadcast != 0 one (ndim,)
+ * vector for the whole grid. */
+int agd_prep_geom_diagonal(int ndim, const int *shape, const int *shape_i, const float *costs, int broadcast,
+                           int is_dual, const double *grid_scales, float *geom, agd_stream_t stream);
 
 /* Grid layout -> tile layout for `nplanes` planes, padding with `pad`
  * (fd.block_expand).  src_broadcast != 0: src holds one value per plane. */

@@ -131,13 +131,13 @@ void sort_order(const T *v, int *o, int n) {
 // -------------------------------------------------------------- problem ---
 template <class T>
 struct Problem {
-    int D = 2, model = 0;  // model 0: isotropic, 1: Riemann
+    int D = 2, model = 0;  // model 0: isotropic, 1: Riemann, 2: diagonal
     int shape[3] = {1, 1, 1}, shape_i[3] = {1, 1, 1}, shape_o[3] = {1, 1, 1};
     int size_i = 1, size_o = 1;
     long size = 1;
     int nact = 2;
     T iso_w[3] = {0, 0, 0};
-    const float *geom = nullptr;  // dual metric planes, grid layout
+    const float *geom = nullptr;  // dual metric planes (Riemann), squared dual costs (diagonal); grid layout
     const float *rhs = nullptr;
     const unsigned char *seed = nullptr;
     // Source factorisation: within fact_r2 (squared, index units) of fact_origin,
@@ -178,7 +178,7 @@ struct Problem {
     }
 
     T scal_fact(const T *x, const T *y) const {
-        if (model == 0) {
+        if (model != 1) {
             T r = 0;
             for (int i = 0; i < D; ++i) r += fact_m[i] * x[i] * y[i];
             return r;
@@ -225,7 +225,7 @@ struct Problem {
             size_o *= shape_o[k];
             size *= shape[k];
         }
-        nact = model == 0 ? D : D * (D + 1) / 2;
+        nact = model == 1 ? D * (D + 1) / 2 : D;
     }
     long flat(const int *x) const {
         long n = 0;
@@ -239,9 +239,9 @@ struct Problem {
     }
     // Stencil at grid point n: weights w[nact], offsets e[nact][D].
     void stencil(long n, T *w, int (*e)[3]) const {
-        if (model == 0) {
+        if (model != 1) {  // unit offsets; weights h^-2 (isotropic) or per point (diagonal, Isotropic_.h:32-36)
             for (int k = 0; k < D; ++k) {
-                w[k] = iso_w[k];
+                w[k] = model == 0 ? iso_w[k] : T(geom[k * size + n]);
                 for (int c = 0; c < D; ++c) e[k][c] = (c == k);
             }
             return;

@@ -26,6 +26,8 @@ DEFAULT_TRAITS = {  # agd/Eikonal/HFM_CUDA/kernel_traits.py:61-88
     "Riemann3": ((4, 4, 4), 4, 6),
     "Isotropic2": ((16, 16), 16, 4),
     "Isotropic3": ((4, 4, 4), 8, 4),
+    "Diagonal2": ((16, 16), 16, 4),
+    "Diagonal3": ((4, 4, 4), 8, 4),
 }
 STOP_CODES = ["Continue", "AtSeed", "InWall", "Stationnary", "PastSeed", "VanishingFlow"]
 
@@ -114,6 +116,7 @@ def prepare(case):
     pr.model = str(case["model"])
     pr.ndim = int(pr.model[-1])
     pr.riemann = pr.model.startswith("Riemann")
+    pr.diagonal = pr.model.startswith("Diagonal")
     pr.shape = tuple(int(s) for s in np.asarray(case["dims"]))
     pr.h = np.broadcast_to(np.asarray(case.get("gridScales", case.get("gridScale")), np.float32), (pr.ndim,)).copy()
     pr.origin = np.asarray(case.get("origin", np.zeros(pr.ndim)), np.float32)
@@ -125,6 +128,10 @@ def prepare(case):
     pr.shape_i, pr.niter_i, pr.front = tuple(si), niter, int(case.get("fim_front_width", front))
     cost = np.broadcast_to(np.asarray(case.get("cost", 1.0), np.float32), pr.shape).astype(np.float32)
     pr.geom = dual_metric_flat(case["metric"], pr.h) if pr.riemann else None
+    if pr.diagonal:  # squared dual costs 1 / (c h)^2, float32 (_SetGeometry.py:134-135)
+        costs = np.moveaxis(np.broadcast_to(np.asarray(case["metric"], np.float32), pr.shape + (pr.ndim,)), -1, 0)
+        pr.geom = np.ascontiguousarray((np.float32(1) / (costs * pr.h.reshape((-1,) + (1,) * pr.ndim))) ** 2,
+                                       np.float32)
     res = np.finfo(np.float32).resolution
     pr.atol = float(np.float32(np.nanmean(cost) * res * 5.0)) if "atol" not in case else float(case["atol"])
     pr.rtol = float(np.float32(res * 5.0)) if "rtol" not in case else float(case["rtol"])
@@ -160,7 +167,7 @@ def prepare(case):
         mask[pr.walls] = 1
         rhs[pr.walls] = np.inf
     pr.rhs, pr.seed_mask = rhs, mask
-    pr.iso_w = (pr.h.astype(np.float64) ** -2) if not pr.riemann else None
+    pr.iso_w = (pr.h.astype(np.float64) ** -2) if not (pr.riemann or pr.diagonal) else None
     if pr.iso_w is not None:
         pr.iso_w = np.asarray(pr.h.astype(np.float32) ** -2, np.float64)
     return pr
@@ -181,6 +188,11 @@ def _cost_metric(pr, case, cost):
             for q, (i, j) in enumerate(tri):
                 M[i, j] = M[j, i] = mf[tuple(p)][q]
             return c[tuple(p)] ** 2 * M * np.outer(h, h)
+    elif pr.diagonal:
+        mc = np.broadcast_to(np.asarray(case["metric"], np.float64), tuple(pr.shape) + (nd,))
+
+        def cm(p):
+            return np.diag((mc[tuple(p)] * c[tuple(p)] * h) ** 2)
     else:
         def cm(p):
             return np.diag((c[tuple(p)] * h) ** 2)
@@ -189,7 +201,8 @@ def _cost_metric(pr, case, cost):
 
 def _seed_metric(pr, case, cost, seed):
     """The cost metric at a seed (continuous index coordinates), multilinearly
-    interpolated: its entries (Riemann), or the costs c*h (Isotropic)."""
+    interpolated: its entries (Riemann), or the costs c*h per axis (Isotropic,
+    Diagonal)."""
     nd = pr.ndim
     shape = np.array(pr.shape)
     cm = _cost_metric(pr, case, cost)
@@ -197,13 +210,13 @@ def _seed_metric(pr, case, cost, seed):
     lo = np.clip(np.floor(seed).astype(int), 0, shape - 1)
     frac = np.clip(seed - lo, 0.0, 1.0)
     m0 = np.zeros((nd, nd))
-    c0 = 0.0
+    c0 = np.zeros(nd)
     for bits in np.ndindex(*([2] * nd)):
         w = np.prod([f if b else 1.0 - f for b, f in zip(bits, frac)])
         p = np.minimum(lo + np.array(bits), shape - 1)
         m0 += w * cm(p)
-        c0 += w * c[tuple(p)]
-    return m0 if pr.riemann else np.diag((c0 * pr.h.astype(np.float64)) ** 2)
+        c0 += w * np.sqrt(np.diag(cm(p)))  # the costs c*h per axis
+    return m0 if pr.riemann else np.diag(c0 ** 2)
 
 
 def _spread_seed(pr, case, cost, seed, seed_value, r):
@@ -255,7 +268,7 @@ def eikonal(pr, dtype=np.float32, values=None, nthreads=1, flow=False, nitermax=
         met = np.zeros(6)
         met[: len(fac[2])] = fac[2]
         L.agdo_set_factor(ctypes.c_double(fac[0]), _p(org), _p(met))
-    niter = L.agdo_eikonal(int(dtype == np.float64), pr.ndim, 1 if pr.riemann else 0,
+    niter = L.agdo_eikonal(int(dtype == np.float64), pr.ndim, 1 if pr.riemann else (2 if pr.diagonal else 0),
                            (ctypes.c_int * pr.ndim)(*pr.shape), (ctypes.c_int * pr.ndim)(*pr.shape_i),
                            pr.niter_i, pr.front, _p(iso), _p(geom), _p(np.ascontiguousarray(pr.rhs)),
                            _p(np.ascontiguousarray(pr.seed_mask)), _p(u), ctypes.c_double(pr.atol),

@@ -4,7 +4,8 @@
 // pin the oracle; never linked by the product.
 //
 // Compile-time configuration (set by oracle/ref_emul/Makefile):
-//   AGDREF_ISO (0|1), AGDREF_NDIM, AGDREF_SHAPE_I (comma list), AGDREF_SIZE_I,
+//   AGDREF_ISO (0|1), AGDREF_DIAG (0|1: the Diagonal model, Isotropic_.h with
+//   per-point squared dual costs as geometry, _SetGeometry.py:134-135), AGDREF_NDIM, AGDREF_SHAPE_I (comma list), AGDREF_SIZE_I,
 //   AGDREF_LOG2_SIZE_I, AGDREF_NITER_I, AGDREF_MULTIP (0|1), AGDREF_FLOW (0|1),
 //   AGDREF_FACTOR (0|1, source factorisation, factor_macro of _Kernel.py:47-49),
 //   AGDREF_ORDER2 (0|1, second order scheme, order2_macro of _Kernel.py:51-54),
@@ -63,8 +64,14 @@ const int niter_i = AGDREF_FLOW ? 1 : AGDREF_NITER_I;
 #define periodic_macro false
 #define isotropic_macro AGDREF_ISO
 #define walls_macro AGDREF_WALLS
+#ifndef AGDREF_DIAG
+#define AGDREF_DIAG 0
+#endif
 #if AGDREF_ISO
 #define geom_indep_macro AGDREF_NDIM
+#elif AGDREF_DIAG
+#define geom_indep_macro 0
+#define geom_size_macro AGDREF_NDIM
 #else
 #define geom_indep_macro 0
 #define geom_size_macro ((AGDREF_NDIM * (AGDREF_NDIM + 1)) / 2)
@@ -75,7 +82,7 @@ const int log2_size_i = AGDREF_LOG2_SIZE_I;
 
 // The reference's module constant `atol` would collide with the C library's atol().
 #define atol agdref_atol
-#if AGDREF_ISO
+#if AGDREF_ISO || AGDREF_DIAG
 #include "Isotropic_.h"
 #else
 // Riemann_.h includes EuclideanFactor.h inside a FACTOR(...) macro argument, which
@@ -276,7 +283,7 @@ int agdref_flow(const int *shape, const float *iso_w, float mstep, float mmax, f
 
 // Direct access to the reference's per-point Selling decomposition
 // (Geometry2.h:21-48 / Geometry3.h:22-58, via Riemann_.h:23-29) for golden vectors.
-#if !AGDREF_ISO && !AGDREF_FLOW && !AGDREF_MULTIP
+#if !AGDREF_ISO && !AGDREF_DIAG && !AGDREF_FLOW && !AGDREF_MULTIP
 void agdref_selling(const float *m, int n, float *w, int *e) {
     for (int p = 0; p < n; ++p) {
         Scalar wl[symdim];

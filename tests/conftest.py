@@ -38,6 +38,7 @@ RADIUS_CASES = ["riem2_radius", "iso2_radius"]  # seeds spread over a radius (va
 FACTOR_CASES = ["riem2_factor", "iso2_factor"]  # source factorisation (factoringRadius)
 ORDER2_CASES = ["riem2_order2", "iso2_order2", "riem3_order2"]  # second order scheme (order: 2)
 WALL_CASES = ["riem2_walls", "iso2_walls", "riem3_walls"]  # obstacles (walls, wallDistBound)
+DIAG_CASES = ["diag2", "diag2_factor", "diag2_order2", "diag2_walls", "diag3"]  # Diagonal2/3 models
 
 
 @pytest.fixture(params=CASES)

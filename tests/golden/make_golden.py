@@ -80,6 +80,9 @@ MODELS = {
     "Isotropic3": dict(tag="iso3", shape_i=(4, 4, 4), niter_i=8, front=4),
     "Riemann2": dict(tag="riem2", shape_i=(8, 8), niter_i=8, front=4),
     "Riemann3": dict(tag="riem3", shape_i=(4, 4, 4), niter_i=4, front=6),
+    # the linear (AD) kernels depend on the tile shape only: the Isotropic builds serve
+    "Diagonal2": dict(tag="diag2", lin="iso2", shape_i=(16, 16), niter_i=16, front=4),
+    "Diagonal3": dict(tag="diag3", lin="iso3", shape_i=(4, 4, 4), niter_i=8, front=4),
 }
 
 
@@ -120,6 +123,10 @@ class RefPipeline:
             metric = self.Metrics.Riemann.from_HFM(np.asarray(c["metric"], np.float32))
             dual = metric.with_costs(self.h).dual()
             self.geom = self.bexp(dual.flatten().astype(np.float32), np.inf)
+        elif self.model.startswith("Diagonal"):  # geom = dualMetric.costs**2 (_SetGeometry.py:134-135)
+            metric = self.Metrics.Diagonal.from_HFM(np.asarray(c["metric"], np.float32))
+            dual = metric.with_costs(self.h).dual()
+            self.geom = self.bexp((dual.costs ** 2).astype(np.float32), np.inf)
         else:
             self.geom = np.zeros(1, np.float32)
         float_res = np.finfo(np.float32).resolution
@@ -192,6 +199,8 @@ class RefPipeline:
         nd = self.ndim
         if self.model.startswith("Riemann"):
             metric = self.Metrics.Riemann.from_HFM(np.asarray(self.c["metric"], np.float64))
+        elif self.model.startswith("Diagonal"):
+            metric = self.Metrics.Diagonal.from_HFM(np.asarray(self.c["metric"], np.float64))
         else:
             metric = self.Metrics.Diagonal(np.ones(nd))
         cm = metric.with_costs(self.h.astype(np.float64)).with_cost(np.asarray(cost, np.float64))
@@ -257,7 +266,7 @@ class RefPipeline:
         L = lib(f"libagdref_flow_{self.md['tag']}{'f' if self.factor else ''}{self.o2tag}.so")
         self.set_factor(L)
         nd, st = self.ndim, self.size_o * self.size_i
-        nact = self.ndim if self.model.startswith("Iso") else self.ndim * (self.ndim + 1) // 2
+        nact = self.ndim if not self.model.startswith("Riemann") else self.ndim * (self.ndim + 1) // 2
         self.nact = nact
         oi = self.shape_o + self.shape_i
         self.fw = np.empty((nact,) + oi, np.float32)
@@ -339,7 +348,7 @@ class RefPipeline:
         idxT, wT = self.graph_reverse(indices, weights, invalid)
         rhs = self.bexp(np.moveaxis(sens, -1, 0).astype(np.float32), np.nan)
         rhs = np.ascontiguousarray(rhs.astype(np.float32))
-        tag = self.md["tag"]
+        tag = self.md.get("lin", self.md["tag"])
         L = lib(f"libagdref_lin_{tag}_r.so")
         L.agdref_nindex.restype = ctypes.c_int
         nidx = L.agdref_nindex()
@@ -384,7 +393,7 @@ class RefPipeline:
         for j in range(n_ad):
             grad[j][pos] = seed_var[j]
         rhs_grid = np.where(self.seedTags, grad, grad * value).astype(np.float32)
-        L = lib(f"libagdref_lin_{self.md['tag']}_f.so")
+        L = lib(f"libagdref_lin_{self.md.get('lin', self.md['tag'])}_f.so")
         L.agdref_nindex.restype = ctypes.c_int
         assert L.agdref_nindex() == len(indices)
         float_res = np.finfo(np.float32).resolution
@@ -569,6 +578,47 @@ def make_cases():
         cv[..., 1].reshape(-1)[rng.choice(int(np.prod(shp)), 3, replace=False)] = 1.0
         cc["costVariation"] = cv
         cc["seedValueVariation"] = np.ascontiguousarray(rng.uniform(-1, 1, (len(cc["seeds"]), 2)).T).astype(np.float32)
+    # Diagonal models (axis costs per point), with their own random stream
+    rng = np.random.default_rng(4321)
+    sh = (70, 53)
+    c = dict(model="Diagonal2", **rect(sh, 1.0 / 70))
+    c["metric"] = np.stack([np.exp(0.4 * smooth_noise(rng, sh, 3.0)), 2.0 * np.exp(0.4 * smooth_noise(rng, sh, 3.0))],
+                           -1).astype(np.float32)  # HFM layout (*shape, ndim): the costs per axis
+    c["cost"] = np.exp(0.3 * smooth_noise(rng, sh, 4.0)).astype(np.float32)
+    c["seeds"] = np.array([[0.31, 0.22], [0.72, 0.55]], np.float32)
+    c["seedValues"] = np.array([0.0, 0.05], np.float32)
+    c["tips"] = rng.uniform(0.05, 0.7, (5, 2)).astype(np.float32)
+    sens = np.zeros(sh + (1,), np.float32)
+    sens.reshape(-1)[rng.choice(int(np.prod(sh)), 5, replace=False)] = 1.0
+    c["sensitivity"] = sens
+    cases["diag2"] = c
+    c = {k: v for k, v in cases["diag2"].items() if k not in ("sensitivity", "seedValues", "tips")}
+    c["seeds"] = np.array([[0.37, 0.3]], np.float32)
+    c["factoringRadius"] = 10.0
+    cases["diag2_factor"] = c
+    c = {k: v for k, v in cases["diag2"].items() if k != "sensitivity"}
+    c["order"] = 2
+    cases["diag2_order2"] = c
+    c = {k: v for k, v in cases["diag2"].items() if k != "sensitivity"}
+    w = np.zeros(sh, bool)
+    w[10:65, 26] = True
+    w[40:43, 26] = False
+    c["walls"] = w
+    cases["diag2_walls"] = c
+    sh = (21, 18, 23)
+    c = dict(model="Diagonal3", **rect(sh, 1.0 / 21))
+    c["metric"] = np.stack([np.exp(0.4 * smooth_noise(rng, sh, 2.0)) for _ in range(3)], -1).astype(np.float32)
+    c["seeds"] = np.array([[0.5, 0.4, 0.5]], np.float32)
+    c["tips"] = rng.uniform(0.05, 0.8, (3, 3)).astype(np.float32)
+    sens = np.zeros(sh + (1,), np.float32)
+    sens.reshape(-1)[rng.choice(int(np.prod(sh)), 5, replace=False)] = 1.0
+    c["sensitivity"] = sens
+    cases["diag3"] = c
+    cc = cases["diag2"]
+    cv = np.stack([smooth_noise(rng, sh2 := (70, 53), 2.0), np.zeros(sh2)], -1).astype(np.float32)
+    cv[..., 1].reshape(-1)[rng.choice(70 * 53, 3, replace=False)] = 1.0
+    cc["costVariation"] = cv
+    cc["seedValueVariation"] = np.ascontiguousarray(rng.uniform(-1, 1, (2, 2)).T).astype(np.float32)
     return cases
 
 

@@ -8,7 +8,7 @@ import numpy as np
 import pytest
 
 from oracle import oracle as O
-from conftest import load_case, CASES, RADIUS_CASES, FACTOR_CASES, ORDER2_CASES, WALL_CASES
+from conftest import load_case, CASES, DIAG_CASES, RADIUS_CASES, FACTOR_CASES, ORDER2_CASES, WALL_CASES
 
 REL = 1e-5  # parity bar for float32 values
 
@@ -22,7 +22,7 @@ def _geodesic_split(out):
     return res
 
 
-@pytest.mark.parametrize("name", CASES + RADIUS_CASES + FACTOR_CASES + ORDER2_CASES + WALL_CASES)
+@pytest.mark.parametrize("name", CASES + RADIUS_CASES + FACTOR_CASES + ORDER2_CASES + WALL_CASES + DIAG_CASES)
 @pytest.mark.parametrize("dtype", [np.float32, np.float64])
 def test_values(name, dtype):
     case, ref = load_case(name)
@@ -38,7 +38,7 @@ def test_values(name, dtype):
 
 
 @pytest.mark.parametrize("name", [c for c in CASES if c != "ad_notebook"] + ["riem2_factor"] + ORDER2_CASES +
-                         ["riem2_walls", "riem3_walls", "iso2_walls"])
+                         ["riem2_walls", "riem3_walls", "iso2_walls", "diag2", "diag3", "diag2_walls", "diag2_order2"])
 def test_geodesics(name):
     case, ref = load_case(name)
     r = O.run(case, np.float32)
@@ -48,7 +48,7 @@ def test_geodesics(name):
         assert np.abs(p - g).max() < 1e-4 * np.abs(g).max()
 
 
-@pytest.mark.parametrize("name", ["iso2", "riem2", "iso3", "riem3", "ad_notebook"])
+@pytest.mark.parametrize("name", ["iso2", "riem2", "iso3", "riem3", "ad_notebook", "diag2", "diag3"])
 def test_reverse_sensitivity(name):
     case, ref = load_case(name)
     r = O.run(case, np.float64)
@@ -125,7 +125,7 @@ def test_reference_scheme_meets_the_parity_criteria(seed):
     assert rel_err(O.run(dict(case, **TIGHT), np.float32, nthreads=4)["values"], exact) < TIGHT_REL
 
 
-@pytest.mark.parametrize("name", ["iso2", "riem2", "riem3"])
+@pytest.mark.parametrize("name", ["iso2", "riem2", "riem3", "diag2"])
 def test_forward_ad_vs_reference(name):
     """valueVariation of the oracle (float64, exact solve of the forward
     linearisation) against the reference's forward AD (its linear kernel, float32)."""
@@ -173,7 +173,7 @@ def test_wall_visibility_matters():
     assert np.abs(u[fin] - ref["values"][fin]).max() > 1e-2
 
 
-@pytest.mark.parametrize("name", ["iso2", "iso3", "riem2", "riem3", "riem2_walls"])
+@pytest.mark.parametrize("name", ["iso2", "iso3", "riem2", "riem3", "riem2_walls", "diag2", "diag3"])
 def test_active_neighs(name):
     """exportActiveNeighs: the bits of the positive flow weights equal the
     reference's flow_weightpos (cuda/Update.h:187,206) point for point."""
