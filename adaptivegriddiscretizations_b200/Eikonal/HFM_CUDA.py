@@ -4,7 +4,7 @@
 Interface class of _Interface.py:23-174: every key is read through GetValue,
 which records help texts, defaults, used and unused keys in
 hfmOut['keys']; the same keys, defaults and errors as the reference are used
-for the Isotropic2/3, Diagonal2/3 and Riemann2/3 models.  The work is done by
+for the Isotropic2/3, Diagonal2/3, Riemann2/3 and Rander2/3 models.  The work is done by
 libagd_b200.so through the C ABI of include/agd_b200.h:
   SetGeometry/SetArgs  -> agd_prep_geom(_diagonal), agd_block_expand, agd_prep_seeds,
                           agd_prep_walls
@@ -33,6 +33,8 @@ DEFAULT_TRAITS = {
     "Isotropic3": ((4, 4, 4), 8, 4),
     "Diagonal2": ((16, 16), 16, 4),
     "Diagonal3": ((4, 4, 4), 8, 4),
+    "Rander2": ((8, 8), 12, 8),
+    "Rander3": ((4, 4, 4), 8, 8),
 }
 SUPPORTED_TILES = {2: {(8, 8), (16, 16)}, 3: {(4, 4, 4)}}
 GEODESIC_CODES = ["Continue", "AtSeed", "InWall", "Stationnary", "PastSeed", "VanishingFlow"]
@@ -366,6 +368,26 @@ class Interface:
             hs = (ctypes.c_double * 3)(*[float(x) for x in self.h], *([1.0] * (3 - self.ndim)))
             _lib.check(L.agd_prep_geom(self.ndim, self.c_shape, self.c_shape_i, _lib.ptr(self._metric_flat), bcast,
                                        is_dual, hs, _lib.ptr(self.geom), self.stream), "prep_geom")
+        elif self.model_ == "Rander":  # geom = metric.flatten(inverse_m=True) (_SetGeometry.py:138-139)
+            metric = self.GetValue("metric", default=None, verbosity=3, help="Metric of the minimal path model")
+            dual = self.GetValue("dualMetric", default=None, verbosity=3,
+                                 help="Dual metric of the minimal path model")
+            if metric is None and dual is None:
+                raise ValueError("Missing value for key metric")
+            src, is_dual = (metric, 0) if metric is not None else (dual, 1)
+            self._metric_is_dual = bool(is_dual)
+            flat = _rander_hfm(src, self.ndim)
+            bcast = 1 if flat.dim() == 1 else 0
+            if not bcast and tuple(flat.shape[:-1]) != self.shape:
+                raise ValueError("Inconsistent dimensions for geometry data. "
+                                 "It should match (the last coordinates of) domain shape.")
+            self._metric_flat = flat.contiguous()
+            symdim = self.ndim * (self.ndim + 1) // 2
+            self.geom = torch.empty((symdim + self.ndim) * self.size_tot, dtype=torch.float32, device="cuda")
+            hs = (ctypes.c_double * 3)(*[float(x) for x in self.h], *([1.0] * (3 - self.ndim)))
+            _lib.check(L.agd_prep_geom_rander(self.ndim, self.c_shape, self.c_shape_i, _lib.ptr(self._metric_flat),
+                                              bcast, is_dual, hs, _lib.ptr(self.geom), self.stream),
+                       "prep_geom_rander")
         elif self.model_ == "Diagonal":  # geom = dualMetric.costs**2 (_SetGeometry.py:134-135)
             metric = self.GetValue("metric", default=None, verbosity=3, help="Metric of the minimal path model")
             dual = self.GetValue("dualMetric", default=None, verbosity=3,
@@ -507,7 +529,7 @@ class Interface:
                 raise ValueError("factoringRadius needs a single seed (as the reference)")
             m0 = self._seed_metric(np.asarray(ci[0], np.float64))
             nd = self.ndim
-            fm = ([m0[i, j] for i in range(nd) for j in range(i + 1)] if self.model_ == "Riemann"
+            fm = ([m0[i, j] for i in range(nd) for j in range(i + 1)] if self.model_ in ("Riemann", "Rander")
                   else list(np.diag(m0)))
             self.factor = (self.factoringRadius ** 2, np.asarray(ci[0], np.float64), np.asarray(fm, np.float64))
         if seedRadius:
@@ -538,14 +560,49 @@ class Interface:
                                         self.wallDistBound, _lib.ptr(self.wall_dist), _lib.ptr(tmp),
                                         _lib.ptr(self.rhs_t), _lib.ptr(self.seedbits), self.stream), "walls")
 
-    def _cost_metrics(self, pts):
+    def _rander_parts(self, pts=None):
+        """Rander metric (M, w) with the grid scales applied (index units, no
+        cost), float64 host arrays, at the grid points pts (k, ndim) or at every
+        point (pts None): the dual metric is turned into the metric first."""
+        nd = self.ndim
+        sd = nd * (nd + 1) // 2
+        fm = self._metric_flat.reshape(-1, sd + nd)
+        if pts is not None:
+            flat = torch.as_tensor(np.ravel_multi_index(np.asarray(pts).T, self.shape), device="cuda")
+            fm = fm[flat] if fm.shape[0] > 1 else fm.expand(len(pts), sd + nd)
+        fm = fm.double().cpu().numpy()
+        M = np.zeros((len(fm), nd, nd))
+        k = 0
+        for i in range(nd):
+            for j in range(i + 1):
+                M[:, i, j] = M[:, j, i] = fm[:, k]
+                k += 1
+        w = fm[:, sd:]
+        h = self.h.astype(np.float64)
+        if self._metric_is_dual:  # dualMetric.with_speeds(h), then dual() (rander.py:35-39)
+            M, w = M / np.outer(h, h), w / h
+            s_ = np.linalg.inv(M - w[:, :, None] * w[:, None, :])
+            om = np.einsum("kij,kj->ki", s_, w)
+            return (1 + (w * om).sum(-1))[:, None, None] * s_, -om
+        return M * np.outer(h, h), w * h
+
+    def _cost_metrics(self, pts, drift=False):
         """The metric with the grid scales and the cost applied (index units;
         Interface.CostMetric, _Interface.py:202-211) at the grid points pts
-        (k, ndim): (k, ndim, ndim) float64, and the cost there."""
+        (k, ndim): (k, ndim, ndim) float64 (the quadratic part for Rander), and
+        the cost there; with drift, also the Rander drift (k, ndim) (zero for
+        the other models)."""
         nd = self.ndim
         flat = torch.as_tensor(np.ravel_multi_index(np.asarray(pts).T, self.shape), device="cuda")
         cost = self.cost.reshape(-1)[flat] if self.cost.dim() else self.cost.expand(len(pts))
         cost = cost.double().cpu().numpy()
+        if self.model_ == "Rander":  # Rander.with_cost: (c^2 M, c w)
+            M, w = self._rander_parts(pts)
+            M = cost[:, None, None] ** 2 * M
+            return (M, cost, cost[:, None] * w) if drift else (M, cost)
+        if drift:
+            M, c = self._cost_metrics(pts)
+            return M, c, np.zeros((len(pts), nd))
         h = self.h.astype(np.float64)
         if self.model_ == "Isotropic":  # Diagonal(ones).with_costs(h).with_cost(cost)
             return np.einsum("ki,ij->kij", (cost[:, None] * h) ** 2, np.eye(nd)), cost
@@ -581,10 +638,23 @@ class Interface:
         frac = np.clip(seed - lo, 0.0, 1.0)
         wc = np.prod(np.where(bits == 1, frac, 1.0 - frac), axis=1)
         m, cost = self._cost_metrics(corners)
-        if self.model_ == "Riemann":
+        if self.model_ in ("Riemann", "Rander"):
             return np.tensordot(wc, m, axes=1)
         # diagonal metrics: the costs c*h per axis are interpolated, then squared
         return np.diag(np.dot(wc, np.sqrt(np.diagonal(m, axis1=1, axis2=2))) ** 2)
+
+    def _seed_drift(self, seed):
+        """The drift of the cost metric at a seed, interpolated multilinearly
+        (zero for the models without drift)."""
+        import itertools
+        nd = self.ndim
+        shape = np.array(self.shape)
+        lo = np.clip(np.floor(seed).astype(np.int64), 0, shape - 1)
+        bits = np.array(list(itertools.product((0, 1), repeat=nd)))
+        corners = np.minimum(lo + bits, shape - 1)
+        frac = np.clip(seed - lo, 0.0, 1.0)
+        wc = np.prod(np.where(bits == 1, frac, 1.0 - frac), axis=1)
+        return wc @ self._cost_metrics(corners, drift=True)[2]
 
     def _spread_seed(self, seed, seed_value, r):
         """SetRHS's seed spreading (agd/Eikonal/HFM_CUDA/_SetArgs.py:46-75): the grid
@@ -598,17 +668,18 @@ class Interface:
         neigh = np.stack(np.meshgrid(*aX, indexing="ij"), axis=-1).reshape(-1, nd)
         neigh = neigh[np.linalg.norm(neigh - seed, axis=-1) < r]
         neigh = neigh[np.all((-0.5 <= neigh) & (neigh < shape - 0.5), axis=-1)]
-        m1, _ = self._cost_metrics(neigh)
+        m1, _, w1 = self._cost_metrics(neigh, drift=True)
         m0 = self._seed_metric(seed)
-        d = neigh - seed
-        n0 = np.sqrt(np.einsum("ki,ij,kj->k", d, m0, d))
-        n1 = np.sqrt(np.einsum("ki,kij,kj->k", d, m1, d))
+        w0 = self._seed_drift(seed)
+        d = neigh - seed  # Rander norms add the drift term <w, d>
+        n0 = np.sqrt(np.einsum("ki,ij,kj->k", d, m0, d)) + d @ w0
+        n1 = np.sqrt(np.einsum("ki,kij,kj->k", d, m1, d)) + np.einsum("ki,ki->k", d, w1)
         return neigh.astype(np.int64), (seed_value + 0.5 * (n0 + n1)).astype(np.float32)
 
     def instance(self):
         inst = _lib.AgdInstance()
-        inst.model = {"Riemann": _lib.AGD_MODEL_RIEMANN, "Diagonal": _lib.AGD_MODEL_DIAGONAL}.get(
-            self.model_, _lib.AGD_MODEL_ISOTROPIC)
+        inst.model = {"Riemann": _lib.AGD_MODEL_RIEMANN, "Diagonal": _lib.AGD_MODEL_DIAGONAL,
+                      "Rander": _lib.AGD_MODEL_RANDER}.get(self.model_, _lib.AGD_MODEL_ISOTROPIC)
         inst.ndim = self.ndim
         for k in range(3):
             inst.shape[k] = self.shape[k] if k < self.ndim else 1
@@ -714,10 +785,11 @@ class Interface:
             help="Export which finite differences are active, and the min/max index."))
         self.flow_needed = (self.reverseAD or self.forwardAD or self.hasTips or self.exportGeodesicFlow
                             or self.exportActiveNeighs)
+        self.flow_normalization = None
         if not self.flow_needed:
             return
         L = _lib.lib()
-        nact = self.ndim * (self.ndim + 1) // 2 if self.model_ == "Riemann" else self.ndim
+        nact = self.ndim * (self.ndim + 1) // 2 if self.model_ in ("Riemann", "Rander") else self.ndim
         self.nact = nact
         self.flow_vector = torch.empty(self.ndim * self.size_tot, dtype=torch.float32, device="cuda")
         self.flow_weightsum = torch.empty(self.size_tot, dtype=torch.float32, device="cuda")
@@ -728,8 +800,23 @@ class Interface:
         inst = self.instance()
         _lib.check(L.agd_flow(ctypes.byref(inst), _lib.ptr(self.flow_vector), _lib.ptr(self.flow_weightsum),
                               _lib.ptr(self.flow_weights), _lib.ptr(self.flow_indices), self.stream), "flow")
+        # drift models: the flow is normalised by the metric norm of -flow at the
+        # non-seed points (_PostProcess.py:80-88), for the export and for AD
+        if self.model_ == "Rander" and (self.exportGeodesicFlow or self.forwardAD or self.reverseAD):
+            fv = self.squeeze(self.flow_vector, self.ndim)
+            M, w = self._rander_parts()
+            M = torch.as_tensor(M, device="cuda").reshape(self.shape + (self.ndim, self.ndim)) \
+                if len(M) > 1 else torch.as_tensor(M[0], device="cuda")
+            w = torch.as_tensor(w, device="cuda").reshape(self.shape + (self.ndim,)) \
+                if len(w) > 1 else torch.as_tensor(w[0], device="cuda")
+            v = -torch.movedim(fv, 0, -1).double()
+            n = torch.sqrt(torch.einsum("...i,...ij,...j->...", v, M.expand(v.shape + (self.ndim,)), v)) + \
+                (w.expand(v.shape) * v).sum(-1)
+            self.flow_normalization = torch.where(self._seed_tags(), torch.ones_like(n), n).float()
         if self.exportGeodesicFlow:
             fv = self.squeeze(self.flow_vector, self.ndim)
+            if self.flow_normalization is not None:
+                fv = fv / self.flow_normalization
             h = torch.as_tensor(self.h, device="cuda").reshape((self.ndim,) + (1,) * self.ndim)
             self.hfmOut["flow"] = fv * (-h)
         if self.exportActiveNeighs:
@@ -740,6 +827,14 @@ class Interface:
             for k in range(nact):
                 bits |= (fw[k] > 0).to(torch.int32) << k
             self.hfmOut["activeNeighs"] = bits
+
+    def _seed_tags(self):
+        """Seeds and walls, grid layout (the reference's seedTags)."""
+        tags = torch.zeros(self.shape, dtype=torch.bool, device="cuda")
+        tags[tuple(torch.as_tensor(self.seedIndices.T, device="cuda").long())] = True
+        if getattr(self, "walls", None) is not None:
+            tags |= self.walls.bool()
+        return tags
 
     def SolveAD(self):
         """Forward and reverse differentiation (agd/Eikonal/HFM_CUDA/_PostProcess.py:155-219)."""
@@ -781,6 +876,8 @@ class Interface:
         pos = tuple(torch.as_tensor(self.seedIndices.T, device="cuda").long())
         seedS = allS[pos].clone()
         allS[pos] = 0
+        if self.flow_normalization is not None:  # drift models (_PostProcess.py:213-214)
+            allS = allS / self.flow_normalization[..., None]
         self.hfmOut["costSensitivity"] = allS
         if self.nseeds_in != len(self.seedIndices):  # spread seeds: each depends on its seed with weight 1
             owner = torch.as_tensor(self.seed_owner, device="cuda")
@@ -805,6 +902,8 @@ class Interface:
         rhs_all[pos] = sv.T[torch.as_tensor(self.seed_owner, device="cuda")] if sv is not None else 0.0
         if self.walls is not None:  # the walls' right-hand side +inf does not vary
             rhs_all[self.walls.bool()] = 0.0
+        if self.flow_normalization is not None:  # drift models (_PostProcess.py:185)
+            rhs_all = rhs_all * self.flow_normalization[..., None]
         inst = self.instance()
         nbytes = L.agd_reverse_workspace_bytes(ctypes.byref(inst))
         ws = torch.empty(max(int(nbytes), 1), dtype=torch.uint8, device="cuda")
@@ -911,6 +1010,26 @@ class Interface:
 
 def _host_scalar(x):
     return float(x.item()) if isinstance(x, torch.Tensor) else float(x)
+
+
+def _rander_hfm(src, ndim):
+    """A Rander metric given as a Metrics.Rander-like object (attributes m of
+    shape (d, d, *shape) and w of shape (d, *shape)) or as an HFM array
+    (*shape, symdim + d) -> float32 CUDA tensor (*shape, symdim + d), or
+    (symdim + d,) for a constant metric.  (The reference's Rander.from_HFM
+    infers d from the length alone and fails for d = 2: its users pass the
+    object; both forms are taken here.)"""
+    sd = ndim * (ndim + 1) // 2
+    if hasattr(src, "m") and hasattr(src, "w"):
+        m, w = _to_tensor(src.m), _to_tensor(src.w)
+        if m.shape[0] != ndim or w.shape[0] != ndim:
+            raise ValueError("Metric dimension does not match the model")
+        rows = [m[i, j] for i in range(ndim) for j in range(i + 1)] + [w[i] for i in range(ndim)]
+        return torch.movedim(torch.stack(torch.broadcast_tensors(*rows)), 0, -1).contiguous()
+    arr = _to_tensor(src)
+    if arr.shape[-1] != sd + ndim:
+        raise ValueError(f"Rander metric array must have {sd + ndim} components in its last axis (HFM layout)")
+    return arr.contiguous()
 
 
 def _costs_hfm(src, ndim):

@@ -1,7 +1,7 @@
-"""Metrics accepted by the eikonal solver: Riemann, Isotropic, Diagonal.
+"""Metrics accepted by the eikonal solver: Riemann, Rander, Isotropic, Diagonal.
 
 The subset of agd/Metrics used by the GPU eikonal path (riemann.py:13-165,
-isotropic.py:8-98, diagonal.py, base.py:175-250, misc.py:8-27): tensors are
+rander.py:10-77, isotropic.py:8-98, diagonal.py, base.py:175-250, misc.py:8-27): tensors are
 stored geometry first, m of shape (d, d, *shape); `flatten` packs the lower
 triangle [m00, m10, m11, m20, m21, m22]; the HFM layout puts that packing
 last, (*shape, symdim).  Arrays may be numpy arrays or torch tensors.
@@ -186,3 +186,58 @@ class Isotropic(Base):
     @classmethod
     def from_HFM(cls, arr):
         return cls(arr)
+
+
+class Rander(Base):
+    """F(x) = sqrt(<x, m x>) + <w, x>, with |w|_{m^-1} < 1 (rander.py:10-77).
+    m of shape (d, d, *shape), w of shape (d, *shape).  The HFM layout is the
+    lower triangle of m followed by w, last axis (*shape, symdim + d)."""
+
+    def __init__(self, m, w):
+        self.m, self.w = _asarray(m), _asarray(w)
+
+    @property
+    def vdim(self):
+        return len(self.m)
+
+    def norm(self, v):
+        v = _asarray(v)
+        xp = _xp(v)
+        quad = (self.m * v[None] * v[:, None]).sum(axis=0).sum(axis=0) if xp is np else \
+            (self.m * v[None] * v[:, None]).sum(0).sum(0)
+        return quad ** 0.5 + (self.w * v).sum(0)
+
+    def dual(self):
+        """The dual of a Rander norm is a Rander norm (rander.py:35-39)."""
+        xp = _xp(self.m)
+        m = xp.moveaxis(self.m, (0, 1), (-2, -1)) if xp is np else torch.movedim(self.m, (0, 1), (-2, -1))
+        w = xp.moveaxis(self.w, 0, -1) if xp is np else torch.movedim(self.w, 0, -1)
+        s = (np.linalg.inv if xp is np else torch.linalg.inv)(m - w[..., :, None] * w[..., None, :])
+        om = (s @ w[..., :, None])[..., 0]
+        mm = (1 + (w * om).sum(-1))[..., None, None] * s
+        back = (lambda a, src, dst: np.moveaxis(a, src, dst)) if xp is np else torch.movedim
+        return Rander(back(mm, (-2, -1), (0, 1)), back(-om, -1, 0))
+
+    def with_costs(self, costs):
+        c = _asarray(costs)
+        return Rander(self.m * c[:, None] * c[None, :] if c.ndim == 1 and self.m.ndim == 2 else
+                      self.m * (c[:, None] * c[None, :]), self.w * c)
+
+    def flatten(self, inverse_m=False):
+        m = self.m
+        xp = _xp(m)
+        if inverse_m:
+            mm = xp.moveaxis(m, (0, 1), (-2, -1)) if xp is np else torch.movedim(m, (0, 1), (-2, -1))
+            mi = (np.linalg.inv if xp is np else torch.linalg.inv)(mm)
+            m = np.moveaxis(mi, (-2, -1), (0, 1)) if xp is np else torch.movedim(mi, (-2, -1), (0, 1))
+        f = flatten_symmetric_matrix(m)
+        return np.concatenate([f, self.w], 0) if xp is np else torch.cat([f, self.w], 0)
+
+    @classmethod
+    def expand(cls, arr):
+        d = 0
+        while d * (d + 3) // 2 < len(arr):  # symdim + d components
+            d += 1
+        assert len(arr) == d * (d + 3) // 2, "a Rander metric has d(d+1)/2 + d components"
+        sd = d * (d + 1) // 2
+        return cls(expand_symmetric_matrix(arr[:sd]), arr[sd:])

@@ -22,6 +22,7 @@ AGD_STATUS_UNSUPPORTED = 32
 AGD_MODEL_ISOTROPIC = 0
 AGD_MODEL_RIEMANN = 1
 AGD_MODEL_DIAGONAL = 2
+AGD_MODEL_RANDER = 3
 AGD_FLAG_ACTIVATE_ALL = 1
 
 _c_int3 = ctypes.c_int * 3
@@ -75,6 +76,7 @@ SIGNATURES = {
     "agd_eikonal_solve_fixed_scratch": (_I, [_P, _I, _P, _P, _P]),
     "agd_prep_geom": (_I, [_I, _P, _P, _P, _I, _I, _P, _P, _P]),
     "agd_prep_geom_diagonal": (_I, [_I, _P, _P, _P, _I, _I, _P, _P, _P]),
+    "agd_prep_geom_rander": (_I, [_I, _P, _P, _P, _I, _I, _P, _P, _P]),
     "agd_block_expand": (_I, [_I, _P, _P, _I, _P, _I, ctypes.c_float, _P, _P]),
     "agd_block_squeeze": (_I, [_I, _P, _P, _I, _P, _P, _P]),
     "agd_prep_seeds": (_I, [_I, _P, _P, _P, _P, _I, _P, _P, _P, _P]),

@@ -279,7 +279,7 @@ static bool rev_layout(const agd_instance *a, RevLayout &R, std::vector<Inst> *i
     const Inst &I = (*insts)[0];
     R.size_tot = I.size_tot;
     R.size_i = I.size_i;
-    R.nact = a->model == AGD_MODEL_RIEMANN ? a->ndim * (a->ndim + 1) / 2 : a->ndim;
+    R.nact = (a->model == AGD_MODEL_RIEMANN || a->model == AGD_MODEL_RANDER) ? a->ndim * (a->ndim + 1) / 2 : a->ndim;
     size_t off = R.L.total;
     const long long nblk = (R.size_tot + 1 + 1023) / 1024;
     R.rowptr = off; off = align256(off + sizeof(int) * (R.size_tot + 1));

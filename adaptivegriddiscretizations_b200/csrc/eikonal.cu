@@ -221,12 +221,18 @@ __global__ void mp_copy_kernel(Sched S, int dir) {
 // Jacobi sweeps inside the tile and double-buffered epochs, as the reference
 // forces strict_iter_i and strict_iter_o with it (_Kernel.py:39-45).
 // FACT: source factorisation (shifted neighbour values near the seed).
+// MODEL Rander: the Riemann stencil of the first symdim geometry planes, and
+// the neighbour values at x -/+ e shifted by +/-<w, e> for the drift w of the
+// next ndim planes (FiniteDifferences.h:41-45).
 // ORD2: second order scheme (neighbours two steps away, cuda/HFM.h:91-138).
 // WALLS: neighbours hidden by a wall read +inf (bits of the stencil cache).
 template <class TL, int MODEL, bool MP = false, bool FACT = false, bool ORD2 = false, bool WALLS = false>
 struct Visit {
     static constexpr int D = TL::D, P = TL::P;
-    static constexpr int NACT = MODEL == AGD_MODEL_RIEMANN ? D * (D + 1) / 2 : D;
+    static constexpr bool kSelling = MODEL == AGD_MODEL_RIEMANN || MODEL == AGD_MODEL_RANDER;
+    static constexpr bool kDrift = MODEL == AGD_MODEL_RANDER;
+    static constexpr bool SHIFT = FACT || kDrift;  // neighbour values shifted (fsh)
+    static constexpr int NACT = kSelling ? D * (D + 1) / 2 : D;
     static constexpr int NTOT = 2 * NACT;
     static constexpr int SD = D * (D + 1) / 2;
 
@@ -296,7 +302,7 @@ struct Visit {
     // (cached weights and packed offsets, or the dual metric; Diagonal: the
     // weights), then the weights and offsets (unpacked, or by Selling's
     // decomposition; unit offsets for Isotropic and Diagonal).
-    static constexpr int kRaw = MODEL == AGD_MODEL_ISOTROPIC ? 1 : (MODEL == AGD_MODEL_DIAGONAL ? D : 2 * SD);
+    static constexpr int kRaw = MODEL == AGD_MODEL_ISOTROPIC ? 1 : (MODEL == AGD_MODEL_DIAGONAL ? D : 2 * SD + (kDrift ? D : 0));
     __device__ __forceinline__ static void stencil_load(const Inst &I, size_t n_t, float *raw) {
         if constexpr (MODEL == AGD_MODEL_ISOTROPIC) return;
         if constexpr (MODEL == AGD_MODEL_DIAGONAL) {
@@ -311,6 +317,21 @@ struct Visit {
 #pragma unroll
             for (int c = 0; c < SD; ++c) raw[c] = __ldg(I.a.geom + (size_t)c * I.size_tot + n_t);
         }
+        if constexpr (kDrift) {  // the drift, after the stencil words
+#pragma unroll
+            for (int c = 0; c < D; ++c) raw[2 * SD + c] = __ldg(I.a.geom + (size_t)(SD + c) * I.size_tot + n_t);
+        }
+    }
+    // Drift shifts <w, e_k> of the offsets (scal_vv order), w = raw[2 SD ..].
+    __device__ __forceinline__ static void drift_shifts(const float *raw, const int (*e)[3], float *f) {
+#pragma unroll
+        for (int k = 0; k < NACT; ++k) {
+            float s = 0.f;
+#pragma unroll
+            for (int c = 0; c < D; ++c) s += raw[2 * SD + c] * float(e[k][c]);
+            f[2 * k] += s;
+            f[2 * k + 1] -= s;
+        }
     }
     // hide[k]: the hidden-neighbour bits of offset k (WALLS: from the cache; else 0).
     // Isotropic offsets are unit vectors, hidden exactly when the neighbour is a
@@ -319,7 +340,7 @@ struct Visit {
                                                           unsigned *hide) {
 #pragma unroll
         for (int k = 0; k < NACT; ++k) hide[k] = 0u;
-        if constexpr (MODEL != AGD_MODEL_RIEMANN) {
+        if constexpr (!kSelling) {
 #pragma unroll
             for (int k = 0; k < D; ++k) {
                 w[k] = MODEL == AGD_MODEL_ISOTROPIC ? I.a.iso_weights[k] : raw[k];
@@ -406,7 +427,7 @@ struct Visit {
         float nbv[kSlots ? 1 : P][kSlots ? 1 : NTOT];
         int nbq[MP ? P : 1][MP ? NTOT : 1];
         unsigned nba[kSlots ? P : 1][kSlots ? NTOT : 1];
-        float fsh[FACT ? P : 1][FACT ? NTOT : 1];  // factorisation shifts of the neighbour values
+        float fsh[SHIFT ? P : 1][SHIFT ? NTOT : 1];  // factorisation and drift shifts of the neighbour values
         // second order: the neighbours two steps away, as nba / nbv
         unsigned nba2[ORD2 && kSlots ? P : 1][ORD2 && kSlots ? NTOT : 1];
         float nbv2[ORD2 && !kSlots ? P : 1][ORD2 && !kSlots ? NTOT : 1];
@@ -447,7 +468,15 @@ struct Visit {
             unsigned hide[NACT];
             if (seed[p]) continue;  // seeds (and padding) keep their value: no stencil needed
             stencil_decode(I, raw[p], wts[p], ev, hide);
-            if constexpr (FACT) factor_shifts<D, NACT, MODEL != AGD_MODEL_RIEMANN>(A, xt, ev, fsh[p]);
+            if constexpr (SHIFT) {
+                if constexpr (FACT) {
+                    factor_shifts<D, NACT, !kSelling>(A, xt, ev, fsh[p]);
+                } else {
+#pragma unroll
+                    for (int k = 0; k < NTOT; ++k) fsh[p][k] = 0.f;
+                }
+                if constexpr (kDrift) drift_shifts(raw[p], ev, fsh[p]);
+            }
 #pragma unroll
             for (int k = 0; k < NACT; ++k) {
 #pragma unroll
@@ -528,6 +557,10 @@ struct Visit {
                         int aq, bq;
                         neighbour_mp(nbv[p][2 * k], nbq[p][2 * k], us, uqs, a, aq);
                         neighbour_mp(nbv[p][2 * k + 1], nbq[p][2 * k + 1], us, uqs, b, bq);
+                        if constexpr (SHIFT) {  // the float part carries the shift (HFM.h:46-53)
+                            a += fsh[p][2 * k];
+                            b += fsh[p][2 * k + 1];
+                        }
                         const bool take_b = greater(a, aq, b, bq, step);  // HFM.h:52-57
                         v[k] = take_b ? b : a;
                         vq[k] = take_b ? bq : aq;
@@ -575,7 +608,7 @@ struct Visit {
                                 a = neighbour(nbv[p][2 * k], us);
                                 b = neighbour(nbv[p][2 * k + 1], us);
                             }
-                            if constexpr (FACT) {
+                            if constexpr (SHIFT) {
                                 a += fsh[p][2 * k];
                                 b += fsh[p][2 * k + 1];
                             }
@@ -765,6 +798,36 @@ __device__ __forceinline__ void dispatch(const Sched &S, int t, int e, int lane,
         case V_DIAG3_4_O2:
             if constexpr ((VMASK >> V_DIAG3_4_O2) & 1) Visit<Tile<3, 4, 4, 4>, AGD_MODEL_DIAGONAL, false, false, true>::run(S, I, ii, n_o, e, lane, us);
             break;
+        case V_RAND2_8:
+            if constexpr ((VMASK >> V_RAND2_8) & 1) Visit<Tile<2, 8, 8, 1>, AGD_MODEL_RANDER>::run(S, I, ii, n_o, e, lane, us);
+            break;
+        case V_RAND3_4:
+            if constexpr ((VMASK >> V_RAND3_4) & 1) Visit<Tile<3, 4, 4, 4>, AGD_MODEL_RANDER>::run(S, I, ii, n_o, e, lane, us);
+            break;
+        case V_RAND2_8_W:
+            if constexpr ((VMASK >> V_RAND2_8_W) & 1) Visit<Tile<2, 8, 8, 1>, AGD_MODEL_RANDER, false, false, false, true>::run(S, I, ii, n_o, e, lane, us);
+            break;
+        case V_RAND3_4_W:
+            if constexpr ((VMASK >> V_RAND3_4_W) & 1) Visit<Tile<3, 4, 4, 4>, AGD_MODEL_RANDER, false, false, false, true>::run(S, I, ii, n_o, e, lane, us);
+            break;
+        case V_RAND2_8_MP:
+            if constexpr ((VMASK >> V_RAND2_8_MP) & 1) Visit<Tile<2, 8, 8, 1>, AGD_MODEL_RANDER, true, false, false, true>::run(S, I, ii, n_o, e, lane, us);
+            break;
+        case V_RAND3_4_MP:
+            if constexpr ((VMASK >> V_RAND3_4_MP) & 1) Visit<Tile<3, 4, 4, 4>, AGD_MODEL_RANDER, true, false, false, true>::run(S, I, ii, n_o, e, lane, us);
+            break;
+        case V_RAND2_8_F:
+            if constexpr ((VMASK >> V_RAND2_8_F) & 1) Visit<Tile<2, 8, 8, 1>, AGD_MODEL_RANDER, false, true, false, true>::run(S, I, ii, n_o, e, lane, us);
+            break;
+        case V_RAND3_4_F:
+            if constexpr ((VMASK >> V_RAND3_4_F) & 1) Visit<Tile<3, 4, 4, 4>, AGD_MODEL_RANDER, false, true, false, true>::run(S, I, ii, n_o, e, lane, us);
+            break;
+        case V_RAND2_8_O2:
+            if constexpr ((VMASK >> V_RAND2_8_O2) & 1) Visit<Tile<2, 8, 8, 1>, AGD_MODEL_RANDER, false, false, true, true>::run(S, I, ii, n_o, e, lane, us);
+            break;
+        case V_RAND3_4_O2:
+            if constexpr ((VMASK >> V_RAND3_4_O2) & 1) Visit<Tile<3, 4, 4, 4>, AGD_MODEL_RANDER, false, false, true, true>::run(S, I, ii, n_o, e, lane, us);
+            break;
         default:
             break;
     }
@@ -805,6 +868,14 @@ constexpr int smem_floats() {
     if ((VMASK >> V_DIAG2_8_O2) & 1) m = std::max(m, Visit<Tile<2, 8, 8, 1>, AGD_MODEL_DIAGONAL, false, false, true>::kSmemFloats);
     if ((VMASK >> V_DIAG2_16_O2) & 1) m = std::max(m, Visit<Tile<2, 16, 16, 1>, AGD_MODEL_DIAGONAL, false, false, true>::kSmemFloats);
     if ((VMASK >> V_DIAG3_4_O2) & 1) m = std::max(m, Visit<Tile<3, 4, 4, 4>, AGD_MODEL_DIAGONAL, false, false, true>::kSmemFloats);
+    if ((VMASK >> V_RAND2_8) & 1) m = std::max(m, Visit<Tile<2, 8, 8, 1>, AGD_MODEL_RANDER>::kSmemFloats);
+    if ((VMASK >> V_RAND3_4) & 1) m = std::max(m, Visit<Tile<3, 4, 4, 4>, AGD_MODEL_RANDER>::kSmemFloats);
+    if ((VMASK >> V_RAND2_8_W) & 1) m = std::max(m, Visit<Tile<2, 8, 8, 1>, AGD_MODEL_RANDER, false, false, false, true>::kSmemFloats);
+    if ((VMASK >> V_RAND3_4_W) & 1) m = std::max(m, Visit<Tile<3, 4, 4, 4>, AGD_MODEL_RANDER, false, false, false, true>::kSmemFloats);
+    if ((VMASK >> V_RAND2_8_F) & 1) m = std::max(m, Visit<Tile<2, 8, 8, 1>, AGD_MODEL_RANDER, false, true, false, true>::kSmemFloats);
+    if ((VMASK >> V_RAND3_4_F) & 1) m = std::max(m, Visit<Tile<3, 4, 4, 4>, AGD_MODEL_RANDER, false, true, false, true>::kSmemFloats);
+    if ((VMASK >> V_RAND2_8_O2) & 1) m = std::max(m, Visit<Tile<2, 8, 8, 1>, AGD_MODEL_RANDER, false, false, true, true>::kSmemFloats);
+    if ((VMASK >> V_RAND3_4_O2) & 1) m = std::max(m, Visit<Tile<3, 4, 4, 4>, AGD_MODEL_RANDER, false, false, true, true>::kSmemFloats);
     return m;
 }
 
@@ -818,7 +889,8 @@ struct EikonalVisitor {
                   (1ull << V_ISO2_16_O2) | (1ull << V_RIEM2_16_W) | (1ull << V_DIAG2_16) |
                   (1ull << V_DIAG2_16_MP) | (1ull << V_DIAG2_16_F) | (1ull << V_DIAG2_16_O2)))      ? 4
         : (VMASK & ((1ull << V_RIEM3_4) | (1ull << V_RIEM3_4_MP) | (1ull << V_RIEM3_4_F) | (1ull << V_RIEM3_4_O2) |
-                    (1ull << V_RIEM3_4_W)))                                                     ? 6
+                    (1ull << V_RIEM3_4_W) | (1ull << V_RAND3_4) | (1ull << V_RAND3_4_W) | (1ull << V_RAND3_4_MP) |
+                    (1ull << V_RAND3_4_F) | (1ull << V_RAND3_4_O2)))                             ? 6
         : (VMASK & (kMpVariants | kFactorVariants | kOrder2Variants))                                ? 7
                                                                                                      : 9;
     struct Args {};
@@ -835,16 +907,18 @@ struct EikonalVisitor {
         constexpr unsigned long long kRiemann = (1ull << V_RIEM2_8) | (1ull << V_RIEM3_4) | (1ull << V_RIEM2_16) |
                                       (1ull << V_RIEM2_8_MP) | (1ull << V_RIEM3_4_MP) | (1ull << V_RIEM2_8_F) |
                                       (1ull << V_RIEM3_4_F) | (1ull << V_RIEM2_8_O2) | (1ull << V_RIEM3_4_O2) |
-                                      kWallVariants;
+                                      kWallVariants | kRanderVariants;
         if (VMASK & kMpVariants) mp_copy_kernel<<<(L.total_tiles + 7) / 8, 256, 0, st>>>(S, 0);
         if (!(VMASK & kRiemann) || L.stencil == L.total) return cudaGetLastError();
         // variants that read the hidden-neighbour bits: the walls pass follows
         constexpr unsigned long long kWallCapable = kWallVariants | (1ull << V_RIEM2_8_MP) | (1ull << V_RIEM3_4_MP) |
                                           (1ull << V_RIEM2_8_F) | (1ull << V_RIEM3_4_F) | (1ull << V_RIEM2_8_O2) |
-                                          (1ull << V_RIEM3_4_O2);
+                                          (1ull << V_RIEM3_4_O2) | (kRanderVariants & ~((1ull << V_RAND2_8) |
+                                                                                      (1ull << V_RAND3_4)));
         const unsigned grid = (L.total_tiles + 7) / 8;
         if (VMASK & ((1ull << V_RIEM3_4) | (1ull << V_RIEM3_4_MP) | (1ull << V_RIEM3_4_F) | (1ull << V_RIEM3_4_O2) |
-                     (1ull << V_RIEM3_4_W))) {
+                     (1ull << V_RIEM3_4_W) | (1ull << V_RAND3_4) | (1ull << V_RAND3_4_W) | (1ull << V_RAND3_4_MP) |
+                     (1ull << V_RAND3_4_F) | (1ull << V_RAND3_4_O2))) {
             stencil_kernel<3><<<grid, 256, 0, st>>>(S.inst, S.ninst, L.total_tiles, S.ctrl);
             if (VMASK & kWallCapable) stencil_walls_kernel<3><<<grid, 256, 0, st>>>(S.inst, S.ninst, L.total_tiles);
         } else {
@@ -886,7 +960,7 @@ static int validate(const agd_instance *host, const Inst *insts, int n, bool ste
             code = AGD_STATUS_UNSUPPORTED;
         }
         else if (insts[i].variant < 0) { bad = "model/tile shape not built"; code = AGD_STATUS_UNSUPPORTED; }
-        else if (a.wall_dist && a.model == AGD_MODEL_RIEMANN && !stencil_cache) {
+        else if (a.wall_dist && (a.model == AGD_MODEL_RIEMANN || a.model == AGD_MODEL_RANDER) && !stencil_cache) {
             bad = "walls on a Riemann instance need the stencil cache (agd_eikonal_solve)";
             code = AGD_STATUS_UNSUPPORTED;
         }
@@ -932,6 +1006,24 @@ static int run_variants(int ndim, unsigned long long vmask, const WsLayout &L, v
     constexpr unsigned long long MP3 = (1ull << V_ISO3_4_MP) | (1ull << V_RIEM3_4_MP);
     // Riemann with walls, beside plain instances of every family
     constexpr unsigned long long W2 = (1ull << V_RIEM2_8_W) | (1ull << V_RIEM2_16_W), W3 = 1ull << V_RIEM3_4_W;
+    if (vmask & kRanderVariants) {  // Rander instances run in kernels of their own
+        constexpr unsigned long long RB2 = (1ull << V_RAND2_8) | (1ull << V_RAND2_8_W);
+        constexpr unsigned long long RB3 = (1ull << V_RAND3_4) | (1ull << V_RAND3_4_W);
+        if (vmask & ~kRanderVariants) return set_error(AGD_STATUS_UNSUPPORTED, "Rander instances beside other models in one plan");
+        const bool mp = vmask & kMpVariants, f = vmask & kFactorVariants, o2 = vmask & kOrder2Variants;
+        if (int(mp) + int(f) + int(o2) > 1)
+            return set_error(AGD_STATUS_UNSUPPORTED, "Rander instances of several option families in one plan");
+        if (ndim == 2) {
+            if (o2) return run_sched<EikonalVisitor<(1ull << V_RAND2_8_O2) | RB2>>(L, ws, n, {}, stats, cfg, st);
+            if (f) return run_sched<EikonalVisitor<(1ull << V_RAND2_8_F) | RB2>>(L, ws, n, {}, stats, cfg, st);
+            if (mp) return run_sched<EikonalVisitor<(1ull << V_RAND2_8_MP) | RB2>>(L, ws, n, {}, stats, cfg, st);
+            return run_sched<EikonalVisitor<RB2>>(L, ws, n, {}, stats, cfg, st);
+        }
+        if (o2) return run_sched<EikonalVisitor<(1ull << V_RAND3_4_O2) | RB3>>(L, ws, n, {}, stats, cfg, st);
+        if (f) return run_sched<EikonalVisitor<(1ull << V_RAND3_4_F) | RB3>>(L, ws, n, {}, stats, cfg, st);
+        if (mp) return run_sched<EikonalVisitor<(1ull << V_RAND3_4_MP) | RB3>>(L, ws, n, {}, stats, cfg, st);
+        return run_sched<EikonalVisitor<RB3>>(L, ws, n, {}, stats, cfg, st);
+    }
     if (vmask & kDiagVariants) {  // Diagonal instances run in kernels of their own
         constexpr unsigned long long D2 = (1ull << V_DIAG2_8) | (1ull << V_DIAG2_16), D3 = 1ull << V_DIAG3_4;
         constexpr unsigned long long DMP2 = (1ull << V_DIAG2_8_MP) | (1ull << V_DIAG2_16_MP), DMP3 = 1ull << V_DIAG3_4_MP;
@@ -1089,16 +1181,22 @@ __global__ void flow_kernel(Inst I, float *fvec, float *fwsum, float *fw, int *f
         int ev[NACT][3], side[NACT];
         V::stencil(I, n_t, w, ev);
         unsigned hide[NACT];  // neighbours hidden by a wall (Riemann offsets; see Visit::stencil_decode)
-        const int wd0 = (MODEL == AGD_MODEL_RIEMANN && A.wall_dist && in) ? (int)__ldg(A.wall_dist + n_t) : 255;
+        const int wd0 = (V::kSelling && A.wall_dist && in) ? (int)__ldg(A.wall_dist + n_t) : 255;
 #pragma unroll
         for (int k = 0; k < NACT; ++k)
             hide[k] = hidden_bits<D>(A, wd0, xt, ev[k], [&](const int *y) { return bilevel_index<D, TL>(y, I.shape_o); });
         float v[NACT], fsh[2 * NACT];
         if (A.factor_radius2 > 0.f) {
-            factor_shifts<D, NACT, MODEL != AGD_MODEL_RIEMANN>(A, xt, ev, fsh);
+            factor_shifts<D, NACT, !V::kSelling>(A, xt, ev, fsh);
         } else {
 #pragma unroll
             for (int k = 0; k < 2 * NACT; ++k) fsh[k] = 0.f;
+        }
+        if constexpr (V::kDrift) {
+            float raw[V::kRaw];
+#pragma unroll
+            for (int c = 0; c < D; ++c) raw[2 * V::SD + c] = __ldg(A.geom + (size_t)(V::SD + c) * I.size_tot + n_t);
+            V::drift_shifts(raw, ev, fsh);
         }
 #pragma unroll
         for (int k = 0; k < NACT; ++k) {
@@ -1182,6 +1280,8 @@ static int flow_impl(const agd_instance *a, float *fvec, float *fwsum, float *fw
         case V_DIAG2_8: flow_kernel<Tile<2, 8, 8, 1>, AGD_MODEL_DIAGONAL><<<grid, wpb * 32, 0, st>>>(I, fvec, fwsum, fw, fidx); break;
         case V_DIAG2_16: flow_kernel<Tile<2, 16, 16, 1>, AGD_MODEL_DIAGONAL><<<grid, wpb * 32, 0, st>>>(I, fvec, fwsum, fw, fidx); break;
         case V_DIAG3_4: flow_kernel<Tile<3, 4, 4, 4>, AGD_MODEL_DIAGONAL><<<grid, wpb * 32, 0, st>>>(I, fvec, fwsum, fw, fidx); break;
+        case V_RAND2_8: flow_kernel<Tile<2, 8, 8, 1>, AGD_MODEL_RANDER><<<grid, wpb * 32, 0, st>>>(I, fvec, fwsum, fw, fidx); break;
+        case V_RAND3_4: flow_kernel<Tile<3, 4, 4, 4>, AGD_MODEL_RANDER><<<grid, wpb * 32, 0, st>>>(I, fvec, fwsum, fw, fidx); break;
         default: return set_error(AGD_STATUS_UNSUPPORTED, "model/tile shape not built");
     }
     const cudaError_t err = cudaGetLastError();
@@ -1331,6 +1431,69 @@ __global__ void prep_diag_kernel(Geo g, const float *costs, int bcast, int is_du
         }
         geom[k * g.size_tot + n_t] = w;
     }
+}
+
+// Inverse of a packed symmetric matrix [a00, a10, a11(, a20, a21, a22)] by the
+// adjugate formula.
+__device__ __forceinline__ void sym_inverse(int nd, const float *s, float *out) {
+    if (nd == 2) {
+        const float det = s[0] * s[2] - s[1] * s[1];
+        out[0] = s[2] / det;
+        out[1] = -s[1] / det;
+        out[2] = s[0] / det;
+        return;
+    }
+    const float a = s[0], b = s[1], c = s[2], d = s[3], e = s[4], f = s[5];
+    const float A00 = c * f - e * e, A10 = d * e - b * f, A11 = a * f - d * d;
+    const float A20 = b * e - c * d, A21 = b * d - a * e, A22 = a * c - b * b;
+    const float det = a * A00 + b * A10 + d * A20;
+    out[0] = A00 / det; out[1] = A10 / det; out[2] = A11 / det;
+    out[3] = A20 / det; out[4] = A21 / det; out[5] = A22 / det;
+}
+
+// Rander model: (inverse of m * outer(h, h), w * h) per point, +inf at padding
+// (Metrics/rander.py:61-68).  With is_dual the input (m_d, w_d) is the dual
+// metric: scaled by with_speeds(h), then turned into the metric by
+// rander.py:35-39, m = (1 + <w_d, s w_d>) s, w = -s w_d with s = (m_d - w_d w_d^T)^-1,
+// so that the inverse of m is (m_d - w_d w_d^T) / (1 + <w_d, s w_d>).
+__global__ void prep_rander_kernel(Geo g, const float *metric, int bcast, int is_dual, double h0, double h1,
+                                   double h2, float *geom) {
+    const long long n_t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (n_t >= g.size_tot) return;
+    const int nd = g.nd, sd = nd * (nd + 1) / 2;
+    int x[3];
+    long long flat;
+    const bool in = grid_coords(g, n_t, x, flat);
+    if (!in) {
+        for (int c = 0; c < sd + nd; ++c) geom[c * g.size_tot + n_t] = finf();
+        return;
+    }
+    const float hh[3] = {(float)h0, (float)h1, (float)h2};
+    float hs[3];  // the grid scales (metric), or their inverses (with_speeds of a dual metric)
+    for (int k = 0; k < nd; ++k) hs[k] = is_dual ? 1.f / hh[k] : hh[k];
+    const float *src = bcast ? metric : metric + flat * (sd + nd);
+    float m[6], w[3], mi[6];
+    int q = 0;
+    for (int i = 0; i < nd; ++i)
+        for (int j = 0; j <= i; ++j, ++q) m[q] = src[q] * (hs[i] * hs[j]);  // m * outer(h, h)
+    for (int k = 0; k < nd; ++k) w[k] = src[sd + k] * hs[k];
+    if (!is_dual) {
+        sym_inverse(nd, m, mi);
+    } else {
+        float t[6], s_[6], om[3] = {0.f, 0.f, 0.f};
+        q = 0;
+        for (int i = 0; i < nd; ++i)
+            for (int j = 0; j <= i; ++j, ++q) t[q] = m[q] - w[i] * w[j];
+        sym_inverse(nd, t, s_);
+        for (int i = 0; i < nd; ++i)
+            for (int j = 0; j < nd; ++j) om[i] += s_[i >= j ? i * (i + 1) / 2 + j : j * (j + 1) / 2 + i] * w[j];
+        float wo = 0.f;
+        for (int i = 0; i < nd; ++i) wo += w[i] * om[i];
+        for (int c = 0; c < sd; ++c) mi[c] = t[c] / (1.f + wo);
+        for (int k = 0; k < nd; ++k) w[k] = -om[k];
+    }
+    for (int c = 0; c < sd; ++c) geom[c * g.size_tot + n_t] = mi[c];
+    for (int k = 0; k < nd; ++k) geom[(sd + k) * g.size_tot + n_t] = w[k];
 }
 
 // Seed bits: one 32-bit word (32 points) per thread, padding bits set.
@@ -1612,6 +1775,18 @@ int agd_prep_geom_diagonal(int ndim, const int *shape, const int *shape_i, const
         geom);
     const cudaError_t err = cudaGetLastError();
     return err == cudaSuccess ? AGD_STATUS_OK : set_cuda_error("prep_geom_diagonal", err);
+}
+
+int agd_prep_geom_rander(int ndim, const int *shape, const int *shape_i, const float *metric, int broadcast,
+                         int is_dual, const double *grid_scales, float *geom, agd_stream_t stream) {
+    clear_error();
+    Geo g;
+    if ((ndim != 2 && ndim != 3) || !geo_of(ndim, shape, shape_i, g) || !metric || !geom || !grid_scales)
+        return set_error(AGD_STATUS_INVALID, "agd_prep_geom_rander: bad arguments");
+    prep_rander_kernel<<<blocks_for(g.size_tot, 256), 256, 0, (cudaStream_t)stream>>>(
+        g, metric, broadcast, is_dual, grid_scales[0], grid_scales[1], ndim == 3 ? grid_scales[2] : 1.0, geom);
+    const cudaError_t err = cudaGetLastError();
+    return err == cudaSuccess ? AGD_STATUS_OK : set_cuda_error("prep_geom_rander", err);
 }
 
 int agd_block_expand(int ndim, const int *shape, const int *shape_i, int nplanes, const float *src, int src_broadcast,

@@ -27,20 +27,28 @@ enum Variant {
     V_RIEM2_8_W, V_RIEM2_16_W, V_RIEM3_4_W,
     // Diagonal: plain, multiprecision, factorisation, second order
     V_DIAG2_8, V_DIAG2_16, V_DIAG3_4, V_DIAG2_8_MP, V_DIAG2_16_MP, V_DIAG3_4_MP,
-    V_DIAG2_8_F, V_DIAG2_16_F, V_DIAG3_4_F, V_DIAG2_8_O2, V_DIAG2_16_O2, V_DIAG3_4_O2, V_COUNT
+    V_DIAG2_8_F, V_DIAG2_16_F, V_DIAG3_4_F, V_DIAG2_8_O2, V_DIAG2_16_O2, V_DIAG3_4_O2,
+    // Rander: plain, walls, multiprecision, factorisation, second order
+    V_RAND2_8, V_RAND3_4, V_RAND2_8_W, V_RAND3_4_W, V_RAND2_8_MP, V_RAND3_4_MP, V_RAND2_8_F, V_RAND3_4_F,
+    V_RAND2_8_O2, V_RAND3_4_O2, V_COUNT
 };
 static_assert(V_COUNT <= 64, "variant masks are 64-bit");
 constexpr unsigned long long kMpVariants = (1ull << V_ISO2_8_MP) | (1ull << V_ISO2_16_MP) | (1ull << V_RIEM2_8_MP) |
                                  (1ull << V_ISO3_4_MP) | (1ull << V_RIEM3_4_MP) | (1ull << V_DIAG2_8_MP) |
-                                 (1ull << V_DIAG2_16_MP) | (1ull << V_DIAG3_4_MP);
+                                 (1ull << V_DIAG2_16_MP) | (1ull << V_DIAG3_4_MP) | (1ull << V_RAND2_8_MP) |
+                                 (1ull << V_RAND3_4_MP);
 constexpr unsigned long long kFactorVariants = (1ull << V_ISO2_8_F) | (1ull << V_ISO2_16_F) | (1ull << V_RIEM2_8_F) |
                                      (1ull << V_ISO3_4_F) | (1ull << V_RIEM3_4_F) | (1ull << V_DIAG2_8_F) |
-                                     (1ull << V_DIAG2_16_F) | (1ull << V_DIAG3_4_F);
+                                     (1ull << V_DIAG2_16_F) | (1ull << V_DIAG3_4_F) | (1ull << V_RAND2_8_F) |
+                                     (1ull << V_RAND3_4_F);
 constexpr unsigned long long kOrder2Variants = (1ull << V_ISO2_8_O2) | (1ull << V_ISO2_16_O2) | (1ull << V_RIEM2_8_O2) |
                                      (1ull << V_ISO3_4_O2) | (1ull << V_RIEM3_4_O2) | (1ull << V_DIAG2_8_O2) |
-                                     (1ull << V_DIAG2_16_O2) | (1ull << V_DIAG3_4_O2);
-constexpr unsigned long long kWallVariants = (1ull << V_RIEM2_8_W) | (1ull << V_RIEM2_16_W) | (1ull << V_RIEM3_4_W);
+                                     (1ull << V_DIAG2_16_O2) | (1ull << V_DIAG3_4_O2) | (1ull << V_RAND2_8_O2) |
+                                     (1ull << V_RAND3_4_O2);
+constexpr unsigned long long kWallVariants = (1ull << V_RIEM2_8_W) | (1ull << V_RIEM2_16_W) | (1ull << V_RIEM3_4_W) |
+                                           (1ull << V_RAND2_8_W) | (1ull << V_RAND3_4_W);
 constexpr unsigned long long kDiagVariants = ((1ull << (V_DIAG3_4_O2 + 1)) - 1) & ~((1ull << V_DIAG2_8) - 1);
+constexpr unsigned long long kRanderVariants = ((1ull << (V_RAND3_4_O2 + 1)) - 1) & ~((1ull << V_RAND2_8) - 1);
 
 static int base_variant_of(const agd_instance &a);
 
@@ -57,6 +65,8 @@ static int variant_of(const agd_instance &a) {
             case V_DIAG2_8: return V_DIAG2_8_O2;
             case V_DIAG2_16: return V_DIAG2_16_O2;
             case V_DIAG3_4: return V_DIAG3_4_O2;
+            case V_RAND2_8: return V_RAND2_8_O2;
+            case V_RAND3_4: return V_RAND3_4_O2;
             default: return -1;
         }
     }
@@ -71,16 +81,20 @@ static int variant_of(const agd_instance &a) {
             case V_DIAG2_8: return V_DIAG2_8_F;
             case V_DIAG2_16: return V_DIAG2_16_F;
             case V_DIAG3_4: return V_DIAG3_4_F;
+            case V_RAND2_8: return V_RAND2_8_F;
+            case V_RAND3_4: return V_RAND3_4_F;
             default: return -1;
         }
     }
     if (v < 0) return v;
     if (a.multip_step == 0.f) {
-        if (a.wall_dist && a.model == AGD_MODEL_RIEMANN) {
+        if (a.wall_dist && (a.model == AGD_MODEL_RIEMANN || a.model == AGD_MODEL_RANDER)) {
             switch (v) {
                 case V_RIEM2_8: return V_RIEM2_8_W;
                 case V_RIEM2_16: return V_RIEM2_16_W;
                 case V_RIEM3_4: return V_RIEM3_4_W;
+                case V_RAND2_8: return V_RAND2_8_W;
+                case V_RAND3_4: return V_RAND3_4_W;
                 default: return -1;
             }
         }
@@ -95,6 +109,8 @@ static int variant_of(const agd_instance &a) {
         case V_DIAG2_8: return V_DIAG2_8_MP;
         case V_DIAG2_16: return V_DIAG2_16_MP;
         case V_DIAG3_4: return V_DIAG3_4_MP;
+        case V_RAND2_8: return V_RAND2_8_MP;
+        case V_RAND3_4: return V_RAND3_4_MP;
         default: return -1;  // no multiprecision build of this tile shape
     }
 }
@@ -108,10 +124,12 @@ static int base_variant_of(const agd_instance &a) {
         if (a.model == AGD_MODEL_ISOTROPIC && a.shape_i[0] == 16 && a.shape_i[1] == 16) return V_ISO2_16;
         if (a.model == AGD_MODEL_DIAGONAL && a.shape_i[0] == 8 && a.shape_i[1] == 8) return V_DIAG2_8;
         if (a.model == AGD_MODEL_DIAGONAL && a.shape_i[0] == 16 && a.shape_i[1] == 16) return V_DIAG2_16;
+        if (a.model == AGD_MODEL_RANDER && a.shape_i[0] == 8 && a.shape_i[1] == 8) return V_RAND2_8;
     } else if (a.ndim == 3 && a.shape_i[0] == 4 && a.shape_i[1] == 4 && a.shape_i[2] == 4) {
         if (a.model == AGD_MODEL_RIEMANN) return V_RIEM3_4;
         if (a.model == AGD_MODEL_ISOTROPIC) return V_ISO3_4;
         if (a.model == AGD_MODEL_DIAGONAL) return V_DIAG3_4;
+        if (a.model == AGD_MODEL_RANDER) return V_RAND3_4;
     }
     return -1;
 }
@@ -160,7 +178,7 @@ static bool layout(const agd_instance *a, int n, WsLayout &L, Inst *out, bool st
         I.variant = variant_of(a[i]);
         I.stencil = nullptr;
         I.stencil_off = -1;
-        if (stencil_cache && a[i].model == AGD_MODEL_RIEMANN) {
+        if (stencil_cache && (a[i].model == AGD_MODEL_RIEMANN || a[i].model == AGD_MODEL_RANDER)) {
             I.stencil_off = stencil_floats;  // the pointer is set once the workspace is known
             stencil_floats += 2ll * (a[i].ndim * (a[i].ndim + 1) / 2) * I.size_tot;
         }

@@ -38,8 +38,12 @@ enum agd_status {
 };
 
 /* Diagonal: the Isotropic scheme (unit offsets) with weights per point and
- * axis, the squared dual costs (Isotropic_.h:32-36, _SetGeometry.py:134-135). */
-enum agd_model { AGD_MODEL_ISOTROPIC = 0, AGD_MODEL_RIEMANN = 1, AGD_MODEL_DIAGONAL = 2 };
+ * axis, the squared dual costs (Isotropic_.h:32-36, _SetGeometry.py:134-135).
+ * Rander: the Riemann scheme on the inverse of the quadratic part, with the
+ * neighbour values at x -/+ e shifted by +/-<w, e> for the drift w
+ * (Riemann_.h:23-29, FiniteDifferences.h:41-45; the second order neighbour
+ * is not shifted). */
+enum agd_model { AGD_MODEL_ISOTROPIC = 0, AGD_MODEL_RIEMANN = 1, AGD_MODEL_DIAGONAL = 2, AGD_MODEL_RANDER = 3 };
 
 /* One eikonal problem.  Mirrors what the reference's Interface prepares for its
  * `Update` kernel: traits (shape_i, niter_i, fim_front_width), module constants
@@ -65,7 +69,9 @@ typedef struct agd_instance {
     float *values_next; /* multiprecision: second buffers of the double-buffered */
     int32_t *valuesq_next; /*  iterations (valuesNext, valuesqNext of _SetArgs.py:171-177) */
     const float *geom;  /* Riemann: dual metric, symdim planes; Diagonal: squared dual
-                           costs 1/(c_k h_k)^2, ndim planes; tile layout (Isotropic: NULL) */
+                           costs 1/(c_k h_k)^2, ndim planes; Rander: the inverse of the
+                           quadratic part (symdim planes) then the drift (ndim planes),
+                           grid scales applied; tile layout (Isotropic: NULL) */
     const float *rhs;   /* tile layout: cost, seed values at seeds, +inf padding */
     const uint8_t *seedbits; /* tile layout bits, little endian, padding bits set;
                                 4-byte aligned */
@@ -184,6 +190,16 @@ int agd_prep_geom(int ndim, const int *shape, const int *shape_i, const float *m
  * vector for the whole grid. */
 int agd_prep_geom_diagonal(int ndim, const int *shape, const int *shape_i, const float *costs, int broadcast,
                            int is_dual, const double *grid_scales, float *geom, agd_stream_t stream);
+
+/* Rander model: metric.with_costs(gridScales).flatten(inverse_m=True), i.e. the
+ * inverse of m * outer(h, h) (symdim planes) then w * h (ndim planes), tile
+ * layout padded with +inf (_SetGeometry.py:138-139, Metrics/rander.py:61-68).
+ * metric: grid layout (*shape, symdim + ndim) [m lower triangle, w]; with
+ * is_dual it holds the dual metric, scaled by with_speeds(gridScales) and
+ * turned into the metric by Rander.dual (rander.py:35-39); broadcast != 0: one
+ * (symdim + ndim,) vector for the whole grid. */
+int agd_prep_geom_rander(int ndim, const int *shape, const int *shape_i, const float *metric, int broadcast,
+                         int is_dual, const double *grid_scales, float *geom, agd_stream_t stream);
 
 /* Grid layout -> tile layout for `nplanes` planes, padding with `pad`
  * (fd.block_expand).  src_broadcast != 0: src holds one value per plane. */

@@ -131,13 +131,15 @@ void sort_order(const T *v, int *o, int n) {
 // -------------------------------------------------------------- problem ---
 template <class T>
 struct Problem {
-    int D = 2, model = 0;  // model 0: isotropic, 1: Riemann, 2: diagonal
+    int D = 2, model = 0;  // model 0: isotropic, 1: Riemann, 2: diagonal, 3: Rander (Riemann + drift)
     int shape[3] = {1, 1, 1}, shape_i[3] = {1, 1, 1}, shape_o[3] = {1, 1, 1};
     int size_i = 1, size_o = 1;
     long size = 1;
     int nact = 2;
     T iso_w[3] = {0, 0, 0};
-    const float *geom = nullptr;  // dual metric planes (Riemann), squared dual costs (diagonal); grid layout
+    // dual metric planes (Riemann), squared dual costs (diagonal), the inverse of
+    // the quadratic part then the drift (Rander); grid layout
+    const float *geom = nullptr;
     const float *rhs = nullptr;
     const unsigned char *seed = nullptr;
     // Source factorisation: within fact_r2 (squared, index units) of fact_origin,
@@ -177,8 +179,9 @@ struct Problem {
         return true;
     }
 
+    bool diagonal() const { return model == 0 || model == 2; }  // unit offsets
     T scal_fact(const T *x, const T *y) const {
-        if (model != 1) {
+        if (diagonal()) {
             T r = 0;
             for (int i = 0; i < D; ++i) r += fact_m[i] * x[i] * y[i];
             return r;
@@ -189,9 +192,23 @@ struct Problem {
             for (int j = 0; j <= i; ++j, ++k) r += (i == j ? x[i] * y[i] : x[i] * y[j] + x[j] * y[i]) * fact_m[k];
         return r;
     }
-    // Shifts of the neighbour values at x - e_k (f[2k]) and x + e_k (f[2k+1]).
-    void shifts(const int *x, int (*e)[3], T *f) const {
+    // Shifts of the neighbour values at x - e_k (f[2k]) and x + e_k (f[2k+1]) of
+    // grid point x (flat index n): the factorisation's, then the drift's
+    // +<w, e_k> and -<w, e_k> (FiniteDifferences.h:41-45).
+    void shifts(const int *x, long n, int (*e)[3], T *f) const {
         for (int k = 0; k < 2 * nact; ++k) f[k] = 0;
+        factor_shifts(x, e, f);
+        if (model == 3) {
+            const int sd = D * (D + 1) / 2;
+            for (int k = 0; k < nact; ++k) {
+                T s = 0;
+                for (int c = 0; c < D; ++c) s += T(geom[(sd + c) * size + n]) * T(e[k][c]);
+                f[2 * k] += s;
+                f[2 * k + 1] -= s;
+            }
+        }
+    }
+    void factor_shifts(const int *x, int (*e)[3], T *f) const {
         if (!(fact_r2 > 0)) return;
         T xr[3] = {0, 0, 0}, r2 = 0;
         for (int c = 0; c < D; ++c) {
@@ -225,7 +242,7 @@ struct Problem {
             size_o *= shape_o[k];
             size *= shape[k];
         }
-        nact = model == 1 ? D * (D + 1) / 2 : D;
+        nact = diagonal() ? D : D * (D + 1) / 2;
     }
     long flat(const int *x) const {
         long n = 0;
@@ -239,7 +256,7 @@ struct Problem {
     }
     // Stencil at grid point n: weights w[nact], offsets e[nact][D].
     void stencil(long n, T *w, int (*e)[3]) const {
-        if (model != 1) {  // unit offsets; weights h^-2 (isotropic) or per point (diagonal, Isotropic_.h:32-36)
+        if (diagonal()) {  // unit offsets; weights h^-2 (isotropic) or per point (diagonal, Isotropic_.h:32-36)
             for (int k = 0; k < D; ++k) {
                 w[k] = model == 0 ? iso_w[k] : T(geom[k * size + n]);
                 for (int c = 0; c < D; ++c) e[k][c] = (c == k);
@@ -307,7 +324,9 @@ void order2_correct(T u0, T *v, const T *v2, int nact, T thr, char *o2) {
     for (int k = 0; k < nact; ++k) {
         const T d2 = std::fabs(u0 - 2 * v[k] + v2[k]);
         o2[k] = d2 < thr * bound && u0 > v[k];
-        if (o2[k]) v[k] += (v[k] - v2[k]) / 3;
+        // v + (v - v2) / 3 with the quotient and the sum in double, rounded once
+        // (the reference divides by the double literal 3., HFM.h:129)
+        if (o2[k]) v[k] = T(double(v[k]) + double(v[k] - v2[k]) / 3.0);
     }
 }
 
@@ -358,7 +377,7 @@ struct Solver {
             ul[n] = seed[n] ? rhs[n] : uold[n];
             int e[6][3];
             P.stencil(p, &w[n * 6], e);
-            if (!seed[n]) P.shifts(xt.data() + n * 3, e, &sh[n * 12]);
+            if (!seed[n]) P.shifts(xt.data() + n * 3, p, e, &sh[n * 12]);
             for (int k = 0; k < NA; ++k)
                 for (int s = 0; s < 2; ++s) {
                     const int ks = 2 * k + s, eps = 2 * s - 1;
@@ -526,7 +545,7 @@ struct Solver {
             if (!sd) {
                 P.stencil(p, wts, e);
                 T v[6], sh[12];
-                P.shifts(x, e, sh);
+                P.shifts(x, p, e, sh);
                 bool hid[12];
                 for (int k = 0; k < NA; ++k) {
                     for (int s = 0; s < 2; ++s) {

@@ -28,6 +28,8 @@ DEFAULT_TRAITS = {  # agd/Eikonal/HFM_CUDA/kernel_traits.py:61-88
     "Isotropic3": ((4, 4, 4), 8, 4),
     "Diagonal2": ((16, 16), 16, 4),
     "Diagonal3": ((4, 4, 4), 8, 4),
+    "Rander2": ((8, 8), 12, 8),
+    "Rander3": ((4, 4, 4), 8, 8),
 }
 STOP_CODES = ["Continue", "AtSeed", "InWall", "Stationnary", "PastSeed", "VanishingFlow"]
 
@@ -89,6 +91,20 @@ class Prepared:
     pass
 
 
+def rander_parts(metric_hfm, nd):
+    """Quadratic part (..., nd, nd) and drift (..., nd) of a Rander metric in HFM
+    layout (*shape, symdim + nd), float64."""
+    a = np.asarray(metric_hfm, np.float64)
+    sd = nd * (nd + 1) // 2
+    M = np.zeros(a.shape[:-1] + (nd, nd))
+    k = 0
+    for i in range(nd):
+        for j in range(i + 1):
+            M[..., i, j] = M[..., j, i] = a[..., k]
+            k += 1
+    return M, a[..., sd:]
+
+
 def wall_distance(walls, bound):
     """L1 distance to the nearest wall point, saturated at 255 and set to 255
     beyond `bound` (_SetGeometry.py:262-280): `bound` min-plus passes of the
@@ -115,7 +131,8 @@ def prepare(case):
     pr = Prepared()
     pr.model = str(case["model"])
     pr.ndim = int(pr.model[-1])
-    pr.riemann = pr.model.startswith("Riemann")
+    pr.rander = pr.model.startswith("Rander")
+    pr.riemann = pr.model.startswith("Riemann") or pr.rander  # Selling stencil
     pr.diagonal = pr.model.startswith("Diagonal")
     pr.shape = tuple(int(s) for s in np.asarray(case["dims"]))
     pr.h = np.broadcast_to(np.asarray(case.get("gridScales", case.get("gridScale")), np.float32), (pr.ndim,)).copy()
@@ -127,7 +144,16 @@ def prepare(case):
         niter = int(tr.get("niter_i", niter))
     pr.shape_i, pr.niter_i, pr.front = tuple(si), niter, int(case.get("fim_front_width", front))
     cost = np.broadcast_to(np.asarray(case.get("cost", 1.0), np.float32), pr.shape).astype(np.float32)
-    pr.geom = dual_metric_flat(case["metric"], pr.h) if pr.riemann else None
+    pr.geom = dual_metric_flat(case["metric"], pr.h) if pr.riemann and not pr.rander else None
+    if pr.rander:  # metric.with_costs(h).flatten(inverse_m=True), float32 (_SetGeometry.py:138-139)
+        mh = np.broadcast_to(np.asarray(case["metric"], np.float32), pr.shape + (pr.ndim * (pr.ndim + 3) // 2,))
+        M, w = rander_parts(mh, pr.ndim)
+        hf = pr.h.astype(np.float32)
+        hh = (hf[:, None] * hf[None, :]).astype(np.float32)  # Rander.with_costs: m * outer(h, h)
+        Mi = np.linalg.inv((M.astype(np.float32) * hh).astype(np.float32)).astype(np.float32)
+        wh = (w.astype(np.float32) * hf).astype(np.float32)
+        planes = [Mi[..., i, j] for i in range(pr.ndim) for j in range(i + 1)] + [wh[..., i] for i in range(pr.ndim)]
+        pr.geom = np.ascontiguousarray(np.stack(planes), np.float32)
     if pr.diagonal:  # squared dual costs 1 / (c h)^2, float32 (_SetGeometry.py:134-135)
         costs = np.moveaxis(np.broadcast_to(np.asarray(case["metric"], np.float32), pr.shape + (pr.ndim,)), -1, 0)
         pr.geom = np.ascontiguousarray((np.float32(1) / (costs * pr.h.reshape((-1,) + (1,) * pr.ndim))) ** 2,
@@ -179,7 +205,13 @@ def _cost_metric(pr, case, cost):
     nd = pr.ndim
     h = pr.h.astype(np.float64)
     c = np.asarray(cost, np.float64)
-    if pr.riemann:
+    if pr.rander:  # (M, w) -> (c^2 h M h, c h w): the quadratic part; _cost_drift gives the drift
+        M, _ = rander_parts(np.broadcast_to(np.asarray(case["metric"], np.float64),
+                                            tuple(pr.shape) + (nd * (nd + 3) // 2,)), nd)
+
+        def cm(p):
+            return c[tuple(p)] ** 2 * M[tuple(p)] * np.outer(h, h)
+    elif pr.riemann:
         mf = np.broadcast_to(np.asarray(case["metric"], np.float64), tuple(pr.shape) + (nd * (nd + 1) // 2,))
         tri = [(i, j) for i in range(nd) for j in range(i + 1)]
 
@@ -197,6 +229,29 @@ def _cost_metric(pr, case, cost):
         def cm(p):
             return np.diag((c[tuple(p)] * h) ** 2)
     return cm
+
+
+def _cost_drift(pr, case, cost):
+    """Rander: grid point -> the drift of the cost metric, c h w (index units)."""
+    nd = pr.ndim
+    _, w = rander_parts(np.broadcast_to(np.asarray(case["metric"], np.float64), tuple(pr.shape) + (nd * (nd + 3) // 2,)),
+                        nd)
+    c = np.asarray(cost, np.float64)
+    h = pr.h.astype(np.float64)
+    return lambda p: c[tuple(p)] * h * w[tuple(p)]
+
+
+def _interp(pr, seed, f):
+    """Multilinear interpolation of the grid function f at a continuous index seed."""
+    nd = pr.ndim
+    shape = np.array(pr.shape)
+    lo = np.clip(np.floor(seed).astype(int), 0, shape - 1)
+    frac = np.clip(seed - lo, 0.0, 1.0)
+    out = 0.0
+    for bits in np.ndindex(*([2] * nd)):
+        w = np.prod([fr if b else 1.0 - fr for b, fr in zip(bits, frac)])
+        out = out + w * f(np.minimum(lo + np.array(bits), shape - 1))
+    return out
 
 
 def _seed_metric(pr, case, cost, seed):
@@ -233,10 +288,12 @@ def _spread_seed(pr, case, cost, seed, seed_value, r):
     pts = pts[np.all((pts >= -0.5) & (pts < shape - 0.5), axis=1)]
     cm = _cost_metric(pr, case, cost)
     m0 = _seed_metric(pr, case, cost, seed)
+    drift = _cost_drift(pr, case, cost) if pr.rander else (lambda p: np.zeros(nd))
+    w0 = _interp(pr, seed, drift) if pr.rander else np.zeros(nd)
     vals = []
     for p in pts:
-        d = p - seed
-        vals.append(seed_value + 0.5 * (np.sqrt(d @ m0 @ d) + np.sqrt(d @ cm(p) @ d)))
+        d = p - seed  # Rander norms: sqrt(<d, M d>) + <w, d>
+        vals.append(seed_value + 0.5 * (np.sqrt(d @ m0 @ d) + w0 @ d + np.sqrt(d @ cm(p) @ d) + drift(p) @ d))
     return pts.astype(int), np.asarray(vals, np.float32)
 
 
@@ -268,7 +325,8 @@ def eikonal(pr, dtype=np.float32, values=None, nthreads=1, flow=False, nitermax=
         met = np.zeros(6)
         met[: len(fac[2])] = fac[2]
         L.agdo_set_factor(ctypes.c_double(fac[0]), _p(org), _p(met))
-    niter = L.agdo_eikonal(int(dtype == np.float64), pr.ndim, 1 if pr.riemann else (2 if pr.diagonal else 0),
+    niter = L.agdo_eikonal(int(dtype == np.float64), pr.ndim,
+                           3 if pr.rander else (1 if pr.riemann else (2 if pr.diagonal else 0)),
                            (ctypes.c_int * pr.ndim)(*pr.shape), (ctypes.c_int * pr.ndim)(*pr.shape_i),
                            pr.niter_i, pr.front, _p(iso), _p(geom), _p(np.ascontiguousarray(pr.rhs)),
                            _p(np.ascontiguousarray(pr.seed_mask)), _p(u), ctypes.c_double(pr.atol),
@@ -378,8 +436,11 @@ def run(case, dtype=np.float32, nthreads=1):
     if "tips" in case:
         out["geodesics"], out["geodesic_stopping_criteria"] = geodesics(
             pr, r["values"], r["flow_vector"], r["flow_weightsum"], case["tips"])
+    norm = flow_normalization(pr, case, r["flow_vector"]) if need_flow and pr.rander else None
     if "costVariation" in case:
         rhs = forward_rhs(pr, case["costVariation"], case.get("seedValueVariation"))
+        if norm is not None:  # drift models (_PostProcess.py:185)
+            rhs = rhs * norm
         out["valueVariation"] = np.stack(
             [forward(pr, r["values"], r["flow_weights"], r["flow_indices"], r["flow_weightsum"], x) for x in rhs], -1)
     if "sensitivity" in case:
@@ -389,5 +450,20 @@ def run(case, dtype=np.float32, nthreads=1):
         out["seedValueSensitivity"] = lam[pos][:, None]
         cs = lam.copy()
         cs[pos] = 0
+        if norm is not None:  # drift models (_PostProcess.py:213-214)
+            cs = cs / norm
         out["costSensitivity"] = cs[..., None]
     return out
+
+
+def flow_normalization(pr, case, flow_vector):
+    """Drift models: 1 at the seeds, else the norm of -flow_vector for the
+    metric with the grid scales applied (_PostProcess.py:80-88)."""
+    nd = pr.ndim
+    M, w = rander_parts(np.broadcast_to(np.asarray(case["metric"], np.float64),
+                                        tuple(pr.shape) + (nd * (nd + 3) // 2,)), nd)
+    h = pr.h.astype(np.float64)
+    v = -np.moveaxis(np.asarray(flow_vector, np.float64), 0, -1)
+    Mh = M * np.outer(h, h)
+    n = np.sqrt(np.einsum("...i,...ij,...j->...", v, Mh, v)) + np.einsum("...i,...i->...", w * h, v)
+    return np.where(pr.seed_mask.astype(bool), 1.0, n)

@@ -9,7 +9,8 @@
 //   AGDREF_LOG2_SIZE_I, AGDREF_NITER_I, AGDREF_MULTIP (0|1), AGDREF_FLOW (0|1),
 //   AGDREF_FACTOR (0|1, source factorisation, factor_macro of _Kernel.py:47-49),
 //   AGDREF_ORDER2 (0|1, second order scheme, order2_macro of _Kernel.py:51-54),
-//   AGDREF_WALLS (0|1, obstacles, walls_macro of _Kernel.py:111).
+//   AGDREF_WALLS (0|1, obstacles, walls_macro of _Kernel.py:111),
+//   AGDREF_DRIFT (0|1, the Rander model: Riemann_.h with a drift, _Kernel.py:58-59).
 //
 // The block below states the same compile-time traits that the reference's
 // `cupy_module_helper.traits_header` emits for these models
@@ -67,6 +68,12 @@ const int niter_i = AGDREF_FLOW ? 1 : AGDREF_NITER_I;
 #ifndef AGDREF_DIAG
 #define AGDREF_DIAG 0
 #endif
+#ifndef AGDREF_DRIFT
+#define AGDREF_DRIFT 0
+#endif
+#if AGDREF_DRIFT
+#define drift_macro 1
+#endif
 #if AGDREF_ISO
 #define geom_indep_macro AGDREF_NDIM
 #elif AGDREF_DIAG
@@ -74,7 +81,7 @@ const int niter_i = AGDREF_FLOW ? 1 : AGDREF_NITER_I;
 #define geom_size_macro AGDREF_NDIM
 #else
 #define geom_indep_macro 0
-#define geom_size_macro ((AGDREF_NDIM * (AGDREF_NDIM + 1)) / 2)
+#define geom_size_macro ((AGDREF_NDIM * (AGDREF_NDIM + 1)) / 2 + (AGDREF_DRIFT ? AGDREF_NDIM : 0))
 #endif
 #define hfm_debug_macro false
 const int size_i = AGDREF_SIZE_I;
@@ -283,7 +290,7 @@ int agdref_flow(const int *shape, const float *iso_w, float mstep, float mmax, f
 
 // Direct access to the reference's per-point Selling decomposition
 // (Geometry2.h:21-48 / Geometry3.h:22-58, via Riemann_.h:23-29) for golden vectors.
-#if !AGDREF_ISO && !AGDREF_DIAG && !AGDREF_FLOW && !AGDREF_MULTIP
+#if !AGDREF_ISO && !AGDREF_DIAG && !AGDREF_DRIFT && !AGDREF_FLOW && !AGDREF_MULTIP
 void agdref_selling(const float *m, int n, float *w, int *e) {
     for (int p = 0; p < n; ++p) {
         Scalar wl[symdim];

@@ -39,6 +39,7 @@ FACTOR_CASES = ["riem2_factor", "iso2_factor"]  # source factorisation (factorin
 ORDER2_CASES = ["riem2_order2", "iso2_order2", "riem3_order2"]  # second order scheme (order: 2)
 WALL_CASES = ["riem2_walls", "iso2_walls", "riem3_walls"]  # obstacles (walls, wallDistBound)
 DIAG_CASES = ["diag2", "diag2_factor", "diag2_order2", "diag2_walls", "diag3"]  # Diagonal2/3 models
+RANDER_CASES = ["rand2", "rand2_factor", "rand2_order2", "rand2_walls", "rand3"]  # Rander2/3 (drift)
 
 
 @pytest.fixture(params=CASES)

@@ -83,6 +83,8 @@ MODELS = {
     # the linear (AD) kernels depend on the tile shape only: the Isotropic builds serve
     "Diagonal2": dict(tag="diag2", lin="iso2", shape_i=(16, 16), niter_i=16, front=4),
     "Diagonal3": dict(tag="diag3", lin="iso3", shape_i=(4, 4, 4), niter_i=8, front=4),
+    "Rander2": dict(tag="rand2", lin="riem2", shape_i=(8, 8), niter_i=12, front=8),
+    "Rander3": dict(tag="rand3", lin="riem3", shape_i=(4, 4, 4), niter_i=8, front=8),
 }
 
 
@@ -104,6 +106,21 @@ class RefPipeline:
         self.size_o = int(np.prod(self.shape_o))
         self.multip = bool(case.get("multiprecision", False))
 
+    def rander(self, dtype):
+        """Metrics.Rander(m, w) from the case's HFM array (*shape, symdim + ndim).
+        (The reference's Rander.from_HFM infers the dimension from the array
+        length alone, which fails for Rander2: its users build the object.)"""
+        nd = self.ndim
+        arr = np.moveaxis(np.asarray(self.c["metric"], dtype), -1, 0)
+        sd = nd * (nd + 1) // 2
+        m = np.zeros((nd, nd) + arr.shape[1:], dtype)
+        k = 0
+        for i in range(nd):
+            for j in range(i + 1):
+                m[i, j] = m[j, i] = arr[k]
+                k += 1
+        return self.Metrics.Rander(m, arr[sd:])
+
     def bexp(self, a, cval):
         return np.ascontiguousarray(self.fd.block_expand(a, self.shape_i, mode="constant", constant_values=cval))
 
@@ -123,6 +140,9 @@ class RefPipeline:
             metric = self.Metrics.Riemann.from_HFM(np.asarray(c["metric"], np.float32))
             dual = metric.with_costs(self.h).dual()
             self.geom = self.bexp(dual.flatten().astype(np.float32), np.inf)
+        elif self.model.startswith("Rander"):  # geom = metric.flatten(inverse_m=True) (_SetGeometry.py:138-139)
+            self.metric = self.rander(np.float32).with_costs(self.h)
+            self.geom = self.bexp(np.asarray(self.metric.flatten(inverse_m=True), np.float32), np.inf)
         elif self.model.startswith("Diagonal"):  # geom = dualMetric.costs**2 (_SetGeometry.py:134-135)
             metric = self.Metrics.Diagonal.from_HFM(np.asarray(c["metric"], np.float32))
             dual = metric.with_costs(self.h).dual()
@@ -139,7 +159,9 @@ class RefPipeline:
         if fr:  # _Kernel.py:47-49, 301-308; seedRadius defaults to 2 (_SetArgs.py:40-43)
             seed = self.point_from_index(seeds, to=True)[0].astype(np.float64)
             hfm = np.asarray(self.cost_metric(cost).at(seed).to_HFM(), np.float32)
-            if not self.model.startswith("Riemann"):
+            if self.model.startswith("Rander"):  # the drift is left out (_Kernel.py:305-306)
+                hfm = hfm[: -self.ndim]
+            elif not self.model.startswith("Riemann"):
                 hfm = hfm ** 2
             self.factor = (seed.astype(np.float32), np.float32(fr * fr), hfm.astype(np.float32))
         radius = float(c.get("seedRadius", 2.0 if fr else 0.0))
@@ -201,6 +223,8 @@ class RefPipeline:
             metric = self.Metrics.Riemann.from_HFM(np.asarray(self.c["metric"], np.float64))
         elif self.model.startswith("Diagonal"):
             metric = self.Metrics.Diagonal.from_HFM(np.asarray(self.c["metric"], np.float64))
+        elif self.model.startswith("Rander"):
+            metric = self.rander(np.float64)
         else:
             metric = self.Metrics.Diagonal(np.ones(nd))
         cm = metric.with_costs(self.h.astype(np.float64)).with_cost(np.asarray(cost, np.float64))
@@ -266,7 +290,7 @@ class RefPipeline:
         L = lib(f"libagdref_flow_{self.md['tag']}{'f' if self.factor else ''}{self.o2tag}.so")
         self.set_factor(L)
         nd, st = self.ndim, self.size_o * self.size_i
-        nact = self.ndim if not self.model.startswith("Riemann") else self.ndim * (self.ndim + 1) // 2
+        nact = self.ndim * (self.ndim + 1) // 2 if self.model.startswith(("Riemann", "Rander")) else self.ndim
         self.nact = nact
         oi = self.shape_o + self.shape_i
         self.fw = np.empty((nact,) + oi, np.float32)
@@ -276,6 +300,10 @@ class RefPipeline:
         L.agdref_flow((ctypes.c_int * nd)(*self.shape), ptr(self.iso_w), ctypes.c_float(0), ctypes.c_float(0),
                       ptr(self.values_b), None, ptr(self.geom), ptr(self.seeds_b), ptr(self.rhs_b),
                       ptr(self.fw), ptr(self.fws), ptr(self.fi), ptr(self.fv))
+        self.flow_norm = None
+        if self.model.startswith("Rander"):  # drift models: flow normalisation (_PostProcess.py:80-88)
+            fv = np.stack([self.bsq(v) for v in self.fv])
+            self.flow_norm = np.where(self.seedTags, np.float32(1), self.metric.norm(-fv)).astype(np.float32)
 
     def infconv_eucl(self):
         nd = self.ndim
@@ -373,6 +401,8 @@ class RefPipeline:
         pos = tuple(self.seedIndices.T)
         seedS = allS[pos].copy()
         allS[pos] = 0
+        if self.flow_norm is not None:  # _PostProcess.py:213-214
+            allS = allS / self.flow_norm[..., None]
         return allS, seedS
 
     def forward_ad(self, cost_var, seed_var):
@@ -393,6 +423,8 @@ class RefPipeline:
         for j in range(n_ad):
             grad[j][pos] = seed_var[j]
         rhs_grid = np.where(self.seedTags, grad, grad * value).astype(np.float32)
+        if self.flow_norm is not None:  # _PostProcess.py:185
+            rhs_grid = (rhs_grid * self.flow_norm).astype(np.float32)
         L = lib(f"libagdref_lin_{self.md.get('lin', self.md['tag'])}_f.so")
         L.agdref_nindex.restype = ctypes.c_int
         assert L.agdref_nindex() == len(indices)
@@ -619,6 +651,60 @@ def make_cases():
     cv[..., 1].reshape(-1)[rng.choice(70 * 53, 3, replace=False)] = 1.0
     cc["costVariation"] = cv
     cc["seedValueVariation"] = np.ascontiguousarray(rng.uniform(-1, 1, (2, 2)).T).astype(np.float32)
+    # Rander models (Riemann metric plus a drift with |w|_{M^-1} < 1), own random stream
+    rng = np.random.default_rng(8765)
+
+    def rander(shape, nd, sigma, lam_max, wmax):
+        m = riemann2_metric(rng, shape, sigma, lam_max) if nd == 2 else riemann3_metric(rng, shape, sigma, lam_max)
+        M = np.moveaxis(m, (0, 1), (-2, -1)).astype(np.float64)
+        w = np.stack([smooth_noise(rng, shape, sigma) for _ in range(nd)], -1)
+        # scale the drift to a fraction of the unit ball of the dual norm: |w|_{M^-1} <= wmax
+        wn = np.sqrt(np.einsum("...i,...ij,...j->...", w, np.linalg.inv(M), w))
+        w = w / wn.max() * wmax
+        flat = np.stack([M[..., i, j] for i in range(nd) for j in range(i + 1)], -1)
+        return np.concatenate([flat, w], -1).astype(np.float32)  # HFM layout (*shape, symdim + ndim)
+    sh = (61, 77)
+    c = dict(model="Rander2", **rect(sh, 1.0 / 61))
+    c["metric"] = rander(sh, 2, 6.0, 10.0, 0.7)
+    c["seeds"] = np.array([[0.2, 0.3], [0.7, 0.9]], np.float32)
+    c["seedValues"] = np.array([0.0, 0.1], np.float32)
+    c["tips"] = rng.uniform(0.05, 0.95, (5, 2)).astype(np.float32) * np.array([1.0, 77 / 61], np.float32)
+    sens = np.zeros(sh + (1,), np.float32)
+    sens.reshape(-1)[rng.choice(int(np.prod(sh)), 5, replace=False)] = 1.0
+    c["sensitivity"] = sens
+    cv = np.stack([smooth_noise(rng, sh, 2.0), np.zeros(sh)], -1).astype(np.float32)
+    cv[..., 1].reshape(-1)[rng.choice(int(np.prod(sh)), 3, replace=False)] = 1.0
+    c["costVariation"] = cv
+    c["seedValueVariation"] = np.ascontiguousarray(rng.uniform(-1, 1, (2, 2)).T).astype(np.float32)
+    cases["rand2"] = c
+    c = {k: v for k, v in cases["rand2"].items() if k not in ("sensitivity", "costVariation", "seedValueVariation",
+                                                              "seedValues")}
+    c["seeds"] = np.array([[0.43, 0.61]], np.float32)
+    c["factoringRadius"] = 8.0
+    c["tips"] = c["tips"][:3]
+    cases["rand2_factor"] = c
+    c = {k: v for k, v in cases["rand2"].items() if k not in ("sensitivity", "costVariation", "seedValueVariation")}
+    c["order"] = 2
+    cases["rand2_order2"] = c
+    c = {k: v for k, v in cases["rand2"].items() if k not in ("sensitivity", "costVariation", "seedValueVariation")}
+    w = np.zeros(sh, bool)
+    w[25, 5:70] = True
+    w[25, 40:44] = False
+    c["walls"] = w
+    cases["rand2_walls"] = c
+    c = {k: v for k, v in cases["rand2"].items() if k not in ("sensitivity", "costVariation", "seedValueVariation",
+                                                              "tips")}
+    c["multiprecision"] = True
+    cases["rand2_mp"] = c
+    sh = (20, 22, 19)
+    c = dict(model="Rander3", **rect(sh, 1.0 / 20))
+    c["metric"] = rander(sh, 3, 2.0, 6.0, 0.6)
+    c["seeds"] = np.array([[0.45, 0.5, 0.48]], np.float32)
+    c["tips"] = rng.uniform(0.05, 0.9, (3, 3)).astype(np.float32)
+    sens = np.zeros(sh + (1,), np.float32)
+    sens.reshape(-1)[rng.choice(int(np.prod(sh)), 5, replace=False)] = 1.0
+    c["sensitivity"] = sens
+    cases["rand3"] = c
     return cases
 
 
@@ -643,6 +729,9 @@ def run_case(name, case):
         out["values_after_flow"] = pipe.values().astype(np.float32)
         out["flow_vector"] = np.stack([pipe.bsq(v) for v in pipe.fv]).astype(np.float32)
         out["flow_weightsum"] = pipe.bsq(pipe.fws).astype(np.float32)
+        if pipe.flow_norm is not None:  # hfmOut['flow'] of a drift model: normalised, physical units
+            h = pipe.h.reshape((-1,) + (1,) * pipe.ndim)
+            out["flow_export"] = (out["flow_vector"] / pipe.flow_norm * -h).astype(np.float32)
         # exportActiveNeighs: positive flow weights as bits (cuda/Update.h:187,206)
         out["activeNeighs"] = sum((pipe.bsq(w) > 0).astype(np.int32) << k for k, w in enumerate(pipe.fw))
         if "tips" in case:
