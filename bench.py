@@ -190,7 +190,7 @@ def main():
     ap.add_argument("--ctas", type=int, default=0)
     ap.add_argument("--wpc", type=int, default=4)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--e2e-steps", type=int, default=5)
+    ap.add_argument("--e2e-steps", type=int, default=12)
     ap.add_argument("--niter-i", type=int, default=0, help="local iterations per tile visit (0: the default, 8)")
     ap.add_argument("--front", type=int, default=0, help="FIM front width (0: the default, 4)")
     ap.add_argument("--tile", type=int, default=8, help="tile side (8: the default, or 16)")
