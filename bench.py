@@ -153,6 +153,17 @@ def cpu_baseline(n, seconds_budget=25.0):
     return solves / dt, updates / dt, cores, f"{solves} Riemann2 {n}^2 solve(s) of the same field distribution, float32"
 
 
+def max_over_ranks(x, dist, device="cuda"):
+    """The largest value of x over the ranks (every rank gets it); x itself
+    without a process group.  Timings of several ranks are reported this way."""
+    if dist is None:
+        return float(x)
+    import torch
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t)
+
+
 def run_reference(args, rank):
     if rank != 0:
         return
@@ -281,10 +292,7 @@ def main():
         torch.cuda.synchronize()
     elapsed = t0.elapsed_time(t1) / 1000.0
     kern = np.array([a.elapsed_time(b) / 1000.0 for a, b in evs])
-    if dist:
-        tt = torch.tensor([elapsed], device="cuda")
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        elapsed = float(tt)
+    elapsed = max_over_ranks(elapsed, dist)
     niter, status, visits = plan.read_stats()
     assert not status.any()
     updates_per_step = int(visits.sum()) * args.tile ** 2
@@ -326,9 +334,11 @@ def main():
 
         run_solver(3)  # warm up both buffer sets
         torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
         t_e = time.perf_counter()
         run_solver(args.e2e_steps)
-        te = time.perf_counter() - t_e
+        te = max_over_ranks(time.perf_counter() - t_e, dist)
         e2e = {"value": B * args.e2e_steps * world / te, "unit": "solves/s", "h2d_bytes_per_step": int(h2d),
                "d2h_bytes_per_step": int(d2h), "api": "Eikonal.BatchSolver.submit (two buffer sets)"}
         del solver
@@ -357,9 +367,11 @@ def main():
 
         run_dictin(2)
         torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
         t_e = time.perf_counter()
         run_dictin(args.e2e_steps)
-        te = time.perf_counter() - t_e
+        te = max_over_ranks(time.perf_counter() - t_e, dist)
         e2e_dictin = {"value": B * args.e2e_steps * world / te, "unit": "solves/s",
                       "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
                       "api": "Eikonal.SubmitBatch of dictIn inputs (two streams)"}
