@@ -140,6 +140,7 @@ struct InstState {
     int pending;       // tiles of the current epoch not yet finished
     unsigned cnt[2];   // lengths of the instance's lists, by epoch parity
     int done;
+    unsigned first;    // ticket of the first entry of epoch 1
 };
 
 struct Ctrl {
@@ -516,26 +517,38 @@ static __global__ void setup_tiles(Sched S, int total_tiles) {
 
 // Epoch 1 of every instance: one warp per instance publishes its first list.
 static __global__ void publish_first(Sched S) {
-    const int ii = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
-    const int lane = threadIdx.x & 31;
+    const int ii = blockIdx.x * blockDim.x + threadIdx.x;
     if (ii >= S.ninst) return;
-    const Inst &I = S.inst[ii];
     InstState &st = S.ist[ii];
     const int n = (int)st.cnt[1];
     if (n == 0) {
-        if (lane == 0) { st.done = 1; S.stats[ii].niter_o = 0; }
+        st.done = 1;
+        S.stats[ii].niter_o = 0;
         return;
     }
-    if (lane == 0) {
-        st.cnt[0] = 0u;
-        st.pending = n;
-        st.epoch = 1;
-        S.stats[ii].tile_visits = n;
-        atomicAdd(&S.ctrl->active, 1);
-        __threadfence();
+    st.cnt[0] = 0u;
+    st.pending = n;
+    st.epoch = 1;
+    S.stats[ii].tile_visits = n;
+    atomicAdd(&S.ctrl->active, 1);
+    st.first = atomicAdd(&S.ctrl->tail, (unsigned)n);  // the instance's tickets for epoch 1
+}
+
+// The entries of epoch 1, one thread per tile position: the queue was just
+// cleared, so every slot is free, and the workers start after this kernel.
+static __global__ void publish_first_slots(Sched S, int total_tiles) {
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= total_tiles) return;
+    int lo = 0, hi = S.ninst - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (S.inst[mid].tile_base <= j) lo = mid; else hi = mid - 1;
     }
-    __syncwarp();
-    enqueue_warp(S, S.list1 + I.tile_base, n, 1, lane);
+    const InstState &st = S.ist[lo];
+    const int k = j - S.inst[lo].tile_base;
+    if (k >= (int)st.cnt[1]) return;
+    const unsigned ticket = st.first + (unsigned)k;
+    S.queue[ticket % S.qcap] = slot_word(ticket, 1, (unsigned)S.list1[j]);
 }
 
 static __global__ void finish_stats(Sched S, agd_stats *out) {
@@ -609,7 +622,8 @@ static int run_sched(const WsLayout &L, void *ws, int n, const typename Visitor:
     if ((err = Visitor::prepare(S, L, st)) != cudaSuccess) return set_cuda_error("prepare", err);
     setup_tiles<<<(L.total_tiles + 255) / 256, 256, 0, st>>>(S, L.total_tiles);
     if ((err = cudaGetLastError()) != cudaSuccess) return set_cuda_error("setup_tiles", err);
-    publish_first<<<(n + 7) / 8, 256, 0, st>>>(S);
+    publish_first<<<(n + 127) / 128, 128, 0, st>>>(S);
+    publish_first_slots<<<(L.total_tiles + 255) / 256, 256, 0, st>>>(S, L.total_tiles);
     if ((err = cudaGetLastError()) != cudaSuccess) return set_cuda_error("publish_first", err);
     // 8-warp CTAs only where their static shared memory fits in 48 KB
     constexpr bool kWide = sizeof(typename Visitor::Smem) * 8 + sizeof(int) * kSmemInst <= 48 * 1024;

@@ -190,6 +190,90 @@ def run_reference(args, rank):
     }), flush=True)
 
 
+def run_other_path(args):
+    """The other two kernels of the path, timed on their configurations' sizes
+    (one GPU, CUDA events): `--path geodesic`, the backtracking ODE from 64 tips
+    on Riemann2 1024^2 (one thread per tip: latency-bound, so the figure is ODE
+    steps/s, with the bytes an ODE step reads: 4 cells x (value, 2 flow planes,
+    weight sum) x 4 B); `--path reverse`, the reverse adjoint (transpose and
+    linear solve) of the arrival times at 128 receivers on Riemann3 200^3, with
+    the algorithmic bytes of a linear tile visit point: 6 weights, 6 indices
+    and the sensitivity read, the sensitivity written (56 B)."""
+    import torch
+    from scipy.ndimage import gaussian_filter
+    from adaptivegriddiscretizations_b200 import Eikonal
+    from adaptivegriddiscretizations_b200.Eikonal.HFM_CUDA import Interface
+    torch.cuda.set_device(0)
+    rng = np.random.default_rng(5)
+    if args.path == "geodesic":
+        n = 1024
+        metrics, seeds = make_fields(n, 1, 21, sigma=16.0)
+        tips = rng.uniform(0.02, 0.98, (64, 2)).astype(np.float32)
+        d = dict(model="Riemann2", dims=np.array([n, n], np.float32), gridScales=np.full(2, 1.0 / n, np.float32),
+                 origin=np.zeros(2, np.float32), metric=metrics[0], seeds=seeds[0], tips=tips, verbosity=0)
+        workload = f"Riemann2 {n}x{n}, geodesics from 64 tips (flow already computed)"
+    else:
+        n = 200
+        q = gaussian_filter(rng.standard_normal((4, n, n, n)).astype(np.float32), (0, 6, 6, 6), mode="wrap")
+        q /= np.linalg.norm(q, axis=0, keepdims=True)
+        w, x, y, z = q
+        rot = np.stack([np.stack([1 - 2 * (y * y + z * z), 2 * (x * y - z * w), 2 * (x * z + y * w)], -1),
+                        np.stack([2 * (x * y + z * w), 1 - 2 * (x * x + z * z), 2 * (y * z - x * w)], -1),
+                        np.stack([2 * (x * z - y * w), 2 * (y * z + x * w), 1 - 2 * (x * x + y * y)], -1)], -2)
+        ev = np.exp(rng.uniform(0, np.log(25.0), (n, n, n, 3))).astype(np.float32)
+        M = rot @ (ev[..., :, None] * np.swapaxes(rot, -1, -2))
+        metric = np.stack([M[..., i, j] for i in range(3) for j in range(i + 1)], -1).astype(np.float32)
+        sens = np.zeros((n, n, n, 1), np.float32)
+        sens.reshape(-1)[rng.choice(n ** 3, 128, replace=False)] = 1.0
+        d = dict(model="Riemann3", dims=np.array([n] * 3, np.float32), gridScales=np.full(3, 1.0 / n, np.float32),
+                 origin=np.zeros(3, np.float32), metric=metric, seeds=np.array([[0.5, 0.5, 0.5]], np.float32),
+                 sensitivity=sens, verbosity=0)
+        workload = f"Riemann3 {n}^3, reverse sensitivity of the arrival times at 128 receivers (flow already computed)"
+    itf = Interface(Eikonal.dictIn(d))
+    itf.SetKernelTraits()
+    itf.SetGeometry()
+    itf.SetArgs()
+    itf.Solve()
+    itf.PostProcess()
+    import copy
+    keys = copy.deepcopy(itf.hfmOut["keys"])  # each key is read once per Run: restored for every repetition
+    call = itf.GetGeodesics if args.path == "geodesic" else itf.SolveAD
+
+    def work():
+        itf.hfmOut["keys"] = copy.deepcopy(keys)
+        call()
+
+    for _ in range(max(3, args.warmup)):
+        work()
+    torch.cuda.synchronize()
+    ts = []
+    for _ in range(args.steps):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        itf.hfmOut["keys"] = copy.deepcopy(keys)
+        e0.record()
+        call()
+        e1.record()
+        torch.cuda.synchronize()
+        ts.append(e0.elapsed_time(e1) / 1e3)
+    t = float(np.median(ts))
+    hbm, peak_kind = peaks()
+    if args.path == "geodesic":
+        steps = sum(int(g.shape[1]) for g in itf.hfmOut["geodesics"])
+        value, unit, nbytes = steps / t, "geodesic ODE steps/s", steps * 64
+        extra = {"stops": {c: itf.hfmOut["geodesic_stopping_criteria"].count(c)
+                           for c in set(itf.hfmOut["geodesic_stopping_criteria"])}, "points": steps}
+    else:
+        visits = int(itf.stats["reverseAD"]["nupdate_o_total"])
+        value, unit, nbytes = 1.0 / t, "reverse solves/s", visits * itf.size_i * 56
+        extra = {"tile_visits": visits, "epochs": int(itf.stats["reverseAD"]["niter_o"])}
+    print(json.dumps({"metric": f"{args.path} path", "value": value, "unit": unit, "ms_per_step": 1e3 * t,
+                      "steps": args.steps, "warmup": args.warmup, "data": "synthetic",
+                      "config": dict({"workload": workload}, **extra),
+                      "roofline": {"bound": "latency" if args.path == "geodesic" else "hbm",
+                                   "achieved": nbytes / t / 1e9, "peak": hbm, "unit": "GB/s",
+                                   "frac": nbytes / t / 1e9 / hbm, "peak_kind": peak_kind}}), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -205,6 +289,8 @@ def main():
     ap.add_argument("--niter-i", type=int, default=0, help="local iterations per tile visit (0: the default, 8)")
     ap.add_argument("--front", type=int, default=0, help="FIM front width (0: the default, 4)")
     ap.add_argument("--tile", type=int, default=8, help="tile side (8: the default, or 16)")
+    ap.add_argument("--path", default="solve", choices=["solve", "geodesic", "reverse"],
+                    help="solve: the benchmark (default); geodesic / reverse: the other kernels of the path")
     ap.add_argument("--warm-oracle", type=float, default=0.0,
                     help="experiment: warm start every solve from (1+eps) x its cold solution, all tiles active")
     args = ap.parse_args()
@@ -213,6 +299,9 @@ def main():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     if args.impl == "reference":
         run_reference(args, rank)
+        return
+    if args.path != "solve":
+        run_other_path(args)
         return
 
     import torch
