@@ -1,9 +1,9 @@
 // Geodesic backtracking on B200: the distance-to-seed map used by the stopping
-// criteria, and the midpoint ODE on the upwind flow, one thread per tip.
+// criteria, and the midpoint ODE on the upwind flow, one warp per tip.
 //
 // The reference runs its GeodesicODE kernel in chunks of `typical_len` steps
 // and restarts each unfinished geodesic from its last point on the host
-// (agd/Eikonal/HFM_CUDA/_GetGeodesics.py:111-134).  Here a thread runs all of
+// (agd/Eikonal/HFM_CUDA/_GetGeodesics.py:111-134).  Here a warp runs all of
 // its chunks in one launch; a chunk boundary resets the same state the
 // reference's restart resets (stopping-criteria history, cell cache), so the
 // paths are the reference's.  The stepping follows
@@ -88,43 +88,134 @@ struct GeoArgs {
 
 constexpr int kMaxHist = 256;  // bound on 1 + max(eucl_delay, nymin_delay)
 
+// The point data around the current cell, in shared memory, one per warp: the
+// values, flow weight sums, flow planes and distance-to-seed bytes of a W^D
+// box of grid points, with the stopping criteria's history.  A warp traces one
+// geodesic; its 32 lanes fill the box together (asynchronous 4-byte copies for
+// the floats, batched loads for the bytes), and then all of them step the same
+// ODE on the same data, so that the control flow stays warp-uniform and the
+// steps read shared memory instead of waiting on global loads.  The box is
+// refilled, centred on the current cell, when a cell leaves it: after at least
+// W/2 - 1 points of travel.
+template <int D>
+struct GeoWindow {
+    static constexpr int W = D == 2 ? 32 : 12;
+    static constexpr int WT = D == 2 ? W * W : W * W * W;
+    static constexpr int NJ = WT / 32;  // points per lane
+    static_assert(WT % 32 == 0, "whole warps of points");
+    float u[WT], wsum[WT], flow[D][WT];
+    uint8_t eucl[WT];
+    int org[D];
+    int tq[D][W], tr[D][W];  // per axis: tile and in-tile coordinate of org + t, tq -1 outside the grid
+    long long nymin_p[kMaxHist];
+    uint8_t eucl_p[kMaxHist];
+};
+
+__device__ __forceinline__ void cp_async4(void *smem, const void *gmem) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+
 template <int D>
 struct Walker {
+    using Win = GeoWindow<D>;
     static constexpr int NC = 1 << D;
-    const GeoArgs &A;
+    static constexpr int W = Win::W;
+    const GeoArgs A;  // a copy: the fields stay in registers
+    Win &S;
+    const int lane;
     int xq[D];
-    long long nymin;     // bilevel index of the retained corner
-    long long nymin_grid;
+    long long nymin;  // grid index of the retained corner (the reference keeps its
+                      // bilevel index: the same point, so the same equality tests)
+    int eucl_min;     // distance-to-seed byte at that corner
     float thr;
     float flow_c[NC][D], dist_c[NC], wsum_c[NC];
 
-    __device__ Walker(const GeoArgs &a) : A(a) { reset(); }
-    __device__ void reset() {
+    __device__ __forceinline__ Walker(const GeoArgs &a, Win &s, int ln) : A(a), S(s), lane(ln) { reset(); }
+    __device__ __forceinline__ void reset() {
         for (int k = 0; k < D; ++k) xq[k] = kIntMax;
-        nymin = kIntMax;
-        nymin_grid = kIntMax;
+        nymin = -1;
+        eucl_min = 255;
         thr = 0.f;
     }
-    __device__ bool inside(const int *y) const {
+    __device__ __forceinline__ bool inside(const int *y) const {
         for (int k = 0; k < D; ++k)
             if (y[k] < 0 || y[k] >= A.shape[k]) return false;
         return true;
     }
-    __device__ long long bilevel(const int *y) const {
-        long long n_o = 0, n_i = 0;
-        for (int k = 0; k < D; ++k) {
-            n_o = n_o * A.shape_o[k] + y[k] / A.shape_i[k];
-            n_i = n_i * A.shape_i[k] + y[k] % A.shape_i[k];
-        }
-        return n_o * A.size_i + n_i;
-    }
-    __device__ long long gridindex(const int *y) const {
+    __device__ __forceinline__ long long gridindex(const int *y) const {
         long long n = 0;
         for (int k = 0; k < D; ++k) n = n * A.shape[k] + y[k];
         return n;
     }
+    // Position in the box of a grid point that it holds.  When the cell
+    // xq..xq+1 passes covers(), a corner that is inside the grid has box
+    // coordinates in [0, W) on every axis.
+    __device__ __forceinline__ int local(const int *y) const {
+        int li = 0;
+        for (int k = 0; k < D; ++k) li = li * W + (y[k] - S.org[k]);
+        return li;
+    }
+    __device__ __forceinline__ bool covers() const {
+        bool ok = true;
+        for (int k = 0; k < D; ++k) ok = ok && xq[k] >= S.org[k] && xq[k] < S.org[k] + (W - 1);
+        return ok;
+    }
+    // Refill the box around the cell at xq (all lanes, warp-uniform).
+    __device__ __forceinline__ void fill() {
+        __syncwarp();  // every lane has finished reading the previous box
+        int org[D];
+        for (int k = 0; k < D; ++k) org[k] = xq[k] - (W / 2 - 1);
+        if (lane < W) {
+            for (int k = 0; k < D; ++k) {
+                const int y = org[k] + lane;
+                const bool in = y >= 0 && y < A.shape[k];
+                S.tq[k][lane] = in ? y / A.shape_i[k] : -1;
+                S.tr[k][lane] = in ? y % A.shape_i[k] : 0;
+            }
+        }
+        if (lane == 0)
+            for (int k = 0; k < D; ++k) S.org[k] = org[k];
+        __syncwarp();
+        constexpr int G = 16;  // byte loads in flight per lane
+#pragma unroll 1
+        for (int j0 = 0; j0 < Win::NJ; j0 += G) {
+            int e[G];
+#pragma unroll
+            for (int jj = 0; jj < G; ++jj) {
+                e[jj] = 255;
+                const int j = j0 + jj;
+                if (j >= Win::NJ) continue;
+                const int p = j * 32 + lane;
+                int t[D], r = p;
+                for (int k = D - 1; k >= 0; --k) { t[k] = r % W; r /= W; }
+                bool in = true;
+                long long n_o = 0, g = 0;
+                int n_i = 0;
+                for (int k = 0; k < D; ++k) {
+                    const int q = S.tq[k][t[k]];
+                    in = in && q >= 0;
+                    n_o = n_o * A.shape_o[k] + q;
+                    n_i = n_i * A.shape_i[k] + S.tr[k][t[k]];
+                    g = g * A.shape[k] + (org[k] + t[k]);
+                }
+                if (!in) continue;
+                const long long n = n_o * A.size_i + n_i;
+                cp_async4(&S.u[p], A.u + n);
+                cp_async4(&S.wsum[p], A.fwsum + n);
+                for (int k = 0; k < D; ++k) cp_async4(&S.flow[k][p], A.fvec + k * A.size_tot + n);
+                e[jj] = __ldg(A.eucl + g);
+            }
+#pragma unroll
+            for (int jj = 0; jj < G; ++jj)
+                if (j0 + jj < Win::NJ) S.eucl[(j0 + jj) * 32 + lane] = (uint8_t)e[jj];
+        }
+        cp_async_wait_all();
+        __syncwarp();
+    }
     // Kernel_GeodesicODE.h:164-260 (NormalizedFlow)
-    __device__ int normalized_flow(const float *x, float *flow) {
+    __device__ __forceinline__ int normalized_flow(const float *x, float *flow) {
         bool newcell = false;
         for (int k = 0; k < D; ++k) {
             const int q = (int)floorf(x[k]);
@@ -139,6 +230,7 @@ struct Walker {
             wts[i] = w;
         }
         if (newcell) {
+            if (!covers()) fill();
             for (int i = 0; i < NC; ++i) {
                 int y[D];
                 for (int k = 0; k < D; ++k) y[k] = xq[k] + ((i >> k) & 1);
@@ -146,24 +238,23 @@ struct Walker {
                     dist_c[i] = finf();
                     continue;
                 }
-                const long long n = bilevel(y);
-                dist_c[i] = __ldg(A.u + n);
-                wsum_c[i] = __ldg(A.fwsum + n);
-                for (int k = 0; k < D; ++k) flow_c[i][k] = __ldg(A.fvec + k * A.size_tot + n);
+                const int li = local(y);
+                dist_c[i] = S.u[li];
+                wsum_c[i] = S.wsum[li];
+                for (int k = 0; k < D; ++k) flow_c[i][k] = S.flow[k][li];
             }
-            float dmin = finf();
+            float dmin = finf(), ws = 0.f;
             int imin = 0;
             const float wthr = 0.5f / NC;
             for (int i = 0; i < NC; ++i) {
                 if (wts[i] < wthr) continue;
-                if (dist_c[i] < dmin) { imin = i; dmin = dist_c[i]; }
+                if (dist_c[i] < dmin) { imin = i; dmin = dist_c[i]; ws = wsum_c[i]; }
             }
             if (dmin == finf()) return kInWall;
             int y[D];
             for (int k = 0; k < D; ++k) y[k] = xq[k] + ((imin >> k) & 1);
-            nymin = bilevel(y);
-            nymin_grid = gridindex(y);
-            const float ws = wsum_c[imin];
+            nymin = gridindex(y);
+            eucl_min = S.eucl[local(y)];
             if (ws == 0.f) return kAtSeed;
             thr = dmin + A.causality / ws;
         }
@@ -176,60 +267,79 @@ struct Walker {
         for (int k = 0; k < D; ++k) n2 += flow[k] * flow[k];
         const float nrm = sqrtf(n2);
         if (!(nrm > 0.f)) return kVanishingFlow;
-        const float l = (float)(1.0 / (double)nrm);
+        // The correctly rounded float reciprocal: the reference divides in
+        // double and rounds to float, which gives the same value (a double
+        // quotient has more than 2 x 24 + 2 bits, so the second rounding is
+        // innocuous).
+        const float l = __frcp_rn(nrm);
         for (int k = 0; k < D; ++k) flow[k] *= l;
         return kContinue;
     }
 };
 
+// One warp per tip.
 template <int D>
-__global__ void geodesic_kernel(GeoArgs A) {
-    const int tid = blockIdx.x * blockDim.x + threadIdx.x;
-    if (tid >= A.ntips) return;
-    float *out = A.paths + (long long)tid * A.cap * D;
+__global__ void __launch_bounds__(32) geodesic_kernel(GeoArgs A) {
+    __shared__ GeoWindow<D> S;
+    const int tip = blockIdx.x;
+    const int lane = threadIdx.x;
+    if (tip >= A.ntips) return;
+    float *out = A.paths + (long long)tip * A.cap * D;
     float x[D];
-    for (int k = 0; k < D; ++k) {
-        x[k] = A.tips[tid * D + k];
-        out[k] = x[k];
-    }
+    for (int k = 0; k < D; ++k) x[k] = A.tips[tip * D + k];
+    if (lane == 0)
+        for (int k = 0; k < D; ++k) out[k] = x[k];
+    if (lane < D) S.org[lane] = kIntMax / 2;  // an empty box: the first cell fills it
+    __syncwarp();
     int pos = 1, stop = kContinue;
     const int hlen = 1 + max(A.eucl_delay, A.nymin_delay);
-    uint8_t eucl_p[kMaxHist];
-    long long nymin_p[kMaxHist];
-    Walker<D> W(A);
+    Walker<D> Wk(A, S, lane);
     for (int chunk = 0; chunk < A.max_chunks; ++chunk) {
         // a chunk starts afresh from the last point, as the reference's restart does
-        for (int l = 0; l < hlen; ++l) {
-            eucl_p[l] = 255;
-            nymin_p[l] = kIntMax;
+        for (int l = lane; l < hlen; l += 32) {
+            S.eucl_p[l] = 255;
+            S.nymin_p[l] = -1;
         }
-        W.reset();
+        __syncwarp();
+        Wk.reset();
+        int l = 1 % hlen;  // len % hlen
         int len;
         for (len = 1; len < A.typical_len; ++len) {
-            const int l = len % hlen;
             float xp[D], xm[D], flow[D];
             for (int k = 0; k < D; ++k) xp[k] = x[k];
-            stop = W.normalized_flow(x, flow);
+            stop = Wk.normalized_flow(x, flow);
             if (stop != kContinue) break;
-            nymin_p[l] = W.nymin;
-            eucl_p[l] = __ldg(A.eucl + W.nymin_grid);
-            if (W.nymin == nymin_p[(l - A.nymin_delay + hlen) % hlen]) { stop = kStationnary; break; }
+            // every lane holds the same values: the history is written alike by
+            // all, once every lane has read the previous step's entries
+            __syncwarp();
+            S.nymin_p[l] = Wk.nymin;
+            S.eucl_p[l] = (uint8_t)Wk.eucl_min;
+            __syncwarp();
+            int ln = l - A.nymin_delay, le = l - A.eucl_delay;
+            if (ln < 0) ln += hlen;
+            if (le < 0) le += hlen;
+            if (Wk.nymin == S.nymin_p[ln]) { stop = kStationnary; break; }
             // The reference's subscript is a boolean expression (cuda/Kernel_GeodesicODE.h:331).
-            const int cmp = (((l - A.eucl_delay + hlen) % hlen) != 0) && (len >= 0);
-            if (eucl_p[l] > eucl_p[cmp]) { stop = kPastSeed; break; }
+            const int cmp = le != 0;
+            if (S.eucl_p[l] > S.eucl_p[cmp]) { stop = kPastSeed; break; }
             for (int k = 0; k < D; ++k) xm[k] = (0.5f * A.step) * flow[k] + xp[k];
-            stop = W.normalized_flow(xm, flow);
+            stop = Wk.normalized_flow(xm, flow);
             if (stop != kContinue) break;
             for (int k = 0; k < D; ++k) x[k] = A.step * flow[k] + xp[k];
             if (pos < A.cap) {
-                for (int k = 0; k < D; ++k) out[pos * D + k] = x[k];
+                if (lane == 0)
+                    for (int k = 0; k < D; ++k) out[pos * D + k] = x[k];
                 ++pos;
             }
+            l = l + 1 == hlen ? 0 : l + 1;
         }
         if (stop != kContinue) break;
+        __syncwarp();  // the history is reset only once every lane has read it
     }
-    A.lengths[tid] = pos;
-    A.stops[tid] = (int8_t)stop;
+    if (lane == 0) {
+        A.lengths[tip] = pos;
+        A.stops[tip] = (int8_t)stop;
+    }
 }
 
 static inline unsigned nblocks(long long n, int bs) { return (unsigned)((n + bs - 1) / bs); }
@@ -316,9 +426,9 @@ int agd_geodesics(const agd_instance *inst, const float *flow_vector, const floa
     A.cap = cap;
     A.lengths = lengths;
     A.stops = stops;
-    const int bs = 32;  // geodesics are few and sequential: small blocks spread them over SMs
-    if (A.nd == 2) geodesic_kernel<2><<<nblocks(ntips, bs), bs, 0, (cudaStream_t)stream>>>(A);
-    else geodesic_kernel<3><<<nblocks(ntips, bs), bs, 0, (cudaStream_t)stream>>>(A);
+    // one warp per geodesic, one geodesic per block: the tips spread over the SMs
+    if (A.nd == 2) geodesic_kernel<2><<<(unsigned)ntips, 32, 0, (cudaStream_t)stream>>>(A);
+    else geodesic_kernel<3><<<(unsigned)ntips, 32, 0, (cudaStream_t)stream>>>(A);
     const cudaError_t err = cudaGetLastError();
     return err == cudaSuccess ? AGD_STATUS_OK : set_cuda_error("geodesics", err);
 }
