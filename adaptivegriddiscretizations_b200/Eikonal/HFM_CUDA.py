@@ -948,6 +948,9 @@ class Interface:
         typical_len = int(max(40, 0.5 * np.max(self.shape) / step))
         typical_len = int(self.GetValue("geodesic_typical_length", default=min(max_len, typical_len),
                                         help="Typical expected length of geodesics (number of points)."))
+        pastseed_delay = int(self.GetValue("pastseed_delay", default=0,
+                                           help="Number of geodesic backtracking steps before checking "
+                                                "the PastSeed criterion (use if seed and tip are close)"))
         causality = float(self.GetValue("geodesic_causalityTolerance", default=4.0,
                                         help="Used in criterion for rejecting points in flow interpolation"))
         eucl_bound = float(self.GetValue("geodesic_targetTolerance", default=6,
@@ -975,14 +978,15 @@ class Interface:
         _lib.check(L.agd_geodesics(ctypes.byref(inst), _lib.ptr(self.flow_vector), _lib.ptr(self.flow_weightsum),
                                    _lib.ptr(eucl), _lib.ptr(tips_c), ntips, ctypes.c_float(step),
                                    ctypes.c_float(causality), typical_len, max_chunks, eucl_delay, nymin_delay,
-                                   _lib.ptr(paths), cap, _lib.ptr(lengths), _lib.ptr(stops), self.stream),
+                                   pastseed_delay, _lib.ptr(paths), cap, _lib.ptr(lengths), _lib.ptr(stops), self.stream),
                    "geodesics")
         lens = lengths.cpu().numpy()
         codes = stops.cpu().numpy()
-        geos = []
-        for i in range(ntips):
-            g = paths[i, : int(lens[i])] * hh + start
-            geos.append(g.T.contiguous())
+        # all paths to physical coordinates at once; each geodesic is a (ndim, len)
+        # view, transposed like the reference's PointFromIndex(geo).T
+        maxlen = int(lens.max()) if ntips else 0
+        phys = paths[:, :maxlen] * hh + start
+        geos = [phys[i, : int(lens[i])].T for i in range(ntips)]
         crit = []
         for i in range(ntips):
             if codes[i] == 0:

@@ -86,8 +86,8 @@ SIGNATURES = {
     "agd_voronoi_decomposition": (_I, [_I, _P, ctypes.c_longlong, _P, _P, _I, _P]),
     "agd_flow": (_I, [_P, _P, _P, _P, _P, _P]),
     "agd_eucl_map": (_I, [_I, _P, _P, _I, _I, _P, _P, _P]),
-    "agd_geodesics": (_I, [_P, _P, _P, _P, _P, _I, ctypes.c_float, ctypes.c_float, _I, _I, _I, _I, _P, _I, _P,
-                           _P, _P]),
+    "agd_geodesics": (_I, [_P, _P, _P, _P, _P, _I, ctypes.c_float, ctypes.c_float, _I, _I, _I, _I, _I, _P, _I,
+                           _P, _P, _P]),
     "agd_reverse_workspace_bytes": (ctypes.c_size_t, [_P]),
     "agd_reverse": (_I, [_P, _P, _P, _P, _P, _P, ctypes.c_float, ctypes.c_float, _P, ctypes.c_size_t, _P, _P,
                          _P]),
@@ -123,7 +123,7 @@ def lib():
                 fn = getattr(L, name)
                 fn.restype = res
                 fn.argtypes = args
-            if L.agd_version() != 3:
+            if L.agd_version() != 4:
                 raise RuntimeError("libagd_b200.so has an unexpected ABI version")
             _lib = L
     return _lib

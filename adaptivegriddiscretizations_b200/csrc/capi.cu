@@ -24,5 +24,5 @@ int set_cuda_error(const char *what, cudaError_t err) {
 
 extern "C" {
 const char *agd_last_error(void) { return agd::g_msg; }
-int agd_version(void) { return 3; }
+int agd_version(void) { return 4; }
 }

@@ -11,6 +11,7 @@
 // GeodesicODE_Opt.h:236-245, in float.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <vector>
 
 #include "agd_common.cuh"
@@ -27,33 +28,66 @@ struct EGeo {
 // One min-plus pass: out(x) = min over the 3^d neighbours y of min(255, in(y) + k(y - x)),
 // k = round(5 |y - x|) (inf_convolution with distance_kernel(1, ndim, uint8, mult=5)),
 // or with l1, k = |y - x|_1 (distance_kernel(1, ndim, uint8, ord=1)).
-__global__ void infconv_kernel(EGeo g, const uint8_t *in, int l1, uint8_t *out) {
-    const long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-    if (p >= g.n) return;
-    int x[3] = {0, 0, 0};
-    long long r = p;
-    for (int k = g.nd - 1; k >= 0; --k) { x[k] = (int)(r % g.shape[k]); r /= g.shape[k]; }
-    const int nk = g.nd == 2 ? 9 : 27;
-    int best = 255;
-    for (int ic = 0; ic < nk; ++ic) {
-        int y[3] = {0, 0, 0}, q = ic, n2 = 0;
-        bool ok = true;
-        for (int k = g.nd - 1; k >= 0; --k) {
-            const int o = q % 3 - 1;
-            q /= 3;
-            y[k] = x[k] + o;
-            n2 += o * o;
-            ok = ok && y[k] >= 0 && y[k] < g.shape[k];
+// FROM_MASK: `in` is the mask, read as 0 at its points and 255 elsewhere (the
+// first pass); CUT: values above `cut` become 255 (the last pass).
+// Threads run along the last axis, blocks stride over the rows of the others.
+template <int D, bool FROM_MASK, bool CUT>
+__global__ void __launch_bounds__(256) infconv_kernel(EGeo g, const uint8_t *__restrict__ in, int l1, int cut,
+                                                      uint8_t *__restrict__ out) {
+    constexpr int NK = D == 2 ? 9 : 27;
+    const int nlast = g.shape[D - 1];
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= nlast) return;
+    const long long nrows = g.n / nlast;
+    long long stride[D];
+    stride[D - 1] = 1;
+    for (int k = D - 2; k >= 0; --k) stride[k] = stride[k + 1] * g.shape[k + 1];
+    for (long long r = blockIdx.y * (long long)blockDim.y + threadIdx.y; r < nrows;
+         r += (long long)gridDim.y * blockDim.y) {
+        int x[D];
+        x[D - 1] = c;
+        if (D == 3) {
+            x[0] = (int)(r / g.shape[1]);
+            x[1] = (int)(r - (long long)x[0] * g.shape[1]);
+        } else {
+            x[0] = (int)r;
         }
-        if (!ok) continue;
-        long long m = 0;
-        for (int k = 0; k < g.nd; ++k) m = m * g.shape[k] + y[k];
-        // offsets in {-1, 0, 1}^d: |o|_1 = |o|^2; round(5 |o|) = 0, 5, 7, 9
-        const int kv = l1 ? n2 : (n2 == 0 ? 0 : (n2 == 1 ? 5 : (n2 == 2 ? 7 : 9)));
-        const int a = in[m];
-        best = min(best, (a >= 255 - kv) ? 255 : a + kv);
+        const long long p = r * nlast + c;
+        int best = 255;
+#pragma unroll
+        for (int ic = 0; ic < NK; ++ic) {
+            int n2 = 0;
+            bool ok = true;
+            long long m = p;
+#pragma unroll
+            for (int k = 0, q = ic; k < D; ++k, q /= 3) {
+                const int o = q % 3 - 1;
+                n2 += o * o;
+                const int y = x[k] + o;
+                ok = ok && y >= 0 && y < g.shape[k];
+                m += o * stride[k];
+            }
+            if (!ok) continue;
+            // offsets in {-1, 0, 1}^d: |o|_1 = |o|^2; round(5 |o|) = 0, 5, 7, 9
+            const int kv = l1 ? n2 : (n2 == 0 ? 0 : (n2 == 1 ? 5 : (n2 == 2 ? 7 : 9)));
+            const int a = FROM_MASK ? (in[m] ? 0 : 255) : in[m];
+            best = min(best, (a >= 255 - kv) ? 255 : a + kv);
+        }
+        if (CUT && best > cut) best = 255;
+        out[p] = (uint8_t)best;
     }
-    out[p] = (uint8_t)best;
+}
+
+template <int D>
+static void infconv_pass(const EGeo &g, const uint8_t *in, bool from_mask, bool cut_it, int l1, int cut,
+                         uint8_t *out, cudaStream_t st) {
+    const dim3 block(32, 8);
+    const long long nrows = g.n / g.shape[D - 1];
+    const dim3 grid((unsigned)((g.shape[D - 1] + 31) / 32), (unsigned)std::min<long long>((nrows + 7) / 8, 16384));
+    if (from_mask && cut_it) infconv_kernel<D, true, true><<<grid, block, 0, st>>>(g, in, l1, cut, out);
+    else if (from_mask) infconv_kernel<D, true, false><<<grid, block, 0, st>>>(g, in, l1, cut, out);
+    else if (cut_it) infconv_kernel<D, false, true><<<grid, block, 0, st>>>(g, in, l1, cut, out);
+    else infconv_kernel<D, false, false><<<grid, block, 0, st>>>(g, in, l1, cut, out);
 }
 
 __global__ void eucl_init_kernel(EGeo g, const uint8_t *mask, uint8_t *out) {
@@ -79,7 +113,7 @@ struct GeoArgs {
     const float *tips;
     int ntips;
     float step, causality;
-    int typical_len, max_chunks, eucl_delay, nymin_delay;
+    int typical_len, max_chunks, eucl_delay, nymin_delay, pastseed_delay;
     float *paths;
     int cap;
     int *lengths;
@@ -302,6 +336,9 @@ __global__ void __launch_bounds__(32) geodesic_kernel(GeoArgs A) {
         }
         __syncwarp();
         Wk.reset();
+        // the PastSeed test waits pastseed_delay steps in the first chunk only
+        // (_GetGeodesics.py:107-109,133)
+        const int ps_delay = chunk == 0 ? A.pastseed_delay : 0;
         int l = 1 % hlen;  // len % hlen
         int len;
         for (len = 1; len < A.typical_len; ++len) {
@@ -320,7 +357,7 @@ __global__ void __launch_bounds__(32) geodesic_kernel(GeoArgs A) {
             if (le < 0) le += hlen;
             if (Wk.nymin == S.nymin_p[ln]) { stop = kStationnary; break; }
             // The reference's subscript is a boolean expression (cuda/Kernel_GeodesicODE.h:331).
-            const int cmp = le != 0;
+            const int cmp = (le != 0) && (len >= ps_delay);
             if (S.eucl_p[l] > S.eucl_p[cmp]) { stop = kPastSeed; break; }
             for (int k = 0; k < D; ++k) xm[k] = (0.5f * A.step) * flow[k] + xp[k];
             stop = Wk.normalized_flow(xm, flow);
@@ -346,6 +383,8 @@ static inline unsigned nblocks(long long n, int bs) { return (unsigned)((n + bs 
 
 // Min-plus distance map in grid layout: 0 at the mask points, 255 elsewhere,
 // then `npasses` passes of infconv_kernel and values above `cut` set to 255.
+// The first pass reads the mask and the last one applies the cut; the passes
+// alternate between `out` and `tmp` so that the last one writes `out`.
 // tmp: scratch of prod(shape) bytes.
 int distance_map(int ndim, const int *shape, const uint8_t *mask, int npasses, int cut, bool l1, uint8_t *out,
                  uint8_t *tmp, cudaStream_t st) {
@@ -361,14 +400,18 @@ int distance_map(int ndim, const int *shape, const uint8_t *mask, int npasses, i
         g.n *= shape[k];
     }
     const int bs = 256;
-    uint8_t *a = out, *b = tmp;
-    eucl_init_kernel<<<nblocks(g.n, bs), bs, 0, st>>>(g, mask, a);
-    for (int it = 0; it < npasses; ++it) {
-        infconv_kernel<<<nblocks(g.n, bs), bs, 0, st>>>(g, a, l1 ? 1 : 0, b);
-        uint8_t *t = a; a = b; b = t;
+    if (npasses == 0) {
+        eucl_init_kernel<<<nblocks(g.n, bs), bs, 0, st>>>(g, mask, tmp);
+        eucl_cut_kernel<<<nblocks(g.n, bs), bs, 0, st>>>(g, tmp, cut, out);
+    } else {
+        const uint8_t *src = mask;
+        for (int it = 0; it < npasses; ++it) {
+            uint8_t *dst = ((npasses - 1 - it) % 2 == 0) ? out : tmp;
+            if (ndim == 2) infconv_pass<2>(g, src, it == 0, it == npasses - 1, l1 ? 1 : 0, cut, dst, st);
+            else infconv_pass<3>(g, src, it == 0, it == npasses - 1, l1 ? 1 : 0, cut, dst, st);
+            src = dst;
+        }
     }
-    eucl_cut_kernel<<<nblocks(g.n, bs), bs, 0, st>>>(g, a, cut, b);
-    if (b != out) cudaMemcpyAsync(out, b, (size_t)g.n, cudaMemcpyDeviceToDevice, st);
     const cudaError_t err = cudaGetLastError();
     return err == cudaSuccess ? AGD_STATUS_OK : set_cuda_error("distance map", err);
 }
@@ -387,11 +430,11 @@ int agd_eucl_map(int ndim, const int *shape, const uint8_t *seed_mask, int npass
 
 int agd_geodesics(const agd_instance *inst, const float *flow_vector, const float *flow_weightsum, const uint8_t *eucl,
                   const float *tips, int ntips, float step, float causality, int typical_len, int max_chunks,
-                  int eucl_delay, int nymin_delay, float *paths, int cap, int32_t *lengths, int8_t *stops,
-                  agd_stream_t stream) {
+                  int eucl_delay, int nymin_delay, int pastseed_delay, float *paths, int cap, int32_t *lengths,
+                  int8_t *stops, agd_stream_t stream) {
     clear_error();
     if (!inst || (inst->ndim != 2 && inst->ndim != 3) || ntips < 0 || !flow_vector || !flow_weightsum || !eucl ||
-        !inst->values || typical_len < 2 || max_chunks < 1 || eucl_delay < 0 || nymin_delay < 0 ||
+        !inst->values || typical_len < 2 || max_chunks < 1 || eucl_delay < 0 || nymin_delay < 0 || pastseed_delay < 0 ||
         1 + (eucl_delay > nymin_delay ? eucl_delay : nymin_delay) > kMaxHist || cap < 1 ||
         (ntips > 0 && (!tips || !paths || !lengths || !stops)))
         return set_error(AGD_STATUS_INVALID, "agd_geodesics: bad arguments");
@@ -422,6 +465,7 @@ int agd_geodesics(const agd_instance *inst, const float *flow_vector, const floa
     A.max_chunks = max_chunks;
     A.eucl_delay = eucl_delay;
     A.nymin_delay = nymin_delay;
+    A.pastseed_delay = pastseed_delay;
     A.paths = paths;
     A.cap = cap;
     A.lengths = lengths;

@@ -294,18 +294,20 @@ int agd_flow(const agd_instance *inst, float *flow_vector, float *flow_weightsum
 int agd_eucl_map(int ndim, const int *shape, const uint8_t *seed_mask, int npasses, int cut,
                  uint8_t *eucl, uint8_t *tmp, agd_stream_t stream);
 
-/* Geodesic backtracking, one thread per tip, with the reference's chunking
+/* Geodesic backtracking, one warp per tip, with the reference's chunking
  * (chunks of `typical_len` points restarting the stopping-criteria history,
  * at most `max_chunks` chunks), midpoint rule, causality filtered multilinear
  * flow and stop codes (0 Continue, 1 AtSeed, 2 InWall, 3 Stationnary,
- * 4 PastSeed, 5 VanishingFlow).  Replaces GetGeodesics + GeodesicODE
- * (_GetGeodesics.py:9-147, cuda/Kernel_GeodesicODE.h:265-412).
+ * 4 PastSeed, 5 VanishingFlow).  The PastSeed test starts after
+ * `pastseed_delay` steps in the first chunk, at once in the later ones.
+ * Replaces GetGeodesics + GeodesicODE (_GetGeodesics.py:9-147,
+ * cuda/Kernel_GeodesicODE.h:265-412).
  * tips: (ntips, ndim) continuous grid indices.  paths: (ntips, cap, ndim),
  * with cap >= max_chunks*(typical_len-1)+1; lengths, stops: ntips entries. */
 int agd_geodesics(const agd_instance *inst, const float *flow_vector, const float *flow_weightsum,
                   const uint8_t *eucl, const float *tips, int ntips, float step, float causality,
-                  int typical_len, int max_chunks, int eucl_delay, int nymin_delay, float *paths,
-                  int cap, int32_t *lengths, int8_t *stops, agd_stream_t stream);
+                  int typical_len, int max_chunks, int eucl_delay, int nymin_delay, int pastseed_delay,
+                  float *paths, int cap, int32_t *lengths, int8_t *stops, agd_stream_t stream);
 
 /* ---------------------------------------------------------------- adjoint -- */
 
@@ -337,7 +339,7 @@ int agd_forward(const agd_instance *inst, const float *flow_weights, const int32
 /* ------------------------------------------------------------------- misc -- */
 
 const char *agd_last_error(void);
-int agd_version(void); /* 3: agd_instance with the factorisation, second order and wall fields */
+int agd_version(void); /* 4: agd_geodesics with pastseed_delay */
 
 #if defined(__GNUC__)
 #pragma GCC visibility pop

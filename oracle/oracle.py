@@ -339,8 +339,10 @@ def eikonal(pr, dtype=np.float32, values=None, nthreads=1, flow=False, nitermax=
     return out
 
 
-def geodesics(pr, values, flow_vector, flow_weightsum, tips, step=0.25, causality=4.0):
-    """Backtrack from physical tips; returns (list of (ndim, len) physical paths, stop codes)."""
+def geodesics(pr, values, flow_vector, flow_weightsum, tips, step=0.25, causality=4.0, pastseed_delay=0):
+    """Backtrack from physical tips; returns (list of (ndim, len) physical paths, stop codes).
+    The PastSeed test waits pastseed_delay steps in the first chunk only
+    (_GetGeodesics.py:107-109,133)."""
     L = lib()
     nd = pr.ndim
     shp = (ctypes.c_int * nd)(*pr.shape)
@@ -366,7 +368,7 @@ def geodesics(pr, values, flow_vector, flow_weightsum, tips, step=0.25, causalit
         x_s[:, 0] = np.stack([geos[i][-1][-1] for i in corresp])
         len_s = np.zeros(n, np.int32)
         stop_s = np.zeros(n, np.int8)
-        L.agdo_geodesic_chunk(nd, shp, n, typical, 0, ctypes.c_float(causality), ctypes.c_float(step), eucl_delay,
+        L.agdo_geodesic_chunk(nd, shp, n, typical, pastseed_delay if it == 1 else 0, ctypes.c_float(causality), ctypes.c_float(step), eucl_delay,
                               nymin_delay, _p(u), _p(fv), _p(fws), _p(eucl), _p(x_s), _p(len_s), _p(stop_s))
         nxt = []
         for i, x, l, s in zip(corresp, x_s, len_s, stop_s):
@@ -435,7 +437,8 @@ def run(case, dtype=np.float32, nthreads=1):
         out["flow_vector"], out["flow_weightsum"] = r["flow_vector"], r["flow_weightsum"]
     if "tips" in case:
         out["geodesics"], out["geodesic_stopping_criteria"] = geodesics(
-            pr, r["values"], r["flow_vector"], r["flow_weightsum"], case["tips"])
+            pr, r["values"], r["flow_vector"], r["flow_weightsum"], case["tips"],
+            pastseed_delay=int(case.get("pastseed_delay", 0)))
     norm = flow_normalization(pr, case, r["flow_vector"]) if need_flow and pr.rander else None
     if "costVariation" in case:
         rhs = forward_rhs(pr, case["costVariation"], case.get("seedValueVariation"))

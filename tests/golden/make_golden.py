@@ -322,7 +322,7 @@ class RefPipeline:
         arr[arr > 5 * 6] = 255
         return arr
 
-    def geodesics(self, tips):
+    def geodesics(self, tips, pastseed_delay=0):
         nd = self.ndim
         L = lib(f"libagdref_geo{nd}_{self.shape_i[0]}.so")
         eucl = self.infconv_eucl()
@@ -336,7 +336,7 @@ class RefPipeline:
         corresp = list(range(len(tips_c)))
         codes = ["Continue", "AtSeed", "InWall", "Stationnary", "PastSeed", "VanishingFlow"]
         geoIt, geoMaxIt = 0, int(np.ceil(max_len / typical_len))
-        pastseed = 0
+        pastseed = pastseed_delay  # first chunk only (_GetGeodesics.py:107-109,133)
         while corresp:
             if geoIt >= geoMaxIt:
                 break
@@ -576,6 +576,13 @@ def make_cases():
         c = {k: v for k, v in cases[key].items() if k != "sensitivity"}
         c["order"] = 2
         cases[key + "_order2"] = c
+    # tips a few pixels from the seeds, with the PastSeed test delayed by 20 steps:
+    # the first four stop as PastSeed within a few steps without the delay
+    c = {k: v for k, v in cases["riem2"].items() if k != "sensitivity"}
+    c["pastseed_delay"] = 20
+    c["tips"] = np.array([[0.1958, 0.2319], [0.6943, 0.9547], [0.6748, 0.8182], [0.4959, 0.5293],
+                          [0.25, 0.3], [0.7, 0.95]], np.float32)
+    cases["riem2_pastseed"] = c
     # walls (obstacles), with a gap, a one-pixel diagonal wall (leaky for diagonal
     # offsets, as the reference's visibility test is) and a tip inside a wall
     c = {k: v for k, v in cases["riem2"].items() if k != "sensitivity"}
@@ -735,7 +742,7 @@ def run_case(name, case):
         # exportActiveNeighs: positive flow weights as bits (cuda/Update.h:187,206)
         out["activeNeighs"] = sum((pipe.bsq(w) > 0).astype(np.int32) << k for k, w in enumerate(pipe.fw))
         if "tips" in case:
-            geos, stops, eucl = pipe.geodesics(case["tips"])
+            geos, stops, eucl = pipe.geodesics(case["tips"], int(case.get("pastseed_delay", 0)))
             out["geodesic_lengths"] = np.array([g.shape[1] for g in geos], np.int32)
             out["geodesics_concat"] = np.concatenate(geos, axis=1).astype(np.float32)
             out["geodesic_stopping_criteria"] = np.array(stops)

@@ -10,7 +10,7 @@ import torch
 from conftest import CASES, ORDER2_CASES, load_case, make_dictin
 
 pytestmark = pytest.mark.gpu
-GEO_CASES = [c for c in CASES if c != "ad_notebook"] + ["riem2_factor"]
+GEO_CASES = [c for c in CASES if c != "ad_notebook"] + ["riem2_factor", "riem2_pastseed"]
 
 
 def _split(ref):

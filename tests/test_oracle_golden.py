@@ -45,8 +45,8 @@ def test_values(name, dtype):
 
 
 @pytest.mark.parametrize("name", [c for c in CASES if c != "ad_notebook"] + ["riem2_factor"] + ORDER2_CASES +
-                         ["riem2_walls", "riem3_walls", "iso2_walls", "diag2", "diag3", "diag2_walls", "diag2_order2"] +
-                         RANDER_CASES)
+                         ["riem2_walls", "riem3_walls", "iso2_walls", "diag2", "diag3", "diag2_walls", "diag2_order2",
+                          "riem2_pastseed"] + RANDER_CASES)
 def test_geodesics(name):
     case, ref = load_case(name)
     r = O.run(case, np.float32)
@@ -54,6 +54,15 @@ def test_geodesics(name):
     for p, g in zip(r["geodesics"], _geodesic_split(ref)):
         assert p.shape == g.shape
         assert np.abs(p - g).max() < 1e-4 * np.abs(g).max()
+
+
+def test_geodesics_pastseed_delay_matters():
+    """Without the delay, four of the six geodesics of the case stop as PastSeed
+    within a few steps of their tips; with it (the fixture), all reach a seed."""
+    case, ref = load_case("riem2_pastseed")
+    r = O.run(dict(case, pastseed_delay=0), np.float32)
+    assert r["geodesic_stopping_criteria"][:4] == ["PastSeed"] * 4
+    assert all(str(s) == "AtSeed" for s in ref["geodesic_stopping_criteria"])
 
 
 @pytest.mark.parametrize("name", ["iso2", "riem2", "iso3", "riem3", "ad_notebook", "diag2", "diag3", "rand2", "rand3"])
