@@ -206,14 +206,14 @@ def run_other_path(args):
     torch.cuda.set_device(0)
     rng = np.random.default_rng(5)
     if args.path == "geodesic":
-        n = 1024
+        n = args.path_size or 1024
         metrics, seeds = make_fields(n, 1, 21, sigma=16.0)
         tips = rng.uniform(0.02, 0.98, (64, 2)).astype(np.float32)
         d = dict(model="Riemann2", dims=np.array([n, n], np.float32), gridScales=np.full(2, 1.0 / n, np.float32),
                  origin=np.zeros(2, np.float32), metric=metrics[0], seeds=seeds[0], tips=tips, verbosity=0)
         workload = f"Riemann2 {n}x{n}, geodesics from 64 tips (flow already computed)"
     else:
-        n = 200
+        n = args.path_size or 200
         q = gaussian_filter(rng.standard_normal((4, n, n, n)).astype(np.float32), (0, 6, 6, 6), mode="wrap")
         q /= np.linalg.norm(q, axis=0, keepdims=True)
         w, x, y, z = q
@@ -291,6 +291,8 @@ def main():
     ap.add_argument("--tile", type=int, default=8, help="tile side (8: the default, or 16)")
     ap.add_argument("--path", default="solve", choices=["solve", "geodesic", "reverse"],
                     help="solve: the benchmark (default); geodesic / reverse: the other kernels of the path")
+    ap.add_argument("--path-size", type=int, default=0,
+                    help="grid side for --path (0: 1024 for geodesic, 200 for reverse; smaller for profiler captures)")
     ap.add_argument("--warm-oracle", type=float, default=0.0,
                     help="experiment: warm start every solve from (1+eps) x its cold solution, all tiles active")
     args = ap.parse_args()
