@@ -884,6 +884,9 @@ struct EikonalVisitor {
     // Resident 4-warp CTAs per SM the register budget must allow: 256-point tiles
     // keep 8 points per lane in registers, Riemann3 twelve neighbours per point,
     // multiprecision an integer part beside every value.
+    // The one-round-trip-per-32-entries publication loop: batching it costs
+    // registers, which spill in the variants at their budget.
+    static constexpr bool kBulkPublish = false;
     static constexpr int kMinCtas =
         (VMASK & ((1ull << V_RIEM2_16) | (1ull << V_ISO2_16) | (1ull << V_ISO2_16_MP) | (1ull << V_ISO2_16_F) |
                   (1ull << V_ISO2_16_O2) | (1ull << V_RIEM2_16_W) | (1ull << V_DIAG2_16) |

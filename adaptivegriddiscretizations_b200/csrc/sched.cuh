@@ -315,14 +315,44 @@ __device__ __forceinline__ bool put_slot(const Sched &S, unsigned ticket, int ep
 }
 
 // Appends the n tile ids src[0..n), to be visited at epoch e, to the global queue;
-// warp-cooperative.
+// warp-cooperative.  BULK: each lane handles kPubBatch entries at a time, their
+// list reads and slot checks issued together (one L2 round trip for 32 x
+// kPubBatch entries instead of one per 32), at the cost of the registers that
+// hold them; a slot still holding its previous lap's entry is waited for by
+// put_slot.
+constexpr int kPubBatch = 8;
+template <bool BULK>
 static __device__ void enqueue_warp(const Sched &S, const int *src, int n, int e, int lane) {
     unsigned start = 0;
     if (lane == 0) start = atomicAdd(&S.ctrl->tail, (unsigned)n);
     start = __shfl_sync(kFull, start, 0);
     fence_acq_rel();  // release: the instance state and the tiles' values before the entries
-    for (int k = lane; k < n; k += 32)
-        if (!put_slot(S, start + (unsigned)k, e, (unsigned)__ldcg(src + k))) break;
+    if constexpr (BULK) {
+        bool ok = true;
+        for (int k0 = 0; k0 < n && ok; k0 += 32 * kPubBatch) {
+            int tile[kPubBatch];
+            unsigned long long prev[kPubBatch];
+#pragma unroll
+            for (int u = 0; u < kPubBatch; ++u) {
+                const int k = k0 + 32 * u + lane;
+                if (k < n) {
+                    tile[u] = __ldcg(src + k);
+                    prev[u] = ld_relaxed_u64(S.queue + (start + (unsigned)k) % S.qcap);
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < kPubBatch; ++u) {
+                const int k = k0 + 32 * u + lane;
+                if (k >= n || !ok) continue;
+                const unsigned ticket = start + (unsigned)k;
+                if (prev[u] == kSlotEmpty) st_relaxed_u64(S.queue + ticket % S.qcap, slot_word(ticket, e, (unsigned)tile[u]));
+                else ok = put_slot(S, ticket, e, (unsigned)tile[u]);
+            }
+        }
+    } else {
+        for (int k = lane; k < n; k += 32)
+            if (!put_slot(S, start + (unsigned)k, e, (unsigned)__ldcg(src + k))) break;
+    }
     __syncwarp();
 }
 
@@ -330,6 +360,7 @@ static __device__ void enqueue_warp(const Sched &S, const int *src, int n, int e
 // tile): publish the next list, or retire the instance.  The stop test is the
 // reference's: no tile left to update, or nitermax_o epochs run
 // (_solvers.py:94-120 with _StopCriterion.py:62-84, _solvers.py:53-57).
+template <bool BULK>
 static __device__ void close_epoch(const Sched &S, int ii, int e, int lane) {
     const Inst &I = S.inst[ii];
     InstState &st = S.ist[ii];
@@ -365,7 +396,7 @@ static __device__ void close_epoch(const Sched &S, int ii, int e, int lane) {
     }
     __syncwarp();
     const int *src = (((e + 1) & 1) ? S.list1 : S.list0) + I.tile_base;
-    enqueue_warp(S, src, n, e + 1, lane);
+    enqueue_warp<BULK>(S, src, n, e + 1, lane);
 }
 
 
@@ -405,6 +436,8 @@ __device__ __forceinline__ unsigned long long take_slot(const Sched &S, unsigned
 // Visitor provides: Args (by value), Smem (per warp), and
 //   static void visit(const Sched&, const Args&, int t, int ii, int e, int lane, Smem&).
 // Visitor::kMinCtas: resident 4-warp CTAs per SM that its register budget must allow.
+// Visitor::kBulkPublish: publish epochs with enqueue_warp<true> (more registers
+// in the worker loop, for visitors whose budget has them).
 constexpr int kSmemInst = 1024;  // instances whose tile bases a CTA keeps in shared memory
 
 // Decrement with release semantics (publishes this warp's writes); the warp
@@ -456,7 +489,7 @@ __global__ void __launch_bounds__(WPB * 32, Visitor::kMinCtas * 4 / WPB) sched_w
         lastone = __shfl_sync(kFull, lastone, 0);
         if (lastone) {
             fence_acq_rel();
-            close_epoch(S, ii, e, lane);
+            close_epoch<Visitor::kBulkPublish>(S, ii, e, lane);
         }
     }
 }
