@@ -158,7 +158,9 @@ struct WsLayout {
 
 static size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
 constexpr long long kMaxWarps = 148 * 64;  // resident warps of a launch, upper bound
-constexpr int kPairInstances = 32;  // launches of this many instances take queue tickets in pairs
+// Launches of this many instances take queue tickets in pairs (Riemann2 512^2:
+// -7 % at 32 instances, +3 % at 64, +10 % at 128, +13 % at 256).
+constexpr int kPairInstances = 64;
 
 static bool layout(const agd_instance *a, int n, WsLayout &L, Inst *out, bool stencil_cache = true) {
     long long tiles = 0, stencil_floats = 0;
@@ -466,10 +468,10 @@ __global__ void __launch_bounds__(WPB * 32, Visitor::kMinCtas * 4 / WPB) sched_w
     // taken when a visit starts, so the atomic's latency overlaps the visit.
     // With tgroup 2 a warp takes two consecutive tickets per atomic: the head
     // counter is a single address that every visit of the launch hits, and at
-    // ~250 visits/us (a batch of 128 instances) its atomics are a bound (+10 %
-    // solves/s at batch 128, +13 % at 256).  A warp then visits two tiles of
-    // the queue in turn, which lengthens the tail of a small epoch: one
-    // instance alone solves 11 % slower that way, so small launches take one.
+    // ~250 visits/us (a batch of 128 instances) its atomics are a bound.  A
+    // warp then visits two tiles of the queue in turn, which lengthens the
+    // tail of a small epoch: one instance alone solves 11 % slower that way,
+    // so launches of fewer than kPairInstances instances take one.
     unsigned ticket = 0;
     int spare = 0;  // tickets of the group still ahead of `ticket`
     if (lane == 0) {
