@@ -162,6 +162,7 @@ struct LinearVisitor {
     // reading the rest from global memory).  Without this cache every sweep
     // re-read the rows through L2: 4.3 us a sweep, 70 % of a visit at 200^3.
     static constexpr int K = SIZE == 256 ? 4 : 8;
+    static constexpr int kRowUnroll = K < 6 ? K : 6;  // row entries unrolled in the init (nact <= 6)
     struct Smem {
         float l[SIZE];
         float cw[K][SIZE];
@@ -194,8 +195,26 @@ struct LinearVisitor {
             r0[p] = __ldg(A.rowptr + n_t);
             r1[p] = __ldg(A.rowptr + n_t + 1);
             int c = 0;
+            // Out-of-tile entries are summed once per visit, in row order; the
+            // in-tile ones are cached.  The first kRowUnroll entries of a row are
+            // unrolled so that their loads are issued together: a row walked
+            // one entry at a time costs two dependent L2 round trips per entry.
             if constexpr (FWD) {
-                for (int k = 0; k < A.nact; ++k) {  // upwind neighbours outside the tile: read once per visit
+#pragma unroll
+                for (int k = 0; k < kRowUnroll; ++k) {  // upwind neighbours: nact <= kRowUnroll
+                    if (k >= A.nact) continue;
+                    const float w = __ldg(A.fw + k * I.size_tot + n_t);
+                    const int y = __ldg(A.fidx + k * I.size_tot + n_t);
+                    if (w == 0.f || y < 0 || (long long)y >= I.size_tot) continue;
+                    if ((long long)y / SIZE != n_o) {
+                        a += w * __ldcg(A.lam + y);
+                    } else {  // c <= k < K
+                        sm.cw[c][n_i] = w;
+                        sm.cz[c][n_i] = (unsigned char)(y - (int)base);
+                        ++c;
+                    }
+                }
+                for (int k = kRowUnroll; k < A.nact; ++k) {  // more neighbours than the unrolled part
                     const float w = __ldg(A.fw + k * I.size_tot + n_t);
                     const int y = __ldg(A.fidx + k * I.size_tot + n_t);
                     if (w == 0.f || y < 0 || (long long)y >= I.size_tot) continue;
@@ -210,7 +229,21 @@ struct LinearVisitor {
                     }
                 }
             } else {
-                for (int j = r0[p]; j < r1[p]; ++j) {  // sources outside the tile: read once per visit
+#pragma unroll
+                for (int q = 0; q < kRowUnroll; ++q) {  // sources
+                    const int j = r0[p] + q;
+                    if (j >= r1[p]) continue;
+                    const int z = __ldg(A.src + j);
+                    const float w = __ldg(A.wt + j);
+                    if ((long long)z / SIZE != n_o) {
+                        a += w * __ldcg(A.lam + z);
+                    } else {  // c <= q < K
+                        sm.cw[c][n_i] = w;
+                        sm.cz[c][n_i] = (unsigned char)(z - (int)base);
+                        ++c;
+                    }
+                }
+                for (int j = r0[p] + kRowUnroll; j < r1[p]; ++j) {  // the rest of a long row
                     const int z = __ldg(A.src + j);
                     const float w = __ldg(A.wt + j);
                     if ((long long)z / SIZE != n_o) {
