@@ -879,14 +879,18 @@ constexpr int smem_floats() {
     return m;
 }
 
-template <unsigned long long VMASK>
+template <unsigned long long VMASK, bool BULK = false>
 struct EikonalVisitor {
     // Resident 4-warp CTAs per SM the register budget must allow: 256-point tiles
     // keep 8 points per lane in registers, Riemann3 twelve neighbours per point,
     // multiprecision an integer part beside every value.
-    // The one-round-trip-per-32-entries publication loop: batching it costs
-    // registers, which spill in the variants at their budget.
-    static constexpr bool kBulkPublish = false;
+    // BULK: epochs published in batches (enqueue_warp<true>).  Its registers
+    // make the variants at their budget spill (Riemann2 8x8: 164 -> 504 bytes,
+    // -13 % solves/s at a batch of 128 instances), but an instance of tens of
+    // thousands of tiles per epoch is bound by its publication (Riemann3 200^3:
+    // -13 % solve time, Riemann2 1024^2: -5 %): plans of a few large instances
+    // use these instantiations (run_variants).
+    static constexpr bool kBulkPublish = BULK;
     static constexpr int kMinCtas =
         (VMASK & ((1ull << V_RIEM2_16) | (1ull << V_ISO2_16) | (1ull << V_ISO2_16_MP) | (1ull << V_ISO2_16_F) |
                   (1ull << V_ISO2_16_O2) | (1ull << V_RIEM2_16_W) | (1ull << V_DIAG2_16) |
@@ -1068,6 +1072,17 @@ static int run_variants(int ndim, unsigned long long vmask, const WsLayout &L, v
             return run_sched<EikonalVisitor<R2 | I16 | I8 | R2L | MP2 | W2>>(L, ws, n, {}, stats, cfg, st);
         }
         return run_sched<EikonalVisitor<R3 | I3 | MP3 | W3>>(L, ws, n, {}, stats, cfg, st);
+    }
+    // A plan of a few instances of 8192 tiles or more on average: batched epoch
+    // publication, for the base variants.
+    const bool bulk = n < kPairInstances && (long long)L.total_tiles >= 8192LL * n;
+    if (bulk) {
+        if (vmask == R2) return run_sched<EikonalVisitor<R2, true>>(L, ws, n, {}, stats, cfg, st);
+        if (vmask == R2L) return run_sched<EikonalVisitor<R2L, true>>(L, ws, n, {}, stats, cfg, st);
+        if (vmask == I16) return run_sched<EikonalVisitor<I16, true>>(L, ws, n, {}, stats, cfg, st);
+        if (vmask == I8) return run_sched<EikonalVisitor<I8, true>>(L, ws, n, {}, stats, cfg, st);
+        if (vmask == R3) return run_sched<EikonalVisitor<R3, true>>(L, ws, n, {}, stats, cfg, st);
+        if (vmask == I3) return run_sched<EikonalVisitor<I3, true>>(L, ws, n, {}, stats, cfg, st);
     }
     if (ndim == 2) {
         if (vmask == R2) return run_sched<EikonalVisitor<R2>>(L, ws, n, {}, stats, cfg, st);
