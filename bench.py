@@ -193,7 +193,7 @@ def run_reference(args, rank):
 def run_other_path(args):
     """The other two kernels of the path, timed on their configurations' sizes
     (one GPU, CUDA events): `--path geodesic`, the backtracking ODE from 64 tips
-    on Riemann2 1024^2 (one thread per tip: latency-bound, so the figure is ODE
+    on Riemann2 1024^2 (one warp per tip: latency-bound, so the figure is ODE
     steps/s, with the bytes an ODE step reads: 4 cells x (value, 2 flow planes,
     weight sum) x 4 B); `--path reverse`, the reverse adjoint (transpose and
     linear solve) of the arrival times at 128 receivers on Riemann3 200^3, with
