@@ -170,7 +170,10 @@ struct LinearVisitor {
     };
     static cudaError_t prepare(const Sched &, const WsLayout &, cudaStream_t) { return cudaSuccess; }
     static cudaError_t finalize(const Sched &, const WsLayout &, cudaStream_t) { return cudaSuccess; }
-    static constexpr int kMinCtas = SIZE == 256 ? 4 : 6;
+    // Resident CTAs per SM: the reverse worker fits 64 registers with 20 bytes of
+    // spills (8 CTAs: -3 % time per Riemann3 200^3 call against 6 at 80
+    // registers), the forward one 72 registers (7 CTAs).
+    static constexpr int kMinCtas = SIZE == 256 ? 4 : (FWD ? 7 : 8);
     // A linear solve is usually one large instance: its epochs (~15 k tiles at
     // 200^3) are published in batches; the worker's registers stay within the
     // kMinCtas budget.
