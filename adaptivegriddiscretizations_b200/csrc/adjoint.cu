@@ -59,10 +59,47 @@ __global__ void rev_fill_kernel(RevGeom g, const float *fw, const int *fidx, con
 }
 
 // Rows in increasing source order: the fill order depends on the schedule.
+// A row of up to kSortRegs entries is sorted in registers (an insertion
+// network with fixed indices, strict comparisons as below); longer rows in
+// place in global memory.
+constexpr int kSortRegs = 12;
 __global__ void rev_sort_kernel(RevGeom g, const int *rowptr, int *src, float *wt) {
     const long long y = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (y >= g.size_tot) return;
     const int a = rowptr[y], b = rowptr[y + 1];
+    const int len = b - a;
+    if (len <= 1) return;
+    if (len <= kSortRegs) {
+        int sr[kSortRegs];
+        float wr[kSortRegs];
+#pragma unroll
+        for (int i = 0; i < kSortRegs; ++i)
+            if (i < len) {
+                sr[i] = src[a + i];
+                wr[i] = wt[a + i];
+            }
+#pragma unroll
+        for (int i = 1; i < kSortRegs; ++i) {
+#pragma unroll
+            for (int j = i; j > 0; --j) {
+                if (i < len && sr[j - 1] > sr[j]) {
+                    const int ts = sr[j - 1];
+                    sr[j - 1] = sr[j];
+                    sr[j] = ts;
+                    const float tw = wr[j - 1];
+                    wr[j - 1] = wr[j];
+                    wr[j] = tw;
+                }
+            }
+        }
+#pragma unroll
+        for (int i = 0; i < kSortRegs; ++i)
+            if (i < len) {
+                src[a + i] = sr[i];
+                wt[a + i] = wr[i];
+            }
+        return;
+    }
     for (int i = a + 1; i < b; ++i) {
         const int s = src[i];
         const float w = wt[i];
