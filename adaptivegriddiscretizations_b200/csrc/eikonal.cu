@@ -884,6 +884,9 @@ struct EikonalVisitor {
     // Resident 4-warp CTAs per SM the register budget must allow: 256-point tiles
     // keep 8 points per lane in registers, Riemann3 twelve neighbours per point,
     // multiprecision an integer part beside every value.
+    // Riemann3 / Rander3: 5 CTAs at up to 96 registers (a single 200^3 solve:
+    // 24.1 ms, against 26.1 ms at 6 CTAs and 80 registers with 2.5x the
+    // spills, and 29.6 ms at 7).
     // BULK: epochs published in batches (enqueue_warp<true>).  Its registers
     // make the variants at their budget spill (Riemann2 8x8: 164 -> 504 bytes,
     // -13 % solves/s at a batch of 128 instances), but an instance of tens of
@@ -897,7 +900,7 @@ struct EikonalVisitor {
                   (1ull << V_DIAG2_16_MP) | (1ull << V_DIAG2_16_F) | (1ull << V_DIAG2_16_O2)))      ? 4
         : (VMASK & ((1ull << V_RIEM3_4) | (1ull << V_RIEM3_4_MP) | (1ull << V_RIEM3_4_F) | (1ull << V_RIEM3_4_O2) |
                     (1ull << V_RIEM3_4_W) | (1ull << V_RAND3_4) | (1ull << V_RAND3_4_W) | (1ull << V_RAND3_4_MP) |
-                    (1ull << V_RAND3_4_F) | (1ull << V_RAND3_4_O2)))                             ? 6
+                    (1ull << V_RAND3_4_F) | (1ull << V_RAND3_4_O2)))                             ? 5
         : (VMASK & (kMpVariants | kFactorVariants | kOrder2Variants))                                ? 7
                                                                                                      : 9;
     struct Args {};
