@@ -842,37 +842,11 @@ class Interface:
             self._forward_ad()
         if not self.reverseAD:
             return
-        L = _lib.lib()
         sens = self.GetValue("sensitivity", help="Reverse automatic differentiation")
         sens = _to_tensor(sens)
         if tuple(sens.shape[:-1]) != self.shape:
             raise ValueError(f"Reverse AD rhs shape {tuple(sens.shape)} does not start with {self.shape}")
-        nrhs = sens.shape[-1]
-        inst = self.instance()
-        nbytes = L.agd_reverse_workspace_bytes(ctypes.byref(inst))
-        ws = torch.empty(max(int(nbytes), 1), dtype=torch.uint8, device="cuda")
-        stats = torch.zeros(2, dtype=torch.int64, device="cuda")
-        res = rtol = _FLOAT_RES * 5.0
-        lam_all = []
-        for r in range(nrhs):
-            col = sens[..., r].contiguous()
-            s_t = torch.empty(self.size_tot, dtype=torch.float32, device="cuda")
-            _lib.check(L.agd_block_expand(self.ndim, self.c_shape, self.c_shape_i, 1, _lib.ptr(col), 0,
-                                          ctypes.c_float(0.0), _lib.ptr(s_t), self.stream), "sensitivity")
-            fin = col[torch.isfinite(col)]
-            atol = float(rtol * fin.abs().mean()) if fin.numel() else 0.0
-            lam = torch.empty(self.size_tot, dtype=torch.float32, device="cuda")
-            _lib.check(L.agd_reverse(ctypes.byref(inst), _lib.ptr(self.flow_weights), _lib.ptr(self.flow_indices),
-                                     _lib.ptr(self.flow_weightsum), _lib.ptr(s_t), _lib.ptr(lam),
-                                     ctypes.c_float(atol), ctypes.c_float(res), _lib.ptr(ws), int(nbytes),
-                                     _lib.ptr(stats), None, self.stream), "reverse")
-            st = stats.cpu().numpy()
-            status = int((st[0] >> 32) & 0xffffffff)
-            if status:
-                raise _lib.AgdError(status, "reverse sensitivity solve failed on the device")
-            self.stats["reverseAD"] = {"niter_o": int(st[0] & 0xffffffff), "nupdate_o_total": int(st[1])}
-            lam_all.append(self.squeeze(lam))
-        allS = torch.stack(lam_all, dim=-1)
+        allS = self.reverse_columns(sens)
         pos = tuple(torch.as_tensor(self.seedIndices.T, device="cuda").long())
         seedS = allS[pos].clone()
         allS[pos] = 0
@@ -885,12 +859,56 @@ class Interface:
                                 device="cuda").index_add_(0, owner, seedS)
         self.hfmOut["seedValueSensitivity"] = seedS
 
+    def _linear_columns(self, rhs, reverse):
+        """Solves the transposed (reverse) or plain (forward) linear system of the
+        flow pass's weights for each column of rhs (*shape, n), grid layout;
+        returns the unknowns (*shape, n).  Tolerances: rtol = 5 float32
+        resolutions, atol = rtol * mean |rhs| (_PostProcess.py:155-219)."""
+        L = _lib.lib()
+        inst = self.instance()
+        nbytes = L.agd_reverse_workspace_bytes(ctypes.byref(inst))
+        ws = torch.empty(max(int(nbytes), 1), dtype=torch.uint8, device="cuda")
+        stats = torch.zeros(2, dtype=torch.int64, device="cuda")
+        rtol = _FLOAT_RES * 5.0
+        fn = L.agd_reverse if reverse else L.agd_forward
+        name = "reverse" if reverse else "forward"
+        out = []
+        for r in range(rhs.shape[-1]):
+            col = rhs[..., r].contiguous()
+            r_t = torch.empty(self.size_tot, dtype=torch.float32, device="cuda")
+            _lib.check(L.agd_block_expand(self.ndim, self.c_shape, self.c_shape_i, 1, _lib.ptr(col), 0,
+                                          ctypes.c_float(0.0), _lib.ptr(r_t), self.stream), name + " rhs")
+            fin = col[torch.isfinite(col)]
+            atol = float(rtol * fin.abs().mean()) if fin.numel() else 0.0
+            x = torch.empty(self.size_tot, dtype=torch.float32, device="cuda")
+            _lib.check(fn(ctypes.byref(inst), _lib.ptr(self.flow_weights), _lib.ptr(self.flow_indices),
+                          _lib.ptr(self.flow_weightsum), _lib.ptr(r_t), _lib.ptr(x), ctypes.c_float(atol),
+                          ctypes.c_float(rtol), _lib.ptr(ws), int(nbytes), _lib.ptr(stats), None, self.stream), name)
+            st = stats.cpu().numpy()
+            status = int((st[0] >> 32) & 0xffffffff)
+            if status:
+                raise _lib.AgdError(status, f"{name} linear solve failed on the device")
+            self.stats["reverseAD" if reverse else "forwardAD"] = {"niter_o": int(st[0] & 0xffffffff),
+                                                                   "nupdate_o_total": int(st[1])}
+            out.append(self.squeeze(x))
+        return torch.stack(out, dim=-1)
+
+    def reverse_columns(self, sens):
+        """Adjoint unknowns lam (*shape, n) of the right-hand sides sens (*shape, n):
+        diag lam - W^T lam = sens, from the flow of the last PostProcess (no
+        key is read; seeds are not zeroed)."""
+        return self._linear_columns(sens, reverse=True)
+
+    def forward_columns(self, rhs):
+        """Variations du (*shape, n) of the right-hand sides rhs (*shape, n):
+        diag du - W du = rhs, from the flow of the last PostProcess."""
+        return self._linear_columns(rhs, reverse=False)
+
     def _forward_ad(self):
         """valueVariation (*shape, n): the linearised solve with the right-hand side
         cost * costVariation, and seedValueVariation at the seeds
         (_PostProcess.py:181-191).  The reference returns the values as a dense AD
         array with these coefficients; they are the hfmOut key valueVariation here."""
-        L = _lib.lib()
         cv, sv = self.costVariation, self.seedValueVariation
         n = cv.shape[-1] if cv is not None else sv.shape[0]
         if cv is None:
@@ -904,31 +922,7 @@ class Interface:
             rhs_all[self.walls.bool()] = 0.0
         if self.flow_normalization is not None:  # drift models (_PostProcess.py:185)
             rhs_all = rhs_all * self.flow_normalization[..., None]
-        inst = self.instance()
-        nbytes = L.agd_reverse_workspace_bytes(ctypes.byref(inst))
-        ws = torch.empty(max(int(nbytes), 1), dtype=torch.uint8, device="cuda")
-        stats = torch.zeros(2, dtype=torch.int64, device="cuda")
-        rtol = _FLOAT_RES * 5.0
-        out = []
-        for j in range(n):
-            col = rhs_all[..., j].contiguous()
-            r_t = torch.empty(self.size_tot, dtype=torch.float32, device="cuda")
-            _lib.check(L.agd_block_expand(self.ndim, self.c_shape, self.c_shape_i, 1, _lib.ptr(col), 0,
-                                          ctypes.c_float(0.0), _lib.ptr(r_t), self.stream), "forward rhs")
-            fin = col[torch.isfinite(col)]
-            atol = float(rtol * fin.abs().mean()) if fin.numel() else 0.0
-            du = torch.empty(self.size_tot, dtype=torch.float32, device="cuda")
-            _lib.check(L.agd_forward(ctypes.byref(inst), _lib.ptr(self.flow_weights), _lib.ptr(self.flow_indices),
-                                     _lib.ptr(self.flow_weightsum), _lib.ptr(r_t), _lib.ptr(du),
-                                     ctypes.c_float(atol), ctypes.c_float(rtol), _lib.ptr(ws), int(nbytes),
-                                     _lib.ptr(stats), None, self.stream), "forward")
-            st = stats.cpu().numpy()
-            status = int((st[0] >> 32) & 0xffffffff)
-            if status:
-                raise _lib.AgdError(status, "forward variation solve failed on the device")
-            self.stats["forwardAD"] = {"niter_o": int(st[0] & 0xffffffff), "nupdate_o_total": int(st[1])}
-            out.append(self.squeeze(du))
-        self.hfmOut["valueVariation"] = torch.stack(out, dim=-1)
+        self.hfmOut["valueVariation"] = self.forward_columns(rhs_all)
 
     def GetGeodesics(self):
         """Geodesic backtracking (agd/Eikonal/HFM_CUDA/_GetGeodesics.py:9-147)."""

@@ -2,12 +2,18 @@
 
 `EikonalValues.apply(cost, hfmIn)` returns the values of the eikonal solve of
 hfmIn with its 'cost' replaced by `cost` (a CUDA tensor of the grid shape).
-The backward pass runs the reverse-mode adjoint of libagd_b200 (agd_reverse)
-with the incoming gradient as the 'sensitivity' right-hand side.  The adjoint
-unknown lam satisfies dJ/dcost = lam * cost (the forward linearisation of the
-scheme uses the right-hand side cost * dcost, agd/Eikonal/HFM_CUDA/_PostProcess.py:181-183),
-and the reference reports lam itself as 'costSensitivity'.  Forward mode
-(torch.autograd.forward_ad) runs agd_forward with the tangent as 'costVariation'.
+The forward pass solves once and records the causal dependency of the
+solution: the upwind flow weights and neighbour indices of every point
+(agd_flow), as the reference's SolveAD does before its linear solves
+(agd/Eikonal/HFM_CUDA/_PostProcess.py:155-219).  The backward pass reverse-
+sweeps that record: it runs the adjoint linear solve of libagd_b200
+(agd_reverse) on the saved flow with the incoming gradient as right-hand side,
+without solving the eikonal equation again.  The adjoint unknown lam satisfies
+dJ/dcost = lam * cost (the forward linearisation of the scheme uses the
+right-hand side cost * dcost, _PostProcess.py:181-183), and the reference
+reports lam itself as 'costSensitivity'.  Forward mode
+(torch.autograd.forward_ad) runs agd_forward on the same saved flow with the
+tangent times the cost as right-hand side.
 """
 import torch
 
@@ -20,32 +26,44 @@ class EikonalValues(torch.autograd.Function):
         h = hfmIn.copy()
         h["cost"] = cost.detach()
         h["exportValues"] = True
-        h.store.pop("sensitivity", None)
-        h.store.pop("tips", None)
+        for key in ("sensitivity", "tips", "costVariation", "seedValueVariation"):
+            h.store.pop(key, None)
         itf = Interface(h)
         itf.SetKernelTraits()
         itf.SetGeometry()
         itf.SetArgs()
         itf.Solve()
+        itf.reverseAD = True  # the flow pass records the upwind weights and indices
+        itf.PostProcess()
         values = itf.values.clone()
-        ctx.hfmIn = h
+        ctx.itf = itf
         ctx.save_for_backward(cost)
         return values
 
     @staticmethod
+    def _seed_positions(itf):
+        return tuple(torch.as_tensor(itf.seedIndices.T, device="cuda").long())
+
+    @staticmethod
     def jvp(ctx, dcost, _):
-        h = ctx.hfmIn.copy()
-        h["costVariation"] = dcost.detach().float().contiguous()[..., None]
-        out = h.Run()
-        return out["valueVariation"][..., 0]
+        itf = ctx.itf
+        cost = itf.cost.expand(itf.shape) if itf.cost.dim() == 0 else itf.cost
+        rhs = dcost.detach().float() * cost
+        rhs[EikonalValues._seed_positions(itf)] = 0.0  # seed values do not depend on the cost
+        if getattr(itf, "walls", None) is not None:
+            rhs[itf.walls.bool()] = 0.0
+        if itf.flow_normalization is not None:  # drift models (_PostProcess.py:185)
+            rhs = rhs * itf.flow_normalization
+        return itf.forward_columns(rhs.contiguous()[..., None])[..., 0]
 
     @staticmethod
     def backward(ctx, grad):
         (cost,) = ctx.saved_tensors
-        h = ctx.hfmIn.copy()
-        h["sensitivity"] = grad.detach().float().contiguous()[..., None]
-        out = h.Run()
-        lam = out["costSensitivity"][..., 0]
+        itf = ctx.itf
+        lam = itf.reverse_columns(grad.detach().float().contiguous()[..., None])[..., 0]
+        lam[EikonalValues._seed_positions(itf)] = 0.0
+        if itf.flow_normalization is not None:  # drift models (_PostProcess.py:213-214)
+            lam = lam / itf.flow_normalization
         return lam * cost, None
 
 

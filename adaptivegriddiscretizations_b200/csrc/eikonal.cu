@@ -1119,6 +1119,10 @@ static __device__ __align__(256) unsigned char g_fixed_scratch[kFixedScratchByte
 constexpr int kMaxDevices = 64;
 static void *g_fixed_scratch_addr[kMaxDevices];
 static std::mutex g_fixed_scratch_lock;
+// Host staging of the instance descriptors (about 64 KiB at the maximum count):
+// a file-scope array rather than a stack one, since plugin threads may have
+// small stacks.  Used under g_fixed_scratch_lock until the upload has read it.
+static Inst g_fixed_scratch_insts[kFixedScratchMaxInstances];
 
 static int fixed_scratch_solve(const agd_instance *host, int n, agd_stats *stats, const agd_launch *cfg,
                                cudaStream_t st) {
@@ -1130,19 +1134,16 @@ static int fixed_scratch_solve(const agd_instance *host, int n, agd_stats *stats
     cudaError_t err = cudaGetDevice(&dev);
     if (err != cudaSuccess) return set_cuda_error("cudaGetDevice", err);
     if (dev < 0 || dev >= kMaxDevices) return set_error(AGD_STATUS_UNSUPPORTED, "device ordinal too large");
-    void *scratch = nullptr;
-    {
-        std::lock_guard<std::mutex> guard(g_fixed_scratch_lock);
-        if (!g_fixed_scratch_addr[dev]) {  // first call on this device: resolve the array's device address
-            err = cudaGetSymbolAddress(&g_fixed_scratch_addr[dev], g_fixed_scratch);
-            if (err != cudaSuccess) {
-                g_fixed_scratch_addr[dev] = nullptr;
-                return set_cuda_error("cudaGetSymbolAddress(fixed scratch)", err);
-            }
+    std::lock_guard<std::mutex> guard(g_fixed_scratch_lock);  // held until the descriptors are staged
+    if (!g_fixed_scratch_addr[dev]) {  // first call on this device: resolve the array's device address
+        err = cudaGetSymbolAddress(&g_fixed_scratch_addr[dev], g_fixed_scratch);
+        if (err != cudaSuccess) {
+            g_fixed_scratch_addr[dev] = nullptr;
+            return set_cuda_error("cudaGetSymbolAddress(fixed scratch)", err);
         }
-        scratch = g_fixed_scratch_addr[dev];
     }
-    Inst insts[kFixedScratchMaxInstances];
+    void *scratch = g_fixed_scratch_addr[dev];
+    Inst *insts = g_fixed_scratch_insts;
     WsLayout L;
     if (!layout(host, n, L, insts, /*stencil_cache=*/false)) return set_error(AGD_STATUS_INVALID, "bad instance shape");
     unsigned long long vmask = 0;
@@ -1151,7 +1152,8 @@ static int fixed_scratch_solve(const agd_instance *host, int n, agd_stats *stats
     if (L.total > kFixedScratchBytes)
         return set_error(AGD_STATUS_WORKSPACE, "agd_eikonal_solve_fixed_scratch: these instances need more "
                                                "scratch than AGD_FIXED_SCRATCH_BYTES; use agd_eikonal_solve");
-    // Pageable host source: the call returns once the descriptors are staged.
+    // Pageable host source: the call returns once the descriptors are staged,
+    // after which the host array may be reused.
     err = cudaMemcpyAsync(static_cast<char *>(scratch) + L.inst, insts, sizeof(Inst) * n, cudaMemcpyHostToDevice, st);
     if (err != cudaSuccess) return set_cuda_error("descriptor upload", err);
     return run_variants(host[0].ndim, vmask, L, scratch, n, stats, cfg, st);

@@ -59,6 +59,20 @@ def make_fields(n, batch, seed, sigma=8.0):
     return metrics, seeds
 
 
+def make_iso256(seed, n=256, sigma=8.0):
+    """The Isotropic2 256^2 configuration: g = white noise smoothed by a Gaussian
+    of sigma pixels, renormalised to unit variance, cost = exp(0.5 g), one seed
+    at the grid centre, gridScale 1/n, tolerance 1e-6 (case dictionary with the
+    dictIn keys)."""
+    from scipy.ndimage import gaussian_filter
+    rng = np.random.default_rng(seed)
+    g = gaussian_filter(rng.standard_normal((n, n)), sigma, mode="wrap")
+    g = (g - g.mean()) / g.std()
+    return dict(model="Isotropic2", dims=np.array([n, n], np.float32), gridScales=np.full(2, 1.0 / n, np.float32),
+                origin=np.zeros(2, np.float32), cost=np.exp(0.5 * g).astype(np.float32),
+                seeds=np.array([[0.5, 0.5]], np.float32), tol=1e-6)
+
+
 def dictins(metrics, seeds, n, to_device=True, pinned=False, traits=None):
     """One dictIn per instance; metrics and seeds are numpy arrays or (pinned)
     host tensors, moved to the device first if to_device."""
@@ -133,24 +147,34 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
-def cpu_baseline(n, seconds_budget=25.0):
-    """The oracle (C++ restatement of the scheme), OpenMP over all host cores, on
-    instances of the same workload; returns (solves/s, grid-updates/s, cores, sample)."""
+def cpu_cases(n, count=4, seed=1234):
+    """Oracle inputs of `count` instances of the benchmark's field distribution."""
+    metrics, seeds = make_fields(n, count, seed)
+    return [dict(model="Riemann2", dims=np.array([n, n], np.float32), gridScales=np.full(2, 1.0 / n, np.float32),
+                 origin=np.zeros(2, np.float32), metric=m, seeds=s) for m, s in zip(metrics, seeds)]
+
+
+def cpu_baseline(n, cases, seconds_budget=15.0, min_solves=1):
+    """The oracle (C++ restatement of the scheme), OpenMP over all host cores,
+    solving the prepared cases in turn (inputs made before the clock starts)
+    until `seconds_budget` has passed; returns (solves/s, grid-updates/s, cores,
+    sample, tile visits of each case solved)."""
     from oracle import oracle as O
     cores = os.cpu_count() or 1
-    metrics, seeds = make_fields(n, 4, 1234)
     t0 = time.perf_counter()
-    solves, updates = 0, 0
-    for m, s in zip(metrics, seeds):
-        case = dict(model="Riemann2", dims=np.array([n, n], np.float32), gridScales=np.full(2, 1.0 / n, np.float32),
-                    origin=np.zeros(2, np.float32), metric=m, seeds=s)
-        r = O.run(case, np.float32, nthreads=cores)
+    solves, updates, visits = 0, 0, {}
+    while True:
+        k = solves % len(cases)
+        r = O.run(cases[k], np.float32, nthreads=cores)
         solves += 1
         updates += r["tile_visits"] * 64
-        if time.perf_counter() - t0 > seconds_budget:
+        visits[k] = int(r["tile_visits"])
+        if solves >= min_solves and time.perf_counter() - t0 > seconds_budget:
             break
     dt = time.perf_counter() - t0
-    return solves / dt, updates / dt, cores, f"{solves} Riemann2 {n}^2 solve(s) of the same field distribution, float32"
+    return (solves / dt, updates / dt, cores,
+            f"{solves} Riemann2 {n}^2 solves ({len(cases)} instances of the same field distribution in turn), "
+            f"float32, {dt:.1f} s", visits)
 
 
 def max_over_ranks(x, dist, device="cuda"):
@@ -165,16 +189,19 @@ def max_over_ranks(x, dist, device="cuda"):
 
 
 def run_reference(args, rank):
+    """The reference arm: the CPU scheme on the host cores, one solve per step.
+    The inputs of the step's instances are made before the clock starts."""
     if rank != 0:
         return
     n = args.n
-    vals = []
-    for _ in range(args.warmup):
-        cpu_baseline(n, seconds_budget=1e-9)
+    cases = cpu_cases(n, 4, 1234)
+    from oracle import oracle as O
+    cores = os.cpu_count() or 1
+    for k in range(args.warmup):
+        O.run(cases[k % len(cases)], np.float32, nthreads=cores)
     t0 = time.perf_counter()
-    for _ in range(args.steps):
-        v, gu, cores, sample = cpu_baseline(n, seconds_budget=1e-9)
-        vals.append(v)
+    for k in range(args.steps):
+        O.run(cases[k % len(cases)], np.float32, nthreads=cores)
     dt = time.perf_counter() - t0
     value = args.steps / dt
     print(json.dumps({
@@ -184,8 +211,9 @@ def run_reference(args, rank):
         "config": {"workload": f"Riemann2 {n}x{n}, 1 instance per step on the host cores (oracle port)",
                    "grid": n, "seeds": 4},
         "cpu_baseline": {"value": value, "unit": "solves/s", "cores": cores, "kind": "port",
-                         "sample": "one Riemann2 solve per step; the reference's own CPU path (the external HFM "
-                                   "library) is not available, the oracle is the C++ restatement of its scheme"},
+                         "sample": f"one Riemann2 {n}^2 solve per step, 4 prepared instances in turn (inputs made "
+                                   "before the clock); the reference's own CPU path (the external HFM library) is "
+                                   "not available, the oracle is the C++ restatement of its scheme"},
         "e2e": {"value": value, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }), flush=True)
 
@@ -467,11 +495,28 @@ def main():
                       "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
                       "api": "Eikonal.SubmitBatch of dictIn inputs (two streams)"}
 
-    cpu = None
+    cpu = schedule = None
     if rank == 0 and not args.no_cpu_baseline:
-        v, gu, cores, sample = cpu_baseline(n)
+        cases = cpu_cases(n, 4, 1234)
+        v, gu, cores, sample, ref_visits = cpu_baseline(n, cases, min_solves=len(cases))
         cpu = {"value": v, "unit": "solves/s", "cores": cores, "kind": "port", "sample": sample,
                "grid_updates_per_s": gu}
+        # Useful work: this solver's tile visits against the reference schedule's
+        # (the oracle reproduces _solvers.fast_iterative_method's visit count) on
+        # the same instances.
+        sitfs = [Interface(h) for h in dictins([c["metric"] for c in cases], [c["seeds"] for c in cases], n,
+                                               traits=traits)]
+        for it in sitfs:
+            it.SetKernelTraits()
+            it.SetGeometry()
+            it.SetArgs()
+        splan = BatchPlan(sitfs, launch=launch)
+        splan.run()
+        gv = [int(x) for x in splan.read_stats()[2]]
+        rv = [ref_visits[k] for k in range(len(cases))]
+        schedule = {"instances": len(cases), "gpu_tile_visits": gv, "reference_schedule_tile_visits": rv,
+                    "ratio": float(np.sum(gv) / np.sum(rv))}
+        del splan, sitfs
 
     if rank == 0:
         line = {
@@ -492,7 +537,7 @@ def main():
                          "frac": achieved / hbm, "traffic": traffic, "peak_kind": peak_kind,
                          "kernel": "sched_worker<EikonalVisitor>", "kernel_ms": float(kern.mean() * 1000),
                          "bytes_per_update": BYTES_PER_UPDATE["Riemann2"]},
-            "cpu_baseline": cpu, "e2e": e2e, "e2e_dictin": e2e_dictin, "gpu_launches": 5 * args.steps,
+            "cpu_baseline": cpu, "schedule_vs_reference": schedule, "e2e": e2e, "e2e_dictin": e2e_dictin, "gpu_launches": 5 * args.steps,
             "clocks": clk.summary(),
         }
         print(json.dumps(line), flush=True)

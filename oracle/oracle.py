@@ -159,7 +159,9 @@ def prepare(case):
         pr.geom = np.ascontiguousarray((np.float32(1) / (costs * pr.h.reshape((-1,) + (1,) * pr.ndim))) ** 2,
                                        np.float32)
     res = np.finfo(np.float32).resolution
-    pr.atol = float(np.float32(np.nanmean(cost) * res * 5.0)) if "atol" not in case else float(case["atol"])
+    # atol: the `atol` key, else `tol`, else 5 float32 resolutions of the mean cost (_SetGeometry.py:238-250)
+    pr.atol = float(case["atol"]) if "atol" in case else float(case["tol"]) if "tol" in case else \
+        float(np.float32(np.nanmean(cost) * res * 5.0))
     pr.rtol = float(np.float32(res * 5.0)) if "rtol" not in case else float(case["rtol"])
     seeds = np.asarray(case["seeds"], np.float32).reshape(-1, pr.ndim)
     sv = np.asarray(case.get("seedValues", np.zeros(len(seeds))), np.float32)

@@ -52,7 +52,7 @@ def make_dictin(case, mode="gpu", extra=None):
     from adaptivegriddiscretizations_b200 import Eikonal
     d = {"model": case["model"], "mode": mode, "arrayOrdering": "RowMajor", "verbosity": 0}
     for k in ("dims", "gridScales", "origin", "seeds", "seedValues", "cost", "tips", "traits", "sensitivity",
-              "seedRadius", "factoringRadius", "order", "walls", "wallDistBound", "pastseed_delay"):
+              "seedRadius", "factoringRadius", "order", "walls", "wallDistBound", "pastseed_delay", "tol"):
         if k in case:
             d[k] = case[k]
     if "metric" in case:

@@ -1,7 +1,7 @@
 """Generate the golden fixtures of the GPU eikonal path from the reference itself.
 
 Runs only where the reference source tree is available (``--ref``, default
-/root/reference): it imports the reference's numpy modules (``agd.Metrics``,
+$AGD_REFERENCE, else a checkout named ``reference`` beside the repository): it imports the reference's numpy modules (``agd.Metrics``,
 ``agd.FiniteDifferences``, ``agd.Selling``) for the host-side preparation, and
 drives the reference's own CUDA kernels compiled for the host by
 ``oracle/ref_emul/Makefile`` (libraries in ``oracle/_ref/``).
@@ -16,8 +16,8 @@ The host loops around the kernels restate, in numpy, the reference's driver code
 Output: one ``<case>.npz`` per case in this directory, holding the dictIn inputs
 and the reference outputs.  Usage::
 
-    make -C oracle/ref_emul REF=/root/reference
-    python tests/golden/make_golden.py [--ref /root/reference]
+    make -C oracle/ref_emul REF=<reference checkout>
+    python tests/golden/make_golden.py [--ref <reference checkout>]
 """
 import argparse
 import ctypes
@@ -712,6 +712,21 @@ def make_cases():
     sens.reshape(-1)[rng.choice(int(np.prod(sh)), 5, replace=False)] = 1.0
     c["sensitivity"] = sens
     cases["rand3"] = c
+    # Riemann3 32^3 with the 200^3 workload's metric distribution (eigenvalues
+    # log-uniform in [1, 25], orientations smoothed over 6 voxels in proportion),
+    # one source, reverse sensitivity of 24 receivers: the largest 3D size the
+    # host build of the reference's kernels solves in a few minutes; own stream
+    rng = np.random.default_rng(3232)
+    sh = (32, 32, 32)
+    c = dict(model="Riemann3", **rect(sh, 1.0 / 32))
+    m = riemann3_metric(rng, sh, 6.0 * 32 / 200 * 4, 25.0)
+    c["metric"] = np.moveaxis(np.stack([m[i, j] for i in range(3) for j in range(i + 1)]), 0, -1)
+    c["cost"] = np.exp(0.3 * smooth_noise(rng, sh, 3.0)).astype(np.float32)
+    c["seeds"] = np.array([[0.5, 0.5, 0.5]], np.float32)
+    sens = np.zeros(sh + (1,), np.float32)
+    sens.reshape(-1)[rng.choice(int(np.prod(sh)), 24, replace=False)] = 1.0
+    c["sensitivity"] = sens
+    cases["riem3_32"] = c
     return cases
 
 
@@ -807,7 +822,9 @@ def save(name, case, out):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default="/root/reference")
+    ap.add_argument("--ref", default=os.environ.get("AGD_REFERENCE") or
+                    os.path.join(os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__)))),
+                                 "..", "reference"))
     ap.add_argument("--only", default=None)
     args = ap.parse_args()
     sys.path.insert(0, args.ref)

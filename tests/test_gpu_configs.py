@@ -2,6 +2,10 @@
 that hold at any size (seeded synthetic fields with the configurations'
 shapes and distributions):
 
+  * Isotropic2 256^2 (cost exp(0.5 g), g smoothed white noise of unit
+    variance, sigma 8 px, one seed at the centre, tolerance 1e-6; the
+    Isotropic scheme of cuda/Isotropic_.h:20-41): the parity criteria against
+    the float64 oracle's discrete solution, through dictIn.Run;
   * Riemann2 1024^2 (angle field smoothed over 16 px, lambda in [1, 100], 4
     seeds) with geodesics from 64 tips: the parity criteria against the float64
     oracle's discrete solution, the stop codes of the oracle's geodesics, paths
@@ -10,10 +14,12 @@ shapes and distributions):
     over 6 voxels, 1 source) with the reverse sensitivity of the sum of the
     arrival times at 128 receivers: against central differences (h = 1e-3 of
     the cost) of multiprecision solves at tight tolerances with float64 values,
-    on 8 voxels where the sensitivity is not negligible;
+    on 32 voxels drawn uniformly over the grid and on 8 voxels where the
+    sensitivity is not negligible (4 drawn among them, the 4 largest);
   * 512 Isotropic2 / Riemann2 instances of sides 64 to 512 with 1 to 8 seeds,
     solved in one persistent launch replayed from a CUDA graph: every instance
-    converges, a sample meets the parity criteria against the discrete solution.
+    converges; after the replays, one instance of every side and model meets
+    the parity criteria against the discrete solution.
 """
 import os
 import sys
@@ -37,6 +43,15 @@ def _riemann2(n, seed, nseeds=4, sigma=16.0):
     seeds = np.random.default_rng(seed + 7).uniform(0.05, 0.95, (nseeds, 2)).astype(np.float32)
     return dict(model="Riemann2", dims=np.array([n, n], np.float32), gridScales=np.full(2, 1.0 / n, np.float32),
                 origin=np.zeros(2, np.float32), metric=metrics[0], seeds=seeds)
+
+
+def test_isotropic2_256_config():
+    import bench
+    case = bench.make_iso256(11)
+    out = make_dictin(case, extra={"exportValues": True}).Run()
+    assert out["keys"]["used"].count("tol") == 1
+    v = out["values"].cpu().numpy()
+    assert_near_discrete(v, case, discrete_solution(case, nthreads=os.cpu_count()))
 
 
 def test_riemann2_1024_with_64_tips():
@@ -102,9 +117,12 @@ def test_riemann3_200_reverse_vs_finite_differences():
         u = make_dictin(dict(case, cost=cost), extra=dict(tight, exportValues=True)).Run()["values"]
         return float(u.double().reshape(-1)[flat_recv].sum())
 
-    # voxels where the sensitivity is not negligible: 4 drawn among them, the 4 largest
+    # 32 voxels drawn uniformly over the grid (most have no receiver downstream,
+    # so the difference quotient must vanish there too), and voxels where the
+    # sensitivity is not negligible: 4 drawn among them, the 4 largest
     gmax = np.abs(grad).max()
-    voxels = list(rng.choice(np.flatnonzero(np.abs(grad) > 1e-2 * gmax), 4, replace=False)) + \
+    voxels = list(rng.choice(n ** 3, 32, replace=False)) + \
+        list(rng.choice(np.flatnonzero(np.abs(grad) > 1e-2 * gmax), 4, replace=False)) + \
         list(np.argsort(-np.abs(grad))[:4])
     for idx in voxels:
         h = 1e-3 * case["cost"].reshape(-1)[idx]
@@ -162,8 +180,12 @@ def test_batched_512_mixed_cuda_graph():
     torch.cuda.synchronize()
     niter, status, visits = plan.read_stats()
     assert not status.any() and (niter > 0).all()
-    sample = [i for i in range(512) if int(cases[i]["dims"][0]) <= 128][:12]
-    for i in sample:
+    # one instance of every side and model, after the graph replays
+    sample = {}
+    for i, c in enumerate(cases):
+        sample.setdefault((int(c["dims"][0]), c["model"]), i)
+    assert len(sample) == 10
+    for i in sample.values():
         it = itfs[i]
         v = it.squeeze(it.values_t).cpu().numpy()
         assert_near_discrete(v, cases[i])

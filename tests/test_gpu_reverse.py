@@ -14,7 +14,7 @@ from oracle import oracle as O
 pytestmark = pytest.mark.gpu
 
 
-@pytest.mark.parametrize("name", ["iso2", "riem2", "iso3", "riem3", "ad_notebook"])
+@pytest.mark.parametrize("name", ["iso2", "riem2", "iso3", "riem3", "ad_notebook", "riem3_32"])
 def test_reverse_vs_reference(name):
     case, ref = load_case(name)
     case = {k: v for k, v in case.items() if k != "tips"}
@@ -75,18 +75,27 @@ def test_reverse_vs_finite_differences():
         assert abs(fd - grad.reshape(-1)[idx]) <= 2e-3 * abs(fd) + 1e-6 * abs(base), (idx, fd, grad.reshape(-1)[idx])
 
 
-def test_autograd_function():
+def test_autograd_function(monkeypatch):
+    """The backward pass reverse-sweeps the flow recorded by the forward pass: one
+    eikonal solve in all, and the gradient is the reference's costSensitivity
+    times the cost."""
     from adaptivegriddiscretizations_b200 import Eikonal
+    from adaptivegriddiscretizations_b200.Eikonal.HFM_CUDA import Interface
     from adaptivegriddiscretizations_b200.autograd import eikonal_values
     case = _small_riemann(n=32)
     h = Eikonal.dictIn({k: case[k] for k in ("model", "dims", "gridScales", "origin", "metric", "seeds")}
                        | {"verbosity": 0})
     cost = torch.as_tensor(case["cost"], device="cuda").requires_grad_(True)
+    solves = []
+    solve = Interface.Solve
+    monkeypatch.setattr(Interface, "Solve", lambda self: (solves.append(1), solve(self))[1])
     u = eikonal_values(h, cost)
     w = torch.zeros_like(u)
     w[-1, -1] = 1.0
     w[5, 20] = 2.0
     (u * w).sum().backward()
+    assert len(solves) == 1, "the backward pass solved the eikonal equation again"
+    monkeypatch.setattr(Interface, "Solve", solve)
     g = cost.grad.cpu().numpy()
     out = make_dictin(dict(case, sensitivity=w.cpu().numpy()[..., None])).Run()
     lam = out["costSensitivity"].cpu().numpy()[..., 0]

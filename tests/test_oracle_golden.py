@@ -23,7 +23,7 @@ def _geodesic_split(out):
 
 
 @pytest.mark.parametrize("name", CASES + RADIUS_CASES + FACTOR_CASES + ORDER2_CASES + WALL_CASES + DIAG_CASES +
-                         RANDER_CASES)
+                         RANDER_CASES + ["riem3_32"])
 @pytest.mark.parametrize("dtype", [np.float32, np.float64])
 def test_values(name, dtype):
     case, ref = load_case(name)
@@ -65,7 +65,8 @@ def test_geodesics_pastseed_delay_matters():
     assert all(str(s) == "AtSeed" for s in ref["geodesic_stopping_criteria"])
 
 
-@pytest.mark.parametrize("name", ["iso2", "riem2", "iso3", "riem3", "ad_notebook", "diag2", "diag3", "rand2", "rand3"])
+@pytest.mark.parametrize("name", ["iso2", "riem2", "iso3", "riem3", "ad_notebook", "diag2", "diag3", "rand2", "rand3",
+                                  "riem3_32"])
 def test_reverse_sensitivity(name):
     case, ref = load_case(name)
     r = O.run(case, np.float64)
