@@ -703,6 +703,8 @@ class Interface:
             inst.trigger = self.trigger_t.data_ptr()
         if getattr(self, "wall_dist", None) is not None:
             inst.wall_dist = self.wall_dist.data_ptr()
+        if getattr(self, "release_t", None) is not None:  # tile release epochs (learned schedule)
+            inst.release = self.release_t.data_ptr()
         inst.order2_threshold = getattr(self, "order2_threshold", 0.0)
         if getattr(self, "factor", None) is not None:
             r2, origin, fm = self.factor

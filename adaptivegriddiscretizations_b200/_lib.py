@@ -39,7 +39,7 @@ class AgdInstance(ctypes.Structure):
         ("valuesq_next", ctypes.c_void_p), ("geom", ctypes.c_void_p),
         ("rhs", ctypes.c_void_p), ("seedbits", ctypes.c_void_p), ("trigger", ctypes.c_void_p),
         ("factor_radius2", ctypes.c_float), ("factor_origin", _c_float3), ("factor_metric", ctypes.c_float * 6),
-        ("order2_threshold", ctypes.c_float), ("wall_dist", ctypes.c_void_p),
+        ("order2_threshold", ctypes.c_float), ("wall_dist", ctypes.c_void_p), ("release", ctypes.c_void_p),
     ]
 
 
@@ -60,6 +60,20 @@ class AgdBatchPrep(ctypes.Structure):
         ("rhs", ctypes.c_void_p), ("values", ctypes.c_void_p), ("seedbits", ctypes.c_void_p),
         ("bad_seed", ctypes.c_void_p),
     ]
+
+
+class AgdConvSrc(ctypes.Structure):
+    _fields_ = [("data", ctypes.c_void_p), ("channels", ctypes.c_int), ("up", ctypes.c_int)]
+
+
+class AgdConv(ctypes.Structure):
+    _fields_ = [("n", ctypes.c_int), ("H", ctypes.c_int), ("W", ctypes.c_int), ("src", AgdConvSrc * 2),
+                ("cout", ctypes.c_int)]
+
+
+class AgdWsTerm(ctypes.Structure):
+    _fields_ = [("data", ctypes.c_void_p), ("mode", ctypes.c_int), ("channels", ctypes.c_int),
+                ("offset", ctypes.c_int)]
 
 
 # Every exported symbol, with its ctypes signature.
@@ -93,6 +107,22 @@ SIGNATURES = {
                          _P]),
     "agd_forward": (_I, [_P, _P, _P, _P, _P, _P, ctypes.c_float, ctypes.c_float, _P, ctypes.c_size_t, _P, _P,
                          _P]),
+    # the learned warm start (include/agd_warmstart.h)
+    "agd_conv_kpad": (_I, [_I]),
+    "agd_conv3x3_forward": (_I, [_P, _P, _P, _I, _P, _P, _P, _P]),
+    "agd_conv3x3_weight_grad": (_I, [_P, _P, _P, _P, _P]),
+    "agd_conv_weight_flip": (_I, [_I, _I, _P, _P, _P]),
+    "agd_ws_features": (_I, [_P, _P, _I, _I, _I, _I, ctypes.c_float, _P, _P, _P]),
+    "agd_ws_target": (_I, [_P, _I, _I, _I, _P, _P, _P]),
+    "agd_ws_avgpool": (_I, [_P, _I, _I, _I, _I, _P, _P]),
+    "agd_ws_route": (_I, [_I, _I, _I, _I, _P, AgdWsTerm, AgdWsTerm, _P, _P]),
+    "agd_ws_bias_grad": (_I, [_P, ctypes.c_longlong, _I, _P, _P]),
+    "agd_ws_head_forward": (_I, [_P, ctypes.c_longlong, _P, _P, _P, _P]),
+    "agd_ws_head_loss_backward": (_I, [_P, ctypes.c_longlong, _P, _P, _P, ctypes.c_longlong, _P, _P, _P, _P, _P]),
+    "agd_ws_adam": (_I, [_P, _P, _P, _P, ctypes.c_longlong, ctypes.c_float, ctypes.c_float, ctypes.c_float,
+                         ctypes.c_float, _I, _P, _P]),
+    "agd_ws_release": (_I, [_P, _I, _I, _I, ctypes.c_float, _I, _P, _P]),
+    "agd_ws_warm_values": (_I, [_P, _I, _I, _I, ctypes.c_float, _P, _P]),
     "agd_last_error": (ctypes.c_char_p, []),
     "agd_version": (_I, []),
 }

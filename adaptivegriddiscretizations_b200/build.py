@@ -8,7 +8,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 REPO = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libagd_b200.so")
-SOURCES = ["capi.cu", "eikonal.cu", "geodesic.cu", "adjoint.cu"]
+SOURCES = ["capi.cu", "eikonal.cu", "geodesic.cu", "adjoint.cu", "unet.cu"]
 NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", "-std=c++17",
               "--shared", "-Xcompiler", "-fPIC", "-Xcompiler", "-fvisibility=hidden",
               "-I" + os.path.join(REPO, "include")]
@@ -23,7 +23,8 @@ def nvcc():
 
 def build(verbose=False, extra=()):
     srcs = [os.path.join(CSRC, s) for s in SOURCES]
-    newest = max(os.path.getmtime(p) for p in srcs + [os.path.join(REPO, "include", "agd_b200.h")] +
+    newest = max(os.path.getmtime(p) for p in srcs + [os.path.join(REPO, "include", f) for f in
+                                                      ("agd_b200.h", "agd_warmstart.h")] +
                  [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".cuh", ".h"))])
     if os.path.exists(LIB) and os.path.getmtime(LIB) >= newest and not extra:
         return LIB

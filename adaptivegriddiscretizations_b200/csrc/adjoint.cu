@@ -388,6 +388,7 @@ static bool rev_layout(const agd_instance *a, RevLayout &R, std::vector<Inst> *i
     agd_instance b = *a;
     b.flags |= AGD_FLAG_ACTIVATE_ALL;
     b.trigger = nullptr;
+    b.release = nullptr;  // the linear solves keep the two-list schedule
     if (!layout(&b, 1, R.L, insts, /*stencil_cache=*/false)) return false;
     const Inst &I = (*insts)[0];
     R.size_tot = I.size_tot;

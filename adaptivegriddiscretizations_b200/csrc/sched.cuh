@@ -134,11 +134,16 @@ static int base_variant_of(const agd_instance &a) {
     return -1;
 }
 
+// Epoch lists per instance: two (by epoch parity), or kMaxLists in a plan whose
+// instances have release epochs (a tile pushed before its release epoch waits
+// in the list of that epoch, at most kMaxLists - 1 epochs ahead).
+constexpr int kMaxLists = 32;
+
 // Per-instance epoch state.
 struct InstState {
     int epoch;         // current epoch (1-based)
     int pending;       // tiles of the current epoch not yet finished
-    unsigned cnt[2];   // lengths of the instance's lists, by epoch parity
+    unsigned cnt[kMaxLists];  // lengths of the instance's lists, by epoch modulo the list count
     int done;
     unsigned first;    // ticket of the first entry of epoch 1
 };
@@ -149,10 +154,11 @@ struct Ctrl {
     unsigned err;
 };
 
-// Workspace: [Inst][InstState][tile_inst][list0][list1][flags][score0][score1][queue][Ctrl][stats]
+// Workspace: [Inst][InstState][tile_inst][lists][flags][score0][score1][queue][Ctrl][stats]
 struct WsLayout {
-    size_t inst, istate, tile_inst, list0, list1, flags, score0, score1, queue, ctrl, stats, stencil, total;
+    size_t inst, istate, tile_inst, lists, flags, score0, score1, queue, ctrl, stats, stencil, total;
     int total_tiles;
+    int nlists;  // epoch lists per instance (2, or kMaxLists with release epochs)
     unsigned qcap;
 };
 
@@ -164,7 +170,9 @@ constexpr int kPairInstances = 64;
 
 static bool layout(const agd_instance *a, int n, WsLayout &L, Inst *out, bool stencil_cache = true) {
     long long tiles = 0, stencil_floats = 0;
+    bool gated = false;
     for (int i = 0; i < n; ++i) {
+        gated = gated || a[i].release != nullptr;
         Inst I;
         std::memset(&I, 0, sizeof(I));
         I.a = a[i];
@@ -197,8 +205,8 @@ static bool layout(const agd_instance *a, int n, WsLayout &L, Inst *out, bool st
     L.inst = off; off = align256(off + sizeof(Inst) * n);
     L.istate = off; off = align256(off + sizeof(InstState) * n);
     L.tile_inst = off; off = align256(off + sizeof(int) * tiles);
-    L.list0 = off; off = align256(off + sizeof(int) * tiles);
-    L.list1 = off; off = align256(off + sizeof(int) * tiles);
+    L.nlists = gated ? kMaxLists : 2;
+    L.lists = off; off = align256(off + sizeof(int) * tiles * L.nlists);
     L.flags = off; off = align256(off + sizeof(unsigned) * tiles);
     L.score0 = off; off = align256(off + sizeof(unsigned) * tiles);
     L.score1 = off; off = align256(off + sizeof(unsigned) * tiles);
@@ -232,7 +240,9 @@ struct Sched {
     const Inst *inst;
     InstState *ist;
     const int *tile_inst;
-    int *list0, *list1;
+    int *lists;       // list k of instance i: lists + k * ntiles + tile_base(i)
+    unsigned lmask;   // list count - 1
+    int ntiles;       // tiles of the launch
     unsigned *flags, *score0, *score1;
     unsigned long long *queue;
     unsigned qcap;
@@ -285,13 +295,21 @@ __device__ __forceinline__ void st_relaxed_u64(unsigned long long *p, unsigned l
 }
 __device__ __forceinline__ void fence_acq_rel() { asm volatile("fence.acq_rel.gpu;" ::: "memory"); }
 
-// Tile t is to be visited at epoch e+1 of its instance (pushed during epoch e).
+__device__ __forceinline__ int *list_of(const Sched &S, const Inst &I, int epoch) {
+    return S.lists + (size_t)((unsigned)epoch & S.lmask) * S.ntiles + I.tile_base;
+}
+
+// Tile t is to be visited at epoch e+1 of its instance (pushed during epoch e),
+// or, with release epochs, at its release epoch if that is later (at most
+// lmask epochs ahead).  The epoch a tile is pushed for never decreases, so the
+// epoch-stamped flag keeps one entry per tile and epoch.
 __device__ __forceinline__ void push_tile(const Sched &S, const Inst &I, int ii, int t, int e) {
-    const unsigned tag = (unsigned)(e + 1);
+    int r = e + 1;
+    if (S.lmask > 1u && I.a.release) r = max(r, min((int)__ldg(I.a.release + (t - I.tile_base)), e + (int)S.lmask));
+    const unsigned tag = (unsigned)r;
     if (atomicMax(&S.flags[t], tag) < tag) {
-        int *nxt = ((e + 1) & 1) ? S.list1 : S.list0;
-        const unsigned idx = atomicAdd(&S.ist[ii].cnt[(e + 1) & 1], 1u);
-        nxt[I.tile_base + idx] = t;
+        const unsigned idx = atomicAdd(&S.ist[ii].cnt[tag & S.lmask], 1u);
+        list_of(S, I, r)[idx] = t;
     }
 }
 
@@ -368,9 +386,21 @@ template <bool BULK>
 static __device__ void close_epoch(const Sched &S, int ii, int e, int lane) {
     const Inst &I = S.inst[ii];
     InstState &st = S.ist[ii];
-    int n = 0;
-    if (lane == 0) n = (int)atomicAdd(&st.cnt[(e + 1) & 1], 0u);
-    n = __shfl_sync(kFull, n, 0);
+    // The next epoch that has tiles: e+1, or with release epochs the first of
+    // e+1 .. e+lmask whose list is not empty (the epochs between are empty).
+    int n = 0, en = e + 1;
+    if (S.lmask > 1u) {
+        const unsigned c = lane < (int)S.lmask ? atomicAdd(&st.cnt[(unsigned)(e + 1 + lane) & S.lmask], 0u) : 0u;
+        const unsigned nz = __ballot_sync(kFull, c != 0u);
+        if (nz) {
+            const int k = __ffs(nz) - 1;
+            n = (int)__shfl_sync(kFull, c, k);
+            en = e + 1 + k;
+        }
+    } else {
+        if (lane == 0) n = (int)atomicAdd(&st.cnt[(e + 1) & 1], 0u);
+        n = __shfl_sync(kFull, n, 0);
+    }
     if (n == 0 || e >= I.a.nitermax_o) {
         int last = 0;
         if (lane == 0) {
@@ -393,15 +423,14 @@ static __device__ void close_epoch(const Sched &S, int ii, int e, int lane) {
         return;
     }
     if (lane == 0) {
-        st.cnt[e & 1] = 0u;  // the list of epoch e is consumed; epoch e+1 fills it for epoch e+2
+        st.cnt[(unsigned)e & S.lmask] = 0u;  // the list of epoch e is consumed; it is refilled for a later epoch
         st.pending = n;
-        st.epoch = e + 1;
+        st.epoch = en;
         S.stats[ii].tile_visits += n;  // tile visits = the lengths of the published lists
         __threadfence();
     }
     __syncwarp();
-    const int *src = (((e + 1) & 1) ? S.list1 : S.list0) + I.tile_base;
-    enqueue_warp<BULK>(S, src, n, e + 1, lane);
+    enqueue_warp<BULK>(S, list_of(S, I, en), n, en, lane);
 }
 
 
@@ -567,7 +596,7 @@ static __global__ void setup_tiles(Sched S, int total_tiles) {
     if (active) {
         S.flags[t] = 1u;
         const unsigned idx = atomicAdd(&S.ist[lo].cnt[1], 1u);
-        S.list1[I.tile_base + idx] = t;
+        list_of(S, I, 1)[idx] = t;
     }
 }
 
@@ -604,7 +633,7 @@ static __global__ void publish_first_slots(Sched S, int total_tiles) {
     const int k = j - S.inst[lo].tile_base;
     if (k >= (int)st.cnt[1]) return;
     const unsigned ticket = st.first + (unsigned)k;
-    S.queue[ticket % S.qcap] = slot_word(ticket, 1, (unsigned)S.list1[j]);
+    S.queue[ticket % S.qcap] = slot_word(ticket, 1, (unsigned)list_of(S, S.inst[lo], 1)[k]);
 }
 
 static __global__ void finish_stats(Sched S, agd_stats *out) {
@@ -647,8 +676,9 @@ static Sched sched_at(const WsLayout &L, void *ws, int ninst) {
     S.inst = reinterpret_cast<const Inst *>(w + L.inst);
     S.ist = reinterpret_cast<InstState *>(w + L.istate);
     S.tile_inst = reinterpret_cast<const int *>(w + L.tile_inst);
-    S.list0 = reinterpret_cast<int *>(w + L.list0);
-    S.list1 = reinterpret_cast<int *>(w + L.list1);
+    S.lists = reinterpret_cast<int *>(w + L.lists);
+    S.lmask = (unsigned)L.nlists - 1u;
+    S.ntiles = L.total_tiles;
     S.flags = reinterpret_cast<unsigned *>(w + L.flags);
     S.score0 = reinterpret_cast<unsigned *>(w + L.score0);
     S.score1 = reinterpret_cast<unsigned *>(w + L.score1);

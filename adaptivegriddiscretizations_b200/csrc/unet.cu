@@ -1,0 +1,848 @@
+// unet.cu - the learned warm start: a 4-level convolutional U-Net over NHWC
+// bf16 activations whose 3x3 convolutions (forward, input gradient and weight
+// gradient) are implicit GEMMs on the tcgen05 tensor cores (fp32 accumulators
+// in tensor memory), plus the memory-bound layers around them (features,
+// pooling, gradient routing, the 1x1 head and its loss, bias gradients, Adam)
+// and the two uses of a prediction by the solver: per-tile release epochs and
+// warm-start values.  The reference has no learned component; this file has
+// no counterpart there.  C ABI: include/agd_warmstart.h.
+#include <cuda_bf16.h>
+
+#include <algorithm>
+#include <cstdint>
+
+#include "../../include/agd_warmstart.h"
+#include "agd_internal.h"
+#include "umma.cuh"
+
+namespace agd {
+namespace unet {
+
+using bf16 = __nv_bfloat16;
+constexpr int kBM = 128;           // rows (pixels, or weight rows) per CTA tile
+constexpr int kBK = 64;            // K elements per pipeline stage (8 x 16-byte units)
+constexpr int kStages = 4;
+constexpr int kThreads = 160;      // 4 producer / epilogue warps + 1 MMA warp
+constexpr unsigned long long kWaitNs = 2000000000ull;  // bound on every barrier wait
+
+__host__ __device__ inline int kpad_of(int k) { return (k + kBK - 1) / kBK * kBK; }
+
+struct Src {
+    const bf16 *p;
+    int C;   // channels (multiple of 8)
+    int up;  // 1: the tensor is at half resolution, read nearest-upsampled
+};
+
+struct GemmArgs {
+    int nimg, H, W;  // output (and full-resolution input) shape
+    Src s0, s1;      // input channels [0, s0.C) then [s0.C, s0.C + s1.C)
+    int cin8;        // (s0.C + s1.C) / 8
+    int K8;          // 9 * cin8: 16-byte K units
+    int kchunks;     // ceil(K8 / 8)
+    int N, BN;       // output channels; channels per CTA tile (multiple of 16, <= 256)
+    const bf16 *wmat;  // (N, kpad) bf16, K contiguous
+    int kpad;
+    const float *bias;
+    int relu;
+    bf16 *out_bf;
+    float *out_f;
+    long long M;  // pixels
+    unsigned *err;
+};
+
+__device__ __forceinline__ const bf16 *src_ptr(const Src &s, int nb, int y, int x, int H, int W, int ch) {
+    const int Hs = H >> s.up, Ws = W >> s.up;
+    return s.p + (((long long)nb * Hs + (y >> s.up)) * Ws + (x >> s.up)) * s.C + ch;
+}
+
+__device__ __forceinline__ uint32_t tmem_cols(int bn) {
+    uint32_t c = 32;
+    while (c < (uint32_t)bn) c <<= 1;
+    return c;
+}
+
+// D[m, n] = sum_k A[m, k] B[n, k]: A the implicit im2col of the input (m a
+// pixel, k = tap * cin + ci, tap = 3 (dy + 1) + (dx + 1), zero outside the
+// image), B the weight matrix.  Epilogue: + bias, ReLU, bf16 or fp32 NHWC.
+// Shared memory per stage: A 128 x 64 and B BN x 64 bf16 in the no-swizzle
+// K-major core-matrix layout (16-byte unit u at byte 16 u, u = (row / 8) * 64 +
+// kunit * 8 + row % 8), which makes every producer lane's unit a single cp.async.
+__global__ void __launch_bounds__(kThreads) conv_gemm_kernel(GemmArgs g) {
+    extern __shared__ __align__(1024) unsigned char smem[];
+    __shared__ __align__(8) uint64_t full[kStages], empty[kStages], accf;
+    __shared__ uint32_t s_taddr;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const long long m0 = (long long)blockIdx.x * kBM;
+    const int n0 = blockIdx.y * g.BN;
+    const uint32_t ncols = tmem_cols(g.BN);
+    const uint32_t a_bytes = kBM * kBK * 2, b_bytes = (uint32_t)g.BN * kBK * 2;
+    const uint32_t stage_bytes = a_bytes + b_bytes;
+    const uint32_t sbase = umma::smem_u32(smem);
+
+    if (warp == 4) {
+        umma::tmem_alloc(&s_taddr, ncols);
+        umma::tmem_relinquish();
+    }
+    if (tid == 0) {
+        for (int s = 0; s < kStages; ++s) {
+            umma::mbar_init(&full[s], 128);
+            umma::mbar_init(&empty[s], 1);
+        }
+        umma::mbar_init(&accf, 1);
+        umma::fence_mbar_init();
+    }
+    umma::tc_fence_before_sync();
+    __syncthreads();
+    umma::tc_fence_after_sync();
+    const uint32_t taddr = s_taddr;
+
+    if (warp < 4) {
+        // ---------------------------------------------------------- producer
+        // A: rows 8 * ((tid >> 6) + 2 j) + (tid & 7), j < 8, K unit (tid >> 3) & 7.
+        const int c = (tid >> 3) & 7;
+        int py[8], px[8], pn[8];
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+            const long long m = m0 + 8 * ((tid >> 6) + 2 * j) + (tid & 7);
+            if (m < g.M) {
+                const int hw = g.H * g.W;
+                pn[j] = (int)(m / hw);
+                const int r = (int)(m - (long long)pn[j] * hw);
+                py[j] = r / g.W;
+                px[j] = r - py[j] * g.W;
+            } else {
+                pn[j] = -1;
+                py[j] = px[j] = 0;
+            }
+        }
+        const int nb_units = g.BN * 8;  // B units per stage
+        for (int i = 0; i < g.kchunks; ++i) {
+            const int s = i % kStages;
+            if (i >= kStages && !umma::mbar_wait(&empty[s], ((i / kStages) & 1) ^ 1, g.err, kWaitNs)) break;
+            const uint32_t sa = sbase + s * stage_bytes, sb = sa + a_bytes;
+            const int k8 = i * 8 + c;
+            int tap = 0, ci8 = 0, dy = 0, dx = 0;
+            const bool kin = k8 < g.K8;
+            if (kin) {
+                tap = k8 / g.cin8;
+                ci8 = k8 - tap * g.cin8;
+                dy = tap / 3 - 1;
+                dx = tap - 3 * (tap / 3) - 1;
+            }
+            const bool first = ci8 * 8 < g.s0.C;
+            const Src &S = first ? g.s0 : g.s1;
+            const int ch = first ? ci8 * 8 : ci8 * 8 - g.s0.C;
+#pragma unroll
+            for (int j = 0; j < 8; ++j) {
+                const int u = tid + 128 * j;
+                const int y = py[j] + dy, x = px[j] + dx;
+                const bool ok = kin && pn[j] >= 0 && y >= 0 && y < g.H && x >= 0 && x < g.W;
+                const void *src = ok ? (const void *)src_ptr(S, pn[j], y, x, g.H, g.W, ch) : (const void *)g.wmat;
+                umma::cp_async16(sa + 16u * u, src, ok ? 16u : 0u);
+            }
+            for (int u = tid; u < nb_units; u += 128) {
+                const int n = n0 + ((u >> 6) << 3) + (u & 7);
+                const int kk = i * 8 + ((u >> 3) & 7);
+                const bool ok = n < g.N && kk < g.K8;
+                const void *src = ok ? (const void *)(g.wmat + (long long)n * g.kpad + kk * 8) : (const void *)g.wmat;
+                umma::cp_async16(sb + 16u * u, src, ok ? 16u : 0u);
+            }
+            umma::cp_async_mbar_arrive(&full[s]);
+        }
+        // ---------------------------------------------------------- epilogue
+        const bool ok = umma::mbar_wait(&accf, 0, g.err, kWaitNs);
+        umma::tc_fence_after_sync();
+        if (ok && !*((volatile unsigned *)g.err)) {
+            const long long m = m0 + 32 * warp + lane;
+            for (int c0 = 0; c0 < g.BN; c0 += 16) {
+                uint32_t r[16];
+                umma::tmem_ld16(taddr + ((uint32_t)(32 * warp) << 16) + (uint32_t)c0, r);
+                umma::tmem_ld_wait();
+                const int nc = n0 + c0;
+                if (m >= g.M || nc >= g.N) continue;
+                float v[16];
+#pragma unroll
+                for (int q = 0; q < 16; ++q) {
+                    v[q] = __uint_as_float(r[q]);
+                    if (g.bias) v[q] += __ldg(g.bias + nc + q);
+                    if (g.relu) v[q] = fmaxf(v[q], 0.f);
+                }
+                if (g.out_bf) {
+                    uint4 w[2];
+                    uint32_t *wp = reinterpret_cast<uint32_t *>(w);
+#pragma unroll
+                    for (int q = 0; q < 8; ++q) {
+                        __nv_bfloat162 h = __floats2bfloat162_rn(v[2 * q], v[2 * q + 1]);
+                        wp[q] = *reinterpret_cast<uint32_t *>(&h);
+                    }
+                    uint4 *dst = reinterpret_cast<uint4 *>(g.out_bf + m * g.N + nc);
+                    dst[0] = w[0];
+                    dst[1] = w[1];
+                } else {
+                    float4 *dst = reinterpret_cast<float4 *>(g.out_f + m * g.N + nc);
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) dst[q] = make_float4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
+                }
+            }
+        }
+    } else if (lane == 0) {
+        // ------------------------------------------------------------- MMA
+        const uint32_t idesc = umma::idesc_bf16(kBM, g.BN, 0, 0);
+        for (int i = 0; i < g.kchunks; ++i) {
+            const int s = i % kStages;
+            if (!umma::mbar_wait(&full[s], (i / kStages) & 1, g.err, kWaitNs)) break;
+            umma::fence_proxy_async_smem();
+            umma::tc_fence_after_sync();
+            const uint32_t sa = sbase + s * stage_bytes, sb = sa + a_bytes;
+#pragma unroll
+            for (int kk = 0; kk < kBK / 16; ++kk) {
+                const uint64_t ad = umma::smem_desc(sa + 256u * kk, 128u, 1024u);
+                const uint64_t bd = umma::smem_desc(sb + 256u * kk, 128u, 1024u);
+                umma::mma_bf16(taddr, ad, bd, idesc, (i | kk) != 0);
+            }
+            umma::mma_commit(&empty[s]);
+        }
+        umma::mma_commit(&accf);  // also on a failed wait: completes once the issued MMAs are done
+    }
+    umma::cp_async_wait_all();
+    umma::tc_fence_before_sync();
+    __syncthreads();
+    if (warp == 4) {
+        umma::tc_fence_after_sync();
+        umma::tmem_dealloc(taddr, ncols);
+    }
+}
+
+// Weight gradient: dW[n, r] += sum_p dZ[p, n] X[p + tap(r), ci(r)], r = tap *
+// cin + ci.  GEMM with M = r (128 per CTA), N = n, K = pixels (64 per stage,
+// split over gridDim.z): both operands MN-major (8 consecutive channels of one
+// pixel per 16-byte unit, as they lie in NHWC memory).  Shared layout: unit
+// (group g of 8 rows, pixel k) at byte 16 (g * 64 + k).
+struct WgradArgs {
+    int nimg, H, W;
+    Src s0, s1;
+    int cin8, K8;
+    const bf16 *dz;  // (M, N) bf16
+    int N, BN;
+    float *dw;       // (N, kpad) fp32, accumulated
+    int kpad;
+    long long M;
+    int nchunks, chunks_per_split;
+    unsigned *err;
+};
+
+__global__ void __launch_bounds__(kThreads) conv_wgrad_kernel(WgradArgs g) {
+    extern __shared__ __align__(1024) unsigned char smem[];
+    __shared__ __align__(8) uint64_t full[kStages], empty[kStages], accf;
+    __shared__ uint32_t s_taddr;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int mt = blockIdx.x, n0 = blockIdx.y * g.BN;
+    const int c_begin = blockIdx.z * g.chunks_per_split;
+    const int c_end = min(g.nchunks, c_begin + g.chunks_per_split);
+    const int nk = max(0, c_end - c_begin);
+    const uint32_t ncols = tmem_cols(g.BN);
+    const uint32_t a_bytes = kBM * kBK * 2, b_bytes = (uint32_t)g.BN * kBK * 2;
+    const uint32_t stage_bytes = a_bytes + b_bytes;
+    const uint32_t sbase = umma::smem_u32(smem);
+
+    if (warp == 4) {
+        umma::tmem_alloc(&s_taddr, ncols);
+        umma::tmem_relinquish();
+    }
+    if (tid == 0) {
+        for (int s = 0; s < kStages; ++s) {
+            umma::mbar_init(&full[s], 128);
+            umma::mbar_init(&empty[s], 1);
+        }
+        umma::mbar_init(&accf, 1);
+        umma::fence_mbar_init();
+    }
+    umma::tc_fence_before_sync();
+    __syncthreads();
+    umma::tc_fence_after_sync();
+    const uint32_t taddr = s_taddr;
+
+    if (warp < 4) {
+        const int pk = tid & 63;
+        // the 8 weight-row groups of this thread: g = (tid >> 6) + 2 j
+        int gdy[8], gdx[8], gch[8], gsrc[8];
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+            const int kk8 = mt * 16 + (tid >> 6) + 2 * j;
+            if (kk8 < g.K8) {
+                const int tap = kk8 / g.cin8, ci8 = kk8 - (kk8 / g.cin8) * g.cin8;
+                gdy[j] = tap / 3 - 1;
+                gdx[j] = tap - 3 * (tap / 3) - 1;
+                gsrc[j] = ci8 * 8 < g.s0.C ? 0 : 1;
+                gch[j] = gsrc[j] ? ci8 * 8 - g.s0.C : ci8 * 8;
+            } else {
+                gsrc[j] = -1;
+                gdy[j] = gdx[j] = gch[j] = 0;
+            }
+        }
+        const int nb_units = g.BN * 8;
+        for (int i = 0; i < nk; ++i) {
+            const int s = i % kStages;
+            if (i >= kStages && !umma::mbar_wait(&empty[s], ((i / kStages) & 1) ^ 1, g.err, kWaitNs)) break;
+            const uint32_t sa = sbase + s * stage_bytes, sb = sa + a_bytes;
+            const long long p = (long long)(c_begin + i) * kBK + pk;
+            int nb = -1, y = 0, x = 0;
+            if (p < g.M) {
+                const int hw = g.H * g.W;
+                nb = (int)(p / hw);
+                const int r = (int)(p - (long long)nb * hw);
+                y = r / g.W;
+                x = r - y * g.W;
+            }
+#pragma unroll
+            for (int j = 0; j < 8; ++j) {
+                const int u = tid + 128 * j;
+                const int yy = y + gdy[j], xx = x + gdx[j];
+                const bool ok = nb >= 0 && gsrc[j] >= 0 && yy >= 0 && yy < g.H && xx >= 0 && xx < g.W;
+                const Src &S = gsrc[j] == 1 ? g.s1 : g.s0;
+                const void *src = ok ? (const void *)src_ptr(S, nb, yy, xx, g.H, g.W, gch[j]) : (const void *)g.dz;
+                umma::cp_async16(sa + 16u * u, src, ok ? 16u : 0u);
+            }
+            for (int u = tid; u < nb_units; u += 128) {
+                const int n = n0 + ((u >> 6) << 3);
+                const bool ok = nb >= 0 && n < g.N;
+                const void *src = ok ? (const void *)(g.dz + p * g.N + n) : (const void *)g.dz;
+                umma::cp_async16(sb + 16u * u, src, ok ? 16u : 0u);
+            }
+            umma::cp_async_mbar_arrive(&full[s]);
+        }
+        const bool ok = nk > 0 && umma::mbar_wait(&accf, 0, g.err, kWaitNs);
+        umma::tc_fence_after_sync();
+        if (ok && !*((volatile unsigned *)g.err)) {
+            const int r = mt * kBM + 32 * warp + lane;  // weight row (tap, ci)
+            const bool rin = r < g.K8 * 8;
+            for (int c0 = 0; c0 < g.BN; c0 += 16) {
+                uint32_t v[16];
+                umma::tmem_ld16(taddr + ((uint32_t)(32 * warp) << 16) + (uint32_t)c0, v);
+                umma::tmem_ld_wait();
+                if (!rin) continue;
+#pragma unroll
+                for (int q = 0; q < 16; ++q) {
+                    const int n = n0 + c0 + q;
+                    if (n < g.N) atomicAdd(g.dw + (long long)n * g.kpad + r, __uint_as_float(v[q]));
+                }
+            }
+        }
+    } else if (lane == 0) {
+        const uint32_t idesc = umma::idesc_bf16(kBM, g.BN, 1, 1);
+        for (int i = 0; i < nk; ++i) {
+            const int s = i % kStages;
+            if (!umma::mbar_wait(&full[s], (i / kStages) & 1, g.err, kWaitNs)) break;
+            umma::fence_proxy_async_smem();
+            umma::tc_fence_after_sync();
+            const uint32_t sa = sbase + s * stage_bytes, sb = sa + a_bytes;
+#pragma unroll
+            for (int kk = 0; kk < kBK / 16; ++kk) {
+                const uint64_t ad = umma::smem_desc(sa + 256u * kk, 128u, 1024u);
+                const uint64_t bd = umma::smem_desc(sb + 256u * kk, 128u, 1024u);
+                umma::mma_bf16(taddr, ad, bd, idesc, (i | kk) != 0);
+            }
+            umma::mma_commit(&empty[s]);
+        }
+        umma::mma_commit(&accf);
+    }
+    umma::cp_async_wait_all();
+    umma::tc_fence_before_sync();
+    __syncthreads();
+    if (warp == 4) {
+        umma::tc_fence_after_sync();
+        umma::tmem_dealloc(taddr, ncols);
+    }
+}
+
+// ------------------------------------------------------- memory-bound layers
+// Input features of Riemann2 problems: per output pixel (a 4x4 block of the
+// grid), the block mean of the metric (a = (m00 + m11) / 2, b = (m00 - m11) / 2,
+// c = m10): log(a) / 4, b / a, c / a; the Euclidean distance d from the block
+// centre to the nearest seed (domain units), log(d + 2 h) / 4, 1, 0, 0.
+// dref = d + 2 h, the scale of the predicted arrival time.
+__global__ void features_kernel(const float *metric, const float *seeds, int nseeds, int n, int H, int W, float h,
+                                bf16 *x0, float *dref) {
+    const int Ho = H / 4, Wo = W / 4;
+    const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= (long long)n * Ho * Wo) return;
+    const int b = (int)(idx / (Ho * Wo));
+    const int r = (int)(idx - (long long)b * Ho * Wo);
+    const int oy = r / Wo, ox = r - (r / Wo) * Wo;
+    float s0 = 0.f, s1 = 0.f, s2 = 0.f;
+    for (int dy = 0; dy < 4; ++dy)
+        for (int dx = 0; dx < 4; ++dx) {
+            const float *m = metric + (((long long)b * H + 4 * oy + dy) * W + 4 * ox + dx) * 3;
+            s0 += __ldg(m);
+            s1 += __ldg(m + 1);
+            s2 += __ldg(m + 2);
+        }
+    s0 *= 1.f / 16;
+    s1 *= 1.f / 16;
+    s2 *= 1.f / 16;
+    const float a = 0.5f * (s0 + s2), bb = 0.5f * (s0 - s2);
+    // block centre in domain units: index (4 oy + 1.5) at cell centres (i + 0.5) h
+    const float cy = (4.f * oy + 2.f) * h, cx = (4.f * ox + 2.f) * h;
+    float d2 = 1e30f;
+    for (int k = 0; k < nseeds; ++k) {
+        const float sy = __ldg(seeds + ((long long)b * nseeds + k) * 2), sx = __ldg(seeds + ((long long)b * nseeds + k) * 2 + 1);
+        d2 = fminf(d2, (sy - cy) * (sy - cy) + (sx - cx) * (sx - cx));
+    }
+    const float d = sqrtf(d2);
+    const float f[8] = {0.25f * logf(a), bb / a, s1 / a, d, 0.25f * logf(d + 2.f * h), 1.f, 0.f, 0.f};
+    uint4 w;
+    uint32_t *wp = reinterpret_cast<uint32_t *>(&w);
+    for (int q = 0; q < 4; ++q) {
+        __nv_bfloat162 v = __floats2bfloat162_rn(f[2 * q], f[2 * q + 1]);
+        wp[q] = *reinterpret_cast<uint32_t *>(&v);
+    }
+    reinterpret_cast<uint4 *>(x0)[idx] = w;
+    dref[idx] = d + 2.f * h;
+}
+
+// Training target: log of the 4x4 block mean of the arrival times over dref.
+__global__ void target_kernel(const float *values, int n, int H, int W, const float *dref, float *target) {
+    const int Ho = H / 4, Wo = W / 4;
+    const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= (long long)n * Ho * Wo) return;
+    const int b = (int)(idx / (Ho * Wo));
+    const int r = (int)(idx - (long long)b * Ho * Wo);
+    const int oy = r / Wo, ox = r - (r / Wo) * Wo;
+    float s = 0.f;
+    for (int dy = 0; dy < 4; ++dy)
+        for (int dx = 0; dx < 4; ++dx) s += __ldg(values + ((long long)b * H + 4 * oy + dy) * W + 4 * ox + dx);
+    s *= 1.f / 16;
+    target[idx] = isfinite(s) && s > 0.f ? logf(s / dref[idx]) : __int_as_float(0x7fc00000);
+}
+
+// 2x2 average pooling, NHWC bf16, 8 channels per thread.
+__global__ void avgpool_kernel(const bf16 *x, int n, int H, int W, int C, bf16 *y) {
+    const int Ho = H / 2, Wo = W / 2, C8 = C / 8;
+    const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= (long long)n * Ho * Wo * C8) return;
+    const int c8 = (int)(idx % C8);
+    const long long p = idx / C8;
+    const int b = (int)(p / (Ho * Wo));
+    const int r = (int)(p - (long long)b * Ho * Wo);
+    const int oy = r / Wo, ox = r - (r / Wo) * Wo;
+    float acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    for (int dy = 0; dy < 2; ++dy)
+        for (int dx = 0; dx < 2; ++dx) {
+            const uint4 v = *reinterpret_cast<const uint4 *>(x + (((long long)b * H + 2 * oy + dy) * W + 2 * ox + dx) * C + c8 * 8);
+            const __nv_bfloat162 *h = reinterpret_cast<const __nv_bfloat162 *>(&v);
+            for (int q = 0; q < 4; ++q) {
+                const float2 f = __bfloat1622float2(h[q]);
+                acc[2 * q] += f.x;
+                acc[2 * q + 1] += f.y;
+            }
+        }
+    uint4 w;
+    __nv_bfloat162 *wh = reinterpret_cast<__nv_bfloat162 *>(&w);
+    for (int q = 0; q < 4; ++q) wh[q] = __floats2bfloat162_rn(0.25f * acc[2 * q], 0.25f * acc[2 * q + 1]);
+    *reinterpret_cast<uint4 *>(y + p * C + c8 * 8) = w;
+}
+
+// Backward routing into a layer output Y (n, H, W, C): the gradient of Y is the
+// sum of up to two terms, each read from an fp32 NHWC buffer of Cb channels at
+// channel offset `off`: SAME (same resolution), POOL (the input gradient of a
+// 2x2 average pool of Y: the buffer at half resolution, times 1/4) or UPSUM
+// (the input gradient of a nearest 2x upsampling of Y: the sum of the 2x2
+// buffer pixels at double resolution); times the ReLU mask Y > 0, to bf16.
+struct RouteTerm {
+    const float *p;
+    int mode;  // 0 none, 1 SAME, 2 POOL, 3 UPSUM
+    int Cb, off;
+};
+
+__global__ void route_kernel(int n, int H, int W, int C, const bf16 *y, RouteTerm t0, RouteTerm t1, bf16 *dz) {
+    const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= (long long)n * H * W * C) return;
+    const int c = (int)(idx % C);
+    const long long p = idx / C;
+    const int b = (int)(p / ((long long)H * W));
+    const int r = (int)(p - (long long)b * H * W);
+    const int py = r / W, px = r - (r / W) * W;
+    float g = 0.f;
+    const RouteTerm ts[2] = {t0, t1};
+    for (int k = 0; k < 2; ++k) {
+        const RouteTerm &t = ts[k];
+        if (t.mode == 1) {
+            g += t.p[p * t.Cb + t.off + c];
+        } else if (t.mode == 2) {
+            g += 0.25f * t.p[(((long long)b * (H / 2) + py / 2) * (W / 2) + px / 2) * t.Cb + t.off + c];
+        } else if (t.mode == 3) {
+            for (int dy = 0; dy < 2; ++dy)
+                for (int dx = 0; dx < 2; ++dx)
+                    g += t.p[(((long long)b * (2 * H) + 2 * py + dy) * (2 * W) + 2 * px + dx) * t.Cb + t.off + c];
+        }
+    }
+    if (y && !(__bfloat162float(y[idx]) > 0.f)) g = 0.f;
+    dz[idx] = __float2bfloat16_rn(g);
+}
+
+// Bias gradient: db[c] += sum over pixels of dz[p, c].
+__global__ void bias_grad_kernel(const bf16 *dz, long long M, int C, float *db) {
+    const int c = threadIdx.x % C;
+    const int lanes = blockDim.x / C;
+    const int j = threadIdx.x / C;
+    if (j >= lanes) return;
+    float s = 0.f;
+    for (long long p = (long long)blockIdx.x * lanes + j; p < M; p += (long long)gridDim.x * lanes)
+        s += __bfloat162float(dz[p * C + c]);
+    atomicAdd(db + c, s);
+}
+
+// 1x1 head: r[p] = sum_c y[p, c] w[c] + b (C = 32).
+__global__ void head_forward_kernel(const bf16 *y, long long M, const float *w, const float *b, float *r) {
+    const long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= M) return;
+    float s = b[0];
+    const uint4 *yp = reinterpret_cast<const uint4 *>(y + p * 32);
+    for (int q = 0; q < 4; ++q) {
+        const uint4 v = yp[q];
+        const __nv_bfloat162 *h = reinterpret_cast<const __nv_bfloat162 *>(&v);
+        for (int k = 0; k < 4; ++k) {
+            const float2 f = __bfloat1622float2(h[k]);
+            s += f.x * w[8 * q + 2 * k] + f.y * w[8 * q + 2 * k + 1];
+        }
+    }
+    r[p] = s;
+}
+
+// Mean squared error over the finite targets (count of them: ncount) and its
+// backward through the head: dz[p, c] = dr w[c] (y > 0), dw[c] += dr y[p, c],
+// db += dr, loss += (r - t)^2 / ncount.
+__global__ void head_loss_backward_kernel(const bf16 *y, long long M, const float *w, const float *r,
+                                          const float *target, float inv_count, bf16 *dz, float *dw, float *db,
+                                          float *loss) {
+    __shared__ float s_dw[32], s_db, s_loss;
+    if (threadIdx.x < 32) s_dw[threadIdx.x] = 0.f;
+    if (threadIdx.x == 0) s_db = s_loss = 0.f;
+    __syncthreads();
+    const long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (p < M) {
+        const float t = target[p];
+        const float d = isnan(t) ? 0.f : r[p] - t;
+        const float dr = 2.f * d * inv_count;
+        atomicAdd(&s_loss, d * d * inv_count);
+        atomicAdd(&s_db, dr);
+        const uint4 *yp = reinterpret_cast<const uint4 *>(y + p * 32);
+        uint4 *zp = reinterpret_cast<uint4 *>(dz + p * 32);
+        for (int q = 0; q < 4; ++q) {
+            const uint4 v = yp[q];
+            const __nv_bfloat162 *h = reinterpret_cast<const __nv_bfloat162 *>(&v);
+            uint4 o;
+            __nv_bfloat162 *oh = reinterpret_cast<__nv_bfloat162 *>(&o);
+            for (int k = 0; k < 4; ++k) {
+                const float2 f = __bfloat1622float2(h[k]);
+                const int c = 8 * q + 2 * k;
+                atomicAdd(&s_dw[c], dr * f.x);
+                atomicAdd(&s_dw[c + 1], dr * f.y);
+                oh[k] = __floats2bfloat162_rn(f.x > 0.f ? dr * w[c] : 0.f, f.y > 0.f ? dr * w[c + 1] : 0.f);
+            }
+            zp[q] = o;
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x < 32) atomicAdd(dw + threadIdx.x, s_dw[threadIdx.x]);
+    if (threadIdx.x == 0) {
+        atomicAdd(db, s_db);
+        atomicAdd(loss, s_loss);
+    }
+}
+
+// Adam on fp32 master weights; writes the bf16 copy (if any) and clears the gradient.
+__global__ void adam_kernel(float *w, float *g, float *m, float *v, long long n, float lr, float b1, float b2,
+                            float eps, float bc1, float bc2, bf16 *wb) {
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float gi = g[i];
+    const float mi = b1 * m[i] + (1.f - b1) * gi;
+    const float vi = b2 * v[i] + (1.f - b2) * gi * gi;
+    m[i] = mi;
+    v[i] = vi;
+    const float wi = w[i] - lr * (mi / bc1) / (sqrtf(vi / bc2) + eps);
+    w[i] = wi;
+    g[i] = 0.f;
+    if (wb) wb[i] = __float2bfloat16_rn(wi);
+}
+
+// Weights of the input gradient: wt[ci, tap' * cout + co] = w[co, (8 - tap') * cin + ci].
+__global__ void weight_flip_kernel(const bf16 *w, int cin, int cout, int kpad_in, int kpad_out, bf16 *wt) {
+    const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= (long long)cin * kpad_out) return;
+    const int ci = (int)(idx / kpad_out), k = (int)(idx - (long long)ci * kpad_out);
+    bf16 val = __float2bfloat16_rn(0.f);
+    if (k < 9 * cout) {
+        const int tap = k / cout, co = k - (k / cout) * cout;
+        val = w[(long long)co * kpad_in + (8 - tap) * cin + ci];
+    }
+    wt[idx] = val;
+}
+
+// Release epochs of the tiles of Riemann2 problems from predicted arrival
+// times at block resolution (one value per 4x4 block): per instance, tiles of
+// 8x8 points (2x2 blocks), release = 1 + floor(epochs * tmin / tmax_instance)
+// - lag, at least 1; tmin the tile's smallest prediction.  One CTA per instance.
+__global__ void release_kernel(const float *pred, int Hb, int Wb, int tile_blocks, float epochs, int lag,
+                               uint16_t *release) {
+    const int b = blockIdx.x;
+    const float *P = pred + (long long)b * Hb * Wb;
+    __shared__ float s_max[32];
+    float mx = 0.f;
+    for (int i = threadIdx.x; i < Hb * Wb; i += blockDim.x) {
+        const float v = P[i];
+        if (isfinite(v)) mx = fmaxf(mx, v);
+    }
+    for (int o = 16; o > 0; o >>= 1) mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+    if ((threadIdx.x & 31) == 0) s_max[threadIdx.x >> 5] = mx;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        float v = threadIdx.x < blockDim.x / 32 ? s_max[threadIdx.x] : 0.f;
+        for (int o = 16; o > 0; o >>= 1) v = fmaxf(v, __shfl_xor_sync(0xffffffffu, v, o));
+        if (threadIdx.x == 0) s_max[0] = v;
+    }
+    __syncthreads();
+    const float tmax = s_max[0];
+    const int To = Hb / tile_blocks, Tw = Wb / tile_blocks;
+    for (int t = threadIdx.x; t < To * Tw; t += blockDim.x) {
+        const int ty = t / Tw, tx = t - (t / Tw) * Tw;
+        float mn = 3.4e38f;
+        for (int dy = 0; dy < tile_blocks; ++dy)
+            for (int dx = 0; dx < tile_blocks; ++dx) mn = fminf(mn, P[(ty * tile_blocks + dy) * Wb + tx * tile_blocks + dx]);
+        float e = 1.f;
+        if (tmax > 0.f && isfinite(mn)) e = 1.f + floorf(epochs * fmaxf(mn, 0.f) / tmax) - (float)lag;
+        release[(long long)b * To * Tw + t] = (uint16_t)fminf(fmaxf(e, 1.f), 16000.f);
+    }
+}
+
+// Warm-start values of Riemann2 problems in tile layout (8x8 tiles): (1 +
+// margin) times the bilinear interpolation of the block predictions.
+__global__ void warm_values_kernel(const float *pred, int n, int Hb, int Wb, int H, int W, float margin,
+                                   float *values) {
+    const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long long per = (long long)H * W;
+    if (idx >= per * n) return;
+    const int b = (int)(idx / per);
+    const int r = (int)(idx - (long long)b * per);
+    const int i = r / W, j = r - (r / W) * W;
+    const float *P = pred + (long long)b * Hb * Wb;
+    const float fy = fminf(fmaxf((i + 0.5f) / 4.f - 0.5f, 0.f), (float)(Hb - 1));
+    const float fx = fminf(fmaxf((j + 0.5f) / 4.f - 0.5f, 0.f), (float)(Wb - 1));
+    const int y0 = (int)fy, x0 = (int)fx;
+    const int y1 = min(y0 + 1, Hb - 1), x1 = min(x0 + 1, Wb - 1);
+    const float ay = fy - y0, ax = fx - x0;
+    const float v = (1.f - ay) * ((1.f - ax) * P[y0 * Wb + x0] + ax * P[y0 * Wb + x1]) +
+                    ay * ((1.f - ax) * P[y1 * Wb + x0] + ax * P[y1 * Wb + x1]);
+    const int To = W / 8;
+    const long long t = (long long)(i / 8) * To + j / 8;
+    values[(long long)b * per + t * 64 + (i % 8) * 8 + (j % 8)] = (1.f + margin) * v;
+}
+
+}  // namespace unet
+}  // namespace agd
+
+// ------------------------------------------------------------------ C ABI --
+using namespace agd;
+using namespace agd::unet;
+
+namespace {
+
+cudaStream_t cs(agd_stream_t s) { return reinterpret_cast<cudaStream_t>(s); }
+
+int launched(const char *what) {
+    const cudaError_t e = cudaGetLastError();
+    return e == cudaSuccess ? AGD_STATUS_OK : set_cuda_error(what, e);
+}
+
+// Channels per CTA tile: at most 256, a multiple of 16, tiles of equal width.
+int tile_n(int N, int *ntiles) {
+    *ntiles = (N + 255) / 256;
+    const int per = (N + *ntiles - 1) / *ntiles;
+    return (per + 15) / 16 * 16;
+}
+
+bool check_srcs(const agd_conv *c, Src *s0, Src *s1) {
+    if (!c || c->n <= 0 || c->H <= 0 || c->W <= 0 || !c->src[0].data) return false;
+    for (int k = 0; k < 2; ++k) {
+        const agd_conv_src &s = c->src[k];
+        if (k == 1 && !s.data) continue;
+        if (s.channels <= 0 || s.channels % 8 || (s.up != 0 && s.up != 1)) return false;
+        if (s.up && (c->H % 2 || c->W % 2)) return false;
+        if (reinterpret_cast<uintptr_t>(s.data) % 16) return false;
+    }
+    *s0 = {static_cast<const bf16 *>(c->src[0].data), c->src[0].channels, c->src[0].up};
+    *s1 = c->src[1].data ? Src{static_cast<const bf16 *>(c->src[1].data), c->src[1].channels, c->src[1].up}
+                         : Src{nullptr, 0, 0};
+    return true;
+}
+
+}  // namespace
+
+extern "C" {
+
+int agd_conv_kpad(int cin) { return kpad_of(9 * cin); }
+
+int agd_conv3x3_forward(const agd_conv *c, const void *w, const float *bias, int relu, void *out_bf16,
+                        float *out_f32, unsigned *err, agd_stream_t stream) {
+    GemmArgs g{};
+    if (!check_srcs(c, &g.s0, &g.s1)) return set_error(AGD_STATUS_INVALID, "conv3x3: bad inputs");
+    if (!w || !err || (!out_bf16) == (!out_f32) || c->cout <= 0 || c->cout % 16)
+        return set_error(AGD_STATUS_INVALID, "conv3x3: weights, err, one output and cout % 16 == 0 are required");
+    g.nimg = c->n;
+    g.H = c->H;
+    g.W = c->W;
+    const int cin = g.s0.C + g.s1.C;
+    g.cin8 = cin / 8;
+    g.K8 = 9 * g.cin8;
+    g.kchunks = (g.K8 + 7) / 8;
+    g.N = c->cout;
+    int ntiles = 1;
+    g.BN = tile_n(g.N, &ntiles);
+    g.wmat = static_cast<const bf16 *>(w);
+    g.kpad = kpad_of(9 * cin);
+    g.bias = bias;
+    g.relu = relu;
+    g.out_bf = static_cast<bf16 *>(out_bf16);
+    g.out_f = out_f32;
+    g.M = (long long)c->n * c->H * c->W;
+    g.err = err;
+    const int smem = kStages * (kBM * kBK * 2 + g.BN * kBK * 2);
+    cudaError_t e = cudaFuncSetAttribute(conv_gemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    if (e != cudaSuccess) return set_cuda_error("conv3x3 shared memory", e);
+    const dim3 grid((unsigned)((g.M + kBM - 1) / kBM), (unsigned)ntiles);
+    conv_gemm_kernel<<<grid, kThreads, smem, cs(stream)>>>(g);
+    return launched("conv3x3 forward");
+}
+
+int agd_conv3x3_weight_grad(const agd_conv *c, const void *dz, float *dw, unsigned *err, agd_stream_t stream) {
+    WgradArgs g{};
+    if (!check_srcs(c, &g.s0, &g.s1)) return set_error(AGD_STATUS_INVALID, "conv3x3 weight grad: bad inputs");
+    if (!dz || !dw || !err || c->cout <= 0 || c->cout % 16 || reinterpret_cast<uintptr_t>(dz) % 16)
+        return set_error(AGD_STATUS_INVALID, "conv3x3 weight grad: dz, dw, err and cout % 16 == 0 are required");
+    g.nimg = c->n;
+    g.H = c->H;
+    g.W = c->W;
+    const int cin = g.s0.C + g.s1.C;
+    g.cin8 = cin / 8;
+    g.K8 = 9 * g.cin8;
+    g.dz = static_cast<const bf16 *>(dz);
+    g.N = c->cout;
+    int ntiles = 1;
+    g.BN = tile_n(g.N, &ntiles);
+    g.dw = dw;
+    g.kpad = kpad_of(9 * cin);
+    g.M = (long long)c->n * c->H * c->W;
+    g.err = err;
+    const long long nchunks = (g.M + kBK - 1) / kBK;
+    if (nchunks > 0x7fffffffLL) return set_error(AGD_STATUS_INVALID, "conv3x3 weight grad: too many pixels");
+    g.nchunks = (int)nchunks;
+    const int mtiles = (g.K8 * 8 + kBM - 1) / kBM;
+    int dev = 0, nsm = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    int splits = std::max(1, std::min(g.nchunks, 4 * nsm / std::max(1, mtiles * ntiles)));
+    g.chunks_per_split = (g.nchunks + splits - 1) / splits;
+    splits = (g.nchunks + g.chunks_per_split - 1) / g.chunks_per_split;
+    const int smem = kStages * (kBM * kBK * 2 + g.BN * kBK * 2);
+    cudaError_t e = cudaFuncSetAttribute(conv_wgrad_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    if (e != cudaSuccess) return set_cuda_error("conv3x3 weight grad shared memory", e);
+    conv_wgrad_kernel<<<dim3(mtiles, ntiles, splits), kThreads, smem, cs(stream)>>>(g);
+    return launched("conv3x3 weight grad");
+}
+
+int agd_conv_weight_flip(int cin, int cout, const void *w, void *wt, agd_stream_t stream) {
+    if (cin <= 0 || cout <= 0 || !w || !wt) return set_error(AGD_STATUS_INVALID, "weight flip: bad arguments");
+    const long long n = (long long)cin * kpad_of(9 * cout);
+    weight_flip_kernel<<<(unsigned)((n + 255) / 256), 256, 0, cs(stream)>>>(
+        static_cast<const bf16 *>(w), cin, cout, kpad_of(9 * cin), kpad_of(9 * cout), static_cast<bf16 *>(wt));
+    return launched("weight flip");
+}
+
+int agd_ws_features(const float *metric, const float *seeds, int nseeds, int n, int H, int W, float h, void *x0,
+                    float *dref, agd_stream_t stream) {
+    if (!metric || !seeds || nseeds <= 0 || n <= 0 || H % 8 || W % 8 || H <= 0 || W <= 0 || !x0 || !dref)
+        return set_error(AGD_STATUS_INVALID, "features: bad arguments");
+    const long long m = (long long)n * (H / 4) * (W / 4);
+    features_kernel<<<(unsigned)((m + 255) / 256), 256, 0, cs(stream)>>>(metric, seeds, nseeds, n, H, W, h,
+                                                                         static_cast<bf16 *>(x0), dref);
+    return launched("features");
+}
+
+int agd_ws_target(const float *values, int n, int H, int W, const float *dref, float *target, agd_stream_t stream) {
+    if (!values || !dref || !target || n <= 0 || H % 4 || W % 4) return set_error(AGD_STATUS_INVALID, "target: bad arguments");
+    const long long m = (long long)n * (H / 4) * (W / 4);
+    target_kernel<<<(unsigned)((m + 255) / 256), 256, 0, cs(stream)>>>(values, n, H, W, dref, target);
+    return launched("target");
+}
+
+int agd_ws_avgpool(const void *x, int n, int H, int W, int C, void *y, agd_stream_t stream) {
+    if (!x || !y || n <= 0 || H % 2 || W % 2 || C % 8) return set_error(AGD_STATUS_INVALID, "avgpool: bad arguments");
+    const long long m = (long long)n * (H / 2) * (W / 2) * (C / 8);
+    avgpool_kernel<<<(unsigned)((m + 255) / 256), 256, 0, cs(stream)>>>(static_cast<const bf16 *>(x), n, H, W, C,
+                                                                        static_cast<bf16 *>(y));
+    return launched("avgpool");
+}
+
+int agd_ws_route(int n, int H, int W, int C, const void *y, agd_ws_term t0, agd_ws_term t1, void *dz,
+                 agd_stream_t stream) {
+    if (!dz || n <= 0 || C <= 0) return set_error(AGD_STATUS_INVALID, "route: bad arguments");
+    const agd_ws_term ts[2] = {t0, t1};
+    for (const agd_ws_term &t : ts)
+        if (t.mode < 0 || t.mode > 3 || (t.mode && (!t.data || t.offset + C > t.channels)))
+            return set_error(AGD_STATUS_INVALID, "route: bad term");
+    const long long m = (long long)n * H * W * C;
+    route_kernel<<<(unsigned)((m + 255) / 256), 256, 0, cs(stream)>>>(
+        n, H, W, C, static_cast<const bf16 *>(y), RouteTerm{t0.data, t0.mode, t0.channels, t0.offset},
+        RouteTerm{t1.data, t1.mode, t1.channels, t1.offset}, static_cast<bf16 *>(dz));
+    return launched("route");
+}
+
+int agd_ws_bias_grad(const void *dz, long long M, int C, float *db, agd_stream_t stream) {
+    if (!dz || !db || M <= 0 || C <= 0 || C > 256) return set_error(AGD_STATUS_INVALID, "bias grad: bad arguments");
+    const int threads = 256 / C * C;
+    const long long blocks = std::min<long long>(1184, (M + 255) / 256);
+    bias_grad_kernel<<<(unsigned)blocks, threads, 0, cs(stream)>>>(static_cast<const bf16 *>(dz), M, C, db);
+    return launched("bias grad");
+}
+
+int agd_ws_head_forward(const void *y, long long M, const float *w, const float *b, float *r, agd_stream_t stream) {
+    if (!y || !w || !b || !r || M <= 0) return set_error(AGD_STATUS_INVALID, "head: bad arguments");
+    head_forward_kernel<<<(unsigned)((M + 255) / 256), 256, 0, cs(stream)>>>(static_cast<const bf16 *>(y), M, w, b, r);
+    return launched("head forward");
+}
+
+int agd_ws_head_loss_backward(const void *y, long long M, const float *w, const float *r, const float *target,
+                              long long ncount, void *dz, float *dw, float *db, float *loss, agd_stream_t stream) {
+    if (!y || !w || !r || !target || !dz || !dw || !db || !loss || M <= 0 || ncount <= 0)
+        return set_error(AGD_STATUS_INVALID, "head loss: bad arguments");
+    head_loss_backward_kernel<<<(unsigned)((M + 255) / 256), 256, 0, cs(stream)>>>(
+        static_cast<const bf16 *>(y), M, w, r, target, 1.f / (float)ncount, static_cast<bf16 *>(dz), dw, db, loss);
+    return launched("head loss backward");
+}
+
+int agd_ws_adam(float *w, float *g, float *m, float *v, long long n, float lr, float beta1, float beta2, float eps,
+                int t, void *wb, agd_stream_t stream) {
+    if (!w || !g || !m || !v || n <= 0 || t < 1) return set_error(AGD_STATUS_INVALID, "adam: bad arguments");
+    const float bc1 = 1.f - powf(beta1, (float)t), bc2 = 1.f - powf(beta2, (float)t);
+    adam_kernel<<<(unsigned)((n + 255) / 256), 256, 0, cs(stream)>>>(w, g, m, v, n, lr, beta1, beta2, eps, bc1, bc2,
+                                                                     static_cast<bf16 *>(wb));
+    return launched("adam");
+}
+
+int agd_ws_release(const float *pred, int n, int Hb, int Wb, float epochs, int lag, uint16_t *release,
+                   agd_stream_t stream) {
+    if (!pred || !release || n <= 0 || Hb % 2 || Wb % 2 || !(epochs > 0.f))
+        return set_error(AGD_STATUS_INVALID, "release: bad arguments");
+    release_kernel<<<n, 256, 0, cs(stream)>>>(pred, Hb, Wb, 2, epochs, lag, release);
+    return launched("release");
+}
+
+int agd_ws_warm_values(const float *pred, int n, int H, int W, float margin, float *values, agd_stream_t stream) {
+    if (!pred || !values || n <= 0 || H % 8 || W % 8) return set_error(AGD_STATUS_INVALID, "warm values: bad arguments");
+    const long long m = (long long)n * H * W;
+    warm_values_kernel<<<(unsigned)((m + 255) / 256), 256, 0, cs(stream)>>>(pred, n, H / 4, W / 4, H, W, margin, values);
+    return launched("warm values");
+}
+
+}  // extern "C"

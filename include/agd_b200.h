@@ -100,6 +100,16 @@ typedef struct agd_instance {
      * need the stencil cache of agd_eikonal_solve / agd_plan_run (the fixed
      * scratch entry point refuses them). */
     const uint8_t *wall_dist;
+    /* Release epochs (no counterpart in the reference, whose fast iterative
+     * method visits a tile at the epoch after a neighbour changed,
+     * _solvers.py:94-120): per tile (tile order n_o), the first epoch at which
+     * the tile may be visited.  A tile the method asks for earlier waits in
+     * the list of its release epoch (at most 31 epochs ahead); the iteration
+     * still runs to the reference's stopping test, so the fixed point is the
+     * same.  A schedule made from predicted arrival times (the learned warm
+     * start) visits tiles near their upstream's convergence instead of at the
+     * front's first touch.  NULL: the reference's schedule. */
+    const uint16_t *release;
 } agd_instance;
 
 #define AGD_FLAG_ACTIVATE_ALL 1 /* every tile is active at the first iteration */

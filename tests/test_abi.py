@@ -1,4 +1,4 @@
-"""The C ABI library loads and exports every entry point include/agd_b200.h declares
+"""The C ABI library loads and exports every entry point include/*.h declares
 (no device work: runs without a GPU)."""
 import os
 import re
@@ -7,9 +7,13 @@ from conftest import REPO
 
 
 def _declared():
-    src = open(os.path.join(REPO, "include", "agd_b200.h")).read()
-    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
-    return sorted(set(re.findall(r"\b(agd_[a-z0-9_]+)\s*\(", src)))
+    names = set()
+    inc = os.path.join(REPO, "include")
+    for f in sorted(os.listdir(inc)):
+        if f.endswith(".h"):
+            src = re.sub(r"/\*.*?\*/", "", open(os.path.join(inc, f)).read(), flags=re.S)
+            names |= set(re.findall(r"\b(agd_[a-z0-9_]+)\s*\(", src))
+    return sorted(names)
 
 
 def test_library_exports_declared_symbols():
