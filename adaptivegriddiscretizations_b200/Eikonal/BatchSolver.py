@@ -44,8 +44,10 @@ class _Buffers:
         self.stats_host = torch.empty((s.batch, 2), dtype=torch.int64).pin_memory()
         self.bad_host = torch.empty(1, dtype=torch.int32).pin_memory()
         self.metric = self.cost = self.seed_index = self.seed_values = None  # staging, made on first use
+        self.release = None  # tile release epochs (batch, tiles) uint16, made on first use
         self.plan = None
         self.plan_atol = None
+        self.plan_gated = False
         self.ws = None
         self.job = None
 
@@ -176,8 +178,8 @@ class BatchSolver:
         mean = torch.nanmean(c.reshape(self.batch, -1).float(), dim=1).cpu().numpy().astype(np.float64)
         return (mean * _FLOAT_RES * 5.0).astype(np.float32)
 
-    def _plan(self, buf, atol):
-        if buf.plan is not None and np.array_equal(buf.plan_atol, atol):
+    def _plan(self, buf, atol, gated=False):
+        if buf.plan is not None and np.array_equal(buf.plan_atol, atol) and buf.plan_gated == gated:
             return
         L = _lib.lib()
         arr = (_lib.AgdInstance * self.batch)()
@@ -195,12 +197,15 @@ class BatchSolver:
             inst.geom = buf.geom[i].data_ptr() if self.riemann else None
             inst.rhs = buf.rhs[i].data_ptr()
             inst.seedbits = buf.seedbits[i].data_ptr()
+            if gated:
+                inst.release = buf.release[i].data_ptr()
         plan = ctypes.c_void_p()
         _lib.check(L.agd_plan_create(arr, self.batch, ctypes.byref(plan)), "plan")
         if buf.plan is not None:
             L.agd_plan_destroy(buf.plan)
         buf.plan = plan
         buf.plan_atol = atol
+        buf.plan_gated = gated
         nbytes = int(L.agd_plan_workspace_bytes(plan))
         if buf.ws is None or buf.ws.numel() < nbytes:
             with torch.cuda.stream(buf.stream):
@@ -230,9 +235,14 @@ class BatchSolver:
         return d
 
     # ----------------------------------------------------------------- submit --
-    def submit(self, metric=None, cost=None, seeds=None, seedValues=None, out=None):
+    def submit(self, metric=None, cost=None, seeds=None, seedValues=None, out=None, release=None, values=None):
         """Queues one batch; returns a SolverJob.  out: optional host tensor
-        (batch, *shape) float32 (page-locked for an asynchronous copy)."""
+        (batch, *shape) float32 (page-locked for an asynchronous copy).
+        release: optional device tensor (batch, tiles) of int16/uint16 tile
+        release epochs (agd_instance.release; the learned schedule); values:
+        optional device tensor (batch, tiles * tile size) of initial values in
+        tile layout (a warm start: upper bounds of the solution, since values
+        only decrease), instead of +inf."""
         if seeds is None:
             raise ValueError("Missing value for key seeds")
         if self.riemann and metric is None:
@@ -252,7 +262,14 @@ class BatchSolver:
         L = _lib.lib()
         with torch.cuda.stream(buf.stream):
             buf.stream.wait_stream(user_stream)  # device inputs made on the caller's stream
-            self._plan(buf, atol)
+            if release is not None:
+                ntiles = self.size_tot // int(np.prod(self.shape_i))
+                if tuple(release.shape) != (self.batch, ntiles) or release.dtype not in (torch.int16, torch.uint16):
+                    raise ValueError(f"release must be a 16-bit tensor of shape {(self.batch, ntiles)}")
+                if buf.release is None:
+                    buf.release = torch.empty((self.batch, ntiles), dtype=torch.int16, device="cuda")
+                buf.release.copy_(release.view(torch.int16))
+            self._plan(buf, atol, gated=release is not None)
             prep = _lib.AgdBatchPrep()
             prep.model = _lib.AGD_MODEL_RIEMANN if self.riemann else _lib.AGD_MODEL_ISOTROPIC
             prep.ndim, prep.n = self.ndim, self.batch
@@ -280,6 +297,10 @@ class BatchSolver:
             prep.seedbits, prep.bad_seed = buf.seedbits.data_ptr(), buf.bad.data_ptr()
             st = _lib.stream_ptr(buf.stream)
             _lib.check(L.agd_prep_batch(ctypes.byref(prep), st), "prep_batch")
+            if values is not None:
+                if tuple(values.shape) != (self.batch, self.size_tot) or not values.is_cuda:
+                    raise ValueError(f"values must be a device tensor of shape {(self.batch, self.size_tot)}")
+                buf.values.copy_(values)
             lp = ctypes.byref(self.launch) if self.launch is not None else None
             _lib.check(L.agd_plan_run(buf.plan, _lib.ptr(buf.ws), buf.ws.numel(), _lib.ptr(buf.stats), lp, st),
                        "solve")

@@ -21,8 +21,9 @@ namespace unet {
 using bf16 = __nv_bfloat16;
 constexpr int kBM = 128;           // rows (pixels, or weight rows) per CTA tile
 constexpr int kBK = 64;            // K elements per pipeline stage (8 x 16-byte units)
-constexpr int kStages = 4;
-constexpr int kThreads = 160;      // 4 producer / epilogue warps + 1 MMA warp
+constexpr int kMaxStages = 8;        // operand stages in shared memory (Pipe holds 8 barriers each way)
+constexpr int kSmemBudget = 200 * 1024;  // dynamic shared memory of a conv CTA alone on its SM
+constexpr int kSmemBudget2 = 104 * 1024; // ... of one of two conv CTAs per SM
 constexpr unsigned long long kWaitNs = 2000000000ull;  // bound on every barrier wait
 
 __host__ __device__ inline int kpad_of(int k) { return (k + kBK - 1) / kBK * kBK; }
@@ -47,6 +48,7 @@ struct GemmArgs {
     bf16 *out_bf;
     float *out_f;
     long long M;  // pixels
+    int wshift;   // log2(W) when W is a power of two, else -1
     unsigned *err;
 };
 
@@ -61,104 +63,278 @@ __device__ __forceinline__ uint32_t tmem_cols(int bn) {
     return c;
 }
 
+// The convolution GEMMs are persistent and warp-specialised: each CTA loops
+// over output tiles; warps 0-3 load operands (cp.async, 16 bytes a lane,
+// zero-filled outside the image), warp 4 allocates tensor memory and one of
+// its lanes issues the tcgen05 MMAs, warps 5-8 run the epilogue.  Two CTAs
+// share an SM where their tensor memory (2 x 2 x BN columns) and shared memory
+// allow it: the pipelines' latencies then overlap.  The
+// accumulator is double-buffered in tensor memory, so the epilogue of a tile
+// overlaps the main loop of the next; operand stages cycle through shared
+// memory across tiles.  Every wait is bounded (kWaitNs) and sets *err.
+constexpr int kProducers = 128;  // warps 0-3
+constexpr int kMmaWarp = kProducers / 32;  // warp 4
+constexpr int kEpilogue = 128;   // warps 5-8
+constexpr int kPThreads = kProducers + 32 + kEpilogue;  // 288
+constexpr int kUnitsPerThread = kBM * 8 / kProducers;  // A units (16 bytes) per producer thread and stage
+
+struct Pipe {
+    uint64_t full[8], empty[8], accf[2], acce[2], bready;
+    uint32_t taddr;
+};
+
+__device__ __forceinline__ void pipe_init(Pipe &P, int stages) {
+    for (int s = 0; s < stages; ++s) {
+        umma::mbar_init(&P.full[s], kProducers);
+        umma::mbar_init(&P.empty[s], 1);
+    }
+    for (int a = 0; a < 2; ++a) {
+        umma::mbar_init(&P.accf[a], 1);
+        umma::mbar_init(&P.acce[a], kEpilogue / 32);
+    }
+    umma::mbar_init(&P.bready, kProducers);
+    umma::fence_mbar_init();
+}
+
+// A bounded barrier wait whose result is the same in every lane of the warp
+// (false if any lane gave up), so that the warp leaves its loops together.
+__device__ __forceinline__ bool mbar_wait_warp(uint64_t *bar, uint32_t parity, unsigned *err,
+                                               unsigned long long timeout_ns) {
+    const bool ok = umma::mbar_wait(bar, parity, err, timeout_ns);
+    return __all_sync(0xffffffffu, ok);
+}
+
+// Before the CTA frees its tensor memory: the MMAs of the last tile are complete
+// (its accumulator barrier's phase), also when the epilogue gave up early.
+__device__ __forceinline__ void mma_drain(Pipe &P, int ntile_local, unsigned *err) {
+    if (ntile_local <= 0) return;
+    const int tl = ntile_local - 1;
+    mbar_wait_warp(&P.accf[tl & 1], (tl >> 1) & 1, err, kWaitNs);
+}
+
+// Ring position of a pipeline stage: index and the parity of its current use.
+struct Ring {
+    int s = 0;
+    uint32_t ph = 0;
+    __device__ __forceinline__ void next(int stages) {
+        if (++s == stages) {
+            s = 0;
+            ph ^= 1u;
+        }
+    }
+};
+
+// MMA warp (all lanes wait, lane 0 issues): for each tile, waits for a free
+// accumulator, then for each K chunk its stage, issues 4 MMAs of K = 16, frees
+// the stage; commits the accumulator.  B: per stage (stationary = false) or one
+// resident region of every chunk.
+__device__ __forceinline__ void mma_role(Pipe &P, int ntile_local, int nk, uint32_t sbase,
+                                         uint32_t stage_bytes, uint32_t a_bytes, int stages, bool stationary,
+                                         uint32_t bstat, uint32_t bchunk_bytes, uint32_t idesc, int bn,
+                                         unsigned *err) {
+    const bool leader = (threadIdx.x & 31) == 0;
+    // descriptors advance by the stage size; a K step of 16 is 256 bytes (16 in
+    // the descriptor's address field)
+    const uint64_t ad0 = umma::smem_desc(sbase, 128u, 1024u);
+    const uint64_t bs0 = umma::smem_desc(bstat, 128u, 1024u);
+    const uint64_t dstage = stage_bytes >> 4, dab = a_bytes >> 4, dbchunk = bchunk_bytes >> 4;
+    Ring R;
+    uint64_t ad = ad0;
+    bool ok = true;
+    if (stationary) ok = mbar_wait_warp(&P.bready, 0, err, kWaitNs);
+    for (int tl = 0; tl < ntile_local && ok; ++tl) {
+        const int a = tl & 1;
+        if (tl >= 2 && !mbar_wait_warp(&P.acce[a], ((tl >> 1) & 1) ^ 1, err, kWaitNs)) break;
+        umma::tc_fence_after_sync();
+        const uint32_t d = P.taddr + (uint32_t)(a * bn);
+        uint64_t bsd = bs0;
+        for (int i = 0; i < nk; ++i) {
+            if (!mbar_wait_warp(&P.full[R.s], R.ph, err, kWaitNs)) {
+                ok = false;
+                break;
+            }
+            umma::fence_proxy_async_smem();  // the producers' cp.async writes before the tensor core reads
+            umma::tc_fence_after_sync();
+            const uint64_t bd = stationary ? bsd : ad + dab;
+            if (leader) {
+#pragma unroll
+                for (int kk = 0; kk < kBK / 16; ++kk) umma::mma_bf16(d, ad + 16u * kk, bd + 16u * kk, idesc, (i | kk) != 0);
+                umma::mma_commit(&P.empty[R.s]);
+            }
+            __syncwarp();
+            bsd += dbchunk;
+            ad += dstage;
+            R.next(stages);
+            if (R.s == 0) ad = ad0;
+        }
+        if (leader) umma::mma_commit(&P.accf[a]);
+        __syncwarp();
+    }
+    mma_drain(P, ntile_local, err);
+}
+
+__device__ __forceinline__ int count_tiles(int total) {
+    return total > (int)blockIdx.x ? (total - (int)blockIdx.x + (int)gridDim.x - 1) / (int)gridDim.x : 0;
+}
+
 // D[m, n] = sum_k A[m, k] B[n, k]: A the implicit im2col of the input (m a
 // pixel, k = tap * cin + ci, tap = 3 (dy + 1) + (dx + 1), zero outside the
 // image), B the weight matrix.  Epilogue: + bias, ReLU, bf16 or fp32 NHWC.
 // Shared memory per stage: A 128 x 64 and B BN x 64 bf16 in the no-swizzle
 // K-major core-matrix layout (16-byte unit u at byte 16 u, u = (row / 8) * 64 +
 // kunit * 8 + row % 8), which makes every producer lane's unit a single cp.async.
-__global__ void __launch_bounds__(kThreads) conv_gemm_kernel(GemmArgs g) {
-    extern __shared__ __align__(1024) unsigned char smem[];
-    __shared__ __align__(8) uint64_t full[kStages], empty[kStages], accf;
-    __shared__ uint32_t s_taddr;
-    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const long long m0 = (long long)blockIdx.x * kBM;
-    const int n0 = blockIdx.y * g.BN;
-    const uint32_t ncols = tmem_cols(g.BN);
-    const uint32_t a_bytes = kBM * kBK * 2, b_bytes = (uint32_t)g.BN * kBK * 2;
-    const uint32_t stage_bytes = a_bytes + b_bytes;
-    const uint32_t sbase = umma::smem_u32(smem);
+// With one channel tile and small weights, B stays resident for the whole launch.
+struct GemmLaunch {
+    int stages, stationary, mtiles, ntiles;
+};
 
-    if (warp == 4) {
-        umma::tmem_alloc(&s_taddr, ncols);
+__global__ void __launch_bounds__(kPThreads, 2) conv_gemm_kernel(GemmArgs g, GemmLaunch gl) {
+    extern __shared__ __align__(1024) unsigned char smem[];
+    __shared__ Pipe P;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const uint32_t ncols = tmem_cols(2 * g.BN);
+    const uint32_t a_bytes = kBM * kBK * 2, bchunk = (uint32_t)g.BN * kBK * 2;
+    const uint32_t stage_bytes = a_bytes + (gl.stationary ? 0u : bchunk);
+    const uint32_t sbase = umma::smem_u32(smem);
+    const uint32_t bstat = sbase + gl.stages * stage_bytes;
+    const int total = gl.mtiles * gl.ntiles;
+    const int ntl = count_tiles(total);
+
+    if (warp == kMmaWarp) {
+        umma::tmem_alloc(&P.taddr, ncols);
         umma::tmem_relinquish();
     }
-    if (tid == 0) {
-        for (int s = 0; s < kStages; ++s) {
-            umma::mbar_init(&full[s], 128);
-            umma::mbar_init(&empty[s], 1);
-        }
-        umma::mbar_init(&accf, 1);
-        umma::fence_mbar_init();
-    }
+    if (tid == 0) pipe_init(P, gl.stages);
     umma::tc_fence_before_sync();
     __syncthreads();
     umma::tc_fence_after_sync();
-    const uint32_t taddr = s_taddr;
 
-    if (warp < 4) {
+    if (warp < kMmaWarp) {
         // ---------------------------------------------------------- producer
-        // A: rows 8 * ((tid >> 6) + 2 j) + (tid & 7), j < 8, K unit (tid >> 3) & 7.
-        const int c = (tid >> 3) & 7;
-        int py[8], px[8], pn[8];
-#pragma unroll
-        for (int j = 0; j < 8; ++j) {
-            const long long m = m0 + 8 * ((tid >> 6) + 2 * j) + (tid & 7);
-            if (m < g.M) {
-                const int hw = g.H * g.W;
-                pn[j] = (int)(m / hw);
-                const int r = (int)(m - (long long)pn[j] * hw);
-                py[j] = r / g.W;
-                px[j] = r - py[j] * g.W;
-            } else {
-                pn[j] = -1;
-                py[j] = px[j] = 0;
-            }
-        }
-        const int nb_units = g.BN * 8;  // B units per stage
-        for (int i = 0; i < g.kchunks; ++i) {
-            const int s = i % kStages;
-            if (i >= kStages && !umma::mbar_wait(&empty[s], ((i / kStages) & 1) ^ 1, g.err, kWaitNs)) break;
-            const uint32_t sa = sbase + s * stage_bytes, sb = sa + a_bytes;
-            const int k8 = i * 8 + c;
-            int tap = 0, ci8 = 0, dy = 0, dx = 0;
-            const bool kin = k8 < g.K8;
-            if (kin) {
-                tap = k8 / g.cin8;
-                ci8 = k8 - tap * g.cin8;
-                dy = tap / 3 - 1;
-                dx = tap - 3 * (tap / 3) - 1;
-            }
-            const bool first = ci8 * 8 < g.s0.C;
-            const Src &S = first ? g.s0 : g.s1;
-            const int ch = first ? ci8 * 8 : ci8 * 8 - g.s0.C;
-#pragma unroll
-            for (int j = 0; j < 8; ++j) {
-                const int u = tid + 128 * j;
-                const int y = py[j] + dy, x = px[j] + dx;
-                const bool ok = kin && pn[j] >= 0 && y >= 0 && y < g.H && x >= 0 && x < g.W;
-                const void *src = ok ? (const void *)src_ptr(S, pn[j], y, x, g.H, g.W, ch) : (const void *)g.wmat;
-                umma::cp_async16(sa + 16u * u, src, ok ? 16u : 0u);
-            }
-            for (int u = tid; u < nb_units; u += 128) {
-                const int n = n0 + ((u >> 6) << 3) + (u & 7);
+        if (gl.stationary) {  // every chunk of B once
+            const int units = g.kchunks * g.BN * 8;
+            for (int v = tid; v < units; v += kProducers) {
+                const int i = v / (g.BN * 8), u = v - i * (g.BN * 8);
+                const int n = ((u >> 6) << 3) + (u & 7);
                 const int kk = i * 8 + ((u >> 3) & 7);
                 const bool ok = n < g.N && kk < g.K8;
                 const void *src = ok ? (const void *)(g.wmat + (long long)n * g.kpad + kk * 8) : (const void *)g.wmat;
-                umma::cp_async16(sb + 16u * u, src, ok ? 16u : 0u);
+                umma::cp_async16(bstat + i * bchunk + 16u * u, src, ok ? 16u : 0u);
             }
-            umma::cp_async_mbar_arrive(&full[s]);
+            umma::cp_async_mbar_arrive(&P.bready);
         }
+        // A: rows 8 ((tid >> 6) + (kProducers / 64) j) + (tid & 7), j < kUnitsPerThread, K unit c = (tid >> 3) & 7
+        // of each chunk.  Per tile: each row's pixel address in both inputs and
+        // its mask of taps inside the image (bits 0-8) with the pixel's row and
+        // column parities (bits 9, 10: the offsets of an upsampled input).
+        const int c = (tid >> 3) & 7;
+        const int C0 = g.s0.C, C1 = g.s1.C, W0s = g.W >> g.s0.up, W1s = g.W >> g.s1.up;
+        Ring R;
+        bool wrapped = false, alive = true;
+        for (int tl = 0; tl < ntl && alive; ++tl) {
+            const int t = blockIdx.x + tl * gridDim.x;
+            const int mt = t % gl.mtiles, nt = t / gl.mtiles;
+            const long long m0 = (long long)mt * kBM;
+            const int n0 = nt * g.BN;
+            const bf16 *b0[kUnitsPerThread], *b1[kUnitsPerThread];
+            unsigned vm[kUnitsPerThread];
+            // image of the tile's first row; rows beyond it (a tile straddling
+            // two images) step to the next image below
+            const int hw = g.H * g.W;
+            const int nb0 = (int)(m0 / hw);
+            const int r0 = (int)(m0 - (long long)nb0 * hw);
+#pragma unroll
+            for (int j = 0; j < kUnitsPerThread; ++j) {
+                const int row = 8 * ((tid >> 6) + (kProducers / 64) * j) + (tid & 7);
+                vm[j] = 0u;
+                b0[j] = b1[j] = g.s0.p;
+                if (m0 + row < g.M) {
+                    int r = r0 + row, nb = nb0;
+                    while (r >= hw) {  // at most kBM / hw + 1 steps
+                        r -= hw;
+                        ++nb;
+                    }
+                    const int y = g.wshift >= 0 ? r >> g.wshift : r / g.W;
+                    const int x = r - y * g.W;
+                    b0[j] = src_ptr(g.s0, nb, y, x, g.H, g.W, 0);
+                    if (g.s1.p) b1[j] = src_ptr(g.s1, nb, y, x, g.H, g.W, 0);
+                    unsigned mk = 0u;
+#pragma unroll
+                    for (int tap = 0; tap < 9; ++tap) {
+                        const int yy = y + tap / 3 - 1, xx = x + tap % 3 - 1;
+                        mk |= (yy >= 0 && yy < g.H && xx >= 0 && xx < g.W) ? (1u << tap) : 0u;
+                    }
+                    vm[j] = mk | ((unsigned)(y & 1) << 9) | ((unsigned)(x & 1) << 10);
+                }
+            }
+            int tap = c / g.cin8, ci8 = c - (c / g.cin8) * g.cin8;  // of unit c of chunk 0
+            for (int i = 0; i < g.kchunks; ++i) {
+                if (wrapped && !mbar_wait_warp(&P.empty[R.s], R.ph ^ 1u, g.err, kWaitNs)) {
+                    alive = false;
+                    break;
+                }
+                const uint32_t sa = sbase + R.s * stage_bytes, sb = sa + a_bytes;
+                const bool kin = tap < 9;
+                const int dy = tap / 3 - 1, dx = tap - 3 * (tap / 3) - 1;
+                const bool first = ci8 * 8 < C0;
+                const int ch = first ? ci8 * 8 : ci8 * 8 - C0;
+                const int up = first ? g.s0.up : g.s1.up;
+                const int Cs = first ? C0 : C1, Ws = first ? W0s : W1s;
+                const long long offp = (long long)(dy * Ws + dx) * Cs + ch;  // same-resolution input
+#pragma unroll
+                for (int j = 0; j < kUnitsPerThread; ++j) {
+                    const int u = tid + kProducers * j;
+                    const bool ok = kin && ((vm[j] >> tap) & 1u);
+                    long long off = offp;
+                    if (up) {
+                        const int ey = (int)((vm[j] >> 9) & 1u) + dy, ex = (int)((vm[j] >> 10) & 1u) + dx;
+                        off = (long long)((ey >> 1) * Ws + (ex >> 1)) * Cs + ch;
+                    }
+                    const void *src = ok ? (const void *)((first ? b0[j] : b1[j]) + off) : (const void *)g.wmat;
+                    umma::cp_async16(sa + 16u * u, src, ok ? 16u : 0u);
+                }
+                if (!gl.stationary) {
+                    for (int u = tid; u < g.BN * 8; u += kProducers) {
+                        const int n = n0 + ((u >> 6) << 3) + (u & 7);
+                        const int kk = i * 8 + ((u >> 3) & 7);
+                        const bool ok = n < g.N && kk < g.K8;
+                        const void *src =
+                            ok ? (const void *)(g.wmat + (long long)n * g.kpad + kk * 8) : (const void *)g.wmat;
+                        umma::cp_async16(sb + 16u * u, src, ok ? 16u : 0u);
+                    }
+                }
+                umma::cp_async_mbar_arrive(&P.full[R.s]);
+                R.next(gl.stages);
+                wrapped = wrapped || R.s == 0;
+                // unit c of the next chunk: 8 units further along K
+                ci8 += 8;
+                while (ci8 >= g.cin8 && tap < 9) {
+                    ci8 -= g.cin8;
+                    ++tap;
+                }
+            }
+        }
+    } else if (warp == kMmaWarp) {
+        {
+            mma_role(P, ntl, g.kchunks, sbase, stage_bytes, a_bytes, gl.stages, gl.stationary != 0, bstat, bchunk,
+                     umma::idesc_bf16(kBM, g.BN, 0, 0), g.BN, g.err);
+        }
+    } else {
         // ---------------------------------------------------------- epilogue
-        const bool ok = umma::mbar_wait(&accf, 0, g.err, kWaitNs);
-        umma::tc_fence_after_sync();
-        if (ok && !*((volatile unsigned *)g.err)) {
-            const long long m = m0 + 32 * warp + lane;
+        const int ew = warp & 3;  // TMEM lane quarter of this warp
+        for (int tl = 0; tl < ntl; ++tl) {
+            const int a = tl & 1;
+            const bool ok = mbar_wait_warp(&P.accf[a], (tl >> 1) & 1, g.err, kWaitNs);
+            umma::tc_fence_after_sync();
+            if (!ok) break;
+            const int t = blockIdx.x + tl * gridDim.x;
+            const int mt = t % gl.mtiles, nt = t / gl.mtiles;
+            const long long m = (long long)mt * kBM + 32 * ew + lane;
             for (int c0 = 0; c0 < g.BN; c0 += 16) {
                 uint32_t r[16];
-                umma::tmem_ld16(taddr + ((uint32_t)(32 * warp) << 16) + (uint32_t)c0, r);
+                umma::tmem_ld16(P.taddr + ((uint32_t)(32 * ew) << 16) + (uint32_t)(a * g.BN + c0), r);
                 umma::tmem_ld_wait();
-                const int nc = n0 + c0;
+                const int nc = nt * g.BN + c0;
                 if (m >= g.M || nc >= g.N) continue;
                 float v[16];
 #pragma unroll
@@ -184,40 +360,27 @@ __global__ void __launch_bounds__(kThreads) conv_gemm_kernel(GemmArgs g) {
                     for (int q = 0; q < 4; ++q) dst[q] = make_float4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
                 }
             }
+            umma::tc_fence_before_sync();
+            __syncwarp();
+            if (lane == 0) asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(umma::smem_u32(&P.acce[a])) : "memory");
         }
-    } else if (lane == 0) {
-        // ------------------------------------------------------------- MMA
-        const uint32_t idesc = umma::idesc_bf16(kBM, g.BN, 0, 0);
-        for (int i = 0; i < g.kchunks; ++i) {
-            const int s = i % kStages;
-            if (!umma::mbar_wait(&full[s], (i / kStages) & 1, g.err, kWaitNs)) break;
-            umma::fence_proxy_async_smem();
-            umma::tc_fence_after_sync();
-            const uint32_t sa = sbase + s * stage_bytes, sb = sa + a_bytes;
-#pragma unroll
-            for (int kk = 0; kk < kBK / 16; ++kk) {
-                const uint64_t ad = umma::smem_desc(sa + 256u * kk, 128u, 1024u);
-                const uint64_t bd = umma::smem_desc(sb + 256u * kk, 128u, 1024u);
-                umma::mma_bf16(taddr, ad, bd, idesc, (i | kk) != 0);
-            }
-            umma::mma_commit(&empty[s]);
-        }
-        umma::mma_commit(&accf);  // also on a failed wait: completes once the issued MMAs are done
     }
     umma::cp_async_wait_all();
     umma::tc_fence_before_sync();
     __syncthreads();
-    if (warp == 4) {
+    if (warp == kMmaWarp) {
         umma::tc_fence_after_sync();
-        umma::tmem_dealloc(taddr, ncols);
+        umma::tmem_dealloc(P.taddr, ncols);
     }
 }
 
 // Weight gradient: dW[n, r] += sum_p dZ[p, n] X[p + tap(r), ci(r)], r = tap *
-// cin + ci.  GEMM with M = r (128 per CTA), N = n, K = pixels (64 per stage,
-// split over gridDim.z): both operands MN-major (8 consecutive channels of one
-// pixel per 16-byte unit, as they lie in NHWC memory).  Shared layout: unit
-// (group g of 8 rows, pixel k) at byte 16 (g * 64 + k).
+// cin + ci.  GEMM with M = r (128 per tile), N = n, K = pixels (64 per stage,
+// split over `splits` work items): both operands MN-major (8 consecutive
+// channels of one pixel per 16-byte unit, as they lie in NHWC memory).  Shared
+// layout: unit (group g of 8 rows, pixel k) at byte 16 (g * 64 + k).  Work
+// item t: row tile t % mtiles, channel tile (t / mtiles) % ntiles, split
+// t / (mtiles ntiles); its partial sums go to dw by atomic adds.
 struct WgradArgs {
     int nimg, H, W;
     Src s0, s1;
@@ -228,130 +391,177 @@ struct WgradArgs {
     int kpad;
     long long M;
     int nchunks, chunks_per_split;
+    int mtiles, ntiles, splits, stages;
+    int wshift;  // log2(W) when W is a power of two, else -1
     unsigned *err;
 };
 
-__global__ void __launch_bounds__(kThreads) conv_wgrad_kernel(WgradArgs g) {
+__global__ void __launch_bounds__(kPThreads, 2) conv_wgrad_kernel(WgradArgs g) {
     extern __shared__ __align__(1024) unsigned char smem[];
-    __shared__ __align__(8) uint64_t full[kStages], empty[kStages], accf;
-    __shared__ uint32_t s_taddr;
+    __shared__ Pipe P;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const int mt = blockIdx.x, n0 = blockIdx.y * g.BN;
-    const int c_begin = blockIdx.z * g.chunks_per_split;
-    const int c_end = min(g.nchunks, c_begin + g.chunks_per_split);
-    const int nk = max(0, c_end - c_begin);
-    const uint32_t ncols = tmem_cols(g.BN);
+    const uint32_t ncols = tmem_cols(2 * g.BN);
     const uint32_t a_bytes = kBM * kBK * 2, b_bytes = (uint32_t)g.BN * kBK * 2;
     const uint32_t stage_bytes = a_bytes + b_bytes;
     const uint32_t sbase = umma::smem_u32(smem);
+    const int total = g.mtiles * g.ntiles * g.splits;
+    const int ntl = count_tiles(total);
+    // every split has chunks_per_split chunks except possibly the last; the MMA
+    // and the producers agree on each item's count through item_chunks()
+    auto item_chunks = [&](int t) {
+        const int sp = t / (g.mtiles * g.ntiles);
+        return min(g.nchunks, (sp + 1) * g.chunks_per_split) - sp * g.chunks_per_split;
+    };
 
-    if (warp == 4) {
-        umma::tmem_alloc(&s_taddr, ncols);
+    if (warp == kMmaWarp) {
+        umma::tmem_alloc(&P.taddr, ncols);
         umma::tmem_relinquish();
     }
-    if (tid == 0) {
-        for (int s = 0; s < kStages; ++s) {
-            umma::mbar_init(&full[s], 128);
-            umma::mbar_init(&empty[s], 1);
-        }
-        umma::mbar_init(&accf, 1);
-        umma::fence_mbar_init();
-    }
+    if (tid == 0) pipe_init(P, g.stages);
     umma::tc_fence_before_sync();
     __syncthreads();
     umma::tc_fence_after_sync();
-    const uint32_t taddr = s_taddr;
 
-    if (warp < 4) {
+    if (warp < kMmaWarp) {
         const int pk = tid & 63;
-        // the 8 weight-row groups of this thread: g = (tid >> 6) + 2 j
-        int gdy[8], gdx[8], gch[8], gsrc[8];
+        Ring R;
+        bool wrapped = false, alive = true;
+        for (int tl = 0; tl < ntl && alive; ++tl) {
+            const int t = blockIdx.x + tl * gridDim.x;
+            const int mt = t % g.mtiles, nt = (t / g.mtiles) % g.ntiles, sp = t / (g.mtiles * g.ntiles);
+            const int n0 = nt * g.BN;
+            // the weight-row groups of this thread, (tid >> 6) + (kProducers / 64) j: tap, source, channel
+            int gtap[kUnitsPerThread], gch[kUnitsPerThread], gsrc[kUnitsPerThread];
 #pragma unroll
-        for (int j = 0; j < 8; ++j) {
-            const int kk8 = mt * 16 + (tid >> 6) + 2 * j;
-            if (kk8 < g.K8) {
-                const int tap = kk8 / g.cin8, ci8 = kk8 - (kk8 / g.cin8) * g.cin8;
-                gdy[j] = tap / 3 - 1;
-                gdx[j] = tap - 3 * (tap / 3) - 1;
-                gsrc[j] = ci8 * 8 < g.s0.C ? 0 : 1;
-                gch[j] = gsrc[j] ? ci8 * 8 - g.s0.C : ci8 * 8;
-            } else {
-                gsrc[j] = -1;
-                gdy[j] = gdx[j] = gch[j] = 0;
+            for (int j = 0; j < kUnitsPerThread; ++j) {
+                const int kk8 = mt * 16 + (tid >> 6) + (kProducers / 64) * j;
+                if (kk8 < g.K8) {
+                    const int tap = kk8 / g.cin8, ci8 = kk8 - (kk8 / g.cin8) * g.cin8;
+                    gtap[j] = tap;
+                    gsrc[j] = ci8 * 8 < g.s0.C ? 0 : 1;
+                    gch[j] = gsrc[j] ? ci8 * 8 - g.s0.C : ci8 * 8;
+                } else {
+                    gsrc[j] = -1;
+                    gtap[j] = gch[j] = 0;
+                }
+            }
+            const int nk = item_chunks(t);
+            const int hw = g.H * g.W;
+            // this thread's pixel of the item's first chunk; it advances by kBK a chunk
+            long long p = (long long)sp * g.chunks_per_split * kBK + pk;
+            int pnb = (int)(p / hw), pr = (int)(p - (long long)pnb * hw);
+            for (int i = 0; i < nk; ++i, p += kBK) {
+                if (wrapped && !mbar_wait_warp(&P.empty[R.s], R.ph ^ 1u, g.err, kWaitNs)) {
+                    alive = false;
+                    break;
+                }
+                const uint32_t sa = sbase + R.s * stage_bytes, sb = sa + a_bytes;
+                int nb = -1, y = 0, x = 0;
+                if (p < g.M) {
+                    nb = pnb;
+                    y = g.wshift >= 0 ? pr >> g.wshift : pr / g.W;
+                    x = pr - y * g.W;
+                }
+                pr += kBK;
+                while (pr >= hw) {
+                    pr -= hw;
+                    ++pnb;
+                }
+#pragma unroll
+                for (int j = 0; j < kUnitsPerThread; ++j) {
+                    const int u = tid + kProducers * j;
+                    const int yy = y + gtap[j] / 3 - 1, xx = x + gtap[j] % 3 - 1;
+                    const bool ok = nb >= 0 && gsrc[j] >= 0 && yy >= 0 && yy < g.H && xx >= 0 && xx < g.W;
+                    const Src &S = gsrc[j] == 1 ? g.s1 : g.s0;
+                    const void *src = ok ? (const void *)src_ptr(S, nb, yy, xx, g.H, g.W, gch[j]) : (const void *)g.dz;
+                    umma::cp_async16(sa + 16u * u, src, ok ? 16u : 0u);
+                }
+                const bf16 *dzp = g.dz + p * g.N;
+                for (int u = tid; u < g.BN * 8; u += kProducers) {
+                    const int n = n0 + ((u >> 6) << 3);
+                    const bool ok = nb >= 0 && n < g.N;
+                    const void *src = ok ? (const void *)(dzp + n) : (const void *)g.dz;
+                    umma::cp_async16(sb + 16u * u, src, ok ? 16u : 0u);
+                }
+                umma::cp_async_mbar_arrive(&P.full[R.s]);
+                R.next(g.stages);
+                wrapped = wrapped || R.s == 0;
             }
         }
-        const int nb_units = g.BN * 8;
-        for (int i = 0; i < nk; ++i) {
-            const int s = i % kStages;
-            if (i >= kStages && !umma::mbar_wait(&empty[s], ((i / kStages) & 1) ^ 1, g.err, kWaitNs)) break;
-            const uint32_t sa = sbase + s * stage_bytes, sb = sa + a_bytes;
-            const long long p = (long long)(c_begin + i) * kBK + pk;
-            int nb = -1, y = 0, x = 0;
-            if (p < g.M) {
-                const int hw = g.H * g.W;
-                nb = (int)(p / hw);
-                const int r = (int)(p - (long long)nb * hw);
-                y = r / g.W;
-                x = r - y * g.W;
-            }
+    } else if (warp == kMmaWarp) {
+        {
+            // all lanes wait, lane 0 issues; per-item chunk counts differ only
+            // for the last split, so the loop is written out here
+            const bool leader = lane == 0;
+            const uint32_t idesc = umma::idesc_bf16(kBM, g.BN, 1, 1);
+            const uint64_t ad0 = umma::smem_desc(sbase, 128u, 1024u);
+            const uint64_t dstage = stage_bytes >> 4, dab = a_bytes >> 4;
+            Ring R;
+            uint64_t ad = ad0;
+            for (int tl = 0; tl < ntl; ++tl) {
+                const int a = tl & 1;
+                if (tl >= 2 && !mbar_wait_warp(&P.acce[a], ((tl >> 1) & 1) ^ 1, g.err, kWaitNs)) break;
+                umma::tc_fence_after_sync();
+                const uint32_t d = P.taddr + (uint32_t)(a * g.BN);
+                const int nk = item_chunks(blockIdx.x + tl * gridDim.x);
+                bool ok = true;
+                for (int i = 0; i < nk; ++i) {
+                    if (!mbar_wait_warp(&P.full[R.s], R.ph, g.err, kWaitNs)) {
+                        ok = false;
+                        break;
+                    }
+                    umma::fence_proxy_async_smem();
+                    umma::tc_fence_after_sync();
+                    if (leader) {
 #pragma unroll
-            for (int j = 0; j < 8; ++j) {
-                const int u = tid + 128 * j;
-                const int yy = y + gdy[j], xx = x + gdx[j];
-                const bool ok = nb >= 0 && gsrc[j] >= 0 && yy >= 0 && yy < g.H && xx >= 0 && xx < g.W;
-                const Src &S = gsrc[j] == 1 ? g.s1 : g.s0;
-                const void *src = ok ? (const void *)src_ptr(S, nb, yy, xx, g.H, g.W, gch[j]) : (const void *)g.dz;
-                umma::cp_async16(sa + 16u * u, src, ok ? 16u : 0u);
+                        for (int kk = 0; kk < kBK / 16; ++kk)
+                            umma::mma_bf16(d, ad + 16u * kk, ad + dab + 16u * kk, idesc, (i | kk) != 0);
+                        umma::mma_commit(&P.empty[R.s]);
+                    }
+                    __syncwarp();
+                    ad += dstage;
+                    R.next(g.stages);
+                    if (R.s == 0) ad = ad0;
+                }
+                if (leader) umma::mma_commit(&P.accf[a]);
+                __syncwarp();
+                if (!ok) break;
             }
-            for (int u = tid; u < nb_units; u += 128) {
-                const int n = n0 + ((u >> 6) << 3);
-                const bool ok = nb >= 0 && n < g.N;
-                const void *src = ok ? (const void *)(g.dz + p * g.N + n) : (const void *)g.dz;
-                umma::cp_async16(sb + 16u * u, src, ok ? 16u : 0u);
-            }
-            umma::cp_async_mbar_arrive(&full[s]);
+            mma_drain(P, ntl, g.err);
         }
-        const bool ok = nk > 0 && umma::mbar_wait(&accf, 0, g.err, kWaitNs);
-        umma::tc_fence_after_sync();
-        if (ok && !*((volatile unsigned *)g.err)) {
-            const int r = mt * kBM + 32 * warp + lane;  // weight row (tap, ci)
+    } else {
+        const int ew = warp & 3;
+        for (int tl = 0; tl < ntl; ++tl) {
+            const int a = tl & 1;
+            const bool ok = mbar_wait_warp(&P.accf[a], (tl >> 1) & 1, g.err, kWaitNs);
+            umma::tc_fence_after_sync();
+            if (!ok) break;
+            const int t = blockIdx.x + tl * gridDim.x;
+            const int mt = t % g.mtiles, nt = (t / g.mtiles) % g.ntiles;
+            const int r = mt * kBM + 32 * ew + lane;  // weight row (tap, ci)
             const bool rin = r < g.K8 * 8;
             for (int c0 = 0; c0 < g.BN; c0 += 16) {
                 uint32_t v[16];
-                umma::tmem_ld16(taddr + ((uint32_t)(32 * warp) << 16) + (uint32_t)c0, v);
+                umma::tmem_ld16(P.taddr + ((uint32_t)(32 * ew) << 16) + (uint32_t)(a * g.BN + c0), v);
                 umma::tmem_ld_wait();
                 if (!rin) continue;
 #pragma unroll
-                for (int q = 0; q < 16; ++q) {
-                    const int n = n0 + c0 + q;
-                    if (n < g.N) atomicAdd(g.dw + (long long)n * g.kpad + r, __uint_as_float(v[q]));
+                for (int qq = 0; qq < 16; ++qq) {
+                    const int n = nt * g.BN + c0 + qq;
+                    if (n < g.N) atomicAdd(g.dw + (long long)n * g.kpad + r, __uint_as_float(v[qq]));
                 }
             }
+            umma::tc_fence_before_sync();
+            __syncwarp();
+            if (lane == 0) asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(umma::smem_u32(&P.acce[a])) : "memory");
         }
-    } else if (lane == 0) {
-        const uint32_t idesc = umma::idesc_bf16(kBM, g.BN, 1, 1);
-        for (int i = 0; i < nk; ++i) {
-            const int s = i % kStages;
-            if (!umma::mbar_wait(&full[s], (i / kStages) & 1, g.err, kWaitNs)) break;
-            umma::fence_proxy_async_smem();
-            umma::tc_fence_after_sync();
-            const uint32_t sa = sbase + s * stage_bytes, sb = sa + a_bytes;
-#pragma unroll
-            for (int kk = 0; kk < kBK / 16; ++kk) {
-                const uint64_t ad = umma::smem_desc(sa + 256u * kk, 128u, 1024u);
-                const uint64_t bd = umma::smem_desc(sb + 256u * kk, 128u, 1024u);
-                umma::mma_bf16(taddr, ad, bd, idesc, (i | kk) != 0);
-            }
-            umma::mma_commit(&empty[s]);
-        }
-        umma::mma_commit(&accf);
     }
     umma::cp_async_wait_all();
     umma::tc_fence_before_sync();
     __syncthreads();
-    if (warp == 4) {
+    if (warp == kMmaWarp) {
         umma::tc_fence_after_sync();
-        umma::tmem_dealloc(taddr, ncols);
+        umma::tmem_dealloc(P.taddr, ncols);
     }
 }
 
@@ -650,6 +860,13 @@ namespace {
 
 cudaStream_t cs(agd_stream_t s) { return reinterpret_cast<cudaStream_t>(s); }
 
+int num_sms() {
+    int dev = 0, nsm = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    return nsm;
+}
+
 int launched(const char *what) {
     const cudaError_t e = cudaGetLastError();
     return e == cudaSuccess ? AGD_STATUS_OK : set_cuda_error(what, e);
@@ -697,8 +914,8 @@ int agd_conv3x3_forward(const agd_conv *c, const void *w, const float *bias, int
     g.K8 = 9 * g.cin8;
     g.kchunks = (g.K8 + 7) / 8;
     g.N = c->cout;
-    int ntiles = 1;
-    g.BN = tile_n(g.N, &ntiles);
+    GemmLaunch gl{};
+    g.BN = tile_n(g.N, &gl.ntiles);
     g.wmat = static_cast<const bf16 *>(w);
     g.kpad = kpad_of(9 * cin);
     g.bias = bias;
@@ -707,11 +924,24 @@ int agd_conv3x3_forward(const agd_conv *c, const void *w, const float *bias, int
     g.out_f = out_f32;
     g.M = (long long)c->n * c->H * c->W;
     g.err = err;
-    const int smem = kStages * (kBM * kBK * 2 + g.BN * kBK * 2);
+    g.wshift = (c->W & (c->W - 1)) == 0 ? __builtin_ctz((unsigned)c->W) : -1;
+    const long long mtiles = (g.M + kBM - 1) / kBM;
+    if (mtiles * gl.ntiles > 0x7fffffffLL) return set_error(AGD_STATUS_INVALID, "conv3x3: too many pixels");
+    gl.mtiles = (int)mtiles;
+    const int a_bytes = kBM * kBK * 2, bchunk = g.BN * kBK * 2;
+    const bool two = g.BN <= 128;  // two CTAs per SM: 2 x 2 x BN tensor memory columns
+    const int budget = two ? kSmemBudget2 : kSmemBudget;
+    gl.stationary = gl.ntiles == 1 && g.kchunks * bchunk <= budget / 2;
+    const int stat = gl.stationary ? g.kchunks * bchunk : 0;
+    const int stage = a_bytes + (gl.stationary ? 0 : bchunk);
+    gl.stages = std::min(kMaxStages, (budget - stat) / stage);
+    if (gl.stages < 2) return set_error(AGD_STATUS_UNSUPPORTED, "conv3x3: operands do not fit in shared memory");
+    // a CTA alone on its SM asks for more than half of the shared memory
+    const int smem = two ? gl.stages * stage + stat : std::max(gl.stages * stage + stat, 120 * 1024);
     cudaError_t e = cudaFuncSetAttribute(conv_gemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     if (e != cudaSuccess) return set_cuda_error("conv3x3 shared memory", e);
-    const dim3 grid((unsigned)((g.M + kBM - 1) / kBM), (unsigned)ntiles);
-    conv_gemm_kernel<<<grid, kThreads, smem, cs(stream)>>>(g);
+    const int grid = (int)std::min<long long>(mtiles * gl.ntiles, (two ? 2 : 1) * num_sms());
+    conv_gemm_kernel<<<grid, kPThreads, smem, cs(stream)>>>(g, gl);
     return launched("conv3x3 forward");
 }
 
@@ -728,26 +958,28 @@ int agd_conv3x3_weight_grad(const agd_conv *c, const void *dz, float *dw, unsign
     g.K8 = 9 * g.cin8;
     g.dz = static_cast<const bf16 *>(dz);
     g.N = c->cout;
-    int ntiles = 1;
-    g.BN = tile_n(g.N, &ntiles);
+    g.BN = tile_n(g.N, &g.ntiles);
     g.dw = dw;
     g.kpad = kpad_of(9 * cin);
     g.M = (long long)c->n * c->H * c->W;
     g.err = err;
+    g.wshift = (c->W & (c->W - 1)) == 0 ? __builtin_ctz((unsigned)c->W) : -1;
     const long long nchunks = (g.M + kBK - 1) / kBK;
     if (nchunks > 0x7fffffffLL) return set_error(AGD_STATUS_INVALID, "conv3x3 weight grad: too many pixels");
     g.nchunks = (int)nchunks;
-    const int mtiles = (g.K8 * 8 + kBM - 1) / kBM;
-    int dev = 0, nsm = 148;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-    int splits = std::max(1, std::min(g.nchunks, 4 * nsm / std::max(1, mtiles * ntiles)));
+    g.mtiles = (g.K8 * 8 + kBM - 1) / kBM;
+    const int nsm = num_sms();
+    int splits = std::max(1, std::min(g.nchunks, (8 * nsm + g.mtiles * g.ntiles - 1) / (g.mtiles * g.ntiles)));
     g.chunks_per_split = (g.nchunks + splits - 1) / splits;
-    splits = (g.nchunks + g.chunks_per_split - 1) / g.chunks_per_split;
-    const int smem = kStages * (kBM * kBK * 2 + g.BN * kBK * 2);
+    g.splits = (g.nchunks + g.chunks_per_split - 1) / g.chunks_per_split;
+    const int stage = kBM * kBK * 2 + g.BN * kBK * 2;
+    const bool two = g.BN <= 128;
+    g.stages = std::min(kMaxStages, (two ? kSmemBudget2 : kSmemBudget) / stage);
+    const int smem = two ? g.stages * stage : std::max(g.stages * stage, 120 * 1024);
     cudaError_t e = cudaFuncSetAttribute(conv_wgrad_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     if (e != cudaSuccess) return set_cuda_error("conv3x3 weight grad shared memory", e);
-    conv_wgrad_kernel<<<dim3(mtiles, ntiles, splits), kThreads, smem, cs(stream)>>>(g);
+    const int grid = std::min(g.mtiles * g.ntiles * g.splits, (two ? 2 : 1) * nsm);
+    conv_wgrad_kernel<<<grid, kPThreads, smem, cs(stream)>>>(g);
     return launched("conv3x3 weight grad");
 }
 

@@ -302,6 +302,66 @@ def run_other_path(args):
                                    "frac": nbytes / t / 1e9 / hbm, "peak_kind": peak_kind}}), flush=True)
 
 
+
+
+def unet_flops(nb=128):
+    """Forward FLOPs of the U-Net on one nb x nb block grid (the 3x3 convolutions)."""
+    from adaptivegriddiscretizations_b200.WarmStart.unet import IN_CHANNELS, LEVELS
+    c0, c1, c2, c3 = LEVELS
+    convs = [(0, IN_CHANNELS, c0), (0, c0, c0), (1, c0, c1), (1, c1, c1), (2, c1, c2), (2, c2, c2), (3, c2, c3),
+             (3, c3, c3), (2, c3 + c2, c2), (2, c2, c2), (1, c2 + c1, c1), (1, c1, c1), (0, c1 + c0, c0), (0, c0, c0)]
+    return sum(2 * (nb >> lv) ** 2 * 9 * ci * co for lv, ci, co in convs)
+
+
+def run_warm_start(args, peaks_tf):
+    """The learned warm start on the benchmark's configuration: 20k solver-made
+    training solutions, GPU training of the U-Net by the tensor-core kernels,
+    then cold and warm batched solves of 1k held-out instances side by side
+    (device time; the warm figure includes the network's prediction).  Returns
+    the JSON object of the bench line."""
+    import torch
+    from adaptivegriddiscretizations_b200.WarmStart.warmstart import WarmStart, riemann2_fields
+    n, B = args.n, args.batch
+    ws = WarmStart(n=n, batch=B)
+    gen = torch.Generator(device="cuda").manual_seed(1)
+    t0 = time.perf_counter()
+    X, T = ws.generate(args.warm_train, gen)
+    torch.cuda.synchronize()
+    t_gen = time.perf_counter() - t0
+    Xv, Tv = ws.generate(512, torch.Generator(device="cuda").manual_seed(99))
+    fin = torch.isfinite(Tv)
+    const_loss = float(((Tv - Tv[fin].mean()) ** 2)[fin].mean())
+    hist = ws.train(X, T, args.warm_steps, batch=32, lr=2e-3, gen=torch.Generator(device="cuda").manual_seed(3))
+    val_loss = ws.eval_loss(Xv, Tv)
+    del X, T
+    # inference throughput of the network (forward of a batch, CUDA events)
+    m, sd = riemann2_fields(n, B, torch.Generator(device="cuda").manual_seed(7))
+    x0, _ = ws.features(m, sd)
+    for _ in range(3):
+        ws.net.forward(x0)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(5):
+        ws.net.forward(x0)
+    e1.record()
+    torch.cuda.synchronize()
+    t_fwd = e0.elapsed_time(e1) / 5e3
+    flops = unet_flops(n // 4) * B
+    best = ws.tune(m, sd)
+    res = ws.evaluate(args.warm_eval, torch.Generator(device="cuda").manual_seed(11))
+    res.update({
+        "training": {"solutions": args.warm_train, "generate_s": t_gen, "steps": args.warm_steps, "batch": 32,
+                     "train_s": ws.train_seconds, "ms_per_step": 1e3 * ws.train_seconds / args.warm_steps,
+                     "final_train_loss": hist[-1][1] if hist else None},
+        "validation_mse_log_ratio": val_loss, "constant_predictor_mse": const_loss,
+        "release_epochs_tuned": {"epochs": best[0], "batch_solve_s": best[1]},
+        "unet_forward": {"batch": B, "ms": 1e3 * t_fwd, "tflops": flops / t_fwd / 1e12,
+                         "frac_of_bf16_peak": flops / t_fwd / 1e12 / peaks_tf, "peak_tflops": peaks_tf},
+        "network": "U-Net 4 levels 32/64/128/256 channels, bf16, fp32 accumulation, 128x128 blocks of 4x4 points",
+    })
+    return res
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -321,6 +381,10 @@ def main():
                     help="solve: the benchmark (default); geodesic / reverse: the other kernels of the path")
     ap.add_argument("--path-size", type=int, default=0,
                     help="grid side for --path (0: 1024 for geodesic, 200 for reverse; smaller for profiler captures)")
+    ap.add_argument("--warm-train", type=int, default=20000, help="training solutions of the learned warm start")
+    ap.add_argument("--warm-steps", type=int, default=2000, help="training steps of the learned warm start")
+    ap.add_argument("--warm-eval", type=int, default=1024, help="held-out instances of the warm/cold comparison")
+    ap.add_argument("--no-warm", action="store_true", help="skip the learned warm start leg")
     ap.add_argument("--warm-oracle", type=float, default=0.0,
                     help="experiment: warm start every solve from (1+eps) x its cold solution, all tiles active")
     args = ap.parse_args()
@@ -495,6 +559,15 @@ def main():
                       "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
                       "api": "Eikonal.SubmitBatch of dictIn inputs (two streams)"}
 
+    warm = None
+    if rank == 0 and not args.no_warm:
+        try:
+            with open(os.path.join(REPO, "MEASURED_PEAKS.json")) as f:
+                tf_peak = float(json.load(f)["bf16_tflops"])
+        except Exception:  # noqa: BLE001
+            tf_peak = 1590.0
+        warm = run_warm_start(args, tf_peak)
+
     cpu = schedule = None
     if rank == 0 and not args.no_cpu_baseline:
         cases = cpu_cases(n, 4, 1234)
@@ -537,7 +610,7 @@ def main():
                          "frac": achieved / hbm, "traffic": traffic, "peak_kind": peak_kind,
                          "kernel": "sched_worker<EikonalVisitor>", "kernel_ms": float(kern.mean() * 1000),
                          "bytes_per_update": BYTES_PER_UPDATE["Riemann2"]},
-            "cpu_baseline": cpu, "schedule_vs_reference": schedule, "e2e": e2e, "e2e_dictin": e2e_dictin, "gpu_launches": 5 * args.steps,
+            "cpu_baseline": cpu, "schedule_vs_reference": schedule, "warm_start": warm, "e2e": e2e, "e2e_dictin": e2e_dictin, "gpu_launches": 5 * args.steps,
             "clocks": clk.summary(),
         }
         print(json.dumps(line), flush=True)
