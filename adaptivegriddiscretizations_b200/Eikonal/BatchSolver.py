@@ -53,7 +53,7 @@ class _Buffers:
 
     def staging(self, name, shape, dtype=torch.float32):
         """Device staging tensor for an input, reused while its shape holds."""
-        t = getattr(self, name)
+        t = getattr(self, name, None)
         if t is None or tuple(t.shape) != tuple(shape) or t.dtype != dtype:
             with torch.cuda.stream(self.stream):
                 t = torch.empty(shape, dtype=dtype, device="cuda")

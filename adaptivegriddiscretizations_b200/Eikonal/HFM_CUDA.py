@@ -67,7 +67,15 @@ def SubmitBatch(hfmIns, launch=None):
 
     The host can meanwhile prepare the next batch: submitted on a second
     stream, its uploads and preparation kernels queue while this solve runs.
-    `BatchJob.result()` gives what RunBatch returns."""
+    `BatchJob.result()` gives what RunBatch returns.
+
+    A batch of dictIn that differ only in their data (same model, grid, traits
+    and options; metric or cost arrays of one shape, the same number of seeds)
+    is prepared by one batched kernel (agd_prep_batch, as Eikonal.BatchSolver
+    does) instead of instance by instance."""
+    fast = _submit_uniform(hfmIns, launch)
+    if fast is not None:
+        return fast
     itfs = [Interface(h) for h in hfmIns]
     for it in itfs:
         it.SetKernelTraits()
@@ -76,6 +84,134 @@ def SubmitBatch(hfmIns, launch=None):
     plan = BatchPlan(itfs, launch=launch)
     plan.run()
     return BatchJob(plan)
+
+
+# Keys that the batched preparation takes (anything else: instance by instance).
+_UNIFORM_KEYS = {"model", "mode", "arrayOrdering", "verbosity", "dims", "gridScale", "gridScales", "origin",
+                 "metric", "cost", "seeds", "seedValues", "exportValues", "tol", "atol", "rtol", "traits",
+                 "nitermax_o", "fim_front_width", "raiseOnNonConvergence", "solver", "projective"}
+_UNIFORM_DATA = {"metric", "cost", "seeds", "seedValues"}
+_uniform_solvers = OrderedDict()  # configuration -> (BatchSolver, key bookkeeping of one instance)
+
+
+def _option(h, k):
+    """A comparable host form of an option of a dictIn: small arrays from the
+    host copy the dictIn keeps (no device read), None for large device arrays."""
+    v = h[k]
+    if isinstance(v, (np.ndarray, torch.Tensor)):
+        a = h.host(k) if not (isinstance(v, torch.Tensor) and v.is_cuda and v.numel() > 64) else None
+        return None if a is None else ("array", tuple(np.asarray(a).shape), tuple(np.asarray(a).reshape(-1).tolist()))
+    if isinstance(v, dict):
+        return ("dict", repr(sorted((kk, repr(vv)) for kk, vv in v.items())))
+    if isinstance(v, (list, tuple)):
+        return ("seq", repr(list(v)))
+    return ("value", repr(v))
+
+
+def _submit_uniform(hfmIns, launch):
+    """The batched preparation path of SubmitBatch, or None when the dictIn do
+    not qualify."""
+    from .BatchSolver import BatchSolver
+    B = len(hfmIns)
+    if B < 2:
+        return None
+    h0 = hfmIns[0]
+    model = h0.get("model")
+    if model not in ("Riemann2", "Riemann3", "Isotropic2", "Isotropic3"):
+        return None
+    keys0 = set(h0.keys())
+    data = "metric" if model.startswith("Riemann") else "cost"
+    if not keys0 <= _UNIFORM_KEYS or data not in keys0 or "seeds" not in keys0:
+        return None
+    opts = sorted(keys0 - _UNIFORM_DATA - {"verbosity"})
+    arrays = [k for k in ("metric", "cost", "seeds", "seedValues") if k in keys0]
+    for k in arrays:
+        if not isinstance(h0[k], (np.ndarray, torch.Tensor)):
+            return None
+    shapes = {k: tuple(h0[k].shape) for k in arrays}
+    opt0 = tuple(_option(h0, k) for k in opts)
+    if any(o is None for o in opt0):
+        return None
+    for h in hfmIns[1:]:
+        if set(h.keys()) != keys0 or tuple(_option(h, k) for k in opts) != opt0:
+            return None
+        for k in arrays:
+            if not isinstance(h[k], (np.ndarray, torch.Tensor)) or tuple(h[k].shape) != shapes[k]:
+                return None
+    cfg = (model, tuple(h0.shape), B, id(launch), tuple(zip(opts, opt0)), tuple(sorted(shapes.items())))
+    entry = _uniform_solvers.get(cfg)
+    if entry is None:
+        solver = BatchSolver(h0, B, launch=launch)
+        # the key bookkeeping of one instance, as RunGPU records it
+        itf = Interface(h0)
+        itf.SetKernelTraits()
+        itf.SetGeometry()
+        itf.SetArgs()
+        itf.PostProcess()
+        itf.SolveAD()
+        itf.GetGeodesics()
+        itf.FinalCheck()
+        if itf.extractValues or itf.retself or itf.flow_needed:
+            return None
+        keys = itf.hfmOut["keys"]
+        entry = (solver, keys, bool(h0.get("exportValues", False)))
+        _uniform_solvers[cfg] = entry
+        while len(_uniform_solvers) > 2:
+            _uniform_solvers.popitem(last=False)
+    else:
+        _uniform_solvers.move_to_end(cfg)
+    solver, keys, export = entry
+    user = torch.cuda.current_stream()
+    buf = solver._bufs[solver._next]
+    if buf.job is not None:
+        buf.job.event.synchronize()
+    inputs = {}
+    with torch.cuda.stream(buf.stream):
+        buf.stream.wait_stream(user)
+        for k in arrays:
+            dtype = torch.float32
+            dev = buf.staging("u_" + k, (B,) + shapes[k], dtype)
+            for i, h in enumerate(hfmIns):
+                x = h[k]
+                x = torch.from_numpy(np.asarray(x, np.float32)) if isinstance(x, np.ndarray) else x
+                dev[i].copy_(x, non_blocking=x.device.type == "cpu" and x.is_pinned() or x.is_cuda)
+            inputs[k] = dev
+    job = solver.submit(metric=inputs.get("metric"), cost=inputs.get("cost"), seeds=inputs["seeds"],
+                        seedValues=inputs.get("seedValues"))
+    return UniformBatchJob(job, keys, export, B)
+
+
+class UniformBatchJob:
+    """A batch of SubmitBatch prepared in one go; `result()` gives the list of
+    outputs (values, stats and key bookkeeping per instance)."""
+
+    def __init__(self, job, keys, export, n):
+        self.job, self.keys, self.export, self.n = job, keys, export, n
+        self.stream = job.stream
+        self._outs = None
+
+    def done(self):
+        return self.job.done()
+
+    def result(self):
+        if self._outs is not None:
+            return self._outs
+        values = self.job.result()
+        with torch.cuda.stream(self.stream):
+            values = values.clone() if self.export else None  # the solver's buffer is reused
+        outs = []
+        for i in range(self.n):
+            keys = {k: (list(v) if isinstance(v, list) else OrderedDict(v) if isinstance(v, dict) else v)
+                    for k, v in self.keys.items()}
+            stats = {"eikonal": {"niter_o": int(self.job.niter_o[i]), "time": None,
+                                 "nupdate_o_total": int(self.job.tile_visits[i])},
+                     "flow": {}, "geodesic": {}, "forwardAD": {}, "reverseAD": {}}
+            out = {"keys": keys, "stats": stats, "solverGPUTime": None}
+            if values is not None:
+                out["values"] = values[i]
+            outs.append(out)
+        self._outs = outs
+        return outs
 
 
 class BatchJob:
@@ -285,8 +421,15 @@ class Interface:
         """Traits (agd/Eikonal/HFM_CUDA/_Kernel.py:23-92)."""
         si, niter, front = DEFAULT_TRAITS[self.model]
         traits = {"shape_i": si, "niter_i": niter}
-        traits.update(self.GetValue("traits", default=dict(traits),
-                                    help="Optional trait parameters for the eikonal kernel."))
+        given = self.GetValue("traits", default=dict(traits),
+                              help="Optional trait parameters for the eikonal kernel "
+                                   "('auto': tile shape and niter_i chosen by timed trial solves, cached)")
+        if isinstance(given, str):
+            if given != "auto":
+                raise ValueError(f"traits must be a dict or 'auto', got {given!r}")
+            traits.update(self._autotune())
+        else:
+            traits.update(given)
         self.shape_i = tuple(int(s) for s in traits["shape_i"])
         self.niter_i = int(traits["niter_i"])
         if self.shape_i not in SUPPORTED_TILES[self.ndim]:
@@ -330,6 +473,35 @@ class Interface:
         self.raiseOnNonConvergence = self.GetValue("raiseOnNonConvergence", default=True,
                                                    help="Raise an exception if a solver fails to converge")
         self.size_i = int(np.prod(self.shape_i))
+
+    def _autotune(self):
+        """Traits of traits='auto': the cached choice for this model and grid size
+        on this device, else the fastest of the candidates of Autotune.py in
+        trial solves of this very problem (solve time by CUDA events)."""
+        from .Autotune import Autotuner, bucket_key, candidates
+        key = bucket_key(self.model, self.hfmIn.shape, 1, torch.cuda.get_device_name())
+
+        def run(tr):
+            h = self.hfmIn.copy()
+            h["traits"], h["verbosity"] = dict(tr), 0
+            for k in ("tips", "sensitivity", "costVariation", "seedValueVariation", "exportGeodesicFlow",
+                      "exportActiveNeighs"):
+                h.store.pop(k, None)
+            it = Interface(h)
+            try:
+                it.SetKernelTraits()
+                it.SetGeometry()
+                it.SetArgs()
+                it.Solve()
+            except (ValueError, _lib.AgdError):
+                return float("inf")
+            return it.stats["eikonal"]["time"]
+
+        choice, trials = Autotuner().choose(key, run, candidates(self.model))
+        self.stats["autotune"] = {"key": key, "traits": {k: list(v) if isinstance(v, tuple) else v
+                                                        for k, v in choice.items()},
+                                  "cached": trials is None}
+        return choice
 
     def SetGeometry(self):
         """Domain, metric and cost (agd/Eikonal/HFM_CUDA/_SetGeometry.py:16-282)."""

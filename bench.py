@@ -362,6 +362,42 @@ def run_warm_start(args, peaks_tf):
     return res
 
 
+def run_autotune(n, B, metrics, seeds):
+    """Traits autotuner on the benchmark's batch: every candidate tile shape and
+    local iteration count of Riemann2 (Eikonal/Autotune.py) timed on batched
+    solves of the same instances (BatchSolver, device-resident inputs, CUDA
+    events, best of two); the choice is cached like traits='auto' does."""
+    import torch
+    from adaptivegriddiscretizations_b200 import Eikonal
+    from adaptivegriddiscretizations_b200.Eikonal.Autotune import Autotuner, bucket_key, candidates
+    m = torch.from_numpy(np.stack(metrics)).cuda()
+    sd = torch.from_numpy(np.stack(seeds)).cuda()
+
+    def run(tr):
+        tmpl = dictins(metrics[:1], seeds[:1], n, to_device=False, traits={"traits": dict(tr)})[0]
+        solver = Eikonal.BatchSolver(tmpl, B, nbuffers=1)
+        solver.submit(metric=m, seeds=sd).result()
+        st = solver._bufs[0].stream
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        solver.submit(metric=m, seeds=sd)
+        e1.record(st)
+        e1.synchronize()
+        del solver
+        return e0.elapsed_time(e1) / 1e3
+
+    key = bucket_key("Riemann2", (n, n), B, torch.cuda.get_device_name())
+    tuner = Autotuner()
+    choice, trials = tuner.tune(key, run, candidates("Riemann2"), repeats=2)
+    t = {(tuple(c["shape_i"]), c["niter_i"]): tt for tt, c in trials}
+    t_def = t[((8, 8), 8)]
+    t_best = t[(tuple(choice["shape_i"]), choice["niter_i"])]
+    return {"chosen": {"shape_i": list(choice["shape_i"]), "niter_i": choice["niter_i"]},
+            "reference_default": {"shape_i": [8, 8], "niter_i": 8}, "gain_over_default": t_def / t_best,
+            "solves_per_s_tuned": B / t_best, "solves_per_s_default": B / t_def,
+            "trials_ms": [[list(c["shape_i"]), c["niter_i"], 1e3 * tt] for tt, c in trials]}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -385,6 +421,7 @@ def main():
     ap.add_argument("--warm-steps", type=int, default=2000, help="training steps of the learned warm start")
     ap.add_argument("--warm-eval", type=int, default=1024, help="held-out instances of the warm/cold comparison")
     ap.add_argument("--no-warm", action="store_true", help="skip the learned warm start leg")
+    ap.add_argument("--no-autotune", action="store_true", help="skip the traits autotuner leg")
     ap.add_argument("--warm-oracle", type=float, default=0.0,
                     help="experiment: warm start every solve from (1+eps) x its cold solution, all tiles active")
     args = ap.parse_args()
@@ -559,6 +596,7 @@ def main():
                       "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
                       "api": "Eikonal.SubmitBatch of dictIn inputs (two streams)"}
 
+    tuned = run_autotune(n, B, metrics, seeds) if rank == 0 and not args.no_autotune else None
     warm = None
     if rank == 0 and not args.no_warm:
         try:
@@ -610,7 +648,7 @@ def main():
                          "frac": achieved / hbm, "traffic": traffic, "peak_kind": peak_kind,
                          "kernel": "sched_worker<EikonalVisitor>", "kernel_ms": float(kern.mean() * 1000),
                          "bytes_per_update": BYTES_PER_UPDATE["Riemann2"]},
-            "cpu_baseline": cpu, "schedule_vs_reference": schedule, "warm_start": warm, "e2e": e2e, "e2e_dictin": e2e_dictin, "gpu_launches": 5 * args.steps,
+            "cpu_baseline": cpu, "schedule_vs_reference": schedule, "warm_start": warm, "autotune": tuned, "e2e": e2e, "e2e_dictin": e2e_dictin, "gpu_launches": 5 * args.steps,
             "clocks": clk.summary(),
         }
         print(json.dumps(line), flush=True)

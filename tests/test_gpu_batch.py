@@ -70,3 +70,59 @@ def test_submit_batch_two_streams():
         for v, r in zip(vals, ref):
             assert _rel(v, r) < REL
         assert job.result() is outs
+
+
+def _riemann2_cases(n, count, seed):
+    import bench
+    metrics, seeds = bench.make_fields(n, count, seed, sigma=4.0)
+    return [dict(model="Riemann2", dims=np.array([n, n], np.float32), gridScales=np.full(2, 1.0 / n, np.float32),
+                 origin=np.zeros(2, np.float32), metric=m, seeds=s) for m, s in zip(metrics, seeds)]
+
+
+@pytest.mark.parametrize("pinned", [False, True])
+def test_submit_batch_uniform_path(pinned):
+    """dictIn that differ only in their data go through the batched preparation
+    (one agd_prep_batch launch): values, iteration counts and the key
+    bookkeeping per instance are those of RunGPU on each dictIn."""
+    import os
+    import sys
+    sys.path.insert(0, os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+    from adaptivegriddiscretizations_b200 import Eikonal
+    from adaptivegriddiscretizations_b200.Eikonal.HFM_CUDA import UniformBatchJob
+    from parity import assert_near_discrete
+    cases = _riemann2_cases(96, 6, 17)
+    for rep in range(2):  # the second batch reuses the cached solver
+        job = Eikonal.SubmitBatch([_dictin(c, pinned=pinned) for c in cases])
+        assert isinstance(job, UniformBatchJob)
+        outs = job.result()
+        for c, o in zip(cases, outs):
+            ref = _dictin(c).Run()
+            v = o["values"].cpu().numpy()
+            assert_near_discrete(v, c)
+            assert _rel(v, ref["values"].cpu().numpy()) < 1e-4
+            assert o["stats"]["eikonal"]["niter_o"] > 0
+            for k in ("used", "default", "help"):
+                assert list(o["keys"][k]) == list(ref["keys"][k]), k
+    # a batch whose options differ goes instance by instance
+    mixed = [_dictin(c) for c in cases[:2]]
+    mixed[1]["nitermax_o"] = 500
+    assert not isinstance(Eikonal.SubmitBatch(mixed), UniformBatchJob)
+
+
+def test_traits_auto(tmp_path, monkeypatch):
+    """traits='auto': the autotuner's trial solves pick a tile shape and local
+    iteration count (cached for the next call); the values meet the parity
+    criteria like those of any traits."""
+    import os
+    import sys
+    sys.path.insert(0, os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+    from parity import assert_near_discrete
+    monkeypatch.setenv("AGD_AUTOTUNE_CACHE", str(tmp_path / "autotune.json"))
+    case = _riemann2_cases(128, 1, 23)[0]
+    h = _dictin(dict(case, traits="auto"))
+    out = h.Run()
+    at = out["stats"]["autotune"]
+    assert not at["cached"] and tuple(at["traits"]["shape_i"]) in {(8, 8), (16, 16)}
+    assert_near_discrete(out["values"].cpu().numpy(), case)
+    out2 = _dictin(dict(case, traits="auto")).Run()
+    assert out2["stats"]["autotune"]["cached"] and out2["stats"]["autotune"]["traits"] == at["traits"]

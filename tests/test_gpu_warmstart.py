@@ -1,0 +1,65 @@
+"""The learned warm start end to end on the GPU (Riemann2 512^2, the
+configuration of the benchmark): solver-generated training data, training of
+the U-Net by the tensor-core kernels, and the warm (learned schedule) against
+the cold solves of held-out instances, the cold solve being the judge.
+
+Checked: the trained network beats the constant predictor of the log-ratio
+(it learned something from the metric and the seeds); every warm result meets
+the parity criteria against the scheme's discrete solution on two instances
+and agrees with the cold result within the judge's tolerance elsewhere; the
+release epochs are the ones of a numpy restatement (bit-exact).  The gain or
+loss in solves/s over the cold solve is measured and reported, not asserted:
+the scheme revisits tiles mostly to converge to its tight stopping tolerance,
+which no activation schedule removes."""
+import os
+
+import numpy as np
+import pytest
+import torch
+
+from parity import assert_near_discrete, discrete_solution
+
+pytestmark = pytest.mark.gpu
+
+
+def _release_numpy(pred, epochs, lag):
+    n, Hb, Wb = pred.shape
+    tmax = np.where(np.isfinite(pred), pred, 0).reshape(n, -1).max(1)
+    t = pred.reshape(n, Hb // 2, 2, Wb // 2, 2).min((2, 4)).reshape(n, -1)
+    e = 1.0 + np.floor(np.float32(epochs) * np.maximum(t, 0) / tmax[:, None]) - lag
+    return np.clip(e, 1, 16000).astype(np.int16)
+
+
+def test_release_epochs_match_numpy():
+    from adaptivegriddiscretizations_b200.WarmStart.warmstart import WarmStart
+    ws = WarmStart(n=64, batch=3)
+    rng = np.random.default_rng(2)
+    pred = rng.uniform(0.0, 2.0, (3, 16, 16)).astype(np.float32)
+    rel = ws.release(torch.as_tensor(pred, device="cuda"), epochs=37.0, lag=1).cpu().numpy()
+    np.testing.assert_array_equal(rel, _release_numpy(pred, 37.0, 1))
+
+
+def test_learned_warm_start_riemann2_512():
+    from adaptivegriddiscretizations_b200.WarmStart.warmstart import WarmStart, riemann2_fields
+    ws = WarmStart(n=512, batch=64)
+    X, T = ws.generate(2048, torch.Generator(device="cuda").manual_seed(1))
+    Xv, Tv = ws.generate(256, torch.Generator(device="cuda").manual_seed(99))
+    fin = torch.isfinite(Tv)
+    const = float(((Tv - Tv[fin].mean()) ** 2)[fin].mean())
+    ws.train(X, T, 600, batch=32, lr=2e-3, gen=torch.Generator(device="cuda").manual_seed(3))
+    val = ws.eval_loss(Xv, Tv)
+    assert val < 0.8 * const, (val, const)
+    m, s = riemann2_fields(512, 64, torch.Generator(device="cuda").manual_seed(7))
+    ws.tune(m, s)
+    res = ws.evaluate(128, torch.Generator(device="cuda").manual_seed(11))
+    print("learned warm start:", {k: v for k, v in res.items()})
+    assert res["fallbacks"] <= 4, res
+    # parity of warm results against the discrete solution, two held-out instances
+    m, s = riemann2_fields(512, 64, torch.Generator(device="cuda").manual_seed(12))
+    warm, _, _ = ws.warm_solve(m, s)
+    warm = warm.cpu().numpy()
+    mh, sh = m.cpu().numpy(), s.cpu().numpy()
+    for i in (0, 1):
+        case = dict(model="Riemann2", dims=np.array([512, 512], np.float32), gridScales=np.full(2, 1 / 512, np.float32),
+                    origin=np.zeros(2, np.float32), metric=mh[i], seeds=sh[i])
+        assert_near_discrete(warm[i], case, discrete_solution(case, nthreads=os.cpu_count()))
