@@ -362,6 +362,57 @@ def run_warm_start(args, peaks_tf):
     return res
 
 
+def run_unet(args):
+    """The learned warm start's network alone (`--path unet`): forward passes of
+    a batch of 128 Riemann2 512^2 problems (128 x 128 blocks, 8 feature
+    channels) with random weights, every 3x3 convolution timed by CUDA events:
+    FLOPs = 2 x pixels x 9 cin x cout, against the measured dense bf16 peak."""
+    import torch
+    from adaptivegriddiscretizations_b200.WarmStart.unet import UNet
+    torch.cuda.set_device(0)
+    nb, B = (args.path_size or 512) // 4, args.batch
+    net = UNet(seed=0)
+    x0 = torch.randn((B, nb, nb, 8), device="cuda").to(torch.bfloat16)
+    for _ in range(max(1, args.warmup)):
+        net.forward(x0)
+    torch.cuda.synchronize()
+    orig, layers = net._conv, []
+
+    def timed(layer, n, H, W, srcs, out_bf=None, out_f=None, relu=True, bias=True, weights=None):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        orig(layer, n, H, W, srcs, out_bf, out_f, relu, bias, weights)
+        e1.record()
+        cin = sum(sr[1] for sr in srcs)
+        layers.append((H, cin, layer.cout, e0, e1, 2 * n * H * W * 9 * cin * layer.cout))
+
+    net._conv = timed
+    rows = []
+    for _ in range(args.steps):
+        layers.clear()
+        net.forward(x0)
+        torch.cuda.synchronize()
+        rows.append([(H, ci, co, e0.elapsed_time(e1) / 1e3, fl) for H, ci, co, e0, e1, fl in layers])
+    net._conv = orig
+    try:
+        with open(os.path.join(REPO, "MEASURED_PEAKS.json")) as f:
+            peak = float(json.load(f)["bf16_tflops"])
+    except Exception:  # noqa: BLE001
+        peak = 1590.0
+    per = []
+    for k in range(len(rows[0])):
+        H, ci, co, _, fl = rows[0][k]
+        t = float(np.median([r[k][3] for r in rows]))
+        per.append({"H": H, "cin": ci, "cout": co, "us": 1e6 * t, "tflops": fl / t / 1e12})
+    tot_t = sum(p["us"] for p in per) / 1e6
+    tot_f = sum(r[4] for r in rows[0])
+    print(json.dumps({"metric": "U-Net forward (3x3 convolutions on tcgen05)", "value": tot_f / tot_t / 1e12,
+                      "unit": "TFLOP/s", "batch": B, "blocks": nb, "ms_per_forward_convs": 1e3 * tot_t,
+                      "roofline": {"bound": "tensor", "achieved": tot_f / tot_t / 1e12, "peak": peak,
+                                   "unit": "TFLOP/s", "frac": tot_f / tot_t / 1e12 / peak},
+                      "layers": per}), flush=True)
+
+
 def run_autotune(n, B, metrics, seeds):
     """Traits autotuner on the benchmark's batch: every candidate tile shape and
     local iteration count of Riemann2 (Eikonal/Autotune.py) timed on batched
@@ -413,8 +464,9 @@ def main():
     ap.add_argument("--niter-i", type=int, default=0, help="local iterations per tile visit (0: the default, 8)")
     ap.add_argument("--front", type=int, default=0, help="FIM front width (0: the default, 4)")
     ap.add_argument("--tile", type=int, default=8, help="tile side (8: the default, or 16)")
-    ap.add_argument("--path", default="solve", choices=["solve", "geodesic", "reverse"],
-                    help="solve: the benchmark (default); geodesic / reverse: the other kernels of the path")
+    ap.add_argument("--path", default="solve", choices=["solve", "geodesic", "reverse", "unet"],
+                    help="solve: the benchmark (default); geodesic / reverse: the other kernels of the path; "
+                         "unet: the learned warm start's network")
     ap.add_argument("--path-size", type=int, default=0,
                     help="grid side for --path (0: 1024 for geodesic, 200 for reverse; smaller for profiler captures)")
     ap.add_argument("--warm-train", type=int, default=20000, help="training solutions of the learned warm start")
@@ -430,6 +482,9 @@ def main():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     if args.impl == "reference":
         run_reference(args, rank)
+        return
+    if args.path == "unet":
+        run_unet(args)
         return
     if args.path != "solve":
         run_other_path(args)
