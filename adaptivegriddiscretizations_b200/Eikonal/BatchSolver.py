@@ -143,6 +143,8 @@ class BatchSolver:
         bottom, _ = template.corners
         self.start = (bottom + 0.5 * self.h).astype(np.float32)
         self.niter_i, self.fim_front_width, self.nitermax_o = itf.niter_i, itf.fim_front_width, itf.nitermax_o
+        self.flags = {"adaptive_gauss_siedel_iteration": _lib.AGD_FLAG_SOLVER_AGSI,
+                      "global_iteration": _lib.AGD_FLAG_SOLVER_GLOBAL}.get(itf.solver, 0)
         self.raiseOnNonConvergence = itf.raiseOnNonConvergence
         self.rtol = itf.rtol
         # a tolerance given by the user holds for every instance; otherwise the
@@ -192,6 +194,7 @@ class BatchSolver:
                 inst.shape_i[k] = self.c_shape_i[k]
                 inst.iso_weights[k] = float(self.h[k]) ** -2 if k < self.ndim else 0.0
             inst.niter_i, inst.fim_front_width, inst.nitermax_o = self.niter_i, self.fim_front_width, self.nitermax_o
+            inst.flags = self.flags
             inst.atol, inst.rtol = float(atol[i]), float(self.rtol)
             inst.values = buf.values[i].data_ptr()
             inst.geom = buf.geom[i].data_ptr() if self.riemann else None

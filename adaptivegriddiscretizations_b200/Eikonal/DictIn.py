@@ -28,6 +28,16 @@ _modes = ("gpu", "gpu_transfer")
 _SHADOW_MAX = 4096
 
 
+class _Deferred:
+    """A small host-side array of a 'gpu' mode dictIn, copied to the device when
+    the key is first read (so that building a dictIn makes no device copy)."""
+
+    __slots__ = ("host",)
+
+    def __init__(self, host):
+        self.host = host
+
+
 def _is_array(x):
     return isinstance(x, (np.ndarray, torch.Tensor))
 
@@ -160,8 +170,13 @@ class dictIn(MutableMapping):
         if key in _singleIn:
             key, value = _singleIn[key], [value]
         if key in _array_float_fields:
-            host = _host_copy(value)
-            value = self.array_float_caster(value)
+            host = value.host if isinstance(value, _Deferred) else _host_copy(value)
+            if isinstance(value, _Deferred):
+                pass  # a copied dictIn: the host array stays deferred
+            elif host is not None and self.mode == "gpu" and not (isinstance(value, torch.Tensor) and value.is_cuda):
+                value = _Deferred(host)  # moved to the device when first read
+            else:
+                value = self.array_float_caster(value)
             if host is not None:
                 self._shadow[key] = (value, host)
             else:
@@ -172,11 +187,23 @@ class dictIn(MutableMapping):
 
     def __getitem__(self, key):
         if key in _singleIn:
-            values = self.store[_singleIn[key]]
+            values = self[_singleIn[key]]
             if len(values) != 1:
                 raise ValueError(f"Found {len(values)} values for key {key}")
             return values[0]
-        return self.store[key]
+        value = self.store[key]
+        if isinstance(value, _Deferred):
+            dev = self.array_float_caster(value.host)
+            self.store[key] = dev
+            self._shadow[key] = (dev, value.host)
+            return dev
+        return value
+
+    def raw(self, key):
+        """The stored value without moving a deferred host array to the device:
+        a device tensor, or a float32 numpy array for small host-side arrays."""
+        value = self.store[key]
+        return value.host if isinstance(value, _Deferred) else value
 
     def __delitem__(self, key):
         key = _singleIn.get(key, key)

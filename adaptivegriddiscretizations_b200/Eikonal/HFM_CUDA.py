@@ -97,10 +97,13 @@ _uniform_solvers = OrderedDict()  # configuration -> (BatchSolver, key bookkeepi
 def _option(h, k):
     """A comparable host form of an option of a dictIn: small arrays from the
     host copy the dictIn keeps (no device read), None for large device arrays."""
-    v = h[k]
+    v = h.raw(k)
     if isinstance(v, (np.ndarray, torch.Tensor)):
         a = h.host(k) if not (isinstance(v, torch.Tensor) and v.is_cuda and v.numel() > 64) else None
-        return None if a is None else ("array", tuple(np.asarray(a).shape), tuple(np.asarray(a).reshape(-1).tolist()))
+        if a is None:
+            return None
+        a = np.ascontiguousarray(a)
+        return ("array", a.shape, a.dtype.str, a.tobytes())
     if isinstance(v, dict):
         return ("dict", repr(sorted((kk, repr(vv)) for kk, vv in v.items())))
     if isinstance(v, (list, tuple)):
@@ -126,9 +129,9 @@ def _submit_uniform(hfmIns, launch):
     opts = sorted(keys0 - _UNIFORM_DATA - {"verbosity"})
     arrays = [k for k in ("metric", "cost", "seeds", "seedValues") if k in keys0]
     for k in arrays:
-        if not isinstance(h0[k], (np.ndarray, torch.Tensor)):
+        if not isinstance(h0.raw(k), (np.ndarray, torch.Tensor)):
             return None
-    shapes = {k: tuple(h0[k].shape) for k in arrays}
+    shapes = {k: tuple(h0.raw(k).shape) for k in arrays}
     opt0 = tuple(_option(h0, k) for k in opts)
     if any(o is None for o in opt0):
         return None
@@ -136,7 +139,8 @@ def _submit_uniform(hfmIns, launch):
         if set(h.keys()) != keys0 or tuple(_option(h, k) for k in opts) != opt0:
             return None
         for k in arrays:
-            if not isinstance(h[k], (np.ndarray, torch.Tensor)) or tuple(h[k].shape) != shapes[k]:
+            x = h.raw(k)
+            if not isinstance(x, (np.ndarray, torch.Tensor)) or tuple(x.shape) != shapes[k]:
                 return None
     cfg = (model, tuple(h0.shape), B, id(launch), tuple(zip(opts, opt0)), tuple(sorted(shapes.items())))
     entry = _uniform_solvers.get(cfg)
@@ -169,12 +173,17 @@ def _submit_uniform(hfmIns, launch):
     with torch.cuda.stream(buf.stream):
         buf.stream.wait_stream(user)
         for k in arrays:
-            dtype = torch.float32
-            dev = buf.staging("u_" + k, (B,) + shapes[k], dtype)
-            for i, h in enumerate(hfmIns):
-                x = h[k]
-                x = torch.from_numpy(np.asarray(x, np.float32)) if isinstance(x, np.ndarray) else x
-                dev[i].copy_(x, non_blocking=x.device.type == "cpu" and x.is_pinned() or x.is_cuda)
+            dev = buf.staging("u_" + k, (B,) + shapes[k], torch.float32)
+            xs = [h.raw(k) for h in hfmIns]
+            if all(isinstance(x, torch.Tensor) and x.is_cuda and x.dtype == torch.float32 for x in xs):
+                torch.stack(xs, out=dev)  # one gather on the device
+            elif all(isinstance(x, np.ndarray) for x in xs) and sum(x.size for x in xs) <= 1 << 20:
+                # small host arrays (seeds, seed values): one page-locked upload
+                dev.copy_(torch.from_numpy(np.stack(xs).astype(np.float32, copy=False)).pin_memory(), non_blocking=True)
+            else:
+                for i, x in enumerate(xs):
+                    x = torch.from_numpy(np.asarray(x, np.float32)) if isinstance(x, np.ndarray) else x
+                    dev[i].copy_(x, non_blocking=x.device.type == "cpu" and x.is_pinned() or x.is_cuda)
             inputs[k] = dev
     job = solver.submit(metric=inputs.get("metric"), cost=inputs.get("cost"), seeds=inputs["seeds"],
                         seedValues=inputs.get("seedValues"))
@@ -461,8 +470,8 @@ class Interface:
                                help="Choice of fixed point solver (AGSI, global_iteration)")
         alt = {"FIM": "fast_iterative_method", "AGSI": "adaptive_gauss_siedel_iteration"}
         self.solver = alt.get(solver, solver)
-        if self.solver != "fast_iterative_method":
-            raise NotImplementedError(f"solver {solver!r}: this build schedules tiles by the fast iterative method")
+        if self.solver not in ("fast_iterative_method", "adaptive_gauss_siedel_iteration", "global_iteration"):
+            raise ValueError(f"Unrecognized solver : {self.solver}")
         self.fim_front_width = int(self.GetValue(
             "fim_front_width", default=front,
             help="Dictates the max front width in the FIM variant.\n(original FIM : 2. Must be >=2.)"))
@@ -860,7 +869,9 @@ class Interface:
         inst.niter_i = self.niter_i
         inst.fim_front_width = self.fim_front_width
         inst.nitermax_o = self.nitermax_o
-        inst.flags = _lib.AGD_FLAG_ACTIVATE_ALL if self.activateAll else 0
+        inst.flags = (_lib.AGD_FLAG_ACTIVATE_ALL if self.activateAll else 0) | {
+            "adaptive_gauss_siedel_iteration": _lib.AGD_FLAG_SOLVER_AGSI,
+            "global_iteration": _lib.AGD_FLAG_SOLVER_GLOBAL}.get(getattr(self, "solver", ""), 0)
         inst.atol, inst.rtol = self.atol, self.rtol
         inst.values = self.values_t.data_ptr()
         if self.multiprecision:

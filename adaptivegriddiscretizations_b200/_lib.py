@@ -24,6 +24,8 @@ AGD_MODEL_RIEMANN = 1
 AGD_MODEL_DIAGONAL = 2
 AGD_MODEL_RANDER = 3
 AGD_FLAG_ACTIVATE_ALL = 1
+AGD_FLAG_SOLVER_AGSI = 2
+AGD_FLAG_SOLVER_GLOBAL = 4
 
 _c_int3 = ctypes.c_int * 3
 _c_float3 = ctypes.c_float * 3

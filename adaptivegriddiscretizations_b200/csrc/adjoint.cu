@@ -386,7 +386,7 @@ struct RevLayout {
 
 static bool rev_layout(const agd_instance *a, RevLayout &R, std::vector<Inst> *insts) {
     agd_instance b = *a;
-    b.flags |= AGD_FLAG_ACTIVATE_ALL;
+    b.flags = (b.flags | AGD_FLAG_ACTIVATE_ALL) & ~(AGD_FLAG_SOLVER_AGSI | AGD_FLAG_SOLVER_GLOBAL);
     b.trigger = nullptr;
     b.release = nullptr;  // the linear solves keep the two-list schedule
     if (!layout(&b, 1, R.L, insts, /*stencil_cache=*/false)) return false;

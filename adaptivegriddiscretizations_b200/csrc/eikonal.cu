@@ -654,6 +654,20 @@ struct Visit {
         const bool changed = __any_sync(kFull, notconv);
         __syncwarp();
 
+        // Adaptive Gauss-Seidel iteration: a changed tile is visited again with
+        // its neighbours (cuda/Propagation.h:151-154, Neighbor() including the
+        // tile itself); global iteration: every tile at every epoch until an
+        // epoch changes nothing (_solvers.py:77-92, stop test in close_epoch).
+        if (A.flags & (AGD_FLAG_SOLVER_AGSI | AGD_FLAG_SOLVER_GLOBAL)) {
+            if (A.flags & AGD_FLAG_SOLVER_GLOBAL) {
+                if (changed && lane == 0) atomicMax(&S.ist[ii].changed, e);
+                if (lane == 2 * D) push_tile(S, I, ii, t, e);
+            } else {
+                const int target = !changed ? -1 : lane == 2 * D ? t : nb;
+                if (target >= 0) push_tile(S, I, ii, target, e);
+            }
+            return;
+        }
         // Fast iterative method (cuda/Propagation.h:103-167).
         const int front = A.fim_front_width;
         int sn;

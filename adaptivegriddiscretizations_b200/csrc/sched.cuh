@@ -146,6 +146,7 @@ struct InstState {
     unsigned cnt[kMaxLists];  // lengths of the instance's lists, by epoch modulo the list count
     int done;
     unsigned first;    // ticket of the first entry of epoch 1
+    int changed;       // global iteration: last epoch in which a tile changed
 };
 
 struct Ctrl {
@@ -401,6 +402,8 @@ static __device__ void close_epoch(const Sched &S, int ii, int e, int lane) {
         if (lane == 0) n = (int)atomicAdd(&st.cnt[(e + 1) & 1], 0u);
         n = __shfl_sync(kFull, n, 0);
     }
+    // global iteration: the list holds every tile; an epoch without change ends the solve
+    if ((I.a.flags & AGD_FLAG_SOLVER_GLOBAL) && atomicAdd(&st.changed, 0) < e) n = 0;
     if (n == 0 || e >= I.a.nitermax_o) {
         int last = 0;
         if (lane == 0) {
@@ -565,7 +568,7 @@ static __global__ void setup_tiles(Sched S, int total_tiles) {
     if (t >= I.tile_base + I.size_o) return;  // past the last tile
     const int n_o = t - I.tile_base;
     const_cast<int *>(S.tile_inst)[t] = lo;
-    bool active = (I.a.flags & AGD_FLAG_ACTIVATE_ALL) != 0;
+    bool active = (I.a.flags & (AGD_FLAG_ACTIVATE_ALL | AGD_FLAG_SOLVER_GLOBAL)) != 0;
     if (I.a.trigger) {
         active = active || I.a.trigger[n_o] != 0;
     } else if (!active) {

@@ -113,6 +113,12 @@ typedef struct agd_instance {
 } agd_instance;
 
 #define AGD_FLAG_ACTIVATE_ALL 1 /* every tile is active at the first iteration */
+/* The outer iteration (the `solver` key, _Kernel.py:71-81, _solvers.py:77-193);
+ * neither flag: the fast iterative method (the default). */
+#define AGD_FLAG_SOLVER_AGSI 2   /* adaptive Gauss-Seidel: a tile that changed is
+                                    visited again with its neighbours */
+#define AGD_FLAG_SOLVER_GLOBAL 4 /* global iteration: every tile at every epoch
+                                    until an epoch changes nothing */
 
 /* Per-instance results, written by the solver into device memory. */
 typedef struct agd_stats {

@@ -276,3 +276,23 @@ def test_order2_more_accurate():
     e1 = np.abs(u1 - exact)[far].mean()
     e2 = np.abs(u2 - exact)[far].mean()
     assert e2 < 0.5 * e1
+
+
+@pytest.mark.parametrize("solver", ["AGSI", "global_iteration"])
+@pytest.mark.parametrize("name", ["iso2", "riem2", "riem3"])
+def test_other_solvers_reach_the_discrete_solution(solver, name):
+    """The reference's other outer iterations (the `solver` key: adaptive
+    Gauss-Seidel, global iteration; _solvers.py:77-193) stop at the same
+    discrete fixed point (the parity criteria against the discrete solution);
+    a global iteration visits every tile at every epoch."""
+    case, ref = load_case(name)
+    case = {k: v for k, v in case.items() if k not in ("tips", "sensitivity")}
+    out = make_dictin(case, extra={"solver": solver, "exportValues": True}).Run()
+    v = out["values"].cpu().numpy()
+    assert_near_discrete(v, case)
+    st = out["stats"]["eikonal"]
+    if solver == "global_iteration":
+        shape = [int(s) for s in case["dims"]]
+        si = {2: 16 if case["model"].startswith("Iso") else 8, 3: 4}[len(shape)]
+        ntiles = int(np.prod([-(-s // si) for s in shape]))
+        assert st["nupdate_o_total"] == st["niter_o"] * ntiles
