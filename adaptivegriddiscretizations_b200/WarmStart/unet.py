@@ -106,7 +106,8 @@ class UNet:
             h, w = R[level]
             return torch.empty((n, h, w, ch), dtype=torch.float32, device="cuda")
 
-        B = dict(a0=bf(0, c0), y0=bf(0, c0), p0=bf(1, c0), a1=bf(1, c1), y1=bf(1, c1), p1=bf(2, c1),
+        B = dict(u2=bf(2, c3), u1=bf(1, c2), u0=bf(0, c1),  # upsampled decoder inputs
+                 a0=bf(0, c0), y0=bf(0, c0), p0=bf(1, c0), a1=bf(1, c1), y1=bf(1, c1), p1=bf(2, c1),
                  a2=bf(2, c2), y2=bf(2, c2), p2=bf(3, c2), a3=bf(3, c3), y3=bf(3, c3),
                  d2a=bf(2, c2), d2=bf(2, c2), d1a=bf(1, c1), d1=bf(1, c1), d0a=bf(0, c0), d0=bf(0, c0),
                  r=torch.empty((n, H, W), dtype=torch.float32, device="cuda"),
@@ -147,6 +148,10 @@ class UNet:
         n, H, W, C = x.shape
         _lib.check(_lib.lib().agd_ws_avgpool(_p(x), n, H, W, C, _p(y), _lib.stream_ptr()), "avgpool")
 
+    def _upsample(self, x, y):
+        n, H, W, C = x.shape
+        _lib.check(_lib.lib().agd_ws_upsample(_p(x), n, H, W, C, _p(y), _lib.stream_ptr()), "upsample")
+
     def _route(self, y, terms, dz):
         n, H, W, C = y.shape
         ts = [_lib.AgdWsTerm() for _ in range(2)]
@@ -174,11 +179,14 @@ class UNet:
         self._pool(B["y2"], B["p2"])
         self._conv(e[6], n, *R[3], [(B["p2"], c2, 0)], B["a3"])
         self._conv(e[7], n, *R[3], [(B["a3"], c3, 0)], B["y3"])
-        self._conv(d[0], n, *R[2], [(B["y3"], c3, 1), (B["y2"], c2, 0)], B["d2a"])
+        self._upsample(B["y3"], B["u2"])
+        self._conv(d[0], n, *R[2], [(B["u2"], c3, 0), (B["y2"], c2, 0)], B["d2a"])
         self._conv(d[1], n, *R[2], [(B["d2a"], c2, 0)], B["d2"])
-        self._conv(d[2], n, *R[1], [(B["d2"], c2, 1), (B["y1"], c1, 0)], B["d1a"])
+        self._upsample(B["d2"], B["u1"])
+        self._conv(d[2], n, *R[1], [(B["u1"], c2, 0), (B["y1"], c1, 0)], B["d1a"])
         self._conv(d[3], n, *R[1], [(B["d1a"], c1, 0)], B["d1"])
-        self._conv(d[4], n, *R[0], [(B["d1"], c1, 1), (B["y0"], c0, 0)], B["d0a"])
+        self._upsample(B["d1"], B["u0"])
+        self._conv(d[4], n, *R[0], [(B["u0"], c1, 0), (B["y0"], c0, 0)], B["d0a"])
         self._conv(d[5], n, *R[0], [(B["d0a"], c0, 0)], B["d0"])
         _lib.check(_lib.lib().agd_ws_head_forward(_p(B["d0"]), n * H * W, _p(self.hw), _p(self.hb), _p(B["r"]),
                                                   _lib.stream_ptr()), "head")

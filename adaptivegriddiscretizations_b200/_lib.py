@@ -117,6 +117,7 @@ SIGNATURES = {
     "agd_ws_features": (_I, [_P, _P, _I, _I, _I, _I, ctypes.c_float, _P, _P, _P]),
     "agd_ws_target": (_I, [_P, _I, _I, _I, _P, _P, _P]),
     "agd_ws_avgpool": (_I, [_P, _I, _I, _I, _I, _P, _P]),
+    "agd_ws_upsample": (_I, [_P, _I, _I, _I, _I, _P, _P]),
     "agd_ws_route": (_I, [_I, _I, _I, _I, _P, AgdWsTerm, AgdWsTerm, _P, _P]),
     "agd_ws_bias_grad": (_I, [_P, ctypes.c_longlong, _I, _P, _P]),
     "agd_ws_head_forward": (_I, [_P, ctypes.c_longlong, _P, _P, _P, _P]),

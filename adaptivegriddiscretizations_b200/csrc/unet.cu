@@ -6,9 +6,11 @@
 // and the two uses of a prediction by the solver: per-tile release epochs and
 // warm-start values.  The reference has no learned component; this file has
 // no counterpart there.  C ABI: include/agd_warmstart.h.
+#include <cuda.h>
 #include <cuda_bf16.h>
 
 #include <algorithm>
+#include <cstdlib>
 #include <cstdint>
 
 #include "../../include/agd_warmstart.h"
@@ -374,6 +376,240 @@ __global__ void __launch_bounds__(kPThreads, 2) conv_gemm_kernel(GemmArgs g, Gem
     }
 }
 
+// --------------------------------------------------------- TMA-fed forward
+// The same GEMM with both operands moved by bulk tensor copies (TMA) into
+// swizzled K-major tiles, for inputs whose channel counts are multiples of 32
+// at the output's resolution, images of W | 128 columns and 128 | H W pixels:
+// a tile is 128 / W whole rows of one image.  A K chunk is (tap, input,
+// block of CB = 64 channels, or 32 for a 32-channel input): the A tile is the
+// box (CB channels, W columns, 128 / W rows) of the input at (channel block,
+// dx, y0 + dy, image), zero outside the image by the copy's out-of-bounds
+// fill, in 128-byte (64-byte) swizzled rows; the B tile the box (CB, BN) of
+// the weight matrix at (tap cin + channel offset, n0).  One producer lane
+// issues both copies per stage against one mbarrier transaction count, so
+// the operands bypass the per-lane L1 path.
+struct TmaArgs {
+    int H, W, R;       // rows of the output, columns, rows per tile (128 / W)
+    int C0, C1;        // input channels
+    int cb0, cb1;      // channel block of each input (64 or 32)
+    int cin, N, BN, kchunks;
+    int spc;           // K chunks per pipeline stage (each in its own slot)
+    int rowmax;        // bytes of the widest tile row (2 x the largest channel block)
+    const float *bias;
+    int relu;
+    bf16 *out_bf;
+    float *out_f;
+    long long M;
+    int mtiles, ntiles, stages;
+    unsigned *err;
+};
+
+// K chunk i -> (input s, channel offset c in that input, tap); the order is
+// tap-major, then the inputs' channel blocks.
+__device__ __forceinline__ void tma_chunk(const TmaArgs &g, int i, int &s, int &c, int &tap) {
+    const int per = g.C0 / g.cb0 + (g.C1 ? g.C1 / g.cb1 : 0);
+    tap = i / per;
+    const int j = i - tap * per;
+    const int n0 = g.C0 / g.cb0;
+    if (j < n0) {
+        s = 0;
+        c = j * g.cb0;
+    } else {
+        s = 1;
+        c = (j - n0) * g.cb1;
+    }
+}
+
+__device__ __forceinline__ void tma_load_4d(uint32_t dst, const CUtensorMap *map, int c0, int c1, int c2, int c3,
+                                            uint64_t *bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, %5}], "
+        "[%6];" ::"r"(dst),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(umma::smem_u32(bar))
+        : "memory");
+}
+__device__ __forceinline__ void tma_load_2d(uint32_t dst, const CUtensorMap *map, int c0, int c1, uint64_t *bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::"r"(
+            dst),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(c0), "r"(c1), "r"(umma::smem_u32(bar))
+        : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(umma::smem_u32(bar)), "r"(bytes)
+                 : "memory");
+}
+
+// K-major swizzled descriptor: rows of `row` bytes (128: 128-byte swizzle,
+// 64: 64-byte swizzle), 8-row atoms of 8 row bytes.
+__device__ __forceinline__ uint64_t swz_desc(uint32_t saddr, int row) {
+    const uint64_t layout = row == 128 ? 2ull : 4ull;
+    return (uint64_t)((saddr >> 4) & 0x3fffu) | (1ull << 16) | ((uint64_t)(((8u * row) >> 4) & 0x3fffu) << 32) |
+           (1ull << 46) | (layout << 61);
+}
+
+__global__ void __launch_bounds__(kPThreads, 2)
+    conv_tma_kernel(TmaArgs g, const __grid_constant__ CUtensorMap xa0, const __grid_constant__ CUtensorMap xa1,
+                    const __grid_constant__ CUtensorMap wb64, const __grid_constant__ CUtensorMap wb32) {
+    extern __shared__ __align__(1024) unsigned char smem[];
+    __shared__ Pipe P;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const uint32_t ncols = tmem_cols(2 * g.BN);
+    const uint32_t a_bytes = kBM * g.rowmax, b_bytes = (uint32_t)g.BN * g.rowmax;  // a slot: the widest block
+    const uint32_t slot_bytes = a_bytes + b_bytes, stage_bytes = slot_bytes * g.spc;
+    const uint32_t sbase = (umma::smem_u32(smem) + 1023u) & ~1023u;  // swizzle atoms on 1024-byte boundaries
+    const int ntl = count_tiles(g.mtiles * g.ntiles);
+    const int nstage = (g.kchunks + g.spc - 1) / g.spc;  // stages per tile
+
+    if (warp == kMmaWarp) {
+        umma::tmem_alloc(&P.taddr, ncols);
+        umma::tmem_relinquish();
+    }
+    if (tid == 0) {
+        for (int s = 0; s < g.stages; ++s) {
+            umma::mbar_init(&P.full[s], 1);
+            umma::mbar_init(&P.empty[s], 1);
+        }
+        for (int a = 0; a < 2; ++a) {
+            umma::mbar_init(&P.accf[a], 1);
+            umma::mbar_init(&P.acce[a], kEpilogue / 32);
+        }
+        umma::fence_mbar_init();
+    }
+    umma::tc_fence_before_sync();
+    __syncthreads();
+    umma::tc_fence_after_sync();
+
+    if (warp == 0) {
+        // ---------------------------------------------- producer (one lane)
+        Ring R;
+        bool wrapped = false, alive = true;
+        for (int tl = 0; tl < ntl && alive; ++tl) {
+            const int t = blockIdx.x + tl * gridDim.x;
+            const int mt = t % g.mtiles, nt = t / g.mtiles;
+            const long long m0 = (long long)mt * kBM;
+            const int nimg = (int)(m0 / ((long long)g.H * g.W));
+            const int y0 = (int)((m0 - (long long)nimg * g.H * g.W) / g.W);
+            for (int i0 = 0; i0 < nstage; ++i0) {
+                if (wrapped && !mbar_wait_warp(&P.empty[R.s], R.ph ^ 1u, g.err, kWaitNs)) {
+                    alive = false;
+                    break;
+                }
+                if (lane == 0) {
+                    const int i1 = min(g.kchunks, (i0 + 1) * g.spc);
+                    uint32_t tx = 0;
+                    for (int i = i0 * g.spc; i < i1; ++i) {
+                        int s, c, tap;
+                        tma_chunk(g, i, s, c, tap);
+                        tx += (uint32_t)(kBM + g.BN) * (s ? g.cb1 : g.cb0) * 2;
+                    }
+                    mbar_expect_tx(&P.full[R.s], tx);
+                    for (int i = i0 * g.spc; i < i1; ++i) {
+                        int s, c, tap;
+                        tma_chunk(g, i, s, c, tap);
+                        const int cb = s ? g.cb1 : g.cb0;
+                        const uint32_t sa = sbase + R.s * stage_bytes + (i - i0 * g.spc) * slot_bytes, sb = sa + a_bytes;
+                        tma_load_4d(sa, s ? &xa1 : &xa0, c, tap % 3 - 1, y0 + tap / 3 - 1, nimg, &P.full[R.s]);
+                        tma_load_2d(sb, cb == 64 ? &wb64 : &wb32, tap * g.cin + (s ? g.C0 : 0) + c, nt * g.BN,
+                                    &P.full[R.s]);
+                    }
+                }
+                __syncwarp();
+                R.next(g.stages);
+                wrapped = wrapped || R.s == 0;
+            }
+        }
+    } else if (warp == kMmaWarp) {
+        // ---------------------------------------------- MMA (lane 0 issues)
+        const bool leader = lane == 0;
+        const uint32_t idesc = umma::idesc_bf16(kBM, g.BN, 0, 0);
+        Ring R;
+        bool ok = true;
+        for (int tl = 0; tl < ntl && ok; ++tl) {
+            const int a = tl & 1;
+            if (tl >= 2 && !mbar_wait_warp(&P.acce[a], ((tl >> 1) & 1) ^ 1, g.err, kWaitNs)) break;
+            umma::tc_fence_after_sync();
+            const uint32_t d = P.taddr + (uint32_t)(a * g.BN);
+            for (int i0 = 0; i0 < nstage; ++i0) {
+                if (!mbar_wait_warp(&P.full[R.s], R.ph, g.err, kWaitNs)) {
+                    ok = false;
+                    break;
+                }
+                umma::tc_fence_after_sync();
+                if (leader) {
+                    const int i1 = min(g.kchunks, (i0 + 1) * g.spc);
+                    for (int i = i0 * g.spc; i < i1; ++i) {
+                        int s, c, tap;
+                        tma_chunk(g, i, s, c, tap);
+                        const int row = 2 * (s ? g.cb1 : g.cb0);  // bytes of a tile row
+                        const uint32_t sa = sbase + R.s * stage_bytes + (i - i0 * g.spc) * slot_bytes, sb = sa + a_bytes;
+                        const uint64_t ad = swz_desc(sa, row), bd = swz_desc(sb, row);
+                        for (int kk = 0; kk < row / 32; ++kk)  // K = 16 per MMA: 32 bytes of a row
+                            umma::mma_bf16(d, ad + 2u * kk, bd + 2u * kk, idesc, (i | kk) != 0);
+                    }
+                    umma::mma_commit(&P.empty[R.s]);
+                }
+                __syncwarp();
+                R.next(g.stages);
+            }
+            if (leader) umma::mma_commit(&P.accf[a]);
+            __syncwarp();
+        }
+        mma_drain(P, ntl, g.err);
+    } else if (warp > kMmaWarp) {
+        // ---------------------------------------------------------- epilogue
+        const int ew = warp & 3;
+        for (int tl = 0; tl < ntl; ++tl) {
+            const int a = tl & 1;
+            const bool ok = mbar_wait_warp(&P.accf[a], (tl >> 1) & 1, g.err, kWaitNs);
+            umma::tc_fence_after_sync();
+            if (!ok) break;
+            const int t = blockIdx.x + tl * gridDim.x;
+            const int mt = t % g.mtiles, nt = t / g.mtiles;
+            const long long m = (long long)mt * kBM + 32 * ew + lane;
+            for (int c0 = 0; c0 < g.BN; c0 += 16) {
+                uint32_t r[16];
+                umma::tmem_ld16(P.taddr + ((uint32_t)(32 * ew) << 16) + (uint32_t)(a * g.BN + c0), r);
+                umma::tmem_ld_wait();
+                const int nc = nt * g.BN + c0;
+                if (m >= g.M || nc >= g.N) continue;
+                float v[16];
+#pragma unroll
+                for (int q = 0; q < 16; ++q) {
+                    v[q] = __uint_as_float(r[q]);
+                    if (g.bias) v[q] += __ldg(g.bias + nc + q);
+                    if (g.relu) v[q] = fmaxf(v[q], 0.f);
+                }
+                if (g.out_bf) {
+                    uint4 w[2];
+                    uint32_t *wp = reinterpret_cast<uint32_t *>(w);
+#pragma unroll
+                    for (int q = 0; q < 8; ++q) {
+                        __nv_bfloat162 h = __floats2bfloat162_rn(v[2 * q], v[2 * q + 1]);
+                        wp[q] = *reinterpret_cast<uint32_t *>(&h);
+                    }
+                    uint4 *dst = reinterpret_cast<uint4 *>(g.out_bf + m * g.N + nc);
+                    dst[0] = w[0];
+                    dst[1] = w[1];
+                } else {
+                    float4 *dst = reinterpret_cast<float4 *>(g.out_f + m * g.N + nc);
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) dst[q] = make_float4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
+                }
+            }
+            umma::tc_fence_before_sync();
+            __syncwarp();
+            if (lane == 0) asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(umma::smem_u32(&P.acce[a])) : "memory");
+        }
+    }
+    umma::tc_fence_before_sync();
+    __syncthreads();
+    if (warp == kMmaWarp) {
+        umma::tc_fence_after_sync();
+        umma::tmem_dealloc(P.taddr, ncols);
+    }
+}
+
 // Weight gradient: dW[n, r] += sum_p dZ[p, n] X[p + tap(r), ci(r)], r = tap *
 // cin + ci.  GEMM with M = r (128 per tile), N = n, K = pixels (64 per stage,
 // split over `splits` work items): both operands MN-major (8 consecutive
@@ -652,6 +888,20 @@ __global__ void avgpool_kernel(const bf16 *x, int n, int H, int W, int C, bf16 *
     *reinterpret_cast<uint4 *>(y + p * C + c8 * 8) = w;
 }
 
+// Nearest 2x upsampling, NHWC bf16 (n, H, W, C) -> (n, 2H, 2W, C), 8 channels per thread.
+__global__ void upsample_kernel(const bf16 *x, int n, int H, int W, int C, bf16 *y) {
+    const int C8 = C / 8;
+    const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= (long long)n * 4 * H * W * C8) return;
+    const int c8 = (int)(idx % C8);
+    const long long p = idx / C8;  // output pixel
+    const int b = (int)(p / (4LL * H * W));
+    const int r = (int)(p - (long long)b * 4 * H * W);
+    const int oy = r / (2 * W), ox = r - (r / (2 * W)) * (2 * W);
+    *reinterpret_cast<uint4 *>(y + p * C + c8 * 8) =
+        *reinterpret_cast<const uint4 *>(x + (((long long)b * H + oy / 2) * W + ox / 2) * C + c8 * 8);
+}
+
 // Backward routing into a layer output Y (n, H, W, C): the gradient of Y is the
 // sum of up to two terms, each read from an fp32 NHWC buffer of Cb channels at
 // channel offset `off`: SAME (same resolution), POOL (the input gradient of a
@@ -894,6 +1144,113 @@ bool check_srcs(const agd_conv *c, Src *s0, Src *s1) {
     return true;
 }
 
+typedef CUresult (*EncodeTiledFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
+                                   const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
+                                   CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+// cuTensorMapEncodeTiled through the runtime's driver entry point (no link
+// against the driver library); NULL if unavailable.
+EncodeTiledFn encode_tiled() {
+    static EncodeTiledFn fn = nullptr;
+    static bool tried = false;
+    if (!tried) {
+        tried = true;
+        void *p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<EncodeTiledFn>(p);
+    }
+    return fn;
+}
+
+// bf16 tiled map of `rank` dims (innermost first), swizzle by the inner box
+// row (128 or 64 bytes).
+bool make_map(CUtensorMap *map, const void *base, int rank, const cuuint64_t *dims, const cuuint64_t *strides,
+              const cuuint32_t *box, int row_bytes) {
+    EncodeTiledFn fn = encode_tiled();
+    if (!fn) return false;
+    const cuuint32_t es[5] = {1, 1, 1, 1, 1};
+    return fn(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, (cuuint32_t)rank, const_cast<void *>(base), dims, strides, box,
+              es, CU_TENSOR_MAP_INTERLEAVE_NONE,
+              row_bytes == 128 ? CU_TENSOR_MAP_SWIZZLE_128B : CU_TENSOR_MAP_SWIZZLE_64B,
+              CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+// The TMA-fed forward when the shapes allow it: 1 launched, 0 not applicable.
+int conv_tma(const agd_conv *c, const void *w, const float *bias, int relu, void *out_bf16, float *out_f32,
+             unsigned *err, cudaStream_t st, int *rc) {
+    const agd_conv_src &s0 = c->src[0], &s1 = c->src[1];
+    const bool two_in = s1.data != nullptr;
+    if (s0.up || (two_in && s1.up) || s0.channels % 32 || (two_in && s1.channels % 32)) return 0;
+    if (c->W > 128 || 128 % c->W || ((long long)c->H * c->W) % 128) return 0;
+    TmaArgs g{};
+    g.H = c->H;
+    g.W = c->W;
+    g.R = 128 / c->W;
+    g.C0 = s0.channels;
+    g.C1 = two_in ? s1.channels : 0;
+    g.cb0 = g.C0 % 64 ? 32 : 64;
+    g.cb1 = g.C1 % 64 ? 32 : 64;
+    g.cin = g.C0 + g.C1;
+    g.N = c->cout;
+    g.BN = tile_n(g.N, &g.ntiles);
+    g.kchunks = 9 * (g.C0 / g.cb0 + g.C1 / g.cb1);
+    g.bias = bias;
+    g.relu = relu;
+    g.out_bf = static_cast<bf16 *>(out_bf16);
+    g.out_f = out_f32;
+    g.M = (long long)c->n * c->H * c->W;
+    g.err = err;
+    const long long mtiles = g.M / kBM;
+    if (mtiles * g.ntiles > 0x7fffffffLL) return 0;
+    g.mtiles = (int)mtiles;
+    const int kpad = kpad_of(9 * g.cin);
+    CUtensorMap xa0, xa1, wb64, wb32;
+    const int ins = two_in ? 2 : 1;
+    for (int k = 0; k < ins; ++k) {
+        const agd_conv_src &sr = c->src[k];
+        const int C = sr.channels, cb = C % 64 ? 32 : 64;
+        const cuuint64_t dims[4] = {(cuuint64_t)C, (cuuint64_t)c->W, (cuuint64_t)c->H, (cuuint64_t)c->n};
+        const cuuint64_t strides[3] = {(cuuint64_t)C * 2, (cuuint64_t)c->W * C * 2, (cuuint64_t)c->H * c->W * C * 2};
+        const cuuint32_t box[4] = {(cuuint32_t)cb, (cuuint32_t)c->W, (cuuint32_t)g.R, 1};
+        if (!make_map(k ? &xa1 : &xa0, sr.data, 4, dims, strides, box, 2 * cb)) return 0;
+    }
+    if (!two_in) xa1 = xa0;
+    const cuuint64_t wdims[2] = {(cuuint64_t)kpad, (cuuint64_t)g.N};
+    const cuuint64_t wstr[1] = {(cuuint64_t)kpad * 2};
+    const cuuint32_t box64[2] = {64, (cuuint32_t)g.BN}, box32[2] = {32, (cuuint32_t)g.BN};
+    if (!make_map(&wb64, w, 2, wdims, wstr, box64, 128) || !make_map(&wb32, w, 2, wdims, wstr, box32, 64)) return 0;
+    const bool two = g.BN <= 128;
+    const int budget = (two ? kSmemBudget2 : kSmemBudget) - 1024;
+    // small chunks (32-channel blocks, few output channels) share a stage, so
+    // that a barrier round trip carries more tensor work
+    g.rowmax = 2 * std::max(g.cb0, two_in ? g.cb1 : 0);
+    g.spc = 1;
+    const int slot = (kBM + g.BN) * g.rowmax;
+    static const int spc_max = [] {
+        const char *e = getenv("AGD_CONV_CHUNKS_PER_STAGE");  // tuning: 1, 2 or 4 (default 4)
+        const int v = e ? atoi(e) : 4;
+        return v == 1 || v == 2 ? v : 4;
+    }();
+    while (g.spc < spc_max && g.spc * 2 <= g.kchunks && (g.rowmax == 64 || g.BN <= 32) &&
+           3 * slot * g.spc * 2 <= budget)
+        g.spc *= 2;
+    const int stage = slot * g.spc;
+    g.stages = std::min(kMaxStages, budget / stage);
+    if (g.stages < 2) return 0;
+    const int smem = two ? g.stages * stage + 1024 : std::max(g.stages * stage + 1024, 120 * 1024);
+    cudaError_t e = cudaFuncSetAttribute(conv_tma_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    if (e != cudaSuccess) {
+        *rc = set_cuda_error("conv3x3 shared memory", e);
+        return 1;
+    }
+    const int grid = (int)std::min<long long>(mtiles * g.ntiles, (two ? 2 : 1) * num_sms());
+    conv_tma_kernel<<<grid, kPThreads, smem, st>>>(g, xa0, xa1, wb64, wb32);
+    *rc = launched("conv3x3 forward (TMA)");
+    return 1;
+}
+
 }  // namespace
 
 extern "C" {
@@ -906,6 +1263,9 @@ int agd_conv3x3_forward(const agd_conv *c, const void *w, const float *bias, int
     if (!check_srcs(c, &g.s0, &g.s1)) return set_error(AGD_STATUS_INVALID, "conv3x3: bad inputs");
     if (!w || !err || (!out_bf16) == (!out_f32) || c->cout <= 0 || c->cout % 16)
         return set_error(AGD_STATUS_INVALID, "conv3x3: weights, err, one output and cout % 16 == 0 are required");
+    int rc = AGD_STATUS_OK;
+    if (reinterpret_cast<uintptr_t>(w) % 16 == 0 && conv_tma(c, w, bias, relu, out_bf16, out_f32, err, cs(stream), &rc))
+        return rc;
     g.nimg = c->n;
     g.H = c->H;
     g.W = c->W;
@@ -1014,6 +1374,14 @@ int agd_ws_avgpool(const void *x, int n, int H, int W, int C, void *y, agd_strea
     avgpool_kernel<<<(unsigned)((m + 255) / 256), 256, 0, cs(stream)>>>(static_cast<const bf16 *>(x), n, H, W, C,
                                                                         static_cast<bf16 *>(y));
     return launched("avgpool");
+}
+
+int agd_ws_upsample(const void *x, int n, int H, int W, int C, void *y, agd_stream_t stream) {
+    if (!x || !y || n <= 0 || H <= 0 || W <= 0 || C % 8) return set_error(AGD_STATUS_INVALID, "upsample: bad arguments");
+    const long long m = (long long)n * 4 * H * W * (C / 8);
+    upsample_kernel<<<(unsigned)((m + 255) / 256), 256, 0, cs(stream)>>>(static_cast<const bf16 *>(x), n, H, W, C,
+                                                                         static_cast<bf16 *>(y));
+    return launched("upsample");
 }
 
 int agd_ws_route(int n, int H, int W, int C, const void *y, agd_ws_term t0, agd_ws_term t1, void *dz,

@@ -388,11 +388,12 @@ def run_unet(args):
 
     net._conv = timed
     rows = []
-    for _ in range(args.steps):
-        layers.clear()
-        net.forward(x0)
-        torch.cuda.synchronize()
-        rows.append([(H, ci, co, e0.elapsed_time(e1) / 1e3, fl) for H, ci, co, e0, e1, fl in layers])
+    with ClockSampler(0) as clk:
+        for _ in range(args.steps):
+            layers.clear()
+            net.forward(x0)
+            torch.cuda.synchronize()
+            rows.append([(H, ci, co, e0.elapsed_time(e1) / 1e3, fl) for H, ci, co, e0, e1, fl in layers])
     net._conv = orig
     try:
         with open(os.path.join(REPO, "MEASURED_PEAKS.json")) as f:
@@ -410,7 +411,7 @@ def run_unet(args):
                       "unit": "TFLOP/s", "batch": B, "blocks": nb, "ms_per_forward_convs": 1e3 * tot_t,
                       "roofline": {"bound": "tensor", "achieved": tot_f / tot_t / 1e12, "peak": peak,
                                    "unit": "TFLOP/s", "frac": tot_f / tot_t / 1e12 / peak},
-                      "layers": per}), flush=True)
+                      "clocks": clk.summary(), "layers": per}), flush=True)
 
 
 def run_autotune(n, B, metrics, seeds):

@@ -53,7 +53,10 @@ int agd_conv_kpad(int cin);
 
 /* out = act(conv3x3(inputs, w) + bias): an implicit GEMM on the tensor cores
  * (tcgen05.mma, fp32 accumulators in tensor memory), 128 pixels x up to 256
- * output channels per CTA.  bias may be NULL; relu != 0 applies max(0, .).
+ * output channels per tile.  Inputs at the output's resolution with channel
+ * counts that are multiples of 32, W dividing 128 and 128 dividing H W, are
+ * moved by bulk tensor copies (TMA, swizzled tiles); other shapes by per-lane
+ * cp.async gathers.  bias may be NULL; relu != 0 applies max(0, .).
  * Exactly one of out_bf16 (NHWC bf16) and out_f32 (NHWC fp32) is non NULL.
  * The input gradient of a convolution is this call on the output gradient with
  * the flipped weights of agd_conv_weight_flip, no bias, no ReLU, fp32 output. */
@@ -83,6 +86,11 @@ int agd_ws_target(const float *values, int n, int H, int W, const float *dref, f
 
 /* 2x2 average pooling, NHWC bf16 (n, H, W, C) -> (n, H/2, W/2, C). */
 int agd_ws_avgpool(const void *x, int n, int H, int W, int C, void *y, agd_stream_t stream);
+
+/* Nearest 2x upsampling, NHWC bf16 (n, H, W, C) -> (n, 2H, 2W, C): the decoder's
+ * upsampled input materialised, so that its convolution can take the
+ * bulk-copy operand path. */
+int agd_ws_upsample(const void *x, int n, int H, int W, int C, void *y, agd_stream_t stream);
 
 /* Gradient routing into a layer output y (n, H, W, C): the sum of up to two
  * fp32 NHWC terms (buffer, mode, buffer channels, channel offset): mode 1 the

@@ -66,6 +66,13 @@ CASES = [  # (n, H, W, [(cin, up)], cout)
     (2, 32, 32, [(64, 1), (32, 0)], 32),
     (2, 16, 16, [(256, 1), (128, 0)], 128),
     (1, 8, 8, [(128, 0)], 384),
+    # bulk-copy (TMA) operand path: inputs at the output resolution, channels
+    # multiples of 32, W | 128, 128 | H W; mixed 64- and 32-channel blocks
+    (2, 32, 32, [(64, 0), (32, 0)], 32),
+    (4, 64, 64, [(32, 0)], 64),
+    (2, 16, 16, [(256, 0), (128, 0)], 128),
+    (1, 128, 128, [(32, 0)], 32),
+    (2, 32, 32, [(128, 0)], 256),
 ]
 
 
