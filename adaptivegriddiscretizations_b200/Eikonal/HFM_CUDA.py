@@ -451,8 +451,6 @@ class Interface:
             "multiprecision", default=False, help="Use multiprecision arithmetic, to improve accuracy")
         self.factoringRadius = float(self.GetValue("factoringRadius", default=0,
                                                    help="Use source factorization, to improve accuracy"))
-        if self.factoringRadius and self.multiprecision:
-            raise NotImplementedError("source factorization with multiprecision is not available in this build")
         order = self.GetValue("order", default=1, help="Use second order scheme to improve accuracy")
         if order not in {1, 2}:
             raise ValueError(f"Unsupported scheme order {order}")

@@ -740,6 +740,18 @@ __device__ __forceinline__ void dispatch(const Sched &S, int t, int e, int lane,
         case V_ISO2_8_F:
             if constexpr ((VMASK >> V_ISO2_8_F) & 1) Visit<Tile<2, 8, 8, 1>, AGD_MODEL_ISOTROPIC, false, true>::run(S, I, ii, n_o, e, lane, us);
             break;
+        case V_ISO2_16_FMP:
+            if constexpr ((VMASK >> V_ISO2_16_FMP) & 1) Visit<Tile<2, 16, 16, 1>, AGD_MODEL_ISOTROPIC, true, true>::run(S, I, ii, n_o, e, lane, us);
+            break;
+        case V_RIEM2_8_FMP:
+            if constexpr ((VMASK >> V_RIEM2_8_FMP) & 1) Visit<Tile<2, 8, 8, 1>, AGD_MODEL_RIEMANN, true, true, false, true>::run(S, I, ii, n_o, e, lane, us);
+            break;
+        case V_ISO3_4_FMP:
+            if constexpr ((VMASK >> V_ISO3_4_FMP) & 1) Visit<Tile<3, 4, 4, 4>, AGD_MODEL_ISOTROPIC, true, true>::run(S, I, ii, n_o, e, lane, us);
+            break;
+        case V_RIEM3_4_FMP:
+            if constexpr ((VMASK >> V_RIEM3_4_FMP) & 1) Visit<Tile<3, 4, 4, 4>, AGD_MODEL_RIEMANN, true, true, false, true>::run(S, I, ii, n_o, e, lane, us);
+            break;
         case V_ISO2_16_F:
             if constexpr ((VMASK >> V_ISO2_16_F) & 1) Visit<Tile<2, 16, 16, 1>, AGD_MODEL_ISOTROPIC, false, true>::run(S, I, ii, n_o, e, lane, us);
             break;
@@ -910,11 +922,12 @@ struct EikonalVisitor {
     static constexpr bool kBulkPublish = BULK;
     static constexpr int kMinCtas =
         (VMASK & ((1ull << V_RIEM2_16) | (1ull << V_ISO2_16) | (1ull << V_ISO2_16_MP) | (1ull << V_ISO2_16_F) |
+                  (1ull << V_ISO2_16_FMP) |
                   (1ull << V_ISO2_16_O2) | (1ull << V_RIEM2_16_W) | (1ull << V_DIAG2_16) |
                   (1ull << V_DIAG2_16_MP) | (1ull << V_DIAG2_16_F) | (1ull << V_DIAG2_16_O2)))      ? 4
         : (VMASK & ((1ull << V_RIEM3_4) | (1ull << V_RIEM3_4_MP) | (1ull << V_RIEM3_4_F) | (1ull << V_RIEM3_4_O2) |
                     (1ull << V_RIEM3_4_W) | (1ull << V_RAND3_4) | (1ull << V_RAND3_4_W) | (1ull << V_RAND3_4_MP) |
-                    (1ull << V_RAND3_4_F) | (1ull << V_RAND3_4_O2)))                             ? 5
+                    (1ull << V_RAND3_4_F) | (1ull << V_RAND3_4_O2) | (1ull << V_RIEM3_4_FMP)))   ? 5
         : (VMASK & (kMpVariants | kFactorVariants | kOrder2Variants))                                ? 7
                                                                                                      : 9;
     struct Args {};
@@ -931,18 +944,19 @@ struct EikonalVisitor {
         constexpr unsigned long long kRiemann = (1ull << V_RIEM2_8) | (1ull << V_RIEM3_4) | (1ull << V_RIEM2_16) |
                                       (1ull << V_RIEM2_8_MP) | (1ull << V_RIEM3_4_MP) | (1ull << V_RIEM2_8_F) |
                                       (1ull << V_RIEM3_4_F) | (1ull << V_RIEM2_8_O2) | (1ull << V_RIEM3_4_O2) |
-                                      kWallVariants | kRanderVariants;
+                                      (1ull << V_RIEM2_8_FMP) | (1ull << V_RIEM3_4_FMP) | kWallVariants |
+                                      kRanderVariants;
         if (VMASK & kMpVariants) mp_copy_kernel<<<(L.total_tiles + 7) / 8, 256, 0, st>>>(S, 0);
         if (!(VMASK & kRiemann) || L.stencil == L.total) return cudaGetLastError();
         // variants that read the hidden-neighbour bits: the walls pass follows
         constexpr unsigned long long kWallCapable = kWallVariants | (1ull << V_RIEM2_8_MP) | (1ull << V_RIEM3_4_MP) |
                                           (1ull << V_RIEM2_8_F) | (1ull << V_RIEM3_4_F) | (1ull << V_RIEM2_8_O2) |
-                                          (1ull << V_RIEM3_4_O2) | (kRanderVariants & ~((1ull << V_RAND2_8) |
-                                                                                      (1ull << V_RAND3_4)));
+                                          (1ull << V_RIEM3_4_O2) | (1ull << V_RIEM2_8_FMP) | (1ull << V_RIEM3_4_FMP) |
+                                          (kRanderVariants & ~((1ull << V_RAND2_8) | (1ull << V_RAND3_4)));
         const unsigned grid = (L.total_tiles + 7) / 8;
         if (VMASK & ((1ull << V_RIEM3_4) | (1ull << V_RIEM3_4_MP) | (1ull << V_RIEM3_4_F) | (1ull << V_RIEM3_4_O2) |
                      (1ull << V_RIEM3_4_W) | (1ull << V_RAND3_4) | (1ull << V_RAND3_4_W) | (1ull << V_RAND3_4_MP) |
-                     (1ull << V_RAND3_4_F) | (1ull << V_RAND3_4_O2))) {
+                     (1ull << V_RAND3_4_F) | (1ull << V_RAND3_4_O2) | (1ull << V_RIEM3_4_FMP))) {
             stencil_kernel<3><<<grid, 256, 0, st>>>(S.inst, S.ninst, L.total_tiles, S.ctrl);
             if (VMASK & kWallCapable) stencil_walls_kernel<3><<<grid, 256, 0, st>>>(S.inst, S.ninst, L.total_tiles);
         } else {
@@ -979,10 +993,6 @@ static int validate(const agd_instance *host, const Inst *insts, int n, bool ste
         const char *bad = nullptr;
         int code = AGD_STATUS_INVALID;
         if (a.ndim != host[0].ndim) bad = "all instances of a plan must share ndim";
-        else if (a.factor_radius2 > 0.f && a.multip_step != 0.f) {
-            bad = "source factorisation with multiprecision is not built";
-            code = AGD_STATUS_UNSUPPORTED;
-        }
         else if (insts[i].variant < 0) { bad = "model/tile shape not built"; code = AGD_STATUS_UNSUPPORTED; }
         else if (a.wall_dist && (a.model == AGD_MODEL_RIEMANN || a.model == AGD_MODEL_RANDER) && !stencil_cache) {
             bad = "walls on a Riemann instance need the stencil cache (agd_eikonal_solve)";
@@ -1026,8 +1036,10 @@ static int run_variants(int ndim, unsigned long long vmask, const WsLayout &L, v
                         const agd_launch *cfg, cudaStream_t st) {
     constexpr unsigned long long R2 = 1ull << V_RIEM2_8, I16 = 1ull << V_ISO2_16, I8 = 1ull << V_ISO2_8;
     constexpr unsigned long long R3 = 1ull << V_RIEM3_4, I3 = 1ull << V_ISO3_4, R2L = 1ull << V_RIEM2_16;
-    constexpr unsigned long long MP2 = (1ull << V_ISO2_8_MP) | (1ull << V_ISO2_16_MP) | (1ull << V_RIEM2_8_MP);
-    constexpr unsigned long long MP3 = (1ull << V_ISO3_4_MP) | (1ull << V_RIEM3_4_MP);
+    constexpr unsigned long long MP2 = (1ull << V_ISO2_8_MP) | (1ull << V_ISO2_16_MP) | (1ull << V_RIEM2_8_MP) |
+                                       (1ull << V_ISO2_16_FMP) | (1ull << V_RIEM2_8_FMP);
+    constexpr unsigned long long MP3 = (1ull << V_ISO3_4_MP) | (1ull << V_RIEM3_4_MP) | (1ull << V_ISO3_4_FMP) |
+                                       (1ull << V_RIEM3_4_FMP);
     // Riemann with walls, beside plain instances of every family
     constexpr unsigned long long W2 = (1ull << V_RIEM2_8_W) | (1ull << V_RIEM2_16_W), W3 = 1ull << V_RIEM3_4_W;
     if (vmask & kRanderVariants) {  // Rander instances run in kernels of their own
@@ -1079,7 +1091,8 @@ static int run_variants(int ndim, unsigned long long vmask, const WsLayout &L, v
     if (vmask & kFactorVariants) {  // factored instances, possibly beside plain ones
         constexpr unsigned long long F2 = (1ull << V_ISO2_8_F) | (1ull << V_ISO2_16_F) | (1ull << V_RIEM2_8_F);
         constexpr unsigned long long F3 = (1ull << V_ISO3_4_F) | (1ull << V_RIEM3_4_F);
-        if (vmask & kMpVariants) return set_error(AGD_STATUS_UNSUPPORTED, "factorisation and multiprecision in one plan");
+        if (vmask & kMpVariants)
+            return set_error(AGD_STATUS_UNSUPPORTED, "factored instances without and with multiprecision in one plan");
         if (ndim == 2) return run_sched<EikonalVisitor<F2 | R2 | I16 | I8 | R2L | W2>>(L, ws, n, {}, stats, cfg, st);
         return run_sched<EikonalVisitor<F3 | R3 | I3 | W3>>(L, ws, n, {}, stats, cfg, st);
     }

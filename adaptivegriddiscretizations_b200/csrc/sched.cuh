@@ -30,13 +30,16 @@ enum Variant {
     V_DIAG2_8_F, V_DIAG2_16_F, V_DIAG3_4_F, V_DIAG2_8_O2, V_DIAG2_16_O2, V_DIAG3_4_O2,
     // Rander: plain, walls, multiprecision, factorisation, second order
     V_RAND2_8, V_RAND3_4, V_RAND2_8_W, V_RAND3_4_W, V_RAND2_8_MP, V_RAND3_4_MP, V_RAND2_8_F, V_RAND3_4_F,
-    V_RAND2_8_O2, V_RAND3_4_O2, V_COUNT
+    V_RAND2_8_O2, V_RAND3_4_O2,
+    // source factorisation with multiprecision (the default tile shapes)
+    V_ISO2_16_FMP, V_RIEM2_8_FMP, V_ISO3_4_FMP, V_RIEM3_4_FMP, V_COUNT
 };
 static_assert(V_COUNT <= 64, "variant masks are 64-bit");
 constexpr unsigned long long kMpVariants = (1ull << V_ISO2_8_MP) | (1ull << V_ISO2_16_MP) | (1ull << V_RIEM2_8_MP) |
                                  (1ull << V_ISO3_4_MP) | (1ull << V_RIEM3_4_MP) | (1ull << V_DIAG2_8_MP) |
                                  (1ull << V_DIAG2_16_MP) | (1ull << V_DIAG3_4_MP) | (1ull << V_RAND2_8_MP) |
-                                 (1ull << V_RAND3_4_MP);
+                                 (1ull << V_RAND3_4_MP) | (1ull << V_ISO2_16_FMP) | (1ull << V_RIEM2_8_FMP) |
+                                 (1ull << V_ISO3_4_FMP) | (1ull << V_RIEM3_4_FMP);
 constexpr unsigned long long kFactorVariants = (1ull << V_ISO2_8_F) | (1ull << V_ISO2_16_F) | (1ull << V_RIEM2_8_F) |
                                      (1ull << V_ISO3_4_F) | (1ull << V_RIEM3_4_F) | (1ull << V_DIAG2_8_F) |
                                      (1ull << V_DIAG2_16_F) | (1ull << V_DIAG3_4_F) | (1ull << V_RAND2_8_F) |
@@ -71,7 +74,15 @@ static int variant_of(const agd_instance &a) {
         }
     }
     if (v >= 0 && a.factor_radius2 > 0.f) {
-        if (a.multip_step != 0.f) return -1;  // no build of factorisation with multiprecision
+        if (a.multip_step != 0.f) {
+            switch (v) {
+                case V_ISO2_16: return V_ISO2_16_FMP;
+                case V_RIEM2_8: return V_RIEM2_8_FMP;
+                case V_ISO3_4: return V_ISO3_4_FMP;
+                case V_RIEM3_4: return V_RIEM3_4_FMP;
+                default: return -1;  // no build of factorisation with multiprecision for this model / tile
+            }
+        }
         switch (v) {
             case V_ISO2_8: return V_ISO2_8_F;
             case V_ISO2_16: return V_ISO2_16_F;

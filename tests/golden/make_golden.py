@@ -727,6 +727,16 @@ def make_cases():
     sens.reshape(-1)[rng.choice(int(np.prod(sh)), 24, replace=False)] = 1.0
     c["sensitivity"] = sens
     cases["riem3_32"] = c
+    # source factorisation with multiprecision (the reference composes the two)
+    for key in ("riem2_factor", "iso2_factor"):
+        c = {k: v for k, v in cases[key].items() if k not in ("tips", "sensitivity")}
+        c["multiprecision"] = True
+        cases[key + "_mp"] = c
+    c = {k: v for k, v in cases["riem3"].items() if k not in ("tips", "sensitivity")}
+    c["seeds"] = np.array([[0.45, 0.5, 0.48]], np.float32)
+    c["factoringRadius"] = 5.0
+    c["multiprecision"] = True
+    cases["riem3_factor_mp"] = c
     return cases
 
 

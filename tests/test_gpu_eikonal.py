@@ -296,3 +296,18 @@ def test_other_solvers_reach_the_discrete_solution(solver, name):
         si = {2: 16 if case["model"].startswith("Iso") else 8, 3: 4}[len(shape)]
         ntiles = int(np.prod([-(-s // si) for s in shape]))
         assert st["nupdate_o_total"] == st["niter_o"] * ntiles
+
+
+@pytest.mark.parametrize("name", ["riem2_factor_mp", "iso2_factor_mp", "riem3_factor_mp"])
+def test_factorisation_with_multiprecision_vs_reference(name):
+    """Source factorisation together with multiprecision: against the
+    reference's own kernels built with both (absolute stopping test: two
+    tolerances), also with float64 values."""
+    case, ref = load_case(name)
+    want = ref["values"]
+    fin = np.isfinite(want)
+    for extra in ({"exportValues": True}, {"exportValues": True, "values_float64": True}):
+        out = make_dictin(case, extra=dict(extra, multiprecision=True)).Run()
+        v = out["values"].cpu().numpy()
+        assert np.array_equal(fin, np.isfinite(v))
+        assert np.abs(v[fin] - want[fin]).max() <= 2 * float(ref["atol"])

@@ -199,3 +199,18 @@ def test_active_neighs(name):
     r = O.eikonal(O.prepare(case), np.float32, flow=True)
     bits = sum((w > 0).astype(np.int32) << k for k, w in enumerate(r["flow_weights"]))
     assert np.array_equal(bits, ref["activeNeighs"])
+
+
+@pytest.mark.parametrize("name", ["riem2_factor_mp", "iso2_factor_mp", "riem3_factor_mp"])
+def test_factor_multiprecision_fixtures(name):
+    """The reference's source factorisation with multiprecision (its kernels
+    built with both macros) against the float64 oracle's factored discrete
+    solution: within the absolute stopping tolerance (rtol = 0 with
+    multiprecision)."""
+    case, ref = load_case(name)
+    c = {k: v for k, v in case.items() if k != "multiprecision"}
+    r = O.run(dict(c, atol=1e-12, rtol=1e-12), np.float64)
+    v = ref["values"]
+    fin = np.isfinite(v)
+    assert np.array_equal(fin, np.isfinite(r["values"]))
+    assert np.abs(v[fin] - r["values"][fin]).max() <= float(ref["atol"])
