@@ -1,8 +1,9 @@
 """Repeated batched solves of one problem configuration (the serving path).
 
 A template dictIn fixes the model, the grid, the tile traits, the tolerances and
-the solver options; every submission brings the per-instance data of a batch
-(metrics or costs, seeds, seed values) as arrays with a leading batch axis.
+the solver options (and, optionally, obstacles shared by every instance); every
+submission brings the per-instance data of a batch (metrics or costs, seeds,
+seed values, optionally obstacles) as arrays with a leading batch axis.
 Device buffers and the solver plan are made once.  A submission queues on its
 own CUDA stream: the upload of the host inputs (without blocking the host when
 they are page-locked), two batched preparation kernels (agd_prep_batch), the
@@ -34,7 +35,7 @@ class _Buffers:
         self.stream = torch.cuda.Stream()
         with torch.cuda.stream(self.stream):  # owned by this stream for the allocator
             dev = dict(dtype=torch.float32, device="cuda")
-            self.geom = torch.empty((s.batch, s.symdim * s.size_tot), **dev) if s.riemann else None
+            self.geom = torch.empty((s.batch, s.nmet * s.size_tot), **dev) if s.nmet else None
             self.rhs = torch.empty((s.batch, s.size_tot), **dev)
             self.values = torch.empty((s.batch, s.size_tot), **dev)
             self.seedbits = torch.empty((s.batch, s.size_tot // 8), dtype=torch.uint8, device="cuda")
@@ -45,9 +46,10 @@ class _Buffers:
         self.bad_host = torch.empty(1, dtype=torch.int32).pin_memory()
         self.metric = self.cost = self.seed_index = self.seed_values = None  # staging, made on first use
         self.release = None  # tile release epochs (batch, tiles) uint16, made on first use
+        self.wall_dist = None  # per-instance wall distances (batch, size_tot) uint8, made on first use
+        self.trigger = None  # first tiles with walls (batch, tiles) uint8, made on first use
         self.plan = None
-        self.plan_atol = None
-        self.plan_gated = False
+        self.plan_key = None
         self.ws = None
         self.job = None
 
@@ -104,41 +106,55 @@ class BatchSolver:
     """Solves batches of `batch` instances of the configuration of `template`.
 
     template: a dictIn whose keys (model, dims/gridScale(s)/origin, traits,
-    tol/atol/rtol, nitermax_o, fim_front_width, ...) apply to every instance; it
-    may hold data of one instance (metric, cost, seeds), which is read only to
-    check the keys.  submit(metric=, cost=, seeds=, seedValues=, out=) takes
-    arrays with a leading batch axis: metric (batch, *shape, symdim) HFM packing
-    (Riemann models), cost (batch, *shape) (required by Isotropic models,
-    optional for Riemann), seeds (batch, nseeds, ndim) points, seedValues
-    (batch, nseeds).  Host tensors are copied in (page-locked ones without
-    blocking), device tensors are read in place."""
+    tol/atol/rtol, nitermax_o, fim_front_width, walls, wallDistBound, ...) apply
+    to every instance; it may hold data of one instance (metric, cost, seeds),
+    which is read only to check the keys.  submit(metric=, cost=, seeds=,
+    seedValues=, walls=, out=) takes arrays with a leading batch axis: metric
+    (batch, *shape, k) in HFM packing (Riemann: k = symdim; Diagonal: the costs
+    per axis, k = ndim; Rander: metric then drift, k = symdim + ndim), cost
+    (batch, *shape) (required by Isotropic models, optional for the others),
+    seeds (batch, nseeds, ndim) points, seedValues (batch, nseeds), walls
+    (batch, *shape) booleans (instead of the template's walls).  Host tensors
+    are copied in (page-locked ones without blocking), device tensors are read
+    in place."""
+
+    _MODELS = ("Riemann", "Isotropic", "Diagonal", "Rander")
 
     def __init__(self, template, batch, nbuffers=2, launch=None):
         if batch < 1 or nbuffers < 1:
             raise ValueError("batch and nbuffers must be positive")
-        if "metric" not in template and "dualMetric" not in template and str(template["model"]).startswith("Riemann"):
+        model = str(template["model"])
+        if "metric" not in template and "dualMetric" not in template and model[:-1] in ("Riemann", "Diagonal", "Rander"):
             # the configuration needs no data: a constant metric stands in for the check of the keys
             template = template.copy()
-            nd = int(str(template["model"])[-1])
-            template["metric"] = np.eye(nd, dtype=np.float32)[np.tril_indices(nd)]
+            nd = int(model[-1])
+            eye = np.eye(nd, dtype=np.float32)[np.tril_indices(nd)]
+            template["metric"] = {"Riemann": eye, "Diagonal": np.ones(nd, np.float32),
+                                  "Rander": np.concatenate([eye, np.zeros(nd, np.float32)])}[model[:-1]]
         itf = Interface(template)
         itf.SetKernelTraits()
         itf.SetGeometry()
         if itf.multiprecision:
             raise NotImplementedError("BatchSolver: multiprecision instances go through RunBatch")
-        for key in ("tips", "sensitivity", "exportGeodesicFlow", "walls", "seedRadius", "speed", "dualMetric"):
+        for key in ("tips", "sensitivity", "exportGeodesicFlow", "seedRadius", "speed", "dualMetric"):
             if key in template and template[key] is not None and template[key] is not False:
                 raise NotImplementedError(f"BatchSolver: key {key!r} is not available on the batched path")
         self.template = template
         self.batch, self.nbuffers = int(batch), int(nbuffers)
         self.model = itf.model
-        if itf.model_ not in ("Riemann", "Isotropic"):
+        if itf.model_ not in self._MODELS:
             raise NotImplementedError(f"BatchSolver: model {itf.model} goes through RunGPU / RunBatch")
+        self.model_code = {"Riemann": _lib.AGD_MODEL_RIEMANN, "Isotropic": _lib.AGD_MODEL_ISOTROPIC,
+                           "Diagonal": _lib.AGD_MODEL_DIAGONAL, "Rander": _lib.AGD_MODEL_RANDER}[itf.model_]
         self.riemann = itf.model_ == "Riemann"
         self.ndim = itf.ndim
+        self.symdim = self.ndim * (self.ndim + 1) // 2
+        # metric floats per point (and geometry planes)
+        self.nmet = {"Riemann": self.symdim, "Isotropic": 0, "Diagonal": self.ndim,
+                     "Rander": self.symdim + self.ndim}[itf.model_]
         self.shape, self.shape_i = tuple(itf.shape), tuple(itf.shape_i)
         self.size_tot = itf.size_tot
-        self.symdim = self.ndim * (self.ndim + 1) // 2
+        self.ntiles = self.size_tot // int(np.prod(self.shape_i))
         self.h = np.asarray(itf.h, np.float32)
         bottom, _ = template.corners
         self.start = (bottom + 0.5 * self.h).astype(np.float32)
@@ -153,6 +169,19 @@ class BatchSolver:
         self.launch = launch
         self.c_shape = (ctypes.c_int * 3)(*self.shape, *([1] * (3 - self.ndim)))
         self.c_shape_i = (ctypes.c_int * 3)(*self.shape_i, *([1] * (3 - self.ndim)))
+        # obstacles of the template, shared by every instance: mask and wall distances made once
+        self.wallDistBound = int(template["wallDistBound"]) if "wallDistBound" in template else 10
+        if not 0 <= self.wallDistBound <= 254:
+            raise ValueError("wallDistBound must lie in [0, 254]")
+        self.walls = self.wall_dist = None
+        if getattr(itf, "walls", None) is not None:
+            self.walls = itf.walls  # uint8 device tensor, grid layout
+            self.wall_dist = torch.empty(self.size_tot, dtype=torch.uint8, device="cuda")
+            tmp = torch.empty(2 * int(np.prod(self.shape)), dtype=torch.uint8, device="cuda")
+            _lib.check(_lib.lib().agd_prep_walls(self.ndim, self.c_shape, self.c_shape_i, _lib.ptr(self.walls),
+                                                 self.wallDistBound, _lib.ptr(self.wall_dist), _lib.ptr(tmp), None,
+                                                 None, _lib.stream_ptr()), "walls")
+            torch.cuda.current_stream().synchronize()
         self._bufs = [_Buffers(self) for _ in range(self.nbuffers)]
         self._next = 0
         self.submitted = 0
@@ -180,14 +209,17 @@ class BatchSolver:
         mean = torch.nanmean(c.reshape(self.batch, -1).float(), dim=1).cpu().numpy().astype(np.float64)
         return (mean * _FLOAT_RES * 5.0).astype(np.float32)
 
-    def _plan(self, buf, atol, gated=False):
-        if buf.plan is not None and np.array_equal(buf.plan_atol, atol) and buf.plan_gated == gated:
+    def _plan(self, buf, atol, gated=False, walls=None):
+        """The plan of the buffer set; walls: None, "shared" (the template's) or
+        "batch" (per-instance wall distances in buf.wall_dist)."""
+        key = (atol.tobytes(), gated, walls)
+        if buf.plan is not None and buf.plan_key == key:
             return
         L = _lib.lib()
         arr = (_lib.AgdInstance * self.batch)()
         for i in range(self.batch):
             inst = arr[i]
-            inst.model = _lib.AGD_MODEL_RIEMANN if self.riemann else _lib.AGD_MODEL_ISOTROPIC
+            inst.model = self.model_code
             inst.ndim = self.ndim
             for k in range(3):
                 inst.shape[k] = self.c_shape[k]
@@ -197,18 +229,20 @@ class BatchSolver:
             inst.flags = self.flags
             inst.atol, inst.rtol = float(atol[i]), float(self.rtol)
             inst.values = buf.values[i].data_ptr()
-            inst.geom = buf.geom[i].data_ptr() if self.riemann else None
+            inst.geom = buf.geom[i].data_ptr() if self.nmet else None
             inst.rhs = buf.rhs[i].data_ptr()
             inst.seedbits = buf.seedbits[i].data_ptr()
             if gated:
                 inst.release = buf.release[i].data_ptr()
+            if walls is not None:
+                inst.wall_dist = (self.wall_dist if walls == "shared" else buf.wall_dist[i]).data_ptr()
+                inst.trigger = buf.trigger[i].data_ptr()
         plan = ctypes.c_void_p()
         _lib.check(L.agd_plan_create(arr, self.batch, ctypes.byref(plan)), "plan")
         if buf.plan is not None:
             L.agd_plan_destroy(buf.plan)
         buf.plan = plan
-        buf.plan_atol = atol
-        buf.plan_gated = gated
+        buf.plan_key = key
         nbytes = int(L.agd_plan_workspace_bytes(plan))
         if buf.ws is None or buf.ws.numel() < nbytes:
             with torch.cuda.stream(buf.stream):
@@ -238,9 +272,12 @@ class BatchSolver:
         return d
 
     # ----------------------------------------------------------------- submit --
-    def submit(self, metric=None, cost=None, seeds=None, seedValues=None, out=None, release=None, values=None):
+    def submit(self, metric=None, cost=None, seeds=None, seedValues=None, out=None, release=None, values=None,
+               walls=None):
         """Queues one batch; returns a SolverJob.  out: optional host tensor
         (batch, *shape) float32 (page-locked for an asynchronous copy).
+        walls: optional (batch, *shape) obstacle masks of the instances, in
+        place of the template's (whose wall distances are made once).
         release: optional device tensor (batch, tiles) of int16/uint16 tile
         release epochs (agd_instance.release; the learned schedule); values:
         optional device tensor (batch, tiles * tile size) of initial values in
@@ -248,11 +285,11 @@ class BatchSolver:
         only decrease), instead of +inf."""
         if seeds is None:
             raise ValueError("Missing value for key seeds")
-        if self.riemann and metric is None:
+        if self.nmet and metric is None:
             raise ValueError("Missing value for key metric")
-        if not self.riemann and cost is None:
+        if not self.nmet and cost is None:
             raise ValueError("Missing value for key cost")
-        if not self.riemann and metric is not None:
+        if not self.nmet and metric is not None:
             raise ValueError("Isotropic models take a cost, not a metric")
         if out is not None and (tuple(out.shape) != (self.batch,) + self.shape or out.dtype != torch.float32):
             raise ValueError(f"out must be a float32 tensor of shape {(self.batch,) + self.shape}")
@@ -265,25 +302,45 @@ class BatchSolver:
         L = _lib.lib()
         with torch.cuda.stream(buf.stream):
             buf.stream.wait_stream(user_stream)  # device inputs made on the caller's stream
+            ntiles = self.ntiles
             if release is not None:
-                ntiles = self.size_tot // int(np.prod(self.shape_i))
                 if tuple(release.shape) != (self.batch, ntiles) or release.dtype not in (torch.int16, torch.uint16):
                     raise ValueError(f"release must be a 16-bit tensor of shape {(self.batch, ntiles)}")
                 if buf.release is None:
                     buf.release = torch.empty((self.batch, ntiles), dtype=torch.int16, device="cuda")
                 buf.release.copy_(release.view(torch.int16))
-            self._plan(buf, atol, gated=release is not None)
+            wmode, wmask = None, None
+            if walls is not None:
+                wmask = self._stage(buf, "walls_mask", walls if isinstance(walls, torch.Tensor)
+                                    else np.asarray(walls, np.uint8), (self.batch,) + self.shape, torch.uint8)
+                if buf.wall_dist is None:
+                    buf.wall_dist = torch.empty((self.batch, self.size_tot), dtype=torch.uint8, device="cuda")
+                    buf.walls_tmp = torch.empty(2 * self.batch * int(np.prod(self.shape)), dtype=torch.uint8,
+                                                device="cuda")
+                _lib.check(L.agd_prep_walls_batch(self.ndim, self.c_shape, self.c_shape_i, self.batch,
+                                                  _lib.ptr(wmask), self.wallDistBound, _lib.ptr(buf.wall_dist),
+                                                  _lib.ptr(buf.walls_tmp), _lib.stream_ptr(buf.stream)), "walls")
+                wmode = "batch"
+            elif self.walls is not None:
+                wmode, wmask = "shared", self.walls
+            if wmode is not None and buf.trigger is None:
+                buf.trigger = torch.empty((self.batch, ntiles), dtype=torch.uint8, device="cuda")
+            self._plan(buf, atol, gated=release is not None, walls=wmode)
             prep = _lib.AgdBatchPrep()
-            prep.model = _lib.AGD_MODEL_RIEMANN if self.riemann else _lib.AGD_MODEL_ISOTROPIC
+            prep.model = self.model_code
             prep.ndim, prep.n = self.ndim, self.batch
             for k in range(3):
                 prep.shape[k], prep.shape_i[k] = self.c_shape[k], self.c_shape_i[k]
                 prep.grid_scales[k] = float(self.h[k]) if k < self.ndim else 1.0
             keep = []
-            if self.riemann:
-                m = self._stage(buf, "metric", metric, (self.batch,) + self.shape + (self.symdim,))
+            if self.nmet:
+                m = self._stage(buf, "metric", metric, (self.batch,) + self.shape + (self.nmet,))
                 keep.append(m)
                 prep.metric, prep.geom = m.data_ptr(), buf.geom.data_ptr()
+            if wmode is not None:
+                keep.append(wmask)
+                prep.walls, prep.walls_shared = wmask.data_ptr(), int(wmode == "shared")
+                prep.trigger = buf.trigger.data_ptr()
             if cost is not None:
                 c = self._stage(buf, "cost", cost, (self.batch,) + self.shape)
                 keep.append(c)

@@ -89,7 +89,8 @@ def SubmitBatch(hfmIns, launch=None):
 # Keys that the batched preparation takes (anything else: instance by instance).
 _UNIFORM_KEYS = {"model", "mode", "arrayOrdering", "verbosity", "dims", "gridScale", "gridScales", "origin",
                  "metric", "cost", "seeds", "seedValues", "exportValues", "tol", "atol", "rtol", "traits",
-                 "nitermax_o", "fim_front_width", "raiseOnNonConvergence", "solver", "projective"}
+                 "nitermax_o", "fim_front_width", "raiseOnNonConvergence", "solver", "projective", "walls",
+                 "wallDistBound"}
 _UNIFORM_DATA = {"metric", "cost", "seeds", "seedValues"}
 _uniform_solvers = OrderedDict()  # configuration -> (BatchSolver, key bookkeeping of one instance)
 
@@ -120,10 +121,11 @@ def _submit_uniform(hfmIns, launch):
         return None
     h0 = hfmIns[0]
     model = h0.get("model")
-    if model not in ("Riemann2", "Riemann3", "Isotropic2", "Isotropic3"):
+    if model not in ("Riemann2", "Riemann3", "Isotropic2", "Isotropic3", "Diagonal2", "Diagonal3", "Rander2",
+                     "Rander3"):
         return None
     keys0 = set(h0.keys())
-    data = "metric" if model.startswith("Riemann") else "cost"
+    data = "cost" if model.startswith("Isotropic") else "metric"
     if not keys0 <= _UNIFORM_KEYS or data not in keys0 or "seeds" not in keys0:
         return None
     opts = sorted(keys0 - _UNIFORM_DATA - {"verbosity"})
@@ -457,9 +459,9 @@ class Interface:
         self.order = int(order)
         self.order2_threshold = 0.0
         if order == 2:
-            if self.multiprecision or self.factoringRadius:
-                raise NotImplementedError("the second order scheme with multiprecision or source factorization "
-                                          "is not available in this build")
+            if self.multiprecision and self.factoringRadius:
+                raise NotImplementedError("the second order scheme with both multiprecision and source "
+                                          "factorization is not available in this build")
             self.order2_threshold = float(self.GetValue(  # _Kernel.py:310-314
                 "order2_threshold", 0.3,
                 help="Relative threshold on second order differences / first order difference,"

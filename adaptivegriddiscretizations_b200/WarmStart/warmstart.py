@@ -180,6 +180,28 @@ class WarmStart:
         torch.cuda.synchronize()
         return out, e0.elapsed_time(e1) / 1e3 + t_solve, visits
 
+    def judge(self, warm, cold, tol_factor=8.0):
+        """Instances (batch,) whose warm values differ from the cold ones by more
+        than tol_factor stopping tolerances somewhere: they fall back to the
+        cold result.  Two solves that each meet the parity criteria (within 4
+        stopping tolerances of the discrete solution) are within 8 of each other."""
+        B = warm.shape[0]
+        fin = torch.isfinite(cold)
+        diff = (warm - cold).abs()
+        atol = float(np.float32(1.0 * np.finfo(np.float32).resolution * 5.0))
+        bad = (diff > tol_factor * (atol + float(self.solver.rtol) * cold.abs())) & fin
+        bad |= torch.isfinite(warm) != fin
+        return bad.reshape(B, -1).any(1)
+
+    def judged_solve(self, metric, seeds, margin=None, tol_factor=8.0):
+        """The warm solve with the cold solve as judge and fallback: values
+        (batch, n, n) (device tensor) and the fallback mask (batch,)."""
+        cold, _, _ = self.solve(metric, seeds)
+        cold = cold.clone()
+        warm, _, _ = self.warm_solve(metric, seeds, margin=margin)
+        bad = self.judge(warm, cold, tol_factor)
+        return torch.where(bad.reshape(-1, *([1] * (cold.dim() - 1))), cold, warm), bad
+
     def tune(self, metric, seeds, candidates=(100.0, 130.0, 160.0, 200.0, 260.0)):
         """Chooses the release epoch scale on one batch: the fastest gated solve."""
         pred = self.predict(metric, seeds)
@@ -207,7 +229,6 @@ class WarmStart:
         t_cold = t_warm = 0.0
         v_cold = v_warm = 0
         worst, fallbacks, done = 0.0, 0, 0
-        rtol = float(self.solver.rtol)
         while done < nheld:
             metric, seeds = riemann2_fields(self.n, B, gen)
             cold, tc, vc = self.solve(metric, seeds)
@@ -221,9 +242,7 @@ class WarmStart:
             diff = (warm - cold).abs()
             rel = torch.where(fin, diff / cold.abs().clamp_min(1e-30), torch.zeros_like(diff))
             worst = max(worst, float(rel.max()))
-            atol = float(np.float32(1.0 * np.finfo(np.float32).resolution * 5.0))
-            bad = (diff > tol_factor * (atol + rtol * cold.abs())) & fin
-            fallbacks += int(bad.reshape(B, -1).any(1).sum())
+            fallbacks += int(self.judge(warm, cold, tol_factor).sum())
             done += B
         return {"instances": done, "cold_solves_per_s": done / t_cold, "warm_solves_per_s": done / t_warm,
                 "gain": t_cold / t_warm, "cold_tile_visits": v_cold, "warm_tile_visits": v_warm,

@@ -60,7 +60,8 @@ class AgdBatchPrep(ctypes.Structure):
         ("metric", ctypes.c_void_p), ("cost", ctypes.c_void_p), ("seed_index", ctypes.c_void_p),
         ("seed_values", ctypes.c_void_p), ("nseeds", ctypes.c_int), ("geom", ctypes.c_void_p),
         ("rhs", ctypes.c_void_p), ("values", ctypes.c_void_p), ("seedbits", ctypes.c_void_p),
-        ("bad_seed", ctypes.c_void_p),
+        ("bad_seed", ctypes.c_void_p), ("walls", ctypes.c_void_p), ("walls_shared", ctypes.c_int),
+        ("trigger", ctypes.c_void_p),
     ]
 
 
@@ -98,6 +99,7 @@ SIGNATURES = {
     "agd_prep_seeds": (_I, [_I, _P, _P, _P, _P, _I, _P, _P, _P, _P]),
     "agd_prep_batch": (_I, [_P, _P]),
     "agd_prep_walls": (_I, [_I, _P, _P, _P, _I, _P, _P, _P, _P, _P]),
+    "agd_prep_walls_batch": (_I, [_I, _P, _P, _I, _P, _I, _P, _P, _P]),
     "agd_selling": (_I, [_I, _P, _I, _P, _P, _P]),
     "agd_voronoi_decomposition": (_I, [_I, _P, ctypes.c_longlong, _P, _P, _I, _P]),
     "agd_flow": (_I, [_P, _P, _P, _P, _P, _P]),

@@ -223,9 +223,26 @@ __device__ __forceinline__ float factor_dot(const float *m, const float *x, cons
     return r;
 }
 
-// Shifts f[2k], f[2k+1] of the neighbours x -/+ e_k of grid point xt (0 outside the radius).
+// Second order scheme: the shifts g0, g1 of the neighbours x - 2e and x + 2e,
+// g0 = 2 f0 - ((|x| - |x-e|) + (|x-2e| - |x-e|)) and likewise on the other
+// side (the second differences of the norm |x| - 2|x-e| + |x-2e| added to the
+// first order shift; cuda/EuclideanFactor.h:20-28), each difference of norms
+// again a quotient.
+__device__ __forceinline__ void factor_pair2(float xx, float xe, float ee, float f0, float f1, float &g0,
+                                             float &g1) {
+    const float nx = sqrtf(xx), nm = sqrtf(xx - 2.f * xe + ee), np = sqrtf(xx + 2.f * xe + ee);
+    const float nm2 = sqrtf(xx - 4.f * xe + 4.f * ee), np2 = sqrtf(xx + 4.f * xe + 4.f * ee);
+    const float d0 = (2.f * xe - ee) / (nx + nm), d1 = (-2.f * xe - ee) / (nx + np);  // |x| - |x-/+e|
+    const float e0 = (-2.f * xe + 3.f * ee) / (nm + nm2), e1 = (2.f * xe + 3.f * ee) / (np + np2);  // |x-/+2e| - |x-/+e|
+    g0 = 2.f * f0 - (d0 + e0);
+    g1 = 2.f * f1 - (d1 + e1);
+}
+
+// Shifts f[2k], f[2k+1] of the neighbours x -/+ e_k of grid point xt (0 outside
+// the radius); with f2, those of x -/+ 2 e_k for the second order scheme.
 template <int D, int NACT, bool DIAG>
-__device__ __forceinline__ void factor_shifts(const agd_instance &A, const int *xt, const int (*e)[3], float *f) {
+__device__ __forceinline__ void factor_shifts(const agd_instance &A, const int *xt, const int (*e)[3], float *f,
+                                              float *f2 = nullptr) {
     float xr[3] = {0.f, 0.f, 0.f}, r2 = 0.f;
 #pragma unroll
     for (int c = 0; c < D; ++c) {
@@ -239,11 +256,18 @@ __device__ __forceinline__ void factor_shifts(const agd_instance &A, const int *
         float ek[3] = {0.f, 0.f, 0.f};
 #pragma unroll
         for (int c = 0; c < D; ++c) ek[c] = float(e[k][c]);
-        float f0 = 0.f, f1 = 0.f;
-        if (in) factor_pair(xx, factor_dot<D, DIAG>(A.factor_metric, xr, ek), factor_dot<D, DIAG>(A.factor_metric, ek, ek),
-                            f0, f1);
+        float f0 = 0.f, f1 = 0.f, g0 = 0.f, g1 = 0.f;
+        if (in) {
+            const float xe = factor_dot<D, DIAG>(A.factor_metric, xr, ek), ee = factor_dot<D, DIAG>(A.factor_metric, ek, ek);
+            factor_pair(xx, xe, ee, f0, f1);
+            if (f2) factor_pair2(xx, xe, ee, f0, f1, g0, g1);
+        }
         f[2 * k] = f0;
         f[2 * k + 1] = f1;
+        if (f2) {
+            f2[2 * k] = g0;
+            f2[2 * k + 1] = g1;
+        }
     }
 }
 

@@ -31,8 +31,9 @@ int set_cuda_error(const char *what, cudaError_t err = cudaGetLastError());
 
 // Min-plus distance map in grid layout (geodesic.cu): 0 at the mask points,
 // `npasses` passes of the 3^ndim kernel round(5 |o|) (l1 false) or |o|_1 (l1
-// true), saturated at 255, values above `cut` set to 255.  tmp: prod(shape) bytes.
+// true), saturated at 255, values above `cut` set to 255; nb instances one
+// after the other, each its own map.  tmp: nb prod(shape) bytes.
 int distance_map(int ndim, const int *shape, const uint8_t *mask, int npasses, int cut, bool l1, uint8_t *out,
-                 uint8_t *tmp, cudaStream_t st);
+                 uint8_t *tmp, cudaStream_t st, int nb = 1);
 
 }  // namespace agd

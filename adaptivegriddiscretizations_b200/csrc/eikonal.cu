@@ -428,6 +428,9 @@ struct Visit {
         int nbq[MP ? P : 1][MP ? NTOT : 1];
         unsigned nba[kSlots ? P : 1][kSlots ? NTOT : 1];
         float fsh[SHIFT ? P : 1][SHIFT ? NTOT : 1];  // factorisation and drift shifts of the neighbour values
+        // second order with factorisation: the shifts of the neighbours two steps away
+        float fsh2[FACT && ORD2 ? P : 1][FACT && ORD2 ? NTOT : 1];
+        int nbq2[MP && ORD2 ? P : 1][MP && ORD2 ? NTOT : 1];  // their integer parts (multiprecision)
         // second order: the neighbours two steps away, as nba / nbv
         unsigned nba2[ORD2 && kSlots ? P : 1][ORD2 && kSlots ? NTOT : 1];
         float nbv2[ORD2 && !kSlots ? P : 1][ORD2 && !kSlots ? NTOT : 1];
@@ -470,7 +473,8 @@ struct Visit {
             stencil_decode(I, raw[p], wts[p], ev, hide);
             if constexpr (SHIFT) {
                 if constexpr (FACT) {
-                    factor_shifts<D, NACT, !kSelling>(A, xt, ev, fsh[p]);
+                    if constexpr (ORD2) factor_shifts<D, NACT, !kSelling>(A, xt, ev, fsh[p], fsh2[p]);
+                    else factor_shifts<D, NACT, !kSelling>(A, xt, ev, fsh[p]);
                 } else {
 #pragma unroll
                     for (int k = 0; k < NTOT; ++k) fsh[p][k] = 0.f;
@@ -530,8 +534,11 @@ struct Visit {
                             }
                             nba2[p][2 * k + s] = us_addr + 4u * (unsigned)slot;
                         } else {
-                            nbv2[p][2 * k + s] = in2 ? __int_as_float(kBoxed | TL::local(yi))
-                                                     : (dom2 ? __ldcg(u_in + bilevel_index<D, TL>(yt, I.shape_o)) : finf());
+                            const int ny2 = dom2 ? bilevel_index<D, TL>(yt, I.shape_o) : 0;
+                            float v2o = dom2 ? __ldcg(u_in + ny2) : finf();
+                            if constexpr (FACT) v2o += fsh2[p][2 * k + s];  // outside the tile: value + shift
+                            nbv2[p][2 * k + s] = in2 ? __int_as_float(kBoxed | TL::local(yi)) : v2o;
+                            if constexpr (MP) nbq2[p][2 * k + s] = (!in2 && dom2) ? __ldcg(q_in + ny2) : 0;
                         }
                     }
                 }
@@ -551,6 +558,7 @@ struct Visit {
                     if (seed[p]) continue;
                     float v[NACT], w[NACT];
                     int vq[NACT];
+                    int side[ORD2 ? NACT : 1];
 #pragma unroll
                     for (int k = 0; k < NACT; ++k) {
                         float a, b;
@@ -565,6 +573,7 @@ struct Visit {
                         v[k] = take_b ? b : a;
                         vq[k] = take_b ? bq : aq;
                         w[k] = wts[p][k];
+                        if constexpr (ORD2) side[k] = take_b;
                     }
                     int vqmin = kIntMax;  // HFM.h:79-87
 #pragma unroll
@@ -572,6 +581,27 @@ struct Visit {
                         if (v[k] < finf()) vqmin = min(vqmin, vq[k]);
 #pragma unroll
                     for (int k = 0; k < NACT; ++k) v[k] += (float)(vq[k] - vqmin) * step;
+                    if constexpr (ORD2) {
+                        // second order with multiprecision (HFM.h:89-135): the point's value and
+                        // the farther neighbours' relative to the integer part vqmin; a farther
+                        // neighbour inside the tile takes its factorisation shift after that,
+                        // one outside carries it in its float part already
+                        const int n_i = lane + 32 * p;
+                        if (vqmin != kIntMax) {
+                            const float u0 = us[n_i] + (float)(uqs[n_i] - vqmin) * step;
+                            order2(u0, v, w, side, [&](int k, int sd) {
+                                const float x = nbv2[p][2 * k + sd];
+                                const int b = __float_as_int(x);
+                                if ((b >> 22) == -1) {
+                                    const int li = b & (TL::SIZE - 1);
+                                    float r = us[li] + (float)(uqs[li] - vqmin) * step;
+                                    if constexpr (FACT) r += fsh2[p][2 * k + sd];
+                                    return r;
+                                }
+                                return x + (float)(nbq2[p][2 * k + sd] - vqmin) * step;
+                            }, A.order2_threshold);
+                        }
+                    }
                     float c = hfm_update<NACT>(rhs[p], v, w);
                     int cq = vqmin;
                     if (c == finf()) cq = 0;
@@ -617,8 +647,19 @@ struct Visit {
                             if constexpr (ORD2) side[k] = a > b;
                         }
                         if constexpr (ORD2) order2(us[n_i], v, w, side, [&](int k, int sd) {
-                            if constexpr (kSlots) return lds(nba2[p][2 * k + sd]);
-                            else return neighbour(nbv2[p][2 * k + sd], us);
+                            // (with factorisation, the shift of x +/- 2 e_k; outside the tile
+                            // without slots nbv2 carries it already)
+                            if constexpr (kSlots) {
+                                float r = lds(nba2[p][2 * k + sd]);
+                                if constexpr (FACT) r += fsh2[p][2 * k + sd];
+                                return r;
+                            } else {
+                                const float x = nbv2[p][2 * k + sd];
+                                if ((__float_as_int(x) >> 22) != -1) return x;
+                                float r = us[__float_as_int(x) & (TL::SIZE - 1)];
+                                if constexpr (FACT) r += fsh2[p][2 * k + sd];
+                                return r;
+                            }
                         }, A.order2_threshold);
                         cand = hfm_update<NACT>(rhs[p], v, w);
                     }
@@ -699,8 +740,7 @@ struct Visit {
 };
 
 template <unsigned long long VMASK>
-__device__ __forceinline__ void dispatch(const Sched &S, int t, int e, int lane, float *us) {
-    const int ii = __ldg(S.tile_inst + t);
+__device__ __forceinline__ void dispatch(const Sched &S, int t, int ii, int e, int lane, float *us) {
     const Inst &I = S.inst[ii];
     const int n_o = t - I.tile_base;
     switch (I.variant) {
@@ -751,6 +791,30 @@ __device__ __forceinline__ void dispatch(const Sched &S, int t, int e, int lane,
             break;
         case V_RIEM3_4_FMP:
             if constexpr ((VMASK >> V_RIEM3_4_FMP) & 1) Visit<Tile<3, 4, 4, 4>, AGD_MODEL_RIEMANN, true, true, false, true>::run(S, I, ii, n_o, e, lane, us);
+            break;
+        case V_ISO2_16_O2F:
+            if constexpr ((VMASK >> V_ISO2_16_O2F) & 1) Visit<Tile<2, 16, 16, 1>, AGD_MODEL_ISOTROPIC, false, true, true>::run(S, I, ii, n_o, e, lane, us);
+            break;
+        case V_RIEM2_8_O2F:
+            if constexpr ((VMASK >> V_RIEM2_8_O2F) & 1) Visit<Tile<2, 8, 8, 1>, AGD_MODEL_RIEMANN, false, true, true, true>::run(S, I, ii, n_o, e, lane, us);
+            break;
+        case V_ISO3_4_O2F:
+            if constexpr ((VMASK >> V_ISO3_4_O2F) & 1) Visit<Tile<3, 4, 4, 4>, AGD_MODEL_ISOTROPIC, false, true, true>::run(S, I, ii, n_o, e, lane, us);
+            break;
+        case V_RIEM3_4_O2F:
+            if constexpr ((VMASK >> V_RIEM3_4_O2F) & 1) Visit<Tile<3, 4, 4, 4>, AGD_MODEL_RIEMANN, false, true, true, true>::run(S, I, ii, n_o, e, lane, us);
+            break;
+        case V_ISO2_16_O2MP:
+            if constexpr ((VMASK >> V_ISO2_16_O2MP) & 1) Visit<Tile<2, 16, 16, 1>, AGD_MODEL_ISOTROPIC, true, false, true>::run(S, I, ii, n_o, e, lane, us);
+            break;
+        case V_RIEM2_8_O2MP:
+            if constexpr ((VMASK >> V_RIEM2_8_O2MP) & 1) Visit<Tile<2, 8, 8, 1>, AGD_MODEL_RIEMANN, true, false, true, true>::run(S, I, ii, n_o, e, lane, us);
+            break;
+        case V_ISO3_4_O2MP:
+            if constexpr ((VMASK >> V_ISO3_4_O2MP) & 1) Visit<Tile<3, 4, 4, 4>, AGD_MODEL_ISOTROPIC, true, false, true>::run(S, I, ii, n_o, e, lane, us);
+            break;
+        case V_RIEM3_4_O2MP:
+            if constexpr ((VMASK >> V_RIEM3_4_O2MP) & 1) Visit<Tile<3, 4, 4, 4>, AGD_MODEL_RIEMANN, true, false, true, true>::run(S, I, ii, n_o, e, lane, us);
             break;
         case V_ISO2_16_F:
             if constexpr ((VMASK >> V_ISO2_16_F) & 1) Visit<Tile<2, 16, 16, 1>, AGD_MODEL_ISOTROPIC, false, true>::run(S, I, ii, n_o, e, lane, us);
@@ -902,6 +966,10 @@ constexpr int smem_floats() {
     if ((VMASK >> V_RAND3_4_F) & 1) m = std::max(m, Visit<Tile<3, 4, 4, 4>, AGD_MODEL_RANDER, false, true, false, true>::kSmemFloats);
     if ((VMASK >> V_RAND2_8_O2) & 1) m = std::max(m, Visit<Tile<2, 8, 8, 1>, AGD_MODEL_RANDER, false, false, true, true>::kSmemFloats);
     if ((VMASK >> V_RAND3_4_O2) & 1) m = std::max(m, Visit<Tile<3, 4, 4, 4>, AGD_MODEL_RANDER, false, false, true, true>::kSmemFloats);
+    if ((VMASK >> V_ISO2_16_O2F) & 1) m = std::max(m, Visit<Tile<2, 16, 16, 1>, AGD_MODEL_ISOTROPIC, false, true, true>::kSmemFloats);
+    if ((VMASK >> V_RIEM2_8_O2F) & 1) m = std::max(m, Visit<Tile<2, 8, 8, 1>, AGD_MODEL_RIEMANN, false, true, true, true>::kSmemFloats);
+    if ((VMASK >> V_ISO3_4_O2F) & 1) m = std::max(m, Visit<Tile<3, 4, 4, 4>, AGD_MODEL_ISOTROPIC, false, true, true>::kSmemFloats);
+    if ((VMASK >> V_RIEM3_4_O2F) & 1) m = std::max(m, Visit<Tile<3, 4, 4, 4>, AGD_MODEL_RIEMANN, false, true, true, true>::kSmemFloats);
     return m;
 }
 
@@ -912,7 +980,9 @@ struct EikonalVisitor {
     // multiprecision an integer part beside every value.
     // Riemann3 / Rander3: 5 CTAs at up to 96 registers (a single 200^3 solve:
     // 24.1 ms, against 26.1 ms at 6 CTAs and 80 registers with 2.5x the
-    // spills, and 29.6 ms at 7).
+    // spills, and 29.6 ms at 7).  Riemann2 8x8: 8 CTAs at up to 64 registers
+    // (48 bytes of spills; batch 128 of 512^2: +1 % over 9 CTAs at 56 registers
+    // and 96 bytes, +7 % over 10 CTAs at 48 registers and 160 bytes).
     // BULK: epochs published in batches (enqueue_warp<true>).  Its registers
     // make the variants at their budget spill (Riemann2 8x8: 164 -> 504 bytes,
     // -13 % solves/s at a batch of 128 instances), but an instance of tens of
@@ -922,20 +992,22 @@ struct EikonalVisitor {
     static constexpr bool kBulkPublish = BULK;
     static constexpr int kMinCtas =
         (VMASK & ((1ull << V_RIEM2_16) | (1ull << V_ISO2_16) | (1ull << V_ISO2_16_MP) | (1ull << V_ISO2_16_F) |
-                  (1ull << V_ISO2_16_FMP) |
+                  (1ull << V_ISO2_16_FMP) | (1ull << V_ISO2_16_O2F) | (1ull << V_ISO2_16_O2MP) |
                   (1ull << V_ISO2_16_O2) | (1ull << V_RIEM2_16_W) | (1ull << V_DIAG2_16) |
                   (1ull << V_DIAG2_16_MP) | (1ull << V_DIAG2_16_F) | (1ull << V_DIAG2_16_O2)))      ? 4
         : (VMASK & ((1ull << V_RIEM3_4) | (1ull << V_RIEM3_4_MP) | (1ull << V_RIEM3_4_F) | (1ull << V_RIEM3_4_O2) |
                     (1ull << V_RIEM3_4_W) | (1ull << V_RAND3_4) | (1ull << V_RAND3_4_W) | (1ull << V_RAND3_4_MP) |
-                    (1ull << V_RAND3_4_F) | (1ull << V_RAND3_4_O2) | (1ull << V_RIEM3_4_FMP)))   ? 5
+                    (1ull << V_RAND3_4_F) | (1ull << V_RAND3_4_O2) | (1ull << V_RIEM3_4_FMP) |
+                    (1ull << V_RIEM3_4_O2F) | (1ull << V_RIEM3_4_O2MP)))                          ? 5
         : (VMASK & (kMpVariants | kFactorVariants | kOrder2Variants))                                ? 7
+        : (VMASK & (1ull << V_RIEM2_8))                                                              ? 8
                                                                                                      : 9;
     struct Args {};
     struct Smem {
         float u[smem_floats<VMASK>()];  // values, then out-of-tile neighbours or integer parts
     };
-    __device__ __forceinline__ static void visit(const Sched &S, const Args &, int t, int, int e, int lane, Smem &sm) {
-        dispatch<VMASK>(S, t, e, lane, sm.u);
+    __device__ __forceinline__ static void visit(const Sched &S, const Args &, int t, int ii, int e, int lane, Smem &sm) {
+        dispatch<VMASK>(S, t, ii, e, lane, sm.u);
     }
     // Before the workers: the second buffers of multiprecision instances start
     // as copies of the first (_SetArgs.py:171-177), and the Selling stencils of
@@ -945,18 +1017,22 @@ struct EikonalVisitor {
                                       (1ull << V_RIEM2_8_MP) | (1ull << V_RIEM3_4_MP) | (1ull << V_RIEM2_8_F) |
                                       (1ull << V_RIEM3_4_F) | (1ull << V_RIEM2_8_O2) | (1ull << V_RIEM3_4_O2) |
                                       (1ull << V_RIEM2_8_FMP) | (1ull << V_RIEM3_4_FMP) | kWallVariants |
-                                      kRanderVariants;
+                                      kRanderVariants | (1ull << V_RIEM2_8_O2F) | (1ull << V_RIEM3_4_O2F) |
+                                      (1ull << V_RIEM2_8_O2MP) | (1ull << V_RIEM3_4_O2MP);
         if (VMASK & kMpVariants) mp_copy_kernel<<<(L.total_tiles + 7) / 8, 256, 0, st>>>(S, 0);
         if (!(VMASK & kRiemann) || L.stencil == L.total) return cudaGetLastError();
         // variants that read the hidden-neighbour bits: the walls pass follows
         constexpr unsigned long long kWallCapable = kWallVariants | (1ull << V_RIEM2_8_MP) | (1ull << V_RIEM3_4_MP) |
                                           (1ull << V_RIEM2_8_F) | (1ull << V_RIEM3_4_F) | (1ull << V_RIEM2_8_O2) |
                                           (1ull << V_RIEM3_4_O2) | (1ull << V_RIEM2_8_FMP) | (1ull << V_RIEM3_4_FMP) |
+                                          (1ull << V_RIEM2_8_O2F) | (1ull << V_RIEM3_4_O2F) | (1ull << V_RIEM2_8_O2MP) |
+                                          (1ull << V_RIEM3_4_O2MP) |
                                           (kRanderVariants & ~((1ull << V_RAND2_8) | (1ull << V_RAND3_4)));
         const unsigned grid = (L.total_tiles + 7) / 8;
         if (VMASK & ((1ull << V_RIEM3_4) | (1ull << V_RIEM3_4_MP) | (1ull << V_RIEM3_4_F) | (1ull << V_RIEM3_4_O2) |
                      (1ull << V_RIEM3_4_W) | (1ull << V_RAND3_4) | (1ull << V_RAND3_4_W) | (1ull << V_RAND3_4_MP) |
-                     (1ull << V_RAND3_4_F) | (1ull << V_RAND3_4_O2) | (1ull << V_RIEM3_4_FMP))) {
+                     (1ull << V_RAND3_4_F) | (1ull << V_RAND3_4_O2) | (1ull << V_RIEM3_4_FMP) |
+                     (1ull << V_RIEM3_4_O2F) | (1ull << V_RIEM3_4_O2MP))) {
             stencil_kernel<3><<<grid, 256, 0, st>>>(S.inst, S.ninst, L.total_tiles, S.ctrl);
             if (VMASK & kWallCapable) stencil_walls_kernel<3><<<grid, 256, 0, st>>>(S.inst, S.ninst, L.total_tiles);
         } else {
@@ -1079,6 +1155,20 @@ static int run_variants(int ndim, unsigned long long vmask, const WsLayout &L, v
         if (f) return run_sched<EikonalVisitor<DF3 | D3>>(L, ws, n, {}, stats, cfg, st);
         if (mp) return run_sched<EikonalVisitor<DMP3 | D3>>(L, ws, n, {}, stats, cfg, st);
         return run_sched<EikonalVisitor<D3>>(L, ws, n, {}, stats, cfg, st);
+    }
+    if (vmask & (kOrder2FactorVariants | kOrder2MpVariants)) {  // second order with factorisation or multiprecision
+        const bool f = vmask & kOrder2FactorVariants, mp = vmask & kOrder2MpVariants;
+        if ((f && mp) || (vmask & ~(kOrder2FactorVariants | kOrder2MpVariants)))
+            return set_error(AGD_STATUS_UNSUPPORTED,
+                             "second order with factorisation or multiprecision beside other instances in one plan");
+        constexpr unsigned long long OF2 = (1ull << V_ISO2_16_O2F) | (1ull << V_RIEM2_8_O2F);
+        constexpr unsigned long long OF3 = (1ull << V_ISO3_4_O2F) | (1ull << V_RIEM3_4_O2F);
+        constexpr unsigned long long OM2 = (1ull << V_ISO2_16_O2MP) | (1ull << V_RIEM2_8_O2MP);
+        constexpr unsigned long long OM3 = (1ull << V_ISO3_4_O2MP) | (1ull << V_RIEM3_4_O2MP);
+        if (ndim == 2) return f ? run_sched<EikonalVisitor<OF2>>(L, ws, n, {}, stats, cfg, st)
+                                : run_sched<EikonalVisitor<OM2>>(L, ws, n, {}, stats, cfg, st);
+        return f ? run_sched<EikonalVisitor<OF3>>(L, ws, n, {}, stats, cfg, st)
+                 : run_sched<EikonalVisitor<OM3>>(L, ws, n, {}, stats, cfg, st);
     }
     if (vmask & kOrder2Variants) {  // second order instances, possibly beside plain ones
         constexpr unsigned long long O2 = (1ull << V_ISO2_8_O2) | (1ull << V_ISO2_16_O2) | (1ull << V_RIEM2_8_O2);
@@ -1235,9 +1325,12 @@ __global__ void flow_kernel(Inst I, float *fvec, float *fwsum, float *fw, int *f
 #pragma unroll
         for (int k = 0; k < NACT; ++k)
             hide[k] = hidden_bits<D>(A, wd0, xt, ev[k], [&](const int *y) { return bilevel_index<D, TL>(y, I.shape_o); });
-        float v[NACT], fsh[2 * NACT];
+        float v[NACT], fsh[2 * NACT], fsh2[2 * NACT];
+#pragma unroll
+        for (int k = 0; k < 2 * NACT; ++k) fsh2[k] = 0.f;
         if (A.factor_radius2 > 0.f) {
-            factor_shifts<D, NACT, !V::kSelling>(A, xt, ev, fsh);
+            if (A.order2_threshold > 0.f) factor_shifts<D, NACT, !V::kSelling>(A, xt, ev, fsh, fsh2);
+            else factor_shifts<D, NACT, !V::kSelling>(A, xt, ev, fsh);
         } else {
 #pragma unroll
             for (int k = 0; k < 2 * NACT; ++k) fsh[k] = 0.f;
@@ -1280,7 +1373,7 @@ __global__ void flow_kernel(Inst I, float *fvec, float *fwsum, float *fw, int *f
                         y[c] = xt[c] + 2 * (2 * sd - 1) * ev[k][c];
                         ok = ok && y[c] >= 0 && y[c] < A.shape[c];
                     }
-                    return ok ? __ldg(A.values + bilevel_index<D, TL>(y, I.shape_o)) : finf();
+                    return (ok ? __ldg(A.values + bilevel_index<D, TL>(y, I.shape_o)) : finf()) + fsh2[2 * k + sd];
                 }, A.order2_threshold);
 #pragma unroll
                 for (int k = 0; k < NACT; ++k) v[k] = vs[k];
@@ -1464,6 +1557,13 @@ __global__ void prep_geom_kernel(Geo g, const float *metric, int bcast, int is_d
 // Diagonal model: the squared dual costs 1/(c_k h_k)^2 of metric.with_costs(h)
 // (or (d_k / h_k)^2 of dualMetric.with_speeds(h)) per axis, in float as the
 // reference forms them (_SetGeometry.py:134-135), +inf at padding.
+__device__ __forceinline__ void diag_at(int nd, const float *c, int is_dual, const float h[3], float *out) {
+    for (int k = 0; k < nd; ++k) {
+        const float v = is_dual ? c[k] * (1.f / h[k]) : 1.f / (c[k] * h[k]);
+        out[k] = v * v;
+    }
+}
+
 __global__ void prep_diag_kernel(Geo g, const float *costs, int bcast, int is_dual, double h0, double h1, double h2,
                                  float *geom) {
     const long long n_t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
@@ -1472,15 +1572,9 @@ __global__ void prep_diag_kernel(Geo g, const float *costs, int bcast, int is_du
     long long flat;
     const bool in = grid_coords(g, n_t, x, flat);
     const float h[3] = {(float)h0, (float)h1, (float)h2};
-    for (int k = 0; k < g.nd; ++k) {
-        float w = finf();
-        if (in) {
-            const float c = bcast ? costs[k] : costs[flat * g.nd + k];
-            const float v = is_dual ? c * (1.f / h[k]) : 1.f / (c * h[k]);
-            w = v * v;
-        }
-        geom[k * g.size_tot + n_t] = w;
-    }
+    float out[3];
+    if (in) diag_at(g.nd, bcast ? costs : costs + flat * g.nd, is_dual, h, out);
+    for (int k = 0; k < g.nd; ++k) geom[k * g.size_tot + n_t] = in ? out[k] : finf();
 }
 
 // Inverse of a packed symmetric matrix [a00, a10, a11(, a20, a21, a22)] by the
@@ -1506,22 +1600,11 @@ __device__ __forceinline__ void sym_inverse(int nd, const float *s, float *out) 
 // metric: scaled by with_speeds(h), then turned into the metric by
 // rander.py:35-39, m = (1 + <w_d, s w_d>) s, w = -s w_d with s = (m_d - w_d w_d^T)^-1,
 // so that the inverse of m is (m_d - w_d w_d^T) / (1 + <w_d, s w_d>).
-__global__ void prep_rander_kernel(Geo g, const float *metric, int bcast, int is_dual, double h0, double h1,
-                                   double h2, float *geom) {
-    const long long n_t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-    if (n_t >= g.size_tot) return;
-    const int nd = g.nd, sd = nd * (nd + 1) / 2;
-    int x[3];
-    long long flat;
-    const bool in = grid_coords(g, n_t, x, flat);
-    if (!in) {
-        for (int c = 0; c < sd + nd; ++c) geom[c * g.size_tot + n_t] = finf();
-        return;
-    }
-    const float hh[3] = {(float)h0, (float)h1, (float)h2};
+// out: the sd planes of the inverse metric, then the nd of the drift.
+__device__ __forceinline__ void rander_at(int nd, const float *src, int is_dual, const float hh[3], float *out) {
+    const int sd = nd * (nd + 1) / 2;
     float hs[3];  // the grid scales (metric), or their inverses (with_speeds of a dual metric)
     for (int k = 0; k < nd; ++k) hs[k] = is_dual ? 1.f / hh[k] : hh[k];
-    const float *src = bcast ? metric : metric + flat * (sd + nd);
     float m[6], w[3], mi[6];
     int q = 0;
     for (int i = 0; i < nd; ++i)
@@ -1542,8 +1625,22 @@ __global__ void prep_rander_kernel(Geo g, const float *metric, int bcast, int is
         for (int c = 0; c < sd; ++c) mi[c] = t[c] / (1.f + wo);
         for (int k = 0; k < nd; ++k) w[k] = -om[k];
     }
-    for (int c = 0; c < sd; ++c) geom[c * g.size_tot + n_t] = mi[c];
-    for (int k = 0; k < nd; ++k) geom[(sd + k) * g.size_tot + n_t] = w[k];
+    for (int c = 0; c < sd; ++c) out[c] = mi[c];
+    for (int k = 0; k < nd; ++k) out[sd + k] = w[k];
+}
+
+__global__ void prep_rander_kernel(Geo g, const float *metric, int bcast, int is_dual, double h0, double h1,
+                                   double h2, float *geom) {
+    const long long n_t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (n_t >= g.size_tot) return;
+    const int nd = g.nd, sd = nd * (nd + 1) / 2;
+    int x[3];
+    long long flat;
+    const bool in = grid_coords(g, n_t, x, flat);
+    const float hh[3] = {(float)h0, (float)h1, (float)h2};
+    float out[9];
+    if (in) rander_at(nd, bcast ? metric : metric + flat * (sd + nd), is_dual, hh, out);
+    for (int c = 0; c < sd + nd; ++c) geom[c * g.size_tot + n_t] = in ? out[c] : finf();
 }
 
 // Seed bits: one 32-bit word (32 points) per thread, padding bits set.
@@ -1560,23 +1657,26 @@ __global__ void seedbits_init_kernel(Geo g, unsigned *bits) {
 }
 
 // Seeds in order (a later duplicate overrides an earlier one, as numpy assignment does).
+// walls (grid layout, or NULL): a seed on a wall keeps the wall's +inf right-hand
+// side, since the reference writes the walls after the seeds.
 __device__ void place_seeds(const Geo &g, const int *idx, const float *vals, int n, float *rhs, unsigned *bits,
-                            unsigned char *trigger, int *bad) {
+                            unsigned char *trigger, int *bad, const uint8_t *walls = nullptr) {
     for (int s = 0; s < n; ++s) {
-        long long n_o = 0, n_i = 0;
+        long long n_o = 0, n_i = 0, flat = 0;
         bool ok = true;
         for (int k = 0; k < g.nd; ++k) {
             const int xk = idx[s * g.nd + k];
             ok = ok && xk >= 0 && xk < g.shape[k];
             n_o = n_o * g.so[k] + (ok ? xk / g.si[k] : 0);
             n_i = n_i * g.si[k] + (ok ? xk % g.si[k] : 0);
+            flat = flat * g.shape[k] + (ok ? xk : 0);
         }
         if (!ok) {
             if (bad) *bad = 1;
             continue;
         }
         const long long n_t = n_o * g.size_i + n_i;
-        if (rhs) rhs[n_t] = vals ? vals[s] : 0.f;
+        if (rhs && !(walls && walls[flat])) rhs[n_t] = vals ? vals[s] : 0.f;
         if (bits) bits[n_t >> 5] |= 1u << (n_t & 31);
         if (trigger) trigger[n_o] = 1;
     }
@@ -1591,13 +1691,18 @@ __global__ void seeds_kernel(Geo g, const int *idx, const float *vals, int n, fl
 struct BatchPrep {
     Geo g;
     int si_log2[3];  // log2 of the tile sides, or -1 (all) if one is not a power of two
-    int n, sd, riemann, is_dual, nseeds;
+    int n, model, is_dual, nseeds;
+    int nmet, ngeom;  // metric floats per point, geometry planes
     float h[3];
     const float *metric, *cost, *seed_values;
     const int *seed_index;
     float *geom, *rhs, *values;
     unsigned *bits;
     int *bad;
+    const uint8_t *walls;
+    long long walls_stride;  // 0: one mask for every instance
+    uint8_t *trigger;
+    long long size_o;  // tiles of an instance
 };
 
 // Bilevel index -> grid coordinates for instances of fewer than 2^31 points,
@@ -1646,15 +1751,22 @@ __global__ void prep_batch_kernel(BatchPrep A) {
         const long long i = (long long)inst * size_tot + n_t;
         int flat;
         const bool in = grid_coords32(A.g, A.si_log2, n_t, flat);
+        const bool wall = in && A.walls && A.walls[inst * A.walls_stride + flat];
         A.values[i] = finf();
-        A.rhs[i] = in ? (A.cost ? A.cost[inst * A.g.n + flat] : 1.f) : finf();
-        if (A.riemann) {
-            float out[6];
-            if (in) geom_at(A.g.nd, A.metric + (inst * A.g.n + flat) * A.sd, A.is_dual, A.h, out);
-            float *geo = A.geom + (long long)inst * A.sd * A.g.size_tot + n_t;
-            for (int c = 0; c < A.sd; ++c) geo[c * A.g.size_tot] = in ? out[c] : finf();
+        A.rhs[i] = in && !wall ? (A.cost ? A.cost[inst * A.g.n + flat] : 1.f) : finf();
+        if (A.ngeom) {
+            float out[9];
+            if (in) {
+                const float *m = A.metric + (inst * A.g.n + flat) * A.nmet;
+                if (A.model == AGD_MODEL_RIEMANN) geom_at(A.g.nd, m, A.is_dual, A.h, out);
+                else if (A.model == AGD_MODEL_DIAGONAL) diag_at(A.g.nd, m, A.is_dual, A.h, out);
+                else rander_at(A.g.nd, m, A.is_dual, A.h, out);
+            }
+            float *geo = A.geom + (long long)inst * A.ngeom * A.g.size_tot + n_t;
+            for (int c = 0; c < A.ngeom; ++c) geo[c * A.g.size_tot] = in ? out[c] : finf();
         }
-        const unsigned pad = __ballot_sync(0xffffffffu, !in);
+        if (A.trigger && n_t % A.g.size_i == 0) A.trigger[inst * A.size_o + n_t / A.g.size_i] = 0;
+        const unsigned pad = __ballot_sync(0xffffffffu, !in || wall);
         if ((threadIdx.x & 31) == 0) A.bits[i >> 5] = pad;
     }
 }
@@ -1664,7 +1776,9 @@ __global__ void seeds_batch_kernel(BatchPrep A) {
     if (inst >= A.n) return;
     place_seeds(A.g, A.seed_index + (long long)inst * A.nseeds * A.g.nd,
                 A.seed_values ? A.seed_values + (long long)inst * A.nseeds : nullptr, A.nseeds,
-                A.rhs + inst * A.g.size_tot, A.bits + inst * (A.g.size_tot / 32), nullptr, A.bad);
+                A.rhs + inst * A.g.size_tot, A.bits + inst * (A.g.size_tot / 32),
+                A.trigger ? A.trigger + inst * A.size_o : nullptr, A.bad,
+                A.walls ? A.walls + inst * A.walls_stride : nullptr);
 }
 
 // Wall distances in tile layout (255 at padding); with rhs / bits, the wall
@@ -1683,6 +1797,17 @@ __global__ void walls_kernel(Geo g, const uint8_t *walls, const uint8_t *dist, u
     if (wall && rhs) rhs[n_t] = finf();
     const unsigned word = __ballot_sync(kFull, wall);
     if (bits && word && (threadIdx.x & 31) == 0) bits[n_t >> 5] |= word;
+}
+
+// Wall distances of nb instances, grid layout (dist) -> tile layout (255 at padding).
+__global__ void wall_dist_batch_kernel(Geo g, int nb, const uint8_t *dist, uint8_t *wall_dist) {
+    const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (i >= g.size_tot * nb) return;
+    const long long inst = i / g.size_tot, n_t = i - inst * g.size_tot;
+    int x[3];
+    long long flat;
+    const bool in = grid_coords(g, n_t, x, flat);
+    wall_dist[i] = in ? dist[inst * g.n + flat] : (uint8_t)255;
 }
 
 // Selling's decomposition of n packed symmetric matrices in the planar layouts
@@ -1887,17 +2012,29 @@ int agd_prep_batch(const agd_batch_prep *p, agd_stream_t stream) {
         (g.size_tot % 32) != 0 || p->nseeds < 0 || (p->nseeds > 0 && !p->seed_index) || !p->rhs ||
         !p->values || !p->seedbits)
         return set_error(AGD_STATUS_INVALID, "agd_prep_batch: bad arguments");
-    const bool riemann = p->model == AGD_MODEL_RIEMANN;
-    if (!riemann && p->model != AGD_MODEL_ISOTROPIC)
-        return set_error(AGD_STATUS_INVALID, "agd_prep_batch: unknown model");
-    if (riemann && (!p->metric || !p->geom))
-        return set_error(AGD_STATUS_INVALID, "agd_prep_batch: Riemann instances need metric and geom");
+    const int sd = p->ndim * (p->ndim + 1) / 2;
+    int nmet = 0;
+    switch (p->model) {
+        case AGD_MODEL_ISOTROPIC: nmet = 0; break;
+        case AGD_MODEL_RIEMANN: nmet = sd; break;
+        case AGD_MODEL_DIAGONAL: nmet = p->ndim; break;
+        case AGD_MODEL_RANDER: nmet = sd + p->ndim; break;
+        default: return set_error(AGD_STATUS_INVALID, "agd_prep_batch: unknown model");
+    }
+    if (nmet && (!p->metric || !p->geom))
+        return set_error(AGD_STATUS_INVALID,
+                         "agd_prep_batch: Riemann, Diagonal and Rander instances need metric and geom");
     BatchPrep A;
     A.g = g;
     A.n = p->n;
-    A.sd = p->ndim * (p->ndim + 1) / 2;
-    A.riemann = riemann;
+    A.model = p->model;
+    A.nmet = nmet;
+    A.ngeom = nmet;  // the geometry planes of these models are as many as the metric's floats
     A.is_dual = p->is_dual;
+    A.walls = p->walls;
+    A.walls_stride = p->walls_shared ? 0 : g.n;
+    A.trigger = p->trigger;
+    A.size_o = g.size_tot / g.size_i;
     A.nseeds = p->nseeds;
     for (int k = 0; k < 3; ++k) A.h[k] = k < p->ndim ? (float)p->grid_scales[k] : 1.f;
     A.metric = p->metric;
@@ -1944,6 +2081,22 @@ int agd_prep_walls(int ndim, const int *shape, const int *shape_i, const uint8_t
                                                                        reinterpret_cast<unsigned *>(seedbits));
     const cudaError_t err = cudaGetLastError();
     return err == cudaSuccess ? AGD_STATUS_OK : set_cuda_error("prep_walls", err);
+}
+
+int agd_prep_walls_batch(int ndim, const int *shape, const int *shape_i, int n, const uint8_t *walls, int bound,
+                         uint8_t *wall_dist, uint8_t *tmp, agd_stream_t stream) {
+    clear_error();
+    Geo g;
+    if ((ndim != 2 && ndim != 3) || !shape || !shape_i || !geo_of(ndim, shape, shape_i, g) || n < 1 || !walls ||
+        !wall_dist || !tmp || bound < 0 || bound > 254)
+        return set_error(AGD_STATUS_INVALID, "agd_prep_walls_batch: bad arguments (bound in [0, 254])");
+    cudaStream_t st = (cudaStream_t)stream;
+    const long long np = g.n * n;  // grid points of all the instances
+    const int rc = distance_map(ndim, shape, walls, bound, bound, true, tmp, tmp + np, st, n);
+    if (rc != AGD_STATUS_OK) return rc;
+    wall_dist_batch_kernel<<<blocks_for(g.size_tot * n, 256), 256, 0, st>>>(g, n, tmp, wall_dist);
+    const cudaError_t err = cudaGetLastError();
+    return err == cudaSuccess ? AGD_STATUS_OK : set_cuda_error("prep_walls_batch", err);
 }
 
 int agd_voronoi_decomposition(int ndim, const float *m, long long n, float *weights, void *offsets, int offset_bytes,

@@ -22,7 +22,8 @@ namespace agd {
 // ------------------------------------------------------ distance to seeds ---
 struct EGeo {
     int nd, shape[3];
-    long long n;
+    long long n;  // points of one instance
+    int nb;       // instances, one after the other
 };
 
 // One min-plus pass: out(x) = min over the 3^d neighbours y of min(255, in(y) + k(y - x)),
@@ -42,15 +43,17 @@ __global__ void __launch_bounds__(256) infconv_kernel(EGeo g, const uint8_t *__r
     long long stride[D];
     stride[D - 1] = 1;
     for (int k = D - 2; k >= 0; --k) stride[k] = stride[k + 1] * g.shape[k + 1];
-    for (long long r = blockIdx.y * (long long)blockDim.y + threadIdx.y; r < nrows;
+    // rows of all the instances; a neighbour is one of the same instance
+    for (long long r = blockIdx.y * (long long)blockDim.y + threadIdx.y; r < nrows * g.nb;
          r += (long long)gridDim.y * blockDim.y) {
+        const long long rr = r % nrows;  // row within the instance
         int x[D];
         x[D - 1] = c;
         if (D == 3) {
-            x[0] = (int)(r / g.shape[1]);
-            x[1] = (int)(r - (long long)x[0] * g.shape[1]);
+            x[0] = (int)(rr / g.shape[1]);
+            x[1] = (int)(rr - (long long)x[0] * g.shape[1]);
         } else {
-            x[0] = (int)r;
+            x[0] = (int)rr;
         }
         const long long p = r * nlast + c;
         int best = 255;
@@ -82,7 +85,7 @@ template <int D>
 static void infconv_pass(const EGeo &g, const uint8_t *in, bool from_mask, bool cut_it, int l1, int cut,
                          uint8_t *out, cudaStream_t st) {
     const dim3 block(32, 8);
-    const long long nrows = g.n / g.shape[D - 1];
+    const long long nrows = g.n / g.shape[D - 1] * g.nb;
     const dim3 grid((unsigned)((g.shape[D - 1] + 31) / 32), (unsigned)std::min<long long>((nrows + 7) / 8, 16384));
     if (from_mask && cut_it) infconv_kernel<D, true, true><<<grid, block, 0, st>>>(g, in, l1, cut, out);
     else if (from_mask) infconv_kernel<D, true, false><<<grid, block, 0, st>>>(g, in, l1, cut, out);
@@ -92,12 +95,12 @@ static void infconv_pass(const EGeo &g, const uint8_t *in, bool from_mask, bool 
 
 __global__ void eucl_init_kernel(EGeo g, const uint8_t *mask, uint8_t *out) {
     const long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-    if (p < g.n) out[p] = mask[p] ? 0 : 255;
+    if (p < g.n * g.nb) out[p] = mask[p] ? 0 : 255;
 }
 
 __global__ void eucl_cut_kernel(EGeo g, const uint8_t *in, int cut, uint8_t *out) {
     const long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-    if (p < g.n) out[p] = in[p] > cut ? 255 : in[p];
+    if (p < g.n * g.nb) out[p] = in[p] > cut ? 255 : in[p];
 }
 
 // ------------------------------------------------------------ geodesics ---
@@ -385,13 +388,15 @@ static inline unsigned nblocks(long long n, int bs) { return (unsigned)((n + bs 
 // then `npasses` passes of infconv_kernel and values above `cut` set to 255.
 // The first pass reads the mask and the last one applies the cut; the passes
 // alternate between `out` and `tmp` so that the last one writes `out`.
-// tmp: scratch of prod(shape) bytes.
+// nb instances one after the other, each its own map.  tmp: scratch of nb
+// prod(shape) bytes.
 int distance_map(int ndim, const int *shape, const uint8_t *mask, int npasses, int cut, bool l1, uint8_t *out,
-                 uint8_t *tmp, cudaStream_t st) {
-    if ((ndim != 2 && ndim != 3) || !shape || !mask || !out || !tmp || npasses < 0)
+                 uint8_t *tmp, cudaStream_t st, int nb) {
+    if ((ndim != 2 && ndim != 3) || !shape || !mask || !out || !tmp || npasses < 0 || nb < 1)
         return set_error(AGD_STATUS_INVALID, "distance map: bad arguments");
     EGeo g;
     g.nd = ndim;
+    g.nb = nb;
     g.n = 1;
     for (int k = 0; k < 3; ++k) g.shape[k] = 1;
     for (int k = 0; k < ndim; ++k) {
@@ -401,8 +406,8 @@ int distance_map(int ndim, const int *shape, const uint8_t *mask, int npasses, i
     }
     const int bs = 256;
     if (npasses == 0) {
-        eucl_init_kernel<<<nblocks(g.n, bs), bs, 0, st>>>(g, mask, tmp);
-        eucl_cut_kernel<<<nblocks(g.n, bs), bs, 0, st>>>(g, tmp, cut, out);
+        eucl_init_kernel<<<nblocks(g.n * nb, bs), bs, 0, st>>>(g, mask, tmp);
+        eucl_cut_kernel<<<nblocks(g.n * nb, bs), bs, 0, st>>>(g, tmp, cut, out);
     } else {
         const uint8_t *src = mask;
         for (int it = 0; it < npasses; ++it) {

@@ -32,14 +32,18 @@ enum Variant {
     V_RAND2_8, V_RAND3_4, V_RAND2_8_W, V_RAND3_4_W, V_RAND2_8_MP, V_RAND3_4_MP, V_RAND2_8_F, V_RAND3_4_F,
     V_RAND2_8_O2, V_RAND3_4_O2,
     // source factorisation with multiprecision (the default tile shapes)
-    V_ISO2_16_FMP, V_RIEM2_8_FMP, V_ISO3_4_FMP, V_RIEM3_4_FMP, V_COUNT
+    V_ISO2_16_FMP, V_RIEM2_8_FMP, V_ISO3_4_FMP, V_RIEM3_4_FMP,
+    // second order scheme with source factorisation, and with multiprecision
+    V_ISO2_16_O2F, V_RIEM2_8_O2F, V_ISO3_4_O2F, V_RIEM3_4_O2F,
+    V_ISO2_16_O2MP, V_RIEM2_8_O2MP, V_ISO3_4_O2MP, V_RIEM3_4_O2MP, V_COUNT
 };
 static_assert(V_COUNT <= 64, "variant masks are 64-bit");
 constexpr unsigned long long kMpVariants = (1ull << V_ISO2_8_MP) | (1ull << V_ISO2_16_MP) | (1ull << V_RIEM2_8_MP) |
                                  (1ull << V_ISO3_4_MP) | (1ull << V_RIEM3_4_MP) | (1ull << V_DIAG2_8_MP) |
                                  (1ull << V_DIAG2_16_MP) | (1ull << V_DIAG3_4_MP) | (1ull << V_RAND2_8_MP) |
                                  (1ull << V_RAND3_4_MP) | (1ull << V_ISO2_16_FMP) | (1ull << V_RIEM2_8_FMP) |
-                                 (1ull << V_ISO3_4_FMP) | (1ull << V_RIEM3_4_FMP);
+                                 (1ull << V_ISO3_4_FMP) | (1ull << V_RIEM3_4_FMP) | (1ull << V_ISO2_16_O2MP) |
+                                 (1ull << V_RIEM2_8_O2MP) | (1ull << V_ISO3_4_O2MP) | (1ull << V_RIEM3_4_O2MP);
 constexpr unsigned long long kFactorVariants = (1ull << V_ISO2_8_F) | (1ull << V_ISO2_16_F) | (1ull << V_RIEM2_8_F) |
                                      (1ull << V_ISO3_4_F) | (1ull << V_RIEM3_4_F) | (1ull << V_DIAG2_8_F) |
                                      (1ull << V_DIAG2_16_F) | (1ull << V_DIAG3_4_F) | (1ull << V_RAND2_8_F) |
@@ -47,7 +51,14 @@ constexpr unsigned long long kFactorVariants = (1ull << V_ISO2_8_F) | (1ull << V
 constexpr unsigned long long kOrder2Variants = (1ull << V_ISO2_8_O2) | (1ull << V_ISO2_16_O2) | (1ull << V_RIEM2_8_O2) |
                                      (1ull << V_ISO3_4_O2) | (1ull << V_RIEM3_4_O2) | (1ull << V_DIAG2_8_O2) |
                                      (1ull << V_DIAG2_16_O2) | (1ull << V_DIAG3_4_O2) | (1ull << V_RAND2_8_O2) |
-                                     (1ull << V_RAND3_4_O2);
+                                     (1ull << V_RAND3_4_O2) | (1ull << V_ISO2_16_O2F) | (1ull << V_RIEM2_8_O2F) |
+                                     (1ull << V_ISO3_4_O2F) | (1ull << V_RIEM3_4_O2F) | (1ull << V_ISO2_16_O2MP) |
+                                     (1ull << V_RIEM2_8_O2MP) | (1ull << V_ISO3_4_O2MP) | (1ull << V_RIEM3_4_O2MP);
+// second order with factorisation / with multiprecision
+constexpr unsigned long long kOrder2FactorVariants = (1ull << V_ISO2_16_O2F) | (1ull << V_RIEM2_8_O2F) |
+                                           (1ull << V_ISO3_4_O2F) | (1ull << V_RIEM3_4_O2F);
+constexpr unsigned long long kOrder2MpVariants = (1ull << V_ISO2_16_O2MP) | (1ull << V_RIEM2_8_O2MP) |
+                                       (1ull << V_ISO3_4_O2MP) | (1ull << V_RIEM3_4_O2MP);
 constexpr unsigned long long kWallVariants = (1ull << V_RIEM2_8_W) | (1ull << V_RIEM2_16_W) | (1ull << V_RIEM3_4_W) |
                                            (1ull << V_RAND2_8_W) | (1ull << V_RAND3_4_W);
 constexpr unsigned long long kDiagVariants = ((1ull << (V_DIAG3_4_O2 + 1)) - 1) & ~((1ull << V_DIAG2_8) - 1);
@@ -58,7 +69,17 @@ static int base_variant_of(const agd_instance &a);
 static int variant_of(const agd_instance &a) {
     const int v = base_variant_of(a);
     if (v >= 0 && a.order2_threshold > 0.f) {
-        if (a.multip_step != 0.f || a.factor_radius2 > 0.f) return -1;  // not built
+        const bool mp = a.multip_step != 0.f, fact = a.factor_radius2 > 0.f;
+        if (mp && fact) return -1;  // not built
+        if (mp || fact) {  // the default tile shapes
+            switch (v) {
+                case V_ISO2_16: return mp ? V_ISO2_16_O2MP : V_ISO2_16_O2F;
+                case V_RIEM2_8: return mp ? V_RIEM2_8_O2MP : V_RIEM2_8_O2F;
+                case V_ISO3_4: return mp ? V_ISO3_4_O2MP : V_ISO3_4_O2F;
+                case V_RIEM3_4: return mp ? V_RIEM3_4_O2MP : V_RIEM3_4_O2F;
+                default: return -1;
+            }
+        }
         switch (v) {
             case V_ISO2_8: return V_ISO2_8_O2;
             case V_ISO2_16: return V_ISO2_16_O2;
@@ -168,7 +189,7 @@ struct Ctrl {
 
 // Workspace: [Inst][InstState][tile_inst][lists][flags][score0][score1][queue][Ctrl][stats]
 struct WsLayout {
-    size_t inst, istate, tile_inst, lists, flags, score0, score1, queue, ctrl, stats, stencil, total;
+    size_t inst, istate, tile_inst, lists, flags, bits, score0, score1, queue, ctrl, stats, stencil, total;
     int total_tiles;
     int nlists;  // epoch lists per instance (2, or kMaxLists with release epochs)
     unsigned qcap;
@@ -211,8 +232,9 @@ static bool layout(const agd_instance *a, int n, WsLayout &L, Inst *out, bool st
         if (out) out[i] = I;
     }
     // Queue slots: at most `tiles` entries are outstanding (an instance's current
-    // epoch list), plus the tickets held by waiting warps and the exit sentinels.
-    const unsigned qcap = (unsigned)(2 * tiles + 2 * kMaxWarps) | 1u;  // odd: see kSlotEmpty
+    // epoch list), plus the tickets held by waiting warps (up to 4 a warp) and
+    // the exit sentinels (as many).
+    const unsigned qcap = (unsigned)(2 * tiles + 10 * kMaxWarps) | 1u;  // odd: see kSlotEmpty
     size_t off = 0;
     L.inst = off; off = align256(off + sizeof(Inst) * n);
     L.istate = off; off = align256(off + sizeof(InstState) * n);
@@ -220,6 +242,7 @@ static bool layout(const agd_instance *a, int n, WsLayout &L, Inst *out, bool st
     L.nlists = gated ? kMaxLists : 2;
     L.lists = off; off = align256(off + sizeof(int) * tiles * L.nlists);
     L.flags = off; off = align256(off + sizeof(unsigned) * tiles);
+    L.bits = off; off = align256(off + sizeof(unsigned) * 3 * ((tiles + 31) / 32));
     L.score0 = off; off = align256(off + sizeof(unsigned) * tiles);
     L.score1 = off; off = align256(off + sizeof(unsigned) * tiles);
     L.queue = off; off = align256(off + sizeof(unsigned long long) * qcap);
@@ -264,6 +287,13 @@ struct Sched {
     int nwarps;  // worker warps of the launch
     int tgroup;  // queue tickets a warp takes per atomic on the head counter (1 or 2)
     unsigned long long timeout_ns;
+    // Bitmap pushes (launches of many instances without release epochs, whose
+    // epochs close_epoch_bitmap publishes): the tiles pushed for epoch r are
+    // the bits of bitmap r % 3 (tile t: bit t & 31 of word t >> 5), nwords
+    // words each.
+    unsigned *bits;
+    unsigned nwords;
+    int bitmap;
 };
 
 // Queue slot encoding: ticket (low 20 bits) << 44 | epoch << 30 | tile, empty =
@@ -316,6 +346,10 @@ __device__ __forceinline__ int *list_of(const Sched &S, const Inst &I, int epoch
 // lmask epochs ahead).  The epoch a tile is pushed for never decreases, so the
 // epoch-stamped flag keeps one entry per tile and epoch.
 __device__ __forceinline__ void push_tile(const Sched &S, const Inst &I, int ii, int t, int e) {
+    if (S.bitmap) {  // a bit per tile and epoch: repeated pushes merge, and nothing waits for the result
+        atomicOr(S.bits + (size_t)((unsigned)(e + 1) % 3u) * S.nwords + (t >> 5), 1u << (t & 31));
+        return;
+    }
     int r = e + 1;
     if (S.lmask > 1u && I.a.release) r = max(r, min((int)__ldg(I.a.release + (t - I.tile_base)), e + (int)S.lmask));
     const unsigned tag = (unsigned)r;
@@ -426,7 +460,7 @@ static __device__ void close_epoch(const Sched &S, int ii, int e, int lane) {
         }
         last = __shfl_sync(kFull, last, 0);
         if (last) {  // every instance is done: one exit sentinel per ticket a worker warp may hold
-            const int nexit = S.tgroup * S.nwarps;
+            const int nexit = 2 * S.tgroup * S.nwarps;
             unsigned start = 0;
             if (lane == 0) start = atomicAdd(&S.ctrl->tail, (unsigned)nexit);
             start = __shfl_sync(kFull, start, 0);
@@ -448,11 +482,111 @@ static __device__ void close_epoch(const Sched &S, int ii, int e, int lane) {
 }
 
 
-// Waits (lane 0) for the entry of ticket h.  Gives up with a watchdog error if
-// the queue receives no entry anywhere (no epoch of any instance ends) for
-// timeout_ns, or if an error is raised.
-__device__ __forceinline__ unsigned long long take_slot(const Sched &S, unsigned h) {
-    unsigned long long *slot = S.queue + h % S.qcap;
+// close_epoch of a bitmap launch: the tiles of epoch e + 1 are the set bits of
+// bitmap (e + 1) % 3 in the instance's range, compacted in tile order into its
+// list of epoch e + 1 (a warp prefix sum over the words) and published from
+// there.  Bitmap (e + 2) % 3, last read when epoch e - 1 closed, is cleared for
+// the pushes of epoch e + 1 before the entries go out; bitmap (e + 1) % 3 is
+// only read here, and cleared when epoch e + 2 closes.
+template <bool BULK>
+static __device__ void close_epoch_bitmap(const Sched &S, int ii, int e, int lane) {
+    const Inst &I = S.inst[ii];
+    InstState &st = S.ist[ii];
+    const int t0 = I.tile_base, t1 = I.tile_base + I.size_o;
+    const int w0 = t0 >> 5, w1 = (t1 - 1) >> 5;
+    const unsigned *B = S.bits + (size_t)((unsigned)(e + 1) % 3u) * S.nwords;
+    int *list = list_of(S, I, e + 1);
+    int n = 0;
+    for (int wb = w0; wb <= w1; wb += 32) {
+        const int w = wb + lane;
+        unsigned v = 0;
+        if (w <= w1) {
+            v = __ldcg(B + w);
+            if (w == w0) v &= ~0u << (t0 & 31);
+            if (w == (t1 >> 5)) v &= (1u << (t1 & 31)) - 1u;
+        }
+        const int c = __popc(v);
+        int incl = c;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_up_sync(kFull, incl, o);
+            if (lane >= o) incl += y;
+        }
+        int k = n + incl - c;
+        while (v) {
+            const int b = __ffs(v) - 1;
+            v &= v - 1u;
+            list[k++] = (w << 5) + b;  // the tile id
+        }
+        n += __shfl_sync(kFull, incl, 31);
+    }
+    if ((I.a.flags & AGD_FLAG_SOLVER_GLOBAL) && atomicAdd(&st.changed, 0) < e) n = 0;
+    if (n == 0 || e >= I.a.nitermax_o) {
+        int last = 0;
+        if (lane == 0) {
+            S.stats[ii].niter_o = e;
+            if (e >= I.a.nitermax_o) atomicOr(&S.stats[ii].status, (int)AGD_STATUS_NOT_CONVERGED);
+            st.done = 1;
+            __threadfence();
+            last = atomicSub(&S.ctrl->active, 1) == 1;
+        }
+        last = __shfl_sync(kFull, last, 0);
+        if (last) {
+            const int nexit = 2 * S.tgroup * S.nwarps;
+            unsigned start = 0;
+            if (lane == 0) start = atomicAdd(&S.ctrl->tail, (unsigned)nexit);
+            start = __shfl_sync(kFull, start, 0);
+            fence_acq_rel();
+            for (int k = lane; k < nexit; k += 32)
+                if (!put_slot(S, start + (unsigned)k, 0, kExitTile)) break;
+        }
+        return;
+    }
+    unsigned *C = S.bits + (size_t)((unsigned)(e + 2) % 3u) * S.nwords;
+    for (int w = w0 + lane; w <= w1; w += 32) {
+        unsigned keep = 0u;  // bits of the neighbouring instances in a shared word
+        if (w == w0) keep |= (1u << (t0 & 31)) - 1u;
+        if (w == (t1 >> 5)) keep |= ~0u << (t1 & 31);
+        if (keep) atomicAnd(C + w, keep);
+        else C[w] = 0u;
+    }
+    if (lane == 0) {
+        st.pending = n;
+        st.epoch = e + 1;
+        S.stats[ii].tile_visits += n;
+        __threadfence();
+    }
+    __syncwarp();
+    enqueue_warp<BULK>(S, list, n, e + 1, lane);
+}
+
+// Issues (lane 0) the copy of the 16 bytes that hold the queue slot of ticket h
+// into buf (shared, 16-byte aligned) without waiting for it: take_slot reads
+// it after the visit in between, so that the slot's L2 round trip overlaps the
+// visit.  The queue starts 256-byte aligned and its region is padded to a
+// multiple of 256 bytes, so the pair of the last slot stays in the workspace.
+__device__ __forceinline__ void prefetch_slot(const Sched &S, unsigned h, unsigned long long *buf) {
+    const unsigned long long *pair = S.queue + ((h % S.qcap) & ~1u);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n\tcp.async.commit_group;" ::"r"(
+                     (unsigned)__cvta_generic_to_shared(buf)), "l"(pair)
+                 : "memory");
+}
+
+// Waits (lane 0) for the entry of ticket h; pre: the pair of slots copied by
+// prefetch_slot for h, or NULL.  Gives up with a watchdog error if the queue
+// receives no entry anywhere (no epoch of any instance ends) for timeout_ns,
+// or if an error is raised.
+__device__ __forceinline__ unsigned long long take_slot(const Sched &S, unsigned h, const unsigned long long *pre) {
+    const unsigned idx = h % S.qcap;
+    unsigned long long *slot = S.queue + idx;
+    if (pre) {  // the entry was there when the copy read it: no round trip now
+        asm volatile("cp.async.wait_all;" ::: "memory");
+        const unsigned long long v = pre[idx & 1u];
+        if (v != kSlotEmpty && (unsigned)(v >> 44) == (h & 0xfffffu)) {
+            st_relaxed_u64(slot, kSlotEmpty);
+            return v;
+        }
+    }
     unsigned seen = ld_acquire(&S.ctrl->tail);
     unsigned long long t0 = globaltimer();
     unsigned backoff = 32;
@@ -501,42 +635,51 @@ template <class Visitor, int WPB>
 __global__ void __launch_bounds__(WPB * 32, Visitor::kMinCtas * 4 / WPB) sched_worker(Sched S, typename Visitor::Args VA) {
     __shared__ typename Visitor::Smem smem[WPB];
     __shared__ int s_base[kSmemInst];  // tile bases, to find a tile's instance without a global load
+    __shared__ __align__(16) unsigned long long s_pre[WPB][2];  // prefetched queue slots
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const bool inst_in_smem = S.ninst <= kSmemInst;
     if (inst_in_smem)
         for (int i = threadIdx.x; i < S.ninst; i += blockDim.x) s_base[i] = S.inst[i].tile_base;
     __syncthreads();
     if (ld_acquire_s32(&S.ctrl->active) == 0) return;  // nothing to solve
-    // Each warp holds one queue ticket ahead: the ticket for its next tile is
-    // taken when a visit starts, so the atomic's latency overlaps the visit.
-    // With tgroup 2 a warp takes two consecutive tickets per atomic: the head
-    // counter is a single address that every visit of the launch hits, and at
-    // ~250 visits/us (a batch of 128 instances) its atomics are a bound.  A
-    // warp then visits two tiles of the queue in turn, which lengthens the
-    // tail of a small epoch: one instance alone solves 11 % slower that way,
-    // so launches of fewer than kPairInstances instances take one.
-    unsigned ticket = 0;
+    // Each warp holds queue tickets ahead: when a visit starts, the ticket of
+    // its next tile is already known, so the copy of that tile's queue slot
+    // (prefetch_slot) overlaps the visit, and the atomic on the head counter
+    // that takes the group after is issued one group ahead.  With tgroup 2 a
+    // warp takes two consecutive tickets per atomic: the head counter is a
+    // single address that every visit of the launch hits, and at ~250
+    // visits/us (a batch of 128 instances) its atomics are a bound.  A warp
+    // then visits two tiles of the queue in turn, which lengthens the tail of
+    // a small epoch: one instance alone solves 11 % slower that way, so
+    // launches of fewer than kPairInstances instances take one.  A warp holds
+    // at most 2 tgroup tickets (the exit sentinels of close_epoch cover them).
+    unsigned ticket = 0, group = 0;
     int spare = 0;  // tickets of the group still ahead of `ticket`
     if (lane == 0) {
         ticket = atomicAdd(&S.ctrl->head, (unsigned)S.tgroup);
+        group = atomicAdd(&S.ctrl->head, (unsigned)S.tgroup);  // the next group
         spare = S.tgroup - 1;
     }
+    bool prefetched = false;
     while (true) {
         unsigned long long v = 0;
-        if (lane == 0) v = take_slot(S, ticket);
+        if (lane == 0) v = take_slot(S, ticket, prefetched ? s_pre[warp] : nullptr);
         v = __shfl_sync(kFull, v, 0);
         const unsigned t = (unsigned)(v & 0x3fffffffull);
         const int e = (int)((v >> 30) & 0x3fff);
-        if (t == kExitTile) break;
+        if (t == kExitTile) break;  // (take_slot has waited for this warp's copies)
         if (lane == 0) {
             if (spare > 0) {
                 ticket += 1u;
                 --spare;
             } else {
-                ticket = atomicAdd(&S.ctrl->head, (unsigned)S.tgroup);
+                ticket = group;  // its atomic was issued a group ago
                 spare = S.tgroup - 1;
+                group = atomicAdd(&S.ctrl->head, (unsigned)S.tgroup);
             }
+            prefetch_slot(S, ticket, s_pre[warp]);
         }
+        prefetched = true;
         int ii;
         if (inst_in_smem) {
             int lo = 0, hi = S.ninst - 1;
@@ -555,7 +698,8 @@ __global__ void __launch_bounds__(WPB * 32, Visitor::kMinCtas * 4 / WPB) sched_w
         lastone = __shfl_sync(kFull, lastone, 0);
         if (lastone) {
             fence_acq_rel();
-            close_epoch<Visitor::kBulkPublish>(S, ii, e, lane);
+            if (S.bitmap) close_epoch_bitmap<Visitor::kBulkPublish>(S, ii, e, lane);
+            else close_epoch<Visitor::kBulkPublish>(S, ii, e, lane);
         }
     }
 }
@@ -675,7 +819,7 @@ static int launch_workers(const Sched &S, const typename Visitor::Args &VA, int 
     ctas = std::max(1, std::min(ctas, max_ctas));
     Sched s = S;
     s.nwarps = ctas * WPB;
-    s.tgroup = S.ninst >= kPairInstances ? 2 : 1;  // exit sentinels: tgroup * nwarps <= 2 * kMaxWarps
+    s.tgroup = S.ninst >= kPairInstances ? 2 : 1;  // exit sentinels: 2 tgroup nwarps <= 4 kMaxWarps
     if (s.nwarps > kMaxWarps) return set_error(AGD_STATUS_INVALID, "too many worker warps");
     kern<<<ctas, WPB * 32, 0, st>>>(s, VA);
     const cudaError_t err = cudaGetLastError();
@@ -694,6 +838,9 @@ static Sched sched_at(const WsLayout &L, void *ws, int ninst) {
     S.lmask = (unsigned)L.nlists - 1u;
     S.ntiles = L.total_tiles;
     S.flags = reinterpret_cast<unsigned *>(w + L.flags);
+    S.bits = reinterpret_cast<unsigned *>(w + L.bits);
+    S.nwords = (unsigned)((L.total_tiles + 31) / 32);
+    S.bitmap = 0;
     S.score0 = reinterpret_cast<unsigned *>(w + L.score0);
     S.score1 = reinterpret_cast<unsigned *>(w + L.score1);
     S.queue = reinterpret_cast<unsigned long long *>(w + L.queue);
@@ -714,6 +861,11 @@ static int run_sched(const WsLayout &L, void *ws, int n, const typename Visitor:
                      const agd_launch *cfg, cudaStream_t st) {
     Sched S = sched_at(L, ws, n);
     if (cfg && cfg->timeout_ns > 0) S.timeout_ns = (unsigned long long)cfg->timeout_ns;
+    // Bitmap pushes for launches of many instances: the pushes of a visit then
+    // wait for nothing, and an epoch is published in tile order.  A single
+    // instance keeps the lists, whose push order (the front's) propagates
+    // faster within an epoch when nothing else fills the GPU.
+    S.bitmap = (!Visitor::kBulkPublish && L.nlists == 2 && n >= kPairInstances) ? 1 : 0;
     char *w = static_cast<char *>(ws);
     cudaError_t err = cudaMemsetAsync(w + L.istate, 0, sizeof(InstState) * n, st);
     if (err == cudaSuccess) err = cudaMemsetAsync(w + L.flags, 0, L.queue - L.flags, st);
@@ -728,7 +880,7 @@ static int run_sched(const WsLayout &L, void *ws, int n, const typename Visitor:
     publish_first_slots<<<(L.total_tiles + 255) / 256, 256, 0, st>>>(S, L.total_tiles);
     if ((err = cudaGetLastError()) != cudaSuccess) return set_cuda_error("publish_first", err);
     // 8-warp CTAs only where their static shared memory fits in 48 KB
-    constexpr bool kWide = sizeof(typename Visitor::Smem) * 8 + sizeof(int) * kSmemInst <= 48 * 1024;
+    constexpr bool kWide = (sizeof(typename Visitor::Smem) + 16) * 8 + sizeof(int) * kSmemInst <= 48 * 1024;
     const int rc = (kWide && cfg && cfg->warps_per_cta == 8)
                        ? launch_workers<Visitor, kWide ? 8 : 4>(S, VA, L.total_tiles, cfg, st)
                        : launch_workers<Visitor, 4>(S, VA, L.total_tiles, cfg, st);

@@ -235,32 +235,47 @@ int agd_prep_seeds(int ndim, const int *shape, const int *shape_i, const int32_t
                    agd_stream_t stream);
 
 /* Preparation of n instances that share one grid and tile shape, for repeated
- * batched solves: one launch writes, for every instance, the geometry (Riemann:
- * dual metric planes as agd_prep_geom), the right-hand side (cost, or 1, with
- * +inf padding as agd_block_expand), values = +inf and the padding seed bits;
+ * batched solves: one launch writes, for every instance, the geometry (as
+ * agd_prep_geom, agd_prep_geom_diagonal or agd_prep_geom_rander), the
+ * right-hand side (cost, or 1, with +inf padding as agd_block_expand, +inf at
+ * walls), values = +inf and the padding and wall seed bits;
  * a second launch places the seeds as agd_prep_seeds does, one thread per
  * instance, in seed order.  The reference prepares one instance per call
  * (_SetGeometry.py:16-282, _SetArgs.py:8-177); this batched form has no
  * counterpart there.  Arrays are instance-major, with the per-instance sizes
  * given beside each field. */
 typedef struct agd_batch_prep {
-    int model;                  /* AGD_MODEL_ISOTROPIC or AGD_MODEL_RIEMANN */
+    int model;                  /* AGD_MODEL_ISOTROPIC, _RIEMANN, _DIAGONAL or _RANDER */
     int ndim;                   /* 2 or 3 */
     int shape[3];               /* grid shape (unused trailing entries 1) */
     int shape_i[3];             /* tile shape */
     int n;                      /* number of instances */
-    int is_dual;                /* Riemann: `metric` holds the dual metric */
+    int is_dual;                /* `metric` holds the dual metric (speeds for Diagonal) */
     double grid_scales[3];
-    const float *metric;        /* Riemann: prod(shape) x symdim, HFM packing; NULL otherwise */
+    /* prod(shape) x k per instance, HFM packing: Riemann k = symdim (the
+     * metric), Diagonal k = ndim (the costs per axis), Rander k = symdim + ndim
+     * (metric, then drift); NULL for Isotropic */
+    const float *metric;
     const float *cost;          /* prod(shape), or NULL for cost 1 */
     const int32_t *seed_index;  /* nseeds x ndim grid indices */
     const float *seed_values;   /* nseeds, or NULL for 0 */
     int nseeds;                 /* seeds per instance (>= 0) */
-    float *geom;                /* Riemann: symdim x size_tot (tile layout); NULL otherwise */
+    float *geom;                /* planes in tile layout: symdim (Riemann), ndim (Diagonal),
+                                   symdim + ndim (Rander) x size_tot; NULL for Isotropic */
     float *rhs;                 /* size_tot */
     float *values;              /* size_tot */
     uint8_t *seedbits;          /* size_tot / 8 */
     int32_t *bad_seed;          /* device flag set to 1 for a seed outside the grid; may be NULL */
+    /* Obstacles (optional): wall mask in grid layout, prod(shape) bytes per
+     * instance, or one mask for every instance with walls_shared = 1.  Wall
+     * points become seeds of value +inf, over the seeds (_SetArgs.py:124-126);
+     * the wall distances of agd_instance.wall_dist come from agd_prep_walls or
+     * agd_prep_walls_batch. */
+    const uint8_t *walls;
+    int walls_shared;
+    /* size_o bytes per instance, or NULL: the tiles holding a seed (1) and the
+     * others (0), the first tiles of a solve with walls (_SetArgs.py:119-126) */
+    uint8_t *trigger;
 } agd_batch_prep;
 
 int agd_prep_batch(const agd_batch_prep *prep, agd_stream_t stream);
@@ -275,6 +290,14 @@ int agd_prep_batch(const agd_batch_prep *prep, agd_stream_t stream);
  * bytes of scratch. */
 int agd_prep_walls(int ndim, const int *shape, const int *shape_i, const uint8_t *walls, int bound,
                    uint8_t *wall_dist, uint8_t *tmp, float *rhs, uint8_t *seedbits, agd_stream_t stream);
+
+/* agd_prep_walls for n instances of one grid and tile shape at once (the
+ * distance maps only; the wall points become seeds in agd_prep_batch): walls
+ * n x prod(shape) bytes (grid layout), wall_dist n x size_tot bytes (tile
+ * layout), tmp 2 n prod(shape) bytes of scratch.  No counterpart in the
+ * reference, which prepares one instance per call. */
+int agd_prep_walls_batch(int ndim, const int *shape, const int *shape_i, int n, const uint8_t *walls, int bound,
+                         uint8_t *wall_dist, uint8_t *tmp, agd_stream_t stream);
 
 /* Selling decomposition of n packed symmetric matrices (symdim floats each):
  * weights (n, symdim), integer offsets (n, symdim, ndim).  Same decomposition

@@ -194,10 +194,14 @@ struct Problem {
     }
     // Shifts of the neighbour values at x - e_k (f[2k]) and x + e_k (f[2k+1]) of
     // grid point x (flat index n): the factorisation's, then the drift's
-    // +<w, e_k> and -<w, e_k> (FiniteDifferences.h:41-45).
-    void shifts(const int *x, long n, int (*e)[3], T *f) const {
+    // +<w, e_k> and -<w, e_k> (FiniteDifferences.h:41-45); f2 (or null): the
+    // factorisation's shifts of x -/+ 2 e_k for the second order scheme (the
+    // drift does not shift them).
+    void shifts(const int *x, long n, int (*e)[3], T *f, T *f2 = nullptr) const {
         for (int k = 0; k < 2 * nact; ++k) f[k] = 0;
-        factor_shifts(x, e, f);
+        if (f2)
+            for (int k = 0; k < 2 * nact; ++k) f2[k] = 0;
+        factor_shifts(x, e, f, f2);
         if (model == 3) {
             const int sd = D * (D + 1) / 2;
             for (int k = 0; k < nact; ++k) {
@@ -208,7 +212,7 @@ struct Problem {
             }
         }
     }
-    void factor_shifts(const int *x, int (*e)[3], T *f) const {
+    void factor_shifts(const int *x, int (*e)[3], T *f, T *f2 = nullptr) const {
         if (!(fact_r2 > 0)) return;
         T xr[3] = {0, 0, 0}, r2 = 0;
         for (int c = 0; c < D; ++c) {
@@ -223,8 +227,14 @@ struct Problem {
             const T xe = scal_fact(xr, ek), ee = scal_fact(ek, ek);
             const T nx = std::sqrt(xx), nm = std::sqrt(xx - 2 * xe + ee), np = std::sqrt(xx + 2 * xe + ee);
             const T g = xe / nx;                       // <e, m x> / |x|_m
-            f[2 * k] = -g + (2 * xe - ee) / (nx + nm);     // |x| - |x-e| - <e,mx>/|x|
-            f[2 * k + 1] = g + (-2 * xe - ee) / (nx + np); // |x| - |x+e| + <e,mx>/|x|
+            const T d0 = (2 * xe - ee) / (nx + nm), d1 = (-2 * xe - ee) / (nx + np);  // |x| - |x-/+e|
+            f[2 * k] = -g + d0;     // |x| - |x-e| - <e,mx>/|x|
+            f[2 * k + 1] = g + d1;  // |x| - |x+e| + <e,mx>/|x|
+            if (f2) {  // x -/+ 2e: the first order shift plus |x| - 2|x-/+e| + |x-/+2e| (EuclideanFactor.h:20-28)
+                const T nm2 = std::sqrt(xx - 4 * xe + 4 * ee), np2 = std::sqrt(xx + 4 * xe + 4 * ee);
+                f2[2 * k] = 2 * f[2 * k] - (d0 + (-2 * xe + 3 * ee) / (nm + nm2));
+                f2[2 * k + 1] = 2 * f[2 * k + 1] - (d1 + (2 * xe + 3 * ee) / (np + np2));
+            }
         }
     }
 
@@ -361,7 +371,7 @@ struct Solver {
         std::vector<long> pts(S);
         std::vector<int> xi(3 * S), xt(3 * S);
         tile_points(n_o, pts.data(), xi.data(), xt.data());
-        std::vector<T> ul(S), uold(S), rhs(S), w(S * 6), vo(S * 12), sh(S * 12, T(0)), vo2(S * 12);
+        std::vector<T> ul(S), uold(S), rhs(S), w(S * 6), vo(S * 12), sh(S * 12, T(0)), vo2(S * 12), sh2(S * 12, T(0));
         std::vector<int> vi(S * 12), vi2(S * 12);
         std::vector<char> seed(S);
         for (int n = 0; n < S; ++n) {
@@ -377,7 +387,7 @@ struct Solver {
             ul[n] = seed[n] ? rhs[n] : uold[n];
             int e[6][3];
             P.stencil(p, &w[n * 6], e);
-            if (!seed[n]) P.shifts(xt.data() + n * 3, p, e, &sh[n * 12]);
+            if (!seed[n]) P.shifts(xt.data() + n * 3, p, e, &sh[n * 12], P.order2 > 0 ? &sh2[n * 12] : nullptr);
             for (int k = 0; k < NA; ++k)
                 for (int s = 0; s < 2; ++s) {
                     const int ks = 2 * k + s, eps = 2 * s - 1;
@@ -441,7 +451,7 @@ struct Solver {
                 if (P.order2 > 0) {
                     for (int k = 0; k < NA; ++k) {
                         const int ks = 2 * k + side[k];
-                        v2[k] = vi2[n * 12 + ks] >= 0 ? ul[vi2[n * 12 + ks]] : vo2[n * 12 + ks];
+                        v2[k] = (vi2[n * 12 + ks] >= 0 ? ul[vi2[n * 12 + ks]] : vo2[n * 12 + ks]) + sh2[n * 12 + ks];
                     }
                     char o2[6];
                     order2_correct<T>(ul[n], v, v2, NA, P.order2, o2);
@@ -544,8 +554,8 @@ struct Solver {
             const bool sd = P.seed[p] != 0;
             if (!sd) {
                 P.stencil(p, wts, e);
-                T v[6], sh[12];
-                P.shifts(x, p, e, sh);
+                T v[6], sh[12], sh2[12];
+                P.shifts(x, p, e, sh, sh2);
                 bool hid[12];
                 for (int k = 0; k < NA; ++k) {
                     for (int s = 0; s < 2; ++s) {
@@ -566,7 +576,7 @@ struct Solver {
                     for (int k = 0; k < NA; ++k) {
                         int y[3];
                         for (int c = 0; c < D; ++c) y[c] = x[c] + 2 * (2 * side[k] - 1) * e[k][c];
-                        v2[k] = !hid[2 * k + side[k]] && P.inside(y) ? u[P.flat(y)] : inf<T>();
+                        v2[k] = (!hid[2 * k + side[k]] && P.inside(y) ? u[P.flat(y)] : inf<T>()) + sh2[2 * k + side[k]];
                     }
                     order2_correct<T>(u[p], v, v2, NA, P.order2, o2);
                     for (int k = 0; k < NA; ++k)

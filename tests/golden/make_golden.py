@@ -737,6 +737,18 @@ def make_cases():
     c["factoringRadius"] = 5.0
     c["multiprecision"] = True
     cases["riem3_factor_mp"] = c
+    # the second order scheme with source factorisation, and with multiprecision
+    for key in ("riem2_factor", "iso2_factor"):
+        c = {k: v for k, v in cases[key].items() if k not in ("tips", "sensitivity")}
+        c["order"] = 2
+        cases[key.replace("_factor", "_order2_factor")] = c
+    c = {k: v for k, v in cases["riem3_factor_mp"].items() if k != "multiprecision"}
+    c["order"] = 2
+    cases["riem3_order2_factor"] = c
+    for key in ("riem2_order2", "iso2_order2", "riem3_order2"):
+        c = {k: v for k, v in cases[key].items() if k not in ("tips", "sensitivity")}
+        c["multiprecision"] = True
+        cases[key + "_mp"] = c
     return cases
 
 
