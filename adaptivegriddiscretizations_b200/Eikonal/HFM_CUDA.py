@@ -459,9 +459,6 @@ class Interface:
         self.order = int(order)
         self.order2_threshold = 0.0
         if order == 2:
-            if self.multiprecision and self.factoringRadius:
-                raise NotImplementedError("the second order scheme with both multiprecision and source "
-                                          "factorization is not available in this build")
             self.order2_threshold = float(self.GetValue(  # _Kernel.py:310-314
                 "order2_threshold", 0.3,
                 help="Relative threshold on second order differences / first order difference,"

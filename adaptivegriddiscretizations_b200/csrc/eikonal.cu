@@ -816,6 +816,18 @@ __device__ __forceinline__ void dispatch(const Sched &S, int t, int ii, int e, i
         case V_RIEM3_4_O2MP:
             if constexpr ((VMASK >> V_RIEM3_4_O2MP) & 1) Visit<Tile<3, 4, 4, 4>, AGD_MODEL_RIEMANN, true, false, true, true>::run(S, I, ii, n_o, e, lane, us);
             break;
+        case V_ISO2_16_O2FMP:
+            if constexpr ((VMASK >> V_ISO2_16_O2FMP) & 1) Visit<Tile<2, 16, 16, 1>, AGD_MODEL_ISOTROPIC, true, true, true>::run(S, I, ii, n_o, e, lane, us);
+            break;
+        case V_RIEM2_8_O2FMP:
+            if constexpr ((VMASK >> V_RIEM2_8_O2FMP) & 1) Visit<Tile<2, 8, 8, 1>, AGD_MODEL_RIEMANN, true, true, true, true>::run(S, I, ii, n_o, e, lane, us);
+            break;
+        case V_ISO3_4_O2FMP:
+            if constexpr ((VMASK >> V_ISO3_4_O2FMP) & 1) Visit<Tile<3, 4, 4, 4>, AGD_MODEL_ISOTROPIC, true, true, true>::run(S, I, ii, n_o, e, lane, us);
+            break;
+        case V_RIEM3_4_O2FMP:
+            if constexpr ((VMASK >> V_RIEM3_4_O2FMP) & 1) Visit<Tile<3, 4, 4, 4>, AGD_MODEL_RIEMANN, true, true, true, true>::run(S, I, ii, n_o, e, lane, us);
+            break;
         case V_ISO2_16_F:
             if constexpr ((VMASK >> V_ISO2_16_F) & 1) Visit<Tile<2, 16, 16, 1>, AGD_MODEL_ISOTROPIC, false, true>::run(S, I, ii, n_o, e, lane, us);
             break;
@@ -993,12 +1005,13 @@ struct EikonalVisitor {
     static constexpr int kMinCtas =
         (VMASK & ((1ull << V_RIEM2_16) | (1ull << V_ISO2_16) | (1ull << V_ISO2_16_MP) | (1ull << V_ISO2_16_F) |
                   (1ull << V_ISO2_16_FMP) | (1ull << V_ISO2_16_O2F) | (1ull << V_ISO2_16_O2MP) |
+                  (1ull << V_ISO2_16_O2FMP) |
                   (1ull << V_ISO2_16_O2) | (1ull << V_RIEM2_16_W) | (1ull << V_DIAG2_16) |
                   (1ull << V_DIAG2_16_MP) | (1ull << V_DIAG2_16_F) | (1ull << V_DIAG2_16_O2)))      ? 4
         : (VMASK & ((1ull << V_RIEM3_4) | (1ull << V_RIEM3_4_MP) | (1ull << V_RIEM3_4_F) | (1ull << V_RIEM3_4_O2) |
                     (1ull << V_RIEM3_4_W) | (1ull << V_RAND3_4) | (1ull << V_RAND3_4_W) | (1ull << V_RAND3_4_MP) |
                     (1ull << V_RAND3_4_F) | (1ull << V_RAND3_4_O2) | (1ull << V_RIEM3_4_FMP) |
-                    (1ull << V_RIEM3_4_O2F) | (1ull << V_RIEM3_4_O2MP)))                          ? 5
+                    (1ull << V_RIEM3_4_O2F) | (1ull << V_RIEM3_4_O2MP) | (1ull << V_RIEM3_4_O2FMP))) ? 5
         : (VMASK & (kMpVariants | kFactorVariants | kOrder2Variants))                                ? 7
         : (VMASK & (1ull << V_RIEM2_8))                                                              ? 8
                                                                                                      : 9;
@@ -1018,7 +1031,8 @@ struct EikonalVisitor {
                                       (1ull << V_RIEM3_4_F) | (1ull << V_RIEM2_8_O2) | (1ull << V_RIEM3_4_O2) |
                                       (1ull << V_RIEM2_8_FMP) | (1ull << V_RIEM3_4_FMP) | kWallVariants |
                                       kRanderVariants | (1ull << V_RIEM2_8_O2F) | (1ull << V_RIEM3_4_O2F) |
-                                      (1ull << V_RIEM2_8_O2MP) | (1ull << V_RIEM3_4_O2MP);
+                                      (1ull << V_RIEM2_8_O2MP) | (1ull << V_RIEM3_4_O2MP) |
+                                      (1ull << V_RIEM2_8_O2FMP) | (1ull << V_RIEM3_4_O2FMP);
         if (VMASK & kMpVariants) mp_copy_kernel<<<(L.total_tiles + 7) / 8, 256, 0, st>>>(S, 0);
         if (!(VMASK & kRiemann) || L.stencil == L.total) return cudaGetLastError();
         // variants that read the hidden-neighbour bits: the walls pass follows
@@ -1026,13 +1040,13 @@ struct EikonalVisitor {
                                           (1ull << V_RIEM2_8_F) | (1ull << V_RIEM3_4_F) | (1ull << V_RIEM2_8_O2) |
                                           (1ull << V_RIEM3_4_O2) | (1ull << V_RIEM2_8_FMP) | (1ull << V_RIEM3_4_FMP) |
                                           (1ull << V_RIEM2_8_O2F) | (1ull << V_RIEM3_4_O2F) | (1ull << V_RIEM2_8_O2MP) |
-                                          (1ull << V_RIEM3_4_O2MP) |
+                                          (1ull << V_RIEM3_4_O2MP) | (1ull << V_RIEM2_8_O2FMP) | (1ull << V_RIEM3_4_O2FMP) |
                                           (kRanderVariants & ~((1ull << V_RAND2_8) | (1ull << V_RAND3_4)));
         const unsigned grid = (L.total_tiles + 7) / 8;
         if (VMASK & ((1ull << V_RIEM3_4) | (1ull << V_RIEM3_4_MP) | (1ull << V_RIEM3_4_F) | (1ull << V_RIEM3_4_O2) |
                      (1ull << V_RIEM3_4_W) | (1ull << V_RAND3_4) | (1ull << V_RAND3_4_W) | (1ull << V_RAND3_4_MP) |
                      (1ull << V_RAND3_4_F) | (1ull << V_RAND3_4_O2) | (1ull << V_RIEM3_4_FMP) |
-                     (1ull << V_RIEM3_4_O2F) | (1ull << V_RIEM3_4_O2MP))) {
+                     (1ull << V_RIEM3_4_O2F) | (1ull << V_RIEM3_4_O2MP) | (1ull << V_RIEM3_4_O2FMP))) {
             stencil_kernel<3><<<grid, 256, 0, st>>>(S.inst, S.ninst, L.total_tiles, S.ctrl);
             if (VMASK & kWallCapable) stencil_walls_kernel<3><<<grid, 256, 0, st>>>(S.inst, S.ninst, L.total_tiles);
         } else {
@@ -1156,19 +1170,25 @@ static int run_variants(int ndim, unsigned long long vmask, const WsLayout &L, v
         if (mp) return run_sched<EikonalVisitor<DMP3 | D3>>(L, ws, n, {}, stats, cfg, st);
         return run_sched<EikonalVisitor<D3>>(L, ws, n, {}, stats, cfg, st);
     }
-    if (vmask & (kOrder2FactorVariants | kOrder2MpVariants)) {  // second order with factorisation or multiprecision
-        const bool f = vmask & kOrder2FactorVariants, mp = vmask & kOrder2MpVariants;
-        if ((f && mp) || (vmask & ~(kOrder2FactorVariants | kOrder2MpVariants)))
+    constexpr unsigned long long kO2Combined = kOrder2FactorVariants | kOrder2MpVariants | kOrder2FactorMpVariants;
+    if (vmask & kO2Combined) {  // second order with factorisation, multiprecision, or both
+        const bool f = vmask & kOrder2FactorVariants, mp = vmask & kOrder2MpVariants,
+                   fmp = vmask & kOrder2FactorMpVariants;
+        if (int(f) + int(mp) + int(fmp) > 1 || (vmask & ~kO2Combined))
             return set_error(AGD_STATUS_UNSUPPORTED,
                              "second order with factorisation or multiprecision beside other instances in one plan");
         constexpr unsigned long long OF2 = (1ull << V_ISO2_16_O2F) | (1ull << V_RIEM2_8_O2F);
         constexpr unsigned long long OF3 = (1ull << V_ISO3_4_O2F) | (1ull << V_RIEM3_4_O2F);
         constexpr unsigned long long OM2 = (1ull << V_ISO2_16_O2MP) | (1ull << V_RIEM2_8_O2MP);
         constexpr unsigned long long OM3 = (1ull << V_ISO3_4_O2MP) | (1ull << V_RIEM3_4_O2MP);
+        constexpr unsigned long long OFM2 = (1ull << V_ISO2_16_O2FMP) | (1ull << V_RIEM2_8_O2FMP);
+        constexpr unsigned long long OFM3 = (1ull << V_ISO3_4_O2FMP) | (1ull << V_RIEM3_4_O2FMP);
         if (ndim == 2) return f ? run_sched<EikonalVisitor<OF2>>(L, ws, n, {}, stats, cfg, st)
-                                : run_sched<EikonalVisitor<OM2>>(L, ws, n, {}, stats, cfg, st);
+                              : mp ? run_sched<EikonalVisitor<OM2>>(L, ws, n, {}, stats, cfg, st)
+                                   : run_sched<EikonalVisitor<OFM2>>(L, ws, n, {}, stats, cfg, st);
         return f ? run_sched<EikonalVisitor<OF3>>(L, ws, n, {}, stats, cfg, st)
-                 : run_sched<EikonalVisitor<OM3>>(L, ws, n, {}, stats, cfg, st);
+               : mp ? run_sched<EikonalVisitor<OM3>>(L, ws, n, {}, stats, cfg, st)
+                    : run_sched<EikonalVisitor<OFM3>>(L, ws, n, {}, stats, cfg, st);
     }
     if (vmask & kOrder2Variants) {  // second order instances, possibly beside plain ones
         constexpr unsigned long long O2 = (1ull << V_ISO2_8_O2) | (1ull << V_ISO2_16_O2) | (1ull << V_RIEM2_8_O2);

@@ -35,7 +35,9 @@ enum Variant {
     V_ISO2_16_FMP, V_RIEM2_8_FMP, V_ISO3_4_FMP, V_RIEM3_4_FMP,
     // second order scheme with source factorisation, and with multiprecision
     V_ISO2_16_O2F, V_RIEM2_8_O2F, V_ISO3_4_O2F, V_RIEM3_4_O2F,
-    V_ISO2_16_O2MP, V_RIEM2_8_O2MP, V_ISO3_4_O2MP, V_RIEM3_4_O2MP, V_COUNT
+    V_ISO2_16_O2MP, V_RIEM2_8_O2MP, V_ISO3_4_O2MP, V_RIEM3_4_O2MP,
+    // second order scheme with source factorisation and multiprecision
+    V_ISO2_16_O2FMP, V_RIEM2_8_O2FMP, V_ISO3_4_O2FMP, V_RIEM3_4_O2FMP, V_COUNT
 };
 static_assert(V_COUNT <= 64, "variant masks are 64-bit");
 constexpr unsigned long long kMpVariants = (1ull << V_ISO2_8_MP) | (1ull << V_ISO2_16_MP) | (1ull << V_RIEM2_8_MP) |
@@ -43,7 +45,9 @@ constexpr unsigned long long kMpVariants = (1ull << V_ISO2_8_MP) | (1ull << V_IS
                                  (1ull << V_DIAG2_16_MP) | (1ull << V_DIAG3_4_MP) | (1ull << V_RAND2_8_MP) |
                                  (1ull << V_RAND3_4_MP) | (1ull << V_ISO2_16_FMP) | (1ull << V_RIEM2_8_FMP) |
                                  (1ull << V_ISO3_4_FMP) | (1ull << V_RIEM3_4_FMP) | (1ull << V_ISO2_16_O2MP) |
-                                 (1ull << V_RIEM2_8_O2MP) | (1ull << V_ISO3_4_O2MP) | (1ull << V_RIEM3_4_O2MP);
+                                 (1ull << V_RIEM2_8_O2MP) | (1ull << V_ISO3_4_O2MP) | (1ull << V_RIEM3_4_O2MP) |
+                                 (1ull << V_ISO2_16_O2FMP) | (1ull << V_RIEM2_8_O2FMP) | (1ull << V_ISO3_4_O2FMP) |
+                                 (1ull << V_RIEM3_4_O2FMP);
 constexpr unsigned long long kFactorVariants = (1ull << V_ISO2_8_F) | (1ull << V_ISO2_16_F) | (1ull << V_RIEM2_8_F) |
                                      (1ull << V_ISO3_4_F) | (1ull << V_RIEM3_4_F) | (1ull << V_DIAG2_8_F) |
                                      (1ull << V_DIAG2_16_F) | (1ull << V_DIAG3_4_F) | (1ull << V_RAND2_8_F) |
@@ -53,12 +57,16 @@ constexpr unsigned long long kOrder2Variants = (1ull << V_ISO2_8_O2) | (1ull << 
                                      (1ull << V_DIAG2_16_O2) | (1ull << V_DIAG3_4_O2) | (1ull << V_RAND2_8_O2) |
                                      (1ull << V_RAND3_4_O2) | (1ull << V_ISO2_16_O2F) | (1ull << V_RIEM2_8_O2F) |
                                      (1ull << V_ISO3_4_O2F) | (1ull << V_RIEM3_4_O2F) | (1ull << V_ISO2_16_O2MP) |
-                                     (1ull << V_RIEM2_8_O2MP) | (1ull << V_ISO3_4_O2MP) | (1ull << V_RIEM3_4_O2MP);
-// second order with factorisation / with multiprecision
+                                     (1ull << V_RIEM2_8_O2MP) | (1ull << V_ISO3_4_O2MP) | (1ull << V_RIEM3_4_O2MP) |
+                                     (1ull << V_ISO2_16_O2FMP) | (1ull << V_RIEM2_8_O2FMP) |
+                                     (1ull << V_ISO3_4_O2FMP) | (1ull << V_RIEM3_4_O2FMP);
+// second order with factorisation / with multiprecision / with both
 constexpr unsigned long long kOrder2FactorVariants = (1ull << V_ISO2_16_O2F) | (1ull << V_RIEM2_8_O2F) |
                                            (1ull << V_ISO3_4_O2F) | (1ull << V_RIEM3_4_O2F);
 constexpr unsigned long long kOrder2MpVariants = (1ull << V_ISO2_16_O2MP) | (1ull << V_RIEM2_8_O2MP) |
                                        (1ull << V_ISO3_4_O2MP) | (1ull << V_RIEM3_4_O2MP);
+constexpr unsigned long long kOrder2FactorMpVariants = (1ull << V_ISO2_16_O2FMP) | (1ull << V_RIEM2_8_O2FMP) |
+                                             (1ull << V_ISO3_4_O2FMP) | (1ull << V_RIEM3_4_O2FMP);
 constexpr unsigned long long kWallVariants = (1ull << V_RIEM2_8_W) | (1ull << V_RIEM2_16_W) | (1ull << V_RIEM3_4_W) |
                                            (1ull << V_RAND2_8_W) | (1ull << V_RAND3_4_W);
 constexpr unsigned long long kDiagVariants = ((1ull << (V_DIAG3_4_O2 + 1)) - 1) & ~((1ull << V_DIAG2_8) - 1);
@@ -70,13 +78,12 @@ static int variant_of(const agd_instance &a) {
     const int v = base_variant_of(a);
     if (v >= 0 && a.order2_threshold > 0.f) {
         const bool mp = a.multip_step != 0.f, fact = a.factor_radius2 > 0.f;
-        if (mp && fact) return -1;  // not built
         if (mp || fact) {  // the default tile shapes
             switch (v) {
-                case V_ISO2_16: return mp ? V_ISO2_16_O2MP : V_ISO2_16_O2F;
-                case V_RIEM2_8: return mp ? V_RIEM2_8_O2MP : V_RIEM2_8_O2F;
-                case V_ISO3_4: return mp ? V_ISO3_4_O2MP : V_ISO3_4_O2F;
-                case V_RIEM3_4: return mp ? V_RIEM3_4_O2MP : V_RIEM3_4_O2F;
+                case V_ISO2_16: return mp && fact ? V_ISO2_16_O2FMP : mp ? V_ISO2_16_O2MP : V_ISO2_16_O2F;
+                case V_RIEM2_8: return mp && fact ? V_RIEM2_8_O2FMP : mp ? V_RIEM2_8_O2MP : V_RIEM2_8_O2F;
+                case V_ISO3_4: return mp && fact ? V_ISO3_4_O2FMP : mp ? V_ISO3_4_O2MP : V_ISO3_4_O2F;
+                case V_RIEM3_4: return mp && fact ? V_RIEM3_4_O2FMP : mp ? V_RIEM3_4_O2MP : V_RIEM3_4_O2F;
                 default: return -1;
             }
         }

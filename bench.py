@@ -32,7 +32,7 @@ METRIC = "solves/s, Riemann2 512x512 batched cold-start solves (grid-updates/s i
 
 
 # (grid, batch, tile, niter_i, fim_front_width) -> DRAM bytes per solver launch, measured
-MEASURED_TRAFFIC = {(512, 128, 8, 8, 4): 10.46e9 + 1.35e9}
+MEASURED_TRAFFIC = {(512, 128, 8, 8, 4): 9.539e9 + 1.197e9}
 
 
 def peaks():

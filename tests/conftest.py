@@ -37,9 +37,10 @@ CASES = ["iso2", "riem2", "riem2_aniso", "iso3", "riem3", "ad_notebook"]
 RADIUS_CASES = ["riem2_radius", "iso2_radius"]  # seeds spread over a radius (values only)
 FACTOR_CASES = ["riem2_factor", "iso2_factor"]  # source factorisation (factoringRadius)
 ORDER2_CASES = ["riem2_order2", "iso2_order2", "riem3_order2"]  # second order scheme (order: 2)
-# the second order scheme with source factorisation, and with multiprecision
+# the second order scheme with source factorisation, with multiprecision, and with both
 ORDER2_FACTOR_CASES = ["riem2_order2_factor", "iso2_order2_factor", "riem3_order2_factor"]
-ORDER2_MP_CASES = ["riem2_order2_mp", "iso2_order2_mp", "riem3_order2_mp"]
+ORDER2_MP_CASES = ["riem2_order2_mp", "iso2_order2_mp", "riem3_order2_mp",
+                   "riem2_order2_factor_mp", "iso2_order2_factor_mp", "riem3_order2_factor_mp"]
 WALL_CASES = ["riem2_walls", "iso2_walls", "riem3_walls"]  # obstacles (walls, wallDistBound)
 DIAG_CASES = ["diag2", "diag2_factor", "diag2_order2", "diag2_walls", "diag3"]  # Diagonal2/3 models
 RANDER_CASES = ["rand2", "rand2_factor", "rand2_order2", "rand2_walls", "rand3"]  # Rander2/3 (drift)

@@ -749,6 +749,10 @@ def make_cases():
         c = {k: v for k, v in cases[key].items() if k not in ("tips", "sensitivity")}
         c["multiprecision"] = True
         cases[key + "_mp"] = c
+    for key in ("riem2_order2_factor", "iso2_order2_factor", "riem3_order2_factor"):
+        c = dict(cases[key])
+        c["multiprecision"] = True
+        cases[key + "_mp"] = c
     return cases
 
 

@@ -42,16 +42,18 @@ def default_tolerances(case):
     return pr.atol, pr.rtol
 
 
-def assert_near_discrete(v, case, exact=None):
-    """Values of a solve at the case's stopping tolerances against the discrete solution."""
+def assert_near_discrete(v, case, exact=None, ntol=4.0, rel=REL):
+    """Values of a solve at the case's stopping tolerances against the discrete
+    solution: within ntol stopping tolerances everywhere, 99.9 % of the points
+    within rel relative."""
     exact = discrete_solution(case) if exact is None else exact
     v, exact = np.asarray(v, np.float64), np.asarray(exact, np.float64)
     fin = np.isfinite(exact)
     assert np.array_equal(fin, np.isfinite(v)), "finite masks differ"
     atol, rtol = default_tolerances(case)
     err = np.abs(v[fin] - exact[fin])
-    bound = 4.0 * (atol + rtol * np.abs(exact[fin]))
+    bound = ntol * (atol + rtol * np.abs(exact[fin]))
     worst = np.argmax(err / bound)
     assert (err <= bound).all(), f"{err[worst]:.3g} > {bound[worst]:.3g} at u = {exact[fin][worst]:.4g}"
     q = np.quantile(err / np.maximum(np.abs(exact[fin]), 1e-30), 0.999)
-    assert q <= REL, f"99.9% quantile of the relative error {q:.3g}"
+    assert q <= rel, f"99.9% quantile of the relative error {q:.3g}"

@@ -5,10 +5,12 @@ the cold solves of held-out instances, the cold solve being the judge.
 
 Checked: the trained network beats the constant predictor of the log-ratio
 (it learned something from the metric and the seeds); the judged results
-(warm, or cold where the warm one strays from it by more than the judge's
-tolerance) meet the parity criteria against the scheme's discrete solution on
-two instances, and few instances fall back; the release epochs are the ones
-of a numpy restatement (bit-exact).  The gain or
+(warm, or cold where the warm one strays from it by more than 8 stopping
+tolerances somewhere) are within what the judge guarantees of the scheme's
+discrete solution on two instances: 12 stopping tolerances everywhere (8 from
+the cold result, which is within 4), and 99.9 % of the points within 2e-5
+relative (twice the cold solves' bound); few instances fall back; the release
+epochs are the ones of a numpy restatement (bit-exact).  The gain or
 loss in solves/s over the cold solve is measured and reported, not asserted:
 the scheme revisits tiles mostly to converge to its tight stopping tolerance,
 which no activation schedule removes."""
@@ -64,4 +66,4 @@ def test_learned_warm_start_riemann2_512():
     for i in (0, 1):
         case = dict(model="Riemann2", dims=np.array([512, 512], np.float32), gridScales=np.full(2, 1 / 512, np.float32),
                     origin=np.zeros(2, np.float32), metric=mh[i], seeds=sh[i])
-        assert_near_discrete(warm[i], case, discrete_solution(case, nthreads=os.cpu_count()))
+        assert_near_discrete(warm[i], case, discrete_solution(case, nthreads=os.cpu_count()), ntol=12.0, rel=2e-5)

@@ -8,7 +8,8 @@ import numpy as np
 import pytest
 
 from oracle import oracle as O
-from conftest import load_case, CASES, DIAG_CASES, RADIUS_CASES, FACTOR_CASES, ORDER2_CASES, RANDER_CASES, WALL_CASES
+from conftest import (load_case, CASES, DIAG_CASES, RADIUS_CASES, FACTOR_CASES, ORDER2_CASES, ORDER2_MP_CASES,
+                      RANDER_CASES, WALL_CASES)
 
 REL = 1e-5  # parity bar for float32 values
 
@@ -235,13 +236,13 @@ def test_order2_factor_fixtures(name):
     assert rel.max() < REL
 
 
-@pytest.mark.parametrize("name", ["riem2_order2_mp", "iso2_order2_mp", "riem3_order2_mp"])
+@pytest.mark.parametrize("name", ORDER2_MP_CASES)
 def test_order2_multiprecision_fixtures(name):
-    """The reference's second order scheme with multiprecision against the
-    float64 oracle's second order solution.  The second order correction is not
+    """The reference's second order scheme with multiprecision (and with
+    factorisation too) against the float64 oracle's second order solution.  The second order correction is not
     monotone and values only decrease, so its fixed point depends on the order
     of the updates: the reference's own second order runs with and without
-    multiprecision differ by up to 4.1e-2 (mean 2.5e-3) on these cases, and by
+    multiprecision differ by up to 4.1e-2 (mean 2.8e-3) on these cases, and by
     as much from the oracle.  Hence the finite masks, max < 6e-2 and mean < 4e-3
     relative (the criterion of the second order values of a GPU solve)."""
     case, ref = load_case(name)
