@@ -215,6 +215,7 @@ struct LinearVisitor {
     // 200^3) are published in batches; the worker's registers stay within the
     // kMinCtas budget.
     static constexpr bool kBulkPublish = true;
+    static constexpr bool kBatchScheduling = false;
 
     __device__ static void visit(const Sched &S, const Args &A, int t, int ii, int e, int lane, Smem &sm) {
         const Inst &I = S.inst[ii];
@@ -356,7 +357,7 @@ struct LinearVisitor {
                 for (int j = r0[p]; j < r1[p]; ++j) {  // the points that depend on this one
                     const int ty = __ldg(A.src + j) / SIZE;
                     if (ty == n_o) self = true;
-                    else push_tile(S, I, ii, I.tile_base + ty, e);
+                    else push_tile<false>(S, I, ii, I.tile_base + ty, e);
                 }
             } else {
                 for (int k = 0; k < A.nact; ++k) {  // the points that depend on this one
@@ -365,12 +366,12 @@ struct LinearVisitor {
                     if (w == 0.f || y < 0 || (long long)y >= I.size_tot) continue;
                     const int ty = y / SIZE;
                     if (ty == n_o) self = true;
-                    else push_tile(S, I, ii, I.tile_base + ty, e);
+                    else push_tile<false>(S, I, ii, I.tile_base + ty, e);
                 }
             }
         }
         __syncwarp();
-        if (!settled && lane == 0) push_tile(S, I, ii, t, e);
+        if (!settled && lane == 0) push_tile<false>(S, I, ii, t, e);
         (void)self;
     }
 };

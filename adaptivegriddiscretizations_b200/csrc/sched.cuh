@@ -352,8 +352,11 @@ __device__ __forceinline__ int *list_of(const Sched &S, const Inst &I, int epoch
 // or, with release epochs, at its release epoch if that is later (at most
 // lmask epochs ahead).  The epoch a tile is pushed for never decreases, so the
 // epoch-stamped flag keeps one entry per tile and epoch.
+// BITMAP false: a visitor that never runs with bitmap pushes (its code stays
+// out of the visit).
+template <bool BITMAP = true>
 __device__ __forceinline__ void push_tile(const Sched &S, const Inst &I, int ii, int t, int e) {
-    if (S.bitmap) {  // a bit per tile and epoch: repeated pushes merge, and nothing waits for the result
+    if (BITMAP && S.bitmap) {  // a bit per tile and epoch: repeated pushes merge, and nothing waits for the result
         atomicOr(S.bits + (size_t)((unsigned)(e + 1) % 3u) * S.nwords + (t >> 5), 1u << (t & 31));
         return;
     }
@@ -627,6 +630,10 @@ __device__ __forceinline__ unsigned long long take_slot(const Sched &S, unsigned
 // Visitor::kMinCtas: resident 4-warp CTAs per SM that its register budget must allow.
 // Visitor::kBulkPublish: publish epochs with enqueue_warp<true> (more registers
 // in the worker loop, for visitors whose budget has them).
+// Visitor::kBatchScheduling: the worker may run launches of many instances with
+// the queue-slot prefetch, the ticket group taken ahead and bitmap pushes; a
+// visitor without it keeps the worker loop of one ticket ahead and list
+// pushes, and their registers (the linear visitor's budget has none to spare).
 constexpr int kSmemInst = 1024;  // instances whose tile bases a CTA keeps in shared memory
 
 // Decrement with release semantics (publishes this warp's writes); the warp
@@ -649,22 +656,26 @@ __global__ void __launch_bounds__(WPB * 32, Visitor::kMinCtas * 4 / WPB) sched_w
         for (int i = threadIdx.x; i < S.ninst; i += blockDim.x) s_base[i] = S.inst[i].tile_base;
     __syncthreads();
     if (ld_acquire_s32(&S.ctrl->active) == 0) return;  // nothing to solve
-    // Each warp holds queue tickets ahead: when a visit starts, the ticket of
-    // its next tile is already known, so the copy of that tile's queue slot
-    // (prefetch_slot) overlaps the visit, and the atomic on the head counter
-    // that takes the group after is issued one group ahead.  With tgroup 2 a
-    // warp takes two consecutive tickets per atomic: the head counter is a
-    // single address that every visit of the launch hits, and at ~250
-    // visits/us (a batch of 128 instances) its atomics are a bound.  A warp
-    // then visits two tiles of the queue in turn, which lengthens the tail of
-    // a small epoch: one instance alone solves 11 % slower that way, so
-    // launches of fewer than kPairInstances instances take one.  A warp holds
-    // at most 2 tgroup tickets (the exit sentinels of close_epoch cover them).
+    // Each warp holds one queue ticket ahead: the ticket for its next tile is
+    // taken when a visit starts, so the atomic's latency overlaps the visit.
+    // With tgroup 2 a warp takes two consecutive tickets per atomic: the head
+    // counter is a single address that every visit of the launch hits, and at
+    // ~250 visits/us (a batch of 128 instances) its atomics are a bound.  A
+    // warp then visits two tiles of the queue in turn, which lengthens the
+    // tail of a small epoch: one instance alone solves 11 % slower that way,
+    // so launches of fewer than kPairInstances instances take one.  Those of
+    // kPairInstances or more also hold the group after (its atomic issued a
+    // group ahead), so that the ticket of the next tile is known when a visit
+    // starts and the copy of its queue slot (prefetch_slot) overlaps the
+    // visit; a warp then holds up to 2 tgroup tickets (the exit sentinels of
+    // close_epoch cover them).  Few instances keep one ticket ahead: a tile
+    // held behind a busy warp lengthens their small epochs.
+    const bool ahead = Visitor::kBatchScheduling && S.tgroup > 1;
     unsigned ticket = 0, group = 0;
     int spare = 0;  // tickets of the group still ahead of `ticket`
     if (lane == 0) {
         ticket = atomicAdd(&S.ctrl->head, (unsigned)S.tgroup);
-        group = atomicAdd(&S.ctrl->head, (unsigned)S.tgroup);  // the next group
+        if (ahead) group = atomicAdd(&S.ctrl->head, (unsigned)S.tgroup);  // the next group
         spare = S.tgroup - 1;
     }
     bool prefetched = false;
@@ -679,14 +690,17 @@ __global__ void __launch_bounds__(WPB * 32, Visitor::kMinCtas * 4 / WPB) sched_w
             if (spare > 0) {
                 ticket += 1u;
                 --spare;
-            } else {
+            } else if (ahead) {
                 ticket = group;  // its atomic was issued a group ago
                 spare = S.tgroup - 1;
                 group = atomicAdd(&S.ctrl->head, (unsigned)S.tgroup);
+            } else {
+                ticket = atomicAdd(&S.ctrl->head, (unsigned)S.tgroup);
+                spare = S.tgroup - 1;
             }
-            prefetch_slot(S, ticket, s_pre[warp]);
+            if (ahead) prefetch_slot(S, ticket, s_pre[warp]);
         }
-        prefetched = true;
+        prefetched = ahead;
         int ii;
         if (inst_in_smem) {
             int lo = 0, hi = S.ninst - 1;
@@ -705,7 +719,7 @@ __global__ void __launch_bounds__(WPB * 32, Visitor::kMinCtas * 4 / WPB) sched_w
         lastone = __shfl_sync(kFull, lastone, 0);
         if (lastone) {
             fence_acq_rel();
-            if (S.bitmap) close_epoch_bitmap<Visitor::kBulkPublish>(S, ii, e, lane);
+            if (Visitor::kBatchScheduling && S.bitmap) close_epoch_bitmap<Visitor::kBulkPublish>(S, ii, e, lane);
             else close_epoch<Visitor::kBulkPublish>(S, ii, e, lane);
         }
     }
@@ -872,7 +886,7 @@ static int run_sched(const WsLayout &L, void *ws, int n, const typename Visitor:
     // wait for nothing, and an epoch is published in tile order.  A single
     // instance keeps the lists, whose push order (the front's) propagates
     // faster within an epoch when nothing else fills the GPU.
-    S.bitmap = (!Visitor::kBulkPublish && L.nlists == 2 && n >= kPairInstances) ? 1 : 0;
+    S.bitmap = (Visitor::kBatchScheduling && !Visitor::kBulkPublish && L.nlists == 2 && n >= kPairInstances) ? 1 : 0;
     char *w = static_cast<char *>(ws);
     cudaError_t err = cudaMemsetAsync(w + L.istate, 0, sizeof(InstState) * n, st);
     if (err == cudaSuccess) err = cudaMemsetAsync(w + L.flags, 0, L.queue - L.flags, st);
