@@ -362,6 +362,67 @@ def run_warm_start(args, peaks_tf):
     return res
 
 
+def run_iso256(args):
+    """The Isotropic2 256^2 configuration (one solve, tolerance 1e-6): solves/s
+    through `dictIn(...).Run()` with host numpy inputs and the values read back
+    (e2e: inputs copied in, preparation, solve, readback), the device time of
+    the same call by CUDA events, and the oracle on all host cores timed on the
+    same case (float32).  Parity: the largest relative difference of the GPU
+    values from the float64 oracle's discrete solution."""
+    import torch
+    from adaptivegriddiscretizations_b200 import Eikonal
+    from oracle import oracle as O
+    torch.cuda.set_device(0)
+    case = make_iso256(1)
+
+    def solve(traits=None):
+        d = dict(case, mode="gpu", verbosity=0, exportValues=True)
+        if traits is not None:
+            d["traits"] = traits
+        out = Eikonal.dictIn(d).Run()
+        return out["values"].cpu().numpy(), out["stats"]
+
+    def timed(traits=None):
+        for _ in range(max(3, args.warmup)):
+            solve(traits)
+        torch.cuda.synchronize()
+        walls, devs = [], []
+        for _ in range(args.steps):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            t0 = time.perf_counter()
+            e0.record()
+            v, stats = solve(traits)
+            e1.record()
+            torch.cuda.synchronize()
+            walls.append(time.perf_counter() - t0)
+            devs.append(e0.elapsed_time(e1) / 1e3)
+        return v, stats, float(np.median(walls)), float(np.median(devs))
+
+    v, _, t, tdev = timed()  # the reference's default traits (16x16 tiles, 16 local iterations)
+    _, st_auto, t_auto, tdev_auto = timed("auto")  # the autotuner's choice
+    exact = O.run(dict(case, atol=1e-14, rtol=1e-14), np.float64, nthreads=os.cpu_count() or 1)["values"]
+    pos = np.isfinite(exact) & (exact > 0)  # (the seed's value is 0)
+    err = float((np.abs(v[pos] - exact[pos]) / exact[pos]).max())
+    cores = os.cpu_count() or 1
+    t0 = time.perf_counter()
+    ncpu = 0
+    while ncpu < 3 or time.perf_counter() - t0 < 5.0:
+        r = O.run(case, np.float32, nthreads=cores)
+        ncpu += 1
+    tcpu = (time.perf_counter() - t0) / ncpu
+    print(json.dumps({"metric": "iso256 path", "value": 1.0 / tdev, "unit": "solves/s",
+                      "ms_per_step": 1e3 * tdev, "steps": args.steps, "warmup": args.warmup,
+                      "data": "synthetic", "dtype": "f32",
+                      "config": {"workload": "Isotropic2 256x256, cost exp(0.5 g) (g a sigma-8 Gaussian field), "
+                                             "one seed at the centre, tolerance 1e-6, one solve per step"},
+                      "e2e": {"value": 1.0 / t, "unit": "solves/s", "api": "dictIn(...).Run() from numpy inputs"},
+                      "max_rel_diff_vs_discrete": err,
+                      "traits_auto": {"solves_per_s": 1.0 / tdev_auto, "e2e_solves_per_s": 1.0 / t_auto,
+                                      "traits": st_auto.get("autotune", {}).get("traits")},
+                      "cpu_baseline": {"value": 1.0 / tcpu, "unit": "solves/s", "cores": cores, "kind": "port",
+                                       "sample": f"{ncpu} solves of the same case, float32"}}))
+
+
 def run_unet(args):
     """The learned warm start's network alone (`--path unet`): forward passes of
     a batch of 128 Riemann2 512^2 problems (128 x 128 blocks, 8 feature
@@ -465,9 +526,10 @@ def main():
     ap.add_argument("--niter-i", type=int, default=0, help="local iterations per tile visit (0: the default, 8)")
     ap.add_argument("--front", type=int, default=0, help="FIM front width (0: the default, 4)")
     ap.add_argument("--tile", type=int, default=8, help="tile side (8: the default, or 16)")
-    ap.add_argument("--path", default="solve", choices=["solve", "geodesic", "reverse", "unet"],
+    ap.add_argument("--path", default="solve", choices=["solve", "geodesic", "reverse", "unet", "iso256"],
                     help="solve: the benchmark (default); geodesic / reverse: the other kernels of the path; "
-                         "unet: the learned warm start's network")
+                         "unet: the learned warm start's network; iso256: the Isotropic2 256^2 configuration "
+                         "with the oracle timed beside it")
     ap.add_argument("--path-size", type=int, default=0,
                     help="grid side for --path (0: 1024 for geodesic, 200 for reverse; smaller for profiler captures)")
     ap.add_argument("--warm-train", type=int, default=20000, help="training solutions of the learned warm start")
@@ -486,6 +548,9 @@ def main():
         return
     if args.path == "unet":
         run_unet(args)
+        return
+    if args.path == "iso256":
+        run_iso256(args)
         return
     if args.path != "solve":
         run_other_path(args)
