@@ -66,8 +66,8 @@ class _Buffers:
 class SolverJob:
     """A batch submitted to a BatchSolver; `result()` waits for it."""
 
-    def __init__(self, solver, buf, out):
-        self.solver, self.buf, self.out = solver, buf, out
+    def __init__(self, solver, buf, out, dev_out=None):
+        self.solver, self.buf, self.out, self.dev_out = solver, buf, out, dev_out
         self.event = torch.cuda.Event()
         self.event.record(buf.stream)
         self.stream = buf.stream
@@ -79,8 +79,9 @@ class SolverJob:
 
     def result(self):
         """Values of the batch, shape (batch, *grid shape): the host buffer given to
-        submit(), else a device tensor that stays valid until this buffer set is
-        reused (after the solver's `nbuffers` next submissions)."""
+        submit(), else a device tensor: its own with submit(fresh_out=True), or
+        the buffer set's, valid until the set is reused (after the solver's
+        `nbuffers` next submissions)."""
         self.event.synchronize()
         if not self._done:
             self._done = True
@@ -99,7 +100,13 @@ class SolverJob:
                 if self.solver.raiseOnNonConvergence:
                     raise ValueError(msg)
                 warnings.warn(msg)
-        return self.out if self.out is not None else self.buf.out
+        if self.out is not None:
+            return self.out
+        if self.dev_out is not None:
+            # (made on the buffer set's stream: the caller's stream uses it from now on)
+            self.dev_out.record_stream(torch.cuda.current_stream())
+            return self.dev_out
+        return self.buf.out
 
 
 class BatchSolver:
@@ -273,11 +280,15 @@ class BatchSolver:
 
     # ----------------------------------------------------------------- submit --
     def submit(self, metric=None, cost=None, seeds=None, seedValues=None, out=None, release=None, values=None,
-               walls=None):
+               walls=None, fresh_out=False):
         """Queues one batch; returns a SolverJob.  out: optional host tensor
         (batch, *shape) float32 (page-locked for an asynchronous copy).
         walls: optional (batch, *shape) obstacle masks of the instances, in
         place of the template's (whose wall distances are made once).
+        fresh_out: the values go to a device tensor of this submission's own
+        (written by the reordering kernel right behind the solve), which stays
+        valid when the buffer set is reused: no copy is needed afterwards,
+        which would have to wait for the SMs behind the next batch's solve.
         release: optional device tensor (batch, tiles) of int16/uint16 tile
         release epochs (agd_instance.release; the learned schedule); values:
         optional device tensor (batch, tiles * tile size) of initial values in
@@ -364,8 +375,10 @@ class BatchSolver:
             lp = ctypes.byref(self.launch) if self.launch is not None else None
             _lib.check(L.agd_plan_run(buf.plan, _lib.ptr(buf.ws), buf.ws.numel(), _lib.ptr(buf.stats), lp, st),
                        "solve")
+            dev_out = torch.empty_like(buf.out) if fresh_out and out is None else None
+            target = dev_out if dev_out is not None else buf.out
             _lib.check(L.agd_block_squeeze(self.ndim, self.c_shape, self.c_shape_i, self.batch, _lib.ptr(buf.values),
-                                           _lib.ptr(buf.out), st), "block_squeeze")
+                                           _lib.ptr(target), st), "block_squeeze")
             buf.stats_host.copy_(buf.stats, non_blocking=True)
             buf.bad_host.copy_(buf.bad, non_blocking=True)
             if out is not None:
@@ -373,7 +386,7 @@ class BatchSolver:
             for t in keep:  # inputs read in place on this stream stay alive until it gets past them
                 if t.is_cuda:
                     t.record_stream(buf.stream)
-            job = SolverJob(self, buf, out)
+            job = SolverJob(self, buf, out, dev_out)
         buf.job = job
         self.submitted += 1
         return job

@@ -188,7 +188,7 @@ def _submit_uniform(hfmIns, launch):
                     dev[i].copy_(x, non_blocking=x.device.type == "cpu" and x.is_pinned() or x.is_cuda)
             inputs[k] = dev
     job = solver.submit(metric=inputs.get("metric"), cost=inputs.get("cost"), seeds=inputs["seeds"],
-                        seedValues=inputs.get("seedValues"))
+                        seedValues=inputs.get("seedValues"), fresh_out=export)
     return UniformBatchJob(job, keys, export, B)
 
 
@@ -207,9 +207,9 @@ class UniformBatchJob:
     def result(self):
         if self._outs is not None:
             return self._outs
-        values = self.job.result()
-        with torch.cuda.stream(self.stream):
-            values = values.clone() if self.export else None  # the solver's buffer is reused
+        values = self.job.result()  # the submission's own tensor when exported (fresh_out)
+        if not self.export:
+            values = None
         outs = []
         for i in range(self.n):
             keys = {k: (list(v) if isinstance(v, list) else OrderedDict(v) if isinstance(v, dict) else v)
