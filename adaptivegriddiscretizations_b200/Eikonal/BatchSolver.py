@@ -262,8 +262,9 @@ class BatchSolver:
         if isinstance(seeds, torch.Tensor) and seeds.is_cuda:
             if seeds.dim() != 3 or seeds.shape[0] != self.batch or seeds.shape[2] != self.ndim:
                 raise ValueError(f"seeds must have shape (batch, nseeds, {self.ndim})")
-            start = torch.as_tensor(self.start, device="cuda")
-            h = torch.as_tensor(self.h, device="cuda")
+            if getattr(self, "_start_h", None) is None:  # made once: a copy from host memory blocks the host
+                self._start_h = (torch.as_tensor(self.start, device="cuda"), torch.as_tensor(self.h, device="cuda"))
+            start, h = self._start_h
             return torch.round((seeds.float() - start) / h).to(torch.int32).contiguous()  # checked on the device
         s = seeds.numpy() if isinstance(seeds, torch.Tensor) else np.asarray(seeds, np.float32)
         s = s.astype(np.float32, copy=False)
