@@ -8,7 +8,7 @@ layer runs on the tensor cores or in memory-bound kernels of libagd_b200
 (include/agd_warmstart.h).  `WarmStart` (warmstart.py) generates training
 data with the solver itself, trains the network on the GPU and turns its
 predictions into per-tile release epochs and warm-start values for batched
-solves, with the cold solve as the judge and fallback.
+solves, with the cold solve as the check and fallback.
 """
 from .unet import UNet  # noqa: F401
 

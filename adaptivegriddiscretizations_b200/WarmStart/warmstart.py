@@ -12,7 +12,7 @@ which the predicted front reaches them) and, optionally, warm-start values
 (agd_ws_warm_values: (1 + margin) T, an upper bound where the prediction is
 good, since the scheme's values only decrease).  The solver still runs to the
 reference's stopping test, so the fixed point is the one of the cold start up
-to the stopping tolerance.  The cold solve is the judge: evaluate() compares
+to the stopping tolerance.  The cold solve is the check: evaluate() compares
 every warm result with the cold one and counts the instances that would fall
 back to it.
 """
@@ -180,7 +180,7 @@ class WarmStart:
         torch.cuda.synchronize()
         return out, e0.elapsed_time(e1) / 1e3 + t_solve, visits
 
-    def judge(self, warm, cold, tol_factor=8.0):
+    def fallback_mask(self, warm, cold, tol_factor=8.0):
         """Instances (batch,) whose warm values differ from the cold ones by more
         than tol_factor stopping tolerances somewhere: they fall back to the
         cold result.  Two solves that each meet the parity criteria (within 4
@@ -193,13 +193,13 @@ class WarmStart:
         bad |= torch.isfinite(warm) != fin
         return bad.reshape(B, -1).any(1)
 
-    def judged_solve(self, metric, seeds, margin=None, tol_factor=8.0):
-        """The warm solve with the cold solve as judge and fallback: values
+    def checked_solve(self, metric, seeds, margin=None, tol_factor=8.0):
+        """The warm solve with the cold solve as check and fallback: values
         (batch, n, n) (device tensor) and the fallback mask (batch,)."""
         cold, _, _ = self.solve(metric, seeds)
         cold = cold.clone()
         warm, _, _ = self.warm_solve(metric, seeds, margin=margin)
-        bad = self.judge(warm, cold, tol_factor)
+        bad = self.fallback_mask(warm, cold, tol_factor)
         return torch.where(bad.reshape(-1, *([1] * (cold.dim() - 1))), cold, warm), bad
 
     def tune(self, metric, seeds, candidates=(100.0, 130.0, 160.0, 200.0, 260.0)):
@@ -242,7 +242,7 @@ class WarmStart:
             diff = (warm - cold).abs()
             rel = torch.where(fin, diff / cold.abs().clamp_min(1e-30), torch.zeros_like(diff))
             worst = max(worst, float(rel.max()))
-            fallbacks += int(self.judge(warm, cold, tol_factor).sum())
+            fallbacks += int(self.fallback_mask(warm, cold, tol_factor).sum())
             done += B
         return {"instances": done, "cold_solves_per_s": done / t_cold, "warm_solves_per_s": done / t_warm,
                 "gain": t_cold / t_warm, "cold_tile_visits": v_cold, "warm_tile_visits": v_warm,

@@ -1,12 +1,12 @@
 """The learned warm start end to end on the GPU (Riemann2 512^2, the
 configuration of the benchmark): solver-generated training data, training of
 the U-Net by the tensor-core kernels, and the warm (learned schedule) against
-the cold solves of held-out instances, the cold solve being the judge.
+the cold solves of held-out instances, the cold solve being the check.
 
 Checked: the trained network beats the constant predictor of the log-ratio
-(it learned something from the metric and the seeds); the judged results
+(it learned something from the metric and the seeds); the checked results
 (warm, or cold where the warm one strays from it by more than 8 stopping
-tolerances somewhere) are within what the judge guarantees of the scheme's
+tolerances somewhere) are within what that check guarantees of the scheme's
 discrete solution on two instances: 12 stopping tolerances everywhere (8 from
 the cold result, which is within 4), and 99.9 % of the points within 2e-5
 relative (twice the cold solves' bound); few instances fall back; the release
@@ -57,9 +57,9 @@ def test_learned_warm_start_riemann2_512():
     res = ws.evaluate(128, torch.Generator(device="cuda").manual_seed(11))
     print("learned warm start:", {k: v for k, v in res.items()})
     assert res["fallbacks"] <= 4, res
-    # parity of the judged results against the discrete solution, two held-out instances
+    # parity of the checked results against the discrete solution, two held-out instances
     m, s = riemann2_fields(512, 64, torch.Generator(device="cuda").manual_seed(12))
-    warm, fallback = ws.judged_solve(m, s)
+    warm, fallback = ws.checked_solve(m, s)
     assert int(fallback.sum()) <= 4, fallback
     warm = warm.cpu().numpy()
     mh, sh = m.cpu().numpy(), s.cpu().numpy()
