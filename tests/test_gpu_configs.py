@@ -77,6 +77,42 @@ def test_riemann2_1024_with_64_tips():
             assert np.min(np.linalg.norm(seeds - g[:, -1], axis=1)) < 8.0 / n
 
 
+def test_riemann2_1024_geodesics_from_oracle_values():
+    """The flow and geodesic kernels on the oracle's own float32 values of the
+    Riemann2 1024^2 configuration (the solve replaced by them): all 64 stop
+    codes are the oracle's, the paths within 1.5 grid steps of its paths and
+    their lengths within 2 % (the oracle's threads update in an order that
+    moves its values by a few 1e-6, and a path's last steps with them).  The
+    stop codes that differ in the end-to-end test above come from the last
+    bits of the solved values, not from the flow or the ODE."""
+    import ctypes
+    from oracle import oracle as O
+    from adaptivegriddiscretizations_b200 import Eikonal, _lib
+    from adaptivegriddiscretizations_b200.Eikonal.HFM_CUDA import Interface
+    n = 1024
+    case = _riemann2(n, 21)
+    tips = np.random.default_rng(22).uniform(0.02, 0.98, (64, 2)).astype(np.float32)
+    ref = O.run(dict(case, tips=tips), np.float32, nthreads=os.cpu_count())
+    itf = Interface(Eikonal.dictIn(dict(case, mode="gpu", verbosity=0, tips=tips)))
+    itf.SetKernelTraits()
+    itf.SetGeometry()
+    itf.SetArgs()
+    v = torch.as_tensor(np.ascontiguousarray(ref["values"], np.float32), device="cuda").reshape(-1)
+    _lib.check(_lib.lib().agd_block_expand(itf.ndim, itf.c_shape, itf.c_shape_i, 1, _lib.ptr(v), 0,
+                                           ctypes.c_float(float("inf")), _lib.ptr(itf.values_t), itf.stream))
+    itf.PostProcess()
+    itf.GetGeodesics()
+    assert list(itf.hfmOut["geodesic_stopping_criteria"]) == [str(s) for s in ref["geodesic_stopping_criteria"]]
+    dev, dlen = [], []
+    for g, w in zip(itf.hfmOut["geodesics"], ref["geodesics"]):
+        g = g.cpu().numpy()
+        m = min(g.shape[1], w.shape[1])
+        dev.append(np.abs(g[:, :m] - w[:, :m]).max())
+        dlen.append(abs(g.shape[1] - w.shape[1]) / w.shape[1])
+    print("path deviation", max(dev) * n, "grid steps; length difference", max(dlen))
+    assert max(dev) < 1.5 / n and max(dlen) < 0.02
+
+
 def _riemann3_200(seed):
     from scipy.ndimage import gaussian_filter
     n = 200
