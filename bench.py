@@ -714,8 +714,10 @@ def main():
                 collect(job)
                 job = nxt
 
-        run_dictin(2)
+        run_dictin(2)  # (its first SubmitBatch prepares the cached solver of the configuration)
         torch.cuda.synchronize()
+        gc.collect()  # the objects made since the first freeze, out of the scans too
+        gc.freeze()
         if dist:
             dist.barrier()
         t_e = time.perf_counter()
