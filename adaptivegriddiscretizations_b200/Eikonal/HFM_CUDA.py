@@ -112,6 +112,43 @@ def _option(h, k):
     return ("value", repr(v))
 
 
+_SCALARS = (bool, int, float, str, type(None))
+
+
+def _eq(x, y):
+    """x == y for scalars of one type, with repr's float identity: -0.0 is
+    not 0.0, and NaN is NaN."""
+    if type(x) is float:
+        return (x == y and math.copysign(1.0, x) == math.copysign(1.0, y)) or (x != x and y != y)
+    return x == y
+
+
+def _same_option(a, b):
+    """True or False when a and b (raw option values of two dictIn) are
+    scalars, lists/tuples of scalars of the same types element by element, or
+    small numpy arrays: their equality, as _option's comparison would give it
+    without building its host forms; None for anything else (compare by
+    _option)."""
+    if a is b:
+        return True
+    ta = type(a)
+    if ta in _SCALARS:
+        return ta is type(b) and _eq(a, b)
+    if ta is np.ndarray:  # small host arrays (dims, gridScale, origin after SetRect): their bytes
+        if type(b) is not np.ndarray or a.size > 64:
+            return None
+        return a.shape == b.shape and a.dtype.str == b.dtype.str and a.tobytes() == b.tobytes()
+    if ta in (list, tuple) and type(b) is ta and len(a) == len(b):
+        for x, y in zip(a, b):
+            tx = type(x)
+            if tx not in _SCALARS or tx is not type(y):
+                return None
+            if not _eq(x, y):
+                return False
+        return True
+    return None
+
+
 def _submit_uniform(hfmIns, launch):
     """The batched preparation path of SubmitBatch, or None when the dictIn do
     not qualify."""
@@ -137,9 +174,16 @@ def _submit_uniform(hfmIns, launch):
     opt0 = tuple(_option(h0, k) for k in opts)
     if any(o is None for o in opt0):
         return None
+    raw0 = [h0.raw(k) for k in opts]
     for h in hfmIns[1:]:
-        if set(h.keys()) != keys0 or tuple(_option(h, k) for k in opts) != opt0:
+        if set(h.keys()) != keys0:
             return None
+        for k, r0, o0 in zip(opts, raw0, opt0):
+            same = _same_option(h.raw(k), r0)
+            if same is None:
+                same = _option(h, k) == o0
+            if not same:
+                return None
         for k in arrays:
             x = h.raw(k)
             if not isinstance(x, (np.ndarray, torch.Tensor)) or tuple(x.shape) != shapes[k]:

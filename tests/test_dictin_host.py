@@ -35,3 +35,37 @@ def test_large_fields_keep_no_host_copy():
     t = torch.zeros(3)
     d["origin"] = t
     assert np.allclose(d.host("origin"), 0)
+
+
+def test_uniform_batch_option_comparison():
+    """SubmitBatch's check that dictIn differ only in their data compares the
+    scalar and short-list options directly; it must agree with the comparison
+    of their host forms (_option) wherever it answers."""
+    from adaptivegriddiscretizations_b200.Eikonal.HFM_CUDA import _option, _same_option
+
+    class Store:
+        def __init__(self, v):
+            self.v = v
+
+        def raw(self, k):
+            return self.v
+
+        def host(self, k):
+            return np.asarray(self.v)
+
+    vals = [1, 1.0, 0.5, True, False, None, "Riemann2", "gpu", [512, 512], [512.0, 512.0], (0.0, 0.0), [0.0, 0.0],
+            [np.float32(1), 2], [1, 2, 3], [float("nan")], float("nan"), -0.0, 0.0, [-0.0, 0.0], {"a": 1},
+            np.array([1.0, 2.0]), np.array([1.0, 2.0], np.float32), np.array([512, 512]), np.array([-0.0, 0.0]),
+            np.array([0.0, 0.0]), np.array([[1.0, 2.0]])]
+    answered = 0
+    for a in vals:
+        for b in vals:
+            r = _same_option(a, b)
+            if r is None:
+                continue
+            answered += 1
+            assert r == (_option(Store(a), "k") == _option(Store(b), "k")), (a, b)
+    assert answered > 200
+    assert _same_option([0.0, 1.0], [0.0, 1.0]) and not _same_option([0.0, 1.0], [0.0, 2.0])
+    assert _same_option(np.zeros(65), np.zeros(65)) is None  # larger arrays: compared by _option
+    assert _same_option(torch.zeros(2), torch.zeros(2)) is None
